@@ -1,15 +1,1319 @@
+/* Oracle: hand-written CPU restatement of the reference's CM1 dynamics kernels.
+ * TEST INFRASTRUCTURE ONLY (see oracle.h).  Each kernel cites the WGSL file of the
+ * reference (data/kernels/<name>.wgsl, main() body) whose arithmetic it restates, in
+ * the same operation order: every binary32 operation rounds once, fmaf() exactly where
+ * the reference writes fma, IEEE division (the reference's div_cr is a correctly
+ * rounded division, adv_flux_x_weno.wgsl:29-50, restated as te_div_cr below).
+ * Build: oracle/Makefile (-ffp-contract=off, no fast-math, -fwrapv).
+ */
 #include "oracle.h"
-#include <xmmintrin.h>
+
+#include <math.h>
 #include <omp.h>
-uint32_t te_fnv1a(const uint32_t* w, size_t n) {
+#include <string.h>
+#include <xmmintrin.h>
+
+/* ------------------------------------------------------------------ utilities */
+
+uint32_t te_fnv1a(const uint32_t *w, size_t n) {
+  /* FNV-1a over u32 words (web/view.js:1063-1068) */
   uint32_t h = 0x811c9dc5u;
   for (size_t i = 0; i < n; i++) h = (h ^ w[i]) * 0x01000193u;
   return h;
 }
-/* Flush-to-zero + denormals-are-zero on every OpenMP worker and the caller. */
+
 void te_set_ftz(int on) {
+  /* flush-to-zero + denormals-are-zero on every OpenMP worker and on the caller */
   unsigned bits = 0x8000u | 0x0040u;
 #pragma omp parallel
-  { unsigned c = _mm_getcsr(); _mm_setcsr(on ? (c | bits) : (c & ~bits)); }
-  unsigned c = _mm_getcsr(); _mm_setcsr(on ? (c | bits) : (c & ~bits));
+  {
+    unsigned c = _mm_getcsr();
+    _mm_setcsr(on ? (c | bits) : (c & ~bits));
+  }
+  unsigned c = _mm_getcsr();
+  _mm_setcsr(on ? (c | bits) : (c & ~bits));
+}
+
+static inline uint32_t fbits(float x) { uint32_t u; memcpy(&u, &x, 4); return u; }
+static inline float bitsf(uint32_t u) { float x; memcpy(&x, &u, 4); return x; }
+
+/* div_core / div_cr (adv_flux_x_weno.wgsl:29-50): quotient, then up to four
+ * neighbour corrections by exact fma residual; tiny numerators are scaled by 2^64. */
+static float div_core(float a, float b) {
+  float q0 = a / b;
+  int special = q0 == 0.0f || fabsf(q0) > 3.0e38f || q0 != q0 || fabsf(q0) < 1.0e-37f;
+  float q = q0;
+  float r = fabsf(fmaf(-q, b, a));
+  for (int k = 0; k < 4; k++) {
+    float qu = bitsf(fbits(q) + 1u);
+    float qd = bitsf(fbits(q) - 1u);
+    float ru = fabsf(fmaf(-qu, b, a));
+    float rd = fabsf(fmaf(-qd, b, a));
+    int up = ru < r;
+    int dn = !up && rd < r;
+    q = up ? qu : (dn ? qd : q);
+    r = up ? ru : (dn ? rd : r);
+  }
+  return special ? q0 : q;
+}
+
+float te_div_cr(float a, float b) {
+  int small = fabsf(a) < 8.67361738e-19f && a != 0.0f;
+  float q = div_core(small ? a * 1.8446744e19f : a, b);
+  return small ? q * 5.42101086e-20f : q;
+}
+#define DCR te_div_cr
+
+/* sqrt_core / sqrt_cr (adv_flux_x_weno.wgsl:53-71) */
+static float sqrt_core(float x) {
+  float s = sqrtf(x);
+  if (!(x > 1.0e-30f) || x > 3.0e38f) return s;
+  for (int k = 0; k < 4; k++) {
+    float r = fmaf(-s, s, x);
+    float su = bitsf(fbits(s) + 1u);
+    float sd = bitsf(fbits(s) - 1u);
+    if (r > s * (su - s)) s = su;
+    else if (r <= -(s * (s - sd))) s = sd;
+    else break;
+  }
+  return s;
+}
+
+float te_sqrt_cr(float x) {
+  if (x < 8.67361738e-19f && x > 0.0f) return sqrt_core(x * 1.8446744e19f) * 2.32830644e-10f;
+  return sqrt_core(x);
+}
+
+/* WGSL min/max on f32 (the reference maps them to IEEE minNum/maxNum) */
+static inline float fmin_(float a, float b) { return fminf(a, b); }
+static inline float fmax_(float a, float b) { return fmaxf(a, b); }
+
+/* --------------------------------------------------------------- grid access */
+
+typedef struct {
+  int nx, ny, nz, sJ, sK;
+  float rdx, rdy, rdz;
+} Dims;
+
+static Dims dims_at(const uint32_t *M, uint32_t off) {
+  /* GridDims (timestep.js:88-90; ld_GridDims in every kernel) */
+  Dims g;
+  g.nx = (int)M[off + 0];
+  g.ny = (int)M[off + 1];
+  g.nz = (int)M[off + 2];
+  g.sJ = (int)M[off + 3];
+  g.sK = (int)M[off + 4];
+  g.rdx = bitsf(M[off + 5]);
+  g.rdy = bitsf(M[off + 6]);
+  g.rdz = bitsf(M[off + 7]);
+  return g;
+}
+
+typedef struct {
+  float dts, alph, beta, kdiv, smeps;
+} Acoustic;
+
+static Acoustic acoustic_at(const uint32_t *M, uint32_t off) {
+  /* AcousticParamsGPU (timestep.js:46-52) */
+  Acoustic a;
+  a.dts = bitsf(M[off + 0]);
+  a.alph = bitsf(M[off + 1]);
+  a.beta = bitsf(M[off + 2]);
+  a.kdiv = bitsf(M[off + 3]);
+  a.smeps = bitsf(M[off + 4]);
+  return a;
+}
+
+#define B(n) (ARG[4 + (n)])
+#define FPTR(n) ((float *)(M + B(n)))
+#define FVAL(n) (bitsf(M[B(n)]))
+#define IVAL(n) ((int32_t)M[B(n)])
+#define GIDX(g, i, j, k) (((i) + 3) + (g).sJ * (((j) + 3) + (g).sK * (k)))
+#define CP_ 1005.7f
+
+/* horizontal metric planes (grid.js:200-214; f_hm_* helpers of the kernels) */
+static inline float hm_uh(const Dims *g, const float *hm, int i) { return hm[i + 3]; }
+static inline float hm_uf(const Dims *g, const float *hm, int i) { return hm[g->sJ + i + 3]; }
+static inline float hm_vh(const Dims *g, const float *hm, int j) { return hm[2 * g->sJ + j + 3]; }
+static inline float hm_vf(const Dims *g, const float *hm, int j) { return hm[2 * g->sJ + g->sK + j + 3]; }
+
+/* loop over the dispatch grid in threads (ARG[0..2]) */
+#define FOR_GRID                                                   \
+  const long GX = ARG[0], GY = ARG[1], GZ = ARG[2];                \
+  _Pragma("omp parallel for collapse(2) schedule(static)")          \
+  for (long tz = 0; tz < GZ; tz++)                                  \
+    for (long ty = 0; ty < GY; ty++)                                \
+      for (long tx = 0; tx < GX; tx++)
+
+/* --------------------------------------------------------- reconstructions */
+
+/* f_flx5 (adv_flux_x.wgsl:106-143): 5th-order upwind-biased (2,-13,47,27,-3)/60 */
+static inline float flx5(float s1, float s2, float s3, float s4, float s5) {
+  return fmaf(DCR(-3.0f, 60.0f), s5,
+              fmaf(DCR(27.0f, 60.0f), s4, fmaf(DCR(47.0f, 60.0f), s3, fmaf(DCR(2.0f, 60.0f), s1, DCR(-13.0f, 60.0f) * s2))));
+}
+
+/* f_flx3 (adv_flux_z.wgsl:106-113): 3rd-order (-1,5,2)/6 */
+static inline float flx3(float s1, float s2, float s3) {
+  return fmaf(DCR(2.0f, 6.0f), s3, fmaf(DCR(-1.0f, 6.0f), s1, DCR(5.0f, 6.0f) * s2));
+}
+
+/* f_weno5 (adv_flux_x_weno.wgsl:121-151): WENO-JS with clipped ratios */
+float te_weno5(float s1, float s2, float s3, float s4, float s5, float weps) {
+  const float c13 = DCR(13.0f, 12.0f);
+  float e1 = fmaf(-2.0f, s2, s1) + s3;
+  float d1 = fmaf(3.0f, s3, fmaf(-4.0f, s2, s1));
+  float b1 = fmaf(c13 * e1, e1, (0.25f * d1) * d1);
+  float e2 = fmaf(-2.0f, s3, s2) + s4;
+  float d2 = s2 - s4;
+  float b2 = fmaf(c13 * e2, e2, (0.25f * d2) * d2);
+  float e3 = fmaf(-2.0f, s4, s3) + s5;
+  float d3 = fmaf(3.0f, s3, -(4.0f * s4)) + s5;
+  float b3 = fmaf(c13 * e3, e3, (0.25f * d3) * d3);
+  float tau = fabsf(b1 - b3);
+  float r1 = fmin_(1e30f, DCR(tau, b1 + weps));
+  float r2 = fmin_(1e30f, DCR(tau, b2 + weps));
+  float r3 = fmin_(1e30f, DCR(tau, b3 + weps));
+  float m = fmax_(r1, fmax_(r2, r3));
+  float one = 1.0f;
+  if (m > 1e15f) {
+    float im = DCR(1.0f, m);
+    r1 = r1 * im;
+    r2 = r2 * im;
+    r3 = r3 * im;
+    one = im * im;
+  }
+  float w1 = 0.1f * fmaf(r1, r1, one);
+  float w2 = 0.6f * fmaf(r2, r2, one);
+  float w3 = 0.3f * fmaf(r3, r3, one);
+  float p1 = fmaf(DCR(11.0f, 6.0f), s3, fmaf(DCR(2.0f, 6.0f), s1, DCR(-7.0f, 6.0f) * s2));
+  float p2 = fmaf(DCR(2.0f, 6.0f), s4, fmaf(DCR(-1.0f, 6.0f), s2, DCR(5.0f, 6.0f) * s3));
+  float p3 = fmaf(DCR(-1.0f, 6.0f), s5, fmaf(DCR(2.0f, 6.0f), s3, DCR(5.0f, 6.0f) * s4));
+  return DCR(fmaf(w3, p3, fmaf(w1, p1, w2 * p2)), (w1 + w2) + w3);
+}
+#define WENO te_weno5
+
+/* f_weno_pdef_ok (adv_flux_x_weno.wgsl:106-119) */
+static inline int weno_pdef_ok(float s1, float s2, float s3, float s4, float s5, float weps, int pdef) {
+  if (!pdef) return 1;
+  float bmax = fmax_(fmax_(fmax_(fabsf(s1), fabsf(s2)), fmax_(fabsf(s3), fabsf(s4))), fabsf(s5));
+  return bmax > weps;
+}
+
+/* f_upstrpd (adv_flux_z_weno.wgsl:111-120): 3rd-order limited upstream value */
+static inline float upstrpd(float s1, float s2, float s3, float weps) {
+  float dd = s2 - s1;
+  float sgn = bitsf((fbits(weps) & 0x7fffffffu) | (fbits(dd) & 0x80000000u));
+  float rr = DCR(s3 - s2, sgn + dd);
+  float phi = fmax_(0.0f, fmin_(rr, fmin_(fmaf(DCR(2.0f, 6.0f), rr, DCR(1.0f, 6.0f)), 1.0f)));
+  return fmaf(phi, s2 - s1, s2);
+}
+
+/* ------------------------------------------------- linear upwind fluxes (RK 1-2) */
+
+static void flux_lin_h(uint32_t *M, const uint32_t *ARG, int dir) {
+  /* adv_flux_x.wgsl / adv_flux_y.wgsl main: f = rr * flx5(upwind stencil) */
+  Dims g = dims_at(M, B(0));
+  const float *s = FPTR(1), *rr = FPTR(2);
+  float *fo = FPTR(3);
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (dir == 0 ? (i > g.nx || j >= g.ny || k >= g.nz) : (i >= g.nx || j > g.ny || k >= g.nz)) continue;
+    int c = GIDX(g, i, j, k);
+    int d = dir == 0 ? 1 : g.sJ;
+    float u = rr[c];
+    float f = u >= 0.0f ? flx5(s[c - 3 * d], s[c - 2 * d], s[c - d], s[c], s[c + d])
+                        : flx5(s[c + 2 * d], s[c + d], s[c], s[c - d], s[c - 2 * d]);
+    fo[c] = u * f;
+  }
+}
+void teor_adv_flux_x(uint32_t *M, const uint32_t *ARG) { flux_lin_h(M, ARG, 0); }
+void teor_adv_flux_y(uint32_t *M, const uint32_t *ARG) { flux_lin_h(M, ARG, 1); }
+
+void teor_adv_flux_z(uint32_t *M, const uint32_t *ARG) {
+  /* adv_flux_z.wgsl main: 2nd order at k=1 / nz-1 (upwind side), 3rd next to them */
+  Dims g = dims_at(M, B(0));
+  const float *s = FPTR(1), *rrw = FPTR(2), *c1 = FPTR(3), *c2 = FPTR(4);
+  float *fz = FPTR(5);
+  const int sk = g.sJ * g.sK;
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i >= g.nx || j >= g.ny || k > g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    if (k == 0 || k == g.nz) { fz[c] = 0.0f; continue; }
+    float w = rrw[c];
+    int up = w >= 0.0f;
+    float f;
+    if (k == 1) f = up ? fmaf(c1[k], s[c - sk], c2[k] * s[c]) : flx3(s[c + sk], s[c], s[c - sk]);
+    else if (k == 2) f = up ? flx3(s[c - 2 * sk], s[c - sk], s[c]) : flx5(s[c + 2 * sk], s[c + sk], s[c], s[c - sk], s[c - 2 * sk]);
+    else if (k == g.nz - 2) f = up ? flx5(s[c - 3 * sk], s[c - 2 * sk], s[c - sk], s[c], s[c + sk]) : flx3(s[c + sk], s[c], s[c - sk]);
+    else if (k == g.nz - 1) f = up ? flx3(s[c - 2 * sk], s[c - sk], s[c]) : fmaf(c1[k], s[c - sk], c2[k] * s[c]);
+    else f = up ? flx5(s[c - 3 * sk], s[c - 2 * sk], s[c - sk], s[c], s[c + sk])
+                : flx5(s[c + 2 * sk], s[c + sk], s[c], s[c - sk], s[c - 2 * sk]);
+    fz[c] = w * f;
+  }
+}
+
+/* f_flx5_upwind (adv_flux_x_stag.wgsl:106-129): stencil shifted by one when the
+ * variable is staggered along the flux direction */
+static inline float flx5_upwind(const float *a, int c, int s, int up, int shifted) {
+  if (shifted) return up ? flx5(a[c - 2 * s], a[c - s], a[c], a[c + s], a[c + 2 * s])
+                         : flx5(a[c + 3 * s], a[c + 2 * s], a[c + s], a[c], a[c - s]);
+  return up ? flx5(a[c - 3 * s], a[c - 2 * s], a[c - s], a[c], a[c + s])
+            : flx5(a[c + 2 * s], a[c + s], a[c], a[c - s], a[c - 2 * s]);
+}
+
+static void flux_stag_h(uint32_t *M, const uint32_t *ARG, int dir) {
+  /* adv_flux_x_stag.wgsl / adv_flux_y_stag.wgsl main */
+  Dims g = dims_at(M, B(0));
+  int stag = IVAL(1);
+  const float *a = FPTR(2), *rr = dir == 0 ? FPTR(3) : FPTR(4), *c2 = FPTR(7);
+  float *fo = FPTR(8);
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  FOR_GRID {
+    int i = (int)tx - 1, j = (int)ty - 1, k = (int)tz;
+    if (i > g.nx || j > g.ny || k >= g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    if (stag == 4 && k == 0) { fo[c] = 0.0f; continue; }
+    float m;
+    if (dir == 0) {
+      if (stag == 2) m = 0.5f * (rr[c] + rr[c + 1]);
+      else if (stag == 3) m = 0.5f * (rr[c] + rr[c - sj]);
+      else if (stag == 4) { float cc2 = c2[k]; m = fmaf(cc2, rr[c], (1.0f - cc2) * rr[c - sk]); }
+      else m = rr[c];
+      fo[c] = m * flx5_upwind(a, c, 1, m >= 0.0f, stag == 2);
+    } else {
+      if (stag == 2) m = 0.5f * (rr[c] + rr[c - 1]);
+      else if (stag == 3) m = 0.5f * (rr[c] + rr[c + sj]);
+      else if (stag == 4) { float cc2 = c2[k]; m = fmaf(cc2, rr[c], (1.0f - cc2) * rr[c - sk]); }
+      else m = rr[c];
+      fo[c] = m * flx5_upwind(a, c, sj, m >= 0.0f, stag == 3);
+    }
+  }
+}
+void teor_adv_flux_x_stag(uint32_t *M, const uint32_t *ARG) { flux_stag_h(M, ARG, 0); }
+void teor_adv_flux_y_stag(uint32_t *M, const uint32_t *ARG) { flux_stag_h(M, ARG, 1); }
+
+void teor_adv_flux_z_stag(uint32_t *M, const uint32_t *ARG) {
+  /* adv_flux_z_stag.wgsl main (momentum, RK stages 1-2) */
+  Dims g = dims_at(M, B(0));
+  int stag = IVAL(1);
+  const float *a = FPTR(2), *rrw = FPTR(5), *c1 = FPTR(6), *c2 = FPTR(7);
+  float *fz = FPTR(8);
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i > g.nx || j > g.ny || k > g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    float m;
+    if (stag == 2) m = 0.5f * (rrw[c] + rrw[c - 1]);
+    else if (stag == 3) m = 0.5f * (rrw[c] + rrw[c - sj]);
+    else m = 0.5f * (rrw[c] + (k < g.nz ? rrw[c + sk] : 0.0f));
+    int up = m >= 0.0f;
+    float f;
+    if (stag == 4) {
+      if (k > g.nz - 1) { fz[c] = 0.0f; continue; }
+      if (k == 0) f = up ? 0.5f * (a[c] + a[c + sk]) : flx3(a[c + 2 * sk], a[c + sk], a[c]);
+      else if (k == 1) f = up ? flx3(a[c - sk], a[c], a[c + sk]) : flx5(a[c + 3 * sk], a[c + 2 * sk], a[c + sk], a[c], a[c - sk]);
+      else if (k == g.nz - 2) f = up ? flx5(a[c - 2 * sk], a[c - sk], a[c], a[c + sk], a[c + 2 * sk]) : flx3(a[c + 2 * sk], a[c + sk], a[c]);
+      else if (k == g.nz - 1) f = up ? flx3(a[c - sk], a[c], a[c + sk]) : 0.5f * (a[c] + a[c + sk]);
+      else f = up ? flx5(a[c - 2 * sk], a[c - sk], a[c], a[c + sk], a[c + 2 * sk])
+                  : flx5(a[c + 3 * sk], a[c + 2 * sk], a[c + sk], a[c], a[c - sk]);
+    } else {
+      if (k == 0 || k == g.nz) { fz[c] = 0.0f; continue; }
+      if (k == 1) f = up ? fmaf(c1[k], a[c - sk], c2[k] * a[c]) : flx3(a[c + sk], a[c], a[c - sk]);
+      else if (k == 2) f = up ? flx3(a[c - 2 * sk], a[c - sk], a[c]) : flx5(a[c + 2 * sk], a[c + sk], a[c], a[c - sk], a[c - 2 * sk]);
+      else if (k == g.nz - 2) f = up ? flx5(a[c - 3 * sk], a[c - 2 * sk], a[c - sk], a[c], a[c + sk]) : flx3(a[c + sk], a[c], a[c - sk]);
+      else if (k == g.nz - 1) f = up ? flx3(a[c - 2 * sk], a[c - sk], a[c]) : fmaf(c1[k], a[c - sk], c2[k] * a[c]);
+      else f = up ? flx5(a[c - 3 * sk], a[c - 2 * sk], a[c - sk], a[c], a[c + sk])
+                  : flx5(a[c + 2 * sk], a[c + sk], a[c], a[c - sk], a[c - 2 * sk]);
+    }
+    fz[c] = m * f;
+  }
+}
+
+/* ------------------------------------------------------ WENO fluxes (RK stage 3) */
+
+static void flux_weno_h(uint32_t *M, const uint32_t *ARG, int dir) {
+  /* adv_flux_x_weno.wgsl / adv_flux_y_weno.wgsl main (scalars, optional pdef gate) */
+  Dims g = dims_at(M, B(0));
+  const float *a = FPTR(1), *rr = FPTR(2);
+  float weps = FVAL(3);
+  int pdef = IVAL(4);
+  float *fo = FPTR(5);
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (dir == 0 ? (i > g.nx || j >= g.ny || k >= g.nz) : (i >= g.nx || j > g.ny || k >= g.nz)) continue;
+    int c = GIDX(g, i, j, k);
+    int d = dir == 0 ? 1 : g.sJ;
+    float s1, s2, s3, s4, s5;
+    if (rr[c] >= 0.0f) { s1 = a[c - 3 * d]; s2 = a[c - 2 * d]; s3 = a[c - d]; s4 = a[c]; s5 = a[c + d]; }
+    else { s1 = a[c + 2 * d]; s2 = a[c + d]; s3 = a[c]; s4 = a[c - d]; s5 = a[c - 2 * d]; }
+    fo[c] = weno_pdef_ok(s1, s2, s3, s4, s5, weps, pdef == 1) ? rr[c] * WENO(s1, s2, s3, s4, s5, weps) : 0.0f;
+  }
+}
+void teor_adv_flux_x_weno(uint32_t *M, const uint32_t *ARG) { flux_weno_h(M, ARG, 0); }
+void teor_adv_flux_y_weno(uint32_t *M, const uint32_t *ARG) { flux_weno_h(M, ARG, 1); }
+
+void teor_adv_flux_z_weno(uint32_t *M, const uint32_t *ARG) {
+  /* adv_flux_z_weno.wgsl main: face kf = k+1; c1/c2 interpolation and upstrpd next
+   * to the boundaries, positive-definite gating by pdefweno */
+  Dims g = dims_at(M, B(0));
+  const float *a = FPTR(1), *rrw = FPTR(2), *c1 = FPTR(3), *c2 = FPTR(4);
+  float weps = FVAL(5);
+  int pdefweno = IVAL(7);
+  float *fz = FPTR(8);
+  const int sk = g.sJ * g.sK, nk = g.nz;
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, kf = (int)tz + 1;
+    if (i >= g.nx || j >= g.ny || kf > g.nz + 1) continue;
+    int k = kf - 1;
+    int c = GIDX(g, i, j, k);
+    if (kf == 1 || kf == g.nz + 1) { fz[c] = 0.0f; continue; }
+#define A(o) a[c + (o) * sk]
+    float w = rrw[c];
+    if (kf == 2) {
+      fz[c] = w >= 0.0f ? w * fmaf(c1[k], A(-1), c2[k] * A(0)) : w * upstrpd(A(1), A(0), A(-1), weps);
+      continue;
+    }
+    if (kf == nk) {
+      fz[c] = w > 0.0f ? w * upstrpd(A(-2), A(-1), A(0), weps) : w * fmaf(c1[k], A(-1), c2[k] * A(0));
+      continue;
+    }
+    float s1, s2, s3, s4, s5;
+    if (w >= 0.0f) { s1 = A(-3); s2 = A(-2); s3 = A(-1); s4 = A(0); s5 = A(1); }
+    else { s1 = A(2); s2 = A(1); s3 = A(0); s4 = A(-1); s5 = A(-2); }
+    if (pdefweno == 1) {
+      int doit = weno_pdef_ok(s1, s2, s3, s4, s5, weps, 1);
+      if (kf == 3 && w > 0.0f) doit = 0;
+      if (kf == nk - 1 && w < 0.0f) doit = 0;
+      if (doit) { fz[c] = w * WENO(s1, s2, s3, s4, s5, weps); continue; }
+      if (kf != 3 && kf != nk - 1) { fz[c] = 0.0f; continue; }
+    }
+    if (kf == 3) {
+      fz[c] = w >= 0.0f ? w * upstrpd(A(-2), A(-1), A(0), weps) : w * WENO(A(2), A(1), A(0), A(-1), A(-2), weps);
+      continue;
+    }
+    if (kf == nk - 1) {
+      fz[c] = w >= 0.0f ? w * WENO(A(-3), A(-2), A(-1), A(0), A(1), weps) : w * upstrpd(A(1), A(0), A(-1), weps);
+      continue;
+    }
+    fz[c] = w * WENO(s1, s2, s3, s4, s5, weps);
+#undef A
+  }
+}
+
+/* f_weno5_upwind (adv_flux_x_weno_uv.wgsl:106-129) */
+static inline float weno5_upwind(const float *a, int c, int s, int up, int shifted, float weps) {
+  if (shifted) return up ? WENO(a[c - 2 * s], a[c - s], a[c], a[c + s], a[c + 2 * s], weps)
+                         : WENO(a[c + 3 * s], a[c + 2 * s], a[c + s], a[c], a[c - s], weps);
+  return up ? WENO(a[c - 3 * s], a[c - 2 * s], a[c - s], a[c], a[c + s], weps)
+            : WENO(a[c + 2 * s], a[c + s], a[c], a[c - s], a[c - 2 * s], weps);
+}
+
+static void flux_weno_uv_h(uint32_t *M, const uint32_t *ARG, int dir) {
+  /* adv_flux_x_weno_uv.wgsl / adv_flux_y_weno_uv.wgsl main (u, v momentum) */
+  Dims g = dims_at(M, B(0));
+  int stag = IVAL(1);
+  const float *a = FPTR(2), *rr = FPTR(3);
+  float weps = FVAL(4);
+  float *fo = FPTR(5);
+  const int sj = g.sJ;
+  FOR_GRID {
+    int i = (int)tx - 1, j = (int)ty - 1, k = (int)tz;
+    if (i > g.nx || j > g.ny || k >= g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    float m;
+    if (dir == 0) {
+      m = stag == 2 ? 0.5f * (rr[c] + rr[c + 1]) : 0.5f * (rr[c] + rr[c - sj]);
+      fo[c] = m * weno5_upwind(a, c, 1, m >= 0.0f, stag == 2, weps);
+    } else {
+      m = stag == 2 ? 0.5f * (rr[c] + rr[c - 1]) : 0.5f * (rr[c] + rr[c + sj]);
+      fo[c] = m * weno5_upwind(a, c, sj, m >= 0.0f, stag == 3, weps);
+    }
+  }
+}
+void teor_adv_flux_x_weno_uv(uint32_t *M, const uint32_t *ARG) { flux_weno_uv_h(M, ARG, 0); }
+void teor_adv_flux_y_weno_uv(uint32_t *M, const uint32_t *ARG) { flux_weno_uv_h(M, ARG, 1); }
+
+void teor_adv_flux_z_weno_uv(uint32_t *M, const uint32_t *ARG) {
+  /* adv_flux_z_weno_uv.wgsl main: order reduction at k = 1, 2, nz-2, nz-1 */
+  Dims g = dims_at(M, B(0));
+  int stag = IVAL(1);
+  const float *a = FPTR(2), *rrw = FPTR(3), *c1 = FPTR(4), *c2 = FPTR(5);
+  float weps = FVAL(6);
+  float *fz = FPTR(7);
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i > g.nx || j > g.ny || k > g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    if (k == 0 || k == g.nz) { fz[c] = 0.0f; continue; }
+#define A(o) a[c + (o) * sk]
+    float m = stag == 2 ? 0.5f * (rrw[c] + rrw[c - 1]) : 0.5f * (rrw[c] + rrw[c - sj]);
+    int up = m >= 0.0f;
+    float f;
+    if (k == 1) f = up ? fmaf(c1[k], A(-1), c2[k] * A(0)) : upstrpd(A(1), A(0), A(-1), weps);
+    else if (k == 2) f = up ? upstrpd(A(-2), A(-1), A(0), weps) : WENO(A(2), A(1), A(0), A(-1), A(-2), weps);
+    else if (k == g.nz - 2) f = up ? WENO(A(-3), A(-2), A(-1), A(0), A(1), weps) : upstrpd(A(1), A(0), A(-1), weps);
+    else if (k == g.nz - 1) f = up ? upstrpd(A(-2), A(-1), A(0), weps) : fmaf(c1[k], A(-1), c2[k] * A(0));
+    else f = up ? WENO(A(-3), A(-2), A(-1), A(0), A(1), weps) : WENO(A(2), A(1), A(0), A(-1), A(-2), weps);
+    fz[c] = m * f;
+#undef A
+  }
+}
+
+static void flux_weno_w_h(uint32_t *M, const uint32_t *ARG, int dir) {
+  /* adv_flux_x_weno_w.wgsl / adv_flux_y_weno_w.wgsl main (w momentum) */
+  Dims g = dims_at(M, B(0));
+  const float *a = FPTR(1), *rr = FPTR(2), *c2 = FPTR(3);
+  float weps = FVAL(4);
+  float *fo = FPTR(5);
+  const int sk = g.sJ * g.sK;
+  FOR_GRID {
+    int i = (int)tx - 1, j = (int)ty - 1, k = (int)tz;
+    if (i < 0 || j < 0 || i > g.nx || j > g.ny || k >= g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    if (k == 0) { fo[c] = 0.0f; continue; }
+    int d = dir == 0 ? 1 : g.sJ;
+    float cc2 = c2[k];
+    float cc1 = 1.0f - cc2;
+    float ub = fmaf(cc2, rr[c], cc1 * rr[c - sk]);
+    fo[c] = ub >= 0.0f ? ub * WENO(a[c - 3 * d], a[c - 2 * d], a[c - d], a[c], a[c + d], weps)
+                       : ub * WENO(a[c + 2 * d], a[c + d], a[c], a[c - d], a[c - 2 * d], weps);
+  }
+}
+void teor_adv_flux_x_weno_w(uint32_t *M, const uint32_t *ARG) { flux_weno_w_h(M, ARG, 0); }
+void teor_adv_flux_y_weno_w(uint32_t *M, const uint32_t *ARG) { flux_weno_w_h(M, ARG, 1); }
+
+void teor_adv_flux_z_weno_w(uint32_t *M, const uint32_t *ARG) {
+  /* adv_flux_z_weno_w.wgsl main: w flux at cell centres, wbar = (rrw_k + rrw_k+1)/2 */
+  Dims g = dims_at(M, B(0));
+  const float *a = FPTR(1), *rrw = FPTR(2);
+  float weps = FVAL(3);
+  float *fz = FPTR(4);
+  const int sk = g.sJ * g.sK, nz = g.nz;
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i > g.nx || j > g.ny || k > g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    if (k > g.nz - 1) { fz[c] = 0.0f; continue; }
+#define A(o) a[c + (o) * sk]
+    float wb = 0.5f * (rrw[c] + rrw[c + sk]);
+    float f;
+    if (k == 0) f = wb >= 0.0f ? 0.5f * (A(0) + A(1)) : upstrpd(A(2), A(1), A(0), weps);
+    else if (k == nz - 1) f = wb > 0.0f ? upstrpd(A(-1), A(0), A(1), weps) : 0.5f * (A(0) + A(1));
+    else if (k == 1) f = wb >= 0.0f ? upstrpd(A(-1), A(0), A(1), weps) : WENO(A(3), A(2), A(1), A(0), A(-1), weps);
+    else if (k == nz - 2) f = wb > 0.0f ? WENO(A(-2), A(-1), A(0), A(1), A(2), weps) : upstrpd(A(2), A(1), A(0), weps);
+    else f = wb >= 0.0f ? WENO(A(-2), A(-1), A(0), A(1), A(2), weps) : WENO(A(3), A(2), A(1), A(0), A(-1), weps);
+    fz[c] = wb * f;
+#undef A
+  }
+}
+
+/* ------------------------------------------------------------- flux assembly */
+
+void teor_adv_assemble(uint32_t *M, const uint32_t *ARG) {
+  /* adv_assemble.wgsl main (periodic/closed branches; open-boundary inflow branches
+   * restated too): t = (s*dv - sum dF*rd*m) / rho, optional accumulation */
+  Dims g = dims_at(M, B(0));
+  int stag = IVAL(1);
+  const float *s = FPTR(2), *fx = FPTR(3), *fy = FPTR(4), *fz = FPTR(5), *divx = FPTR(6);
+  const float *rho0 = FPTR(7), *rf0 = FPTR(8), *mh = FPTR(9), *mf = FPTR(10);
+  float *tend = FPTR(11);
+  int accumulate = IVAL(12);
+  const float *rru = FPTR(13), *rrv = FPTR(14), *c1 = FPTR(15), *c2 = FPTR(16);
+  int openx = (int)M[B(17)], openy = (int)M[B(17) + 1];
+  const float *hm = FPTR(30);
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  int st = stag < 0 ? -stag : stag;
+  int iMax = st == 2 ? g.nx : g.nx - 1, jMax = st == 3 ? g.ny : g.ny - 1;
+  int kLo = st == 4 ? 1 : 0, kMax = g.nz - 1;
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i > iMax || j > jMax || k < kLo || k > kMax) continue;
+    if (openx != 0 && st == 2 && (i == 0 || i == g.nx)) continue;
+    if (openy != 0 && st == 3 && (j == 0 || j == g.ny)) continue;
+    int c = GIDX(g, i, j, k);
+    float dFx = st == 2 ? fx[c] - fx[c - 1] : fx[c + 1] - fx[c];
+    float dFy = st == 3 ? fy[c] - fy[c - sj] : fy[c + sj] - fy[c];
+    float dFz = st == 4 ? fz[c] - fz[c - sk] : fz[c + sk] - fz[c];
+    float mz = stag < 0 ? 1.0f : (stag == 4 ? mf[k] : mh[k]);
+    float dv;
+    if (st == 2) dv = 0.5f * (divx[c] + divx[c - 1]);
+    else if (st == 3) dv = 0.5f * (divx[c] + divx[c - sj]);
+    else if (st == 4) dv = fmaf(c2[k], divx[c], c1[k] * divx[c - sk]);
+    else dv = divx[c];
+    if (openx != 0 && st != 2) {
+      int west = i == 0, east = i == g.nx - 1;
+      if (west || east) {
+        int cf = west ? c : c + 1;
+        float un, piece;
+        if (st == 3) {
+          un = rru[cf] + rru[cf - sj];
+          piece = ((0.5f * ((rru[c + 1 - sj] - rru[c - sj]) + (rru[c + 1] - rru[c]))) * g.rdx) * hm_uh(&g, hm, i);
+        } else if (st == 4) {
+          float cc2 = 0.5f * (c2[k - 1] + c2[k]);
+          float cc1 = 1.0f - cc2;
+          un = fmaf(cc2, rru[cf], cc1 * rru[cf - sk]);
+          piece = (fmaf(c1[k], rru[c + 1 - sk] - rru[c - sk], c2[k] * (rru[c + 1] - rru[c])) * g.rdx) * hm_uh(&g, hm, i);
+        } else {
+          un = rru[cf];
+          piece = ((rru[c + 1] - rru[c]) * g.rdx) * hm_uh(&g, hm, i);
+        }
+        int inflow = west ? un >= 0.0f : un <= 0.0f;
+        if (inflow) { dFx = 0.0f; dv = dv - piece; }
+      }
+    }
+    if (openy != 0 && st != 3) {
+      int south = j == 0, north = j == g.ny - 1;
+      if (south || north) {
+        int cf = south ? c : c + sj;
+        float vn, piece;
+        if (st == 2) {
+          vn = rrv[cf] + rrv[cf - 1];
+          piece = ((0.5f * ((rrv[c + sj - 1] - rrv[c - 1]) + (rrv[c + sj] - rrv[c]))) * g.rdy) * hm_vh(&g, hm, j);
+        } else if (st == 4) {
+          float cc2 = 0.5f * (c2[k - 1] + c2[k]);
+          float cc1 = 1.0f - cc2;
+          vn = fmaf(cc2, rrv[cf], cc1 * rrv[cf - sk]);
+          piece = (fmaf(c1[k], rrv[c + sj - sk] - rrv[c - sk], c2[k] * (rrv[c + sj] - rrv[c])) * g.rdy) * hm_vh(&g, hm, j);
+        } else {
+          vn = rrv[cf];
+          piece = ((rrv[c + sj] - rrv[c]) * g.rdy) * hm_vh(&g, hm, j);
+        }
+        int inflow = south ? vn >= 0.0f : vn <= 0.0f;
+        if (inflow) { dFy = 0.0f; dv = dv - piece; }
+      }
+    }
+    float mx = st == 2 ? hm_uf(&g, hm, i) : hm_uh(&g, hm, i);
+    float my = st == 3 ? hm_vf(&g, hm, j) : hm_vh(&g, hm, j);
+    float divF = fmaf(dFz * g.rdz, mz, fmaf(dFx * g.rdx, mx, (dFy * g.rdy) * my));
+    float rho = st == 4 ? rf0[k] : rho0[k];
+    float t = DCR(fmaf(s[c], dv, -divF), rho);
+    tend[c] = accumulate != 0 ? tend[c] + t : t;
+  }
+}
+
+void teor_rk_update(uint32_t *M, const uint32_t *ARG) {
+  /* rk_update.wgsl main: phi = fma(dttmp, tend, phi_a) */
+  Dims g = dims_at(M, B(0));
+  int stag = IVAL(1);
+  const float *phiA = FPTR(2), *tend = FPTR(3);
+  float *phi = FPTR(4);
+  float dttmp = FVAL(5);
+  int iMax = stag == 2 ? g.nx : g.nx - 1, jMax = stag == 3 ? g.ny : g.ny - 1, kLo = stag == 4 ? 1 : 0;
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i > iMax || j > jMax || k < kLo || k >= g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    phi[c] = fmaf(dttmp, tend[c], phiA[c]);
+  }
+}
+
+/* f_pdef_inflow (pdef_dum.wgsl:108-134) */
+static inline int pdef_inflow(const Dims *g, int dir, int i, int j, int c, int step, const float *rr, int ox, int oy) {
+  if (dir == 0 && ox != 0) {
+    if (i == 0 && rr[c] >= 0.0f) return 1;
+    if (i == g->nx - 1 && rr[c + step] <= 0.0f) return 1;
+  }
+  if (dir == 1 && oy != 0) {
+    if (j == 0 && rr[c] >= 0.0f) return 1;
+    if (j == g->ny - 1 && rr[c + step] <= 0.0f) return 1;
+  }
+  return 0;
+}
+
+void teor_pdef_dum(uint32_t *M, const uint32_t *ARG) {
+  /* pdef_dum.wgsl main: provisional mass after advection along one direction */
+  Dims g = dims_at(M, B(0));
+  int dir = IVAL(1);
+  const float *s = FPTR(2), *s0 = FPTR(3), *f = FPTR(4), *rr = FPTR(5), *rho0 = FPTR(6), *mh = FPTR(7);
+  float dt = FVAL(8);
+  int ox = (int)M[B(9)], oy = (int)M[B(9) + 1];
+  float *dum = FPTR(10);
+  const float *hm = FPTR(30);
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    int step = dir == 0 ? 1 : (dir == 1 ? g.sJ : g.sJ * g.sK);
+    float rd = dir == 0 ? g.rdx : (dir == 1 ? g.rdy : g.rdz);
+    float base = rho0[k] * s0[c];
+    if (pdef_inflow(&g, dir, i, j, c, step, rr, ox, oy)) { dum[c] = base; continue; }
+    float adv = (-(f[c + step] - f[c])) * rd;
+    float sdiv = (s[c] * (rr[c + step] - rr[c])) * rd;
+    float m = dir == 0 ? hm_uh(&g, hm, i) : (dir == 1 ? hm_vh(&g, hm, j) : mh[k]);
+    adv = adv * m;
+    sdiv = sdiv * m;
+    dum[c] = fmaf(dt, adv + sdiv, base);
+  }
+}
+
+/* f_pdef_cell / f_pdef_mass (pdef_apply.wgsl:115-158), K_PDEF_SMEPS = 1e-30 */
+typedef struct { int neg; float f1, f2, foo3; } PdefCell;
+static inline PdefCell pdef_cell(float d, float dm, float dp) {
+  PdefCell r = {0, 0.0f, 0.0f, 0.0f};
+  if (d < 0.0f) {
+    float f1 = fmax_(0.0f, dm), f2 = fmax_(0.0f, dp);
+    if (f1 + f2 > 1e-30f) {
+      r.neg = 1;
+      r.f1 = f1;
+      r.f2 = f2;
+      r.foo3 = DCR(fmax_(d, -(f1 + f2)), f1 + f2);
+    }
+  }
+  return r;
+}
+static inline float pdef_mass(float dm2, float dm1, float d0, float dp1, float dp2, int *flag) {
+  PdefCell l = pdef_cell(dm1, dm2, d0), c = pdef_cell(d0, dm1, dp1), r = pdef_cell(dp1, d0, dp2);
+  float mass = 0.0f;
+  if (l.neg) mass = fmaf(l.f2, l.foo3, mass);
+  if (c.neg) mass = fmaf(-(c.f1 + c.f2), c.foo3, mass);
+  if (r.neg) mass = fmaf(r.f1, r.foo3, mass);
+  *flag = c.neg || (l.neg && d0 > 1e-30f) || (r.neg && d0 > 1e-30f);
+  return mass;
+}
+
+void teor_pdef_apply(uint32_t *M, const uint32_t *ARG) {
+  /* pdef_apply.wgsl main: replace the advective tendency where the provisional mass
+   * would go negative */
+  Dims g = dims_at(M, B(0));
+  const float *s = FPTR(1), *s0 = FPTR(2), *fx = FPTR(3), *fy = FPTR(4), *fz = FPTR(5);
+  const float *rru = FPTR(6), *rrv = FPTR(7), *rrw = FPTR(8), *dumx = FPTR(9), *dumy = FPTR(10), *dumz = FPTR(11);
+  const float *rho0 = FPTR(12), *mh = FPTR(13);
+  float dt = FVAL(14);
+  int ox = (int)M[B(15)], oy = (int)M[B(15) + 1];
+  float *tend = FPTR(16);
+  const float *hm = FPTR(30);
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    float rdt = DCR(1.0f, dt);
+    float base = rho0[k] * s0[c];
+    float delta = 0.0f;
+    int flag;
+    float mx = pdef_mass(dumx[c - 2], dumx[c - 1], dumx[c], dumx[c + 1], dumx[c + 2], &flag);
+    if (flag) {
+      float sdiv = ((s[c] * (rru[c + 1] - rru[c])) * g.rdx) * hm_uh(&g, hm, i);
+      float advOld = pdef_inflow(&g, 0, i, j, c, 1, rru, ox, oy) ? -sdiv : ((-(fx[c + 1] - fx[c])) * g.rdx) * hm_uh(&g, hm, i);
+      float advNew = fmaf((dumx[c] + mx) - base, rdt, -sdiv);
+      delta = delta + (advNew - advOld);
+    }
+    float my = pdef_mass(dumy[c - 2 * sj], dumy[c - sj], dumy[c], dumy[c + sj], dumy[c + 2 * sj], &flag);
+    if (flag) {
+      float sdiv = ((s[c] * (rrv[c + sj] - rrv[c])) * g.rdy) * hm_vh(&g, hm, j);
+      float advOld = pdef_inflow(&g, 1, i, j, c, sj, rrv, ox, oy) ? -sdiv : ((-(fy[c + sj] - fy[c])) * g.rdy) * hm_vh(&g, hm, j);
+      float advNew = fmaf((dumy[c] + my) - base, rdt, -sdiv);
+      delta = delta + (advNew - advOld);
+    }
+    float zm2 = k >= 2 ? dumz[c - 2 * sk] : 0.0f;
+    float zm1 = k >= 1 ? dumz[c - sk] : 0.0f;
+    float zp1 = k + 1 < g.nz ? dumz[c + sk] : 0.0f;
+    float zp2 = k + 2 < g.nz ? dumz[c + 2 * sk] : 0.0f;
+    float mz = pdef_mass(zm2, zm1, dumz[c], zp1, zp2, &flag);
+    if (flag) {
+      float sdiv = ((s[c] * (rrw[c + sk] - rrw[c])) * g.rdz) * mh[k];
+      float advOld = ((-(fz[c + sk] - fz[c])) * g.rdz) * mh[k];
+      float advNew = fmaf((dumz[c] + mz) - base, rdt, -sdiv);
+      delta = delta + (advNew - advOld);
+    }
+    tend[c] = tend[c] + DCR(delta, rho0[k]);
+  }
+}
+
+/* ----------------------------------------------------------- whole-grid glue */
+
+#define FOR_WHOLE(kcond)                                    \
+  FOR_GRID {                                                \
+    int i = (int)tx - 3, j = (int)ty - 3, k = (int)tz;      \
+    if (i > g.nx + 3 || j > g.ny + 3 || !(kcond)) continue; \
+    int c = GIDX(g, i, j, k);
+
+void teor_build_sadv(uint32_t *M, const uint32_t *ARG) {
+  /* build_sadv.wgsl main: sadv = (th0 - 300) + th' */
+  Dims g = dims_at(M, B(0));
+  const float *th0 = FPTR(1), *thp = FPTR(2);
+  float *sadv = FPTR(3);
+  FOR_WHOLE(k < g.nz)
+    sadv[c] = (th0[k] - 300.0f) + thp[c];
+  }
+}
+
+void teor_massflux_from_state(uint32_t *M, const uint32_t *ARG) {
+  /* massflux_from_state.wgsl main: rru = rho0 u, rrv = rho0 v, rrw = rf0 w (0 at k=0, nz) */
+  Dims g = dims_at(M, B(0));
+  const float *u = FPTR(1), *v = FPTR(2), *w = FPTR(3), *rho0 = FPTR(4), *rf0 = FPTR(5);
+  float *rru = FPTR(6), *rrv = FPTR(7), *rrw = FPTR(8);
+  FOR_WHOLE(k <= g.nz)
+    if (k < g.nz) {
+      rru[c] = rho0[k] * u[c];
+      rrv[c] = rho0[k] * v[c];
+    }
+    rrw[c] = (k == 0 || k == g.nz) ? 0.0f : rf0[k] * w[c];
+  }
+}
+
+void teor_div_massflux(uint32_t *M, const uint32_t *ARG) {
+  /* div_massflux.wgsl main */
+  Dims g = dims_at(M, B(0));
+  const float *rru = FPTR(1), *rrv = FPTR(2), *rrw = FPTR(3), *mh = FPTR(4);
+  float *divx = FPTR(5);
+  const float *hm = FPTR(30);
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  FOR_GRID {
+    int i = (int)tx - 3, j = (int)ty - 3, k = (int)tz;
+    if (i > g.nx + 2 || j > g.ny + 2 || k >= g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    divx[c] = fmaf((rrw[c + sk] - rrw[c]) * g.rdz, mh[k],
+                   fmaf((rru[c + 1] - rru[c]) * g.rdx, hm_uh(&g, hm, i), ((rrv[c + sj] - rrv[c]) * g.rdy) * hm_vh(&g, hm, j)));
+  }
+}
+
+void teor_velocity_to_massflux(uint32_t *M, const uint32_t *ARG) {
+  /* velocity_to_massflux.wgsl main */
+  Dims g = dims_at(M, B(0));
+  const float *rho0 = FPTR(1), *rf0 = FPTR(2);
+  float *rru = FPTR(3), *rrv = FPTR(4), *rrw = FPTR(5);
+  FOR_WHOLE(k <= g.nz)
+    if (k < g.nz) {
+      rru[c] = rru[c] * rho0[k];
+      rrv[c] = rrv[c] * rho0[k];
+    }
+    rrw[c] = (k == 0 || k == g.nz) ? 0.0f : rrw[c] * rf0[k];
+  }
+}
+
+void teor_stage_state_reset(uint32_t *M, const uint32_t *ARG) {
+  /* stage_state_reset.wgsl main */
+  Dims g = dims_at(M, B(0));
+  const float *ua = FPTR(1), *va = FPTR(2), *wa = FPTR(3), *ppi = FPTR(4);
+  float *u = FPTR(5), *v = FPTR(6), *w = FPTR(7), *pp3d = FPTR(8), *ppd = FPTR(9);
+  const float *ppx = FPTR(10);
+  FOR_WHOLE(k <= g.nz)
+    u[c] = ua[c];
+    v[c] = va[c];
+    w[c] = wa[c];
+    pp3d[c] = ppi[c];
+    ppd[c] = ppx[c];
+  }
+}
+
+void teor_stage_tendency_reset(uint32_t *M, const uint32_t *ARG) {
+  /* stage_tendency_reset.wgsl main */
+  Dims g = dims_at(M, B(0));
+  float *uten = FPTR(1), *vten = FPTR(2), *wten = FPTR(3);
+  FOR_WHOLE(k <= g.nz)
+    uten[c] = 0.0f;
+    vten[c] = 0.0f;
+    wten[c] = 0.0f;
+  }
+}
+
+void teor_buoyancy_apply(uint32_t *M, const uint32_t *ARG) {
+  /* buoyancy_apply.wgsl main: wten += c1 buoy(k-1) + c2 buoy(k) on interior faces */
+  Dims g = dims_at(M, B(0));
+  const float *buoy = FPTR(1), *c1 = FPTR(2), *c2 = FPTR(3);
+  float *wten = FPTR(4);
+  const int sk = g.sJ * g.sK;
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz + 1;
+    if (i >= g.nx || j >= g.ny || k > g.nz - 1) continue;
+    int c = GIDX(g, i, j, k);
+    wten[c] = wten[c] + fmaf(c1[k], buoy[c - sk], c2[k] * buoy[c]);
+  }
+}
+
+void teor_apply_thterm(uint32_t *M, const uint32_t *ARG) {
+  /* apply_thterm.wgsl main: tend -= div * thterm */
+  Dims g = dims_at(M, B(0));
+  const float *div = FPTR(1), *thterm = FPTR(2);
+  float *tend = FPTR(3);
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    tend[c] = fmaf(-div[c], thterm[c], tend[c]);
+  }
+}
+
+/* ---------------------------------------------------------- acoustic substep */
+
+void teor_acoustic_prepare(uint32_t *M, const uint32_t *ARG) {
+  /* acoustic_prepare.wgsl main: qk, pk1, pk2, mm; the pk fma order depends on
+   * whether i falls in CM1's vectorised part of the loop (vec_v) */
+  Dims g = dims_at(M, B(0));
+  Acoustic a = acoustic_at(M, B(1));
+  const float *ppterm = FPTR(2), *piadv = FPTR(3), *thv = FPTR(4), *rr0 = FPTR(5), *rf0 = FPTR(6);
+  const float *mh = FPTR(7), *mf = FPTR(8), *c1 = FPTR(9), *c2 = FPTR(10);
+  float *qk = FPTR(11), *pk1 = FPTR(12), *pk2 = FPTR(13), *mm = FPTR(14);
+  const int sk = g.sJ * g.sK;
+  const float cp = CP_;
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    float tem = (a.dts * g.rdz) * mh[k];
+    float r2 = (tem * rr0[k]) * rf0[k + 1];
+    float r1 = (tem * rr0[k]) * rf0[k];
+    float tem1 = ((a.dts * g.rdz) * cp) * mf[k];
+    float c1a = c1[k], c1b = c1[k + 1], c2a = c2[k], c2b = c2[k + 1];
+    int vec_v = g.nx > 3 && i < (g.nx / 4) * 4;
+    qk[c] = tem * ppterm[c];
+    float p2 = 0.0f, p1 = 0.0f;
+    if (k != g.nz - 1)
+      p2 = vec_v ? fmaf(-c2b, piadv[c + sk], (1.0f - c1b) * piadv[c])
+                 : fmaf(1.0f - c1b, piadv[c], -(c2b * piadv[c + sk]));
+    if (k != 0)
+      p1 = vec_v ? fmaf(c2a - 1.0f, piadv[c], c1a * piadv[c - sk])
+                 : fmaf(c1a, piadv[c - sk], (c2a - 1.0f) * piadv[c]);
+    pk2[c] = k == g.nz - 1 ? 0.0f : r2 * p2;
+    pk1[c] = k == 0 ? 0.0f : r1 * p1;
+    mm[c] = tem1 * fmaf(c2a, thv[c], c1a * (k == 0 ? thv[c] : thv[c - sk]));
+  }
+}
+
+void teor_acoustic_begin(uint32_t *M, const uint32_t *ARG) {
+  /* acoustic_begin.wgsl main: rru = rrv = 0, rrw = beta w */
+  Dims g = dims_at(M, B(0));
+  Acoustic a = acoustic_at(M, B(1));
+  const float *w = FPTR(2);
+  float *rru = FPTR(3), *rrv = FPTR(4), *rrw = FPTR(5);
+  FOR_WHOLE(k <= g.nz)
+    rru[c] = 0.0f;
+    rrv[c] = 0.0f;
+    rrw[c] = w[c] * a.beta;
+  }
+}
+
+void teor_acoustic_uv(uint32_t *M, const uint32_t *ARG) {
+  /* acoustic_uv.wgsl main: horizontal pi'-gradient update of u and v */
+  Dims g = dims_at(M, B(0));
+  Acoustic a = acoustic_at(M, B(1));
+  const float *ppd = FPTR(2), *thv = FPTR(3), *uten = FPTR(4), *vten = FPTR(5);
+  float *u = FPTR(6), *v = FPTR(7);
+  int ox = (int)M[B(8)], oy = (int)M[B(8) + 1];
+  const float *hm = FPTR(30);
+  const int sj = g.sJ;
+  const float cp = CP_;
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i > g.nx || j > g.ny || k >= g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    float tem1 = (g.rdx * cp) * 0.5f;
+    float tem2 = (g.rdy * cp) * 0.5f;
+    int uEdge = ox != 0 && (i == 0 || i == g.nx);
+    int vEdge = oy != 0 && (j == 0 || j == g.ny);
+    if (!uEdge)
+      u[c] = fmaf(a.dts, fmaf(-((tem1 * (ppd[c] - ppd[c - 1])) * hm_uf(&g, hm, i)), thv[c] + thv[c - 1], uten[c]), u[c]);
+    if (!vEdge)
+      v[c] = fmaf(a.dts, fmaf(-((tem2 * (ppd[c] - ppd[c - sj])) * hm_vf(&g, hm, j)), thv[c] + thv[c - sj], vten[c]), v[c]);
+  }
+}
+
+void teor_acoustic_fpk(uint32_t *M, const uint32_t *ARG) {
+  /* acoustic_fpk.wgsl main: explicit forcing of the pi' equation */
+  Dims g = dims_at(M, B(0));
+  Acoustic a = acoustic_at(M, B(1));
+  const float *u = FPTR(2), *v = FPTR(3), *w = FPTR(4), *piadv = FPTR(5), *ppten = FPTR(6), *ppterm = FPTR(7);
+  const float *pk1 = FPTR(8), *pk2 = FPTR(9), *qk = FPTR(10);
+  float *fpk = FPTR(11);
+  const float *hm = FPTR(30);
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    float temx = (a.dts * 0.5f) * g.rdx;
+    float temy = (a.dts * 0.5f) * g.rdy;
+    float div = fmaf((u[c + 1] - u[c]) * g.rdx, hm_uh(&g, hm, i), ((v[c + sj] - v[c]) * g.rdy) * hm_vh(&g, hm, j));
+    if (fabsf(div) < a.smeps) div = 0.0f;
+    float advPi = fmaf((-fmaf(u[c], piadv[c] - piadv[c - 1], u[c + 1] * (piadv[c + 1] - piadv[c]))) * temx, hm_uh(&g, hm, i),
+                       -((fmaf(v[c], piadv[c] - piadv[c - sj], v[c + sj] * (piadv[c + sj] - piadv[c])) * temy) * hm_vh(&g, hm, j)));
+    fpk[c] = fmaf(a.beta, fmaf(w[c], pk1[c] + qk[c], w[c + sk] * (pk2[c] - qk[c])),
+                  fmaf(a.dts, fmaf(-ppterm[c], div, ppten[c]), advPi));
+  }
+}
+
+void teor_acoustic_w_solve(uint32_t *M, const uint32_t *ARG) {
+  /* acoustic_w_solve.wgsl main + lam_1 (:124-139): per column, tridiagonal Thomas solve
+   * for w on faces k = 1..nz-1 with w(0) = w(nz) = 0; forward sweep stores cA, cB */
+  Dims g = dims_at(M, B(0));
+  Acoustic a = acoustic_at(M, B(1));
+  const float *pk1 = FPTR(2), *pk2 = FPTR(3), *qk = FPTR(4), *mm = FPTR(5), *fpk = FPTR(6), *wten = FPTR(7), *pp3d = FPTR(8);
+  float *w = FPTR(9), *cA = FPTR(10), *cB = FPTR(11);
+  const int sk = g.sJ * g.sK;
+  const long GX = ARG[0], GY = ARG[1];
+#pragma omp parallel for collapse(2) schedule(static)
+  for (long ty = 0; ty < GY; ty++)
+    for (long tx = 0; tx < GX; tx++) {
+      int i = (int)tx, j = (int)ty;
+      if (i >= g.nx || j >= g.ny) continue;
+      float asq = a.alph * a.alph;
+      w[GIDX(g, i, j, 0)] = 0.0f;
+      w[GIDX(g, i, j, g.nz)] = 0.0f;
+      float aa, bb, cc, dd;
+#define LAM(kk)                                                                     \
+  do {                                                                              \
+    int c_ = GIDX(g, i, j, (kk)), cm_ = c_ - sk;                                    \
+    float m_ = mm[c_];                                                              \
+    aa = (-asq) * (m_ * (pk1[cm_] + qk[cm_]));                                      \
+    cc = (-asq) * ((-m_) * (pk2[c_] - qk[c_]));                                     \
+    bb = fmaf(-asq, m_ * ((-(pk1[c_] + qk[c_])) + (pk2[cm_] - qk[cm_])), 1.0f);     \
+    float fw_ = fmaf(a.dts, wten[c_], a.beta * ((-m_) * (pp3d[c_] - pp3d[cm_])));   \
+    dd = fmaf(a.alph, (-m_) * ((pp3d[c_] + fpk[c_]) - (pp3d[cm_] + fpk[cm_])), w[c_] + fw_); \
+  } while (0)
+      {
+        int c = GIDX(g, i, j, 1);
+        LAM(1);
+        float r = DCR(1.0f, bb);
+        cA[c] = (-cc) * r;
+        cB[c] = dd * r;
+      }
+      for (int k = 2; k < g.nz - 1; k++) {
+        int c = GIDX(g, i, j, k);
+        LAM(k);
+        float r = DCR(1.0f, fmaf(aa, cA[c - sk], bb));
+        cA[c] = (-cc) * r;
+        cB[c] = fmaf(-aa, cB[c - sk], dd) * r;
+      }
+      {
+        int k = g.nz - 1, c = GIDX(g, i, j, k);
+        LAM(k);
+        float r = DCR(1.0f, fmaf(aa, cA[c - sk], bb));
+        w[c] = fmaf(-aa, cB[c - sk], dd) * r;
+      }
+#undef LAM
+      for (int k = g.nz - 2; k >= 1; k--) {
+        int c = GIDX(g, i, j, k);
+        w[c] = fmaf(cA[c], w[c + sk], cB[c]);
+      }
+    }
+}
+
+void teor_acoustic_pp(uint32_t *M, const uint32_t *ARG) {
+  /* acoustic_pp.wgsl main: pi' update, divergence damping ppd, ppx on stage 3 */
+  Dims g = dims_at(M, B(0));
+  Acoustic a = acoustic_at(M, B(1));
+  const float *w = FPTR(2), *pk1 = FPTR(3), *pk2 = FPTR(4), *qk = FPTR(5), *fpk = FPTR(6);
+  float *pp3d = FPTR(7), *ppd = FPTR(8), *ppx = FPTR(9);
+  int saveX = IVAL(10);
+  const int sk = g.sJ * g.sK;
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    float prev = pp3d[c];
+    float w1 = w[c], w2 = w[c + sk];
+    float p = fmaf(a.alph, fmaf(w1, pk1[c] + qk[c], w2 * (pk2[c] - qk[c])), prev + fpk[c]);
+    if (fabsf(p) < a.smeps) p = 0.0f;
+    pp3d[c] = p;
+    float dum1 = a.kdiv * (p - prev);
+    ppd[c] = p + dum1;
+    if (saveX != 0) ppx[c] = dum1;
+  }
+}
+
+void teor_acoustic_accumulate(uint32_t *M, const uint32_t *ARG) {
+  /* acoustic_accumulate.wgsl main: substep sums, averaged on the last substep */
+  Dims g = dims_at(M, B(0));
+  Acoustic a = acoustic_at(M, B(1));
+  const float *u = FPTR(2), *v = FPTR(3), *w = FPTR(4);
+  float *rru = FPTR(5), *rrv = FPTR(6), *rrw = FPTR(7);
+  float tavg = FVAL(8);
+  FOR_WHOLE(k <= g.nz)
+    if (tavg > 0.0f) {
+      rru[c] = (rru[c] + u[c]) * tavg;
+      rrv[c] = (rrv[c] + v[c]) * tavg;
+      rrw[c] = fmaf(w[c], a.alph, rrw[c]) * tavg;
+    } else {
+      rru[c] = rru[c] + u[c];
+      rrv[c] = rrv[c] + v[c];
+      rrw[c] = rrw[c] + w[c];
+    }
+  }
+}
+
+/* --------------------------------------------------------- periodic halos */
+
+void teor_bc_periodic_x(uint32_t *M, const uint32_t *ARG) {
+  /* bc_periodic_x.wgsl main: i = -1-h <- nx-1-h (h < 3), i = nx+h <- h (h <= 3) */
+  Dims g = dims_at(M, B(0));
+  float *f = FPTR(1);
+  FOR_GRID {
+    int h = (int)tx, jj = (int)ty - 3, k = (int)tz;
+    if (h > 3 || jj > g.ny + 3 || k > g.nz) continue;
+    int lo = (((-1 - h) % g.nx) + g.nx) % g.nx;
+    int hi = (((g.nx + h) % g.nx) + g.nx) % g.nx;
+    if (h < 3) f[GIDX(g, -1 - h, jj, k)] = f[GIDX(g, lo, jj, k)];
+    f[GIDX(g, g.nx + h, jj, k)] = f[GIDX(g, hi, jj, k)];
+  }
+}
+
+void teor_bc_periodic_y(uint32_t *M, const uint32_t *ARG) {
+  /* bc_periodic_y.wgsl main */
+  Dims g = dims_at(M, B(0));
+  float *f = FPTR(1);
+  FOR_GRID {
+    int h = (int)tx, i = (int)ty - 3, k = (int)tz;
+    if (h > 3 || i > g.nx + 3 || k > g.nz) continue;
+    int lo = (((-1 - h) % g.ny) + g.ny) % g.ny;
+    int hi = (((g.ny + h) % g.ny) + g.ny) % g.ny;
+    if (h < 3) f[GIDX(g, i, -1 - h, k)] = f[GIDX(g, i, lo, k)];
+    f[GIDX(g, i, g.ny + h, k)] = f[GIDX(g, i, hi, k)];
+  }
+}
+
+/* ------------------------------------------------------ thermodynamic glue */
+
+void teor_update_diagnostics_moist(uint32_t *M, const uint32_t *ARG) {
+  /* update_diagnostics_moist.wgsl main: thv, piadv, ppterm, thterm, buoy */
+  Dims g = dims_at(M, B(0));
+  const float *thp = FPTR(1), *ppp = FPTR(2), *th0 = FPTR(3), *pi0 = FPTR(4), *qv0 = FPTR(5), *qc0 = FPTR(6);
+  const float *qi0 = FPTR(7), *rth0 = FPTR(8), *qv = FPTR(9), *qc = FPTR(10), *qr = FPTR(11), *qi = FPTR(12);
+  const float *qs = FPTR(13), *qg = FPTR(14);
+  float *thv = FPTR(15), *ppterm = FPTR(16), *piadv = FPTR(17), *thterm = FPTR(18), *buoy = FPTR(19);
+  const float rd = 287.04f, rv = 461.5f, cp = 1005.7f, cv = 718.66003f, cpv = 1870.0f, cvv = 1408.5f;
+  const float rovcp = 0.28541315f, cpl = 4190.0f, cpi = 2106.0f;
+  FOR_WHOLE(k < g.nz)
+    float reps = DCR(rv, rd);
+    float repsm1 = reps - 1.0f;
+    float gacc = 9.81f;
+    float qvv = fmax_(qv[c], 0.0f);
+    float liq = qc[c] + qr[c];
+    float ice = (qi[c] + qs[c]) + qg[c];
+    float qli = fmax_(0.0f, liq + ice);
+    float cpli = fmaf(cpl, fmax_(0.0f, liq), cpi * fmax_(0.0f, ice));
+    float th = th0[k] + thp[c];
+    float pi = pi0[k] + ppp[c];
+    float cpm = fmaf(cpv, qvv, cp) + cpli;
+    float cvm = DCR(1.0f, fmaf(cvv, qvv, cv) + cpli);
+    thv[c] = DCR(th * fmaf(reps, qvv, 1.0f), (1.0f + qvv) + qli);
+    piadv[c] = pi;
+    ppterm[c] = ((pi * rovcp) * cpm) * cvm;
+    thterm[c] = (th * fmaf(-rovcp, cpm, fmaf(rv, qvv, rd))) * cvm;
+    buoy[c] = gacc * (fmaf(thp[c], rth0[k], repsm1 * (qvv - qv0[k])) - ((qli - qc0[k]) - qi0[k]));
+  }
+}
+
+/* f_rr_* double-float helpers (pressure_tendency.wgsl:114-226): a correctly rounded
+ * powf built from a two-float log and exp */
+typedef struct { float x, y; } F2;
+static inline F2 two_sum(float a, float b) {
+  float s = a + b, bb = s - a;
+  F2 r = {s, (a - (s - bb)) + (b - bb)};
+  return r;
+}
+static inline F2 quick_two_sum(float a, float b) {
+  float s = a + b;
+  F2 r = {s, b - (s - a)};
+  return r;
+}
+static inline F2 mul_ff(F2 a, F2 b) {
+  float p = a.x * b.x;
+  float e = fmaf(a.x, b.x, -p);
+  e = fmaf(a.x, b.y, e);
+  e = fmaf(a.y, b.x, e);
+  return quick_two_sum(p, e);
+}
+static inline F2 add_ff(F2 a, F2 b) {
+  F2 s = two_sum(a.x, b.x), t = two_sum(a.y, b.y);
+  F2 u = quick_two_sum(s.x, s.y + t.x);
+  return quick_two_sum(u.x, u.y + t.y);
+}
+static inline F2 mkf2(float x, float y) { F2 r = {x, y}; return r; }
+static F2 rr_log_ff(float x) {
+  int e;
+  float m = frexpf(x, &e);
+  if (m < 0.70710677f) { m = m * 2.0f; e = e - 1; }
+  float f = m - 1.0f;
+  F2 d = two_sum(2.0f, f);
+  float sh = DCR(f, d.x);
+  float r = fmaf(-sh, d.x, f);
+  r = fmaf(-sh, d.y, r);
+  F2 sf = quick_two_sum(sh, DCR(r, d.x));
+  F2 s2 = mul_ff(sf, sf), s3 = mul_ff(s2, sf);
+  F2 P = mkf2(0.11764706f, -4.3826945e-10f);
+  P = add_ff(mul_ff(P, s2), mkf2(0.13333334f, -6.9538753e-09f));
+  P = add_ff(mul_ff(P, s2), mkf2(0.15384616f, -5.731216e-09f));
+  P = add_ff(mul_ff(P, s2), mkf2(0.18181819f, -5.4186042e-09f));
+  P = add_ff(mul_ff(P, s2), mkf2(0.22222222f, -1.6556846e-09f));
+  P = add_ff(mul_ff(P, s2), mkf2(0.2857143f, -1.2772424e-08f));
+  P = add_ff(mul_ff(P, s2), mkf2(0.4f, -5.9604646e-09f));
+  P = add_ff(mul_ff(P, s2), mkf2(0.6666667f, -1.9868216e-08f));
+  F2 l1p = add_ff(mkf2(2.0f * sf.x, 2.0f * sf.y), mul_ff(s3, P));
+  const float ln2h = 0.69314575f, ln2m = 1.4285906e-06f, ln2l = 1.6198487e-11f;
+  float fe = (float)e;
+  F2 a = add_ff(mkf2(fe * ln2h, fe * ln2m), l1p);
+  return add_ff(a, mkf2(fe * ln2l, 0.0f));
+}
+static float rr_exp_ff(F2 y) {
+  const float ln2h = 0.69314575f, ln2m = 1.4285906e-06f, ln2l = 1.6198487e-11f;
+  float k = nearbyintf(DCR(y.x, 0.6931472f));
+  F2 r = add_ff(y, mkf2((-k) * ln2h, (-k) * ln2m));
+  r = add_ff(r, mkf2((-k) * ln2l, 0.0f));
+  F2 P = mkf2(2.5052108e-08f, 4.417623e-16f);
+  P = add_ff(mul_ff(P, r), mkf2(2.755732e-07f, -7.575112e-15f));
+  P = add_ff(mul_ff(P, r), mkf2(2.7557319e-06f, 3.7935712e-14f));
+  P = add_ff(mul_ff(P, r), mkf2(2.4801588e-05f, -3.406996e-13f));
+  P = add_ff(mul_ff(P, r), mkf2(0.0001984127f, -2.7255969e-12f));
+  P = add_ff(mul_ff(P, r), mkf2(0.0013888889f, -3.3631094e-11f));
+  P = add_ff(mul_ff(P, r), mkf2(0.008333334f, -4.346172e-10f));
+  P = add_ff(mul_ff(P, r), mkf2(0.041666668f, -1.2417635e-09f));
+  P = add_ff(mul_ff(P, r), mkf2(0.16666667f, -4.967054e-09f));
+  P = add_ff(mul_ff(P, r), mkf2(0.5f, 0.0f));
+  P = add_ff(mul_ff(P, r), mkf2(1.0f, 0.0f));
+  F2 Q = mul_ff(P, r);
+  float s = 1.0f + Q.x;
+  float t = (1.0f - s) + Q.x;
+  F2 ur = two_sum(t, Q.y);
+  float res = s + ur.x;
+  float bb = res - s;
+  float e3 = (s - (res - bb)) + (ur.x - bb);
+  if (e3 != 0.0f && ur.y != 0.0f && (e3 > 0.0f) == (ur.y > 0.0f)) {
+    float nb = bitsf(fbits(res) + (e3 > 0.0f ? 1u : 4294967295u));
+    if (e3 + e3 == nb - res) res = nb;
+  }
+  return ldexpf(res, (int)k);
+}
+float te_rr_pow_cr(float x, float p) {
+  if (!(x > 0.0f) || (fbits(x) & 0x7fffffffu) == 0x7f800000u) return powf(x, p);
+  F2 L = rr_log_ff(x);
+  float yh = L.x * p;
+  return rr_exp_ff(quick_two_sum(yh, fmaf(L.y, p, fmaf(L.x, p, -yh))));
+}
+
+void teor_pressure_tendency(uint32_t *M, const uint32_t *ARG) {
+  /* pressure_tendency.wgsl main: pi' forcing from the step tendencies of th and qv */
+  Dims g = dims_at(M, B(0));
+  const float *th = FPTR(1), *qv = FPTR(2), *rho = FPTR(3), *ppi = FPTR(4), *thten = FPTR(5), *qpten = FPTR(6);
+  const float *th0 = FPTR(7), *pi0 = FPTR(8);
+  float dt = FVAL(9);
+  int hasDiabatic = IVAL(10);
+  float *ppten = FPTR(11);
+  int hasStepTend = IVAL(12);
+  const float *qvt = FPTR(13);
+  int moist = IVAL(14);
+  const float rd = 287.04f, rv = 461.5f, cp = 1005.7f, p00 = 1e5f;
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    float rp00 = DCR(1.0f, p00);
+    float rddcv = DCR(rd, cp - rd);
+    float tem = 0.0001f * 0.0001f;
+    float qsmall = 1e-14f;
+    float tht = hasStepTend != 0 ? thten[c] : 0.0f;
+    if (moist == 0) {
+      float p = 0.0f;
+      if (fabsf(dt * tht) > tem) {
+        float thnew = fmaf(dt, tht, th[c]);
+        float pinew = te_rr_pow_cr(((rho[c] * (th0[k] + thnew)) * rd) * rp00, rddcv) - pi0[k];
+        p = DCR(pinew - ppi[c], dt);
+      }
+      ppten[c] = p;
+      continue;
+    }
+    float qvten = qvt[c];
+    float p = 0.0f;
+    if (fabsf(dt * tht) > tem || fabsf(dt * qvten) > qsmall) {
+      float thnew = fmaf(dt, tht, th[c]);
+      float qvnew = fmaf(dt, qvten, qv[c]);
+      float pinew = te_rr_pow_cr(((rho[c] * (th0[k] + thnew)) * fmaf(rv, qvnew, rd)) * rp00, rddcv) - pi0[k];
+      p = DCR(pinew - ppi[c], dt);
+    }
+    if (hasDiabatic != 0) p = p + qpten[c];
+    ppten[c] = p;
+  }
+}
+
+void teor_divergence3d(uint32_t *M, const uint32_t *ARG) {
+  /* divergence3d.wgsl main (|d| < 1e-30 -> 0) */
+  Dims g = dims_at(M, B(0));
+  const float *u = FPTR(1), *v = FPTR(2), *w = FPTR(3), *mh = FPTR(4);
+  float *div = FPTR(5);
+  const float *hm = FPTR(30);
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    float d = fmaf((w[c + sk] - w[c]) * g.rdz, mh[k],
+                   fmaf((u[c + 1] - u[c]) * g.rdx, hm_uh(&g, hm, i), ((v[c + sj] - v[c]) * g.rdy) * hm_vh(&g, hm, j)));
+    div[c] = fabsf(d) < 1e-30f ? 0.0f : d;
+  }
+}
+
+void teor_update_rho_prs(uint32_t *M, const uint32_t *ARG) {
+  /* update_rho_prs.wgsl main: prs = p00 pi^(cp/rd), rho = prs / (th pi rmix) */
+  Dims g = dims_at(M, B(0));
+  int moist = IVAL(1);
+  const float *thp = FPTR(2), *ppp = FPTR(3), *th0 = FPTR(4), *pi0 = FPTR(5), *qv = FPTR(6);
+  float *prs = FPTR(7), *rho = FPTR(8);
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    float cpdrd = DCR(1005.7f, 287.04f);
+    float pi = pi0[k] + ppp[c];
+    float th = th0[k] + thp[c];
+    float p = 1e5f * te_rr_pow_cr(pi, cpdrd);
+    prs[c] = p;
+    float rmix = moist != 0 ? fmaf(fmax_(0.0f, qv[c]), 461.5f, 287.04f) : 287.04f;
+    rho[c] = DCR(p, (th * pi) * rmix);
+  }
+}
+
+void teor_diabatic_unapply(uint32_t *M, const uint32_t *ARG) {
+  /* diabatic_unapply.wgsl main: remove last step's diabatic tendencies, keep values */
+  Dims g = dims_at(M, B(0));
+  float dt = FVAL(1);
+  float *pp3d = FPTR(2), *th = FPTR(3), *qv = FPTR(4), *qc = FPTR(5);
+  float *qpten = FPTR(6), *qtten = FPTR(7), *qvten = FPTR(8), *qcten = FPTR(9);
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    pp3d[c] = fmaf(-dt, qpten[c], pp3d[c]);
+    qpten[c] = pp3d[c];
+    th[c] = fmaf(-dt, qtten[c], th[c]);
+    qtten[c] = th[c];
+    qv[c] = fmaf(-dt, qvten[c], qv[c]);
+    qvten[c] = qv[c];
+    qc[c] = fmaf(-dt, qcten[c], qc[c]);
+    qcten[c] = qc[c];
+  }
+}
+
+void teor_diabatic_rates(uint32_t *M, const uint32_t *ARG) {
+  /* diabatic_rates.wgsl main */
+  Dims g = dims_at(M, B(0));
+  float dt = FVAL(1);
+  const float *pp3d = FPTR(2), *th = FPTR(3), *qv = FPTR(4), *qc = FPTR(5);
+  float *qpten = FPTR(6), *qtten = FPTR(7), *qvten = FPTR(8), *qcten = FPTR(9);
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    float rdt = DCR(1.0f, dt);
+    qpten[c] = (pp3d[c] - qpten[c]) * rdt;
+    qtten[c] = (th[c] - qtten[c]) * rdt;
+    qvten[c] = (qv[c] - qvten[c]) * rdt;
+    qcten[c] = (qc[c] - qcten[c]) * rdt;
+  }
+}
+
+void teor_ppx_finish(uint32_t *M, const uint32_t *ARG) {
+  /* ppx_finish.wgsl main: ppx = pp3d + ppx */
+  Dims g = dims_at(M, B(0));
+  const float *pp3d = FPTR(1);
+  float *ppx = FPTR(2);
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    ppx[c] = pp3d[c] + ppx[c];
+  }
 }

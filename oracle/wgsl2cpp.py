@@ -17,8 +17,10 @@ C++ only into ``oracle/_ref/`` (git-ignored); no reference source is committed.
 
 Semantics kept: every f32 operation is one IEEE binary32 operation (compiled with
 ``-ffp-contract=off``, no fast-math), ``fma`` is a fused multiply-add, i32 wraps
-(``-fwrapv``), ``opq(x)`` is the identity (the slot word ARG[3] is always 0,
-replay.js:266-269), ``select(f, t, c)`` evaluates both operands.
+(``-fwrapv``), ``opq(x)`` returns x (the slot word ARG[3] is always 0,
+replay.js:266-269) through an empty asm so the compiler cannot fold across it, as the
+reference intends (adv_flux_x_weno.wgsl:15-21), ``select(f, t, c)`` evaluates both
+operands.
 
 Usage: python oracle/wgsl2cpp.py --src <kernels dir> --out oracle/_ref/gen
 """
@@ -118,11 +120,14 @@ static inline void W_atomicStore(u32* p, u32 v) { __atomic_store_n(p, v, __ATOMI
 static inline u32 W_atomicAdd(u32* p, u32 v) { return __atomic_fetch_add(p, v, __ATOMIC_RELAXED); }
 static inline u32 W_atomicMax(u32* p, u32 v) { u32 o = __atomic_load_n(p, __ATOMIC_RELAXED);
   while (o < v && !__atomic_compare_exchange_n(p, &o, v, true, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {} return o; }
-static inline f32 opq(f32 x) { return x; }
-static inline vec2<f32> opq2(vec2<f32> x) { return x; }
-static inline vec3<f32> opq3(vec3<f32> x) { return x; }
-static inline vec4<f32> opq4(vec4<f32> x) { return x; }
-static inline f32 nego(f32 x) { return W_bitcast<f32>(W_bitcast<u32>(x) ^ 0x80000000u); }
+// opq(): the reference's rounding barrier (x | Z0 with Z0 = 0 unknown to the compiler).
+// An empty asm on the value keeps the same meaning here: the compiler may not fold or
+// reassociate across it (e.g. -fma(a,b,c) -> fma(-a,b,-c), which flips signed zeros).
+static inline f32 opq(f32 x) { __asm__("" : "+x"(x)); return x; }
+static inline vec2<f32> opq2(vec2<f32> x) { x.x = opq(x.x); x.y = opq(x.y); return x; }
+static inline vec3<f32> opq3(vec3<f32> x) { x.x = opq(x.x); x.y = opq(x.y); x.z = opq(x.z); return x; }
+static inline vec4<f32> opq4(vec4<f32> x) { x.x = opq(x.x); x.y = opq(x.y); x.z = opq(x.z); x.w = opq(x.w); return x; }
+static inline f32 nego(f32 x) { return opq(W_bitcast<f32>(W_bitcast<u32>(x) ^ 0x80000000u)); }
 '''
 
 BUILTINS = ['fma', 'abs', 'min', 'max', 'clamp', 'sqrt', 'floor', 'round', 'trunc', 'exp', 'log', 'log2',
