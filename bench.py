@@ -1,0 +1,440 @@
+"""Benchmark: CM1 large-step dynamics (WENO5 advection + acoustic substeps) on B200.
+
+One "step" is one large time step (3 RK stages, 15 acoustic substeps at nsound=8) of the
+256x256x80 synthetic Weisman-Klemp supercell workload, played as the reference's command
+tape through the C-ABI player.  Metric: grid-pt-steps/s = nx*ny*nz*steps / time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--mode fused|exact]
+
+Multi-GPU (torchrun, one process per GPU): each rank advances its own independent
+replica (ensemble member); no collective on the data path ("replicas only"), the
+timed region is bracketed by barriers and the max over ranks is reported.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = 'grid-pt-steps/s'
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=10)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--mode', default='fused', choices=['fused', 'exact'])
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-e2e', action='store_true')
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- distributed
+
+def dist_init(n):
+    rank = int(os.environ.get('RANK', '0'))
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        backend = 'nccl' if torch.cuda.is_available() else 'gloo'
+        if backend == 'nccl':
+            torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group(backend, timeout=timedelta(seconds=600))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64,
+                     device='cuda' if dist.get_backend() == 'nccl' else 'cpu')
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# --------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,'
+         'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
+         'clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.device), '--query-gpu=' + self.Q,
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['nvidia-smi unavailable']}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(',')]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == 'active':
+                    reasons.add(n)
+        return {'sm_mhz': statistics.median(sm) if sm else None, 'sm_max_mhz': mx, 'reasons': sorted(reasons),
+                'samples': len(sm)}
+
+
+# ------------------------------------------------------------------ workload
+
+def workload(cfg_name='at_scale'):
+    from thunderengine_web_b200 import scenario, timestep
+    cfg = scenario.AT_SCALE if cfg_name == 'at_scale' else scenario.SMALL
+    run = timestep.Run(cfg)
+    return cfg, run
+
+
+def peaks():
+    p = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d['hbm_gbs']), 'measured'
+    return 6650.0, 'fallback'
+
+
+def cpu_baseline_sample(run_small_steps=1):
+    """Time the reference's kernels (oracle/_ref, else the oracle port) on the host cores:
+    one large step of a 64x64x80 horizontal sub-domain of the benchmark configuration."""
+    from tests import helpers
+    from thunderengine_web_b200 import scenario, timestep
+    ref = helpers.reference()
+    kind = 'reference' if ref is not None else 'port'
+    kern = (ref or helpers.oracle()).get
+    helpers.oracle()   # FTZ on the OpenMP team
+    cfg = scenario.Config('cm1-dyn-64x64x80-of-256x256x80', 64, 64, 80, 500.0, 250.0, 3.0, 8, 25.0, 1)
+    run = timestep.Run(cfg)
+    tape = run.tape(1)
+    init = run.initial_buffers()
+    from oracle.player import CpuPlayer
+    p = CpuPlayer(tape, helpers.kernels_meta())
+    p.plan(False)
+    for i, b in init.items():
+        p.upload(i, b)
+    p.run(kern)                      # warm-up step
+    t0 = time.perf_counter()
+    for _ in range(run_small_steps):
+        p.run(kern)
+    dt = time.perf_counter() - t0
+    pts = cfg.nx * cfg.ny * cfg.nz
+    return {'value': pts * run_small_steps / dt, 'unit': METRIC, 'cores': os.cpu_count(), 'kind': kind,
+            'sample': '%d large step(s) of a 64x64x80 sub-domain of the 256x256x80 workload (same dx, dz, dt, '
+                      'nsound) with %s kernels, OpenMP over the dispatch grid' % (
+                          run_small_steps, 'the reference\'s WGSL translated to C++' if kind == 'reference'
+                          else 'the oracle'),
+            'seconds': dt}
+
+
+# ---------------------------------------------------------------- our arm
+
+def run_ours(a, rank, world, local):
+    import torch
+    from thunderengine_web_b200.replayer import Replayer, TE_MODE_EXACT, TE_MODE_FUSED
+    from tests import helpers
+    dev = local if torch.cuda.device_count() > local else 0
+    torch.cuda.set_device(dev)
+    cfg, run = workload()
+    tape = run.tape(1)
+    run.tape_cmds = tape['steps'][0]
+    init = run.initial_buffers()
+    r = Replayer(tape, None, device=dev)
+    r.plan(False)
+    r.build()
+    for i, b in init.items():
+        r.upload(i, b)
+    stream = torch.cuda.current_stream(dev)
+    r.set_stream(stream.cuda_stream)
+    mode = TE_MODE_FUSED if a.mode == 'fused' else TE_MODE_EXACT
+    r.set_mode(mode)
+    pts = cfg.nx * cfg.ny * cfg.nz
+    for _ in range(max(a.warmup, 3)):
+        r.encode_steps(1)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(dev)
+    sampler.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    r.encode_steps(a.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(ms, world)
+    value = pts * a.steps * world / (ms / 1e3)
+
+    # per-kernel timing for the roofline: each distinct op of the step alone, events on
+    # the launch stream; achieved = algorithmic bytes per launch / launch time
+    roof = kernel_roofline(r, run, stream, mode)
+
+    # end to end through the public API with host buffers: every step uploads the state
+    # fields from pinned memory, plays the step, reads the prognostic fields back
+    e2e = None if a.no_e2e else end_to_end(r, run, init, cfg, a, world)
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline_sample()
+    ops = r.num_ops
+    launches = roof.pop('_launches_per_step')
+    out = {
+        'metric': METRIC, 'value': value, 'unit': METRIC, 'n_gpus': world, 'steps': a.steps, 'warmup': a.warmup,
+        'ms_per_step': ms / a.steps, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+        'dtype': 'f32', 'data': 'synthetic (Weisman-Klemp sounding, 2 K bubble, seeded noise)',
+        'config': dict(cfg.as_dict(), grid_points=pts, mode=a.mode, parallelism='replicas x%d' % world,
+                       tape_ops_per_step=ops,
+                       l2='inputs larger than L2: %.2f GB arena per replica' % (run.arena_bytes / 1e9)),
+        'roofline': roof, 'cpu_baseline': cpu, 'e2e': e2e, 'gpu_launches': launches * a.steps, 'clocks': clocks,
+    }
+    if rank == 0:
+        print(json.dumps(out))
+    r.close()
+
+
+def kernel_roofline(r, run, stream, mode):
+    import torch
+    from tests import helpers
+    peak, src = peaks()
+    tape_fields = run.fields
+    g = run.grid
+    field_of = {}
+    arena_base = r.base[run.rec.ids['arena']]
+    for n, off in tape_fields.items():
+        field_of[arena_base + off // 4] = n
+    km = helpers.kernels_meta()
+    stats = {}
+    nops = r.num_ops
+    names = [r.op_name(i) for i in range(nops)]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # time each distinct kernel (first occurrence), reps launches
+    seen = {}
+    for i, n in enumerate(names):
+        if n == 'copy':
+            continue
+        seen.setdefault(n, []).append(i)
+    reps = 5
+    for n, idx in seen.items():
+        i = idx[0]
+        r.run_ops(i, i)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            r.run_ops(i, i)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / reps
+        stats[n] = {'ms': t, 'launches': len(idx)}
+    tot = sum(s['ms'] * s['launches'] for s in stats.values())
+    top = max(stats, key=lambda n: stats[n]['ms'] * stats[n]['launches'])
+    disp = tape_dispatches(run, run.tape_cmds)
+    bytes_per_launch = dispatch_bytes(disp[seen[top][0]], km)
+    ms = stats[top]['ms']
+    achieved = bytes_per_launch / (ms / 1e3) / 1e9
+    shares = sorted(((n, s['ms'] * s['launches'] / tot) for n, s in stats.items()), key=lambda x: -x[1])
+    launches_per_step = sum(s['launches'] for s in stats.values())
+    return {'kernel': top, 'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+            'frac': achieved / peak, 'peak_source': '%s (MEASURED_PEAKS.json hbm_gbs)' % src if src == 'measured'
+            else 'fallback 6650 GB/s', 'algorithmic_bytes_per_launch': bytes_per_launch,
+            'launch_ms': ms, 'traffic': None, 'share_of_step': shares[0][1],
+            'top_kernels': [[n, round(s, 4)] for n, s in shares[:8]], '_launches_per_step': launches_per_step}
+
+
+# Fields a kernel both reads and writes at the same points (binding indices), counted
+# twice in the algorithmic bytes; every other bound arena field counts once.
+RMW = {
+    'acoustic_uv': (6, 7), 'acoustic_w_solve': (9,), 'acoustic_pp': (7,), 'acoustic_accumulate': (5, 6, 7),
+    'pdef_apply': (16,), 'buoyancy_apply': (4,), 'apply_thterm': (3,), 'velocity_to_massflux': (3, 4, 5),
+    'diabatic_unapply': (2, 3, 4, 5, 6, 7, 8, 9), 'diabatic_rates': (6, 7, 8, 9), 'ppx_finish': (2,),
+    'bc_periodic_x': (1,), 'bc_periodic_y': (1,),
+}
+
+
+def tape_dispatches(run, cmds):
+    """Per op of a step (dispatches and copies, in op order): kernel name, grid and the
+    arena field bound at each binding index."""
+    by_off = {off: n for n, off in run.fields.items()}
+    arena_id = run.rec.ids['arena']
+    out, bind, pipe = [], {}, None
+    for c in cmds:
+        op = c['op']
+        if op == 'pipe':
+            pipe = c['name']
+        elif op == 'buf':
+            bind[c['index']] = by_off.get(c['offset']) if c['buf'] == arena_id else None
+        elif op == 'bytes':
+            bind[c['index']] = None
+        elif op == 'end':
+            bind = {}
+        elif op == 'copy':
+            out.append({'name': 'copy', 'grid': [c['size'] // 4, 1, 1], 'fields': {}})
+        elif op == 'dispatch':
+            out.append({'name': pipe, 'grid': c['grid'], 'fields': dict(bind)})
+    return out
+
+
+def dispatch_bytes(d, km):
+    """Algorithmic bytes of one dispatch: (distinct arena fields bound to its pointer
+    parameters, read-modify-write fields twice) x 4 B x dispatch points."""
+    params = {p['index']: p for p in km[d['name']]['params']}
+    fields = {}
+    for idx, f in d['fields'].items():
+        p = params.get(idx)
+        if f is None or p is None or p['kind'] != 'ptr':
+            continue
+        w = 2 if idx in RMW.get(d['name'], ()) else 1
+        fields[f] = max(fields.get(f, 0), w)
+    pts = d['grid'][0] * d['grid'][1] * d['grid'][2]
+    return sum(fields.values()) * 4 * pts
+
+
+def end_to_end(r, run, init, cfg, a, world):
+    import torch
+    from thunderengine_web_b200.timestep import SCRATCH_FIELDS
+    g = run.grid
+    aid = run.rec.ids['arena']
+    base = r.base[aid]
+    arena0 = np.frombuffer(init[aid], dtype=np.uint32)
+    state = [n for n in run.fields if n not in SCRATCH_FIELDS]
+    outs = ['th', 'qv', 'u', 'v', 'w', 'pp3d']
+    fw = g.field_stride // 4
+    pin_in = torch.empty((len(state), g.count), dtype=torch.int32).pin_memory()
+    for q, n in enumerate(state):
+        o = run.fields[n] // 4
+        pin_in[q].numpy()[:] = arena0[o:o + g.count].view(np.int32)
+    pin_out = torch.empty((len(outs), g.count), dtype=torch.int32).pin_memory()
+    lib = r.lib
+
+    def one_step():
+        for q, n in enumerate(state):
+            r._check(lib.te_write_words(r.h, base + run.fields[n] // 4, pin_in[q].data_ptr(), g.count * 4))
+        r.encode_steps(1)
+        for q, n in enumerate(outs):
+            r._check(lib.te_read(r.h, base + run.fields[n] // 4, g.count, pin_out[q].data_ptr()))
+
+    for _ in range(2):
+        one_step()
+    torch.cuda.synchronize()
+    barrier(world)
+    steps = max(1, min(a.steps, 5))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        one_step()
+    torch.cuda.synchronize()
+    dt = max_over_ranks(time.perf_counter() - t0, world)
+    barrier(world)
+    pts = cfg.nx * cfg.ny * cfg.nz
+    return {'value': pts * steps * world / dt, 'unit': METRIC, 'h2d_bytes_per_step': len(state) * g.count * 4,
+            'd2h_bytes_per_step': len(outs) * g.count * 4, 'steps': steps,
+            'path': 'Replayer.write_words (pinned host) -> encode_steps(1) -> read (pinned host)'}
+
+
+# -------------------------------------------------------- reference arm (CPU)
+
+def run_reference(a, rank, world):
+    """The reference's own kernels (its WGSL translated to C++, oracle/_ref) on the host
+    cores, same metric; rank 0 only."""
+    if rank != 0:
+        return
+    from tests import helpers
+    from thunderengine_web_b200 import scenario, timestep
+    from oracle.player import CpuPlayer
+    ref = helpers.reference()
+    kind = 'reference' if ref is not None else 'port'
+    kern = (ref or helpers.oracle()).get
+    helpers.oracle()
+    cfg = scenario.Config('cm1-dyn-64x64x80-of-256x256x80', 64, 64, 80, 500.0, 250.0, 3.0, 8, 25.0, 1)
+    run = timestep.Run(cfg)
+    tape = run.tape(1)
+    init = run.initial_buffers()
+    p = CpuPlayer(tape, helpers.kernels_meta())
+    p.plan(False)
+    for i, b in init.items():
+        p.upload(i, b)
+    for _ in range(a.warmup):
+        p.run(kern)
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        p.run(kern)
+    dt = time.perf_counter() - t0
+    pts = cfg.nx * cfg.ny * cfg.nz
+    v = pts * a.steps / dt
+    big = scenario.AT_SCALE
+    out = {'metric': METRIC, 'value': v, 'unit': METRIC, 'n_gpus': world, 'steps': a.steps, 'warmup': a.warmup,
+           'ms_per_step': dt / a.steps * 1e3, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+           'dtype': 'f32', 'data': 'synthetic', 'impl': 'reference',
+           'config': dict(big.as_dict(), sample='64x64x80 horizontal sub-domain, same dx/dz/dt/nsound'),
+           'cpu_baseline': {'value': v, 'unit': METRIC, 'cores': os.cpu_count(), 'kind': kind,
+                            'sample': 'each step = one large step of a 64x64x80 sub-domain of the 256x256x80 workload'},
+           'e2e': {'value': v, 'unit': METRIC, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+    print(json.dumps(out))
+
+
+def main():
+    a = parse()
+    rank, world, local = dist_init(a.gpus)
+    try:
+        if a.impl == 'reference':
+            run_reference(a, rank, world)
+        else:
+            run_ours(a, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,128 @@
+/* thunderstep: B200 (sm_100a) tape player for ThunderEngine's CM1 large-step dynamics.
+ *
+ * Drop-in for the reference's WebGPU tape player `Replayer` (web/replay.js:36-396).
+ * A caller that records tapes with the reference's step encoder (TimeStep.encode,
+ * web/core/timestep.js:797; driver.js:53-74) plays them here unchanged: same tape JSON,
+ * same kernel ABI (data/kernels/kernels.json), same word-addressed memory layout, same
+ * per-dispatch region hashes (replay.js:407-418).  Offsets are 64-bit words (the
+ * reference's ARG slots hold u32 word offsets, replay.js:266-268).
+ *
+ * Conventions: every call returns 0 on success or a negative TE_E* code; the message of
+ * the last failure is te_last_error(ctx).  One context = one CUDA device + one stream;
+ * a context is not thread-safe.  Device work is stream-ordered; te_read, te_read_hashes
+ * and te_sync block until it finishes.
+ */
+#ifndef THUNDERSTEP_H
+#define THUNDERSTEP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TE_OK 0
+#define TE_EINVAL -1     /* bad argument or malformed tape / kernels JSON */
+#define TE_ENOKERNEL -2  /* the tape names a kernel this library does not implement */
+#define TE_ECUDA -3      /* a CUDA runtime call failed */
+#define TE_ESTATE -4     /* call out of order (e.g. te_run before te_plan) */
+#define TE_ERANGE -5     /* offset / size outside the planned memory */
+
+/* Execution modes of te_run (te_set_mode). */
+#define TE_MODE_EXACT 0  /* one CUDA kernel per tape dispatch, reference order */
+#define TE_MODE_FUSED 1  /* recognised step phases run as fused kernels (see te_set_mode) */
+
+typedef struct te_ctx te_ctx;
+
+typedef struct te_config {
+  int device;          /* CUDA device ordinal */
+  int flags;           /* reserved, 0 */
+  uint64_t reserved[4];
+} te_config;
+
+typedef struct te_info {
+  uint64_t mem_words;    /* Replayer.memWords (replay.js:65) */
+  uint64_t buffers_end;  /* Replayer.buffersEnd (replay.js:51) */
+  uint64_t scratch_base; /* word offset of the per-thread scratch area (replay.js:63) */
+  uint32_t hash_count;   /* Replayer.hashCount (replay.js:113) */
+  uint32_t num_buffers;  /* tape.buffers.length */
+  uint32_t num_ops;      /* ops of the active step (kernel dispatches + copies) */
+  uint32_t num_dispatches;
+} te_info;
+
+/* new Replayer(device, tape, kernels, sources) (replay.js:37-42): create a context. */
+int te_create(const te_config *cfg, te_ctx **out);
+
+/* Replayer.plan(withHashes) + Replayer.build() (replay.js:46-66, 180-209): lay out the
+ * word memory for `tape_json`, allocate it on the device, write the setBytes payloads
+ * and prepare the dispatch list of tape.steps[0].  `kernels_json` is the reference's
+ * kernels.json (parameter ABI per kernel; NULL = the built-in table of this library). */
+int te_plan(te_ctx *ctx, const char *tape_json, size_t tape_len, const char *kernels_json,
+            size_t kernels_len, int with_hashes);
+
+int te_get_info(te_ctx *ctx, te_info *out);
+
+/* Replayer.base[buf_id] (replay.js:49): word offset of a tape buffer in memory. */
+int te_buffer_base(te_ctx *ctx, int buf_id, uint64_t *word_off);
+
+/* Replayer.upload(id, u8) (replay.js:301): copy host bytes to the start of a buffer. */
+int te_upload(te_ctx *ctx, int buf_id, const void *data, size_t bytes);
+
+/* Replayer.writeWords(off, data) (replay.js:212-225): copy host bytes to word `word_off`. */
+int te_write_words(te_ctx *ctx, uint64_t word_off, const void *data, size_t bytes);
+
+/* Replayer.useStep(cmds) (replay.js:127-146): make `cmds_json` (a JSON array of tape
+ * commands) the active step.  Same structure as a known step: only changed setBytes
+ * payloads are rewritten; a new structure is planned once and cached. */
+int te_use_step(te_ctx *ctx, const char *cmds_json, size_t len);
+
+/* Replayer.encodeSteps(enc, n, withHashes) + queue submit (replay.js:335-366): play the
+ * active step `nsteps` times.  With hashes, every written binding of every dispatch adds
+ * its region hash to its slot (replay.js:102-115, 407-418); slots are not cleared. */
+int te_run(te_ctx *ctx, int nsteps, int with_hashes);
+
+/* encodeSteps(enc, 1, withHashes, lastOp) restricted to ops [first_op, last_op]. */
+int te_run_ops(te_ctx *ctx, int first_op, int last_op, int with_hashes);
+
+/* Replayer.encodeDiag(enc) (replay.js:299): play tape.diag once. */
+int te_run_diag(te_ctx *ctx);
+
+/* Replayer.read(words, offWords) (replay.js:368-383): copy memory words to the host. */
+int te_read(te_ctx *ctx, uint64_t word_off, uint64_t words, void *out);
+
+/* Replayer.readHashes() (replay.js:385-395): copy min(n, hash_count) slots. */
+int te_read_hashes(te_ctx *ctx, uint32_t *out, size_t n);
+int te_clear_hashes(te_ctx *ctx);
+
+/* Device address of memory word `word_off`, for callers that keep data on the GPU. */
+int te_device_ptr(te_ctx *ctx, uint64_t word_off, void **out);
+
+/* TE_MODE_EXACT (default) or TE_MODE_FUSED.  Fused mode replaces recognised phases of
+ * the step (acoustic substeps, advection of a variable) by fused kernels; prognostic
+ * fields are bit-identical to exact mode, the contents of the step's scratch fields
+ * (fx, fy, fz, fpk, cA, cB, ...) are not kept.  Hash runs always use exact mode. */
+int te_set_mode(te_ctx *ctx, int mode);
+
+/* Name of op `op` of the active step ("copy" for a blit copy), or NULL. */
+const char *te_op_name(te_ctx *ctx, int op);
+
+int te_sync(te_ctx *ctx);
+void te_destroy(te_ctx *ctx);
+const char *te_last_error(te_ctx *ctx);
+
+/* Run on a caller-owned CUDA stream (a cudaStream_t; NULL = the context's own stream),
+ * e.g. to time launches with events recorded on that stream. */
+int te_set_stream(te_ctx *ctx, void *cuda_stream);
+
+/* The built-in kernel table as kernels.json-shaped JSON ({name: {params: [...]}}),
+ * written to buf (NUL-terminated, truncated to n).  Returns the full length. */
+size_t te_kernel_table_json(char *buf, size_t n);
+
+/* Region hash of `words` host words with the reference formula (replay.js:407-418). */
+uint32_t te_region_hash_host(const uint32_t *words, uint64_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -84,9 +84,11 @@ float te_sqrt_cr(float x) {
   return sqrt_core(x);
 }
 
-/* WGSL min/max on f32 (the reference maps them to IEEE minNum/maxNum) */
-static inline float fmin_(float a, float b) { return fminf(a, b); }
-static inline float fmax_(float a, float b) { return fmaxf(a, b); }
+/* WGSL min/max on f32: min(a, b) is b if b < a, else a; max(a, b) is b if a < b,
+ * else a; a NaN operand yields the other one.  This fixes the sign of a zero result
+ * when the operands are +0 and -0. */
+static inline float fmin_(float a, float b) { return (b < a || a != a) ? b : a; }
+static inline float fmax_(float a, float b) { return (a < b || a != a) ? b : a; }
 
 /* --------------------------------------------------------------- grid access */
 

@@ -70,8 +70,9 @@ static inline vec4<f32> W_fma(vec4<f32> a, vec4<f32> b, vec4<f32> c) { return ve
 static inline f32 W_abs(f32 a) { return fabsf(a); }
 static inline i32 W_abs(i32 a) { return a < 0 ? -a : a; }
 static inline u32 W_abs(u32 a) { return a; }
-static inline f32 W_min(f32 a, f32 b) { return fminf(a, b); }
-static inline f32 W_max(f32 a, f32 b) { return fmaxf(a, b); }
+// WGSL min/max: min(a, b) = b if b < a else a; max(a, b) = b if a < b else a; NaN -> other
+static inline f32 W_min(f32 a, f32 b) { return (b < a || a != a) ? b : a; }
+static inline f32 W_max(f32 a, f32 b) { return (a < b || a != a) ? b : a; }
 static inline i32 W_min(i32 a, i32 b) { return a < b ? a : b; }
 static inline i32 W_max(i32 a, i32 b) { return a > b ? a : b; }
 static inline u32 W_min(u32 a, u32 b) { return a < b ? a : b; }

@@ -1,0 +1,35 @@
+"""Copy the reference's golden recordings used by the parity tests into tests/golden/.
+
+Run in a checkout that has the reference at REF (default /root/reference):
+    python tests/golden/make_golden.py [REF]
+Copies, unchanged:
+  data/kernels/kernels.json          kernel parameter ABI (binding index, ptr/ref, write)
+  data/single_cell/tape.json         recorded command stream of steps 1-2 (718 dispatches)
+  data/single_cell/state/<id>.bin.gz every buffer before step 1
+  data/single_cell/hashes.ref.bin    1010 per-dispatch region hashes of step 1
+  data/single_cell/step1.json        FNV-1a of every buffer after step 1
+These are recordings of the upstream implementation shipped with the reference
+(web/view.js:1039-1068, web/replay.html:190-232); the tests replay them.
+"""
+import os
+import shutil
+import sys
+
+REF = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def main():
+    shutil.copy(os.path.join(REF, 'data/kernels/kernels.json'), os.path.join(OUT, 'kernels.json'))
+    src = os.path.join(REF, 'data/single_cell')
+    dst = os.path.join(OUT, 'single_cell')
+    os.makedirs(os.path.join(dst, 'state'), exist_ok=True)
+    for f in ('tape.json', 'hashes.ref.bin', 'step1.json'):
+        shutil.copy(os.path.join(src, f), os.path.join(dst, f))
+    for f in os.listdir(os.path.join(src, 'state')):
+        shutil.copy(os.path.join(src, 'state', f), os.path.join(dst, 'state', f))
+    print('golden fixtures written to', OUT)
+
+
+if __name__ == '__main__':
+    main()

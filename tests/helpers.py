@@ -1,0 +1,116 @@
+"""Shared test helpers: oracle / reference kernel sets, CPU replays, GPU replays."""
+import ctypes
+import json
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, 'tests', 'golden')
+ORACLE_SO = os.path.join(ROOT, 'oracle', 'liboracle.so')
+REF_SO = os.path.join(ROOT, 'oracle', '_ref', 'libteref.so')
+
+# Scratch fields of a step (timestep.js:334-337 Fields.scratchFields): their contents
+# between dispatches are not part of the step's result.
+SCRATCH = ['rru', 'rrv', 'rrw', 'fx', 'fy', 'fz', 'tend', 'divx', 'qk', 'pk1', 'pk2', 'mm', 'fpk', 'cA', 'cB',
+           'sadv']
+
+_ORACLE = None
+_REF = None
+
+
+def oracle():
+    """The hand-written C oracle (built by oracle/Makefile), FTZ/DAZ enabled."""
+    global _ORACLE
+    if _ORACLE is None:
+        from oracle.player import KernelSet
+        if not os.path.exists(ORACLE_SO):
+            subprocess.check_call(['make', '-C', os.path.join(ROOT, 'oracle')])
+        _ORACLE = KernelSet(ORACLE_SO, 'teor_')
+        _ORACLE.lib.te_set_ftz(1)
+    return _ORACLE
+
+
+def reference():
+    """The reference's own kernels translated to C++ (oracle/_ref), or None."""
+    global _REF
+    if _REF is None:
+        if not os.path.exists(REF_SO):
+            return None
+        from oracle.player import KernelSet
+        _REF = KernelSet(REF_SO, 'teref_')
+        oracle()   # FTZ/DAZ on the shared OpenMP team
+    return _REF
+
+
+def kernels_meta():
+    with open(os.path.join(GOLDEN, 'kernels.json')) as fh:
+        return json.load(fh)
+
+
+def mixed(name):
+    """Oracle kernel where one exists, else the translated reference kernel."""
+    o = oracle()
+    if o.has(name):
+        return o.get(name)
+    r = reference()
+    if r is None:
+        raise RuntimeError('kernel %s needs oracle/_ref' % name)
+    return r.get(name)
+
+
+def cpu_run(tape, init, nsteps=1, hashes=True, kernels=None):
+    """Replay a tape on the CPU oracle; returns the player (memory in .M)."""
+    from oracle.player import CpuPlayer
+    p = CpuPlayer(tape, kernels_meta())
+    p.plan(hashes)
+    for i, b in init.items():
+        p.upload(i, b)
+    kern = kernels or oracle().get
+    for _ in range(nsteps):
+        p.run(kern, with_hashes=hashes)
+    return p
+
+
+def gpu_replayer(tape, init, hashes=True, kernels_json=True, mode=0):
+    from thunderengine_web_b200.replayer import Replayer
+    r = Replayer(tape, kernels_meta() if kernels_json else None)
+    r.plan(hashes)
+    r.build()
+    for i, b in init.items():
+        r.upload(i, b)
+    if mode:
+        r.set_mode(mode)
+    return r
+
+
+def field_view(mem, run_or_tape, base, name):
+    """(k, j, i) float32 view of an arena field from a memory word array."""
+    if hasattr(run_or_tape, 'fields'):
+        fields, g = run_or_tape.fields, run_or_tape.grid
+        sJ, sK, nz, count = g.strideJ, g.strideK, g.nz, g.count
+    else:
+        t = run_or_tape
+        fields = t['fields']
+        sJ, sK, nz = t['nx'] + 7, t['ny'] + 7, t['nz']
+        count = sJ * sK * (nz + 1)
+    off = base + fields[name] // 4
+    return mem[off:off + count].view(np.float32).reshape(nz + 1, sK, sJ)
+
+
+def load_golden_scenario(name='single_cell'):
+    import gzip
+    d = os.path.join(GOLDEN, name)
+    with open(os.path.join(d, 'tape.json')) as fh:
+        tape = json.load(fh)
+    init = {}
+    for b in tape['buffers']:
+        p = os.path.join(d, 'state', '%d.bin.gz' % b['id'])
+        if os.path.exists(p):
+            with gzip.open(p, 'rb') as fh:
+                init[b['id']] = fh.read()
+    hashes = np.fromfile(os.path.join(d, 'hashes.ref.bin'), dtype=np.uint32)
+    with open(os.path.join(d, 'step1.json')) as fh:
+        step1 = {int(k): v for k, v in json.load(fh).items()}
+    return tape, init, hashes, step1

@@ -1,0 +1,159 @@
+"""CUDA path (through the C-ABI) against the CPU oracle and the golden recording."""
+import numpy as np
+import pytest
+
+from tests import helpers
+from thunderengine_web_b200 import scenario, timestep
+
+pytestmark = pytest.mark.gpu
+
+
+def _compare(run, tape, init, nsteps, mode=0, hashes=True):
+    cpu = helpers.cpu_run(tape, init, nsteps=nsteps, hashes=hashes)
+    gpu = helpers.gpu_replayer(tape, init, hashes=hashes, mode=mode)
+    for _ in range(nsteps):
+        gpu.encode_steps(1, with_hashes=hashes)
+    mem = gpu.read(gpu.buffers_end)
+    return cpu, gpu, mem
+
+
+def test_tiny_step_bit_exact_every_dispatch():
+    run = timestep.Run(scenario.tiny(16, 12, 10))
+    tape = run.tape(1)
+    init = run.initial_buffers()
+    cpu, gpu, mem = _compare(run, tape, init, nsteps=2)
+    assert gpu.hash_count == cpu.hash_count
+    h = gpu.read_hashes()
+    bad = np.nonzero(h != cpu.hashes[:gpu.hash_count])[0]
+    assert bad.size == 0, [gpu.op_name(0)] + list(bad[:5])
+    assert np.array_equal(mem, cpu.M[:gpu.buffers_end])
+
+
+def test_small_config_step_bit_exact():
+    cfg = scenario.SMALL   # 64x64x40, dt 6 s, nsound 6
+    run = timestep.Run(cfg)
+    tape = run.tape(1)
+    init = run.initial_buffers()
+    cpu, gpu, mem = _compare(run, tape, init, nsteps=1, hashes=False)
+    assert np.array_equal(mem, cpu.M[:gpu.buffers_end])
+
+
+def test_nsound8_grid_not_multiple_of_block():
+    run = timestep.Run(scenario.tiny(37, 29, 13, dx=500.0, dz=250.0, dt=3.0, nsound=8, us=25.0))
+    tape = run.tape(1)
+    init = run.initial_buffers()
+    cpu, gpu, mem = _compare(run, tape, init, nsteps=1)
+    assert np.array_equal(gpu.read_hashes(), cpu.hashes[:gpu.hash_count])
+    assert np.array_equal(mem, cpu.M[:gpu.buffers_end])
+
+
+def test_subnormal_inputs_flush_like_the_oracle():
+    """Perturbations scaled to ~1e-36 drive WENO smoothness terms below FLT_MIN."""
+    run = timestep.Run(scenario.tiny(16, 12, 10))
+    tape = run.tape(1)
+    init = run.initial_buffers()
+    arena = np.frombuffer(init[run.rec.ids['arena']], dtype=np.float32).copy()
+    g = run.grid
+    for name in ('th', 'th_a'):
+        o = run.fields[name] // 4
+        arena[o:o + g.count] *= np.float32(1e-36)
+    o = run.fields['w'] // 4
+    arena[o:o + g.count] = np.float32(3e-39)          # subnormal input
+    init[run.rec.ids['arena']] = arena.tobytes()
+    cpu, gpu, mem = _compare(run, tape, init, nsteps=1)
+    assert np.array_equal(gpu.read_hashes(), cpu.hashes[:gpu.hash_count])
+    assert np.array_equal(mem, cpu.M[:gpu.buffers_end])
+
+
+def test_use_step_rewrites_changed_parameters():
+    run = timestep.Run(scenario.tiny(16, 12, 10))
+    tape = run.tape(1)
+    init = run.initial_buffers()
+    gpu = helpers.gpu_replayer(tape, init, hashes=False)
+    gpu.encode_steps(1)
+    run.dt = timestep.f(5.0)                       # new dt: same structure, new bytes
+    run.schedule = timestep.AcousticSchedule(6, run.dt)
+    cmds = run.encode()
+    gpu.use_step(cmds)
+    gpu.encode_steps(1)
+    mem = gpu.read(gpu.buffers_end)
+    cpu = helpers.cpu_run(tape, init, nsteps=1, hashes=False)
+    cpu.use_step(cmds)
+    cpu.run(helpers.oracle().get)
+    assert np.array_equal(mem, cpu.M[:gpu.buffers_end])
+
+
+def test_unknown_kernel_is_an_error():
+    run = timestep.Run(scenario.tiny(8, 8, 6))
+    tape = run.tape(1)
+    tape['steps'][0] = [{'op': 'pipe', 'name': 'no_such_kernel'},
+                        {'op': 'dispatch', 'kind': 'threads', 'grid': [1, 1, 1], 'tg': [1, 1, 1]}]
+    from thunderengine_web_b200.replayer import Replayer
+    r = Replayer(tape, helpers.kernels_meta())
+    r.plan(False)
+    with pytest.raises(RuntimeError, match='no kernel'):
+        r.build()
+
+
+def test_golden_single_cell_in_scope_dispatches():
+    """Recorded single_cell step 1: every in-scope dispatch runs on the GPU (the others on
+    the CPU reference build); region hashes and buffer FNVs are compared with the
+    recording.  Scratch tend/fpk hashes are exempt as the reference documents."""
+    ref = helpers.reference()
+    if ref is None:
+        pytest.skip('oracle/_ref not built')
+    from oracle.player import CpuPlayer, fnv1a
+    tape, init, want, step1 = helpers.load_golden_scenario()
+    km = helpers.kernels_meta()
+    cpu = CpuPlayer(tape, km)
+    cpu.plan(True)
+    for i, b in init.items():
+        cpu.upload(i, b)
+    gpu = helpers.gpu_replayer(tape, init, hashes=True)
+    assert gpu.mem_words == cpu.mem_words and gpu.hash_count == want.size
+    from thunderengine_web_b200 import replayer as rp
+    import ctypes
+    # which ops the GPU library implements
+    lib = rp.load_library()
+    n = lib.te_kernel_table_json(None, 0)
+    buf = ctypes.create_string_buffer(n + 1)
+    lib.te_kernel_table_json(buf, n + 1)
+    import json
+    ours = set(json.loads(buf.value.decode()))
+    del gpu
+    # CPU replay; before every in-scope dispatch, hand the GPU the regions written since
+    ngpu = 0
+    gpu_hashes = {}
+    from thunderengine_web_b200.replayer import Replayer
+    r = Replayer(tape, km)
+    r.plan(True)
+    r.build()
+    dirty = [(0, cpu.buffers_end)]
+    for oi, o in enumerate(cpu.ops):
+        if o.kind == 'k' and o.name in ours:
+            for off, ln in dirty:
+                r.write_words(off, cpu.M[off:off + ln])
+            dirty = []
+            r.clear_hashes()
+            r.run_ops(oi, oi, with_hashes=True)
+            h = r.read_hashes()
+            for slot, off, ln in o.hashes:
+                gpu_hashes[slot] = int(h[slot])
+            ngpu += 1
+            # the CPU continues with the oracle so the two memories stay identical
+            cpu.run(helpers.oracle().get, with_hashes=True, ops=[o])
+            for slot, off, ln in o.hashes:
+                assert gpu_hashes[slot] == int(cpu.hashes[slot]), (oi, o.name)
+        else:
+            cpu.run(ref.get, with_hashes=True, ops=[o])
+            if o.kind == 'copy':
+                dirty.append((o.dst, o.n))
+            else:
+                dirty.extend((off, ln) for _, off, ln in o.hashes if off is not None and ln)
+    assert ngpu >= 350
+    fields = {v // 4 + cpu.base[2]: k for k, v in tape['fields'].items()}
+    slot_field = {s: fields.get(off) for o in cpu.ops if o.kind == 'k' for s, off, _ in o.hashes}
+    bad = [s for s in gpu_hashes if gpu_hashes[s] != int(want[s])]
+    assert {slot_field[s] for s in bad} <= {'tend', 'fpk'}
+    for b in tape['buffers']:
+        assert fnv1a(cpu.buffer_words(b['id'])) == step1[b['id']], b['label']

@@ -1,0 +1,27 @@
+// Fused execution of recognised step phases (TE_MODE_FUSED).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+namespace te {
+
+struct Op;
+struct Plan;
+
+// A step's op list rewritten into segments: runs of exact per-dispatch kernels and
+// fused phase kernels that produce bit-identical prognostic fields.
+struct FusedSegment {
+  int kind = 0;  // 0 = exact ops [first, last]; >0 = a fused phase
+  int first = 0, last = 0;
+  int aux[16] = {0};
+};
+
+struct FusedStep {
+  std::vector<FusedSegment> segs;
+  void build(Plan& P, std::vector<Op>& ops);
+  void launch(Plan& P, std::vector<Op>& ops);
+  void release() { segs.clear(); }
+};
+
+}  // namespace te

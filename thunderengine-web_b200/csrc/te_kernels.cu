@@ -1,0 +1,1101 @@
+// Per-dispatch CUDA kernels of the CM1 large-step dynamics path (sm_100a).
+//
+// One kernel per reference kernel name (data/kernels/<name>.wgsl of ThunderEngine),
+// with the reference's dispatch semantics: the launch covers the tape's grid in
+// threads, each thread applies the kernel's own range check, and computes the same
+// binary32 operations in the same order (te_math.cuh).  These are the "exact" path of
+// the player: every dispatch of a tape runs here when the caller asks for per-dispatch
+// hashes; the fused step kernels (te_fused.cu) are checked against them.
+#include <cuda_runtime.h>
+
+#include <cstring>
+
+#include "te_kernels.cuh"
+#include "te_math.cuh"
+
+namespace te {
+
+#define TE_K3                                                   \
+  const int tx = blockIdx.x * blockDim.x + threadIdx.x;         \
+  const int ty = blockIdx.y * blockDim.y + threadIdx.y;         \
+  const int tz = blockIdx.z;                                    \
+  if (tx >= A.gx || ty >= A.gy || tz >= A.gz) return;           \
+  const Dims& g = A.g;                                          \
+  (void)g;
+
+static void launch3(void (*k)(KArgs), const KArgs& A, cudaStream_t s) {
+  dim3 b(32, 4, 1);
+  dim3 gr((A.gx + 31) / 32, (A.gy + 3) / 4, A.gz);
+  k<<<gr, b, 0, s>>>(A);
+}
+
+#define TE_LAUNCH3(name) \
+  static void launch_##name(const KArgs& A, cudaStream_t s) { launch3(k_##name, A, s); }
+
+// ------------------------------------------------------------------ fluxes
+
+// adv_flux_x / adv_flux_y: f = rr * flx5(upwind stencil)
+template <int DIR>
+__global__ void k_flux_lin_h(KArgs A) {
+  TE_K3
+  const float *s = A.p[1], *rr = A.p[2];
+  float* fo = A.p[3];
+  int i = tx, j = ty, k = tz;
+  if (DIR == 0 ? (i > g.nx || j >= g.ny || k >= g.nz) : (i >= g.nx || j > g.ny || k >= g.nz)) return;
+  int c = gidx(g, i, j, k);
+  const int d = DIR == 0 ? 1 : g.sJ;
+  float u = rr[c];
+  float f = u >= 0.0f ? flx5(s[c - 3 * d], s[c - 2 * d], s[c - d], s[c], s[c + d])
+                      : flx5(s[c + 2 * d], s[c + d], s[c], s[c - d], s[c - 2 * d]);
+  fo[c] = u * f;
+}
+static void launch_adv_flux_x(const KArgs& A, cudaStream_t s) { launch3(k_flux_lin_h<0>, A, s); }
+static void launch_adv_flux_y(const KArgs& A, cudaStream_t s) { launch3(k_flux_lin_h<1>, A, s); }
+
+__global__ void k_adv_flux_z(KArgs A) {
+  TE_K3
+  const float *s = A.p[1], *rrw = A.p[2], *c1 = A.p[3], *c2 = A.p[4];
+  float* fz = A.p[5];
+  const int sk = g.sJ * g.sK;
+  int i = tx, j = ty, k = tz;
+  if (i >= g.nx || j >= g.ny || k > g.nz) return;
+  int c = gidx(g, i, j, k);
+  if (k == 0 || k == g.nz) {
+    fz[c] = 0.0f;
+    return;
+  }
+  float w = rrw[c];
+  bool up = w >= 0.0f;
+  float f;
+  if (k == 1) f = up ? fmaf(c1[k], s[c - sk], c2[k] * s[c]) : flx3(s[c + sk], s[c], s[c - sk]);
+  else if (k == 2) f = up ? flx3(s[c - 2 * sk], s[c - sk], s[c]) : flx5(s[c + 2 * sk], s[c + sk], s[c], s[c - sk], s[c - 2 * sk]);
+  else if (k == g.nz - 2) f = up ? flx5(s[c - 3 * sk], s[c - 2 * sk], s[c - sk], s[c], s[c + sk]) : flx3(s[c + sk], s[c], s[c - sk]);
+  else if (k == g.nz - 1) f = up ? flx3(s[c - 2 * sk], s[c - sk], s[c]) : fmaf(c1[k], s[c - sk], c2[k] * s[c]);
+  else f = up ? flx5(s[c - 3 * sk], s[c - 2 * sk], s[c - sk], s[c], s[c + sk])
+              : flx5(s[c + 2 * sk], s[c + sk], s[c], s[c - sk], s[c - 2 * sk]);
+  fz[c] = w * f;
+}
+TE_LAUNCH3(adv_flux_z)
+
+__device__ __forceinline__ float flx5_upwind(const float* a, int c, int s, bool up, bool shifted) {
+  if (shifted) return up ? flx5(a[c - 2 * s], a[c - s], a[c], a[c + s], a[c + 2 * s])
+                         : flx5(a[c + 3 * s], a[c + 2 * s], a[c + s], a[c], a[c - s]);
+  return up ? flx5(a[c - 3 * s], a[c - 2 * s], a[c - s], a[c], a[c + s])
+            : flx5(a[c + 2 * s], a[c + s], a[c], a[c - s], a[c - 2 * s]);
+}
+
+// adv_flux_x_stag / adv_flux_y_stag (momentum, RK stages 1-2)
+template <int DIR>
+__global__ void k_flux_stag_h(KArgs A) {
+  TE_K3
+  const int stag = A.iv[1];
+  const float *a = A.p[2], *rr = DIR == 0 ? A.p[3] : A.p[4], *c2 = A.p[7];
+  float* fo = A.p[8];
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  int i = tx - 1, j = ty - 1, k = tz;
+  if (i > g.nx || j > g.ny || k >= g.nz) return;
+  int c = gidx(g, i, j, k);
+  if (stag == 4 && k == 0) {
+    fo[c] = 0.0f;
+    return;
+  }
+  float m;
+  if (DIR == 0) {
+    if (stag == 2) m = 0.5f * (rr[c] + rr[c + 1]);
+    else if (stag == 3) m = 0.5f * (rr[c] + rr[c - sj]);
+    else if (stag == 4) { float cc2 = c2[k]; m = fmaf(cc2, rr[c], (1.0f - cc2) * rr[c - sk]); }
+    else m = rr[c];
+    fo[c] = m * flx5_upwind(a, c, 1, m >= 0.0f, stag == 2);
+  } else {
+    if (stag == 2) m = 0.5f * (rr[c] + rr[c - 1]);
+    else if (stag == 3) m = 0.5f * (rr[c] + rr[c + sj]);
+    else if (stag == 4) { float cc2 = c2[k]; m = fmaf(cc2, rr[c], (1.0f - cc2) * rr[c - sk]); }
+    else m = rr[c];
+    fo[c] = m * flx5_upwind(a, c, sj, m >= 0.0f, stag == 3);
+  }
+}
+static void launch_adv_flux_x_stag(const KArgs& A, cudaStream_t s) { launch3(k_flux_stag_h<0>, A, s); }
+static void launch_adv_flux_y_stag(const KArgs& A, cudaStream_t s) { launch3(k_flux_stag_h<1>, A, s); }
+
+__global__ void k_adv_flux_z_stag(KArgs A) {
+  TE_K3
+  const int stag = A.iv[1];
+  const float *a = A.p[2], *rrw = A.p[5], *c1 = A.p[6], *c2 = A.p[7];
+  float* fz = A.p[8];
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  int i = tx, j = ty, k = tz;
+  if (i > g.nx || j > g.ny || k > g.nz) return;
+  int c = gidx(g, i, j, k);
+  float m;
+  if (stag == 2) m = 0.5f * (rrw[c] + rrw[c - 1]);
+  else if (stag == 3) m = 0.5f * (rrw[c] + rrw[c - sj]);
+  else m = 0.5f * (rrw[c] + (k < g.nz ? rrw[c + sk] : 0.0f));
+  bool up = m >= 0.0f;
+  float f;
+  if (stag == 4) {
+    if (k > g.nz - 1) {
+      fz[c] = 0.0f;
+      return;
+    }
+    if (k == 0) f = up ? 0.5f * (a[c] + a[c + sk]) : flx3(a[c + 2 * sk], a[c + sk], a[c]);
+    else if (k == 1) f = up ? flx3(a[c - sk], a[c], a[c + sk]) : flx5(a[c + 3 * sk], a[c + 2 * sk], a[c + sk], a[c], a[c - sk]);
+    else if (k == g.nz - 2) f = up ? flx5(a[c - 2 * sk], a[c - sk], a[c], a[c + sk], a[c + 2 * sk]) : flx3(a[c + 2 * sk], a[c + sk], a[c]);
+    else if (k == g.nz - 1) f = up ? flx3(a[c - sk], a[c], a[c + sk]) : 0.5f * (a[c] + a[c + sk]);
+    else f = up ? flx5(a[c - 2 * sk], a[c - sk], a[c], a[c + sk], a[c + 2 * sk])
+                : flx5(a[c + 3 * sk], a[c + 2 * sk], a[c + sk], a[c], a[c - sk]);
+  } else {
+    if (k == 0 || k == g.nz) {
+      fz[c] = 0.0f;
+      return;
+    }
+    if (k == 1) f = up ? fmaf(c1[k], a[c - sk], c2[k] * a[c]) : flx3(a[c + sk], a[c], a[c - sk]);
+    else if (k == 2) f = up ? flx3(a[c - 2 * sk], a[c - sk], a[c]) : flx5(a[c + 2 * sk], a[c + sk], a[c], a[c - sk], a[c - 2 * sk]);
+    else if (k == g.nz - 2) f = up ? flx5(a[c - 3 * sk], a[c - 2 * sk], a[c - sk], a[c], a[c + sk]) : flx3(a[c + sk], a[c], a[c - sk]);
+    else if (k == g.nz - 1) f = up ? flx3(a[c - 2 * sk], a[c - sk], a[c]) : fmaf(c1[k], a[c - sk], c2[k] * a[c]);
+    else f = up ? flx5(a[c - 3 * sk], a[c - 2 * sk], a[c - sk], a[c], a[c + sk])
+                : flx5(a[c + 2 * sk], a[c + sk], a[c], a[c - sk], a[c - 2 * sk]);
+  }
+  fz[c] = m * f;
+}
+TE_LAUNCH3(adv_flux_z_stag)
+
+// adv_flux_x_weno / adv_flux_y_weno (scalars, positive-definite gate)
+template <int DIR>
+__global__ void k_flux_weno_h(KArgs A) {
+  TE_K3
+  const float *a = A.p[1], *rr = A.p[2];
+  const float weps = A.f[3];
+  const int pdef = A.iv[4];
+  float* fo = A.p[5];
+  int i = tx, j = ty, k = tz;
+  if (DIR == 0 ? (i > g.nx || j >= g.ny || k >= g.nz) : (i >= g.nx || j > g.ny || k >= g.nz)) return;
+  int c = gidx(g, i, j, k);
+  const int d = DIR == 0 ? 1 : g.sJ;
+  float s1, s2, s3, s4, s5;
+  float r = rr[c];
+  if (r >= 0.0f) { s1 = a[c - 3 * d]; s2 = a[c - 2 * d]; s3 = a[c - d]; s4 = a[c]; s5 = a[c + d]; }
+  else { s1 = a[c + 2 * d]; s2 = a[c + d]; s3 = a[c]; s4 = a[c - d]; s5 = a[c - 2 * d]; }
+  bool ok = pdef != 1 || weno_pdef_ok(s1, s2, s3, s4, s5, weps);
+  fo[c] = ok ? r * weno5(s1, s2, s3, s4, s5, weps) : 0.0f;
+}
+static void launch_adv_flux_x_weno(const KArgs& A, cudaStream_t s) { launch3(k_flux_weno_h<0>, A, s); }
+static void launch_adv_flux_y_weno(const KArgs& A, cudaStream_t s) { launch3(k_flux_weno_h<1>, A, s); }
+
+__global__ void k_adv_flux_z_weno(KArgs A) {
+  TE_K3
+  const float *a = A.p[1], *rrw = A.p[2], *c1 = A.p[3], *c2 = A.p[4];
+  const float weps = A.f[5];
+  const int pdefweno = A.iv[7];
+  float* fz = A.p[8];
+  const int sk = g.sJ * g.sK, nk = g.nz;
+  int i = tx, j = ty, kf = tz + 1;
+  if (i >= g.nx || j >= g.ny || kf > g.nz + 1) return;
+  int k = kf - 1;
+  int c = gidx(g, i, j, k);
+  if (kf == 1 || kf == g.nz + 1) {
+    fz[c] = 0.0f;
+    return;
+  }
+#define AZ(o) a[c + (o) * sk]
+  float w = rrw[c];
+  if (kf == 2) {
+    fz[c] = w >= 0.0f ? w * fmaf(c1[k], AZ(-1), c2[k] * AZ(0)) : w * upstrpd(AZ(1), AZ(0), AZ(-1), weps);
+    return;
+  }
+  if (kf == nk) {
+    fz[c] = w > 0.0f ? w * upstrpd(AZ(-2), AZ(-1), AZ(0), weps) : w * fmaf(c1[k], AZ(-1), c2[k] * AZ(0));
+    return;
+  }
+  float s1, s2, s3, s4, s5;
+  if (w >= 0.0f) { s1 = AZ(-3); s2 = AZ(-2); s3 = AZ(-1); s4 = AZ(0); s5 = AZ(1); }
+  else { s1 = AZ(2); s2 = AZ(1); s3 = AZ(0); s4 = AZ(-1); s5 = AZ(-2); }
+  if (pdefweno == 1) {
+    bool doit = weno_pdef_ok(s1, s2, s3, s4, s5, weps);
+    if (kf == 3 && w > 0.0f) doit = false;
+    if (kf == nk - 1 && w < 0.0f) doit = false;
+    if (doit) {
+      fz[c] = w * weno5(s1, s2, s3, s4, s5, weps);
+      return;
+    }
+    if (kf != 3 && kf != nk - 1) {
+      fz[c] = 0.0f;
+      return;
+    }
+  }
+  if (kf == 3) {
+    fz[c] = w >= 0.0f ? w * upstrpd(AZ(-2), AZ(-1), AZ(0), weps) : w * weno5(AZ(2), AZ(1), AZ(0), AZ(-1), AZ(-2), weps);
+    return;
+  }
+  if (kf == nk - 1) {
+    fz[c] = w >= 0.0f ? w * weno5(AZ(-3), AZ(-2), AZ(-1), AZ(0), AZ(1), weps) : w * upstrpd(AZ(1), AZ(0), AZ(-1), weps);
+    return;
+  }
+  fz[c] = w * weno5(s1, s2, s3, s4, s5, weps);
+#undef AZ
+}
+TE_LAUNCH3(adv_flux_z_weno)
+
+__device__ __forceinline__ float weno5_upwind(const float* a, int c, int s, bool up, bool shifted, float weps) {
+  if (shifted) return up ? weno5(a[c - 2 * s], a[c - s], a[c], a[c + s], a[c + 2 * s], weps)
+                         : weno5(a[c + 3 * s], a[c + 2 * s], a[c + s], a[c], a[c - s], weps);
+  return up ? weno5(a[c - 3 * s], a[c - 2 * s], a[c - s], a[c], a[c + s], weps)
+            : weno5(a[c + 2 * s], a[c + s], a[c], a[c - s], a[c - 2 * s], weps);
+}
+
+// adv_flux_x_weno_uv / adv_flux_y_weno_uv (u, v momentum, RK stage 3)
+template <int DIR>
+__global__ void k_flux_weno_uv_h(KArgs A) {
+  TE_K3
+  const int stag = A.iv[1];
+  const float *a = A.p[2], *rr = A.p[3];
+  const float weps = A.f[4];
+  float* fo = A.p[5];
+  const int sj = g.sJ;
+  int i = tx - 1, j = ty - 1, k = tz;
+  if (i > g.nx || j > g.ny || k >= g.nz) return;
+  int c = gidx(g, i, j, k);
+  if (DIR == 0) {
+    float m = stag == 2 ? 0.5f * (rr[c] + rr[c + 1]) : 0.5f * (rr[c] + rr[c - sj]);
+    fo[c] = m * weno5_upwind(a, c, 1, m >= 0.0f, stag == 2, weps);
+  } else {
+    float m = stag == 2 ? 0.5f * (rr[c] + rr[c - 1]) : 0.5f * (rr[c] + rr[c + sj]);
+    fo[c] = m * weno5_upwind(a, c, sj, m >= 0.0f, stag == 3, weps);
+  }
+}
+static void launch_adv_flux_x_weno_uv(const KArgs& A, cudaStream_t s) { launch3(k_flux_weno_uv_h<0>, A, s); }
+static void launch_adv_flux_y_weno_uv(const KArgs& A, cudaStream_t s) { launch3(k_flux_weno_uv_h<1>, A, s); }
+
+__global__ void k_adv_flux_z_weno_uv(KArgs A) {
+  TE_K3
+  const int stag = A.iv[1];
+  const float *a = A.p[2], *rrw = A.p[3], *c1 = A.p[4], *c2 = A.p[5];
+  const float weps = A.f[6];
+  float* fz = A.p[7];
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  int i = tx, j = ty, k = tz;
+  if (i > g.nx || j > g.ny || k > g.nz) return;
+  int c = gidx(g, i, j, k);
+  if (k == 0 || k == g.nz) {
+    fz[c] = 0.0f;
+    return;
+  }
+#define AZ(o) a[c + (o) * sk]
+  float m = stag == 2 ? 0.5f * (rrw[c] + rrw[c - 1]) : 0.5f * (rrw[c] + rrw[c - sj]);
+  bool up = m >= 0.0f;
+  float f;
+  if (k == 1) f = up ? fmaf(c1[k], AZ(-1), c2[k] * AZ(0)) : upstrpd(AZ(1), AZ(0), AZ(-1), weps);
+  else if (k == 2) f = up ? upstrpd(AZ(-2), AZ(-1), AZ(0), weps) : weno5(AZ(2), AZ(1), AZ(0), AZ(-1), AZ(-2), weps);
+  else if (k == g.nz - 2) f = up ? weno5(AZ(-3), AZ(-2), AZ(-1), AZ(0), AZ(1), weps) : upstrpd(AZ(1), AZ(0), AZ(-1), weps);
+  else if (k == g.nz - 1) f = up ? upstrpd(AZ(-2), AZ(-1), AZ(0), weps) : fmaf(c1[k], AZ(-1), c2[k] * AZ(0));
+  else f = up ? weno5(AZ(-3), AZ(-2), AZ(-1), AZ(0), AZ(1), weps) : weno5(AZ(2), AZ(1), AZ(0), AZ(-1), AZ(-2), weps);
+  fz[c] = m * f;
+#undef AZ
+}
+TE_LAUNCH3(adv_flux_z_weno_uv)
+
+// adv_flux_x_weno_w / adv_flux_y_weno_w (w momentum, RK stage 3)
+template <int DIR>
+__global__ void k_flux_weno_w_h(KArgs A) {
+  TE_K3
+  const float *a = A.p[1], *rr = A.p[2], *c2 = A.p[3];
+  const float weps = A.f[4];
+  float* fo = A.p[5];
+  const int sk = g.sJ * g.sK;
+  int i = tx - 1, j = ty - 1, k = tz;
+  if (i < 0 || j < 0 || i > g.nx || j > g.ny || k >= g.nz) return;
+  int c = gidx(g, i, j, k);
+  if (k == 0) {
+    fo[c] = 0.0f;
+    return;
+  }
+  const int d = DIR == 0 ? 1 : g.sJ;
+  float cc2 = c2[k];
+  float cc1 = 1.0f - cc2;
+  float ub = fmaf(cc2, rr[c], cc1 * rr[c - sk]);
+  fo[c] = ub >= 0.0f ? ub * weno5(a[c - 3 * d], a[c - 2 * d], a[c - d], a[c], a[c + d], weps)
+                     : ub * weno5(a[c + 2 * d], a[c + d], a[c], a[c - d], a[c - 2 * d], weps);
+}
+static void launch_adv_flux_x_weno_w(const KArgs& A, cudaStream_t s) { launch3(k_flux_weno_w_h<0>, A, s); }
+static void launch_adv_flux_y_weno_w(const KArgs& A, cudaStream_t s) { launch3(k_flux_weno_w_h<1>, A, s); }
+
+__global__ void k_adv_flux_z_weno_w(KArgs A) {
+  TE_K3
+  const float *a = A.p[1], *rrw = A.p[2];
+  const float weps = A.f[3];
+  float* fz = A.p[4];
+  const int sk = g.sJ * g.sK, nz = g.nz;
+  int i = tx, j = ty, k = tz;
+  if (i > g.nx || j > g.ny || k > g.nz) return;
+  int c = gidx(g, i, j, k);
+  if (k > g.nz - 1) {
+    fz[c] = 0.0f;
+    return;
+  }
+#define AZ(o) a[c + (o) * sk]
+  float wb = 0.5f * (rrw[c] + rrw[c + sk]);
+  float f;
+  if (k == 0) f = wb >= 0.0f ? 0.5f * (AZ(0) + AZ(1)) : upstrpd(AZ(2), AZ(1), AZ(0), weps);
+  else if (k == nz - 1) f = wb > 0.0f ? upstrpd(AZ(-1), AZ(0), AZ(1), weps) : 0.5f * (AZ(0) + AZ(1));
+  else if (k == 1) f = wb >= 0.0f ? upstrpd(AZ(-1), AZ(0), AZ(1), weps) : weno5(AZ(3), AZ(2), AZ(1), AZ(0), AZ(-1), weps);
+  else if (k == nz - 2) f = wb > 0.0f ? weno5(AZ(-2), AZ(-1), AZ(0), AZ(1), AZ(2), weps) : upstrpd(AZ(2), AZ(1), AZ(0), weps);
+  else f = wb >= 0.0f ? weno5(AZ(-2), AZ(-1), AZ(0), AZ(1), AZ(2), weps) : weno5(AZ(3), AZ(2), AZ(1), AZ(0), AZ(-1), weps);
+  fz[c] = wb * f;
+#undef AZ
+}
+TE_LAUNCH3(adv_flux_z_weno_w)
+
+// ------------------------------------------------------------ assembly
+
+__global__ void k_adv_assemble(KArgs A) {
+  TE_K3
+  const int stag = A.iv[1];
+  const float *s = A.p[2], *fx = A.p[3], *fy = A.p[4], *fz = A.p[5], *divx = A.p[6];
+  const float *rho0 = A.p[7], *rf0 = A.p[8], *mh = A.p[9], *mf = A.p[10];
+  float* tend = A.p[11];
+  const int accumulate = A.iv[12];
+  const float *rru = A.p[13], *rrv = A.p[14], *c1 = A.p[15], *c2 = A.p[16];
+  const int openx = A.iv[17], openy = A.iv2[17];
+  const float* hm = A.p[30];
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  const int st = stag < 0 ? -stag : stag;
+  const int iMax = st == 2 ? g.nx : g.nx - 1, jMax = st == 3 ? g.ny : g.ny - 1;
+  const int kLo = st == 4 ? 1 : 0, kMax = g.nz - 1;
+  int i = tx, j = ty, k = tz;
+  if (i > iMax || j > jMax || k < kLo || k > kMax) return;
+  if (openx != 0 && st == 2 && (i == 0 || i == g.nx)) return;
+  if (openy != 0 && st == 3 && (j == 0 || j == g.ny)) return;
+  int c = gidx(g, i, j, k);
+  float dFx = st == 2 ? fx[c] - fx[c - 1] : fx[c + 1] - fx[c];
+  float dFy = st == 3 ? fy[c] - fy[c - sj] : fy[c + sj] - fy[c];
+  float dFz = st == 4 ? fz[c] - fz[c - sk] : fz[c + sk] - fz[c];
+  float mz = stag < 0 ? 1.0f : (stag == 4 ? mf[k] : mh[k]);
+  float dv;
+  if (st == 2) dv = 0.5f * (divx[c] + divx[c - 1]);
+  else if (st == 3) dv = 0.5f * (divx[c] + divx[c - sj]);
+  else if (st == 4) dv = fmaf(c2[k], divx[c], c1[k] * divx[c - sk]);
+  else dv = divx[c];
+  if (openx != 0 && st != 2) {
+    bool west = i == 0, east = i == g.nx - 1;
+    if (west || east) {
+      int cf = west ? c : c + 1;
+      float un, piece;
+      if (st == 3) {
+        un = rru[cf] + rru[cf - sj];
+        piece = ((0.5f * ((rru[c + 1 - sj] - rru[c - sj]) + (rru[c + 1] - rru[c]))) * g.rdx) * hm_uh(g, hm, i);
+      } else if (st == 4) {
+        float cc2 = 0.5f * (c2[k - 1] + c2[k]);
+        float cc1 = 1.0f - cc2;
+        un = fmaf(cc2, rru[cf], cc1 * rru[cf - sk]);
+        piece = (fmaf(c1[k], rru[c + 1 - sk] - rru[c - sk], c2[k] * (rru[c + 1] - rru[c])) * g.rdx) * hm_uh(g, hm, i);
+      } else {
+        un = rru[cf];
+        piece = ((rru[c + 1] - rru[c]) * g.rdx) * hm_uh(g, hm, i);
+      }
+      bool inflow = west ? un >= 0.0f : un <= 0.0f;
+      if (inflow) {
+        dFx = 0.0f;
+        dv = dv - piece;
+      }
+    }
+  }
+  if (openy != 0 && st != 3) {
+    bool south = j == 0, north = j == g.ny - 1;
+    if (south || north) {
+      int cf = south ? c : c + sj;
+      float vn, piece;
+      if (st == 2) {
+        vn = rrv[cf] + rrv[cf - 1];
+        piece = ((0.5f * ((rrv[c + sj - 1] - rrv[c - 1]) + (rrv[c + sj] - rrv[c]))) * g.rdy) * hm_vh(g, hm, j);
+      } else if (st == 4) {
+        float cc2 = 0.5f * (c2[k - 1] + c2[k]);
+        float cc1 = 1.0f - cc2;
+        vn = fmaf(cc2, rrv[cf], cc1 * rrv[cf - sk]);
+        piece = (fmaf(c1[k], rrv[c + sj - sk] - rrv[c - sk], c2[k] * (rrv[c + sj] - rrv[c])) * g.rdy) * hm_vh(g, hm, j);
+      } else {
+        vn = rrv[cf];
+        piece = ((rrv[c + sj] - rrv[c]) * g.rdy) * hm_vh(g, hm, j);
+      }
+      bool inflow = south ? vn >= 0.0f : vn <= 0.0f;
+      if (inflow) {
+        dFy = 0.0f;
+        dv = dv - piece;
+      }
+    }
+  }
+  float mx = st == 2 ? hm_uf(g, hm, i) : hm_uh(g, hm, i);
+  float my = st == 3 ? hm_vf(g, hm, j) : hm_vh(g, hm, j);
+  float divF = fmaf(dFz * g.rdz, mz, fmaf(dFx * g.rdx, mx, (dFy * g.rdy) * my));
+  float rho = st == 4 ? rf0[k] : rho0[k];
+  float t = dcr(fmaf(s[c], dv, -divF), rho);
+  tend[c] = accumulate != 0 ? tend[c] + t : t;
+}
+TE_LAUNCH3(adv_assemble)
+
+__global__ void k_rk_update(KArgs A) {
+  TE_K3
+  const int stag = A.iv[1];
+  const float *phiA = A.p[2], *tend = A.p[3];
+  float* phi = A.p[4];
+  const float dttmp = A.f[5];
+  const int iMax = stag == 2 ? g.nx : g.nx - 1, jMax = stag == 3 ? g.ny : g.ny - 1, kLo = stag == 4 ? 1 : 0;
+  int i = tx, j = ty, k = tz;
+  if (i > iMax || j > jMax || k < kLo || k >= g.nz) return;
+  int c = gidx(g, i, j, k);
+  phi[c] = fmaf(dttmp, tend[c], phiA[c]);
+}
+TE_LAUNCH3(rk_update)
+
+__device__ __forceinline__ bool pdef_inflow(const Dims& g, int dir, int i, int j, int c, int step, const float* rr, int ox, int oy) {
+  if (dir == 0 && ox != 0) {
+    if (i == 0 && rr[c] >= 0.0f) return true;
+    if (i == g.nx - 1 && rr[c + step] <= 0.0f) return true;
+  }
+  if (dir == 1 && oy != 0) {
+    if (j == 0 && rr[c] >= 0.0f) return true;
+    if (j == g.ny - 1 && rr[c + step] <= 0.0f) return true;
+  }
+  return false;
+}
+
+__global__ void k_pdef_dum(KArgs A) {
+  TE_K3
+  const int dir = A.iv[1];
+  const float *s = A.p[2], *s0 = A.p[3], *f = A.p[4], *rr = A.p[5], *rho0 = A.p[6], *mh = A.p[7];
+  const float dt = A.f[8];
+  const int ox = A.iv[9], oy = A.iv2[9];
+  float* dum = A.p[10];
+  const float* hm = A.p[30];
+  int i = tx, j = ty, k = tz;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  int c = gidx(g, i, j, k);
+  int step = dir == 0 ? 1 : (dir == 1 ? g.sJ : g.sJ * g.sK);
+  float rd = dir == 0 ? g.rdx : (dir == 1 ? g.rdy : g.rdz);
+  float base = rho0[k] * s0[c];
+  if (pdef_inflow(g, dir, i, j, c, step, rr, ox, oy)) {
+    dum[c] = base;
+    return;
+  }
+  float adv = (-(f[c + step] - f[c])) * rd;
+  float sdiv = (s[c] * (rr[c + step] - rr[c])) * rd;
+  float m = dir == 0 ? hm_uh(g, hm, i) : (dir == 1 ? hm_vh(g, hm, j) : mh[k]);
+  adv = adv * m;
+  sdiv = sdiv * m;
+  dum[c] = fmaf(dt, adv + sdiv, base);
+}
+TE_LAUNCH3(pdef_dum)
+
+struct PdefCell {
+  bool neg;
+  float f1, f2, foo3;
+};
+__device__ __forceinline__ PdefCell pdef_cell(float d, float dm, float dp) {
+  PdefCell r{false, 0.0f, 0.0f, 0.0f};
+  if (d < 0.0f) {
+    float f1 = wmax(0.0f, dm), f2 = wmax(0.0f, dp);
+    if (f1 + f2 > 1e-30f) {
+      r.neg = true;
+      r.f1 = f1;
+      r.f2 = f2;
+      r.foo3 = dcr(wmax(d, -(f1 + f2)), f1 + f2);
+    }
+  }
+  return r;
+}
+__device__ __forceinline__ float pdef_mass(float dm2, float dm1, float d0, float dp1, float dp2, bool* flag) {
+  PdefCell l = pdef_cell(dm1, dm2, d0), c = pdef_cell(d0, dm1, dp1), r = pdef_cell(dp1, d0, dp2);
+  float mass = 0.0f;
+  if (l.neg) mass = fmaf(l.f2, l.foo3, mass);
+  if (c.neg) mass = fmaf(-(c.f1 + c.f2), c.foo3, mass);
+  if (r.neg) mass = fmaf(r.f1, r.foo3, mass);
+  *flag = c.neg || (l.neg && d0 > 1e-30f) || (r.neg && d0 > 1e-30f);
+  return mass;
+}
+
+__global__ void k_pdef_apply(KArgs A) {
+  TE_K3
+  const float *s = A.p[1], *s0 = A.p[2], *fx = A.p[3], *fy = A.p[4], *fz = A.p[5];
+  const float *rru = A.p[6], *rrv = A.p[7], *rrw = A.p[8], *dumx = A.p[9], *dumy = A.p[10], *dumz = A.p[11];
+  const float *rho0 = A.p[12], *mh = A.p[13];
+  const float dt = A.f[14];
+  const int ox = A.iv[15], oy = A.iv2[15];
+  float* tend = A.p[16];
+  const float* hm = A.p[30];
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  int i = tx, j = ty, k = tz;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  int c = gidx(g, i, j, k);
+  float rdt = dcr(1.0f, dt);
+  float base = rho0[k] * s0[c];
+  float delta = 0.0f;
+  bool flag;
+  float mx = pdef_mass(dumx[c - 2], dumx[c - 1], dumx[c], dumx[c + 1], dumx[c + 2], &flag);
+  if (flag) {
+    float sdiv = ((s[c] * (rru[c + 1] - rru[c])) * g.rdx) * hm_uh(g, hm, i);
+    float advOld = pdef_inflow(g, 0, i, j, c, 1, rru, ox, oy) ? -sdiv : ((-(fx[c + 1] - fx[c])) * g.rdx) * hm_uh(g, hm, i);
+    float advNew = fmaf((dumx[c] + mx) - base, rdt, -sdiv);
+    delta = delta + (advNew - advOld);
+  }
+  float my = pdef_mass(dumy[c - 2 * sj], dumy[c - sj], dumy[c], dumy[c + sj], dumy[c + 2 * sj], &flag);
+  if (flag) {
+    float sdiv = ((s[c] * (rrv[c + sj] - rrv[c])) * g.rdy) * hm_vh(g, hm, j);
+    float advOld = pdef_inflow(g, 1, i, j, c, sj, rrv, ox, oy) ? -sdiv : ((-(fy[c + sj] - fy[c])) * g.rdy) * hm_vh(g, hm, j);
+    float advNew = fmaf((dumy[c] + my) - base, rdt, -sdiv);
+    delta = delta + (advNew - advOld);
+  }
+  float zm2 = k >= 2 ? dumz[c - 2 * sk] : 0.0f;
+  float zm1 = k >= 1 ? dumz[c - sk] : 0.0f;
+  float zp1 = k + 1 < g.nz ? dumz[c + sk] : 0.0f;
+  float zp2 = k + 2 < g.nz ? dumz[c + 2 * sk] : 0.0f;
+  float mz = pdef_mass(zm2, zm1, dumz[c], zp1, zp2, &flag);
+  if (flag) {
+    float sdiv = ((s[c] * (rrw[c + sk] - rrw[c])) * g.rdz) * mh[k];
+    float advOld = ((-(fz[c + sk] - fz[c])) * g.rdz) * mh[k];
+    float advNew = fmaf((dumz[c] + mz) - base, rdt, -sdiv);
+    delta = delta + (advNew - advOld);
+  }
+  tend[c] = tend[c] + dcr(delta, rho0[k]);
+}
+TE_LAUNCH3(pdef_apply)
+
+// --------------------------------------------------------- whole-grid glue
+
+#define TE_WHOLE(kcond)                                          \
+  int i = tx - 3, j = ty - 3, k = tz;                            \
+  if (i > g.nx + 3 || j > g.ny + 3 || !(kcond)) return;          \
+  int c = gidx(g, i, j, k);
+
+__global__ void k_build_sadv(KArgs A) {
+  TE_K3
+  const float *th0 = A.p[1], *thp = A.p[2];
+  float* sadv = A.p[3];
+  TE_WHOLE(k < g.nz)
+  sadv[c] = (th0[k] - 300.0f) + thp[c];
+}
+TE_LAUNCH3(build_sadv)
+
+__global__ void k_massflux_from_state(KArgs A) {
+  TE_K3
+  const float *u = A.p[1], *v = A.p[2], *w = A.p[3], *rho0 = A.p[4], *rf0 = A.p[5];
+  float *rru = A.p[6], *rrv = A.p[7], *rrw = A.p[8];
+  TE_WHOLE(k <= g.nz)
+  if (k < g.nz) {
+    rru[c] = rho0[k] * u[c];
+    rrv[c] = rho0[k] * v[c];
+  }
+  rrw[c] = (k == 0 || k == g.nz) ? 0.0f : rf0[k] * w[c];
+}
+TE_LAUNCH3(massflux_from_state)
+
+__global__ void k_div_massflux(KArgs A) {
+  TE_K3
+  const float *rru = A.p[1], *rrv = A.p[2], *rrw = A.p[3], *mh = A.p[4];
+  float* divx = A.p[5];
+  const float* hm = A.p[30];
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  int i = tx - 3, j = ty - 3, k = tz;
+  if (i > g.nx + 2 || j > g.ny + 2 || k >= g.nz) return;
+  int c = gidx(g, i, j, k);
+  divx[c] = fmaf((rrw[c + sk] - rrw[c]) * g.rdz, mh[k],
+                 fmaf((rru[c + 1] - rru[c]) * g.rdx, hm_uh(g, hm, i), ((rrv[c + sj] - rrv[c]) * g.rdy) * hm_vh(g, hm, j)));
+}
+TE_LAUNCH3(div_massflux)
+
+__global__ void k_velocity_to_massflux(KArgs A) {
+  TE_K3
+  const float *rho0 = A.p[1], *rf0 = A.p[2];
+  float *rru = A.p[3], *rrv = A.p[4], *rrw = A.p[5];
+  TE_WHOLE(k <= g.nz)
+  if (k < g.nz) {
+    rru[c] = rru[c] * rho0[k];
+    rrv[c] = rrv[c] * rho0[k];
+  }
+  rrw[c] = (k == 0 || k == g.nz) ? 0.0f : rrw[c] * rf0[k];
+}
+TE_LAUNCH3(velocity_to_massflux)
+
+__global__ void k_stage_state_reset(KArgs A) {
+  TE_K3
+  const float *ua = A.p[1], *va = A.p[2], *wa = A.p[3], *ppi = A.p[4];
+  float *u = A.p[5], *v = A.p[6], *w = A.p[7], *pp3d = A.p[8], *ppd = A.p[9];
+  const float* ppx = A.p[10];
+  TE_WHOLE(k <= g.nz)
+  u[c] = ua[c];
+  v[c] = va[c];
+  w[c] = wa[c];
+  pp3d[c] = ppi[c];
+  ppd[c] = ppx[c];
+}
+TE_LAUNCH3(stage_state_reset)
+
+__global__ void k_stage_tendency_reset(KArgs A) {
+  TE_K3
+  float *uten = A.p[1], *vten = A.p[2], *wten = A.p[3];
+  TE_WHOLE(k <= g.nz)
+  uten[c] = 0.0f;
+  vten[c] = 0.0f;
+  wten[c] = 0.0f;
+}
+TE_LAUNCH3(stage_tendency_reset)
+
+__global__ void k_buoyancy_apply(KArgs A) {
+  TE_K3
+  const float *buoy = A.p[1], *c1 = A.p[2], *c2 = A.p[3];
+  float* wten = A.p[4];
+  const int sk = g.sJ * g.sK;
+  int i = tx, j = ty, k = tz + 1;
+  if (i >= g.nx || j >= g.ny || k > g.nz - 1) return;
+  int c = gidx(g, i, j, k);
+  wten[c] = wten[c] + fmaf(c1[k], buoy[c - sk], c2[k] * buoy[c]);
+}
+TE_LAUNCH3(buoyancy_apply)
+
+__global__ void k_apply_thterm(KArgs A) {
+  TE_K3
+  const float *div = A.p[1], *thterm = A.p[2];
+  float* tend = A.p[3];
+  int i = tx, j = ty, k = tz;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  int c = gidx(g, i, j, k);
+  tend[c] = fmaf(-div[c], thterm[c], tend[c]);
+}
+TE_LAUNCH3(apply_thterm)
+
+// ------------------------------------------------------ acoustic substep
+
+__global__ void k_acoustic_prepare(KArgs A) {
+  TE_K3
+  const Acoustic a = A.a;
+  const float *ppterm = A.p[2], *piadv = A.p[3], *thv = A.p[4], *rr0 = A.p[5], *rf0 = A.p[6];
+  const float *mh = A.p[7], *mf = A.p[8], *c1 = A.p[9], *c2 = A.p[10];
+  float *qk = A.p[11], *pk1 = A.p[12], *pk2 = A.p[13], *mm = A.p[14];
+  const int sk = g.sJ * g.sK;
+  const float cp = 1005.7f;
+  int i = tx, j = ty, k = tz;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  int c = gidx(g, i, j, k);
+  float tem = (a.dts * g.rdz) * mh[k];
+  float r2 = (tem * rr0[k]) * rf0[k + 1];
+  float r1 = (tem * rr0[k]) * rf0[k];
+  float tem1 = ((a.dts * g.rdz) * cp) * mf[k];
+  float c1a = c1[k], c1b = c1[k + 1], c2a = c2[k], c2b = c2[k + 1];
+  bool vec_v = g.nx > 3 && i < (g.nx / 4) * 4;
+  qk[c] = tem * ppterm[c];
+  float p2 = 0.0f, p1 = 0.0f;
+  if (k != g.nz - 1)
+    p2 = vec_v ? fmaf(-c2b, piadv[c + sk], (1.0f - c1b) * piadv[c]) : fmaf(1.0f - c1b, piadv[c], -(c2b * piadv[c + sk]));
+  if (k != 0)
+    p1 = vec_v ? fmaf(c2a - 1.0f, piadv[c], c1a * piadv[c - sk]) : fmaf(c1a, piadv[c - sk], (c2a - 1.0f) * piadv[c]);
+  pk2[c] = k == g.nz - 1 ? 0.0f : r2 * p2;
+  pk1[c] = k == 0 ? 0.0f : r1 * p1;
+  mm[c] = tem1 * fmaf(c2a, thv[c], c1a * (k == 0 ? thv[c] : thv[c - sk]));
+}
+TE_LAUNCH3(acoustic_prepare)
+
+__global__ void k_acoustic_begin(KArgs A) {
+  TE_K3
+  const float* w = A.p[2];
+  float *rru = A.p[3], *rrv = A.p[4], *rrw = A.p[5];
+  TE_WHOLE(k <= g.nz)
+  rru[c] = 0.0f;
+  rrv[c] = 0.0f;
+  rrw[c] = w[c] * A.a.beta;
+}
+TE_LAUNCH3(acoustic_begin)
+
+__global__ void k_acoustic_uv(KArgs A) {
+  TE_K3
+  const Acoustic a = A.a;
+  const float *ppd = A.p[2], *thv = A.p[3], *uten = A.p[4], *vten = A.p[5];
+  float *u = A.p[6], *v = A.p[7];
+  const int ox = A.iv[8], oy = A.iv2[8];
+  const float* hm = A.p[30];
+  const int sj = g.sJ;
+  const float cp = 1005.7f;
+  int i = tx, j = ty, k = tz;
+  if (i > g.nx || j > g.ny || k >= g.nz) return;
+  int c = gidx(g, i, j, k);
+  float tem1 = (g.rdx * cp) * 0.5f;
+  float tem2 = (g.rdy * cp) * 0.5f;
+  bool uEdge = ox != 0 && (i == 0 || i == g.nx);
+  bool vEdge = oy != 0 && (j == 0 || j == g.ny);
+  if (!uEdge) u[c] = fmaf(a.dts, fmaf(-((tem1 * (ppd[c] - ppd[c - 1])) * hm_uf(g, hm, i)), thv[c] + thv[c - 1], uten[c]), u[c]);
+  if (!vEdge) v[c] = fmaf(a.dts, fmaf(-((tem2 * (ppd[c] - ppd[c - sj])) * hm_vf(g, hm, j)), thv[c] + thv[c - sj], vten[c]), v[c]);
+}
+TE_LAUNCH3(acoustic_uv)
+
+__global__ void k_acoustic_fpk(KArgs A) {
+  TE_K3
+  const Acoustic a = A.a;
+  const float *u = A.p[2], *v = A.p[3], *w = A.p[4], *piadv = A.p[5], *ppten = A.p[6], *ppterm = A.p[7];
+  const float *pk1 = A.p[8], *pk2 = A.p[9], *qk = A.p[10];
+  float* fpk = A.p[11];
+  const float* hm = A.p[30];
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  int i = tx, j = ty, k = tz;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  int c = gidx(g, i, j, k);
+  float temx = (a.dts * 0.5f) * g.rdx;
+  float temy = (a.dts * 0.5f) * g.rdy;
+  float div = fmaf((u[c + 1] - u[c]) * g.rdx, hm_uh(g, hm, i), ((v[c + sj] - v[c]) * g.rdy) * hm_vh(g, hm, j));
+  if (fabsf(div) < a.smeps) div = 0.0f;
+  float advPi = fmaf((-fmaf(u[c], piadv[c] - piadv[c - 1], u[c + 1] * (piadv[c + 1] - piadv[c]))) * temx, hm_uh(g, hm, i),
+                     -((fmaf(v[c], piadv[c] - piadv[c - sj], v[c + sj] * (piadv[c + sj] - piadv[c])) * temy) * hm_vh(g, hm, j)));
+  fpk[c] = fmaf(a.beta, fmaf(w[c], pk1[c] + qk[c], w[c + sk] * (pk2[c] - qk[c])), fmaf(a.dts, fmaf(-ppterm[c], div, ppten[c]), advPi));
+}
+TE_LAUNCH3(acoustic_fpk)
+
+// Vertically implicit w-pi' solve: one column per thread, columns of a warp adjacent
+// in i (coalesced), the Thomas recurrence sequential in k as in the reference.
+__global__ void k_acoustic_w_solve(KArgs A) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const Dims& g = A.g;
+  if (i >= A.gx || j >= A.gy) return;
+  if (i >= g.nx || j >= g.ny) return;
+  const Acoustic a = A.a;
+  const float *pk1 = A.p[2], *pk2 = A.p[3], *qk = A.p[4], *mm = A.p[5], *fpk = A.p[6], *wten = A.p[7], *pp3d = A.p[8];
+  float *w = A.p[9], *cA = A.p[10], *cB = A.p[11];
+  const int sk = g.sJ * g.sK;
+  const float asq = a.alph * a.alph;
+  w[gidx(g, i, j, 0)] = 0.0f;
+  w[gidx(g, i, j, g.nz)] = 0.0f;
+  float aa, bb, cc, dd;
+  auto lam = [&](int kk) {
+    int c = gidx(g, i, j, kk), cm = c - sk;
+    float m = mm[c];
+    aa = (-asq) * (m * (pk1[cm] + qk[cm]));
+    cc = (-asq) * ((-m) * (pk2[c] - qk[c]));
+    bb = fmaf(-asq, m * ((-(pk1[c] + qk[c])) + (pk2[cm] - qk[cm])), 1.0f);
+    float fw = fmaf(a.dts, wten[c], a.beta * ((-m) * (pp3d[c] - pp3d[cm])));
+    dd = fmaf(a.alph, (-m) * ((pp3d[c] + fpk[c]) - (pp3d[cm] + fpk[cm])), w[c] + fw);
+  };
+  {
+    int c = gidx(g, i, j, 1);
+    lam(1);
+    float r = dcr(1.0f, bb);
+    cA[c] = (-cc) * r;
+    cB[c] = dd * r;
+  }
+  for (int k = 2; k < g.nz - 1; k++) {
+    int c = gidx(g, i, j, k);
+    lam(k);
+    float r = dcr(1.0f, fmaf(aa, cA[c - sk], bb));
+    cA[c] = (-cc) * r;
+    cB[c] = fmaf(-aa, cB[c - sk], dd) * r;
+  }
+  {
+    int k = g.nz - 1, c = gidx(g, i, j, k);
+    lam(k);
+    float r = dcr(1.0f, fmaf(aa, cA[c - sk], bb));
+    w[c] = fmaf(-aa, cB[c - sk], dd) * r;
+  }
+  for (int k = g.nz - 2; k >= 1; k--) {
+    int c = gidx(g, i, j, k);
+    w[c] = fmaf(cA[c], w[c + sk], cB[c]);
+  }
+}
+static void launch_acoustic_w_solve(const KArgs& A, cudaStream_t s) {
+  dim3 b(32, 4, 1);
+  dim3 gr((A.gx + 31) / 32, (A.gy + 3) / 4, 1);
+  k_acoustic_w_solve<<<gr, b, 0, s>>>(A);
+}
+
+__global__ void k_acoustic_pp(KArgs A) {
+  TE_K3
+  const Acoustic a = A.a;
+  const float *w = A.p[2], *pk1 = A.p[3], *pk2 = A.p[4], *qk = A.p[5], *fpk = A.p[6];
+  float *pp3d = A.p[7], *ppd = A.p[8], *ppx = A.p[9];
+  const int saveX = A.iv[10];
+  const int sk = g.sJ * g.sK;
+  int i = tx, j = ty, k = tz;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  int c = gidx(g, i, j, k);
+  float prev = pp3d[c];
+  float p = fmaf(a.alph, fmaf(w[c], pk1[c] + qk[c], w[c + sk] * (pk2[c] - qk[c])), prev + fpk[c]);
+  if (fabsf(p) < a.smeps) p = 0.0f;
+  pp3d[c] = p;
+  float dum1 = a.kdiv * (p - prev);
+  ppd[c] = p + dum1;
+  if (saveX != 0) ppx[c] = dum1;
+}
+TE_LAUNCH3(acoustic_pp)
+
+__global__ void k_acoustic_accumulate(KArgs A) {
+  TE_K3
+  const float *u = A.p[2], *v = A.p[3], *w = A.p[4];
+  float *rru = A.p[5], *rrv = A.p[6], *rrw = A.p[7];
+  const float tavg = A.f[8];
+  TE_WHOLE(k <= g.nz)
+  if (tavg > 0.0f) {
+    rru[c] = (rru[c] + u[c]) * tavg;
+    rrv[c] = (rrv[c] + v[c]) * tavg;
+    rrw[c] = fmaf(w[c], A.a.alph, rrw[c]) * tavg;
+  } else {
+    rru[c] = rru[c] + u[c];
+    rrv[c] = rrv[c] + v[c];
+    rrw[c] = rrw[c] + w[c];
+  }
+}
+TE_LAUNCH3(acoustic_accumulate)
+
+// ------------------------------------------------------- periodic halos
+
+__global__ void k_bc_periodic_x(KArgs A) {
+  TE_K3
+  float* f = A.p[1];
+  int h = tx, jj = ty - 3, k = tz;
+  if (h > 3 || jj > g.ny + 3 || k > g.nz) return;
+  int lo = (((-1 - h) % g.nx) + g.nx) % g.nx;
+  int hi = (((g.nx + h) % g.nx) + g.nx) % g.nx;
+  if (h < 3) f[gidx(g, -1 - h, jj, k)] = f[gidx(g, lo, jj, k)];
+  f[gidx(g, g.nx + h, jj, k)] = f[gidx(g, hi, jj, k)];
+}
+TE_LAUNCH3(bc_periodic_x)
+
+__global__ void k_bc_periodic_y(KArgs A) {
+  TE_K3
+  float* f = A.p[1];
+  int h = tx, i = ty - 3, k = tz;
+  if (h > 3 || i > g.nx + 3 || k > g.nz) return;
+  int lo = (((-1 - h) % g.ny) + g.ny) % g.ny;
+  int hi = (((g.ny + h) % g.ny) + g.ny) % g.ny;
+  if (h < 3) f[gidx(g, i, -1 - h, k)] = f[gidx(g, i, lo, k)];
+  f[gidx(g, i, g.ny + h, k)] = f[gidx(g, i, hi, k)];
+}
+TE_LAUNCH3(bc_periodic_y)
+
+// -------------------------------------------------- thermodynamic glue
+
+__global__ void k_update_diagnostics_moist(KArgs A) {
+  TE_K3
+  const float *thp = A.p[1], *ppp = A.p[2], *th0 = A.p[3], *pi0 = A.p[4], *qv0 = A.p[5], *qc0 = A.p[6];
+  const float *qi0 = A.p[7], *rth0 = A.p[8], *qv = A.p[9], *qc = A.p[10], *qr = A.p[11], *qi = A.p[12];
+  const float *qs = A.p[13], *qg = A.p[14];
+  float *thv = A.p[15], *ppterm = A.p[16], *piadv = A.p[17], *thterm = A.p[18], *buoy = A.p[19];
+  const float rd = 287.04f, rv = 461.5f, cp = 1005.7f, cv = 718.66003f, cpv = 1870.0f, cvv = 1408.5f;
+  const float rovcp = 0.28541315f, cpl = 4190.0f, cpi = 2106.0f;
+  TE_WHOLE(k < g.nz)
+  float reps = dcr(rv, rd);
+  float repsm1 = reps - 1.0f;
+  float gacc = 9.81f;
+  float qvv = wmax(qv[c], 0.0f);
+  float liq = qc[c] + qr[c];
+  float ice = (qi[c] + qs[c]) + qg[c];
+  float qli = wmax(0.0f, liq + ice);
+  float cpli = fmaf(cpl, wmax(0.0f, liq), cpi * wmax(0.0f, ice));
+  float th = th0[k] + thp[c];
+  float pi = pi0[k] + ppp[c];
+  float cpm = fmaf(cpv, qvv, cp) + cpli;
+  float cvm = dcr(1.0f, fmaf(cvv, qvv, cv) + cpli);
+  thv[c] = dcr(th * fmaf(reps, qvv, 1.0f), (1.0f + qvv) + qli);
+  piadv[c] = pi;
+  ppterm[c] = ((pi * rovcp) * cpm) * cvm;
+  thterm[c] = (th * fmaf(-rovcp, cpm, fmaf(rv, qvv, rd))) * cvm;
+  buoy[c] = gacc * (fmaf(thp[c], rth0[k], repsm1 * (qvv - qv0[k])) - ((qli - qc0[k]) - qi0[k]));
+}
+TE_LAUNCH3(update_diagnostics_moist)
+
+__global__ void k_pressure_tendency(KArgs A) {
+  TE_K3
+  const float *th = A.p[1], *qv = A.p[2], *rho = A.p[3], *ppi = A.p[4], *thten = A.p[5], *qpten = A.p[6];
+  const float *th0 = A.p[7], *pi0 = A.p[8];
+  const float dt = A.f[9];
+  const int hasDiabatic = A.iv[10];
+  float* ppten = A.p[11];
+  const int hasStepTend = A.iv[12];
+  const float* qvt = A.p[13];
+  const int moist = A.iv[14];
+  const float rd = 287.04f, rv = 461.5f, cp = 1005.7f, p00 = 1e5f;
+  int i = tx, j = ty, k = tz;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  int c = gidx(g, i, j, k);
+  float rp00 = dcr(1.0f, p00);
+  float rddcv = dcr(rd, cp - rd);
+  float tem = 0.0001f * 0.0001f;
+  float qsmall = 1e-14f;
+  float tht = hasStepTend != 0 ? thten[c] : 0.0f;
+  if (moist == 0) {
+    float p = 0.0f;
+    if (fabsf(dt * tht) > tem) {
+      float thnew = fmaf(dt, tht, th[c]);
+      float pinew = rr_pow_cr(((rho[c] * (th0[k] + thnew)) * rd) * rp00, rddcv) - pi0[k];
+      p = dcr(pinew - ppi[c], dt);
+    }
+    ppten[c] = p;
+    return;
+  }
+  float qvten = qvt[c];
+  float p = 0.0f;
+  if (fabsf(dt * tht) > tem || fabsf(dt * qvten) > qsmall) {
+    float thnew = fmaf(dt, tht, th[c]);
+    float qvnew = fmaf(dt, qvten, qv[c]);
+    float pinew = rr_pow_cr(((rho[c] * (th0[k] + thnew)) * fmaf(rv, qvnew, rd)) * rp00, rddcv) - pi0[k];
+    p = dcr(pinew - ppi[c], dt);
+  }
+  if (hasDiabatic != 0) p = p + qpten[c];
+  ppten[c] = p;
+}
+TE_LAUNCH3(pressure_tendency)
+
+__global__ void k_divergence3d(KArgs A) {
+  TE_K3
+  const float *u = A.p[1], *v = A.p[2], *w = A.p[3], *mh = A.p[4];
+  float* div = A.p[5];
+  const float* hm = A.p[30];
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  int i = tx, j = ty, k = tz;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  int c = gidx(g, i, j, k);
+  float d = fmaf((w[c + sk] - w[c]) * g.rdz, mh[k],
+                 fmaf((u[c + 1] - u[c]) * g.rdx, hm_uh(g, hm, i), ((v[c + sj] - v[c]) * g.rdy) * hm_vh(g, hm, j)));
+  div[c] = fabsf(d) < 1e-30f ? 0.0f : d;
+}
+TE_LAUNCH3(divergence3d)
+
+__global__ void k_update_rho_prs(KArgs A) {
+  TE_K3
+  const int moist = A.iv[1];
+  const float *thp = A.p[2], *ppp = A.p[3], *th0 = A.p[4], *pi0 = A.p[5], *qv = A.p[6];
+  float *prs = A.p[7], *rho = A.p[8];
+  int i = tx, j = ty, k = tz;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  int c = gidx(g, i, j, k);
+  float cpdrd = dcr(1005.7f, 287.04f);
+  float pi = pi0[k] + ppp[c];
+  float th = th0[k] + thp[c];
+  float p = 1e5f * rr_pow_cr(pi, cpdrd);
+  prs[c] = p;
+  float rmix = moist != 0 ? fmaf(wmax(0.0f, qv[c]), 461.5f, 287.04f) : 287.04f;
+  rho[c] = dcr(p, (th * pi) * rmix);
+}
+TE_LAUNCH3(update_rho_prs)
+
+__global__ void k_diabatic_unapply(KArgs A) {
+  TE_K3
+  const float dt = A.f[1];
+  float *pp3d = A.p[2], *th = A.p[3], *qv = A.p[4], *qc = A.p[5];
+  float *qpten = A.p[6], *qtten = A.p[7], *qvten = A.p[8], *qcten = A.p[9];
+  int i = tx, j = ty, k = tz;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  int c = gidx(g, i, j, k);
+  float x;
+  x = fmaf(-dt, qpten[c], pp3d[c]);
+  pp3d[c] = x;
+  qpten[c] = x;
+  x = fmaf(-dt, qtten[c], th[c]);
+  th[c] = x;
+  qtten[c] = x;
+  x = fmaf(-dt, qvten[c], qv[c]);
+  qv[c] = x;
+  qvten[c] = x;
+  x = fmaf(-dt, qcten[c], qc[c]);
+  qc[c] = x;
+  qcten[c] = x;
+}
+TE_LAUNCH3(diabatic_unapply)
+
+__global__ void k_diabatic_rates(KArgs A) {
+  TE_K3
+  const float dt = A.f[1];
+  const float *pp3d = A.p[2], *th = A.p[3], *qv = A.p[4], *qc = A.p[5];
+  float *qpten = A.p[6], *qtten = A.p[7], *qvten = A.p[8], *qcten = A.p[9];
+  int i = tx, j = ty, k = tz;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  int c = gidx(g, i, j, k);
+  float rdt = dcr(1.0f, dt);
+  qpten[c] = (pp3d[c] - qpten[c]) * rdt;
+  qtten[c] = (th[c] - qtten[c]) * rdt;
+  qvten[c] = (qv[c] - qvten[c]) * rdt;
+  qcten[c] = (qc[c] - qcten[c]) * rdt;
+}
+TE_LAUNCH3(diabatic_rates)
+
+__global__ void k_ppx_finish(KArgs A) {
+  TE_K3
+  const float* pp3d = A.p[1];
+  float* ppx = A.p[2];
+  int i = tx, j = ty, k = tz;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  int c = gidx(g, i, j, k);
+  ppx[c] = pp3d[c] + ppx[c];
+}
+TE_LAUNCH3(ppx_finish)
+
+// ------------------------------------------------------------ registry
+// Parameter tables: binding index, ptr/ref, written (the reference kernel ABI,
+// data/kernels/kernels.json); the write order defines the per-dispatch hash slots.
+
+#define R(i) {i, kRef, 0}
+#define P(i) {i, kPtr, 0}
+#define W(i) {i, kPtr, 1}
+
+static const KernelSpec kTable[] = {
+    {"adv_flux_x", 4, {R(0), P(1), P(2), W(3)}, false, launch_adv_flux_x},
+    {"adv_flux_y", 4, {R(0), P(1), P(2), W(3)}, false, launch_adv_flux_y},
+    {"adv_flux_z", 6, {R(0), P(1), P(2), P(3), P(4), W(5)}, false, launch_adv_flux_z},
+    {"adv_flux_x_stag", 9, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), P(7), W(8)}, false, launch_adv_flux_x_stag},
+    {"adv_flux_y_stag", 9, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), P(7), W(8)}, false, launch_adv_flux_y_stag},
+    {"adv_flux_z_stag", 10, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), P(7), W(8), P(30)}, false, launch_adv_flux_z_stag},
+    {"adv_flux_x_weno", 6, {R(0), P(1), P(2), R(3), R(4), W(5)}, false, launch_adv_flux_x_weno},
+    {"adv_flux_y_weno", 6, {R(0), P(1), P(2), R(3), R(4), W(5)}, false, launch_adv_flux_y_weno},
+    {"adv_flux_z_weno", 9, {R(0), P(1), P(2), P(3), P(4), R(5), R(6), R(7), W(8)}, false, launch_adv_flux_z_weno},
+    {"adv_flux_x_weno_uv", 6, {R(0), R(1), P(2), P(3), R(4), W(5)}, false, launch_adv_flux_x_weno_uv},
+    {"adv_flux_y_weno_uv", 6, {R(0), R(1), P(2), P(3), R(4), W(5)}, false, launch_adv_flux_y_weno_uv},
+    {"adv_flux_z_weno_uv", 9, {R(0), R(1), P(2), P(3), P(4), P(5), R(6), W(7), P(30)}, false, launch_adv_flux_z_weno_uv},
+    {"adv_flux_x_weno_w", 6, {R(0), P(1), P(2), P(3), R(4), W(5)}, false, launch_adv_flux_x_weno_w},
+    {"adv_flux_y_weno_w", 6, {R(0), P(1), P(2), P(3), R(4), W(5)}, false, launch_adv_flux_y_weno_w},
+    {"adv_flux_z_weno_w", 5, {R(0), P(1), P(2), R(3), W(4)}, false, launch_adv_flux_z_weno_w},
+    {"adv_assemble", 24, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), W(11), R(12), P(13), P(14),
+                          P(15), P(16), R(17), P(30), P(18), W(19), R(27), P(24), P(25)}, false, launch_adv_assemble},
+    {"rk_update", 6, {R(0), R(1), P(2), P(3), W(4), R(5)}, false, launch_rk_update},
+    {"pdef_dum", 12, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), P(7), R(8), R(9), W(10), P(30)}, false, launch_pdef_dum},
+    {"pdef_apply", 18, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), P(11), P(12), P(13), R(14),
+                        R(15), W(16), P(30)}, false, launch_pdef_apply},
+    {"build_sadv", 4, {R(0), P(1), P(2), W(3)}, false, launch_build_sadv},
+    {"massflux_from_state", 10, {R(0), P(1), P(2), P(3), P(4), P(5), W(6), W(7), W(8), P(24)}, false, launch_massflux_from_state},
+    {"div_massflux", 8, {R(0), P(1), P(2), P(3), P(4), W(5), P(30), P(25)}, false, launch_div_massflux},
+    {"velocity_to_massflux", 7, {R(0), P(1), P(2), W(3), W(4), W(5), P(24)}, false, launch_velocity_to_massflux},
+    {"stage_state_reset", 11, {R(0), P(1), P(2), P(3), P(4), W(5), W(6), W(7), W(8), W(9), P(10)}, false, launch_stage_state_reset},
+    {"stage_tendency_reset", 4, {R(0), W(1), W(2), W(3)}, false, launch_stage_tendency_reset},
+    {"buoyancy_apply", 5, {R(0), P(1), P(2), P(3), W(4)}, false, launch_buoyancy_apply},
+    {"apply_thterm", 4, {R(0), P(1), P(2), W(3)}, false, launch_apply_thterm},
+    {"acoustic_prepare", 17, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), W(11), W(12), W(13),
+                              W(14), P(24), P(25)}, true, launch_acoustic_prepare},
+    {"acoustic_begin", 6, {R(0), R(1), P(2), W(3), W(4), W(5)}, true, launch_acoustic_begin},
+    {"acoustic_uv", 13, {R(0), R(1), P(2), P(3), P(4), P(5), W(6), W(7), R(8), P(30), P(21), P(23), P(25)}, true, launch_acoustic_uv},
+    {"acoustic_fpk", 19, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), W(11), P(30), P(15), P(16),
+                          P(17), P(24), P(25), R(26)}, true, launch_acoustic_fpk},
+    {"acoustic_w_solve", 12, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), W(9), W(10), W(11)}, true, launch_acoustic_w_solve},
+    {"acoustic_pp", 11, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), W(7), W(8), W(9), R(10)}, true, launch_acoustic_pp},
+    {"acoustic_accumulate", 9, {R(0), R(1), P(2), P(3), P(4), W(5), W(6), W(7), R(8)}, true, launch_acoustic_accumulate},
+    {"bc_periodic_x", 2, {R(0), W(1)}, false, launch_bc_periodic_x},
+    {"bc_periodic_y", 2, {R(0), W(1)}, false, launch_bc_periodic_y},
+    {"update_diagnostics_moist", 20, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), P(11), P(12),
+                                      P(13), P(14), W(15), W(16), W(17), W(18), W(19)}, false, launch_update_diagnostics_moist},
+    {"pressure_tendency", 15, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), R(9), R(10), R(12), P(13), R(14), W(11)},
+     false, launch_pressure_tendency},
+    {"divergence3d", 7, {R(0), P(1), P(2), P(3), P(4), W(5), P(30)}, false, launch_divergence3d},
+    {"update_rho_prs", 9, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), W(7), W(8)}, false, launch_update_rho_prs},
+    {"diabatic_unapply", 10, {R(0), R(1), W(2), W(3), W(4), W(5), W(6), W(7), W(8), W(9)}, false, launch_diabatic_unapply},
+    {"diabatic_rates", 10, {R(0), R(1), P(2), P(3), P(4), P(5), W(6), W(7), W(8), W(9)}, false, launch_diabatic_rates},
+    {"ppx_finish", 3, {R(0), P(1), W(2)}, false, launch_ppx_finish},
+};
+
+#undef R
+#undef P
+#undef W
+
+const KernelSpec* kernel_table(int* count) {
+  *count = (int)(sizeof(kTable) / sizeof(kTable[0]));
+  return kTable;
+}
+
+const KernelSpec* find_kernel(const char* name) {
+  int n;
+  const KernelSpec* t = kernel_table(&n);
+  for (int i = 0; i < n; i++)
+    if (std::strcmp(t[i].name, name) == 0) return &t[i];
+  return nullptr;
+}
+
+}  // namespace te

@@ -1,0 +1,48 @@
+// Kernel registry: one CUDA kernel per reference kernel name on the dynamics path.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "te_math.cuh"
+
+namespace te {
+
+constexpr int kMaxBind = 40;
+
+// Decoded arguments of one dispatch.  `p[n]` is the device address of binding n
+// (memory word offset of the tape player), `f[n]`/`iv[n]`/`iv2[n]` are the f32 / i32 /
+// second i32 word of a setBytes struct bound at n.
+struct KArgs {
+  Dims g;
+  Acoustic a;
+  int gx, gy, gz;
+  float* p[kMaxBind];
+  float f[kMaxBind];
+  int iv[kMaxBind];
+  int iv2[kMaxBind];
+};
+
+enum ParamKind : uint8_t { kPtr = 0, kRef = 1 };
+
+struct ParamSpec {
+  int8_t index;
+  uint8_t kind;
+  uint8_t write;
+};
+
+typedef void (*LaunchFn)(const KArgs&, cudaStream_t);
+
+struct KernelSpec {
+  const char* name;
+  int nparams;
+  ParamSpec params[24];
+  bool acoustic;  // binding 1 is AcousticParams
+  LaunchFn launch;
+};
+
+// All kernels this library implements (te_kernels.cu).
+const KernelSpec* kernel_table(int* count);
+const KernelSpec* find_kernel(const char* name);
+
+}  // namespace te

@@ -1,0 +1,221 @@
+"""``Replayer``: host-side mirror of the reference's tape player over the CUDA C-ABI.
+
+The reference player (web/replay.js:36-396) is a JavaScript class driving WebGPU.  This
+class has the same methods and fields, with the same argument meaning, but plays the
+tape on a B200 through ``libthunderstep.so`` (include/thunderstep.h):
+
+=========================================  ==========================================
+reference (web/replay.js)                  here
+=========================================  ==========================================
+``new Replayer(device, tape, kernels, s)``  ``Replayer(tape, kernels=None, device=0)``
+``plan(withHashes)`` + ``await build()``   ``plan(with_hashes)`` + ``build()``
+``upload(id, u8)`` / ``uploadAsync``       ``upload(buf_id, data)``
+``await useStep(cmds)``                    ``use_step(cmds)``
+``encodeSteps(enc, n, withHashes, last)``  ``encode_steps(n, with_hashes, last_op)``
+``encodeDiag(enc)``                        ``encode_diag()``
+``await read(words, offWords)``            ``read(words, off_words)`` -> numpy uint32
+``await readHashes()``                     ``read_hashes()`` -> numpy uint32
+``base``, ``buffersEnd``, ``memWords``,     ``base``, ``buffers_end``, ``mem_words``,
+``hashCount``                              ``hash_count``
+=========================================  ==========================================
+
+Errors raise ``RuntimeError`` with the library's message, where the reference throws
+``Error`` (unknown kernel, bytes overflow, ...).  There is no CPU fallback: when the
+library cannot be loaded or no CUDA device is present, construction fails.
+"""
+import ctypes
+import json
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, 'libthunderstep.so')
+
+TE_MODE_EXACT = 0
+TE_MODE_FUSED = 1
+
+_LIB = None
+
+
+class TeInfo(ctypes.Structure):
+    _fields_ = [('mem_words', ctypes.c_uint64), ('buffers_end', ctypes.c_uint64),
+                ('scratch_base', ctypes.c_uint64), ('hash_count', ctypes.c_uint32),
+                ('num_buffers', ctypes.c_uint32), ('num_ops', ctypes.c_uint32),
+                ('num_dispatches', ctypes.c_uint32)]
+
+
+class TeConfig(ctypes.Structure):
+    _fields_ = [('device', ctypes.c_int), ('flags', ctypes.c_int), ('reserved', ctypes.c_uint64 * 4)]
+
+
+EXPORTS = {
+    'te_create': ([ctypes.POINTER(TeConfig), ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    'te_plan': ([ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_int],
+                ctypes.c_int),
+    'te_get_info': ([ctypes.c_void_p, ctypes.POINTER(TeInfo)], ctypes.c_int),
+    'te_buffer_base': ([ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
+    'te_upload': ([ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t], ctypes.c_int),
+    'te_write_words': ([ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_size_t], ctypes.c_int),
+    'te_use_step': ([ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
+    'te_run': ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    'te_run_ops': ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    'te_run_diag': ([ctypes.c_void_p], ctypes.c_int),
+    'te_read': ([ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p], ctypes.c_int),
+    'te_read_hashes': ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t], ctypes.c_int),
+    'te_clear_hashes': ([ctypes.c_void_p], ctypes.c_int),
+    'te_device_ptr': ([ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    'te_set_mode': ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    'te_op_name': ([ctypes.c_void_p, ctypes.c_int], ctypes.c_char_p),
+    'te_sync': ([ctypes.c_void_p], ctypes.c_int),
+    'te_destroy': ([ctypes.c_void_p], None),
+    'te_last_error': ([ctypes.c_void_p], ctypes.c_char_p),
+    'te_region_hash_host': ([ctypes.c_void_p, ctypes.c_uint64], ctypes.c_uint32),
+    'te_set_stream': ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    'te_kernel_table_json': ([ctypes.c_char_p, ctypes.c_size_t], ctypes.c_size_t),
+}
+
+
+def load_library(path=LIB_PATH):
+    """Load ``libthunderstep.so`` (raises if it is missing: there is no fallback)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise RuntimeError('libthunderstep.so is not built (%s); run __graft_entry__.build()' % path)
+    lib = ctypes.CDLL(path)
+    for name, (args, res) in EXPORTS.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    _LIB = lib
+    return lib
+
+
+def _json_bytes(x):
+    if isinstance(x, (bytes, bytearray)):
+        return bytes(x)
+    if isinstance(x, str):
+        return x.encode()
+    return json.dumps(x, separators=(',', ':')).encode()
+
+
+class Replayer:
+    """Plays a ThunderEngine command tape on one B200 (see the module docstring)."""
+
+    def __init__(self, tape, kernels=None, device=0):
+        self.lib = load_library()
+        self.tape = tape
+        self.kernels = kernels
+        self.device = device
+        cfg = TeConfig(device=device, flags=0)
+        h = ctypes.c_void_p()
+        rc = self.lib.te_create(ctypes.byref(cfg), ctypes.byref(h))
+        self.h = h
+        if rc != 0:
+            msg = self.lib.te_last_error(h).decode() if h else 'te_create failed'
+            self.lib.te_destroy(h)
+            self.h = None
+            raise RuntimeError(msg)
+        self.base = []
+        self.buffers_end = self.mem_words = self.hash_count = 0
+        self._with_hashes = False
+
+    # ---- helpers
+    def _check(self, rc):
+        if rc != 0:
+            raise RuntimeError('thunderstep error %d: %s' % (rc, self.lib.te_last_error(self.h).decode()))
+
+    def close(self):
+        if getattr(self, 'h', None):
+            self.lib.te_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- Replayer API
+    def plan(self, with_hashes=False):
+        """Record the layout request; memory is laid out and allocated by ``build``."""
+        self._with_hashes = bool(with_hashes)
+
+    def build(self):
+        tj = _json_bytes(self.tape)
+        kj = _json_bytes(self.kernels) if self.kernels is not None else None
+        self._check(self.lib.te_plan(self.h, tj, len(tj), kj, len(kj) if kj else 0, 1 if self._with_hashes else 0))
+        info = TeInfo()
+        self._check(self.lib.te_get_info(self.h, ctypes.byref(info)))
+        self.mem_words = info.mem_words
+        self.buffers_end = info.buffers_end
+        self.hash_count = info.hash_count
+        self.num_ops = info.num_ops
+        self.num_dispatches = info.num_dispatches
+        self.base = []
+        for i in range(info.num_buffers):
+            o = ctypes.c_uint64()
+            self._check(self.lib.te_buffer_base(self.h, i, ctypes.byref(o)))
+            self.base.append(o.value)
+
+    def upload(self, buf_id, data):
+        b = np.ascontiguousarray(np.frombuffer(bytes(data), dtype=np.uint8) if isinstance(data, (bytes, bytearray))
+                                 else np.asarray(data)).view(np.uint8)
+        self._check(self.lib.te_upload(self.h, int(buf_id), b.ctypes.data_as(ctypes.c_void_p), b.nbytes))
+
+    def write_words(self, off, data):
+        b = np.ascontiguousarray(np.asarray(data)).view(np.uint8)
+        self._check(self.lib.te_write_words(self.h, int(off), b.ctypes.data_as(ctypes.c_void_p), b.nbytes))
+
+    def use_step(self, cmds):
+        j = _json_bytes(cmds)
+        self._check(self.lib.te_use_step(self.h, j, len(j)))
+        info = TeInfo()
+        self._check(self.lib.te_get_info(self.h, ctypes.byref(info)))
+        self.num_ops = info.num_ops
+
+    def encode_steps(self, n=1, with_hashes=False, last_op=None):
+        if last_op is None:
+            self._check(self.lib.te_run(self.h, int(n), 1 if with_hashes else 0))
+        else:
+            for _ in range(int(n)):
+                self._check(self.lib.te_run_ops(self.h, 0, int(last_op), 1 if with_hashes else 0))
+
+    def run_ops(self, first, last, with_hashes=False):
+        self._check(self.lib.te_run_ops(self.h, int(first), int(last), 1 if with_hashes else 0))
+
+    def encode_diag(self):
+        self._check(self.lib.te_run_diag(self.h))
+
+    def read(self, words, off_words=0):
+        out = np.empty(int(words), dtype=np.uint32)
+        self._check(self.lib.te_read(self.h, int(off_words), int(words), out.ctypes.data_as(ctypes.c_void_p)))
+        return out
+
+    def read_hashes(self):
+        out = np.zeros(max(self.hash_count, 1), dtype=np.uint32)
+        self._check(self.lib.te_read_hashes(self.h, out.ctypes.data_as(ctypes.c_void_p), self.hash_count))
+        return out[:self.hash_count]
+
+    def clear_hashes(self):
+        self._check(self.lib.te_clear_hashes(self.h))
+
+    def set_mode(self, mode):
+        self._check(self.lib.te_set_mode(self.h, int(mode)))
+
+    def device_ptr(self, off_words):
+        p = ctypes.c_void_p()
+        self._check(self.lib.te_device_ptr(self.h, int(off_words), ctypes.byref(p)))
+        return p.value
+
+    def op_name(self, i):
+        r = self.lib.te_op_name(self.h, int(i))
+        return r.decode() if r else None
+
+    def set_stream(self, stream_handle):
+        """Launch on a caller-owned CUDA stream (int handle; 0 = the context's own)."""
+        self._check(self.lib.te_set_stream(self.h, ctypes.c_void_p(int(stream_handle) or None)))
+
+    def sync(self):
+        self._check(self.lib.te_sync(self.h))
