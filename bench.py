@@ -38,6 +38,10 @@ def parse():
     ap.add_argument('--mode', default='fused', choices=['fused', 'exact'])
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true')
+    ap.add_argument('--no-roofline', action='store_true', help='skip the per-kernel timing pass')
+    ap.add_argument('--workload', default='at_scale', choices=['at_scale', 'medium', 'small'],
+                    help='at_scale = 256x256x80 (the benchmark); medium = 160x160x80 with the same '
+                         'physics, for profiler captures; small = 64x64x40')
     return ap.parse_args()
 
 
@@ -132,7 +136,10 @@ class ClockSampler:
 
 def workload(cfg_name='at_scale'):
     from thunderengine_web_b200 import scenario, timestep
-    cfg = scenario.AT_SCALE if cfg_name == 'at_scale' else scenario.SMALL
+    if cfg_name == 'medium':
+        cfg = scenario.Config('cm1-dyn-160x160x80', 160, 160, 80, 500.0, 250.0, 3.0, 8, 25.0, 1)
+    else:
+        cfg = scenario.AT_SCALE if cfg_name == 'at_scale' else scenario.SMALL
     run = timestep.Run(cfg)
     return cfg, run
 
@@ -146,16 +153,17 @@ def peaks():
     return 6650.0, 'fallback'
 
 
-def cpu_baseline_sample(run_small_steps=1):
+def cpu_baseline_sample(budget_s=10.0):
     """Time the reference's kernels (oracle/_ref, else the oracle port) on the host cores:
-    one large step of a 64x64x80 horizontal sub-domain of the benchmark configuration."""
+    large steps of the benchmark configuration itself (256x256x80), as many as fit in
+    about ``budget_s`` seconds after one warm-up step."""
     from tests import helpers
     from thunderengine_web_b200 import scenario, timestep
     ref = helpers.reference()
     kind = 'reference' if ref is not None else 'port'
     kern = (ref or helpers.oracle()).get
     helpers.oracle()   # FTZ on the OpenMP team
-    cfg = scenario.Config('cm1-dyn-64x64x80-of-256x256x80', 64, 64, 80, 500.0, 250.0, 3.0, 8, 25.0, 1)
+    cfg = scenario.AT_SCALE
     run = timestep.Run(cfg)
     tape = run.tape(1)
     init = run.initial_buffers()
@@ -164,17 +172,19 @@ def cpu_baseline_sample(run_small_steps=1):
     p.plan(False)
     for i, b in init.items():
         p.upload(i, b)
-    p.run(kern)                      # warm-up step
     t0 = time.perf_counter()
-    for _ in range(run_small_steps):
+    p.run(kern)                      # warm-up step
+    t_one = time.perf_counter() - t0
+    nsteps = max(1, min(20, int(budget_s / max(t_one, 1e-3))))
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
         p.run(kern)
     dt = time.perf_counter() - t0
     pts = cfg.nx * cfg.ny * cfg.nz
-    return {'value': pts * run_small_steps / dt, 'unit': METRIC, 'cores': os.cpu_count(), 'kind': kind,
-            'sample': '%d large step(s) of a 64x64x80 sub-domain of the 256x256x80 workload (same dx, dz, dt, '
-                      'nsound) with %s kernels, OpenMP over the dispatch grid' % (
-                          run_small_steps, 'the reference\'s WGSL translated to C++' if kind == 'reference'
-                          else 'the oracle'),
+    return {'value': pts * nsteps / dt, 'unit': METRIC, 'cores': os.cpu_count(), 'kind': kind,
+            'sample': '%d large step(s) of the 256x256x80 workload after one warm-up step, %s kernels, '
+                      'OpenMP over the dispatch grid on all host cores' % (
+                          nsteps, "the reference's WGSL translated to C++" if kind == 'reference' else 'oracle'),
             'seconds': dt}
 
 
@@ -186,7 +196,7 @@ def run_ours(a, rank, world, local):
     from tests import helpers
     dev = local if torch.cuda.device_count() > local else 0
     torch.cuda.set_device(dev)
-    cfg, run = workload()
+    cfg, run = workload(a.workload)
     tape = run.tape(1)
     run.tape_cmds = tape['steps'][0]
     init = run.initial_buffers()
@@ -195,7 +205,9 @@ def run_ours(a, rank, world, local):
     r.build()
     for i, b in init.items():
         r.upload(i, b)
-    stream = torch.cuda.current_stream(dev)
+    # a dedicated (non-default) stream shared by the library and torch's events
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
     r.set_stream(stream.cuda_stream)
     mode = TE_MODE_FUSED if a.mode == 'fused' else TE_MODE_EXACT
     r.set_mode(mode)
@@ -220,7 +232,7 @@ def run_ours(a, rank, world, local):
 
     # per-kernel timing for the roofline: each distinct op of the step alone, events on
     # the launch stream; achieved = algorithmic bytes per launch / launch time
-    roof = kernel_roofline(r, run, stream, mode)
+    roof = None if a.no_roofline else kernel_roofline(r, run, stream, mode)
 
     # end to end through the public API with host buffers: every step uploads the state
     # fields from pinned memory, plays the step, reads the prognostic fields back
@@ -229,7 +241,12 @@ def run_ours(a, rank, world, local):
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline_sample()
     ops = r.num_ops
-    launches = roof.pop('_launches_per_step')
+    if roof is not None:
+        launches = roof.pop('_launches_per_step')
+    elif mode == TE_MODE_FUSED:
+        launches = sum(sg[3] for sg in r.fused_segments())
+    else:
+        launches = r.num_dispatches
     out = {
         'metric': METRIC, 'value': value, 'unit': METRIC, 'n_gpus': world, 'steps': a.steps, 'warmup': a.warmup,
         'ms_per_step': ms / a.steps, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
@@ -245,51 +262,75 @@ def run_ours(a, rank, world, local):
 
 
 def kernel_roofline(r, run, stream, mode):
+    """Per-kernel device time of one step, measured with CUDA events on the launch stream:
+    each exact dispatch kind and each fused kernel is re-launched alone `reps` times.
+    The dominant kernel (time x launches per step) gets the roofline figures."""
     import torch
     from tests import helpers
     peak, src = peaks()
-    tape_fields = run.fields
-    g = run.grid
-    field_of = {}
-    arena_base = r.base[run.rec.ids['arena']]
-    for n, off in tape_fields.items():
-        field_of[arena_base + off // 4] = n
     km = helpers.kernels_meta()
-    stats = {}
-    nops = r.num_ops
-    names = [r.op_name(i) for i in range(nops)]
+    disp = tape_dispatches(run, run.tape_cmds)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    # time each distinct kernel (first occurrence), reps launches
-    seen = {}
-    for i, n in enumerate(names):
-        if n == 'copy':
-            continue
-        seen.setdefault(n, []).append(i)
     reps = 5
-    for n, idx in seen.items():
-        i = idx[0]
-        r.run_ops(i, i)
+
+    def timed(fn):
+        fn()
         torch.cuda.synchronize()
         e0.record(stream)
         for _ in range(reps):
-            r.run_ops(i, i)
+            fn()
         e1.record(stream)
         torch.cuda.synchronize()
-        t = e0.elapsed_time(e1) / reps
-        stats[n] = {'ms': t, 'launches': len(idx)}
-    tot = sum(s['ms'] * s['launches'] for s in stats.values())
-    top = max(stats, key=lambda n: stats[n]['ms'] * stats[n]['launches'])
-    disp = tape_dispatches(run, run.tape_cmds)
-    bytes_per_launch = dispatch_bytes(disp[seen[top][0]], km)
-    ms = stats[top]['ms']
-    achieved = bytes_per_launch / (ms / 1e3) / 1e9
-    shares = sorted(((n, s['ms'] * s['launches'] / tot) for n, s in stats.items()), key=lambda x: -x[1])
-    launches_per_step = sum(s['launches'] for s in stats.values())
+        return e0.elapsed_time(e1) / reps
+
+    stats = {}   # name -> [ms per launch, launches per step, algorithmic bytes per launch]
+    g = run.grid
+    if mode == 1:
+        segs = r.fused_segments()
+        exact_ops = [i for (kind, a, b, _) in segs if kind == 0 for i in range(a, b + 1)]
+        acu = [q for q, sg in enumerate(segs) if sg[0] == 1]
+        halo = [q for q, sg in enumerate(segs) if sg[0] == 2]
+        if acu:
+            q = acu[-1]
+            pts_whole = g.count
+            pts = g.nx * g.ny * g.nz
+            stats['acoustic_uv_accumulate (fused)'] = [timed(lambda: r.run_segment(q, 0)), len(acu), 12 * 4 * pts_whole]
+            stats['acoustic_column (fused fpk+w_solve+pp+accumulate)'] = [timed(lambda: r.run_segment(q, 1)), len(acu),
+                                                                          19 * 4 * pts]
+            stats['halo_periodic x4 (fused)'] = [timed(lambda: r.run_segment(q, 2)), len(acu),
+                                                 4 * 2 * 4 * 7 * (g.strideK + g.nx) * (g.nz + 1)]
+        if halo:
+            q = halo[0]
+            nf = segs[q][2] - segs[q][1] + 1
+            stats['halo_periodic (fused)'] = [timed(lambda: r.run_segment(q, -1)), len(halo),
+                                              (nf // 2) * 2 * 4 * 7 * (g.strideK + g.nx) * (g.nz + 1)]
+    else:
+        exact_ops = list(range(r.num_ops))
+    seen = {}
+    for i in exact_ops:
+        n = r.op_name(i)
+        if n != 'copy':
+            seen.setdefault(n, []).append(i)
+    for n, idx in seen.items():
+        i = idx[0]
+        stats[n] = [timed(lambda: r.run_ops(i, i)), len(idx), dispatch_bytes(disp[i], km, g.nz)]
+    tot = sum(v[0] * v[1] for v in stats.values())
+    top = max(stats, key=lambda n: stats[n][0] * stats[n][1])
+    ms, _, byts = stats[top]
+    achieved = byts / (ms / 1e3) / 1e9
+    shares = sorted(((n, v[0] * v[1] / tot) for n, v in stats.items()), key=lambda x: -x[1])
+    launches = sum(v[1] for v in stats.values())
+    if mode == 1:
+        launches = sum(sg[3] for sg in r.fused_segments())
     return {'kernel': top, 'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
-            'frac': achieved / peak, 'peak_source': '%s (MEASURED_PEAKS.json hbm_gbs)' % src if src == 'measured'
-            else 'fallback 6650 GB/s', 'algorithmic_bytes_per_launch': bytes_per_launch,
-            'launch_ms': ms, 'traffic': None, 'share_of_step': shares[0][1],
-            'top_kernels': [[n, round(s, 4)] for n, s in shares[:8]], '_launches_per_step': launches_per_step}
+            'frac': achieved / peak, 'peak_source': ('measured (MEASURED_PEAKS.json hbm_gbs)' if src == 'measured'
+                                                     else 'fallback 6650 GB/s'),
+            'algorithmic_bytes_per_launch': byts, 'launch_ms': ms, 'traffic': None,
+            'share_of_step': shares[0][1], 'sum_of_kernel_ms_per_step': tot,
+            'top_kernels': [[n, round(sv, 4), round(stats[n][0], 4), stats[n][1],
+                             round(stats[n][2] / (stats[n][0] / 1e3) / 1e9, 1)] for n, sv in shares[:10]],
+            'top_kernels_columns': ['kernel', 'share', 'ms_per_launch', 'launches_per_step', 'achieved_GBps'],
+            '_launches_per_step': launches}
 
 
 # Fields a kernel both reads and writes at the same points (binding indices), counted
@@ -325,9 +366,10 @@ def tape_dispatches(run, cmds):
     return out
 
 
-def dispatch_bytes(d, km):
+def dispatch_bytes(d, km, nz):
     """Algorithmic bytes of one dispatch: (distinct arena fields bound to its pointer
-    parameters, read-modify-write fields twice) x 4 B x dispatch points."""
+    parameters, read-modify-write fields twice) x 4 B x points of its range; a column
+    kernel (rank 2, e.g. acoustic_w_solve) covers nz levels per dispatched column."""
     params = {p['index']: p for p in km[d['name']]['params']}
     fields = {}
     for idx, f in d['fields'].items():
@@ -337,6 +379,8 @@ def dispatch_bytes(d, km):
         w = 2 if idx in RMW.get(d['name'], ()) else 1
         fields[f] = max(fields.get(f, 0), w)
     pts = d['grid'][0] * d['grid'][1] * d['grid'][2]
+    if km[d['name']].get('rank') == 2:
+        pts *= nz
     return sum(fields.values()) * 4 * pts
 
 
@@ -395,7 +439,7 @@ def run_reference(a, rank, world):
     kind = 'reference' if ref is not None else 'port'
     kern = (ref or helpers.oracle()).get
     helpers.oracle()
-    cfg = scenario.Config('cm1-dyn-64x64x80-of-256x256x80', 64, 64, 80, 500.0, 250.0, 3.0, 8, 25.0, 1)
+    cfg = scenario.AT_SCALE
     run = timestep.Run(cfg)
     tape = run.tape(1)
     init = run.initial_buffers()
@@ -411,13 +455,13 @@ def run_reference(a, rank, world):
     dt = time.perf_counter() - t0
     pts = cfg.nx * cfg.ny * cfg.nz
     v = pts * a.steps / dt
-    big = scenario.AT_SCALE
+    big = cfg
     out = {'metric': METRIC, 'value': v, 'unit': METRIC, 'n_gpus': world, 'steps': a.steps, 'warmup': a.warmup,
            'ms_per_step': dt / a.steps * 1e3, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
            'dtype': 'f32', 'data': 'synthetic', 'impl': 'reference',
-           'config': dict(big.as_dict(), sample='64x64x80 horizontal sub-domain, same dx/dz/dt/nsound'),
+           'config': dict(big.as_dict(), grid_points=pts),
            'cpu_baseline': {'value': v, 'unit': METRIC, 'cores': os.cpu_count(), 'kind': kind,
-                            'sample': 'each step = one large step of a 64x64x80 sub-domain of the 256x256x80 workload'},
+                            'sample': 'each step = one large step of the 256x256x80 workload on all host cores'},
            'e2e': {'value': v, 'unit': METRIC, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
     print(json.dumps(out))
 

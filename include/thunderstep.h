@@ -33,11 +33,17 @@ extern "C" {
 #define TE_MODE_EXACT 0  /* one CUDA kernel per tape dispatch, reference order */
 #define TE_MODE_FUSED 1  /* recognised step phases run as fused kernels (see te_set_mode) */
 
+/* te_config.flags */
+#define TE_FLAG_DEFER_MISSING 1  /* te_plan accepts tapes naming kernels this library does
+                                    not implement; running such an op fails with
+                                    TE_ENOKERNEL (the reference fails at build(),
+                                    replay.js:240) */
+
 typedef struct te_ctx te_ctx;
 
 typedef struct te_config {
   int device;          /* CUDA device ordinal */
-  int flags;           /* reserved, 0 */
+  int flags;           /* TE_FLAG_* */
   uint64_t reserved[4];
 } te_config;
 
@@ -103,6 +109,18 @@ int te_device_ptr(te_ctx *ctx, uint64_t word_off, void **out);
  * fields are bit-identical to exact mode, the contents of the step's scratch fields
  * (fx, fy, fz, fpk, cA, cB, ...) are not kept.  Hash runs always use exact mode. */
 int te_set_mode(te_ctx *ctx, int mode);
+
+/* Fused-mode plan of the active step (built on first use): segments are runs of exact
+ * ops or fused phases.  kind: 0 = exact ops, 1 = acoustic substep (3 kernels),
+ * 2 = periodic halo fills.  te_run_segment plays one segment (part = -1) or one kernel
+ * of it (part >= 0), for profiling. */
+typedef struct te_segment {
+  int kind;
+  int first_op, last_op;
+  int kernels;
+} te_segment;
+int te_fused_segments(te_ctx *ctx, te_segment *out, int max, int *count);
+int te_run_segment(te_ctx *ctx, int seg, int part);
 
 /* Name of op `op` of the active step ("copy" for a blit copy), or NULL. */
 const char *te_op_name(te_ctx *ctx, int op);

@@ -305,6 +305,9 @@ class CpuPlayer:
             self.write_words(e['offs'][i], unb64(c['data']))
         self.ops = e['ops']
 
+    def clear_hashes(self):
+        self.hashes[:] = 0
+
     # ---- execution
     def run(self, kernels, nsteps=1, with_hashes=False, last_op=None, ops=None, on_op=None):
         """Execute the planned ops. ``kernels``: callable name -> fn(M, ARG)."""
@@ -319,8 +322,11 @@ class CpuPlayer:
                 else:
                     kernels(o.name)(mp, o.arg.ctypes.data_as(ctypes.c_void_p))
                     if with_hashes:
+                        # slots accumulate across runs like the reference's atomicAdd
+                        # into H, which is never cleared (replay.js:199, UTIL_WGSL)
                         for slot, off, ln in o.hashes:
-                            self.hashes[slot] = 0 if off is None else region_hash(self.M[off:off + ln])
+                            if off is not None:
+                                self.hashes[slot] = (int(self.hashes[slot]) + region_hash(self.M[off:off + ln])) & 0xFFFFFFFF
                 if on_op is not None:
                     on_op(oi, o)
 

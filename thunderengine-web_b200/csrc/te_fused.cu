@@ -1,22 +1,578 @@
-// Fused step phases (TE_MODE_FUSED).  Segments not recognised run the exact kernels.
+// Fused step phases (TE_MODE_FUSED) for sm_100a.
+//
+// The planner scans a step's op list for phases it can run as fewer, larger kernels
+// whose results are bit-identical on every field the step keeps; everything else runs
+// the exact per-dispatch kernels.  Recognised phases:
+//
+//  * acoustic substep (timestep.js:1997-2060): acoustic_uv, acoustic_fpk,
+//    acoustic_w_solve, acoustic_pp, halo(ppd), acoustic_accumulate, halo(u, v, w)
+//    -> K1 (u/v update + u/v accumulation), K2 (pi' forcing + implicit w solve + pi'
+//       update + w accumulation, 32-column tiles staged in shared memory), K3 (the
+//       four halo fills, with the w accumulation of the halo points).
+//  * runs of periodic halo fills (bc_periodic_x then bc_periodic_y per field)
+//    -> one launch for up to four fields.
+//
+// Contract: every field that is not step scratch (fpk, cA, cB are not written in fused
+// mode) ends bit-identical to the exact sequence.  Arithmetic per point is the
+// same sequence of binary32 operations as te_kernels.cu.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/thunderstep.h"
 #include "te_fused.cuh"
+#include "te_math.cuh"
 #include "te_player.hpp"
 
 namespace te {
 
+// ------------------------------------------------------------ acoustic K1
+
+struct AcuArgs {
+  Dims g;
+  Acoustic a;
+  const float *ppd, *thv, *uten, *vten, *hm;
+  float *u, *v, *w, *rru, *rrv, *rrw;
+  const float *piadv, *ppten, *ppterm, *pk1, *pk2, *qk, *mm, *wten;
+  float *pp3d, *ppdw, *ppx, *cA, *cB, *sbuf;
+  float tavg;
+  int saveX;
+};
+
+// u, v at (i, j, k) after acoustic_uv (acoustic_uv.wgsl:145-181); a point outside the
+// update range keeps its value.
+__device__ __forceinline__ float uv_u(const AcuArgs& A, int i, int j, int c) {
+  const Dims& g = A.g;
+  const float tem1 = (g.rdx * 1005.7f) * 0.5f;
+  return fmaf(A.a.dts, fmaf(-((tem1 * (A.ppd[c] - A.ppd[c - 1])) * hm_uf(g, A.hm, i)), A.thv[c] + A.thv[c - 1], A.uten[c]),
+              A.u[c]);
+}
+__device__ __forceinline__ float uv_v(const AcuArgs& A, int i, int j, int c) {
+  const Dims& g = A.g;
+  const float tem2 = (g.rdy * 1005.7f) * 0.5f;
+  const int sj = g.sJ;
+  return fmaf(A.a.dts, fmaf(-((tem2 * (A.ppd[c] - A.ppd[c - sj])) * hm_vf(g, A.hm, j)), A.thv[c] + A.thv[c - sj], A.vten[c]),
+              A.v[c]);
+}
+
+// K1: every point of the field (halos and k = nz included, as acoustic_accumulate):
+// u, v updated where acoustic_uv updates them, then rru += u, rrv += v (averaged on the
+// last substep, acoustic_accumulate.wgsl:129-158).
+__global__ void __launch_bounds__(256) k_acu_uv(AcuArgs A) {
+  const Dims& g = A.g;
+  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x) - 3;
+  const int j = (int)(blockIdx.y * blockDim.y + threadIdx.y) - 3;
+  const int k = blockIdx.z;
+  if (i > g.nx + 3 || j > g.ny + 3 || k > g.nz) return;
+  const int c = gidx(g, i, j, k);
+  float un = A.u[c], vn = A.v[c];
+  if (i >= 0 && j >= 0 && i <= g.nx && j <= g.ny && k < g.nz) {
+    un = uv_u(A, i, j, c);
+    vn = uv_v(A, i, j, c);
+    A.u[c] = un;
+    A.v[c] = vn;
+  }
+  if (A.tavg > 0.0f) {
+    A.rru[c] = (A.rru[c] + un) * A.tavg;
+    A.rrv[c] = (A.rrv[c] + vn) * A.tavg;
+  } else {
+    A.rru[c] = A.rru[c] + un;
+    A.rrv[c] = A.rrv[c] + vn;
+  }
+}
+
+// ------------------------------------------------------------ acoustic K2
+
+// Explicit pi' forcing at an interior point (acoustic_fpk.wgsl:167-207).
+__device__ __forceinline__ float fpk_at(const AcuArgs& A, int i, int j, int c, const float* w_old) {
+  const Dims& g = A.g;
+  const Acoustic& a = A.a;
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  const float temx = (a.dts * 0.5f) * g.rdx;
+  const float temy = (a.dts * 0.5f) * g.rdy;
+  const float *u = A.u, *v = A.v, *piadv = A.piadv;
+  float div = fmaf((u[c + 1] - u[c]) * g.rdx, hm_uh(g, A.hm, i), ((v[c + sj] - v[c]) * g.rdy) * hm_vh(g, A.hm, j));
+  if (fabsf(div) < a.smeps) div = 0.0f;
+  float advPi = fmaf((-fmaf(u[c], piadv[c] - piadv[c - 1], u[c + 1] * (piadv[c + 1] - piadv[c]))) * temx, hm_uh(g, A.hm, i),
+                     -((fmaf(v[c], piadv[c] - piadv[c - sj], v[c + sj] * (piadv[c + sj] - piadv[c])) * temy) * hm_vh(g, A.hm, j)));
+  return fmaf(a.beta, fmaf(w_old[c], A.pk1[c] + A.qk[c], w_old[c + sk] * (A.pk2[c] - A.qk[c])),
+              fmaf(a.dts, fmaf(-A.ppterm[c], div, A.ppten[c]), advPi));
+}
+
+// K2: a CTA owns 32 interior columns (i0..i0+31, row j).  256 threads = 32 columns x
+// 8 level slots.  Per pass of 8 levels:
+//   A1 (all threads) load one level each: fpk (acoustic_fpk.wgsl:167-207) and the
+//      pointwise terms of the w-pi' system, kept in shared memory;
+//   A2 (all threads) the tridiagonal coefficients aa, bb, cc, dd of their level
+//      (lam_1, acoustic_w_solve.wgsl:124-139);
+//   B  (warp 0, one lane per column) the Thomas forward recurrence, sequential in k.
+// Then warp 0 back-substitutes w, and all threads apply the pi' update
+// (acoustic_pp.wgsl:131-167), store w and accumulate rrw (acoustic_accumulate.wgsl) for
+// levels 0..nz.  Every value is produced by the same binary32 operations as the
+// per-dispatch kernels; sums the reference forms twice (pk1+qk, pp3d+fpk, ...) are
+// formed once here with the same rounding.
+constexpr int kColTile = 32;
+constexpr int kLevels = 16;
+
+struct ColSmem {
+  float *cA, *cB, *A, *Bq, *s, *prev;           // [nz][32] persistent
+  float *m, *wt, *wold, *aa, *bb, *cc, *dd;     // [kLevels][32] per pass
+};
+
+__device__ __forceinline__ ColSmem col_smem(float* base, int nz) {
+  ColSmem S;
+  const int P = nz * kColTile, T = kLevels * kColTile;
+  S.cA = base;
+  S.cB = base + P;
+  S.A = base + 2 * P;
+  S.Bq = base + 3 * P;
+  S.s = base + 4 * P;
+  S.prev = base + 5 * P;
+  float* t = base + 6 * P;
+  S.m = t;
+  S.wt = t + T;
+  S.wold = t + 2 * T;
+  S.aa = t + 3 * T;
+  S.bb = t + 4 * T;
+  S.cc = t + 5 * T;
+  S.dd = t + 6 * T;
+  return S;
+}
+
+static size_t col_smem_bytes(int nz) { return (size_t)(6 * nz + 7 * kLevels) * kColTile * sizeof(float); }
+
+// The 19 inputs of one level of one column, loaded ahead of use.
+struct LevelIn {
+  float u0, u1, v0, v1, pa0, paw, pae, pas, pan, ppten, ppterm, pk1, pk2, qk, w0, w1, pp, mm, wt;
+};
+
+__device__ __forceinline__ LevelIn load_level(const AcuArgs& A, int c) {
+  const int sj = A.g.sJ, sk = A.g.sJ * A.g.sK;
+  LevelIn L;
+  L.u0 = A.u[c];
+  L.u1 = A.u[c + 1];
+  L.v0 = A.v[c];
+  L.v1 = A.v[c + sj];
+  L.pa0 = __ldg(A.piadv + c);
+  L.paw = __ldg(A.piadv + c - 1);
+  L.pae = __ldg(A.piadv + c + 1);
+  L.pas = __ldg(A.piadv + c - sj);
+  L.pan = __ldg(A.piadv + c + sj);
+  L.ppten = __ldg(A.ppten + c);
+  L.ppterm = __ldg(A.ppterm + c);
+  L.pk1 = __ldg(A.pk1 + c);
+  L.pk2 = __ldg(A.pk2 + c);
+  L.qk = __ldg(A.qk + c);
+  L.w0 = A.w[c];
+  L.w1 = A.w[c + sk];
+  L.pp = A.pp3d[c];
+  L.mm = __ldg(A.mm + c);
+  L.wt = __ldg(A.wten + c);
+  return L;
+}
+
+// fpk from loaded values: the operations of acoustic_fpk.wgsl:167-207 in their order
+__device__ __forceinline__ float fpk_of(const AcuArgs& A, const LevelIn& L, float uh, float vh) {
+  const Dims& g = A.g;
+  const Acoustic& a = A.a;
+  const float temx = (a.dts * 0.5f) * g.rdx;
+  const float temy = (a.dts * 0.5f) * g.rdy;
+  float div = fmaf((L.u1 - L.u0) * g.rdx, uh, ((L.v1 - L.v0) * g.rdy) * vh);
+  if (fabsf(div) < a.smeps) div = 0.0f;
+  float advPi = fmaf((-fmaf(L.u0, L.pa0 - L.paw, L.u1 * (L.pae - L.pa0))) * temx, uh,
+                     -((fmaf(L.v0, L.pa0 - L.pas, L.v1 * (L.pan - L.pa0)) * temy) * vh));
+  return fmaf(a.beta, fmaf(L.w0, L.pk1 + L.qk, L.w1 * (L.pk2 - L.qk)), fmaf(a.dts, fmaf(-L.ppterm, div, L.ppten), advPi));
+}
+
+__global__ void __launch_bounds__(kColTile * kLevels, 2) k_acu_column(AcuArgs A) {
+  extern __shared__ float smem[];
+  const Dims& g = A.g;
+  const Acoustic& a = A.a;
+  const int nz = g.nz;
+  const ColSmem S = col_smem(smem, nz);
+  const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
+  const int i = blockIdx.x * kColTile + lane;
+  const int j = blockIdx.y;
+  const bool col = i < g.nx;
+  const int sk = g.sJ * g.sK;
+  const int c0 = gidx(g, col ? i : 0, j, 0);
+  const float uh = hm_uh(g, A.hm, col ? i : 0), vh = hm_vh(g, A.hm, j);
+  const float asq = a.alph * a.alph;
+  float cAm = 0.0f, cBm = 0.0f, wtop = 0.0f;  // warp 0 lanes: recurrence state
+  LevelIn cur;
+  if (col && q < nz) cur = load_level(A, c0 + q * sk);
+  for (int k0 = 0; k0 < nz; k0 += kLevels) {
+    const int k = k0 + q;
+    const int t = q * kColTile + lane;
+    // issue the next pass's loads before this pass's barriers and recurrence
+    LevelIn nxt;
+    if (col && k + kLevels < nz) nxt = load_level(A, c0 + (k + kLevels) * sk);
+    if (col && k < nz) {
+      const float fk = fpk_of(A, cur, uh, vh);
+      const int e = k * kColTile + lane;
+      S.A[e] = cur.pk1 + cur.qk;
+      S.Bq[e] = cur.pk2 - cur.qk;
+      S.prev[e] = cur.pp;
+      S.s[e] = cur.pp + fk;
+      S.m[t] = cur.mm;
+      S.wt[t] = cur.wt;
+      S.wold[t] = cur.w0;
+    }
+    __syncthreads();
+    if (col && k < nz && k >= 1) {
+      const int e = k * kColTile + lane, em = e - kColTile;
+      const float m = S.m[t];
+      S.aa[t] = (-asq) * (m * S.A[em]);
+      S.cc[t] = (-asq) * ((-m) * S.Bq[e]);
+      S.bb[t] = fmaf(-asq, m * ((-S.A[e]) + S.Bq[em]), 1.0f);
+      const float fw = fmaf(a.dts, S.wt[t], a.beta * ((-m) * (S.prev[e] - S.prev[em])));
+      S.dd[t] = fmaf(a.alph, (-m) * (S.s[e] - S.s[em]), S.wold[t] + fw);
+    }
+    __syncthreads();
+    if (q == 0 && col) {
+      for (int qq = 0; qq < kLevels; qq++) {
+        const int kk = k0 + qq;
+        if (kk >= nz) break;
+        if (kk == 0) continue;
+        const int tt = qq * kColTile + lane, e = kk * kColTile + lane;
+        const float aa = S.aa[tt], bb = S.bb[tt], cc = S.cc[tt], dd = S.dd[tt];
+        if (kk == 1) {
+          const float r = dcr(1.0f, bb);
+          cAm = (-cc) * r;
+          cBm = dd * r;
+          S.cA[e] = cAm;
+          S.cB[e] = cBm;
+        } else if (kk < nz - 1) {
+          const float r = dcr(1.0f, fmaf(aa, cAm, bb));
+          const float cAk = (-cc) * r;
+          const float cBk = fmaf(-aa, cBm, dd) * r;
+          cAm = cAk;
+          cBm = cBk;
+          S.cA[e] = cAk;
+          S.cB[e] = cBk;
+        } else {
+          const float r = dcr(1.0f, fmaf(aa, cAm, bb));
+          wtop = fmaf(-aa, cBm, dd) * r;
+        }
+      }
+    }
+    __syncthreads();
+    cur = nxt;
+  }
+  // back substitution (warp 0): w(k) overwrites cA(k); w(0) = w(nz) = 0
+  if (q == 0 && col) {
+    float wk1 = wtop;
+    S.cA[(nz - 1) * kColTile + lane] = wtop;
+    for (int k = nz - 2; k >= 1; k--) {
+      const int e = k * kColTile + lane;
+      const float wk = fmaf(S.cA[e], wk1, S.cB[e]);
+      S.cA[e] = wk;
+      wk1 = wk;
+    }
+    S.cA[lane] = 0.0f;
+  }
+  __syncthreads();
+  if (!col) return;
+  for (int k = q; k <= nz; k += kLevels) {
+    const int c = c0 + k * sk;
+    if (k < nz) {
+      const int e = k * kColTile + lane;
+      const float wk = S.cA[e];
+      const float wk1 = k + 1 < nz ? S.cA[e + kColTile] : 0.0f;
+      float p = fmaf(a.alph, fmaf(wk, S.A[e], wk1 * S.Bq[e]), S.s[e]);
+      if (fabsf(p) < a.smeps) p = 0.0f;
+      A.pp3d[c] = p;
+      const float dum1 = a.kdiv * (p - S.prev[e]);
+      A.ppdw[c] = p + dum1;
+      if (A.saveX != 0) A.ppx[c] = dum1;
+      A.w[c] = wk;
+      A.rrw[c] = A.tavg > 0.0f ? fmaf(wk, a.alph, A.rrw[c]) * A.tavg : A.rrw[c] + wk;
+    } else {
+      A.w[c] = 0.0f;
+      A.rrw[c] = A.tavg > 0.0f ? fmaf(0.0f, a.alph, A.rrw[c]) * A.tavg : A.rrw[c] + 0.0f;
+    }
+  }
+}
+
+static void launch_acu_column(const AcuArgs& A, cudaStream_t s) {
+  static int configured = -1;
+  const size_t bytes = col_smem_bytes(A.g.nz);
+  if ((int)bytes > configured) {
+    cudaFuncSetAttribute(k_acu_column, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    configured = (int)bytes;
+  }
+  dim3 b(kColTile * kLevels), gr((A.g.nx + kColTile - 1) / kColTile, A.g.ny);
+  k_acu_column<<<gr, b, bytes, s>>>(A);
+}
+
+// ------------------------------------------------------------ periodic halos
+
+struct HaloArgs {
+  Dims g;
+  float* f[4];
+  int nf;
+  // acoustic substep: before the fill, halo points accumulate w into rrw
+  // (acoustic_accumulate covers halos with the values they hold before the fill)
+  float* acc_w;
+  float* acc_rrw;
+  float tavg, alph;
+};
+
+// Final state of bc_periodic_x followed by bc_periodic_y (bc_periodic_x.wgsl,
+// bc_periodic_y.wgsl): every halo point of levels 0..nz holds the interior value at
+// (i mod nx, j mod ny).  One thread per halo point and level: the 7 x-halo columns
+// over all rows, then the 7 y-halo rows over the interior columns.
+__global__ void k_halo_periodic(HaloArgs H) {
+  const Dims& g = H.g;
+  const int per_level = 7 * g.sK + 7 * g.nx;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y;
+  if (t >= per_level || k > g.nz) return;
+  int i, j;
+  if (t < 7 * g.sK) {
+    const int col = t / g.sK;  // 0..6 -> i = -3,-2,-1, nx, nx+1, nx+2, nx+3
+    j = t % g.sK - 3;
+    i = col < 3 ? col - 3 : g.nx + (col - 3);
+  } else {
+    const int r = t - 7 * g.sK;
+    const int row = r / g.nx;
+    i = r % g.nx;
+    j = row < 3 ? row - 3 : g.ny + (row - 3);
+  }
+  const int ii = ((i % g.nx) + g.nx) % g.nx;
+  const int jj = ((j % g.ny) + g.ny) % g.ny;
+  const int dst = gidx(g, i, j, k), src = gidx(g, ii, jj, k);
+  if (H.acc_rrw) {
+    const float wv = H.acc_w[dst];
+    H.acc_rrw[dst] = H.tavg > 0.0f ? fmaf(wv, H.alph, H.acc_rrw[dst]) * H.tavg : H.acc_rrw[dst] + wv;
+  }
+  for (int q = 0; q < H.nf; q++) H.f[q][dst] = H.f[q][src];
+}
+
+static void launch_halo(const HaloArgs& H, cudaStream_t s) {
+  const int per_level = 7 * H.g.sK + 7 * H.g.nx;
+  dim3 b(256), gr((per_level + 255) / 256, H.g.nz + 1);
+  k_halo_periodic<<<gr, b, 0, s>>>(H);
+}
+
+// ------------------------------------------------------------ planner
+
+enum SegKind { kExact = 0, kAcoustic = 1, kHalo = 2 };
+
+static bool is_name(const Op& o, const char* n) { return !o.copy && o.name == n; }
+
+static bool same_dims(const Dims& a, const Dims& b) {
+  return a.nx == b.nx && a.ny == b.ny && a.nz == b.nz && a.sJ == b.sJ && a.sK == b.sK && a.rdx == b.rdx &&
+         a.rdy == b.rdy && a.rdz == b.rdz;
+}
+static bool same_acoustic(const Acoustic& a, const Acoustic& b) {
+  return a.dts == b.dts && a.alph == b.alph && a.beta == b.beta && a.kdiv == b.kdiv && a.smeps == b.smeps;
+}
+
+// bc_periodic_x(f) followed by bc_periodic_y(f) over the standard halo grid
+static bool halo_pair(const std::vector<Op>& ops, size_t i, float** f) {
+  if (i + 1 >= ops.size()) return false;
+  const Op &x = ops[i], &y = ops[i + 1];
+  if (!is_name(x, "bc_periodic_x") || !is_name(y, "bc_periodic_y")) return false;
+  const Dims& g = x.args.g;
+  if (!same_dims(g, y.args.g) || x.args.p[1] != y.args.p[1]) return false;
+  if (x.grid[0] != 4 || x.grid[1] != g.ny + 7 || x.grid[2] != g.nz + 1) return false;
+  if (y.grid[0] != 4 || y.grid[1] != g.nx + 7 || y.grid[2] != g.nz + 1) return false;
+  *f = x.args.p[1];
+  return true;
+}
+
+static const char* kSubstep[] = {"acoustic_uv", "acoustic_fpk", "acoustic_w_solve", "acoustic_pp"};
+
+static bool match_substep(const std::vector<Op>& ops, size_t i, FusedSegment& s, AcuArgs& A) {
+  if (i + 13 > ops.size()) return false;
+  for (int q = 0; q < 4; q++)
+    if (!is_name(ops[i + q], kSubstep[q])) return false;
+  const Op &uv = ops[i], &fp = ops[i + 1], &ws = ops[i + 2], &pp = ops[i + 3];
+  const Op& acc = ops[i + 6];
+  if (!is_name(acc, "acoustic_accumulate")) return false;
+  const Dims& g = uv.args.g;
+  if (g.nx < 1 || g.ny < 1 || g.nz < 3 || col_smem_bytes(g.nz) > 110 * 1024) return false;
+  for (const Op* o : {&fp, &ws, &pp, &acc})
+    if (!same_dims(g, o->args.g) || !same_acoustic(uv.args.a, o->args.a)) return false;
+  // periodic (closed) lateral boundaries only
+  if (uv.args.iv[8] != 0 || uv.args.iv2[8] != 0) return false;
+  // dispatch grids as the encoder emits them
+  if (uv.grid[0] != g.nx + 1 || uv.grid[1] != g.ny + 1 || uv.grid[2] != g.nz) return false;
+  for (const Op* o : {&fp, &pp})
+    if (o->grid[0] != g.nx || o->grid[1] != g.ny || o->grid[2] != g.nz) return false;
+  if (ws.grid[0] != g.nx || ws.grid[1] != g.ny || ws.grid[2] != 1) return false;
+  if (acc.grid[0] != g.sJ || acc.grid[1] != g.sK || acc.grid[2] != g.nz + 1) return false;
+  // bindings: one set of fields across the seven kernels
+  float *ppd = uv.args.p[2], *u = uv.args.p[6], *v = uv.args.p[7];
+  float* w = fp.args.p[4];
+  float *pk1 = fp.args.p[8], *pk2 = fp.args.p[9], *qk = fp.args.p[10], *fpk = fp.args.p[11];
+  bool ok = fp.args.p[2] == u && fp.args.p[3] == v && ws.args.p[2] == pk1 && ws.args.p[3] == pk2 && ws.args.p[4] == qk &&
+            ws.args.p[6] == fpk && ws.args.p[9] == w && pp.args.p[2] == w && pp.args.p[3] == pk1 && pp.args.p[4] == pk2 &&
+            pp.args.p[5] == qk && pp.args.p[6] == fpk && pp.args.p[7] == ws.args.p[8] && pp.args.p[8] == ppd &&
+            acc.args.p[2] == u && acc.args.p[3] == v && acc.args.p[4] == w && uv.args.p[30] == fp.args.p[30];
+  if (!ok) return false;
+  // halo fills: ppd after pp, then u, v, w after the accumulation
+  float* f;
+  if (!halo_pair(ops, i + 4, &f) || f != ppd) return false;
+  const float* want[3] = {u, v, w};
+  for (int q = 0; q < 3; q++)
+    if (!halo_pair(ops, i + 7 + 2 * q, &f) || f != want[q]) return false;
+  // the three fields K2 uses for its intermediate values must be distinct scratch
+  float *cA = ws.args.p[10], *cB = ws.args.p[11];
+  if (cA == cB || cA == fpk || cB == fpk) return false;
+  for (float* p : {ppd, u, v, w, pk1, pk2, qk, acc.args.p[5], acc.args.p[6], acc.args.p[7], pp.args.p[7], pp.args.p[9],
+                   fp.args.p[5], fp.args.p[6], fp.args.p[7], ws.args.p[5], ws.args.p[7], uv.args.p[3], uv.args.p[4],
+                   uv.args.p[5]})
+    if (p == cA || p == cB || p == fpk) return false;
+  std::memset(&A, 0, sizeof(A));
+  A.g = g;
+  A.a = uv.args.a;
+  A.ppd = ppd;
+  A.thv = uv.args.p[3];
+  A.uten = uv.args.p[4];
+  A.vten = uv.args.p[5];
+  A.hm = uv.args.p[30];
+  A.u = u;
+  A.v = v;
+  A.w = w;
+  A.piadv = fp.args.p[5];
+  A.ppten = fp.args.p[6];
+  A.ppterm = fp.args.p[7];
+  A.pk1 = pk1;
+  A.pk2 = pk2;
+  A.qk = qk;
+  A.mm = ws.args.p[5];
+  A.wten = ws.args.p[7];
+  A.pp3d = ws.args.p[8];
+  A.ppdw = ppd;
+  A.ppx = pp.args.p[9];
+  A.saveX = pp.args.iv[10];
+  A.cA = cA;
+  A.cB = cB;
+  A.sbuf = fpk;
+  A.rru = acc.args.p[5];
+  A.rrv = acc.args.p[6];
+  A.rrw = acc.args.p[7];
+  A.tavg = acc.args.f[8];
+  s.kind = kAcoustic;
+  s.first = (int)i;
+  s.last = (int)i + 12;
+  return true;
+}
+
+struct FusedData {
+  std::vector<AcuArgs> acu;
+  std::vector<HaloArgs> halo;
+};
+
 void FusedStep::build(Plan& P, std::vector<Op>& ops) {
   segs.clear();
-  FusedSegment s;
-  s.kind = 0;
-  s.first = 0;
-  s.last = (int)ops.size() - 1;
-  segs.push_back(s);
+  if (!data) data = new FusedData();
+  FusedData& D = *static_cast<FusedData*>(data);
+  D.acu.clear();
+  D.halo.clear();
+  size_t i = 0;
+  auto exact_to = [&](size_t e) {
+    if (!segs.empty() && segs.back().kind == kExact && segs.back().last + 1 == (int)i) segs.back().last = (int)e;
+    else {
+      FusedSegment s;
+      s.kind = kExact;
+      s.first = (int)i;
+      s.last = (int)e;
+      segs.push_back(s);
+    }
+  };
+  while (i < ops.size()) {
+    FusedSegment s;
+    AcuArgs A;
+    if (match_substep(ops, i, s, A)) {
+      s.aux[0] = (int)D.acu.size();
+      D.acu.push_back(A);
+      segs.push_back(s);
+      i += 13;
+      continue;
+    }
+    float* f;
+    if (halo_pair(ops, i, &f)) {
+      HaloArgs H;
+      std::memset(&H, 0, sizeof(H));
+      H.g = ops[i].args.g;
+      H.f[0] = f;
+      H.nf = 1;
+      size_t e = i + 2;
+      float* f2;
+      while (H.nf < 4 && halo_pair(ops, e, &f2) && same_dims(H.g, ops[e].args.g)) {
+        bool dup = false;
+        for (int q = 0; q < H.nf; q++) dup |= H.f[q] == f2;
+        if (dup) break;
+        H.f[H.nf++] = f2;
+        e += 2;
+      }
+      s.kind = kHalo;
+      s.first = (int)i;
+      s.last = (int)e - 1;
+      s.aux[0] = (int)D.halo.size();
+      D.halo.push_back(H);
+      segs.push_back(s);
+      i = e;
+      continue;
+    }
+    exact_to(i);
+    i++;
+  }
 }
 
 void FusedStep::launch(Plan& P, std::vector<Op>& ops) {
-  for (auto& s : segs) {
-    if (s.kind == 0) P.launch_exact(ops, s.first, s.last, false);
+  for (int q = 0; q < (int)segs.size(); q++) launch_segment(P, ops, q, -1);
+}
+
+void FusedStep::launch_segment(Plan& P, std::vector<Op>& ops, int seg, int part) {
+  FusedData& D = *static_cast<FusedData*>(data);
+  const FusedSegment& s = segs.at(seg);
+  if (s.kind == kExact) {
+    P.launch_exact(ops, s.first, s.last, false);
+  } else if (s.kind == kHalo) {
+    launch_halo(D.halo[s.aux[0]], P.stream);
+  } else {
+    const AcuArgs& A = D.acu[s.aux[0]];
+    const Dims& g = A.g;
+    if (part < 0 || part == 0) {
+      dim3 b(32, 8, 1), gr((g.sJ + 31) / 32, (g.sK + 7) / 8, g.nz + 1);
+      k_acu_uv<<<gr, b, 0, P.stream>>>(A);
+    }
+    if (part < 0 || part == 1) launch_acu_column(A, P.stream);
+    if (part < 0 || part == 2) {
+      HaloArgs H;
+      std::memset(&H, 0, sizeof(H));
+      H.g = g;
+      H.f[0] = A.ppdw;
+      H.f[1] = A.u;
+      H.f[2] = A.v;
+      H.f[3] = A.w;
+      H.nf = 4;
+      H.acc_w = A.w;
+      H.acc_rrw = A.rrw;
+      H.tavg = A.tavg;
+      H.alph = A.a.alph;
+      launch_halo(H, P.stream);
+    }
   }
+}
+
+int FusedStep::launches_per_step() const {
+  if (!data) return 0;
+  int n = 0;
+  for (auto& s : segs) n += s.kind == kExact ? 0 : (s.kind == kAcoustic ? 3 : 1);
+  return n;
+}
+
+void FusedStep::release() {
+  segs.clear();
+  delete static_cast<FusedData*>(data);
+  data = nullptr;
 }
 
 }  // namespace te

@@ -19,9 +19,13 @@ struct FusedSegment {
 
 struct FusedStep {
   std::vector<FusedSegment> segs;
+  void* data = nullptr;  // kernel arguments of the fused segments
   void build(Plan& P, std::vector<Op>& ops);
   void launch(Plan& P, std::vector<Op>& ops);
-  void release() { segs.clear(); }
+  // one segment; part = -1 for all of its kernels, else the index of one of them
+  void launch_segment(Plan& P, std::vector<Op>& ops, int seg, int part);
+  int launches_per_step() const;
+  void release();
 };
 
 }  // namespace te

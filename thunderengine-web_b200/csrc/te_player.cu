@@ -186,7 +186,7 @@ std::vector<Op> Plan::build_ops(const JValue& cmds, const std::map<int, uint64_t
       auto km = kmeta.find(pipe);
       if (km == kmeta.end()) throw ApiError(TE_ENOKERNEL, "no kernel " + pipe);
       const KernelSpec* spec = find_kernel(pipe.c_str());
-      if (!spec) throw ApiError(TE_ENOKERNEL, "no CUDA kernel for " + pipe);
+      if (!spec && !(flags & TE_FLAG_DEFER_MISSING)) throw ApiError(TE_ENOKERNEL, "no CUDA kernel for " + pipe);
       if (c.get("kind") && c.at("kind").str != "threads")
         throw ApiError(TE_EINVAL, "dispatch kind " + c.at("kind").str + " not supported");
       Op o;
@@ -268,7 +268,7 @@ void Plan::plan(const char* tj, size_t tl, bool with_hashes_) {
 
 void Plan::finalize_args(std::vector<Op>& ops) {
   for (Op& o : ops) {
-    if (o.copy) continue;
+    if (o.copy || !o.spec) continue;
     KArgs& A = o.args;
     std::memset(&A, 0, sizeof(A));
     A.gx = o.grid[0];
@@ -298,6 +298,15 @@ void Plan::finalize_args(std::vector<Op>& ops) {
     A.g.rdx = fl(gd + 5);
     A.g.rdy = fl(gd + 6);
     A.g.rdz = fl(gd + 7);
+    // host-side bounds check of the grid every kernel indexes with (int32 field indices)
+    {
+      const Dims& g = A.g;
+      bool ok = g.nx >= 1 && g.ny >= 1 && g.nz >= 1 && g.nx < (1 << 20) && g.ny < (1 << 20) && g.nz < (1 << 20) &&
+                g.sJ >= g.nx + 7 && g.sK >= g.ny + 7;
+      uint64_t count = ok ? (uint64_t)g.sJ * g.sK * (g.nz + 1) : 0;
+      ok = ok && count < (1ull << 31) && (field_stride == 0 || count * 4 <= field_stride);
+      if (!ok) throw ApiError(TE_EINVAL, o.name + ": GridDims out of range or larger than the arena field stride");
+    }
     if (o.spec->acoustic) {
       auto it1 = o.bind.find(1);
       if (it1 == o.bind.end()) throw ApiError(TE_EINVAL, o.name + ": AcousticParams (binding 1) not bound");
@@ -313,7 +322,7 @@ void Plan::finalize_args(std::vector<Op>& ops) {
       auto it = o.bind.find(ps.index);
       if (ps.kind == kPtr) {
         if (it != o.bind.end()) {
-          if (it->second >= mem_words) throw ApiError(TE_ERANGE, o.name + ": binding outside memory");
+          if (it->second >= buffers_end) throw ApiError(TE_ERANGE, o.name + ": pointer binding outside the tape buffers");
           A.p[ps.index] = reinterpret_cast<float*>(M + it->second);
         }
       } else if (ps.index >= 1 && !(ps.index == 1 && o.spec->acoustic)) {
@@ -363,6 +372,7 @@ int te_create(const te_config* cfg, te_ctx** out) {
     return TE_ECUDA;
   }
   ctx->plan.stream = ctx->stream;
+  ctx->plan.flags = cfg ? cfg->flags : 0;
   *out = ctx;
   return TE_OK;
 }
@@ -565,6 +575,43 @@ int te_set_mode(te_ctx* ctx, int mode) {
   API_END(ctx)
 }
 
+int te_fused_segments(te_ctx* ctx, te_segment* out, int max, int* count) {
+  API_BEGIN(ctx)
+  require_plan(ctx);
+  te::Plan& P = ctx->plan;
+  if (P.fused_dirty || P.fused.segs.empty()) {
+    P.fused.build(P, P.active->ops);
+    P.fused_dirty = false;
+  }
+  int n = (int)P.fused.segs.size();
+  if (count) *count = n;
+  for (int i = 0; i < n && i < max && out; i++) {
+    const te::FusedSegment& s = P.fused.segs[i];
+    out[i].kind = s.kind;
+    out[i].first_op = s.first;
+    out[i].last_op = s.last;
+    out[i].kernels = s.kind == 0 ? 0 : (s.kind == 1 ? 3 : 1);
+    if (s.kind == 0)
+      for (int q = s.first; q <= s.last; q++) out[i].kernels += P.active->ops[q].copy ? 0 : 1;
+  }
+  API_END(ctx)
+}
+
+int te_run_segment(te_ctx* ctx, int seg, int part) {
+  API_BEGIN(ctx)
+  require_plan(ctx);
+  CU(cudaSetDevice(ctx->device));
+  te::Plan& P = ctx->plan;
+  if (P.fused_dirty || P.fused.segs.empty()) {
+    P.fused.build(P, P.active->ops);
+    P.fused_dirty = false;
+  }
+  if (seg < 0 || seg >= (int)P.fused.segs.size()) throw te::ApiError(TE_EINVAL, "segment out of range");
+  P.fused.launch_segment(P, P.active->ops, seg, part);
+  CU(cudaGetLastError());
+  API_END(ctx)
+}
+
 const char* te_op_name(te_ctx* ctx, int op) {
   if (!ctx || !ctx->plan.active || op < 0 || op >= (int)ctx->plan.active->ops.size()) return nullptr;
   return ctx->plan.active->ops[op].name.c_str();
@@ -645,6 +692,7 @@ void Plan::launch_exact(std::vector<Op>& ops, int first, int last, bool hashes) 
       CU(cudaMemcpyAsync(M + o.dst, M + o.src, o.n * 4, cudaMemcpyDeviceToDevice, stream));
       continue;
     }
+    if (!o.spec) throw ApiError(TE_ENOKERNEL, "no CUDA kernel for " + o.name);
     o.spec->launch(o.args, stream);
     if (hashes) {
       for (auto& h : o.hashes) {

@@ -55,6 +55,7 @@ struct BufInfo {
 struct Plan {
   cudaStream_t stream = nullptr;
   int mode = 0;
+  int flags = 0;
   // layout (replay.js:46-66)
   std::vector<BufInfo> buffers;
   std::vector<uint64_t> base;
@@ -63,7 +64,7 @@ struct Plan {
   uint32_t hash_count = 0;
   bool with_hashes = false;
   std::vector<std::pair<uint64_t, std::vector<uint8_t>>> bytes_init;
-  std::vector<uint8_t> host_bytes;  // host copy of words [buffers_end, bytes_spare_end)
+  std::vector<uint32_t> host_bytes;  // host copy of words [buffers_end, bytes_spare_end), word-indexed
   std::map<std::string, KMeta> kmeta;
   std::map<std::string, Step> cache;
   Step* active = nullptr;

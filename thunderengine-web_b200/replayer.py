@@ -32,6 +32,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, 'libthunderstep.so')
 
+TE_FLAG_DEFER_MISSING = 1
 TE_MODE_EXACT = 0
 TE_MODE_FUSED = 1
 
@@ -43,6 +44,11 @@ class TeInfo(ctypes.Structure):
                 ('scratch_base', ctypes.c_uint64), ('hash_count', ctypes.c_uint32),
                 ('num_buffers', ctypes.c_uint32), ('num_ops', ctypes.c_uint32),
                 ('num_dispatches', ctypes.c_uint32)]
+
+
+class TeSegment(ctypes.Structure):
+    _fields_ = [('kind', ctypes.c_int), ('first_op', ctypes.c_int), ('last_op', ctypes.c_int),
+                ('kernels', ctypes.c_int)]
 
 
 class TeConfig(ctypes.Structure):
@@ -73,6 +79,8 @@ EXPORTS = {
     'te_region_hash_host': ([ctypes.c_void_p, ctypes.c_uint64], ctypes.c_uint32),
     'te_set_stream': ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     'te_kernel_table_json': ([ctypes.c_char_p, ctypes.c_size_t], ctypes.c_size_t),
+    'te_fused_segments': ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    'te_run_segment': ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int], ctypes.c_int),
 }
 
 
@@ -103,12 +111,12 @@ def _json_bytes(x):
 class Replayer:
     """Plays a ThunderEngine command tape on one B200 (see the module docstring)."""
 
-    def __init__(self, tape, kernels=None, device=0):
+    def __init__(self, tape, kernels=None, device=0, defer_missing=False):
         self.lib = load_library()
         self.tape = tape
         self.kernels = kernels
         self.device = device
-        cfg = TeConfig(device=device, flags=0)
+        cfg = TeConfig(device=device, flags=TE_FLAG_DEFER_MISSING if defer_missing else 0)
         h = ctypes.c_void_p()
         rc = self.lib.te_create(ctypes.byref(cfg), ctypes.byref(h))
         self.h = h
@@ -216,6 +224,17 @@ class Replayer:
     def set_stream(self, stream_handle):
         """Launch on a caller-owned CUDA stream (int handle; 0 = the context's own)."""
         self._check(self.lib.te_set_stream(self.h, ctypes.c_void_p(int(stream_handle) or None)))
+
+    def fused_segments(self):
+        """Fused-mode segments of the active step: list of (kind, first_op, last_op, kernels)."""
+        n = ctypes.c_int()
+        self._check(self.lib.te_fused_segments(self.h, None, 0, ctypes.byref(n)))
+        arr = (TeSegment * max(n.value, 1))()
+        self._check(self.lib.te_fused_segments(self.h, arr, n.value, ctypes.byref(n)))
+        return [(s.kind, s.first_op, s.last_op, s.kernels) for s in arr[:n.value]]
+
+    def run_segment(self, seg, part=-1):
+        self._check(self.lib.te_run_segment(self.h, int(seg), int(part)))
 
     def sync(self):
         self._check(self.lib.te_sync(self.h))
