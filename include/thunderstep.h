@@ -140,6 +140,33 @@ size_t te_kernel_table_json(char *buf, size_t n);
 /* Region hash of `words` host words with the reference formula (replay.js:407-418). */
 uint32_t te_region_hash_host(const uint32_t *words, uint64_t n);
 
+/* Fields of one vertically implicit w-pi' column solve: device pointers to the start of
+ * each field (index 0 = point (i, j, k) = (-3, -3, 0) of the halo-3 layout, strideJ =
+ * nx + 7, strideK = ny + 7). */
+typedef struct te_wsolve_fields {
+  const float *pk1, *pk2, *qk, *mm, *fpk, *wten, *pp3d;
+  float *w; /* in: w before the solve; out: w after it */
+} te_wsolve_fields;
+
+/* No counterpart in the reference: an addition of this library for callers that cannot
+ * allocate device memory where they run the solve (their pool belongs to another
+ * allocator, or the host process forbids allocation after start-up).  It computes the
+ * same w as the tape kernel acoustic_w_solve (bit for bit) but keeps the Thomas
+ * coefficients, which the tape writes to the arena fields cA and cB, in a fixed 64 MiB
+ * array inside this library; it allocates nothing.
+ *   - Limit: nx * ny * (nz - 2) <= 8,388,608 (256 x 256 columns up to nz = 130); larger
+ *     grids, nz < 3 or a NULL field return TE_ERANGE / TE_EINVAL with a message in `err`
+ *     (`err_len` bytes, may be NULL) and launch nothing.
+ *   - Every GPU that loads the library holds the 64 MiB until the process exits.
+ *   - Runs on the current CUDA device, on `cuda_stream` (NULL = legacy default stream),
+ *     asynchronously.  The first call on a device looks up the array's device address;
+ *     make that first call before any stream capture.
+ *   - Nothing in the array has to start at zero: each column's coefficients are written
+ *     before they are read.  All calls share the array, so calls that may overlap on the
+ *     GPU (different streams, or different host threads) race: order them. */
+int te_w_solve_static_scratch(const te_wsolve_fields *f, int nx, int ny, int nz, float dts, float alph,
+                              float beta, void *cuda_stream, char *err, size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -55,6 +55,11 @@ class TeConfig(ctypes.Structure):
     _fields_ = [('device', ctypes.c_int), ('flags', ctypes.c_int), ('reserved', ctypes.c_uint64 * 4)]
 
 
+class TeWSolveFields(ctypes.Structure):
+    """``te_wsolve_fields``: device pointers of one w-pi' column solve."""
+    _fields_ = [(n, ctypes.c_void_p) for n in ('pk1', 'pk2', 'qk', 'mm', 'fpk', 'wten', 'pp3d', 'w')]
+
+
 EXPORTS = {
     'te_create': ([ctypes.POINTER(TeConfig), ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     'te_plan': ([ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_int],
@@ -81,6 +86,9 @@ EXPORTS = {
     'te_kernel_table_json': ([ctypes.c_char_p, ctypes.c_size_t], ctypes.c_size_t),
     'te_fused_segments': ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     'te_run_segment': ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    'te_w_solve_static_scratch': ([ctypes.POINTER(TeWSolveFields), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_void_p,
+                                   ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
 }
 
 
