@@ -304,6 +304,24 @@ def kernel_roofline(r, run, stream, mode):
             nf = segs[q][2] - segs[q][1] + 1
             stats['halo_periodic (fused)'] = [timed(lambda: r.run_segment(q, -1)), len(halo),
                                               (nf // 2) * 2 * 4 * 7 * (g.strideK + g.nx) * (g.nz + 1)]
+        # fused advection: one kernel per variable and stage, grouped by flux kind; bytes =
+        # the distinct arena fields its ops bind, except the fx/fy/fz fluxes it never
+        # touches, x 4 B x interior points
+        for q, sg in enumerate(segs):
+            if sg[0] != 3:
+                continue
+            name = 'advect %s (fused flux+assemble%s)' % (r.op_name(sg[1]).replace('adv_flux_x', '').strip('_') or 'lin',
+                                                          '+rk' if sg[2] - sg[1] > 3 else '')
+            fields = set()
+            for i in range(sg[1], sg[2] + 1):
+                fields |= {f for f in disp[i]['fields'].values() if f is not None}
+            byts = len(fields - {'fx', 'fy', 'fz'}) * 4 * g.nx * g.ny * g.nz
+            ms = timed(lambda: r.run_segment(q, -1))
+            if name in stats:
+                o = stats[name]
+                stats[name] = [(o[0] * o[1] + ms) / (o[1] + 1), o[1] + 1, (o[2] * o[1] + byts) / (o[1] + 1)]
+            else:
+                stats[name] = [ms, 1, byts]
     else:
         exact_ops = list(range(r.num_ops))
     seen = {}

@@ -112,8 +112,8 @@ int te_set_mode(te_ctx *ctx, int mode);
 
 /* Fused-mode plan of the active step (built on first use): segments are runs of exact
  * ops or fused phases.  kind: 0 = exact ops, 1 = acoustic substep (3 kernels),
- * 2 = periodic halo fills.  te_run_segment plays one segment (part = -1) or one kernel
- * of it (part >= 0), for profiling. */
+ * 2 = periodic halo fills, 3 = advection of one variable (1 kernel).  te_run_segment
+ * plays one segment (part = -1) or one kernel of it (part >= 0), for profiling. */
 typedef struct te_segment {
   int kind;
   int first_op, last_op;

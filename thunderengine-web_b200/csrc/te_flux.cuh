@@ -1,0 +1,336 @@
+// Per-face advective fluxes of the flux kernels (data/kernels/adv_flux_*.wgsl) and the
+// cell assembly of adv_assemble, as device functions shared by the per-dispatch kernels
+// (te_kernels.cu) and the fused advection kernel (te_fused.cu): both run this code, so
+// both produce the same bits.  face_*(A, i, j, k) is the value the reference kernel
+// stores at index (i, j, k) of its output field; A holds that kernel's bindings.
+#pragma once
+#include "te_kernels.cuh"
+#include "te_math.cuh"
+
+namespace te {
+
+// Index box [lo, hi] (inclusive) of faces or cells.
+struct FaceRange {
+  int ilo, ihi, jlo, jhi, klo, khi;
+};
+
+__device__ __forceinline__ float flx5_upwind(const float* a, int c, int s, bool up, bool shifted) {
+  if (shifted) return up ? flx5(a[c - 2 * s], a[c - s], a[c], a[c + s], a[c + 2 * s])
+                         : flx5(a[c + 3 * s], a[c + 2 * s], a[c + s], a[c], a[c - s]);
+  return up ? flx5(a[c - 3 * s], a[c - 2 * s], a[c - s], a[c], a[c + s])
+            : flx5(a[c + 2 * s], a[c + s], a[c], a[c - s], a[c - 2 * s]);
+}
+
+__device__ __forceinline__ float weno5_upwind(const float* a, int c, int s, bool up, bool shifted, float weps) {
+  if (shifted) return up ? weno5(a[c - 2 * s], a[c - s], a[c], a[c + s], a[c + 2 * s], weps)
+                         : weno5(a[c + 3 * s], a[c + 2 * s], a[c + s], a[c], a[c - s], weps);
+  return up ? weno5(a[c - 3 * s], a[c - 2 * s], a[c - s], a[c], a[c + s], weps)
+            : weno5(a[c + 2 * s], a[c + s], a[c], a[c - s], a[c - 2 * s], weps);
+}
+
+template <int DIR>
+__device__ __forceinline__ float face_lin_h(const KArgs& A, int i, int j, int k) {
+  const Dims& g = A.g;
+  const float *s = A.p[1], *rr = A.p[2];
+  int c = gidx(g, i, j, k);
+  const int d = DIR == 0 ? 1 : g.sJ;
+  float u = rr[c];
+  float f = u >= 0.0f ? flx5(s[c - 3 * d], s[c - 2 * d], s[c - d], s[c], s[c + d])
+                      : flx5(s[c + 2 * d], s[c + d], s[c], s[c - d], s[c - 2 * d]);
+  return u * f;
+}
+
+__device__ __forceinline__ float face_lin_z(const KArgs& A, int i, int j, int k) {
+  const Dims& g = A.g;
+  const float *s = A.p[1], *rrw = A.p[2], *c1 = A.p[3], *c2 = A.p[4];
+  const int sk = g.sJ * g.sK;
+  int c = gidx(g, i, j, k);
+  if (k == 0 || k == g.nz) {
+    return 0.0f;
+  }
+  float w = rrw[c];
+  bool up = w >= 0.0f;
+  float f;
+  if (k == 1) f = up ? fmaf(c1[k], s[c - sk], c2[k] * s[c]) : flx3(s[c + sk], s[c], s[c - sk]);
+  else if (k == 2) f = up ? flx3(s[c - 2 * sk], s[c - sk], s[c]) : flx5(s[c + 2 * sk], s[c + sk], s[c], s[c - sk], s[c - 2 * sk]);
+  else if (k == g.nz - 2) f = up ? flx5(s[c - 3 * sk], s[c - 2 * sk], s[c - sk], s[c], s[c + sk]) : flx3(s[c + sk], s[c], s[c - sk]);
+  else if (k == g.nz - 1) f = up ? flx3(s[c - 2 * sk], s[c - sk], s[c]) : fmaf(c1[k], s[c - sk], c2[k] * s[c]);
+  else f = up ? flx5(s[c - 3 * sk], s[c - 2 * sk], s[c - sk], s[c], s[c + sk])
+              : flx5(s[c + 2 * sk], s[c + sk], s[c], s[c - sk], s[c - 2 * sk]);
+  return w * f;
+}
+
+template <int DIR>
+__device__ __forceinline__ float face_stag_h(const KArgs& A, int i, int j, int k) {
+  const Dims& g = A.g;
+  const int stag = A.iv[1];
+  const float *a = A.p[2], *rr = DIR == 0 ? A.p[3] : A.p[4], *c2 = A.p[7];
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  int c = gidx(g, i, j, k);
+  if (stag == 4 && k == 0) {
+    return 0.0f;
+  }
+  float m;
+  if (DIR == 0) {
+    if (stag == 2) m = 0.5f * (rr[c] + rr[c + 1]);
+    else if (stag == 3) m = 0.5f * (rr[c] + rr[c - sj]);
+    else if (stag == 4) { float cc2 = c2[k]; m = fmaf(cc2, rr[c], (1.0f - cc2) * rr[c - sk]); }
+    else m = rr[c];
+    return m * flx5_upwind(a, c, 1, m >= 0.0f, stag == 2);
+  } else {
+    if (stag == 2) m = 0.5f * (rr[c] + rr[c - 1]);
+    else if (stag == 3) m = 0.5f * (rr[c] + rr[c + sj]);
+    else if (stag == 4) { float cc2 = c2[k]; m = fmaf(cc2, rr[c], (1.0f - cc2) * rr[c - sk]); }
+    else m = rr[c];
+    return m * flx5_upwind(a, c, sj, m >= 0.0f, stag == 3);
+  }
+}
+
+__device__ __forceinline__ float face_stag_z(const KArgs& A, int i, int j, int k) {
+  const Dims& g = A.g;
+  const int stag = A.iv[1];
+  const float *a = A.p[2], *rrw = A.p[5], *c1 = A.p[6], *c2 = A.p[7];
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  int c = gidx(g, i, j, k);
+  float m;
+  if (stag == 2) m = 0.5f * (rrw[c] + rrw[c - 1]);
+  else if (stag == 3) m = 0.5f * (rrw[c] + rrw[c - sj]);
+  else m = 0.5f * (rrw[c] + (k < g.nz ? rrw[c + sk] : 0.0f));
+  bool up = m >= 0.0f;
+  float f;
+  if (stag == 4) {
+    if (k > g.nz - 1) {
+      return 0.0f;
+    }
+    if (k == 0) f = up ? 0.5f * (a[c] + a[c + sk]) : flx3(a[c + 2 * sk], a[c + sk], a[c]);
+    else if (k == 1) f = up ? flx3(a[c - sk], a[c], a[c + sk]) : flx5(a[c + 3 * sk], a[c + 2 * sk], a[c + sk], a[c], a[c - sk]);
+    else if (k == g.nz - 2) f = up ? flx5(a[c - 2 * sk], a[c - sk], a[c], a[c + sk], a[c + 2 * sk]) : flx3(a[c + 2 * sk], a[c + sk], a[c]);
+    else if (k == g.nz - 1) f = up ? flx3(a[c - sk], a[c], a[c + sk]) : 0.5f * (a[c] + a[c + sk]);
+    else f = up ? flx5(a[c - 2 * sk], a[c - sk], a[c], a[c + sk], a[c + 2 * sk])
+                : flx5(a[c + 3 * sk], a[c + 2 * sk], a[c + sk], a[c], a[c - sk]);
+  } else {
+    if (k == 0 || k == g.nz) {
+      return 0.0f;
+    }
+    if (k == 1) f = up ? fmaf(c1[k], a[c - sk], c2[k] * a[c]) : flx3(a[c + sk], a[c], a[c - sk]);
+    else if (k == 2) f = up ? flx3(a[c - 2 * sk], a[c - sk], a[c]) : flx5(a[c + 2 * sk], a[c + sk], a[c], a[c - sk], a[c - 2 * sk]);
+    else if (k == g.nz - 2) f = up ? flx5(a[c - 3 * sk], a[c - 2 * sk], a[c - sk], a[c], a[c + sk]) : flx3(a[c + sk], a[c], a[c - sk]);
+    else if (k == g.nz - 1) f = up ? flx3(a[c - 2 * sk], a[c - sk], a[c]) : fmaf(c1[k], a[c - sk], c2[k] * a[c]);
+    else f = up ? flx5(a[c - 3 * sk], a[c - 2 * sk], a[c - sk], a[c], a[c + sk])
+                : flx5(a[c + 2 * sk], a[c + sk], a[c], a[c - sk], a[c - 2 * sk]);
+  }
+  return m * f;
+}
+
+template <int DIR>
+__device__ __forceinline__ float face_weno_h(const KArgs& A, int i, int j, int k) {
+  const Dims& g = A.g;
+  const float *a = A.p[1], *rr = A.p[2];
+  const float weps = A.f[3];
+  const int pdef = A.iv[4];
+  int c = gidx(g, i, j, k);
+  const int d = DIR == 0 ? 1 : g.sJ;
+  float s1, s2, s3, s4, s5;
+  float r = rr[c];
+  if (r >= 0.0f) { s1 = a[c - 3 * d]; s2 = a[c - 2 * d]; s3 = a[c - d]; s4 = a[c]; s5 = a[c + d]; }
+  else { s1 = a[c + 2 * d]; s2 = a[c + d]; s3 = a[c]; s4 = a[c - d]; s5 = a[c - 2 * d]; }
+  bool ok = pdef != 1 || weno_pdef_ok(s1, s2, s3, s4, s5, weps);
+  return ok ? r * weno5(s1, s2, s3, s4, s5, weps) : 0.0f;
+}
+
+__device__ __forceinline__ float face_weno_z(const KArgs& A, int i, int j, int k) {
+  const Dims& g = A.g;
+  const int kf = k + 1;
+  const float *a = A.p[1], *rrw = A.p[2], *c1 = A.p[3], *c2 = A.p[4];
+  const float weps = A.f[5];
+  const int pdefweno = A.iv[7];
+  const int sk = g.sJ * g.sK, nk = g.nz;
+  int c = gidx(g, i, j, k);
+  if (kf == 1 || kf == g.nz + 1) {
+    return 0.0f;
+  }
+#define AZ(o) a[c + (o) * sk]
+  float w = rrw[c];
+  if (kf == 2) {
+    return w >= 0.0f ? w * fmaf(c1[k], AZ(-1), c2[k] * AZ(0)) : w * upstrpd(AZ(1), AZ(0), AZ(-1), weps);
+  }
+  if (kf == nk) {
+    return w > 0.0f ? w * upstrpd(AZ(-2), AZ(-1), AZ(0), weps) : w * fmaf(c1[k], AZ(-1), c2[k] * AZ(0));
+  }
+  float s1, s2, s3, s4, s5;
+  if (w >= 0.0f) { s1 = AZ(-3); s2 = AZ(-2); s3 = AZ(-1); s4 = AZ(0); s5 = AZ(1); }
+  else { s1 = AZ(2); s2 = AZ(1); s3 = AZ(0); s4 = AZ(-1); s5 = AZ(-2); }
+  if (pdefweno == 1) {
+    bool doit = weno_pdef_ok(s1, s2, s3, s4, s5, weps);
+    if (kf == 3 && w > 0.0f) doit = false;
+    if (kf == nk - 1 && w < 0.0f) doit = false;
+    if (doit) {
+      return w * weno5(s1, s2, s3, s4, s5, weps);
+    }
+    if (kf != 3 && kf != nk - 1) {
+      return 0.0f;
+    }
+  }
+  if (kf == 3) {
+    return w >= 0.0f ? w * upstrpd(AZ(-2), AZ(-1), AZ(0), weps) : w * weno5(AZ(2), AZ(1), AZ(0), AZ(-1), AZ(-2), weps);
+  }
+  if (kf == nk - 1) {
+    return w >= 0.0f ? w * weno5(AZ(-3), AZ(-2), AZ(-1), AZ(0), AZ(1), weps) : w * upstrpd(AZ(1), AZ(0), AZ(-1), weps);
+  }
+  return w * weno5(s1, s2, s3, s4, s5, weps);
+#undef AZ
+}
+
+template <int DIR>
+__device__ __forceinline__ float face_weno_uv_h(const KArgs& A, int i, int j, int k) {
+  const Dims& g = A.g;
+  const int stag = A.iv[1];
+  const float *a = A.p[2], *rr = A.p[3];
+  const float weps = A.f[4];
+  const int sj = g.sJ;
+  int c = gidx(g, i, j, k);
+  if (DIR == 0) {
+    float m = stag == 2 ? 0.5f * (rr[c] + rr[c + 1]) : 0.5f * (rr[c] + rr[c - sj]);
+    return m * weno5_upwind(a, c, 1, m >= 0.0f, stag == 2, weps);
+  } else {
+    float m = stag == 2 ? 0.5f * (rr[c] + rr[c - 1]) : 0.5f * (rr[c] + rr[c + sj]);
+    return m * weno5_upwind(a, c, sj, m >= 0.0f, stag == 3, weps);
+  }
+}
+
+__device__ __forceinline__ float face_weno_uv_z(const KArgs& A, int i, int j, int k) {
+  const Dims& g = A.g;
+  const int stag = A.iv[1];
+  const float *a = A.p[2], *rrw = A.p[3], *c1 = A.p[4], *c2 = A.p[5];
+  const float weps = A.f[6];
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  int c = gidx(g, i, j, k);
+  if (k == 0 || k == g.nz) {
+    return 0.0f;
+  }
+#define AZ(o) a[c + (o) * sk]
+  float m = stag == 2 ? 0.5f * (rrw[c] + rrw[c - 1]) : 0.5f * (rrw[c] + rrw[c - sj]);
+  bool up = m >= 0.0f;
+  float f;
+  if (k == 1) f = up ? fmaf(c1[k], AZ(-1), c2[k] * AZ(0)) : upstrpd(AZ(1), AZ(0), AZ(-1), weps);
+  else if (k == 2) f = up ? upstrpd(AZ(-2), AZ(-1), AZ(0), weps) : weno5(AZ(2), AZ(1), AZ(0), AZ(-1), AZ(-2), weps);
+  else if (k == g.nz - 2) f = up ? weno5(AZ(-3), AZ(-2), AZ(-1), AZ(0), AZ(1), weps) : upstrpd(AZ(1), AZ(0), AZ(-1), weps);
+  else if (k == g.nz - 1) f = up ? upstrpd(AZ(-2), AZ(-1), AZ(0), weps) : fmaf(c1[k], AZ(-1), c2[k] * AZ(0));
+  else f = up ? weno5(AZ(-3), AZ(-2), AZ(-1), AZ(0), AZ(1), weps) : weno5(AZ(2), AZ(1), AZ(0), AZ(-1), AZ(-2), weps);
+  return m * f;
+#undef AZ
+}
+
+template <int DIR>
+__device__ __forceinline__ float face_weno_w_h(const KArgs& A, int i, int j, int k) {
+  const Dims& g = A.g;
+  const float *a = A.p[1], *rr = A.p[2], *c2 = A.p[3];
+  const float weps = A.f[4];
+  const int sk = g.sJ * g.sK;
+  int c = gidx(g, i, j, k);
+  if (k == 0) {
+    return 0.0f;
+  }
+  const int d = DIR == 0 ? 1 : g.sJ;
+  float cc2 = c2[k];
+  float cc1 = 1.0f - cc2;
+  float ub = fmaf(cc2, rr[c], cc1 * rr[c - sk]);
+  return ub >= 0.0f ? ub * weno5(a[c - 3 * d], a[c - 2 * d], a[c - d], a[c], a[c + d], weps)
+                     : ub * weno5(a[c + 2 * d], a[c + d], a[c], a[c - d], a[c - 2 * d], weps);
+}
+
+__device__ __forceinline__ float face_weno_w_z(const KArgs& A, int i, int j, int k) {
+  const Dims& g = A.g;
+  const float *a = A.p[1], *rrw = A.p[2];
+  const float weps = A.f[3];
+  const int sk = g.sJ * g.sK, nz = g.nz;
+  int c = gidx(g, i, j, k);
+  if (k > g.nz - 1) {
+    return 0.0f;
+  }
+#define AZ(o) a[c + (o) * sk]
+  float wb = 0.5f * (rrw[c] + rrw[c + sk]);
+  float f;
+  if (k == 0) f = wb >= 0.0f ? 0.5f * (AZ(0) + AZ(1)) : upstrpd(AZ(2), AZ(1), AZ(0), weps);
+  else if (k == nz - 1) f = wb > 0.0f ? upstrpd(AZ(-1), AZ(0), AZ(1), weps) : 0.5f * (AZ(0) + AZ(1));
+  else if (k == 1) f = wb >= 0.0f ? upstrpd(AZ(-1), AZ(0), AZ(1), weps) : weno5(AZ(3), AZ(2), AZ(1), AZ(0), AZ(-1), weps);
+  else if (k == nz - 2) f = wb > 0.0f ? weno5(AZ(-2), AZ(-1), AZ(0), AZ(1), AZ(2), weps) : upstrpd(AZ(2), AZ(1), AZ(0), weps);
+  else f = wb >= 0.0f ? weno5(AZ(-2), AZ(-1), AZ(0), AZ(1), AZ(2), weps) : weno5(AZ(3), AZ(2), AZ(1), AZ(0), AZ(-1), weps);
+  return wb * f;
+#undef AZ
+}
+
+// adv_assemble (adv_assemble.wgsl:139-279) at cell (i, j, k) from the flux differences:
+// returns the advective tendency t (before the accumulate/store).
+__device__ __forceinline__ float assemble_t(const KArgs& A, int i, int j, int k, int c, float dFx, float dFy, float dFz) {
+  const Dims& g = A.g;
+  const int stag = A.iv[1];
+  const float *s = A.p[2], *divx = A.p[6];
+  const float *rho0 = A.p[7], *rf0 = A.p[8], *mh = A.p[9], *mf = A.p[10];
+  const float *rru = A.p[13], *rrv = A.p[14], *c1 = A.p[15], *c2 = A.p[16];
+  const int openx = A.iv[17], openy = A.iv2[17];
+  const float* hm = A.p[30];
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  const int st = stag < 0 ? -stag : stag;
+  float mz = stag < 0 ? 1.0f : (stag == 4 ? mf[k] : mh[k]);
+  float dv;
+  if (st == 2) dv = 0.5f * (divx[c] + divx[c - 1]);
+  else if (st == 3) dv = 0.5f * (divx[c] + divx[c - sj]);
+  else if (st == 4) dv = fmaf(c2[k], divx[c], c1[k] * divx[c - sk]);
+  else dv = divx[c];
+  if (openx != 0 && st != 2) {
+    bool west = i == 0, east = i == g.nx - 1;
+    if (west || east) {
+      int cf = west ? c : c + 1;
+      float un, piece;
+      if (st == 3) {
+        un = rru[cf] + rru[cf - sj];
+        piece = ((0.5f * ((rru[c + 1 - sj] - rru[c - sj]) + (rru[c + 1] - rru[c]))) * g.rdx) * hm_uh(g, hm, i);
+      } else if (st == 4) {
+        float cc2 = 0.5f * (c2[k - 1] + c2[k]);
+        float cc1 = 1.0f - cc2;
+        un = fmaf(cc2, rru[cf], cc1 * rru[cf - sk]);
+        piece = (fmaf(c1[k], rru[c + 1 - sk] - rru[c - sk], c2[k] * (rru[c + 1] - rru[c])) * g.rdx) * hm_uh(g, hm, i);
+      } else {
+        un = rru[cf];
+        piece = ((rru[c + 1] - rru[c]) * g.rdx) * hm_uh(g, hm, i);
+      }
+      bool inflow = west ? un >= 0.0f : un <= 0.0f;
+      if (inflow) {
+        dFx = 0.0f;
+        dv = dv - piece;
+      }
+    }
+  }
+  if (openy != 0 && st != 3) {
+    bool south = j == 0, north = j == g.ny - 1;
+    if (south || north) {
+      int cf = south ? c : c + sj;
+      float vn, piece;
+      if (st == 2) {
+        vn = rrv[cf] + rrv[cf - 1];
+        piece = ((0.5f * ((rrv[c + sj - 1] - rrv[c - 1]) + (rrv[c + sj] - rrv[c]))) * g.rdy) * hm_vh(g, hm, j);
+      } else if (st == 4) {
+        float cc2 = 0.5f * (c2[k - 1] + c2[k]);
+        float cc1 = 1.0f - cc2;
+        vn = fmaf(cc2, rrv[cf], cc1 * rrv[cf - sk]);
+        piece = (fmaf(c1[k], rrv[c + sj - sk] - rrv[c - sk], c2[k] * (rrv[c + sj] - rrv[c])) * g.rdy) * hm_vh(g, hm, j);
+      } else {
+        vn = rrv[cf];
+        piece = ((rrv[c + sj] - rrv[c]) * g.rdy) * hm_vh(g, hm, j);
+      }
+      bool inflow = south ? vn >= 0.0f : vn <= 0.0f;
+      if (inflow) {
+        dFy = 0.0f;
+        dv = dv - piece;
+      }
+    }
+  }
+  float mx = st == 2 ? hm_uf(g, hm, i) : hm_uh(g, hm, i);
+  float my = st == 3 ? hm_vf(g, hm, j) : hm_vh(g, hm, j);
+  float divF = fmaf(dFz * g.rdz, mz, fmaf(dFx * g.rdx, mx, (dFy * g.rdy) * my));
+  float rho = st == 4 ? rf0[k] : rho0[k];
+  return dcr(fmaf(s[c], dv, -divF), rho);
+}
+
+}  // namespace te

@@ -17,11 +17,13 @@
 // same sequence of binary32 operations as te_kernels.cu.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <stdexcept>
 #include <string>
 
 #include "../../include/thunderstep.h"
+#include "te_flux.cuh"
 #include "te_fused.cuh"
 #include "te_math.cuh"
 #include "te_player.hpp"
@@ -101,47 +103,50 @@ __device__ __forceinline__ float fpk_at(const AcuArgs& A, int i, int j, int c, c
               fmaf(a.dts, fmaf(-A.ppterm[c], div, A.ppten[c]), advPi));
 }
 
-// K2: a CTA owns 32 interior columns (i0..i0+31, row j).  256 threads = 32 columns x
-// 8 level slots.  Per pass of 8 levels:
-//   A1 (all threads) load one level each: fpk (acoustic_fpk.wgsl:167-207) and the
-//      pointwise terms of the w-pi' system, kept in shared memory;
-//   A2 (all threads) the tridiagonal coefficients aa, bb, cc, dd of their level
-//      (lam_1, acoustic_w_solve.wgsl:124-139);
-//   B  (warp 0, one lane per column) the Thomas forward recurrence, sequential in k.
-// Then warp 0 back-substitutes w, and all threads apply the pi' update
-// (acoustic_pp.wgsl:131-167), store w and accumulate rrw (acoustic_accumulate.wgsl) for
-// levels 0..nz.  Every value is produced by the same binary32 operations as the
-// per-dispatch kernels; sums the reference forms twice (pk1+qk, pp3d+fpk, ...) are
-// formed once here with the same rounding.
+// K2: a CTA owns 32 interior columns (i0..i0+31, row j) and runs their implicit w-pi'
+// solve with warp specialisation.  Warps 0-7 (workers, one level each per pass of 8
+// levels) load the 19 inputs of their level (prefetched one pass ahead), form fpk
+// (acoustic_fpk.wgsl:167-207) and the tridiagonal coefficients aa, bb, cc, dd of the level
+// (lam_1, acoustic_w_solve.wgsl:124-139) into a double-buffered pass store.  Warp 8 (one
+// lane per column) runs the sequential Thomas forward recurrence on the previous pass
+// while the workers prepare the next one, then back-substitutes w.  Finally all warps
+// apply the pi' update (acoustic_pp.wgsl:131-167), store w and accumulate rrw
+// (acoustic_accumulate.wgsl:129-158) for levels 0..nz.  Every value is produced by the
+// same binary32 operations as the per-dispatch kernels; sums the reference forms twice
+// (pk1+qk, pp3d+fpk, ...) are formed once here with the same rounding.
 constexpr int kColTile = 32;
-constexpr int kLevels = 16;
+constexpr int kLevels = 8;                       // worker warps = levels per pass
+constexpr int kWorkers = kColTile * kLevels;     // 256
+constexpr int kColThreads = kWorkers + kColTile; // + the recurrence warp
 
 struct ColSmem {
-  float *cA, *cB, *A, *Bq, *s, *prev;           // [nz][32] persistent
-  float *m, *wt, *wold, *aa, *bb, *cc, *dd;     // [kLevels][32] per pass
+  float *cA, *cB, *A, *Bq, *s, *prev;  // [nz][32], whole column
+  float* co;                           // [2][4][kLevels][32]: aa, bb, cc, dd per pass
 };
 
 __device__ __forceinline__ ColSmem col_smem(float* base, int nz) {
   ColSmem S;
-  const int P = nz * kColTile, T = kLevels * kColTile;
+  const int P = nz * kColTile;
   S.cA = base;
   S.cB = base + P;
   S.A = base + 2 * P;
   S.Bq = base + 3 * P;
   S.s = base + 4 * P;
   S.prev = base + 5 * P;
-  float* t = base + 6 * P;
-  S.m = t;
-  S.wt = t + T;
-  S.wold = t + 2 * T;
-  S.aa = t + 3 * T;
-  S.bb = t + 4 * T;
-  S.cc = t + 5 * T;
-  S.dd = t + 6 * T;
+  S.co = base + 6 * P;
   return S;
 }
 
-static size_t col_smem_bytes(int nz) { return (size_t)(6 * nz + 7 * kLevels) * kColTile * sizeof(float); }
+static size_t col_smem_bytes(int nz) { return (size_t)(6 * nz + 8 * kLevels) * kColTile * sizeof(float); }
+
+// index of coefficient `term` (0 aa, 1 bb, 2 cc, 3 dd) of level slot q, lane, buffer b
+__device__ __forceinline__ int co_at(int b, int term, int q, int lane) {
+  return ((b * 4 + term) * kLevels + q) * kColTile + lane;
+}
+
+__device__ __forceinline__ void workers_sync() {
+  asm volatile("bar.sync 1, %0;" ::"n"(kWorkers) : "memory");
+}
 
 // The 19 inputs of one level of one column, loaded ahead of use.
 struct LevelIn {
@@ -186,58 +191,62 @@ __device__ __forceinline__ float fpk_of(const AcuArgs& A, const LevelIn& L, floa
   return fmaf(a.beta, fmaf(L.w0, L.pk1 + L.qk, L.w1 * (L.pk2 - L.qk)), fmaf(a.dts, fmaf(-L.ppterm, div, L.ppten), advPi));
 }
 
-__global__ void __launch_bounds__(kColTile * kLevels, 2) k_acu_column(AcuArgs A) {
+__global__ void __launch_bounds__(kColThreads, 3) k_acu_column(AcuArgs A) {
   extern __shared__ float smem[];
   const Dims& g = A.g;
   const Acoustic& a = A.a;
   const int nz = g.nz;
   const ColSmem S = col_smem(smem, nz);
   const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
+  const bool worker = q < kLevels;
   const int i = blockIdx.x * kColTile + lane;
   const int j = blockIdx.y;
   const bool col = i < g.nx;
   const int sk = g.sJ * g.sK;
   const int c0 = gidx(g, col ? i : 0, j, 0);
-  const float uh = hm_uh(g, A.hm, col ? i : 0), vh = hm_vh(g, A.hm, j);
   const float asq = a.alph * a.alph;
-  float cAm = 0.0f, cBm = 0.0f, wtop = 0.0f;  // warp 0 lanes: recurrence state
+  const int npass = (nz + kLevels - 1) / kLevels;
+  float cAm = 0.0f, cBm = 0.0f, wtop = 0.0f;  // recurrence state (warp kLevels)
   LevelIn cur;
-  if (col && q < nz) cur = load_level(A, c0 + q * sk);
-  for (int k0 = 0; k0 < nz; k0 += kLevels) {
-    const int k = k0 + q;
-    const int t = q * kColTile + lane;
-    // issue the next pass's loads before this pass's barriers and recurrence
-    LevelIn nxt;
-    if (col && k + kLevels < nz) nxt = load_level(A, c0 + (k + kLevels) * sk);
-    if (col && k < nz) {
-      const float fk = fpk_of(A, cur, uh, vh);
-      const int e = k * kColTile + lane;
-      S.A[e] = cur.pk1 + cur.qk;
-      S.Bq[e] = cur.pk2 - cur.qk;
-      S.prev[e] = cur.pp;
-      S.s[e] = cur.pp + fk;
-      S.m[t] = cur.mm;
-      S.wt[t] = cur.wt;
-      S.wold[t] = cur.w0;
-    }
-    __syncthreads();
-    if (col && k < nz && k >= 1) {
-      const int e = k * kColTile + lane, em = e - kColTile;
-      const float m = S.m[t];
-      S.aa[t] = (-asq) * (m * S.A[em]);
-      S.cc[t] = (-asq) * ((-m) * S.Bq[e]);
-      S.bb[t] = fmaf(-asq, m * ((-S.A[e]) + S.Bq[em]), 1.0f);
-      const float fw = fmaf(a.dts, S.wt[t], a.beta * ((-m) * (S.prev[e] - S.prev[em])));
-      S.dd[t] = fmaf(a.alph, (-m) * (S.s[e] - S.s[em]), S.wold[t] + fw);
-    }
-    __syncthreads();
-    if (q == 0 && col) {
+  if (worker && col) cur = load_level(A, c0 + q * sk);
+  const float uh = hm_uh(g, A.hm, col ? i : 0), vh = hm_vh(g, A.hm, j);
+  for (int p = 0; p <= npass; p++) {
+    if (worker) {
+      if (p < npass) {
+        const int k = p * kLevels + q;
+        LevelIn nxt;
+        if (col && k + kLevels < nz) nxt = load_level(A, c0 + (k + kLevels) * sk);
+        if (col && k < nz) {
+          const float fk = fpk_of(A, cur, uh, vh);
+          const int e = k * kColTile + lane;
+          S.A[e] = cur.pk1 + cur.qk;
+          S.Bq[e] = cur.pk2 - cur.qk;
+          S.prev[e] = cur.pp;
+          S.s[e] = cur.pp + fk;
+        }
+        workers_sync();
+        if (col && k < nz && k >= 1) {
+          const int e = k * kColTile + lane, em = e - kColTile;
+          const float m = cur.mm;
+          const int b = p & 1;
+          S.co[co_at(b, 0, q, lane)] = (-asq) * (m * S.A[em]);
+          S.co[co_at(b, 2, q, lane)] = (-asq) * ((-m) * S.Bq[e]);
+          S.co[co_at(b, 1, q, lane)] = fmaf(-asq, m * ((-S.A[e]) + S.Bq[em]), 1.0f);
+          const float fw = fmaf(a.dts, cur.wt, a.beta * ((-m) * (S.prev[e] - S.prev[em])));
+          S.co[co_at(b, 3, q, lane)] = fmaf(a.alph, (-m) * (S.s[e] - S.s[em]), cur.w0 + fw);
+        }
+        cur = nxt;
+      }
+    } else if (p >= 1 && col) {
+      // forward recurrence over the previous pass (acoustic_w_solve.wgsl:150-190)
+      const int b = (p - 1) & 1;
       for (int qq = 0; qq < kLevels; qq++) {
-        const int kk = k0 + qq;
+        const int kk = (p - 1) * kLevels + qq;
         if (kk >= nz) break;
         if (kk == 0) continue;
-        const int tt = qq * kColTile + lane, e = kk * kColTile + lane;
-        const float aa = S.aa[tt], bb = S.bb[tt], cc = S.cc[tt], dd = S.dd[tt];
+        const int e = kk * kColTile + lane;
+        const float aa = S.co[co_at(b, 0, qq, lane)], bb = S.co[co_at(b, 1, qq, lane)];
+        const float cc = S.co[co_at(b, 2, qq, lane)], dd = S.co[co_at(b, 3, qq, lane)];
         if (kk == 1) {
           const float r = dcr(1.0f, bb);
           cAm = (-cc) * r;
@@ -259,10 +268,9 @@ __global__ void __launch_bounds__(kColTile * kLevels, 2) k_acu_column(AcuArgs A)
       }
     }
     __syncthreads();
-    cur = nxt;
   }
-  // back substitution (warp 0): w(k) overwrites cA(k); w(0) = w(nz) = 0
-  if (q == 0 && col) {
+  // back substitution (recurrence warp): w(k) overwrites cA(k); w(0) = w(nz) = 0
+  if (!worker && col) {
     float wk1 = wtop;
     S.cA[(nz - 1) * kColTile + lane] = wtop;
     for (int k = nz - 2; k >= 1; k--) {
@@ -275,7 +283,7 @@ __global__ void __launch_bounds__(kColTile * kLevels, 2) k_acu_column(AcuArgs A)
   }
   __syncthreads();
   if (!col) return;
-  for (int k = q; k <= nz; k += kLevels) {
+  for (int k = q; k <= nz; k += kLevels + 1) {
     const int c = c0 + k * sk;
     if (k < nz) {
       const int e = k * kColTile + lane;
@@ -303,7 +311,7 @@ static void launch_acu_column(const AcuArgs& A, cudaStream_t s) {
     cudaFuncSetAttribute(k_acu_column, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     configured = (int)bytes;
   }
-  dim3 b(kColTile * kLevels), gr((A.g.nx + kColTile - 1) / kColTile, A.g.ny);
+  dim3 b(kColThreads), gr((A.g.nx + kColTile - 1) / kColTile, A.g.ny);
   k_acu_column<<<gr, b, bytes, s>>>(A);
 }
 
@@ -357,9 +365,9 @@ static void launch_halo(const HaloArgs& H, cudaStream_t s) {
   k_halo_periodic<<<gr, b, 0, s>>>(H);
 }
 
-// ------------------------------------------------------------ planner
+// ------------------------------------------------------------ planner helpers
 
-enum SegKind { kExact = 0, kAcoustic = 1, kHalo = 2 };
+enum SegKind { kExact = 0, kAcoustic = 1, kHalo = 2, kAdvect = 3 };
 
 static bool is_name(const Op& o, const char* n) { return !o.copy && o.name == n; }
 
@@ -370,6 +378,308 @@ static bool same_dims(const Dims& a, const Dims& b) {
 static bool same_acoustic(const Acoustic& a, const Acoustic& b) {
   return a.dts == b.dts && a.alph == b.alph && a.beta == b.beta && a.kdiv == b.kdiv && a.smeps == b.smeps;
 }
+
+// ------------------------------------------------------------ fused advection
+
+// Advection of one variable (timestep.js:1629-1900): the three face-flux dispatches and
+// adv_assemble, optionally followed by apply_thterm and rk_update, as one kernel.  A CTA
+// owns a 32 x 8 tile of columns and a chunk of levels and marches up k: the x and y face
+// fluxes of a level are computed once into shared memory, the z face below a cell is
+// carried from the level below.  The per-face arithmetic is face_* of te_flux.cuh and
+// the assembly assemble_t, i.e. the per-dispatch kernels' own code; the fx, fy, fz
+// fields are neither written nor read.
+enum FaceKind { kLin = 0, kStag, kWeno, kWenoUV, kWenoW };
+
+struct AdvArgs {
+  KArgs fx, fy, fz, as;              // bindings of the four dispatches
+  int ilo, ihi, jlo, jhi, klo, khi;  // cells adv_assemble writes
+  FaceRange rx, ry, rz;              // faces each flux dispatch produces
+  int kchunk;
+  int accumulate, write_dest;
+  float* dest;                       // adv_assemble's tendency output
+  const float *div3d, *thterm;       // apply_thterm (null if not fused)
+  const float* phiA;                 // rk_update (null if not fused)
+  float* phi;
+  float dttmp;
+};
+
+template <int KIND, int DIR>
+__device__ __forceinline__ float adv_face(const KArgs& A, int i, int j, int k) {
+  if (KIND == kLin) return DIR == 2 ? face_lin_z(A, i, j, k) : face_lin_h<DIR>(A, i, j, k);
+  if (KIND == kStag) return DIR == 2 ? face_stag_z(A, i, j, k) : face_stag_h<DIR>(A, i, j, k);
+  if (KIND == kWeno) return DIR == 2 ? face_weno_z(A, i, j, k) : face_weno_h<DIR>(A, i, j, k);
+  if (KIND == kWenoUV) return DIR == 2 ? face_weno_uv_z(A, i, j, k) : face_weno_uv_h<DIR>(A, i, j, k);
+  return DIR == 2 ? face_weno_w_z(A, i, j, k) : face_weno_w_h<DIR>(A, i, j, k);
+}
+
+__device__ __forceinline__ bool in_range(const FaceRange& r, int i, int j, int k) {
+  return i >= r.ilo && i <= r.ihi && j >= r.jlo && j <= r.jhi && k >= r.klo && k <= r.khi;
+}
+
+constexpr int kAdvTX = 32, kAdvTY = 8;
+
+// ST = |stagger| of the advected variable: cell (i, j, k) takes the faces i + dx and
+// i + dx + 1 (dx = -1 along its own staggered axis, else 0), likewise in j and k.
+template <int KIND, int ST>
+__global__ void __launch_bounds__(kAdvTX* kAdvTY) k_adv_fused(AdvArgs A) {
+  __shared__ float fxs[kAdvTY][kAdvTX + 1];
+  __shared__ float fys[kAdvTY + 1][kAdvTX];
+  constexpr int dx = ST == 2 ? -1 : 0, dy = ST == 3 ? -1 : 0, dz = ST == 4 ? -1 : 0;
+  const int lx = threadIdx.x, ly = threadIdx.y;
+  const int i = A.ilo + (int)blockIdx.x * kAdvTX + lx, j = A.jlo + (int)blockIdx.y * kAdvTY + ly;
+  const int kb = A.klo + (int)blockIdx.z * A.kchunk, ke = min(A.khi, kb + A.kchunk - 1);
+  const bool cell = i <= A.ihi && j <= A.jhi;
+  float fzc = 0.0f;
+  if (cell) fzc = adv_face<KIND, 2>(A.fz, i, j, kb + dz);
+  for (int k = kb; k <= ke; k++) {
+    const int fi = i + dx, fj = j + dy;
+    if (in_range(A.rx, fi, j, k)) fxs[ly][lx] = adv_face<KIND, 0>(A.fx, fi, j, k);
+    if (lx == kAdvTX - 1 && in_range(A.rx, fi + 1, j, k)) fxs[ly][kAdvTX] = adv_face<KIND, 0>(A.fx, fi + 1, j, k);
+    if (in_range(A.ry, i, fj, k)) fys[ly][lx] = adv_face<KIND, 1>(A.fy, i, fj, k);
+    if (ly == kAdvTY - 1 && in_range(A.ry, i, fj + 1, k)) fys[kAdvTY][lx] = adv_face<KIND, 1>(A.fy, i, fj + 1, k);
+    __syncthreads();
+    if (cell) {
+      const int c = gidx(A.as.g, i, j, k);
+      const float fzn = adv_face<KIND, 2>(A.fz, i, j, k + dz + 1);
+      const float dFx = fxs[ly][lx + 1] - fxs[ly][lx];
+      const float dFy = fys[ly + 1][lx] - fys[ly][lx];
+      const float dFz = fzn - fzc;
+      fzc = fzn;
+      float t = assemble_t(A.as, i, j, k, c, dFx, dFy, dFz);
+      if (A.accumulate) {
+        A.dest[c] = A.dest[c] + t;
+      } else {
+        if (A.thterm) t = fmaf(-A.div3d[c], A.thterm[c], t);   // apply_thterm.wgsl
+        if (A.write_dest) A.dest[c] = t;
+        if (A.phi) A.phi[c] = fmaf(A.dttmp, t, A.phiA[c]);      // rk_update.wgsl
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <int KIND, int ST>
+static void launch_adv_t(const AdvArgs& A, cudaStream_t s) {
+  const dim3 b(kAdvTX, kAdvTY, 1);
+  const int nk = A.khi - A.klo + 1;
+  const dim3 gr((A.ihi - A.ilo + kAdvTX) / kAdvTX, (A.jhi - A.jlo + kAdvTY) / kAdvTY, (nk + A.kchunk - 1) / A.kchunk);
+  k_adv_fused<KIND, ST><<<gr, b, 0, s>>>(A);
+}
+
+static void launch_adv(const AdvArgs& A, int kind, int st, cudaStream_t s) {
+  switch (kind * 10 + st) {
+    case kLin * 10 + 1: launch_adv_t<kLin, 1>(A, s); break;
+    case kWeno * 10 + 1: launch_adv_t<kWeno, 1>(A, s); break;
+    case kStag * 10 + 2: launch_adv_t<kStag, 2>(A, s); break;
+    case kStag * 10 + 3: launch_adv_t<kStag, 3>(A, s); break;
+    case kStag * 10 + 4: launch_adv_t<kStag, 4>(A, s); break;
+    case kWenoUV * 10 + 2: launch_adv_t<kWenoUV, 2>(A, s); break;
+    case kWenoUV * 10 + 3: launch_adv_t<kWenoUV, 3>(A, s); break;
+    case kWenoW * 10 + 4: launch_adv_t<kWenoW, 4>(A, s); break;
+    default: throw std::runtime_error("fused advection: no kernel for this flux kind / stagger");
+  }
+}
+
+struct FluxNames {
+  const char *x, *y, *z;
+  int kind;
+  int out_h, out_z;  // output binding of the horizontal / vertical flux dispatches
+  int src;           // binding of the advected field
+};
+static const FluxNames kFluxSets[] = {
+    {"adv_flux_x", "adv_flux_y", "adv_flux_z", kLin, 3, 5, 1},
+    {"adv_flux_x_stag", "adv_flux_y_stag", "adv_flux_z_stag", kStag, 8, 8, 2},
+    {"adv_flux_x_weno", "adv_flux_y_weno", "adv_flux_z_weno", kWeno, 5, 8, 1},
+    {"adv_flux_x_weno_uv", "adv_flux_y_weno_uv", "adv_flux_z_weno_uv", kWenoUV, 5, 7, 2},
+    {"adv_flux_x_weno_w", "adv_flux_y_weno_w", "adv_flux_z_weno_w", kWenoW, 5, 4, 1},
+};
+
+// Face indices a flux dispatch writes: its dispatch grid mapped to indices (the staggered
+// horizontal kernels start at -1), cut by the kernel's own range check (te_kernels.cu).
+static FaceRange flux_range(int kind, int dir, const Op& o) {
+  const Dims& g = o.args.g;
+  const bool centred = kind == kLin || kind == kWeno;
+  const int off = !centred && dir != 2 ? -1 : 0;
+  FaceRange r;
+  r.ilo = off;
+  r.jlo = off;
+  r.klo = 0;
+  r.ihi = o.grid[0] - 1 + off;
+  r.jhi = o.grid[1] - 1 + off;
+  r.khi = o.grid[2] - 1;
+  int gi, gj, gk;
+  if (dir == 0) { gi = g.nx; gj = centred ? g.ny - 1 : g.ny; gk = g.nz - 1; }
+  else if (dir == 1) { gi = centred ? g.nx - 1 : g.nx; gj = g.ny; gk = g.nz - 1; }
+  else { gi = centred ? g.nx - 1 : g.nx; gj = centred ? g.ny - 1 : g.ny; gk = g.nz; }
+  if (kind == kWenoW && dir != 2) {
+    r.ilo = std::max(r.ilo, 0);
+    r.jlo = std::max(r.jlo, 0);
+  }
+  r.ihi = std::min(r.ihi, gi);
+  r.jhi = std::min(r.jhi, gj);
+  r.khi = std::min(r.khi, gk);
+  return r;
+}
+
+static bool covers(const FaceRange& r, int ilo, int ihi, int jlo, int jhi, int klo, int khi) {
+  return r.ilo <= ilo && r.ihi >= ihi && r.jlo <= jlo && r.jhi >= jhi && r.klo <= klo && r.khi >= khi;
+}
+
+static bool references(const Op& o, const float* f) {
+  if (o.copy || !o.spec) return false;
+  for (int q = 0; q < o.spec->nparams; q++)
+    if (o.spec->params[q].kind == kPtr && o.args.p[o.spec->params[q].index] == f) return true;
+  return false;
+}
+
+// Does op o overwrite f everywhere it matters without reading it first?  Only the
+// flux kernels (their output binding) and adv_assemble without accumulation (its
+// tendency) are known to; any other kernel that names f counts as a reader.
+static bool writes_first(const Op& o, const float* f) {
+  const std::string& n = o.name;
+  for (auto& fs : kFluxSets) {
+    const bool h = n == fs.x || n == fs.y, z = n == fs.z;
+    if (!h && !z) continue;
+    const int out = h ? fs.out_h : fs.out_z;
+    for (int q = 0; q < o.spec->nparams; q++) {
+      const ParamSpec& ps = o.spec->params[q];
+      if (ps.kind == kPtr && ps.index != out && o.args.p[ps.index] == f) return false;
+    }
+    return o.args.p[out] == f;
+  }
+  if (n == "adv_assemble" && o.args.iv[12] == 0) {
+    for (int q = 0; q < o.spec->nparams; q++) {
+      const ParamSpec& ps = o.spec->params[q];
+      if (ps.kind == kPtr && ps.index != 11 && o.args.p[ps.index] == f) return false;
+    }
+    return o.args.p[11] == f;
+  }
+  return false;
+}
+
+// The values ops [first, last] leave in field f are never read afterwards: scanning the
+// step cyclically from last + 1 (steps repeat), f is next fully rewritten by a kernel
+// that does not read it, or never named again.
+static bool dead_after(const std::vector<Op>& ops, int first, int last, const float* f, uint32_t* M) {
+  const int n = (int)ops.size();
+  for (int s = 1; s < n; s++) {
+    const int q = (last + s) % n;
+    if (q >= first && q <= last) break;
+    const Op& o = ops[q];
+    if (o.copy) {  // a blit that touches f: not proven dead
+      const float *s0 = reinterpret_cast<const float*>(M + o.src), *d0 = reinterpret_cast<const float*>(M + o.dst);
+      if ((f >= s0 && f < s0 + o.n) || (f >= d0 && f < d0 + o.n)) return false;
+      continue;
+    }
+    if (!references(o, f)) continue;
+    return writes_first(o, f);
+  }
+  return true;
+}
+
+// flux_x, flux_y, flux_z of one kind on one field, then adv_assemble of their fluxes;
+// optionally apply_thterm and rk_update of the fresh tendency.
+static bool match_advect(const std::vector<Op>& ops, size_t i, uint32_t* M, FusedSegment& s, AdvArgs& A) {
+  if (i + 4 > ops.size() || ops[i].copy) return false;
+  const FluxNames* fs = nullptr;
+  for (auto& c : kFluxSets)
+    if (ops[i].name == c.x) fs = &c;
+  if (!fs) return false;
+  const Op &ox = ops[i], &oy = ops[i + 1], &oz = ops[i + 2], &oa = ops[i + 3];
+  if (!is_name(oy, fs->y) || !is_name(oz, fs->z) || !is_name(oa, "adv_assemble")) return false;
+  const Dims& g = oa.args.g;
+  if (!same_dims(g, ox.args.g) || !same_dims(g, oy.args.g) || !same_dims(g, oz.args.g)) return false;
+  if (g.nz < 3) return false;
+  if (oa.args.iv[17] != 0 || oa.args.iv2[17] != 0) return false;  // periodic / closed lateral boundaries
+  const int stag = oa.args.iv[1];
+  if (stag < 1 || stag > 4) return false;
+  if ((fs->kind == kLin || fs->kind == kWeno) && stag != 1) return false;
+  if (fs->kind == kStag && stag == 1) return false;
+  if (fs->kind == kWenoUV && stag != 2 && stag != 3) return false;
+  if (fs->kind == kWenoW && stag != 4) return false;
+  if (fs->kind == kStag || fs->kind == kWenoUV)
+    if (ox.args.iv[1] != stag || oy.args.iv[1] != stag || oz.args.iv[1] != stag) return false;
+  float* src = ox.args.p[fs->src];
+  if (oy.args.p[fs->src] != src || oz.args.p[fs->src] != src || oa.args.p[2] != src) return false;
+  float *fx = ox.args.p[fs->out_h], *fy = oy.args.p[fs->out_h], *fz = oz.args.p[fs->out_z];
+  if (oa.args.p[3] != fx || oa.args.p[4] != fy || oa.args.p[5] != fz) return false;
+  if (fx == fy || fx == fz || fy == fz) return false;
+  std::memset(&A, 0, sizeof(A));
+  A.fx = ox.args;
+  A.fy = oy.args;
+  A.fz = oz.args;
+  A.as = oa.args;
+  A.ilo = 0;
+  A.ihi = stag == 2 ? g.nx : g.nx - 1;
+  A.jlo = 0;
+  A.jhi = stag == 3 ? g.ny : g.ny - 1;
+  A.klo = stag == 4 ? 1 : 0;
+  A.khi = g.nz - 1;
+  if (oa.grid[0] <= A.ihi || oa.grid[1] <= A.jhi || oa.grid[2] <= A.khi) return false;
+  A.rx = flux_range(fs->kind, 0, ox);
+  A.ry = flux_range(fs->kind, 1, oy);
+  A.rz = flux_range(fs->kind, 2, oz);
+  const int dx = stag == 2 ? -1 : 0, dy = stag == 3 ? -1 : 0, dz = stag == 4 ? -1 : 0;
+  if (!covers(A.rx, A.ilo + dx, A.ihi + dx + 1, A.jlo, A.jhi, A.klo, A.khi)) return false;
+  if (!covers(A.ry, A.ilo, A.ihi, A.jlo + dy, A.jhi + dy + 1, A.klo, A.khi)) return false;
+  if (!covers(A.rz, A.ilo, A.ihi, A.jlo, A.jhi, A.klo + dz, A.khi + dz + 1)) return false;
+  A.kchunk = 16;
+  A.accumulate = oa.args.iv[12] != 0;
+  A.dest = oa.args.p[11];
+  A.write_dest = 1;
+  // fields the kernel reads at other cells than the one it writes: nothing it writes may
+  // be among them
+  std::vector<const float*> reads;
+  for (int b = 0; b < kMaxBind; b++) {
+    if (b != fs->out_h && A.fx.p[b]) reads.push_back(A.fx.p[b]);
+    if (b != fs->out_h && A.fy.p[b]) reads.push_back(A.fy.p[b]);
+    if (b != fs->out_z && A.fz.p[b]) reads.push_back(A.fz.p[b]);
+    if (b != 11 && b != 19 && A.as.p[b]) reads.push_back(A.as.p[b]);
+  }
+  auto is_read = [&](const float* f) {
+    for (auto* r : reads)
+      if (r == f) return true;
+    return false;
+  };
+  if (is_read(A.dest)) return false;
+  int last = (int)i + 3;
+  if (!A.accumulate) {
+    size_t q = i + 4;
+    if (stag == 1 && q < ops.size() && is_name(ops[q], "apply_thterm") && ops[q].args.p[3] == A.dest &&
+        same_dims(g, ops[q].args.g) && ops[q].grid[0] >= g.nx && ops[q].grid[1] >= g.ny && ops[q].grid[2] >= g.nz &&
+        ops[q].args.p[1] != A.dest && ops[q].args.p[2] != A.dest && !is_read(ops[q].args.p[3])) {
+      A.div3d = ops[q].args.p[1];
+      A.thterm = ops[q].args.p[2];
+      q++;
+    }
+    if (q < ops.size() && is_name(ops[q], "rk_update") && ops[q].args.p[3] == A.dest && ops[q].args.iv[1] == stag &&
+        same_dims(g, ops[q].args.g) && ops[q].grid[0] > A.ihi && ops[q].grid[1] > A.jhi && ops[q].grid[2] > A.khi) {
+      float* phi = ops[q].args.p[4];
+      const float* phiA = ops[q].args.p[2];
+      bool clash = is_read(phi) || phi == A.dest || phiA == A.dest || phi == fx || phi == fy || phi == fz;
+      if (A.thterm) clash |= A.div3d == phi || A.thterm == phi;
+      if (!clash) {
+        A.phi = phi;
+        A.phiA = phiA;
+        A.dttmp = ops[q].args.f[5];
+        last = (int)q;
+      }
+    }
+    if (A.thterm && !A.phi) return false;  // apply_thterm only together with its rk_update
+    if (A.phi) A.write_dest = dead_after(ops, (int)i, last, A.dest, M) ? 0 : 1;
+  }
+  for (float* f : {fx, fy, fz})
+    if (!dead_after(ops, (int)i, last, f, M)) return false;
+  s.kind = kAdvect;
+  s.first = (int)i;
+  s.last = last;
+  s.aux[1] = fs->kind;
+  s.aux[2] = stag;
+  return true;
+}
+
+// ------------------------------------------------------------ planner
+
 
 // bc_periodic_x(f) followed by bc_periodic_y(f) over the standard halo grid
 static bool halo_pair(const std::vector<Op>& ops, size_t i, float** f) {
@@ -466,6 +776,7 @@ static bool match_substep(const std::vector<Op>& ops, size_t i, FusedSegment& s,
 struct FusedData {
   std::vector<AcuArgs> acu;
   std::vector<HaloArgs> halo;
+  std::vector<AdvArgs> adv;
 };
 
 void FusedStep::build(Plan& P, std::vector<Op>& ops) {
@@ -474,6 +785,7 @@ void FusedStep::build(Plan& P, std::vector<Op>& ops) {
   FusedData& D = *static_cast<FusedData*>(data);
   D.acu.clear();
   D.halo.clear();
+  D.adv.clear();
   size_t i = 0;
   auto exact_to = [&](size_t e) {
     if (!segs.empty() && segs.back().kind == kExact && segs.back().last + 1 == (int)i) segs.back().last = (int)e;
@@ -493,6 +805,14 @@ void FusedStep::build(Plan& P, std::vector<Op>& ops) {
       D.acu.push_back(A);
       segs.push_back(s);
       i += 13;
+      continue;
+    }
+    AdvArgs V;
+    if (match_advect(ops, i, P.M, s, V)) {
+      s.aux[0] = (int)D.adv.size();
+      D.adv.push_back(V);
+      segs.push_back(s);
+      i = s.last + 1;
       continue;
     }
     float* f;
@@ -536,6 +856,8 @@ void FusedStep::launch_segment(Plan& P, std::vector<Op>& ops, int seg, int part)
     P.launch_exact(ops, s.first, s.last, false);
   } else if (s.kind == kHalo) {
     launch_halo(D.halo[s.aux[0]], P.stream);
+  } else if (s.kind == kAdvect) {
+    launch_adv(D.adv[s.aux[0]], s.aux[1], s.aux[2], P.stream);
   } else {
     const AcuArgs& A = D.acu[s.aux[0]];
     const Dims& g = A.g;
