@@ -104,10 +104,10 @@ __device__ __forceinline__ float fpk_at(const AcuArgs& A, int i, int j, int c, c
 }
 
 // K2: a CTA owns 32 interior columns (i0..i0+31, row j) and runs their implicit w-pi'
-// solve with warp specialisation.  Warps 0-7 (workers, one level each per pass of 8
-// levels) load the 19 inputs of their level (prefetched one pass ahead), form fpk
+// solve with warp specialisation.  Warps 0-15 (workers, one level each per pass of 16
+// levels) load the 19 inputs of their level, form fpk
 // (acoustic_fpk.wgsl:167-207) and the tridiagonal coefficients aa, bb, cc, dd of the level
-// (lam_1, acoustic_w_solve.wgsl:124-139) into a double-buffered pass store.  Warp 8 (one
+// (lam_1, acoustic_w_solve.wgsl:124-139) into a double-buffered pass store.  Warp 16 (one
 // lane per column) runs the sequential Thomas forward recurrence on the previous pass
 // while the workers prepare the next one, then back-substitutes w.  Finally all warps
 // apply the pi' update (acoustic_pp.wgsl:131-167), store w and accumulate rrw
@@ -115,8 +115,8 @@ __device__ __forceinline__ float fpk_at(const AcuArgs& A, int i, int j, int c, c
 // same binary32 operations as the per-dispatch kernels; sums the reference forms twice
 // (pk1+qk, pp3d+fpk, ...) are formed once here with the same rounding.
 constexpr int kColTile = 32;
-constexpr int kLevels = 8;                       // worker warps = levels per pass
-constexpr int kWorkers = kColTile * kLevels;     // 256
+constexpr int kLevels = 16;                      // worker warps = levels per pass
+constexpr int kWorkers = kColTile * kLevels;     // 512
 constexpr int kColThreads = kWorkers + kColTile; // + the recurrence warp
 
 struct ColSmem {
@@ -191,7 +191,7 @@ __device__ __forceinline__ float fpk_of(const AcuArgs& A, const LevelIn& L, floa
   return fmaf(a.beta, fmaf(L.w0, L.pk1 + L.qk, L.w1 * (L.pk2 - L.qk)), fmaf(a.dts, fmaf(-L.ppterm, div, L.ppten), advPi));
 }
 
-__global__ void __launch_bounds__(kColThreads, 3) k_acu_column(AcuArgs A) {
+__global__ void __launch_bounds__(kColThreads, 2) k_acu_column(AcuArgs A) {
   extern __shared__ float smem[];
   const Dims& g = A.g;
   const Acoustic& a = A.a;
@@ -207,15 +207,13 @@ __global__ void __launch_bounds__(kColThreads, 3) k_acu_column(AcuArgs A) {
   const float asq = a.alph * a.alph;
   const int npass = (nz + kLevels - 1) / kLevels;
   float cAm = 0.0f, cBm = 0.0f, wtop = 0.0f;  // recurrence state (warp kLevels)
-  LevelIn cur;
-  if (worker && col) cur = load_level(A, c0 + q * sk);
   const float uh = hm_uh(g, A.hm, col ? i : 0), vh = hm_vh(g, A.hm, j);
   for (int p = 0; p <= npass; p++) {
     if (worker) {
       if (p < npass) {
         const int k = p * kLevels + q;
-        LevelIn nxt;
-        if (col && k + kLevels < nz) nxt = load_level(A, c0 + (k + kLevels) * sk);
+        LevelIn cur;
+        if (col && k < nz) cur = load_level(A, c0 + k * sk);
         if (col && k < nz) {
           const float fk = fpk_of(A, cur, uh, vh);
           const int e = k * kColTile + lane;
@@ -235,7 +233,6 @@ __global__ void __launch_bounds__(kColThreads, 3) k_acu_column(AcuArgs A) {
           const float fw = fmaf(a.dts, cur.wt, a.beta * ((-m) * (S.prev[e] - S.prev[em])));
           S.co[co_at(b, 3, q, lane)] = fmaf(a.alph, (-m) * (S.s[e] - S.s[em]), cur.w0 + fw);
         }
-        cur = nxt;
       }
     } else if (p >= 1 && col) {
       // forward recurrence over the previous pass (acoustic_w_solve.wgsl:150-190)
@@ -352,11 +349,19 @@ __global__ void k_halo_periodic(HaloArgs H) {
   const int ii = ((i % g.nx) + g.nx) % g.nx;
   const int jj = ((j % g.ny) + g.ny) % g.ny;
   const int dst = gidx(g, i, j, k), src = gidx(g, ii, jj, k);
+  // every load before the first store: a halo point (dst) is never an interior point
+  // (src), so the loads of the four fields and of the accumulation overlap
+  float v[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+    if (q < H.nf) v[q] = H.f[q][src];
   if (H.acc_rrw) {
-    const float wv = H.acc_w[dst];
-    H.acc_rrw[dst] = H.tavg > 0.0f ? fmaf(wv, H.alph, H.acc_rrw[dst]) * H.tavg : H.acc_rrw[dst] + wv;
+    const float wv = H.acc_w[dst], r = H.acc_rrw[dst];
+    H.acc_rrw[dst] = H.tavg > 0.0f ? fmaf(wv, H.alph, r) * H.tavg : r + wv;
   }
-  for (int q = 0; q < H.nf; q++) H.f[q][dst] = H.f[q][src];
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+    if (q < H.nf) H.f[q][dst] = v[q];
 }
 
 static void launch_halo(const HaloArgs& H, cudaStream_t s) {
@@ -382,19 +387,15 @@ static bool same_acoustic(const Acoustic& a, const Acoustic& b) {
 // ------------------------------------------------------------ fused advection
 
 // Advection of one variable (timestep.js:1629-1900): the three face-flux dispatches and
-// adv_assemble, optionally followed by apply_thterm and rk_update, as one kernel.  A CTA
-// owns a 32 x 8 tile of columns and a chunk of levels and marches up k: the x and y face
-// fluxes of a level are computed once into shared memory, the z face below a cell is
-// carried from the level below.  The per-face arithmetic is face_* of te_flux.cuh and
-// the assembly assemble_t, i.e. the per-dispatch kernels' own code; the fx, fy, fz
-// fields are neither written nor read.
+// adv_assemble, optionally followed by apply_thterm and rk_update, as one kernel.  The
+// per-face arithmetic is face_* of te_flux.cuh and the assembly assemble_t, i.e. the
+// per-dispatch kernels' own code; the fx, fy, fz fields are neither written nor read.
 enum FaceKind { kLin = 0, kStag, kWeno, kWenoUV, kWenoW };
 
 struct AdvArgs {
   KArgs fx, fy, fz, as;              // bindings of the four dispatches
   int ilo, ihi, jlo, jhi, klo, khi;  // cells adv_assemble writes
   FaceRange rx, ry, rz;              // faces each flux dispatch produces
-  int kchunk;
   int accumulate, write_dest;
   float* dest;                       // adv_assemble's tendency output
   const float *div3d, *thterm;       // apply_thterm (null if not fused)
@@ -419,50 +420,53 @@ __device__ __forceinline__ bool in_range(const FaceRange& r, int i, int j, int k
 constexpr int kAdvTX = 32, kAdvTY = 8;
 
 // ST = |stagger| of the advected variable: cell (i, j, k) takes the faces i + dx and
-// i + dx + 1 (dx = -1 along its own staggered axis, else 0), likewise in j and k.
+// i + dx + 1 (dx = -1 along its own staggered axis, else 0), likewise in j and k.  A CTA
+// covers a 32 x 8 tile of one level: the 33 x 8 x-faces and 32 x 9 y-faces of the tile
+// are computed once into shared memory (the faces beyond 256 by warps 0 and 1), each
+// cell computes its two z-faces, then assembles.
 template <int KIND, int ST>
 __global__ void __launch_bounds__(kAdvTX* kAdvTY) k_adv_fused(AdvArgs A) {
   __shared__ float fxs[kAdvTY][kAdvTX + 1];
   __shared__ float fys[kAdvTY + 1][kAdvTX];
   constexpr int dx = ST == 2 ? -1 : 0, dy = ST == 3 ? -1 : 0, dz = ST == 4 ? -1 : 0;
-  const int lx = threadIdx.x, ly = threadIdx.y;
-  const int i = A.ilo + (int)blockIdx.x * kAdvTX + lx, j = A.jlo + (int)blockIdx.y * kAdvTY + ly;
-  const int kb = A.klo + (int)blockIdx.z * A.kchunk, ke = min(A.khi, kb + A.kchunk - 1);
+  const int lx = threadIdx.x, ly = threadIdx.y, t = ly * kAdvTX + lx;
+  const int i0 = A.ilo + (int)blockIdx.x * kAdvTX, j0 = A.jlo + (int)blockIdx.y * kAdvTY;
+  const int i = i0 + lx, j = j0 + ly, k = A.klo + (int)blockIdx.z;
+  {
+    const int r = t / (kAdvTX + 1), q = t % (kAdvTX + 1);
+    if (in_range(A.rx, i0 + dx + q, j0 + r, k)) fxs[r][q] = adv_face<KIND, 0>(A.fx, i0 + dx + q, j0 + r, k);
+  }
+  if (in_range(A.ry, i, j0 + dy + ly, k)) fys[ly][lx] = adv_face<KIND, 1>(A.fy, i, j0 + dy + ly, k);
+  if (ly == 0 && lx < kAdvTY) {  // x-faces 256..263 (row-major [8][33]): the tail of row 7
+    const int e = kAdvTX * kAdvTY + lx, r = e / (kAdvTX + 1), q = e % (kAdvTX + 1);
+    if (in_range(A.rx, i0 + dx + q, j0 + r, k)) fxs[r][q] = adv_face<KIND, 0>(A.fx, i0 + dx + q, j0 + r, k);
+  }
+  if (ly == 1 && in_range(A.ry, i, j0 + dy + kAdvTY, k)) fys[kAdvTY][lx] = adv_face<KIND, 1>(A.fy, i, j0 + dy + kAdvTY, k);
   const bool cell = i <= A.ihi && j <= A.jhi;
-  float fzc = 0.0f;
-  if (cell) fzc = adv_face<KIND, 2>(A.fz, i, j, kb + dz);
-  for (int k = kb; k <= ke; k++) {
-    const int fi = i + dx, fj = j + dy;
-    if (in_range(A.rx, fi, j, k)) fxs[ly][lx] = adv_face<KIND, 0>(A.fx, fi, j, k);
-    if (lx == kAdvTX - 1 && in_range(A.rx, fi + 1, j, k)) fxs[ly][kAdvTX] = adv_face<KIND, 0>(A.fx, fi + 1, j, k);
-    if (in_range(A.ry, i, fj, k)) fys[ly][lx] = adv_face<KIND, 1>(A.fy, i, fj, k);
-    if (ly == kAdvTY - 1 && in_range(A.ry, i, fj + 1, k)) fys[kAdvTY][lx] = adv_face<KIND, 1>(A.fy, i, fj + 1, k);
-    __syncthreads();
-    if (cell) {
-      const int c = gidx(A.as.g, i, j, k);
-      const float fzn = adv_face<KIND, 2>(A.fz, i, j, k + dz + 1);
-      const float dFx = fxs[ly][lx + 1] - fxs[ly][lx];
-      const float dFy = fys[ly + 1][lx] - fys[ly][lx];
-      const float dFz = fzn - fzc;
-      fzc = fzn;
-      float t = assemble_t(A.as, i, j, k, c, dFx, dFy, dFz);
-      if (A.accumulate) {
-        A.dest[c] = A.dest[c] + t;
-      } else {
-        if (A.thterm) t = fmaf(-A.div3d[c], A.thterm[c], t);   // apply_thterm.wgsl
-        if (A.write_dest) A.dest[c] = t;
-        if (A.phi) A.phi[c] = fmaf(A.dttmp, t, A.phiA[c]);      // rk_update.wgsl
-      }
-    }
-    __syncthreads();
+  float fz0 = 0.0f, fz1 = 0.0f;
+  if (cell) {
+    fz0 = adv_face<KIND, 2>(A.fz, i, j, k + dz);
+    fz1 = adv_face<KIND, 2>(A.fz, i, j, k + dz + 1);
+  }
+  __syncthreads();
+  if (!cell) return;
+  const int c = gidx(A.as.g, i, j, k);
+  const float dFx = fxs[ly][lx + 1] - fxs[ly][lx];
+  const float dFy = fys[ly + 1][lx] - fys[ly][lx];
+  float tn = assemble_t(A.as, i, j, k, c, dFx, dFy, fz1 - fz0);
+  if (A.accumulate) {
+    A.dest[c] = A.dest[c] + tn;
+  } else {
+    if (A.thterm) tn = fmaf(-A.div3d[c], A.thterm[c], tn);   // apply_thterm.wgsl
+    if (A.write_dest) A.dest[c] = tn;
+    if (A.phi) A.phi[c] = fmaf(A.dttmp, tn, A.phiA[c]);      // rk_update.wgsl
   }
 }
 
 template <int KIND, int ST>
 static void launch_adv_t(const AdvArgs& A, cudaStream_t s) {
   const dim3 b(kAdvTX, kAdvTY, 1);
-  const int nk = A.khi - A.klo + 1;
-  const dim3 gr((A.ihi - A.ilo + kAdvTX) / kAdvTX, (A.jhi - A.jlo + kAdvTY) / kAdvTY, (nk + A.kchunk - 1) / A.kchunk);
+  const dim3 gr((A.ihi - A.ilo + kAdvTX) / kAdvTX, (A.jhi - A.jlo + kAdvTY) / kAdvTY, A.khi - A.klo + 1);
   k_adv_fused<KIND, ST><<<gr, b, 0, s>>>(A);
 }
 
@@ -623,7 +627,6 @@ static bool match_advect(const std::vector<Op>& ops, size_t i, uint32_t* M, Fuse
   if (!covers(A.rx, A.ilo + dx, A.ihi + dx + 1, A.jlo, A.jhi, A.klo, A.khi)) return false;
   if (!covers(A.ry, A.ilo, A.ihi, A.jlo + dy, A.jhi + dy + 1, A.klo, A.khi)) return false;
   if (!covers(A.rz, A.ilo, A.ihi, A.jlo, A.jhi, A.klo + dz, A.khi + dz + 1)) return false;
-  A.kchunk = 16;
   A.accumulate = oa.args.iv[12] != 0;
   A.dest = oa.args.p[11];
   A.write_dest = 1;
