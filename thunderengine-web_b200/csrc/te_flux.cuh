@@ -14,18 +14,27 @@ struct FaceRange {
   int ilo, ihi, jlo, jhi, klo, khi;
 };
 
+// The five values of an upwind-biased stencil at face index c along stride s: on the
+// upwind side (up) c-3s .. c+s, else c+2s .. c-2s (reversed), both moved by `shift`
+// points along the axis.  The side is chosen before the reconstruction, so each face
+// evaluates one reconstruction whatever the flow direction in its warp.
+struct Sten5 {
+  float s1, s2, s3, s4, s5;
+};
+__device__ __forceinline__ Sten5 sten5(const float* a, int c, int s, bool up, int shift) {
+  const int st = up ? s : -s;
+  const int b = c + shift * s + (up ? -3 * s : 2 * s);
+  return Sten5{a[b], a[b + st], a[b + 2 * st], a[b + 3 * st], a[b + 4 * st]};
+}
+__device__ __forceinline__ float flx5(const Sten5& t) { return flx5(t.s1, t.s2, t.s3, t.s4, t.s5); }
+__device__ __forceinline__ float weno5(const Sten5& t, float weps) { return weno5(t.s1, t.s2, t.s3, t.s4, t.s5, weps); }
+
 __device__ __forceinline__ float flx5_upwind(const float* a, int c, int s, bool up, bool shifted) {
-  if (shifted) return up ? flx5(a[c - 2 * s], a[c - s], a[c], a[c + s], a[c + 2 * s])
-                         : flx5(a[c + 3 * s], a[c + 2 * s], a[c + s], a[c], a[c - s]);
-  return up ? flx5(a[c - 3 * s], a[c - 2 * s], a[c - s], a[c], a[c + s])
-            : flx5(a[c + 2 * s], a[c + s], a[c], a[c - s], a[c - 2 * s]);
+  return flx5(sten5(a, c, s, up, shifted ? 1 : 0));
 }
 
 __device__ __forceinline__ float weno5_upwind(const float* a, int c, int s, bool up, bool shifted, float weps) {
-  if (shifted) return up ? weno5(a[c - 2 * s], a[c - s], a[c], a[c + s], a[c + 2 * s], weps)
-                         : weno5(a[c + 3 * s], a[c + 2 * s], a[c + s], a[c], a[c - s], weps);
-  return up ? weno5(a[c - 3 * s], a[c - 2 * s], a[c - s], a[c], a[c + s], weps)
-            : weno5(a[c + 2 * s], a[c + s], a[c], a[c - s], a[c - 2 * s], weps);
+  return weno5(sten5(a, c, s, up, shifted ? 1 : 0), weps);
 }
 
 template <int DIR>
@@ -35,8 +44,7 @@ __device__ __forceinline__ float face_lin_h(const KArgs& A, int i, int j, int k)
   int c = gidx(g, i, j, k);
   const int d = DIR == 0 ? 1 : g.sJ;
   float u = rr[c];
-  float f = u >= 0.0f ? flx5(s[c - 3 * d], s[c - 2 * d], s[c - d], s[c], s[c + d])
-                      : flx5(s[c + 2 * d], s[c + d], s[c], s[c - d], s[c - 2 * d]);
+  float f = flx5(sten5(s, c, d, u >= 0.0f, 0));
   return u * f;
 }
 
@@ -55,8 +63,7 @@ __device__ __forceinline__ float face_lin_z(const KArgs& A, int i, int j, int k)
   else if (k == 2) f = up ? flx3(s[c - 2 * sk], s[c - sk], s[c]) : flx5(s[c + 2 * sk], s[c + sk], s[c], s[c - sk], s[c - 2 * sk]);
   else if (k == g.nz - 2) f = up ? flx5(s[c - 3 * sk], s[c - 2 * sk], s[c - sk], s[c], s[c + sk]) : flx3(s[c + sk], s[c], s[c - sk]);
   else if (k == g.nz - 1) f = up ? flx3(s[c - 2 * sk], s[c - sk], s[c]) : fmaf(c1[k], s[c - sk], c2[k] * s[c]);
-  else f = up ? flx5(s[c - 3 * sk], s[c - 2 * sk], s[c - sk], s[c], s[c + sk])
-              : flx5(s[c + 2 * sk], s[c + sk], s[c], s[c - sk], s[c - 2 * sk]);
+  else f = flx5(sten5(s, c, sk, up, 0));
   return w * f;
 }
 
@@ -106,8 +113,7 @@ __device__ __forceinline__ float face_stag_z(const KArgs& A, int i, int j, int k
     else if (k == 1) f = up ? flx3(a[c - sk], a[c], a[c + sk]) : flx5(a[c + 3 * sk], a[c + 2 * sk], a[c + sk], a[c], a[c - sk]);
     else if (k == g.nz - 2) f = up ? flx5(a[c - 2 * sk], a[c - sk], a[c], a[c + sk], a[c + 2 * sk]) : flx3(a[c + 2 * sk], a[c + sk], a[c]);
     else if (k == g.nz - 1) f = up ? flx3(a[c - sk], a[c], a[c + sk]) : 0.5f * (a[c] + a[c + sk]);
-    else f = up ? flx5(a[c - 2 * sk], a[c - sk], a[c], a[c + sk], a[c + 2 * sk])
-                : flx5(a[c + 3 * sk], a[c + 2 * sk], a[c + sk], a[c], a[c - sk]);
+    else f = flx5(sten5(a, c, sk, up, 1));
   } else {
     if (k == 0 || k == g.nz) {
       return 0.0f;
@@ -116,8 +122,7 @@ __device__ __forceinline__ float face_stag_z(const KArgs& A, int i, int j, int k
     else if (k == 2) f = up ? flx3(a[c - 2 * sk], a[c - sk], a[c]) : flx5(a[c + 2 * sk], a[c + sk], a[c], a[c - sk], a[c - 2 * sk]);
     else if (k == g.nz - 2) f = up ? flx5(a[c - 3 * sk], a[c - 2 * sk], a[c - sk], a[c], a[c + sk]) : flx3(a[c + sk], a[c], a[c - sk]);
     else if (k == g.nz - 1) f = up ? flx3(a[c - 2 * sk], a[c - sk], a[c]) : fmaf(c1[k], a[c - sk], c2[k] * a[c]);
-    else f = up ? flx5(a[c - 3 * sk], a[c - 2 * sk], a[c - sk], a[c], a[c + sk])
-                : flx5(a[c + 2 * sk], a[c + sk], a[c], a[c - sk], a[c - 2 * sk]);
+    else f = flx5(sten5(a, c, sk, up, 0));
   }
   return m * f;
 }
@@ -216,7 +221,7 @@ __device__ __forceinline__ float face_weno_uv_z(const KArgs& A, int i, int j, in
   else if (k == 2) f = up ? upstrpd(AZ(-2), AZ(-1), AZ(0), weps) : weno5(AZ(2), AZ(1), AZ(0), AZ(-1), AZ(-2), weps);
   else if (k == g.nz - 2) f = up ? weno5(AZ(-3), AZ(-2), AZ(-1), AZ(0), AZ(1), weps) : upstrpd(AZ(1), AZ(0), AZ(-1), weps);
   else if (k == g.nz - 1) f = up ? upstrpd(AZ(-2), AZ(-1), AZ(0), weps) : fmaf(c1[k], AZ(-1), c2[k] * AZ(0));
-  else f = up ? weno5(AZ(-3), AZ(-2), AZ(-1), AZ(0), AZ(1), weps) : weno5(AZ(2), AZ(1), AZ(0), AZ(-1), AZ(-2), weps);
+  else f = weno5(sten5(a, c, sk, up, 0), weps);
   return m * f;
 #undef AZ
 }
@@ -235,8 +240,7 @@ __device__ __forceinline__ float face_weno_w_h(const KArgs& A, int i, int j, int
   float cc2 = c2[k];
   float cc1 = 1.0f - cc2;
   float ub = fmaf(cc2, rr[c], cc1 * rr[c - sk]);
-  return ub >= 0.0f ? ub * weno5(a[c - 3 * d], a[c - 2 * d], a[c - d], a[c], a[c + d], weps)
-                     : ub * weno5(a[c + 2 * d], a[c + d], a[c], a[c - d], a[c - 2 * d], weps);
+  return ub * weno5(sten5(a, c, d, ub >= 0.0f, 0), weps);
 }
 
 __device__ __forceinline__ float face_weno_w_z(const KArgs& A, int i, int j, int k) {
@@ -255,7 +259,7 @@ __device__ __forceinline__ float face_weno_w_z(const KArgs& A, int i, int j, int
   else if (k == nz - 1) f = wb > 0.0f ? upstrpd(AZ(-1), AZ(0), AZ(1), weps) : 0.5f * (AZ(0) + AZ(1));
   else if (k == 1) f = wb >= 0.0f ? upstrpd(AZ(-1), AZ(0), AZ(1), weps) : weno5(AZ(3), AZ(2), AZ(1), AZ(0), AZ(-1), weps);
   else if (k == nz - 2) f = wb > 0.0f ? weno5(AZ(-2), AZ(-1), AZ(0), AZ(1), AZ(2), weps) : upstrpd(AZ(2), AZ(1), AZ(0), weps);
-  else f = wb >= 0.0f ? weno5(AZ(-2), AZ(-1), AZ(0), AZ(1), AZ(2), weps) : weno5(AZ(3), AZ(2), AZ(1), AZ(0), AZ(-1), weps);
+  else f = weno5(sten5(a, c, sk, wb >= 0.0f, 1), weps);
   return wb * f;
 #undef AZ
 }

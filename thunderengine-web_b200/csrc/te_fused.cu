@@ -61,27 +61,46 @@ __device__ __forceinline__ float uv_v(const AcuArgs& A, int i, int j, int c) {
 
 // K1: every point of the field (halos and k = nz included, as acoustic_accumulate):
 // u, v updated where acoustic_uv updates them, then rru += u, rrv += v (averaged on the
-// last substep, acoustic_accumulate.wgsl:129-158).
+// last substep, acoustic_accumulate.wgsl:129-158).  A thread takes kUvLevels levels of
+// one (i, j) and issues all their loads before its first store (the points are
+// distinct, so nothing it stores is read by it or by another thread).
+constexpr int kUvLevels = 2;
+
 __global__ void __launch_bounds__(256) k_acu_uv(AcuArgs A) {
   const Dims& g = A.g;
   const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x) - 3;
   const int j = (int)(blockIdx.y * blockDim.y + threadIdx.y) - 3;
-  const int k = blockIdx.z;
-  if (i > g.nx + 3 || j > g.ny + 3 || k > g.nz) return;
-  const int c = gidx(g, i, j, k);
-  float un = A.u[c], vn = A.v[c];
-  if (i >= 0 && j >= 0 && i <= g.nx && j <= g.ny && k < g.nz) {
-    un = uv_u(A, i, j, c);
-    vn = uv_v(A, i, j, c);
-    A.u[c] = un;
-    A.v[c] = vn;
+  const int k0 = blockIdx.z * kUvLevels;
+  if (i > g.nx + 3 || j > g.ny + 3) return;
+  const bool upd = i >= 0 && j >= 0 && i <= g.nx && j <= g.ny;
+  const int sk = g.sJ * g.sK;
+  float un[kUvLevels], vn[kUvLevels], ru[kUvLevels], rv[kUvLevels];
+#pragma unroll
+  for (int q = 0; q < kUvLevels; q++) {
+    const int k = k0 + q;
+    if (k > g.nz) break;
+    const int c = gidx(g, i, j, 0) + k * sk;
+    un[q] = upd && k < g.nz ? uv_u(A, i, j, c) : A.u[c];
+    vn[q] = upd && k < g.nz ? uv_v(A, i, j, c) : A.v[c];
+    ru[q] = A.rru[c];
+    rv[q] = A.rrv[c];
   }
-  if (A.tavg > 0.0f) {
-    A.rru[c] = (A.rru[c] + un) * A.tavg;
-    A.rrv[c] = (A.rrv[c] + vn) * A.tavg;
-  } else {
-    A.rru[c] = A.rru[c] + un;
-    A.rrv[c] = A.rrv[c] + vn;
+#pragma unroll
+  for (int q = 0; q < kUvLevels; q++) {
+    const int k = k0 + q;
+    if (k > g.nz) break;
+    const int c = gidx(g, i, j, 0) + k * sk;
+    if (upd && k < g.nz) {
+      A.u[c] = un[q];
+      A.v[c] = vn[q];
+    }
+    if (A.tavg > 0.0f) {
+      A.rru[c] = (ru[q] + un[q]) * A.tavg;
+      A.rrv[c] = (rv[q] + vn[q]) * A.tavg;
+    } else {
+      A.rru[c] = ru[q] + un[q];
+      A.rrv[c] = rv[q] + vn[q];
+    }
   }
 }
 
@@ -421,52 +440,62 @@ constexpr int kAdvTX = 32, kAdvTY = 8;
 
 // ST = |stagger| of the advected variable: cell (i, j, k) takes the faces i + dx and
 // i + dx + 1 (dx = -1 along its own staggered axis, else 0), likewise in j and k.  A CTA
-// covers a 32 x 8 tile of one level: the 33 x 8 x-faces and 32 x 9 y-faces of the tile
-// are computed once into shared memory (the faces beyond 256 by warps 0 and 1), each
-// cell computes its two z-faces, then assembles.
+// covers a 32 x 8 tile of KZ consecutive levels and walks up them: per level the
+// 33 x 8 x-faces and 32 x 9 y-faces of the tile are computed once into shared memory
+// (double-buffered, one barrier per level; the faces beyond 256 by warps 0 and 1), and
+// each cell computes the z-face above it, reusing the one below from the level before.
+// KZ = 4 where the z-face is a WENO reconstruction (momentum WENO: the saved face pays
+// for the shorter grid); KZ = 1 (most parallel) where faces are cheap.
+template <int KIND>
+struct AdvKZ {
+  static constexpr int value = KIND == kWenoUV || KIND == kWenoW ? 4 : 1;
+};
+
 template <int KIND, int ST>
-__global__ void __launch_bounds__(kAdvTX* kAdvTY) k_adv_fused(AdvArgs A) {
-  __shared__ float fxs[kAdvTY][kAdvTX + 1];
-  __shared__ float fys[kAdvTY + 1][kAdvTX];
+__global__ void __launch_bounds__(kAdvTX* kAdvTY, AdvKZ<KIND>::value > 1 ? 6 : (KIND == kWeno ? 7 : 8)) k_adv_fused(AdvArgs A) {
+  constexpr int kAdvKZ = AdvKZ<KIND>::value;
+  __shared__ float fxs[2][kAdvTY][kAdvTX + 1];
+  __shared__ float fys[2][kAdvTY + 1][kAdvTX];
   constexpr int dx = ST == 2 ? -1 : 0, dy = ST == 3 ? -1 : 0, dz = ST == 4 ? -1 : 0;
   const int lx = threadIdx.x, ly = threadIdx.y, t = ly * kAdvTX + lx;
   const int i0 = A.ilo + (int)blockIdx.x * kAdvTX, j0 = A.jlo + (int)blockIdx.y * kAdvTY;
-  const int i = i0 + lx, j = j0 + ly, k = A.klo + (int)blockIdx.z;
-  {
-    const int r = t / (kAdvTX + 1), q = t % (kAdvTX + 1);
-    if (in_range(A.rx, i0 + dx + q, j0 + r, k)) fxs[r][q] = adv_face<KIND, 0>(A.fx, i0 + dx + q, j0 + r, k);
-  }
-  if (in_range(A.ry, i, j0 + dy + ly, k)) fys[ly][lx] = adv_face<KIND, 1>(A.fy, i, j0 + dy + ly, k);
-  if (ly == 0 && lx < kAdvTY) {  // x-faces 256..263 (row-major [8][33]): the tail of row 7
-    const int e = kAdvTX * kAdvTY + lx, r = e / (kAdvTX + 1), q = e % (kAdvTX + 1);
-    if (in_range(A.rx, i0 + dx + q, j0 + r, k)) fxs[r][q] = adv_face<KIND, 0>(A.fx, i0 + dx + q, j0 + r, k);
-  }
-  if (ly == 1 && in_range(A.ry, i, j0 + dy + kAdvTY, k)) fys[kAdvTY][lx] = adv_face<KIND, 1>(A.fy, i, j0 + dy + kAdvTY, k);
+  const int i = i0 + lx, j = j0 + ly;
+  const int kb = A.klo + (int)blockIdx.z * kAdvKZ, ke = min(A.khi, kb + kAdvKZ - 1);
   const bool cell = i <= A.ihi && j <= A.jhi;
-  float fz0 = 0.0f, fz1 = 0.0f;
-  if (cell) {
-    fz0 = adv_face<KIND, 2>(A.fz, i, j, k + dz);
-    fz1 = adv_face<KIND, 2>(A.fz, i, j, k + dz + 1);
-  }
-  __syncthreads();
-  if (!cell) return;
-  const int c = gidx(A.as.g, i, j, k);
-  const float dFx = fxs[ly][lx + 1] - fxs[ly][lx];
-  const float dFy = fys[ly + 1][lx] - fys[ly][lx];
-  float tn = assemble_t(A.as, i, j, k, c, dFx, dFy, fz1 - fz0);
-  if (A.accumulate) {
-    A.dest[c] = A.dest[c] + tn;
-  } else {
-    if (A.thterm) tn = fmaf(-A.div3d[c], A.thterm[c], tn);   // apply_thterm.wgsl
-    if (A.write_dest) A.dest[c] = tn;
-    if (A.phi) A.phi[c] = fmaf(A.dttmp, tn, A.phiA[c]);      // rk_update.wgsl
+  const int xr = t / (kAdvTX + 1), xq = t % (kAdvTX + 1);                       // x-face of this thread
+  const int e2 = kAdvTX * kAdvTY + lx, xr2 = e2 / (kAdvTX + 1), xq2 = e2 % (kAdvTX + 1);  // 256..263, warp 0
+  float fzb = cell ? adv_face<KIND, 2>(A.fz, i, j, kb + dz) : 0.0f;
+  for (int k = kb, b = 0; k <= ke; k++, b ^= 1) {
+    if (in_range(A.rx, i0 + dx + xq, j0 + xr, k)) fxs[b][xr][xq] = adv_face<KIND, 0>(A.fx, i0 + dx + xq, j0 + xr, k);
+    if (in_range(A.ry, i, j0 + dy + ly, k)) fys[b][ly][lx] = adv_face<KIND, 1>(A.fy, i, j0 + dy + ly, k);
+    if (ly == 0 && lx < kAdvTY && in_range(A.rx, i0 + dx + xq2, j0 + xr2, k))
+      fxs[b][xr2][xq2] = adv_face<KIND, 0>(A.fx, i0 + dx + xq2, j0 + xr2, k);
+    if (ly == 1 && in_range(A.ry, i, j0 + dy + kAdvTY, k))
+      fys[b][kAdvTY][lx] = adv_face<KIND, 1>(A.fy, i, j0 + dy + kAdvTY, k);
+    const float fzt = cell ? adv_face<KIND, 2>(A.fz, i, j, k + dz + 1) : 0.0f;
+    __syncthreads();
+    if (cell) {
+      const int c = gidx(A.as.g, i, j, k);
+      const float dFx = fxs[b][ly][lx + 1] - fxs[b][ly][lx];
+      const float dFy = fys[b][ly + 1][lx] - fys[b][ly][lx];
+      float tn = assemble_t(A.as, i, j, k, c, dFx, dFy, fzt - fzb);
+      if (A.accumulate) {
+        A.dest[c] = A.dest[c] + tn;
+      } else {
+        if (A.thterm) tn = fmaf(-A.div3d[c], A.thterm[c], tn);   // apply_thterm.wgsl
+        if (A.write_dest) A.dest[c] = tn;
+        if (A.phi) A.phi[c] = fmaf(A.dttmp, tn, A.phiA[c]);      // rk_update.wgsl
+      }
+    }
+    fzb = fzt;
   }
 }
 
 template <int KIND, int ST>
 static void launch_adv_t(const AdvArgs& A, cudaStream_t s) {
   const dim3 b(kAdvTX, kAdvTY, 1);
-  const dim3 gr((A.ihi - A.ilo + kAdvTX) / kAdvTX, (A.jhi - A.jlo + kAdvTY) / kAdvTY, A.khi - A.klo + 1);
+  constexpr int kz = AdvKZ<KIND>::value;
+  const dim3 gr((A.ihi - A.ilo + kAdvTX) / kAdvTX, (A.jhi - A.jlo + kAdvTY) / kAdvTY, (A.khi - A.klo + kz) / kz);
   k_adv_fused<KIND, ST><<<gr, b, 0, s>>>(A);
 }
 
@@ -865,7 +894,7 @@ void FusedStep::launch_segment(Plan& P, std::vector<Op>& ops, int seg, int part)
     const AcuArgs& A = D.acu[s.aux[0]];
     const Dims& g = A.g;
     if (part < 0 || part == 0) {
-      dim3 b(32, 8, 1), gr((g.sJ + 31) / 32, (g.sK + 7) / 8, g.nz + 1);
+      dim3 b(32, 8, 1), gr((g.sJ + 31) / 32, (g.sK + 7) / 8, (g.nz + kUvLevels) / kUvLevels);
       k_acu_uv<<<gr, b, 0, P.stream>>>(A);
     }
     if (part < 0 || part == 1) launch_acu_column(A, P.stream);
