@@ -37,15 +37,21 @@ __device__ __forceinline__ float weno5_upwind(const float* a, int c, int s, bool
   return weno5(sten5(a, c, s, up, shifted ? 1 : 0), weps);
 }
 
+// Horizontal faces come in two forms: face_X_h_at reads the advected field's stencil
+// through (a, ca, sa) - values a[ca + n * sa] along the face's axis - so that a caller
+// may stage the field elsewhere (shared memory); face_X_h reads it from the tape field.
+template <int DIR>
+__device__ __forceinline__ float face_lin_h_at(const KArgs& A, int i, int j, int k, const float* a, int ca, int sa) {
+  const Dims& g = A.g;
+  const float* rr = A.p[2];
+  int c = gidx(g, i, j, k);
+  float u = rr[c];
+  float f = flx5(sten5(a, ca, sa, u >= 0.0f, 0));
+  return u * f;
+}
 template <int DIR>
 __device__ __forceinline__ float face_lin_h(const KArgs& A, int i, int j, int k) {
-  const Dims& g = A.g;
-  const float *s = A.p[1], *rr = A.p[2];
-  int c = gidx(g, i, j, k);
-  const int d = DIR == 0 ? 1 : g.sJ;
-  float u = rr[c];
-  float f = flx5(sten5(s, c, d, u >= 0.0f, 0));
-  return u * f;
+  return face_lin_h_at<DIR>(A, i, j, k, A.p[1], gidx(A.g, i, j, k), DIR == 0 ? 1 : A.g.sJ);
 }
 
 __device__ __forceinline__ float face_lin_z(const KArgs& A, int i, int j, int k) {
@@ -68,10 +74,10 @@ __device__ __forceinline__ float face_lin_z(const KArgs& A, int i, int j, int k)
 }
 
 template <int DIR>
-__device__ __forceinline__ float face_stag_h(const KArgs& A, int i, int j, int k) {
+__device__ __forceinline__ float face_stag_h_at(const KArgs& A, int i, int j, int k, const float* a, int ca, int sa) {
   const Dims& g = A.g;
   const int stag = A.iv[1];
-  const float *a = A.p[2], *rr = DIR == 0 ? A.p[3] : A.p[4], *c2 = A.p[7];
+  const float *rr = DIR == 0 ? A.p[3] : A.p[4], *c2 = A.p[7];
   const int sj = g.sJ, sk = g.sJ * g.sK;
   int c = gidx(g, i, j, k);
   if (stag == 4 && k == 0) {
@@ -83,14 +89,18 @@ __device__ __forceinline__ float face_stag_h(const KArgs& A, int i, int j, int k
     else if (stag == 3) m = 0.5f * (rr[c] + rr[c - sj]);
     else if (stag == 4) { float cc2 = c2[k]; m = fmaf(cc2, rr[c], (1.0f - cc2) * rr[c - sk]); }
     else m = rr[c];
-    return m * flx5_upwind(a, c, 1, m >= 0.0f, stag == 2);
+    return m * flx5_upwind(a, ca, sa, m >= 0.0f, stag == 2);
   } else {
     if (stag == 2) m = 0.5f * (rr[c] + rr[c - 1]);
     else if (stag == 3) m = 0.5f * (rr[c] + rr[c + sj]);
     else if (stag == 4) { float cc2 = c2[k]; m = fmaf(cc2, rr[c], (1.0f - cc2) * rr[c - sk]); }
     else m = rr[c];
-    return m * flx5_upwind(a, c, sj, m >= 0.0f, stag == 3);
+    return m * flx5_upwind(a, ca, sa, m >= 0.0f, stag == 3);
   }
+}
+template <int DIR>
+__device__ __forceinline__ float face_stag_h(const KArgs& A, int i, int j, int k) {
+  return face_stag_h_at<DIR>(A, i, j, k, A.p[2], gidx(A.g, i, j, k), DIR == 0 ? 1 : A.g.sJ);
 }
 
 __device__ __forceinline__ float face_stag_z(const KArgs& A, int i, int j, int k) {
@@ -128,19 +138,20 @@ __device__ __forceinline__ float face_stag_z(const KArgs& A, int i, int j, int k
 }
 
 template <int DIR>
-__device__ __forceinline__ float face_weno_h(const KArgs& A, int i, int j, int k) {
+__device__ __forceinline__ float face_weno_h_at(const KArgs& A, int i, int j, int k, const float* a, int ca, int sa) {
   const Dims& g = A.g;
-  const float *a = A.p[1], *rr = A.p[2];
+  const float* rr = A.p[2];
   const float weps = A.f[3];
   const int pdef = A.iv[4];
   int c = gidx(g, i, j, k);
-  const int d = DIR == 0 ? 1 : g.sJ;
-  float s1, s2, s3, s4, s5;
   float r = rr[c];
-  if (r >= 0.0f) { s1 = a[c - 3 * d]; s2 = a[c - 2 * d]; s3 = a[c - d]; s4 = a[c]; s5 = a[c + d]; }
-  else { s1 = a[c + 2 * d]; s2 = a[c + d]; s3 = a[c]; s4 = a[c - d]; s5 = a[c - 2 * d]; }
-  bool ok = pdef != 1 || weno_pdef_ok(s1, s2, s3, s4, s5, weps);
-  return ok ? r * weno5(s1, s2, s3, s4, s5, weps) : 0.0f;
+  const Sten5 t = sten5(a, ca, sa, r >= 0.0f, 0);
+  bool ok = pdef != 1 || weno_pdef_ok(t.s1, t.s2, t.s3, t.s4, t.s5, weps);
+  return ok ? r * weno5(t, weps) : 0.0f;
+}
+template <int DIR>
+__device__ __forceinline__ float face_weno_h(const KArgs& A, int i, int j, int k) {
+  return face_weno_h_at<DIR>(A, i, j, k, A.p[1], gidx(A.g, i, j, k), DIR == 0 ? 1 : A.g.sJ);
 }
 
 __device__ __forceinline__ float face_weno_z(const KArgs& A, int i, int j, int k) {
@@ -187,20 +198,24 @@ __device__ __forceinline__ float face_weno_z(const KArgs& A, int i, int j, int k
 }
 
 template <int DIR>
-__device__ __forceinline__ float face_weno_uv_h(const KArgs& A, int i, int j, int k) {
+__device__ __forceinline__ float face_weno_uv_h_at(const KArgs& A, int i, int j, int k, const float* a, int ca, int sa) {
   const Dims& g = A.g;
   const int stag = A.iv[1];
-  const float *a = A.p[2], *rr = A.p[3];
+  const float* rr = A.p[3];
   const float weps = A.f[4];
   const int sj = g.sJ;
   int c = gidx(g, i, j, k);
   if (DIR == 0) {
     float m = stag == 2 ? 0.5f * (rr[c] + rr[c + 1]) : 0.5f * (rr[c] + rr[c - sj]);
-    return m * weno5_upwind(a, c, 1, m >= 0.0f, stag == 2, weps);
+    return m * weno5_upwind(a, ca, sa, m >= 0.0f, stag == 2, weps);
   } else {
     float m = stag == 2 ? 0.5f * (rr[c] + rr[c - 1]) : 0.5f * (rr[c] + rr[c + sj]);
-    return m * weno5_upwind(a, c, sj, m >= 0.0f, stag == 3, weps);
+    return m * weno5_upwind(a, ca, sa, m >= 0.0f, stag == 3, weps);
   }
+}
+template <int DIR>
+__device__ __forceinline__ float face_weno_uv_h(const KArgs& A, int i, int j, int k) {
+  return face_weno_uv_h_at<DIR>(A, i, j, k, A.p[2], gidx(A.g, i, j, k), DIR == 0 ? 1 : A.g.sJ);
 }
 
 __device__ __forceinline__ float face_weno_uv_z(const KArgs& A, int i, int j, int k) {
@@ -227,20 +242,23 @@ __device__ __forceinline__ float face_weno_uv_z(const KArgs& A, int i, int j, in
 }
 
 template <int DIR>
-__device__ __forceinline__ float face_weno_w_h(const KArgs& A, int i, int j, int k) {
+__device__ __forceinline__ float face_weno_w_h_at(const KArgs& A, int i, int j, int k, const float* a, int ca, int sa) {
   const Dims& g = A.g;
-  const float *a = A.p[1], *rr = A.p[2], *c2 = A.p[3];
+  const float *rr = A.p[2], *c2 = A.p[3];
   const float weps = A.f[4];
   const int sk = g.sJ * g.sK;
   int c = gidx(g, i, j, k);
   if (k == 0) {
     return 0.0f;
   }
-  const int d = DIR == 0 ? 1 : g.sJ;
   float cc2 = c2[k];
   float cc1 = 1.0f - cc2;
   float ub = fmaf(cc2, rr[c], cc1 * rr[c - sk]);
-  return ub * weno5(sten5(a, c, d, ub >= 0.0f, 0), weps);
+  return ub * weno5(sten5(a, ca, sa, ub >= 0.0f, 0), weps);
+}
+template <int DIR>
+__device__ __forceinline__ float face_weno_w_h(const KArgs& A, int i, int j, int k) {
+  return face_weno_w_h_at<DIR>(A, i, j, k, A.p[1], gidx(A.g, i, j, k), DIR == 0 ? 1 : A.g.sJ);
 }
 
 __device__ __forceinline__ float face_weno_w_z(const KArgs& A, int i, int j, int k) {
