@@ -227,12 +227,14 @@ __global__ void __launch_bounds__(kColThreads, 2) k_acu_column(AcuArgs A) {
   const int npass = (nz + kLevels - 1) / kLevels;
   float cAm = 0.0f, cBm = 0.0f, wtop = 0.0f;  // recurrence state (warp kLevels)
   const float uh = hm_uh(g, A.hm, col ? i : 0), vh = hm_vh(g, A.hm, j);
+  // the next pass's inputs are loaded into `cur` as soon as this pass's have been
+  // consumed, so they are in flight across the barriers and the recurrence
+  LevelIn cur;
+  if (worker && col && q < nz) cur = load_level(A, c0 + q * sk);
   for (int p = 0; p <= npass; p++) {
     if (worker) {
       if (p < npass) {
         const int k = p * kLevels + q;
-        LevelIn cur;
-        if (col && k < nz) cur = load_level(A, c0 + k * sk);
         if (col && k < nz) {
           const float fk = fpk_of(A, cur, uh, vh);
           const int e = k * kColTile + lane;
@@ -241,16 +243,17 @@ __global__ void __launch_bounds__(kColThreads, 2) k_acu_column(AcuArgs A) {
           S.prev[e] = cur.pp;
           S.s[e] = cur.pp + fk;
         }
+        const float m = cur.mm, wt = cur.wt, w0 = cur.w0;
+        if (col && k + kLevels < nz) cur = load_level(A, c0 + (k + kLevels) * sk);
         workers_sync();
         if (col && k < nz && k >= 1) {
           const int e = k * kColTile + lane, em = e - kColTile;
-          const float m = cur.mm;
           const int b = p & 1;
           S.co[co_at(b, 0, q, lane)] = (-asq) * (m * S.A[em]);
           S.co[co_at(b, 2, q, lane)] = (-asq) * ((-m) * S.Bq[e]);
           S.co[co_at(b, 1, q, lane)] = fmaf(-asq, m * ((-S.A[e]) + S.Bq[em]), 1.0f);
-          const float fw = fmaf(a.dts, cur.wt, a.beta * ((-m) * (S.prev[e] - S.prev[em])));
-          S.co[co_at(b, 3, q, lane)] = fmaf(a.alph, (-m) * (S.s[e] - S.s[em]), cur.w0 + fw);
+          const float fw = fmaf(a.dts, wt, a.beta * ((-m) * (S.prev[e] - S.prev[em])));
+          S.co[co_at(b, 3, q, lane)] = fmaf(a.alph, (-m) * (S.s[e] - S.s[em]), w0 + fw);
         }
       }
     } else if (p >= 1 && col) {
@@ -416,7 +419,6 @@ struct AdvArgs {
   int ilo, ihi, jlo, jhi, klo, khi;  // cells adv_assemble writes
   FaceRange rx, ry, rz;              // faces each flux dispatch produces
   int accumulate, write_dest;
-  const float* src;                  // the advected field
   float* dest;                       // adv_assemble's tendency output
   const float *div3d, *thterm;       // apply_thterm (null if not fused)
   const float* phiA;                 // rk_update (null if not fused)
@@ -433,16 +435,6 @@ __device__ __forceinline__ float adv_face(const KArgs& A, int i, int j, int k) {
   return DIR == 2 ? face_weno_w_z(A, i, j, k) : face_weno_w_h<DIR>(A, i, j, k);
 }
 
-// horizontal face with the advected field's stencil read from (a, ca, sa)
-template <int KIND, int DIR>
-__device__ __forceinline__ float adv_face_at(const KArgs& A, int i, int j, int k, const float* a, int ca, int sa) {
-  if (KIND == kLin) return face_lin_h_at<DIR>(A, i, j, k, a, ca, sa);
-  if (KIND == kStag) return face_stag_h_at<DIR>(A, i, j, k, a, ca, sa);
-  if (KIND == kWeno) return face_weno_h_at<DIR>(A, i, j, k, a, ca, sa);
-  if (KIND == kWenoUV) return face_weno_uv_h_at<DIR>(A, i, j, k, a, ca, sa);
-  return face_weno_w_h_at<DIR>(A, i, j, k, a, ca, sa);
-}
-
 __device__ __forceinline__ bool in_range(const FaceRange& r, int i, int j, int k) {
   return i >= r.ilo && i <= r.ihi && j >= r.jlo && j <= r.jhi && k >= r.klo && k <= r.khi;
 }
@@ -451,29 +443,23 @@ constexpr int kAdvTX = 32, kAdvTY = 8;
 
 // ST = |stagger| of the advected variable: cell (i, j, k) takes the faces i + dx and
 // i + dx + 1 (dx = -1 along its own staggered axis, else 0), likewise in j and k.  A CTA
-// covers a 32 x 8 tile of KZ consecutive levels and walks up them.  Per level the
-// advected field of the tile and a 4-point rim is staged in shared memory (the next
-// level's while this one's faces are computed), the 33 x 8 x-faces and 32 x 9 y-faces
-// read their stencils from there and land in shared memory, and each cell computes the
-// z-face above it, reusing the one below from the level before.  Stencils of the faces
-// the tape computes lie inside the field ([-3, nx + 3] x [-3, ny + 3]); rim points
-// outside it are not loaded and not read.
+// covers a 32 x 8 tile of KZ consecutive levels and walks up them: per level the
+// 33 x 8 x-faces and 32 x 9 y-faces of the tile are computed once into shared memory
+// (double-buffered, one barrier per level; the faces beyond 256 by warps 0 and 1), and
+// each cell computes the z-face above it, reusing the one below from the level before.
 // KZ = 4 where the z-face is a WENO reconstruction (momentum WENO: the saved face pays
 // for the shorter grid); KZ = 1 (most parallel) where faces are cheap.
 template <int KIND>
 struct AdvKZ {
   static constexpr int value = KIND == kWenoUV || KIND == kWenoW ? 4 : 1;
 };
-constexpr int kRim = 4, kSW = kAdvTX + 2 * kRim, kSH = kAdvTY + 2 * kRim;
 
 template <int KIND, int ST>
 __global__ void __launch_bounds__(kAdvTX* kAdvTY, AdvKZ<KIND>::value > 1 ? 6 : (KIND == kWeno ? 7 : 8)) k_adv_fused(AdvArgs A) {
   constexpr int kAdvKZ = AdvKZ<KIND>::value;
-  __shared__ float at[2][kSH * kSW];
   __shared__ float fxs[2][kAdvTY][kAdvTX + 1];
   __shared__ float fys[2][kAdvTY + 1][kAdvTX];
   constexpr int dx = ST == 2 ? -1 : 0, dy = ST == 3 ? -1 : 0, dz = ST == 4 ? -1 : 0;
-  const Dims& g = A.as.g;
   const int lx = threadIdx.x, ly = threadIdx.y, t = ly * kAdvTX + lx;
   const int i0 = A.ilo + (int)blockIdx.x * kAdvTX, j0 = A.jlo + (int)blockIdx.y * kAdvTY;
   const int i = i0 + lx, j = j0 + ly;
@@ -481,30 +467,18 @@ __global__ void __launch_bounds__(kAdvTX* kAdvTY, AdvKZ<KIND>::value > 1 ? 6 : (
   const bool cell = i <= A.ihi && j <= A.jhi;
   const int xr = t / (kAdvTX + 1), xq = t % (kAdvTX + 1);                       // x-face of this thread
   const int e2 = kAdvTX * kAdvTY + lx, xr2 = e2 / (kAdvTX + 1), xq2 = e2 % (kAdvTX + 1);  // 256..263, warp 0
-  auto stage = [&](int k, int b) {
-    for (int e = t; e < kSH * kSW; e += kAdvTX * kAdvTY) {
-      const int gi = i0 - kRim + e % kSW, gj = j0 - kRim + e / kSW;
-      if (gi >= -3 && gi <= g.nx + 3 && gj >= -3 && gj <= g.ny + 3) at[b][e] = A.src[gidx(g, gi, gj, k)];
-    }
-  };
-  stage(kb, 0);
   float fzb = cell ? adv_face<KIND, 2>(A.fz, i, j, kb + dz) : 0.0f;
-  __syncthreads();
   for (int k = kb, b = 0; k <= ke; k++, b ^= 1) {
-    const float* a = at[b];
-    if (in_range(A.rx, i0 + dx + xq, j0 + xr, k))
-      fxs[b][xr][xq] = adv_face_at<KIND, 0>(A.fx, i0 + dx + xq, j0 + xr, k, a, (xr + kRim) * kSW + dx + xq + kRim, 1);
-    if (in_range(A.ry, i, j0 + dy + ly, k))
-      fys[b][ly][lx] = adv_face_at<KIND, 1>(A.fy, i, j0 + dy + ly, k, a, (dy + ly + kRim) * kSW + lx + kRim, kSW);
+    if (in_range(A.rx, i0 + dx + xq, j0 + xr, k)) fxs[b][xr][xq] = adv_face<KIND, 0>(A.fx, i0 + dx + xq, j0 + xr, k);
+    if (in_range(A.ry, i, j0 + dy + ly, k)) fys[b][ly][lx] = adv_face<KIND, 1>(A.fy, i, j0 + dy + ly, k);
     if (ly == 0 && lx < kAdvTY && in_range(A.rx, i0 + dx + xq2, j0 + xr2, k))
-      fxs[b][xr2][xq2] = adv_face_at<KIND, 0>(A.fx, i0 + dx + xq2, j0 + xr2, k, a, (xr2 + kRim) * kSW + dx + xq2 + kRim, 1);
+      fxs[b][xr2][xq2] = adv_face<KIND, 0>(A.fx, i0 + dx + xq2, j0 + xr2, k);
     if (ly == 1 && in_range(A.ry, i, j0 + dy + kAdvTY, k))
-      fys[b][kAdvTY][lx] = adv_face_at<KIND, 1>(A.fy, i, j0 + dy + kAdvTY, k, a, (dy + kAdvTY + kRim) * kSW + lx + kRim, kSW);
+      fys[b][kAdvTY][lx] = adv_face<KIND, 1>(A.fy, i, j0 + dy + kAdvTY, k);
     const float fzt = cell ? adv_face<KIND, 2>(A.fz, i, j, k + dz + 1) : 0.0f;
-    if (k < ke) stage(k + 1, b ^ 1);
     __syncthreads();
     if (cell) {
-      const int c = gidx(g, i, j, k);
+      const int c = gidx(A.as.g, i, j, k);
       const float dFx = fxs[b][ly][lx + 1] - fxs[b][ly][lx];
       const float dFy = fys[b][ly + 1][lx] - fys[b][ly][lx];
       float tn = assemble_t(A.as, i, j, k, c, dFx, dFy, fzt - fzb);
@@ -686,7 +660,6 @@ static bool match_advect(const std::vector<Op>& ops, size_t i, uint32_t* M, Fuse
   if (!covers(A.ry, A.ilo, A.ihi, A.jlo + dy, A.jhi + dy + 1, A.klo, A.khi)) return false;
   if (!covers(A.rz, A.ilo, A.ihi, A.jlo, A.jhi, A.klo + dz, A.khi + dz + 1)) return false;
   A.accumulate = oa.args.iv[12] != 0;
-  A.src = src;
   A.dest = oa.args.p[11];
   A.write_dest = 1;
   // fields the kernel reads at other cells than the one it writes: nothing it writes may
