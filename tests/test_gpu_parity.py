@@ -199,3 +199,26 @@ def test_fused_mode_matches_oracle_small_config():
 
 def test_fused_mode_odd_sizes_nsound8():
     _fused_vs_oracle(scenario.tiny(37, 29, 13, dx=500.0, dz=250.0, dt=3.0, nsound=8, us=25.0), nsteps=2)
+
+
+def test_aliased_bindings_keep_program_order():
+    """A tape may bind one field to several parameters of a dispatch.  Here
+    stage_state_reset reads v's source from the u it has just written (va := u), so a
+    thread that loaded every input before storing would read the old u; the player must
+    run the dispatch with the ordering the reference kernel has (u first, then v = u)."""
+    run = timestep.Run(scenario.tiny(16, 12, 10))
+    tape = run.tape(1)
+    arena = run.rec.ids['arena']
+    cmds = tape['steps'][0]
+    pipe, changed = None, 0
+    for c in cmds:
+        if c['op'] == 'pipe':
+            pipe = c['name']
+        elif c['op'] == 'buf' and pipe == 'stage_state_reset' and c['index'] == 2 and c['buf'] == arena:
+            c['offset'] = run.fields['u']
+            changed += 1
+    assert changed >= 1
+    init = run.initial_buffers()
+    cpu, gpu, mem = _compare(run, tape, init, nsteps=1)
+    assert np.array_equal(gpu.read_hashes(), cpu.hashes[:gpu.hash_count])
+    assert np.array_equal(mem, cpu.M[:gpu.buffers_end])

@@ -227,24 +227,23 @@ __global__ void __launch_bounds__(kColThreads, 2) k_acu_column(AcuArgs A) {
   const int npass = (nz + kLevels - 1) / kLevels;
   float cAm = 0.0f, cBm = 0.0f, wtop = 0.0f;  // recurrence state (warp kLevels)
   const float uh = hm_uh(g, A.hm, col ? i : 0), vh = hm_vh(g, A.hm, j);
-  // the next pass's inputs are loaded into `cur` as soon as this pass's have been
-  // consumed, so they are in flight across the barriers and the recurrence
-  LevelIn cur;
-  if (worker && col && q < nz) cur = load_level(A, c0 + q * sk);
   for (int p = 0; p <= npass; p++) {
     if (worker) {
       if (p < npass) {
         const int k = p * kLevels + q;
+        float m = 0.0f, wt = 0.0f, w0 = 0.0f;
         if (col && k < nz) {
+          const LevelIn cur = load_level(A, c0 + k * sk);
           const float fk = fpk_of(A, cur, uh, vh);
           const int e = k * kColTile + lane;
           S.A[e] = cur.pk1 + cur.qk;
           S.Bq[e] = cur.pk2 - cur.qk;
           S.prev[e] = cur.pp;
           S.s[e] = cur.pp + fk;
+          m = cur.mm;
+          wt = cur.wt;
+          w0 = cur.w0;
         }
-        const float m = cur.mm, wt = cur.wt, w0 = cur.w0;
-        if (col && k + kLevels < nz) cur = load_level(A, c0 + (k + kLevels) * sk);
         workers_sync();
         if (col && k < nz && k >= 1) {
           const int e = k * kColTile + lane, em = e - kColTile;

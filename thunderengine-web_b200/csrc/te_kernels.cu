@@ -14,7 +14,18 @@
 #include "te_kernels.cuh"
 #include "te_math.cuh"
 
+// TE_R qualifies every field pointer a kernel takes from its bindings.  Built as is it
+// is empty; te_kernels_fast.cu compiles this file again with TE_R = __restrict__ into
+// te::fast, which the player uses for ops whose bound regions do not overlap (the
+// compiler may then issue all of a thread's loads before its stores).
+#ifndef TE_R
+#define TE_R
+#endif
+
 namespace te {
+#ifdef TE_KERNELS_FAST
+namespace fast {
+#endif
 
 #define TE_K3                                                   \
   const int tx = blockIdx.x * blockDim.x + threadIdx.x;         \
@@ -139,8 +150,8 @@ TE_LAUNCH3(adv_flux_z_weno_w)
 __global__ void k_adv_assemble(KArgs A) {
   TE_K3
   const int stag = A.iv[1];
-  const float *fx = A.p[3], *fy = A.p[4], *fz = A.p[5];
-  float* tend = A.p[11];
+  const float *TE_R fx = A.p[3], *TE_R fy = A.p[4], *TE_R fz = A.p[5];
+  float* TE_R tend = A.p[11];
   const int accumulate = A.iv[12];
   const int openx = A.iv[17], openy = A.iv2[17];
   const int sj = g.sJ, sk = g.sJ * g.sK;
@@ -163,8 +174,8 @@ TE_LAUNCH3(adv_assemble)
 __global__ void k_rk_update(KArgs A) {
   TE_K3
   const int stag = A.iv[1];
-  const float *phiA = A.p[2], *tend = A.p[3];
-  float* phi = A.p[4];
+  const float *TE_R phiA = A.p[2], *TE_R tend = A.p[3];
+  float* TE_R phi = A.p[4];
   const float dttmp = A.f[5];
   const int iMax = stag == 2 ? g.nx : g.nx - 1, jMax = stag == 3 ? g.ny : g.ny - 1, kLo = stag == 4 ? 1 : 0;
   int i = tx, j = ty, k = tz;
@@ -189,11 +200,11 @@ __device__ __forceinline__ bool pdef_inflow(const Dims& g, int dir, int i, int j
 __global__ void k_pdef_dum(KArgs A) {
   TE_K3
   const int dir = A.iv[1];
-  const float *s = A.p[2], *s0 = A.p[3], *f = A.p[4], *rr = A.p[5], *rho0 = A.p[6], *mh = A.p[7];
+  const float *TE_R s = A.p[2], *TE_R s0 = A.p[3], *TE_R f = A.p[4], *TE_R rr = A.p[5], *TE_R rho0 = A.p[6], *TE_R mh = A.p[7];
   const float dt = A.f[8];
   const int ox = A.iv[9], oy = A.iv2[9];
-  float* dum = A.p[10];
-  const float* hm = A.p[30];
+  float* TE_R dum = A.p[10];
+  const float* TE_R hm = A.p[30];
   int i = tx, j = ty, k = tz;
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
   int c = gidx(g, i, j, k);
@@ -242,13 +253,13 @@ __device__ __forceinline__ float pdef_mass(float dm2, float dm1, float d0, float
 
 __global__ void k_pdef_apply(KArgs A) {
   TE_K3
-  const float *s = A.p[1], *s0 = A.p[2], *fx = A.p[3], *fy = A.p[4], *fz = A.p[5];
-  const float *rru = A.p[6], *rrv = A.p[7], *rrw = A.p[8], *dumx = A.p[9], *dumy = A.p[10], *dumz = A.p[11];
-  const float *rho0 = A.p[12], *mh = A.p[13];
+  const float *TE_R s = A.p[1], *TE_R s0 = A.p[2], *TE_R fx = A.p[3], *TE_R fy = A.p[4], *TE_R fz = A.p[5];
+  const float *TE_R rru = A.p[6], *TE_R rrv = A.p[7], *TE_R rrw = A.p[8], *TE_R dumx = A.p[9], *TE_R dumy = A.p[10], *TE_R dumz = A.p[11];
+  const float *TE_R rho0 = A.p[12], *TE_R mh = A.p[13];
   const float dt = A.f[14];
   const int ox = A.iv[15], oy = A.iv2[15];
-  float* tend = A.p[16];
-  const float* hm = A.p[30];
+  float* TE_R tend = A.p[16];
+  const float* TE_R hm = A.p[30];
   const int sj = g.sJ, sk = g.sJ * g.sK;
   int i = tx, j = ty, k = tz;
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
@@ -295,8 +306,8 @@ TE_LAUNCH3(pdef_apply)
 
 __global__ void k_build_sadv(KArgs A) {
   TE_K3
-  const float *th0 = A.p[1], *thp = A.p[2];
-  float* sadv = A.p[3];
+  const float *TE_R th0 = A.p[1], *TE_R thp = A.p[2];
+  float* TE_R sadv = A.p[3];
   TE_WHOLE(k < g.nz)
   sadv[c] = (th0[k] - 300.0f) + thp[c];
 }
@@ -304,8 +315,8 @@ TE_LAUNCH3(build_sadv)
 
 __global__ void k_massflux_from_state(KArgs A) {
   TE_K3
-  const float *u = A.p[1], *v = A.p[2], *w = A.p[3], *rho0 = A.p[4], *rf0 = A.p[5];
-  float *rru = A.p[6], *rrv = A.p[7], *rrw = A.p[8];
+  const float *TE_R u = A.p[1], *TE_R v = A.p[2], *TE_R w = A.p[3], *TE_R rho0 = A.p[4], *TE_R rf0 = A.p[5];
+  float *TE_R rru = A.p[6], *TE_R rrv = A.p[7], *TE_R rrw = A.p[8];
   TE_WHOLE(k <= g.nz)
   if (k < g.nz) {
     rru[c] = rho0[k] * u[c];
@@ -317,9 +328,9 @@ TE_LAUNCH3(massflux_from_state)
 
 __global__ void k_div_massflux(KArgs A) {
   TE_K3
-  const float *rru = A.p[1], *rrv = A.p[2], *rrw = A.p[3], *mh = A.p[4];
-  float* divx = A.p[5];
-  const float* hm = A.p[30];
+  const float *TE_R rru = A.p[1], *TE_R rrv = A.p[2], *TE_R rrw = A.p[3], *TE_R mh = A.p[4];
+  float* TE_R divx = A.p[5];
+  const float* TE_R hm = A.p[30];
   const int sj = g.sJ, sk = g.sJ * g.sK;
   int i = tx - 3, j = ty - 3, k = tz;
   if (i > g.nx + 2 || j > g.ny + 2 || k >= g.nz) return;
@@ -331,8 +342,8 @@ TE_LAUNCH3(div_massflux)
 
 __global__ void k_velocity_to_massflux(KArgs A) {
   TE_K3
-  const float *rho0 = A.p[1], *rf0 = A.p[2];
-  float *rru = A.p[3], *rrv = A.p[4], *rrw = A.p[5];
+  const float *TE_R rho0 = A.p[1], *TE_R rf0 = A.p[2];
+  float *TE_R rru = A.p[3], *TE_R rrv = A.p[4], *TE_R rrw = A.p[5];
   TE_WHOLE(k <= g.nz)
   if (k < g.nz) {
     rru[c] = rru[c] * rho0[k];
@@ -344,9 +355,9 @@ TE_LAUNCH3(velocity_to_massflux)
 
 __global__ void k_stage_state_reset(KArgs A) {
   TE_K3
-  const float *ua = A.p[1], *va = A.p[2], *wa = A.p[3], *ppi = A.p[4];
-  float *u = A.p[5], *v = A.p[6], *w = A.p[7], *pp3d = A.p[8], *ppd = A.p[9];
-  const float* ppx = A.p[10];
+  const float *TE_R ua = A.p[1], *TE_R va = A.p[2], *TE_R wa = A.p[3], *TE_R ppi = A.p[4];
+  float *TE_R u = A.p[5], *TE_R v = A.p[6], *TE_R w = A.p[7], *TE_R pp3d = A.p[8], *TE_R ppd = A.p[9];
+  const float* TE_R ppx = A.p[10];
   TE_WHOLE(k <= g.nz)
   u[c] = ua[c];
   v[c] = va[c];
@@ -358,7 +369,7 @@ TE_LAUNCH3(stage_state_reset)
 
 __global__ void k_stage_tendency_reset(KArgs A) {
   TE_K3
-  float *uten = A.p[1], *vten = A.p[2], *wten = A.p[3];
+  float *TE_R uten = A.p[1], *TE_R vten = A.p[2], *TE_R wten = A.p[3];
   TE_WHOLE(k <= g.nz)
   uten[c] = 0.0f;
   vten[c] = 0.0f;
@@ -368,8 +379,8 @@ TE_LAUNCH3(stage_tendency_reset)
 
 __global__ void k_buoyancy_apply(KArgs A) {
   TE_K3
-  const float *buoy = A.p[1], *c1 = A.p[2], *c2 = A.p[3];
-  float* wten = A.p[4];
+  const float *TE_R buoy = A.p[1], *TE_R c1 = A.p[2], *TE_R c2 = A.p[3];
+  float* TE_R wten = A.p[4];
   const int sk = g.sJ * g.sK;
   int i = tx, j = ty, k = tz + 1;
   if (i >= g.nx || j >= g.ny || k > g.nz - 1) return;
@@ -380,8 +391,8 @@ TE_LAUNCH3(buoyancy_apply)
 
 __global__ void k_apply_thterm(KArgs A) {
   TE_K3
-  const float *div = A.p[1], *thterm = A.p[2];
-  float* tend = A.p[3];
+  const float *TE_R div = A.p[1], *TE_R thterm = A.p[2];
+  float* TE_R tend = A.p[3];
   int i = tx, j = ty, k = tz;
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
   int c = gidx(g, i, j, k);
@@ -394,9 +405,9 @@ TE_LAUNCH3(apply_thterm)
 __global__ void k_acoustic_prepare(KArgs A) {
   TE_K3
   const Acoustic a = A.a;
-  const float *ppterm = A.p[2], *piadv = A.p[3], *thv = A.p[4], *rr0 = A.p[5], *rf0 = A.p[6];
-  const float *mh = A.p[7], *mf = A.p[8], *c1 = A.p[9], *c2 = A.p[10];
-  float *qk = A.p[11], *pk1 = A.p[12], *pk2 = A.p[13], *mm = A.p[14];
+  const float *TE_R ppterm = A.p[2], *TE_R piadv = A.p[3], *TE_R thv = A.p[4], *TE_R rr0 = A.p[5], *TE_R rf0 = A.p[6];
+  const float *TE_R mh = A.p[7], *TE_R mf = A.p[8], *TE_R c1 = A.p[9], *TE_R c2 = A.p[10];
+  float *TE_R qk = A.p[11], *TE_R pk1 = A.p[12], *TE_R pk2 = A.p[13], *TE_R mm = A.p[14];
   const int sk = g.sJ * g.sK;
   const float cp = 1005.7f;
   int i = tx, j = ty, k = tz;
@@ -422,8 +433,8 @@ TE_LAUNCH3(acoustic_prepare)
 
 __global__ void k_acoustic_begin(KArgs A) {
   TE_K3
-  const float* w = A.p[2];
-  float *rru = A.p[3], *rrv = A.p[4], *rrw = A.p[5];
+  const float* TE_R w = A.p[2];
+  float *TE_R rru = A.p[3], *TE_R rrv = A.p[4], *TE_R rrw = A.p[5];
   TE_WHOLE(k <= g.nz)
   rru[c] = 0.0f;
   rrv[c] = 0.0f;
@@ -434,10 +445,10 @@ TE_LAUNCH3(acoustic_begin)
 __global__ void k_acoustic_uv(KArgs A) {
   TE_K3
   const Acoustic a = A.a;
-  const float *ppd = A.p[2], *thv = A.p[3], *uten = A.p[4], *vten = A.p[5];
-  float *u = A.p[6], *v = A.p[7];
+  const float *TE_R ppd = A.p[2], *TE_R thv = A.p[3], *TE_R uten = A.p[4], *TE_R vten = A.p[5];
+  float *TE_R u = A.p[6], *TE_R v = A.p[7];
   const int ox = A.iv[8], oy = A.iv2[8];
-  const float* hm = A.p[30];
+  const float* TE_R hm = A.p[30];
   const int sj = g.sJ;
   const float cp = 1005.7f;
   int i = tx, j = ty, k = tz;
@@ -455,10 +466,10 @@ TE_LAUNCH3(acoustic_uv)
 __global__ void k_acoustic_fpk(KArgs A) {
   TE_K3
   const Acoustic a = A.a;
-  const float *u = A.p[2], *v = A.p[3], *w = A.p[4], *piadv = A.p[5], *ppten = A.p[6], *ppterm = A.p[7];
-  const float *pk1 = A.p[8], *pk2 = A.p[9], *qk = A.p[10];
-  float* fpk = A.p[11];
-  const float* hm = A.p[30];
+  const float *TE_R u = A.p[2], *TE_R v = A.p[3], *TE_R w = A.p[4], *TE_R piadv = A.p[5], *TE_R ppten = A.p[6], *TE_R ppterm = A.p[7];
+  const float *TE_R pk1 = A.p[8], *TE_R pk2 = A.p[9], *TE_R qk = A.p[10];
+  float* TE_R fpk = A.p[11];
+  const float* TE_R hm = A.p[30];
   const int sj = g.sJ, sk = g.sJ * g.sK;
   int i = tx, j = ty, k = tz;
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
@@ -482,8 +493,8 @@ __global__ void k_acoustic_w_solve(KArgs A) {
   if (i >= A.gx || j >= A.gy) return;
   if (i >= g.nx || j >= g.ny) return;
   const Acoustic a = A.a;
-  const float *pk1 = A.p[2], *pk2 = A.p[3], *qk = A.p[4], *mm = A.p[5], *fpk = A.p[6], *wten = A.p[7], *pp3d = A.p[8];
-  float *w = A.p[9], *cA = A.p[10], *cB = A.p[11];
+  const float *TE_R pk1 = A.p[2], *TE_R pk2 = A.p[3], *TE_R qk = A.p[4], *TE_R mm = A.p[5], *TE_R fpk = A.p[6], *TE_R wten = A.p[7], *TE_R pp3d = A.p[8];
+  float *TE_R w = A.p[9], *TE_R cA = A.p[10], *TE_R cB = A.p[11];
   const int sk = g.sJ * g.sK;
   const float asq = a.alph * a.alph;
   w[gidx(g, i, j, 0)] = 0.0f;
@@ -532,8 +543,8 @@ static void launch_acoustic_w_solve(const KArgs& A, cudaStream_t s) {
 __global__ void k_acoustic_pp(KArgs A) {
   TE_K3
   const Acoustic a = A.a;
-  const float *w = A.p[2], *pk1 = A.p[3], *pk2 = A.p[4], *qk = A.p[5], *fpk = A.p[6];
-  float *pp3d = A.p[7], *ppd = A.p[8], *ppx = A.p[9];
+  const float *TE_R w = A.p[2], *TE_R pk1 = A.p[3], *TE_R pk2 = A.p[4], *TE_R qk = A.p[5], *TE_R fpk = A.p[6];
+  float *TE_R pp3d = A.p[7], *TE_R ppd = A.p[8], *TE_R ppx = A.p[9];
   const int saveX = A.iv[10];
   const int sk = g.sJ * g.sK;
   int i = tx, j = ty, k = tz;
@@ -551,8 +562,8 @@ TE_LAUNCH3(acoustic_pp)
 
 __global__ void k_acoustic_accumulate(KArgs A) {
   TE_K3
-  const float *u = A.p[2], *v = A.p[3], *w = A.p[4];
-  float *rru = A.p[5], *rrv = A.p[6], *rrw = A.p[7];
+  const float *TE_R u = A.p[2], *TE_R v = A.p[3], *TE_R w = A.p[4];
+  float *TE_R rru = A.p[5], *TE_R rrv = A.p[6], *TE_R rrw = A.p[7];
   const float tavg = A.f[8];
   TE_WHOLE(k <= g.nz)
   if (tavg > 0.0f) {
@@ -571,7 +582,7 @@ TE_LAUNCH3(acoustic_accumulate)
 
 __global__ void k_bc_periodic_x(KArgs A) {
   TE_K3
-  float* f = A.p[1];
+  float* TE_R f = A.p[1];
   int h = tx, jj = ty - 3, k = tz;
   if (h > 3 || jj > g.ny + 3 || k > g.nz) return;
   int lo = (((-1 - h) % g.nx) + g.nx) % g.nx;
@@ -583,7 +594,7 @@ TE_LAUNCH3(bc_periodic_x)
 
 __global__ void k_bc_periodic_y(KArgs A) {
   TE_K3
-  float* f = A.p[1];
+  float* TE_R f = A.p[1];
   int h = tx, i = ty - 3, k = tz;
   if (h > 3 || i > g.nx + 3 || k > g.nz) return;
   int lo = (((-1 - h) % g.ny) + g.ny) % g.ny;
@@ -597,10 +608,10 @@ TE_LAUNCH3(bc_periodic_y)
 
 __global__ void k_update_diagnostics_moist(KArgs A) {
   TE_K3
-  const float *thp = A.p[1], *ppp = A.p[2], *th0 = A.p[3], *pi0 = A.p[4], *qv0 = A.p[5], *qc0 = A.p[6];
-  const float *qi0 = A.p[7], *rth0 = A.p[8], *qv = A.p[9], *qc = A.p[10], *qr = A.p[11], *qi = A.p[12];
-  const float *qs = A.p[13], *qg = A.p[14];
-  float *thv = A.p[15], *ppterm = A.p[16], *piadv = A.p[17], *thterm = A.p[18], *buoy = A.p[19];
+  const float *TE_R thp = A.p[1], *TE_R ppp = A.p[2], *TE_R th0 = A.p[3], *TE_R pi0 = A.p[4], *TE_R qv0 = A.p[5], *TE_R qc0 = A.p[6];
+  const float *TE_R qi0 = A.p[7], *TE_R rth0 = A.p[8], *TE_R qv = A.p[9], *TE_R qc = A.p[10], *TE_R qr = A.p[11], *TE_R qi = A.p[12];
+  const float *TE_R qs = A.p[13], *TE_R qg = A.p[14];
+  float *TE_R thv = A.p[15], *TE_R ppterm = A.p[16], *TE_R piadv = A.p[17], *TE_R thterm = A.p[18], *TE_R buoy = A.p[19];
   const float rd = 287.04f, rv = 461.5f, cp = 1005.7f, cv = 718.66003f, cpv = 1870.0f, cvv = 1408.5f;
   const float rovcp = 0.28541315f, cpl = 4190.0f, cpi = 2106.0f;
   TE_WHOLE(k < g.nz)
@@ -626,13 +637,13 @@ TE_LAUNCH3(update_diagnostics_moist)
 
 __global__ void k_pressure_tendency(KArgs A) {
   TE_K3
-  const float *th = A.p[1], *qv = A.p[2], *rho = A.p[3], *ppi = A.p[4], *thten = A.p[5], *qpten = A.p[6];
-  const float *th0 = A.p[7], *pi0 = A.p[8];
+  const float *TE_R th = A.p[1], *TE_R qv = A.p[2], *TE_R rho = A.p[3], *TE_R ppi = A.p[4], *TE_R thten = A.p[5], *TE_R qpten = A.p[6];
+  const float *TE_R th0 = A.p[7], *TE_R pi0 = A.p[8];
   const float dt = A.f[9];
   const int hasDiabatic = A.iv[10];
-  float* ppten = A.p[11];
+  float* TE_R ppten = A.p[11];
   const int hasStepTend = A.iv[12];
-  const float* qvt = A.p[13];
+  const float* TE_R qvt = A.p[13];
   const int moist = A.iv[14];
   const float rd = 287.04f, rv = 461.5f, cp = 1005.7f, p00 = 1e5f;
   int i = tx, j = ty, k = tz;
@@ -668,9 +679,9 @@ TE_LAUNCH3(pressure_tendency)
 
 __global__ void k_divergence3d(KArgs A) {
   TE_K3
-  const float *u = A.p[1], *v = A.p[2], *w = A.p[3], *mh = A.p[4];
-  float* div = A.p[5];
-  const float* hm = A.p[30];
+  const float *TE_R u = A.p[1], *TE_R v = A.p[2], *TE_R w = A.p[3], *TE_R mh = A.p[4];
+  float* TE_R div = A.p[5];
+  const float* TE_R hm = A.p[30];
   const int sj = g.sJ, sk = g.sJ * g.sK;
   int i = tx, j = ty, k = tz;
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
@@ -684,8 +695,8 @@ TE_LAUNCH3(divergence3d)
 __global__ void k_update_rho_prs(KArgs A) {
   TE_K3
   const int moist = A.iv[1];
-  const float *thp = A.p[2], *ppp = A.p[3], *th0 = A.p[4], *pi0 = A.p[5], *qv = A.p[6];
-  float *prs = A.p[7], *rho = A.p[8];
+  const float *TE_R thp = A.p[2], *TE_R ppp = A.p[3], *TE_R th0 = A.p[4], *TE_R pi0 = A.p[5], *TE_R qv = A.p[6];
+  float *TE_R prs = A.p[7], *TE_R rho = A.p[8];
   int i = tx, j = ty, k = tz;
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
   int c = gidx(g, i, j, k);
@@ -702,8 +713,8 @@ TE_LAUNCH3(update_rho_prs)
 __global__ void k_diabatic_unapply(KArgs A) {
   TE_K3
   const float dt = A.f[1];
-  float *pp3d = A.p[2], *th = A.p[3], *qv = A.p[4], *qc = A.p[5];
-  float *qpten = A.p[6], *qtten = A.p[7], *qvten = A.p[8], *qcten = A.p[9];
+  float *TE_R pp3d = A.p[2], *TE_R th = A.p[3], *TE_R qv = A.p[4], *TE_R qc = A.p[5];
+  float *TE_R qpten = A.p[6], *TE_R qtten = A.p[7], *TE_R qvten = A.p[8], *TE_R qcten = A.p[9];
   int i = tx, j = ty, k = tz;
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
   int c = gidx(g, i, j, k);
@@ -726,8 +737,8 @@ TE_LAUNCH3(diabatic_unapply)
 __global__ void k_diabatic_rates(KArgs A) {
   TE_K3
   const float dt = A.f[1];
-  const float *pp3d = A.p[2], *th = A.p[3], *qv = A.p[4], *qc = A.p[5];
-  float *qpten = A.p[6], *qtten = A.p[7], *qvten = A.p[8], *qcten = A.p[9];
+  const float *TE_R pp3d = A.p[2], *TE_R th = A.p[3], *TE_R qv = A.p[4], *TE_R qc = A.p[5];
+  float *TE_R qpten = A.p[6], *TE_R qtten = A.p[7], *TE_R qvten = A.p[8], *TE_R qcten = A.p[9];
   int i = tx, j = ty, k = tz;
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
   int c = gidx(g, i, j, k);
@@ -741,8 +752,8 @@ TE_LAUNCH3(diabatic_rates)
 
 __global__ void k_ppx_finish(KArgs A) {
   TE_K3
-  const float* pp3d = A.p[1];
-  float* ppx = A.p[2];
+  const float* TE_R pp3d = A.p[1];
+  float* TE_R ppx = A.p[2];
   int i = tx, j = ty, k = tz;
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
   int c = gidx(g, i, j, k);
@@ -827,4 +838,7 @@ const KernelSpec* find_kernel(const char* name) {
   return nullptr;
 }
 
+#ifdef TE_KERNELS_FAST
+}  // namespace fast
+#endif
 }  // namespace te

@@ -45,4 +45,11 @@ struct KernelSpec {
 const KernelSpec* kernel_table(int* count);
 const KernelSpec* find_kernel(const char* name);
 
+// The same kernels with __restrict__ field pointers (te_kernels_fast.cu), for ops whose
+// bound regions do not overlap.
+namespace fast {
+const KernelSpec* kernel_table(int* count);
+const KernelSpec* find_kernel(const char* name);
+}  // namespace fast
+
 }  // namespace te

@@ -332,6 +332,23 @@ void Plan::finalize_args(std::vector<Op>& ops) {
         A.iv2[ps.index] = (int)word(it->second + 1);
       }
     }
+    // the __restrict__ build is valid when no written region overlaps another bound region
+    bool disjoint = true;
+    for (int q1 = 0; q1 < o.spec->nparams && disjoint; q1++) {
+      const ParamSpec& a = o.spec->params[q1];
+      auto ia = o.bind.find(a.index);
+      if (a.kind != kPtr || ia == o.bind.end()) continue;
+      const uint64_t a0 = ia->second, a1 = a0 + region_len(a0);
+      for (int q2 = q1 + 1; q2 < o.spec->nparams && disjoint; q2++) {
+        const ParamSpec& b = o.spec->params[q2];
+        auto ib = o.bind.find(b.index);
+        if (b.kind != kPtr || ib == o.bind.end() || !(a.write || b.write)) continue;
+        const uint64_t b0 = ib->second, b1 = b0 + region_len(b0);
+        if (a0 < b1 && b0 < a1) disjoint = false;
+      }
+    }
+    const KernelSpec* f = disjoint ? fast::find_kernel(o.spec->name) : nullptr;
+    o.launch = f ? f->launch : o.spec->launch;
   }
 }
 
@@ -693,7 +710,7 @@ void Plan::launch_exact(std::vector<Op>& ops, int first, int last, bool hashes) 
       continue;
     }
     if (!o.spec) throw ApiError(TE_ENOKERNEL, "no CUDA kernel for " + o.name);
-    o.spec->launch(o.args, stream);
+    (o.launch ? o.launch : o.spec->launch)(o.args, stream);
     if (hashes) {
       for (auto& h : o.hashes) {
         if (!h.bound || !h.len) continue;

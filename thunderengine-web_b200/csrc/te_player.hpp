@@ -25,6 +25,7 @@ struct Op {
   std::string name;
   uint64_t src = 0, dst = 0, n = 0;
   const KernelSpec* spec = nullptr;
+  LaunchFn launch = nullptr;  // spec->launch, or its __restrict__ twin when the bound regions are disjoint
   int grid[3] = {0, 0, 0}, tg[3] = {0, 0, 0};
   std::map<int, uint64_t> bind;  // binding index -> memory word offset
   std::vector<HashReq> hashes;
