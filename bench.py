@@ -193,7 +193,6 @@ def cpu_baseline_sample(budget_s=10.0):
 def run_ours(a, rank, world, local):
     import torch
     from thunderengine_web_b200.replayer import Replayer, TE_MODE_EXACT, TE_MODE_FUSED
-    from tests import helpers
     dev = local if torch.cuda.device_count() > local else 0
     torch.cuda.set_device(dev)
     cfg, run = workload(a.workload)
@@ -266,9 +265,8 @@ def kernel_roofline(r, run, stream, mode):
     each exact dispatch kind and each fused kernel is re-launched alone `reps` times.
     The dominant kernel (time x launches per step) gets the roofline figures."""
     import torch
-    from tests import helpers
     peak, src = peaks()
-    km = helpers.kernels_meta()
+    km = kernel_meta(r.lib)
     disp = tape_dispatches(run, run.tape_cmds)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     reps = 5
@@ -340,15 +338,28 @@ def kernel_roofline(r, run, stream, mode):
     launches = sum(v[1] for v in stats.values())
     if mode == 1:
         launches = sum(sg[3] for sg in r.fused_segments())
+    dram = NCU_DRAM_BYTES_PER_POINT.get(top)
     return {'kernel': top, 'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
             'frac': achieved / peak, 'peak_source': ('measured (MEASURED_PEAKS.json hbm_gbs)' if src == 'measured'
                                                      else 'fallback 6650 GB/s'),
-            'algorithmic_bytes_per_launch': byts, 'launch_ms': ms, 'traffic': None,
+            'algorithmic_bytes_per_launch': byts, 'launch_ms': ms,
+            'traffic': dram * g.nx * g.ny * g.nz if dram else None,
+            'traffic_source': ('ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on the 160x160x80 '
+                               'workload, scaled by interior points' if dram else None),
             'share_of_step': shares[0][1], 'sum_of_kernel_ms_per_step': tot,
             'top_kernels': [[n, round(sv, 4), round(stats[n][0], 4), stats[n][1],
                              round(stats[n][2] / (stats[n][0] / 1e3) / 1e9, 1)] for n, sv in shares[:10]],
             'top_kernels_columns': ['kernel', 'share', 'ms_per_launch', 'launches_per_step', 'achieved_GBps'],
             '_launches_per_step': launches}
+
+
+# DRAM bytes per interior point of one launch of the dominant kernels: one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum) of the kernel on the 160x160x80 workload
+# (a size ncu captures quickly), divided by its interior points; traffic grows with the
+# points a launch processes.  Writes still held in L2 when the launch ends are not counted.
+NCU_DRAM_BYTES_PER_POINT = {
+    'acoustic_column (fused fpk+w_solve+pp+accumulate)': (112.05e6 + 13.56e6) / (160 * 160 * 80),
+}
 
 
 # Fields a kernel both reads and writes at the same points (binding indices), counted
@@ -382,6 +393,22 @@ def tape_dispatches(run, cmds):
         elif op == 'dispatch':
             out.append({'name': pipe, 'grid': c['grid'], 'fields': dict(bind)})
     return out
+
+
+# Kernels launched once per column (kernels.json "rank": 2): a dispatched thread covers nz levels.
+COLUMN_KERNELS = {'acoustic_w_solve'}
+
+
+def kernel_meta(lib):
+    """The library's own kernel table (kernels.json-shaped: parameter index, kind, write)."""
+    import ctypes
+    n = lib.te_kernel_table_json(None, 0)
+    buf = ctypes.create_string_buffer(n + 1)
+    lib.te_kernel_table_json(buf, n + 1)
+    table = json.loads(buf.value.decode())
+    for name, k in table.items():
+        k['rank'] = 2 if name in COLUMN_KERNELS else 3
+    return table
 
 
 def dispatch_bytes(d, km, nz):

@@ -348,37 +348,52 @@ struct HaloArgs {
 
 // Final state of bc_periodic_x followed by bc_periodic_y (bc_periodic_x.wgsl,
 // bc_periodic_y.wgsl): every halo point of levels 0..nz holds the interior value at
-// (i mod nx, j mod ny).  One thread per halo point and level: the 7 x-halo columns
-// over all rows, then the 7 y-halo rows over the interior columns.
-__global__ void k_halo_periodic(HaloArgs H) {
-  const Dims& g = H.g;
-  const int per_level = 7 * g.sK + 7 * g.nx;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k = blockIdx.y;
-  if (t >= per_level || k > g.nz) return;
-  int i, j;
-  if (t < 7 * g.sK) {
-    const int col = t / g.sK;  // 0..6 -> i = -3,-2,-1, nx, nx+1, nx+2, nx+3
-    j = t % g.sK - 3;
-    i = col < 3 ? col - 3 : g.nx + (col - 3);
-  } else {
-    const int r = t - 7 * g.sK;
-    const int row = r / g.nx;
-    i = r % g.nx;
-    j = row < 3 ? row - 3 : g.ny + (row - 3);
+// (i mod nx, j mod ny).  Two kinds of warps:
+//  * x-halo rows: one warp per (j, k) row, lane = (field, halo column) for the 7 halo
+//    columns of up to 4 fields, so a row's reads and writes are a few sectors per warp;
+//  * y-halo rows: one thread per interior column of the 7 halo rows, all fields.
+// Every halo point is written by exactly one thread, after that thread has read what it
+// needs (a halo point is never an interior point read by another thread).
+constexpr int kHaloX = 7;
+
+__device__ __forceinline__ void halo_point(const HaloArgs& H, int f, int dst, int src) {
+  const float v = H.f[f][src];
+  if (H.acc_rrw && H.f[f] == H.acc_w) {
+    const float wv = H.acc_w[dst], r = H.acc_rrw[dst];
+    H.acc_rrw[dst] = H.tavg > 0.0f ? fmaf(wv, H.alph, r) * H.tavg : r + wv;
   }
-  const int ii = ((i % g.nx) + g.nx) % g.nx;
+  H.f[f][dst] = v;
+}
+
+__global__ void __launch_bounds__(256) k_halo_periodic(HaloArgs H) {
+  const Dims& g = H.g;
+  const int k = blockIdx.y;
+  const int xrows = g.sK;                       // x-halo rows of a level (j = -3 .. ny + 3)
+  const int xwarps = (xrows + 7) / 8;           // blocks of 8 warps
+  if ((int)blockIdx.x < xwarps) {
+    const int row = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    const int f = lane / kHaloX, col = lane % kHaloX;
+    if (row >= xrows || f >= H.nf) return;
+    const int j = row - 3;
+    const int i = col < 3 ? col - 3 : g.nx + (col - 3);
+    const int ii = ((i % g.nx) + g.nx) % g.nx, jj = ((j % g.ny) + g.ny) % g.ny;
+    halo_point(H, f, gidx(g, i, j, k), gidx(g, ii, jj, k));
+    return;
+  }
+  const int t = (blockIdx.x - xwarps) * blockDim.x + threadIdx.x;
+  if (t >= kHaloX * g.nx) return;
+  const int r = t / g.nx, i = t % g.nx;
+  const int j = r < 3 ? r - 3 : g.ny + (r - 3);
   const int jj = ((j % g.ny) + g.ny) % g.ny;
-  const int dst = gidx(g, i, j, k), src = gidx(g, ii, jj, k);
-  // every load before the first store: a halo point (dst) is never an interior point
-  // (src), so the loads of the four fields and of the accumulation overlap
+  const int dst = gidx(g, i, j, k), src = gidx(g, i, jj, k);
+  // all loads before the first store
   float v[4];
 #pragma unroll
   for (int q = 0; q < 4; q++)
     if (q < H.nf) v[q] = H.f[q][src];
   if (H.acc_rrw) {
-    const float wv = H.acc_w[dst], r = H.acc_rrw[dst];
-    H.acc_rrw[dst] = H.tavg > 0.0f ? fmaf(wv, H.alph, r) * H.tavg : r + wv;
+    const float wv = H.acc_w[dst], rr = H.acc_rrw[dst];
+    H.acc_rrw[dst] = H.tavg > 0.0f ? fmaf(wv, H.alph, rr) * H.tavg : rr + wv;
   }
 #pragma unroll
   for (int q = 0; q < 4; q++)
@@ -386,8 +401,8 @@ __global__ void k_halo_periodic(HaloArgs H) {
 }
 
 static void launch_halo(const HaloArgs& H, cudaStream_t s) {
-  const int per_level = 7 * H.g.sK + 7 * H.g.nx;
-  dim3 b(256), gr((per_level + 255) / 256, H.g.nz + 1);
+  const int xblocks = (H.g.sK + 7) / 8, yblocks = (kHaloX * H.g.nx + 255) / 256;
+  dim3 b(256), gr(xblocks + yblocks, H.g.nz + 1);
   k_halo_periodic<<<gr, b, 0, s>>>(H);
 }
 
