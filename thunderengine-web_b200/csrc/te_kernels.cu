@@ -44,6 +44,39 @@ static void launch3(void (*k)(KArgs), const KArgs& A, cudaStream_t s) {
 #define TE_LAUNCH3(name) \
   static void launch_##name(const KArgs& A, cudaStream_t s) { launch3(k_##name, A, s); }
 
+// Point-wise kernels in the __restrict__ build: a thread takes kRowVec consecutive
+// dispatch threads along x (the same (ty, tz)), loads the inputs of all of them, then
+// computes and stores each.  Op::active is the kernel's range check, Op::load reads one
+// point's inputs, Op::store computes and writes it; the operations of a point are the
+// per-dispatch kernel's, and distinct points share no written word, so the results are
+// those of one thread per point.
+enum { kRowVec = 4 };
+
+template <class Op>
+__global__ void __launch_bounds__(128) k_rowvec(KArgs A) {
+  const int tx0 = (blockIdx.x * blockDim.x + threadIdx.x) * kRowVec;
+  const int ty = blockIdx.y * blockDim.y + threadIdx.y;
+  const int tz = blockIdx.z;
+  if (ty >= A.gy || tz >= A.gz) return;
+  typename Op::In in[kRowVec];
+  bool on[kRowVec];
+#pragma unroll
+  for (int q = 0; q < kRowVec; q++) {
+    on[q] = tx0 + q < A.gx && Op::active(A, tx0 + q, ty, tz);
+    if (on[q]) in[q] = Op::load(A, tx0 + q, ty, tz);
+  }
+#pragma unroll
+  for (int q = 0; q < kRowVec; q++)
+    if (on[q]) Op::store(A, tx0 + q, ty, tz, in[q]);
+}
+
+template <class Op>
+static void launch_rowvec(const KArgs& A, cudaStream_t s) {
+  dim3 b(32, 4, 1);
+  dim3 gr((A.gx + 32 * kRowVec - 1) / (32 * kRowVec), (A.gy + 3) / 4, A.gz);
+  k_rowvec<Op><<<gr, b, 0, s>>>(A);
+}
+
 // ------------------------------------------------------------------ fluxes
 
 // Each flux kernel stores face_*(A, i, j, k) (te_flux.cuh) over its dispatch range.
@@ -340,6 +373,29 @@ __global__ void k_div_massflux(KArgs A) {
 }
 TE_LAUNCH3(div_massflux)
 
+struct OpDivMassflux {  // div_massflux as a row-vector op (same operations)
+  struct In {
+    float ru0, ru1, rv0, rv1, rw0, rw1;
+  };
+  static __device__ __forceinline__ bool active(const KArgs& A, int tx, int ty, int tz) {
+    return tx - 3 <= A.g.nx + 2 && ty - 3 <= A.g.ny + 2 && tz < A.g.nz;
+  }
+  static __device__ __forceinline__ In load(const KArgs& A, int tx, int ty, int tz) {
+    const Dims& g = A.g;
+    const float *TE_R rru = A.p[1], *TE_R rrv = A.p[2], *TE_R rrw = A.p[3];
+    const int c = gidx(g, tx - 3, ty - 3, tz), sj = g.sJ, sk = g.sJ * g.sK;
+    return In{rru[c], rru[c + 1], rrv[c], rrv[c + sj], rrw[c], rrw[c + sk]};
+  }
+  static __device__ __forceinline__ void store(const KArgs& A, int tx, int ty, int tz, const In& v) {
+    const Dims& g = A.g;
+    const float *TE_R mh = A.p[4], *TE_R hm = A.p[30];
+    float* TE_R divx = A.p[5];
+    const int i = tx - 3, j = ty - 3, k = tz, c = gidx(g, i, j, k);
+    divx[c] = fmaf((v.rw1 - v.rw0) * g.rdz, mh[k],
+                   fmaf((v.ru1 - v.ru0) * g.rdx, hm_uh(g, hm, i), ((v.rv1 - v.rv0) * g.rdy) * hm_vh(g, hm, j)));
+  }
+};
+
 __global__ void k_velocity_to_massflux(KArgs A) {
   TE_K3
   const float *TE_R rho0 = A.p[1], *TE_R rf0 = A.p[2];
@@ -352,6 +408,32 @@ __global__ void k_velocity_to_massflux(KArgs A) {
   rrw[c] = (k == 0 || k == g.nz) ? 0.0f : rrw[c] * rf0[k];
 }
 TE_LAUNCH3(velocity_to_massflux)
+
+struct OpVelocityToMassflux {  // velocity_to_massflux as a row-vector op
+  struct In {
+    float ru, rv, rw;
+  };
+  static __device__ __forceinline__ bool active(const KArgs& A, int tx, int ty, int tz) {
+    return tx - 3 <= A.g.nx + 3 && ty - 3 <= A.g.ny + 3 && tz <= A.g.nz;
+  }
+  static __device__ __forceinline__ In load(const KArgs& A, int tx, int ty, int tz) {
+    const int c = gidx(A.g, tx - 3, ty - 3, tz);
+    const float *TE_R rru = A.p[3], *TE_R rrv = A.p[4], *TE_R rrw = A.p[5];
+    const int k = tz;
+    return In{k < A.g.nz ? rru[c] : 0.0f, k < A.g.nz ? rrv[c] : 0.0f, (k == 0 || k == A.g.nz) ? 0.0f : rrw[c]};
+  }
+  static __device__ __forceinline__ void store(const KArgs& A, int tx, int ty, int tz, const In& v) {
+    const Dims& g = A.g;
+    const float *TE_R rho0 = A.p[1], *TE_R rf0 = A.p[2];
+    float *TE_R rru = A.p[3], *TE_R rrv = A.p[4], *TE_R rrw = A.p[5];
+    const int k = tz, c = gidx(g, tx - 3, ty - 3, k);
+    if (k < g.nz) {
+      rru[c] = v.ru * rho0[k];
+      rrv[c] = v.rv * rho0[k];
+    }
+    rrw[c] = (k == 0 || k == g.nz) ? 0.0f : v.rw * rf0[k];
+  }
+};
 
 __global__ void k_stage_state_reset(KArgs A) {
   TE_K3
@@ -769,6 +851,13 @@ TE_LAUNCH3(ppx_finish)
 #define P(i) {i, kPtr, 0}
 #define W(i) {i, kPtr, 1}
 
+// the __restrict__ build launches the row-vector form where a kernel has one
+#ifdef TE_KERNELS_FAST
+#define TE_ROWVEC(name, op) launch_rowvec<op>
+#else
+#define TE_ROWVEC(name, op) launch_##name
+#endif
+
 static const KernelSpec kTable[] = {
     {"adv_flux_x", 4, {R(0), P(1), P(2), W(3)}, false, launch_adv_flux_x},
     {"adv_flux_y", 4, {R(0), P(1), P(2), W(3)}, false, launch_adv_flux_y},
@@ -793,8 +882,9 @@ static const KernelSpec kTable[] = {
                         R(15), W(16), P(30)}, false, launch_pdef_apply},
     {"build_sadv", 4, {R(0), P(1), P(2), W(3)}, false, launch_build_sadv},
     {"massflux_from_state", 10, {R(0), P(1), P(2), P(3), P(4), P(5), W(6), W(7), W(8), P(24)}, false, launch_massflux_from_state},
-    {"div_massflux", 8, {R(0), P(1), P(2), P(3), P(4), W(5), P(30), P(25)}, false, launch_div_massflux},
-    {"velocity_to_massflux", 7, {R(0), P(1), P(2), W(3), W(4), W(5), P(24)}, false, launch_velocity_to_massflux},
+    {"div_massflux", 8, {R(0), P(1), P(2), P(3), P(4), W(5), P(30), P(25)}, false, TE_ROWVEC(div_massflux, OpDivMassflux)},
+    {"velocity_to_massflux", 7, {R(0), P(1), P(2), W(3), W(4), W(5), P(24)}, false,
+     TE_ROWVEC(velocity_to_massflux, OpVelocityToMassflux)},
     {"stage_state_reset", 11, {R(0), P(1), P(2), P(3), P(4), W(5), W(6), W(7), W(8), W(9), P(10)}, false, launch_stage_state_reset},
     {"stage_tendency_reset", 4, {R(0), W(1), W(2), W(3)}, false, launch_stage_tendency_reset},
     {"buoyancy_apply", 5, {R(0), P(1), P(2), P(3), W(4)}, false, launch_buoyancy_apply},
