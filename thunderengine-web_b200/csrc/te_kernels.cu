@@ -44,36 +44,36 @@ static void launch3(void (*k)(KArgs), const KArgs& A, cudaStream_t s) {
 #define TE_LAUNCH3(name) \
   static void launch_##name(const KArgs& A, cudaStream_t s) { launch3(k_##name, A, s); }
 
-// Point-wise kernels in the __restrict__ build: a thread takes kRowVec consecutive
-// dispatch threads along x (the same (ty, tz)), loads the inputs of all of them, then
-// computes and stores each.  Op::active is the kernel's range check, Op::load reads one
-// point's inputs, Op::store computes and writes it; the operations of a point are the
-// per-dispatch kernel's, and distinct points share no written word, so the results are
-// those of one thread per point.
+// Point-wise kernels in the __restrict__ build: a thread takes kRowVec dispatch threads
+// of the same (tx, ty) on consecutive levels, loads the inputs of all of them, then
+// computes and stores each (the loads of a warp stay 128-byte rows).  Op::active is the
+// kernel's range check, Op::load reads one point's inputs, Op::store computes and
+// writes it; the operations of a point are the per-dispatch kernel's, and distinct
+// points share no written word, so the results are those of one thread per point.
 enum { kRowVec = 4 };
 
 template <class Op>
 __global__ void __launch_bounds__(128) k_rowvec(KArgs A) {
-  const int tx0 = (blockIdx.x * blockDim.x + threadIdx.x) * kRowVec;
+  const int tx = blockIdx.x * blockDim.x + threadIdx.x;
   const int ty = blockIdx.y * blockDim.y + threadIdx.y;
-  const int tz = blockIdx.z;
-  if (ty >= A.gy || tz >= A.gz) return;
+  const int tz0 = blockIdx.z * kRowVec;
+  if (tx >= A.gx || ty >= A.gy) return;
   typename Op::In in[kRowVec];
   bool on[kRowVec];
 #pragma unroll
   for (int q = 0; q < kRowVec; q++) {
-    on[q] = tx0 + q < A.gx && Op::active(A, tx0 + q, ty, tz);
-    if (on[q]) in[q] = Op::load(A, tx0 + q, ty, tz);
+    on[q] = tz0 + q < A.gz && Op::active(A, tx, ty, tz0 + q);
+    if (on[q]) in[q] = Op::load(A, tx, ty, tz0 + q);
   }
 #pragma unroll
   for (int q = 0; q < kRowVec; q++)
-    if (on[q]) Op::store(A, tx0 + q, ty, tz, in[q]);
+    if (on[q]) Op::store(A, tx, ty, tz0 + q, in[q]);
 }
 
 template <class Op>
 static void launch_rowvec(const KArgs& A, cudaStream_t s) {
   dim3 b(32, 4, 1);
-  dim3 gr((A.gx + 32 * kRowVec - 1) / (32 * kRowVec), (A.gy + 3) / 4, A.gz);
+  dim3 gr((A.gx + 31) / 32, (A.gy + 3) / 4, (A.gz + kRowVec - 1) / kRowVec);
   k_rowvec<Op><<<gr, b, 0, s>>>(A);
 }
 
