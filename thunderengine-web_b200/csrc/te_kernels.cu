@@ -851,6 +851,327 @@ TE_LAUNCH3(ppx_finish)
 #define P(i) {i, kPtr, 0}
 #define W(i) {i, kPtr, 1}
 
+// ------------------------------------------ row-vector forms of point-wise kernels
+// (the __restrict__ build; see k_rowvec).  Each Op restates its kernel above: the same
+// range check (active), the same loads (load) and the same operations (store).
+
+#define TE_OP_WHOLE(kcond)                                                            \
+  static __device__ __forceinline__ bool active(const KArgs& A, int tx, int ty, int tz) { \
+    const Dims& g = A.g;                                                              \
+    const int k = tz;                                                                 \
+    return tx - 3 <= g.nx + 3 && ty - 3 <= g.ny + 3 && (kcond);                       \
+  }
+#define TE_OP_INTERIOR                                                                \
+  static __device__ __forceinline__ bool active(const KArgs& A, int tx, int ty, int tz) { \
+    return tx < A.g.nx && ty < A.g.ny && tz < A.g.nz;                                 \
+  }
+#define TE_OP_C(ioff) const Dims& g = A.g; const int i = tx - (ioff), j = ty - (ioff), k = tz; \
+  const int c = gidx(g, i, j, k); (void)i; (void)j; (void)k
+
+struct OpBuildSadv {
+  struct In { float thp; };
+  TE_OP_WHOLE(k < g.nz)
+  static __device__ __forceinline__ In load(const KArgs& A, int tx, int ty, int tz) {
+    TE_OP_C(3);
+    return In{A.p[2][c]};
+  }
+  static __device__ __forceinline__ void store(const KArgs& A, int tx, int ty, int tz, const In& v) {
+    TE_OP_C(3);
+    A.p[3][c] = (A.p[1][k] - 300.0f) + v.thp;
+  }
+};
+
+struct OpAcousticBegin {
+  struct In { float w; };
+  TE_OP_WHOLE(k <= g.nz)
+  static __device__ __forceinline__ In load(const KArgs& A, int tx, int ty, int tz) {
+    TE_OP_C(3);
+    return In{A.p[2][c]};
+  }
+  static __device__ __forceinline__ void store(const KArgs& A, int tx, int ty, int tz, const In& v) {
+    TE_OP_C(3);
+    A.p[3][c] = 0.0f;
+    A.p[4][c] = 0.0f;
+    A.p[5][c] = v.w * A.a.beta;
+  }
+};
+
+struct OpMassfluxFromState {
+  struct In { float u, v, w; };
+  TE_OP_WHOLE(k <= g.nz)
+  static __device__ __forceinline__ In load(const KArgs& A, int tx, int ty, int tz) {
+    TE_OP_C(3);
+    In r{0.0f, 0.0f, 0.0f};
+    if (k < g.nz) {
+      r.u = A.p[1][c];
+      r.v = A.p[2][c];
+    }
+    if (!(k == 0 || k == g.nz)) r.w = A.p[3][c];
+    return r;
+  }
+  static __device__ __forceinline__ void store(const KArgs& A, int tx, int ty, int tz, const In& v) {
+    TE_OP_C(3);
+    const float *TE_R rho0 = A.p[4], *TE_R rf0 = A.p[5];
+    if (k < g.nz) {
+      A.p[6][c] = rho0[k] * v.u;
+      A.p[7][c] = rho0[k] * v.v;
+    }
+    A.p[8][c] = (k == 0 || k == g.nz) ? 0.0f : rf0[k] * v.w;
+  }
+};
+
+struct OpStageStateReset {
+  struct In { float ua, va, wa, ppi, ppx; };
+  TE_OP_WHOLE(k <= g.nz)
+  static __device__ __forceinline__ In load(const KArgs& A, int tx, int ty, int tz) {
+    TE_OP_C(3);
+    return In{A.p[1][c], A.p[2][c], A.p[3][c], A.p[4][c], A.p[10][c]};
+  }
+  static __device__ __forceinline__ void store(const KArgs& A, int tx, int ty, int tz, const In& v) {
+    TE_OP_C(3);
+    A.p[5][c] = v.ua;
+    A.p[6][c] = v.va;
+    A.p[7][c] = v.wa;
+    A.p[8][c] = v.ppi;
+    A.p[9][c] = v.ppx;
+  }
+};
+
+struct OpAcousticAccumulate {
+  struct In { float u, v, w, ru, rv, rw; };
+  TE_OP_WHOLE(k <= g.nz)
+  static __device__ __forceinline__ In load(const KArgs& A, int tx, int ty, int tz) {
+    TE_OP_C(3);
+    return In{A.p[2][c], A.p[3][c], A.p[4][c], A.p[5][c], A.p[6][c], A.p[7][c]};
+  }
+  static __device__ __forceinline__ void store(const KArgs& A, int tx, int ty, int tz, const In& v) {
+    TE_OP_C(3);
+    const float tavg = A.f[8];
+    if (tavg > 0.0f) {
+      A.p[5][c] = (v.ru + v.u) * tavg;
+      A.p[6][c] = (v.rv + v.v) * tavg;
+      A.p[7][c] = fmaf(v.w, A.a.alph, v.rw) * tavg;
+    } else {
+      A.p[5][c] = v.ru + v.u;
+      A.p[6][c] = v.rv + v.v;
+      A.p[7][c] = v.rw + v.w;
+    }
+  }
+};
+
+struct OpUpdateDiagnosticsMoist {
+  struct In { float thp, ppp, qv, qc, qr, qi, qs, qg; };
+  TE_OP_WHOLE(k < g.nz)
+  static __device__ __forceinline__ In load(const KArgs& A, int tx, int ty, int tz) {
+    TE_OP_C(3);
+    return In{A.p[1][c], A.p[2][c], A.p[9][c], A.p[10][c], A.p[11][c], A.p[12][c], A.p[13][c], A.p[14][c]};
+  }
+  static __device__ __forceinline__ void store(const KArgs& A, int tx, int ty, int tz, const In& v) {
+    TE_OP_C(3);
+    const float *TE_R th0 = A.p[3], *TE_R pi0 = A.p[4], *TE_R qv0 = A.p[5], *TE_R qc0 = A.p[6];
+    const float *TE_R qi0 = A.p[7], *TE_R rth0 = A.p[8];
+    const float rd = 287.04f, rv = 461.5f, cp = 1005.7f, cv = 718.66003f, cpv = 1870.0f, cvv = 1408.5f;
+    const float rovcp = 0.28541315f, cpl = 4190.0f, cpi = 2106.0f;
+    float reps = dcr(rv, rd);
+    float repsm1 = reps - 1.0f;
+    float gacc = 9.81f;
+    float qvv = wmax(v.qv, 0.0f);
+    float liq = v.qc + v.qr;
+    float ice = (v.qi + v.qs) + v.qg;
+    float qli = wmax(0.0f, liq + ice);
+    float cpli = fmaf(cpl, wmax(0.0f, liq), cpi * wmax(0.0f, ice));
+    float th = th0[k] + v.thp;
+    float pi = pi0[k] + v.ppp;
+    float cpm = fmaf(cpv, qvv, cp) + cpli;
+    float cvm = dcr(1.0f, fmaf(cvv, qvv, cv) + cpli);
+    A.p[15][c] = dcr(th * fmaf(reps, qvv, 1.0f), (1.0f + qvv) + qli);
+    A.p[17][c] = pi;
+    A.p[16][c] = ((pi * rovcp) * cpm) * cvm;
+    A.p[18][c] = (th * fmaf(-rovcp, cpm, fmaf(rv, qvv, rd))) * cvm;
+    A.p[19][c] = gacc * (fmaf(v.thp, rth0[k], repsm1 * (qvv - qv0[k])) - ((qli - qc0[k]) - qi0[k]));
+  }
+};
+
+struct OpRkUpdate {
+  struct In { float phiA, tend; };
+  static __device__ __forceinline__ bool active(const KArgs& A, int tx, int ty, int tz) {
+    const Dims& g = A.g;
+    const int stag = A.iv[1];
+    const int iMax = stag == 2 ? g.nx : g.nx - 1, jMax = stag == 3 ? g.ny : g.ny - 1, kLo = stag == 4 ? 1 : 0;
+    return tx <= iMax && ty <= jMax && tz >= kLo && tz < g.nz;
+  }
+  static __device__ __forceinline__ In load(const KArgs& A, int tx, int ty, int tz) {
+    TE_OP_C(0);
+    return In{A.p[2][c], A.p[3][c]};
+  }
+  static __device__ __forceinline__ void store(const KArgs& A, int tx, int ty, int tz, const In& v) {
+    TE_OP_C(0);
+    A.p[4][c] = fmaf(A.f[5], v.tend, v.phiA);
+  }
+};
+
+struct OpApplyThterm {
+  struct In { float div, thterm, tend; };
+  TE_OP_INTERIOR
+  static __device__ __forceinline__ In load(const KArgs& A, int tx, int ty, int tz) {
+    TE_OP_C(0);
+    return In{A.p[1][c], A.p[2][c], A.p[3][c]};
+  }
+  static __device__ __forceinline__ void store(const KArgs& A, int tx, int ty, int tz, const In& v) {
+    TE_OP_C(0);
+    A.p[3][c] = fmaf(-v.div, v.thterm, v.tend);
+  }
+};
+
+struct OpDiabaticUnapply {
+  struct In { float pp, th, qv, qc, qp_t, qt_t, qv_t, qc_t; };
+  TE_OP_INTERIOR
+  static __device__ __forceinline__ In load(const KArgs& A, int tx, int ty, int tz) {
+    TE_OP_C(0);
+    return In{A.p[2][c], A.p[3][c], A.p[4][c], A.p[5][c], A.p[6][c], A.p[7][c], A.p[8][c], A.p[9][c]};
+  }
+  static __device__ __forceinline__ void store(const KArgs& A, int tx, int ty, int tz, const In& v) {
+    TE_OP_C(0);
+    const float dt = A.f[1];
+    float x;
+    x = fmaf(-dt, v.qp_t, v.pp);
+    A.p[2][c] = x;
+    A.p[6][c] = x;
+    x = fmaf(-dt, v.qt_t, v.th);
+    A.p[3][c] = x;
+    A.p[7][c] = x;
+    x = fmaf(-dt, v.qv_t, v.qv);
+    A.p[4][c] = x;
+    A.p[8][c] = x;
+    x = fmaf(-dt, v.qc_t, v.qc);
+    A.p[5][c] = x;
+    A.p[9][c] = x;
+  }
+};
+
+struct OpDiabaticRates {
+  struct In { float pp, th, qv, qc, qp_t, qt_t, qv_t, qc_t; };
+  TE_OP_INTERIOR
+  static __device__ __forceinline__ In load(const KArgs& A, int tx, int ty, int tz) {
+    TE_OP_C(0);
+    return In{A.p[2][c], A.p[3][c], A.p[4][c], A.p[5][c], A.p[6][c], A.p[7][c], A.p[8][c], A.p[9][c]};
+  }
+  static __device__ __forceinline__ void store(const KArgs& A, int tx, int ty, int tz, const In& v) {
+    TE_OP_C(0);
+    float rdt = dcr(1.0f, A.f[1]);
+    A.p[6][c] = (v.pp - v.qp_t) * rdt;
+    A.p[7][c] = (v.th - v.qt_t) * rdt;
+    A.p[8][c] = (v.qv - v.qv_t) * rdt;
+    A.p[9][c] = (v.qc - v.qc_t) * rdt;
+  }
+};
+
+struct OpPpxFinish {
+  struct In { float pp, ppx; };
+  TE_OP_INTERIOR
+  static __device__ __forceinline__ In load(const KArgs& A, int tx, int ty, int tz) {
+    TE_OP_C(0);
+    return In{A.p[1][c], A.p[2][c]};
+  }
+  static __device__ __forceinline__ void store(const KArgs& A, int tx, int ty, int tz, const In& v) {
+    TE_OP_C(0);
+    A.p[2][c] = v.pp + v.ppx;
+  }
+};
+
+struct OpDivergence3d {
+  struct In { float u0, u1, v0, v1, w0, w1; };
+  TE_OP_INTERIOR
+  static __device__ __forceinline__ In load(const KArgs& A, int tx, int ty, int tz) {
+    TE_OP_C(0);
+    const float *TE_R u = A.p[1], *TE_R v = A.p[2], *TE_R w = A.p[3];
+    return In{u[c], u[c + 1], v[c], v[c + g.sJ], w[c], w[c + g.sJ * g.sK]};
+  }
+  static __device__ __forceinline__ void store(const KArgs& A, int tx, int ty, int tz, const In& v) {
+    TE_OP_C(0);
+    const float *TE_R mh = A.p[4], *TE_R hm = A.p[30];
+    float d = fmaf((v.w1 - v.w0) * g.rdz, mh[k],
+                   fmaf((v.u1 - v.u0) * g.rdx, hm_uh(g, hm, i), ((v.v1 - v.v0) * g.rdy) * hm_vh(g, hm, j)));
+    A.p[5][c] = fabsf(d) < 1e-30f ? 0.0f : d;
+  }
+};
+
+struct OpAcousticPrepare {
+  struct In { float ppterm, pa, pa_up, pa_dn, thv, thv_dn; };
+  TE_OP_INTERIOR
+  static __device__ __forceinline__ In load(const KArgs& A, int tx, int ty, int tz) {
+    TE_OP_C(0);
+    const float *TE_R ppterm = A.p[2], *TE_R piadv = A.p[3], *TE_R thv = A.p[4];
+    const int sk = g.sJ * g.sK;
+    In r;
+    r.ppterm = ppterm[c];
+    r.pa = piadv[c];
+    r.pa_up = k != g.nz - 1 ? piadv[c + sk] : 0.0f;
+    r.pa_dn = k != 0 ? piadv[c - sk] : 0.0f;
+    r.thv = thv[c];
+    r.thv_dn = k == 0 ? r.thv : thv[c - sk];
+    return r;
+  }
+  static __device__ __forceinline__ void store(const KArgs& A, int tx, int ty, int tz, const In& v) {
+    TE_OP_C(0);
+    const Acoustic a = A.a;
+    const float *TE_R rr0 = A.p[5], *TE_R rf0 = A.p[6], *TE_R mh = A.p[7], *TE_R mf = A.p[8];
+    const float *TE_R c1 = A.p[9], *TE_R c2 = A.p[10];
+    const float cp = 1005.7f;
+    float tem = (a.dts * g.rdz) * mh[k];
+    float r2 = (tem * rr0[k]) * rf0[k + 1];
+    float r1 = (tem * rr0[k]) * rf0[k];
+    float tem1 = ((a.dts * g.rdz) * cp) * mf[k];
+    float c1a = c1[k], c1b = c1[k + 1], c2a = c2[k], c2b = c2[k + 1];
+    bool vec_v = g.nx > 3 && i < (g.nx / 4) * 4;
+    A.p[11][c] = tem * v.ppterm;
+    float p2 = 0.0f, p1 = 0.0f;
+    if (k != g.nz - 1) p2 = vec_v ? fmaf(-c2b, v.pa_up, (1.0f - c1b) * v.pa) : fmaf(1.0f - c1b, v.pa, -(c2b * v.pa_up));
+    if (k != 0) p1 = vec_v ? fmaf(c2a - 1.0f, v.pa, c1a * v.pa_dn) : fmaf(c1a, v.pa_dn, (c2a - 1.0f) * v.pa);
+    A.p[13][c] = k == g.nz - 1 ? 0.0f : r2 * p2;
+    A.p[12][c] = k == 0 ? 0.0f : r1 * p1;
+    A.p[14][c] = tem1 * fmaf(c2a, v.thv, c1a * v.thv_dn);
+  }
+};
+
+struct OpUpdateRhoPrs {
+  struct In { float thp, ppp, qv; };
+  TE_OP_INTERIOR
+  static __device__ __forceinline__ In load(const KArgs& A, int tx, int ty, int tz) {
+    TE_OP_C(0);
+    return In{A.p[2][c], A.p[3][c], A.iv[1] != 0 ? A.p[6][c] : 0.0f};
+  }
+  static __device__ __forceinline__ void store(const KArgs& A, int tx, int ty, int tz, const In& v) {
+    TE_OP_C(0);
+    const float *TE_R th0 = A.p[4], *TE_R pi0 = A.p[5];
+    float cpdrd = dcr(1005.7f, 287.04f);
+    float pi = pi0[k] + v.ppp;
+    float th = th0[k] + v.thp;
+    float p = 1e5f * rr_pow_cr(pi, cpdrd);
+    A.p[7][c] = p;
+    float rmix = A.iv[1] != 0 ? fmaf(wmax(0.0f, v.qv), 461.5f, 287.04f) : 287.04f;
+    A.p[8][c] = dcr(p, (th * pi) * rmix);
+  }
+};
+
+struct OpBuoyancyApply {
+  struct In { float wten, b_dn, b; };
+  static __device__ __forceinline__ bool active(const KArgs& A, int tx, int ty, int tz) {
+    return tx < A.g.nx && ty < A.g.ny && tz + 1 <= A.g.nz - 1;
+  }
+  static __device__ __forceinline__ In load(const KArgs& A, int tx, int ty, int tz) {
+    const Dims& g = A.g;
+    const int c = gidx(g, tx, ty, tz + 1), sk = g.sJ * g.sK;
+    return In{A.p[4][c], A.p[1][c - sk], A.p[1][c]};
+  }
+  static __device__ __forceinline__ void store(const KArgs& A, int tx, int ty, int tz, const In& v) {
+    const Dims& g = A.g;
+    const int k = tz + 1, c = gidx(g, tx, ty, k);
+    const float *TE_R c1 = A.p[2], *TE_R c2 = A.p[3];
+    A.p[4][c] = v.wten + fmaf(c1[k], v.b_dn, c2[k] * v.b);
+  }
+};
+
 // the __restrict__ build launches the row-vector form where a kernel has one
 #ifdef TE_KERNELS_FAST
 #define TE_ROWVEC(name, op) launch_rowvec<op>
@@ -876,39 +1197,39 @@ static const KernelSpec kTable[] = {
     {"adv_flux_z_weno_w", 5, {R(0), P(1), P(2), R(3), W(4)}, false, launch_adv_flux_z_weno_w},
     {"adv_assemble", 24, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), W(11), R(12), P(13), P(14),
                           P(15), P(16), R(17), P(30), P(18), W(19), R(27), P(24), P(25)}, false, launch_adv_assemble},
-    {"rk_update", 6, {R(0), R(1), P(2), P(3), W(4), R(5)}, false, launch_rk_update},
+    {"rk_update", 6, {R(0), R(1), P(2), P(3), W(4), R(5)}, false, TE_ROWVEC(rk_update, OpRkUpdate)},
     {"pdef_dum", 12, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), P(7), R(8), R(9), W(10), P(30)}, false, launch_pdef_dum},
     {"pdef_apply", 18, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), P(11), P(12), P(13), R(14),
                         R(15), W(16), P(30)}, false, launch_pdef_apply},
-    {"build_sadv", 4, {R(0), P(1), P(2), W(3)}, false, launch_build_sadv},
-    {"massflux_from_state", 10, {R(0), P(1), P(2), P(3), P(4), P(5), W(6), W(7), W(8), P(24)}, false, launch_massflux_from_state},
+    {"build_sadv", 4, {R(0), P(1), P(2), W(3)}, false, TE_ROWVEC(build_sadv, OpBuildSadv)},
+    {"massflux_from_state", 10, {R(0), P(1), P(2), P(3), P(4), P(5), W(6), W(7), W(8), P(24)}, false, TE_ROWVEC(massflux_from_state, OpMassfluxFromState)},
     {"div_massflux", 8, {R(0), P(1), P(2), P(3), P(4), W(5), P(30), P(25)}, false, TE_ROWVEC(div_massflux, OpDivMassflux)},
     {"velocity_to_massflux", 7, {R(0), P(1), P(2), W(3), W(4), W(5), P(24)}, false,
      TE_ROWVEC(velocity_to_massflux, OpVelocityToMassflux)},
-    {"stage_state_reset", 11, {R(0), P(1), P(2), P(3), P(4), W(5), W(6), W(7), W(8), W(9), P(10)}, false, launch_stage_state_reset},
+    {"stage_state_reset", 11, {R(0), P(1), P(2), P(3), P(4), W(5), W(6), W(7), W(8), W(9), P(10)}, false, TE_ROWVEC(stage_state_reset, OpStageStateReset)},
     {"stage_tendency_reset", 4, {R(0), W(1), W(2), W(3)}, false, launch_stage_tendency_reset},
-    {"buoyancy_apply", 5, {R(0), P(1), P(2), P(3), W(4)}, false, launch_buoyancy_apply},
-    {"apply_thterm", 4, {R(0), P(1), P(2), W(3)}, false, launch_apply_thterm},
+    {"buoyancy_apply", 5, {R(0), P(1), P(2), P(3), W(4)}, false, TE_ROWVEC(buoyancy_apply, OpBuoyancyApply)},
+    {"apply_thterm", 4, {R(0), P(1), P(2), W(3)}, false, TE_ROWVEC(apply_thterm, OpApplyThterm)},
     {"acoustic_prepare", 17, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), W(11), W(12), W(13),
-                              W(14), P(24), P(25)}, true, launch_acoustic_prepare},
-    {"acoustic_begin", 6, {R(0), R(1), P(2), W(3), W(4), W(5)}, true, launch_acoustic_begin},
+                              W(14), P(24), P(25)}, true, TE_ROWVEC(acoustic_prepare, OpAcousticPrepare)},
+    {"acoustic_begin", 6, {R(0), R(1), P(2), W(3), W(4), W(5)}, true, TE_ROWVEC(acoustic_begin, OpAcousticBegin)},
     {"acoustic_uv", 13, {R(0), R(1), P(2), P(3), P(4), P(5), W(6), W(7), R(8), P(30), P(21), P(23), P(25)}, true, launch_acoustic_uv},
     {"acoustic_fpk", 19, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), W(11), P(30), P(15), P(16),
                           P(17), P(24), P(25), R(26)}, true, launch_acoustic_fpk},
     {"acoustic_w_solve", 12, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), W(9), W(10), W(11)}, true, launch_acoustic_w_solve},
     {"acoustic_pp", 11, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), W(7), W(8), W(9), R(10)}, true, launch_acoustic_pp},
-    {"acoustic_accumulate", 9, {R(0), R(1), P(2), P(3), P(4), W(5), W(6), W(7), R(8)}, true, launch_acoustic_accumulate},
+    {"acoustic_accumulate", 9, {R(0), R(1), P(2), P(3), P(4), W(5), W(6), W(7), R(8)}, true, TE_ROWVEC(acoustic_accumulate, OpAcousticAccumulate)},
     {"bc_periodic_x", 2, {R(0), W(1)}, false, launch_bc_periodic_x},
     {"bc_periodic_y", 2, {R(0), W(1)}, false, launch_bc_periodic_y},
     {"update_diagnostics_moist", 20, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), P(11), P(12),
-                                      P(13), P(14), W(15), W(16), W(17), W(18), W(19)}, false, launch_update_diagnostics_moist},
+                                      P(13), P(14), W(15), W(16), W(17), W(18), W(19)}, false, TE_ROWVEC(update_diagnostics_moist, OpUpdateDiagnosticsMoist)},
     {"pressure_tendency", 15, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), R(9), R(10), R(12), P(13), R(14), W(11)},
      false, launch_pressure_tendency},
-    {"divergence3d", 7, {R(0), P(1), P(2), P(3), P(4), W(5), P(30)}, false, launch_divergence3d},
-    {"update_rho_prs", 9, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), W(7), W(8)}, false, launch_update_rho_prs},
-    {"diabatic_unapply", 10, {R(0), R(1), W(2), W(3), W(4), W(5), W(6), W(7), W(8), W(9)}, false, launch_diabatic_unapply},
-    {"diabatic_rates", 10, {R(0), R(1), P(2), P(3), P(4), P(5), W(6), W(7), W(8), W(9)}, false, launch_diabatic_rates},
-    {"ppx_finish", 3, {R(0), P(1), W(2)}, false, launch_ppx_finish},
+    {"divergence3d", 7, {R(0), P(1), P(2), P(3), P(4), W(5), P(30)}, false, TE_ROWVEC(divergence3d, OpDivergence3d)},
+    {"update_rho_prs", 9, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), W(7), W(8)}, false, TE_ROWVEC(update_rho_prs, OpUpdateRhoPrs)},
+    {"diabatic_unapply", 10, {R(0), R(1), W(2), W(3), W(4), W(5), W(6), W(7), W(8), W(9)}, false, TE_ROWVEC(diabatic_unapply, OpDiabaticUnapply)},
+    {"diabatic_rates", 10, {R(0), R(1), P(2), P(3), P(4), P(5), W(6), W(7), W(8), W(9)}, false, TE_ROWVEC(diabatic_rates, OpDiabaticRates)},
+    {"ppx_finish", 3, {R(0), P(1), W(2)}, false, TE_ROWVEC(ppx_finish, OpPpxFinish)},
 };
 
 #undef R
