@@ -355,19 +355,12 @@ struct HaloArgs {
 // Every halo point is written by exactly one thread, after that thread has read what it
 // needs (a halo point is never an interior point read by another thread).
 constexpr int kHaloX = 7;
-
-__device__ __forceinline__ void halo_point(const HaloArgs& H, int f, int dst, int src) {
-  const float v = H.f[f][src];
-  if (H.acc_rrw && H.f[f] == H.acc_w) {
-    const float wv = H.acc_w[dst], r = H.acc_rrw[dst];
-    H.acc_rrw[dst] = H.tavg > 0.0f ? fmaf(wv, H.alph, r) * H.tavg : r + wv;
-  }
-  H.f[f][dst] = v;
-}
+constexpr int kHaloLevels = 3;  // levels per thread: their loads are issued together
 
 __global__ void __launch_bounds__(256) k_halo_periodic(HaloArgs H) {
   const Dims& g = H.g;
-  const int k = blockIdx.y;
+  const int k0 = blockIdx.y * kHaloLevels;
+  const int sk = g.sJ * g.sK;
   const int xrows = g.sK;                       // x-halo rows of a level (j = -3 .. ny + 3)
   const int xwarps = (xrows + 7) / 8;           // blocks of 8 warps
   if ((int)blockIdx.x < xwarps) {
@@ -377,7 +370,25 @@ __global__ void __launch_bounds__(256) k_halo_periodic(HaloArgs H) {
     const int j = row - 3;
     const int i = col < 3 ? col - 3 : g.nx + (col - 3);
     const int ii = ((i % g.nx) + g.nx) % g.nx, jj = ((j % g.ny) + g.ny) % g.ny;
-    halo_point(H, f, gidx(g, i, j, k), gidx(g, ii, jj, k));
+    const int dst0 = gidx(g, i, j, 0), src0 = gidx(g, ii, jj, 0);
+    const bool acc = H.acc_rrw && H.f[f] == H.acc_w;
+    float v[kHaloLevels], wv[kHaloLevels], rr[kHaloLevels];
+#pragma unroll
+    for (int q = 0; q < kHaloLevels; q++) {
+      if (k0 + q > g.nz) break;
+      v[q] = H.f[f][src0 + (k0 + q) * sk];
+      if (acc) {
+        wv[q] = H.acc_w[dst0 + (k0 + q) * sk];
+        rr[q] = H.acc_rrw[dst0 + (k0 + q) * sk];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kHaloLevels; q++) {
+      if (k0 + q > g.nz) break;
+      const int dst = dst0 + (k0 + q) * sk;
+      if (acc) H.acc_rrw[dst] = H.tavg > 0.0f ? fmaf(wv[q], H.alph, rr[q]) * H.tavg : rr[q] + wv[q];
+      H.f[f][dst] = v[q];
+    }
     return;
   }
   const int t = (blockIdx.x - xwarps) * blockDim.x + threadIdx.x;
@@ -385,24 +396,34 @@ __global__ void __launch_bounds__(256) k_halo_periodic(HaloArgs H) {
   const int r = t / g.nx, i = t % g.nx;
   const int j = r < 3 ? r - 3 : g.ny + (r - 3);
   const int jj = ((j % g.ny) + g.ny) % g.ny;
-  const int dst = gidx(g, i, j, k), src = gidx(g, i, jj, k);
-  // all loads before the first store
-  float v[4];
+  const int dst0 = gidx(g, i, j, 0), src0 = gidx(g, i, jj, 0);
+  // all loads of the thread's levels before the first store
+  float v[kHaloLevels][4], wv[kHaloLevels], rr[kHaloLevels];
 #pragma unroll
-  for (int q = 0; q < 4; q++)
-    if (q < H.nf) v[q] = H.f[q][src];
-  if (H.acc_rrw) {
-    const float wv = H.acc_w[dst], rr = H.acc_rrw[dst];
-    H.acc_rrw[dst] = H.tavg > 0.0f ? fmaf(wv, H.alph, rr) * H.tavg : rr + wv;
+  for (int q = 0; q < kHaloLevels; q++) {
+    if (k0 + q > g.nz) break;
+#pragma unroll
+    for (int f = 0; f < 4; f++)
+      if (f < H.nf) v[q][f] = H.f[f][src0 + (k0 + q) * sk];
+    if (H.acc_rrw) {
+      wv[q] = H.acc_w[dst0 + (k0 + q) * sk];
+      rr[q] = H.acc_rrw[dst0 + (k0 + q) * sk];
+    }
   }
 #pragma unroll
-  for (int q = 0; q < 4; q++)
-    if (q < H.nf) H.f[q][dst] = v[q];
+  for (int q = 0; q < kHaloLevels; q++) {
+    if (k0 + q > g.nz) break;
+    const int dst = dst0 + (k0 + q) * sk;
+    if (H.acc_rrw) H.acc_rrw[dst] = H.tavg > 0.0f ? fmaf(wv[q], H.alph, rr[q]) * H.tavg : rr[q] + wv[q];
+#pragma unroll
+    for (int f = 0; f < 4; f++)
+      if (f < H.nf) H.f[f][dst] = v[q][f];
+  }
 }
 
 static void launch_halo(const HaloArgs& H, cudaStream_t s) {
   const int xblocks = (H.g.sK + 7) / 8, yblocks = (kHaloX * H.g.nx + 255) / 256;
-  dim3 b(256), gr(xblocks + yblocks, H.g.nz + 1);
+  dim3 b(256), gr(xblocks + yblocks, (H.g.nz + kHaloLevels) / kHaloLevels);
   k_halo_periodic<<<gr, b, 0, s>>>(H);
 }
 
@@ -508,10 +529,69 @@ __global__ void __launch_bounds__(kAdvTX* kAdvTY, AdvKZ<KIND>::value > 1 ? 6 : (
   }
 }
 
+// The linear kinds (and scalar WENO): a CTA takes a 32 x 8 tile of two consecutive
+// levels at once - the x- and y-faces of both levels and the three z-faces of a column
+// pair are independent, so a thread has two levels' loads in flight, and the shared
+// middle z-face is computed once.
+template <int KIND, int ST>
+__global__ void __launch_bounds__(kAdvTX* kAdvTY, 6) k_adv_fused2(AdvArgs A) {
+  __shared__ float fxs[2][kAdvTY][kAdvTX + 1];
+  __shared__ float fys[2][kAdvTY + 1][kAdvTX];
+  constexpr int dx = ST == 2 ? -1 : 0, dy = ST == 3 ? -1 : 0, dz = ST == 4 ? -1 : 0;
+  const int lx = threadIdx.x, ly = threadIdx.y, t = ly * kAdvTX + lx;
+  const int i0 = A.ilo + (int)blockIdx.x * kAdvTX, j0 = A.jlo + (int)blockIdx.y * kAdvTY;
+  const int i = i0 + lx, j = j0 + ly;
+  const int kb = A.klo + 2 * (int)blockIdx.z;
+  const bool two = kb + 1 <= A.khi;
+  const bool cell = i <= A.ihi && j <= A.jhi;
+  const int xr = t / (kAdvTX + 1), xq = t % (kAdvTX + 1);
+  const int e2 = kAdvTX * kAdvTY + lx, xr2 = e2 / (kAdvTX + 1), xq2 = e2 % (kAdvTX + 1);
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    const int k = kb + q;
+    if (q == 1 && !two) break;
+    if (in_range(A.rx, i0 + dx + xq, j0 + xr, k)) fxs[q][xr][xq] = adv_face<KIND, 0>(A.fx, i0 + dx + xq, j0 + xr, k);
+    if (in_range(A.ry, i, j0 + dy + ly, k)) fys[q][ly][lx] = adv_face<KIND, 1>(A.fy, i, j0 + dy + ly, k);
+    if (ly == 0 && lx < kAdvTY && in_range(A.rx, i0 + dx + xq2, j0 + xr2, k))
+      fxs[q][xr2][xq2] = adv_face<KIND, 0>(A.fx, i0 + dx + xq2, j0 + xr2, k);
+    if (ly == 1 && in_range(A.ry, i, j0 + dy + kAdvTY, k))
+      fys[q][kAdvTY][lx] = adv_face<KIND, 1>(A.fy, i, j0 + dy + kAdvTY, k);
+  }
+  float fz[3] = {0.0f, 0.0f, 0.0f};
+  if (cell) {
+    fz[0] = adv_face<KIND, 2>(A.fz, i, j, kb + dz);
+    fz[1] = adv_face<KIND, 2>(A.fz, i, j, kb + dz + 1);
+    if (two) fz[2] = adv_face<KIND, 2>(A.fz, i, j, kb + dz + 2);
+  }
+  __syncthreads();
+  if (!cell) return;
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    const int k = kb + q;
+    if (q == 1 && !two) break;
+    const int c = gidx(A.as.g, i, j, k);
+    const float dFx = fxs[q][ly][lx + 1] - fxs[q][ly][lx];
+    const float dFy = fys[q][ly + 1][lx] - fys[q][ly][lx];
+    float tn = assemble_t(A.as, i, j, k, c, dFx, dFy, fz[q + 1] - fz[q]);
+    if (A.accumulate) {
+      A.dest[c] = A.dest[c] + tn;
+    } else {
+      if (A.thterm) tn = fmaf(-A.div3d[c], A.thterm[c], tn);   // apply_thterm.wgsl
+      if (A.write_dest) A.dest[c] = tn;
+      if (A.phi) A.phi[c] = fmaf(A.dttmp, tn, A.phiA[c]);      // rk_update.wgsl
+    }
+  }
+}
+
 template <int KIND, int ST>
 static void launch_adv_t(const AdvArgs& A, cudaStream_t s) {
   const dim3 b(kAdvTX, kAdvTY, 1);
   constexpr int kz = AdvKZ<KIND>::value;
+  if (kz == 1) {
+    const dim3 gr((A.ihi - A.ilo + kAdvTX) / kAdvTX, (A.jhi - A.jlo + kAdvTY) / kAdvTY, (A.khi - A.klo + 2) / 2);
+    k_adv_fused2<KIND, ST><<<gr, b, 0, s>>>(A);
+    return;
+  }
   const dim3 gr((A.ihi - A.ilo + kAdvTX) / kAdvTX, (A.jhi - A.jlo + kAdvTY) / kAdvTY, (A.khi - A.klo + kz) / kz);
   k_adv_fused<KIND, ST><<<gr, b, 0, s>>>(A);
 }

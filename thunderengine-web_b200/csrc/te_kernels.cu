@@ -920,23 +920,6 @@ struct OpMassfluxFromState {
   }
 };
 
-struct OpStageStateReset {
-  struct In { float ua, va, wa, ppi, ppx; };
-  TE_OP_WHOLE(k <= g.nz)
-  static __device__ __forceinline__ In load(const KArgs& A, int tx, int ty, int tz) {
-    TE_OP_C(3);
-    return In{A.p[1][c], A.p[2][c], A.p[3][c], A.p[4][c], A.p[10][c]};
-  }
-  static __device__ __forceinline__ void store(const KArgs& A, int tx, int ty, int tz, const In& v) {
-    TE_OP_C(3);
-    A.p[5][c] = v.ua;
-    A.p[6][c] = v.va;
-    A.p[7][c] = v.wa;
-    A.p[8][c] = v.ppi;
-    A.p[9][c] = v.ppx;
-  }
-};
-
 struct OpAcousticAccumulate {
   struct In { float u, v, w, ru, rv, rw; };
   TE_OP_WHOLE(k <= g.nz)
@@ -1134,26 +1117,6 @@ struct OpAcousticPrepare {
   }
 };
 
-struct OpUpdateRhoPrs {
-  struct In { float thp, ppp, qv; };
-  TE_OP_INTERIOR
-  static __device__ __forceinline__ In load(const KArgs& A, int tx, int ty, int tz) {
-    TE_OP_C(0);
-    return In{A.p[2][c], A.p[3][c], A.iv[1] != 0 ? A.p[6][c] : 0.0f};
-  }
-  static __device__ __forceinline__ void store(const KArgs& A, int tx, int ty, int tz, const In& v) {
-    TE_OP_C(0);
-    const float *TE_R th0 = A.p[4], *TE_R pi0 = A.p[5];
-    float cpdrd = dcr(1005.7f, 287.04f);
-    float pi = pi0[k] + v.ppp;
-    float th = th0[k] + v.thp;
-    float p = 1e5f * rr_pow_cr(pi, cpdrd);
-    A.p[7][c] = p;
-    float rmix = A.iv[1] != 0 ? fmaf(wmax(0.0f, v.qv), 461.5f, 287.04f) : 287.04f;
-    A.p[8][c] = dcr(p, (th * pi) * rmix);
-  }
-};
-
 struct OpBuoyancyApply {
   struct In { float wten, b_dn, b; };
   static __device__ __forceinline__ bool active(const KArgs& A, int tx, int ty, int tz) {
@@ -1206,7 +1169,7 @@ static const KernelSpec kTable[] = {
     {"div_massflux", 8, {R(0), P(1), P(2), P(3), P(4), W(5), P(30), P(25)}, false, TE_ROWVEC(div_massflux, OpDivMassflux)},
     {"velocity_to_massflux", 7, {R(0), P(1), P(2), W(3), W(4), W(5), P(24)}, false,
      TE_ROWVEC(velocity_to_massflux, OpVelocityToMassflux)},
-    {"stage_state_reset", 11, {R(0), P(1), P(2), P(3), P(4), W(5), W(6), W(7), W(8), W(9), P(10)}, false, TE_ROWVEC(stage_state_reset, OpStageStateReset)},
+    {"stage_state_reset", 11, {R(0), P(1), P(2), P(3), P(4), W(5), W(6), W(7), W(8), W(9), P(10)}, false, launch_stage_state_reset},
     {"stage_tendency_reset", 4, {R(0), W(1), W(2), W(3)}, false, launch_stage_tendency_reset},
     {"buoyancy_apply", 5, {R(0), P(1), P(2), P(3), W(4)}, false, TE_ROWVEC(buoyancy_apply, OpBuoyancyApply)},
     {"apply_thterm", 4, {R(0), P(1), P(2), W(3)}, false, TE_ROWVEC(apply_thterm, OpApplyThterm)},
@@ -1226,7 +1189,7 @@ static const KernelSpec kTable[] = {
     {"pressure_tendency", 15, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), R(9), R(10), R(12), P(13), R(14), W(11)},
      false, launch_pressure_tendency},
     {"divergence3d", 7, {R(0), P(1), P(2), P(3), P(4), W(5), P(30)}, false, TE_ROWVEC(divergence3d, OpDivergence3d)},
-    {"update_rho_prs", 9, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), W(7), W(8)}, false, TE_ROWVEC(update_rho_prs, OpUpdateRhoPrs)},
+    {"update_rho_prs", 9, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), W(7), W(8)}, false, launch_update_rho_prs},
     {"diabatic_unapply", 10, {R(0), R(1), W(2), W(3), W(4), W(5), W(6), W(7), W(8), W(9)}, false, TE_ROWVEC(diabatic_unapply, OpDiabaticUnapply)},
     {"diabatic_rates", 10, {R(0), R(1), P(2), P(3), P(4), P(5), W(6), W(7), W(8), W(9)}, false, TE_ROWVEC(diabatic_rates, OpDiabaticRates)},
     {"ppx_finish", 3, {R(0), P(1), W(2)}, false, TE_ROWVEC(ppx_finish, OpPpxFinish)},
