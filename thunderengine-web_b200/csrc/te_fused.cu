@@ -529,69 +529,10 @@ __global__ void __launch_bounds__(kAdvTX* kAdvTY, AdvKZ<KIND>::value > 1 ? 6 : (
   }
 }
 
-// The linear kinds (and scalar WENO): a CTA takes a 32 x 8 tile of two consecutive
-// levels at once - the x- and y-faces of both levels and the three z-faces of a column
-// pair are independent, so a thread has two levels' loads in flight, and the shared
-// middle z-face is computed once.
-template <int KIND, int ST>
-__global__ void __launch_bounds__(kAdvTX* kAdvTY, 6) k_adv_fused2(AdvArgs A) {
-  __shared__ float fxs[2][kAdvTY][kAdvTX + 1];
-  __shared__ float fys[2][kAdvTY + 1][kAdvTX];
-  constexpr int dx = ST == 2 ? -1 : 0, dy = ST == 3 ? -1 : 0, dz = ST == 4 ? -1 : 0;
-  const int lx = threadIdx.x, ly = threadIdx.y, t = ly * kAdvTX + lx;
-  const int i0 = A.ilo + (int)blockIdx.x * kAdvTX, j0 = A.jlo + (int)blockIdx.y * kAdvTY;
-  const int i = i0 + lx, j = j0 + ly;
-  const int kb = A.klo + 2 * (int)blockIdx.z;
-  const bool two = kb + 1 <= A.khi;
-  const bool cell = i <= A.ihi && j <= A.jhi;
-  const int xr = t / (kAdvTX + 1), xq = t % (kAdvTX + 1);
-  const int e2 = kAdvTX * kAdvTY + lx, xr2 = e2 / (kAdvTX + 1), xq2 = e2 % (kAdvTX + 1);
-#pragma unroll
-  for (int q = 0; q < 2; q++) {
-    const int k = kb + q;
-    if (q == 1 && !two) break;
-    if (in_range(A.rx, i0 + dx + xq, j0 + xr, k)) fxs[q][xr][xq] = adv_face<KIND, 0>(A.fx, i0 + dx + xq, j0 + xr, k);
-    if (in_range(A.ry, i, j0 + dy + ly, k)) fys[q][ly][lx] = adv_face<KIND, 1>(A.fy, i, j0 + dy + ly, k);
-    if (ly == 0 && lx < kAdvTY && in_range(A.rx, i0 + dx + xq2, j0 + xr2, k))
-      fxs[q][xr2][xq2] = adv_face<KIND, 0>(A.fx, i0 + dx + xq2, j0 + xr2, k);
-    if (ly == 1 && in_range(A.ry, i, j0 + dy + kAdvTY, k))
-      fys[q][kAdvTY][lx] = adv_face<KIND, 1>(A.fy, i, j0 + dy + kAdvTY, k);
-  }
-  float fz[3] = {0.0f, 0.0f, 0.0f};
-  if (cell) {
-    fz[0] = adv_face<KIND, 2>(A.fz, i, j, kb + dz);
-    fz[1] = adv_face<KIND, 2>(A.fz, i, j, kb + dz + 1);
-    if (two) fz[2] = adv_face<KIND, 2>(A.fz, i, j, kb + dz + 2);
-  }
-  __syncthreads();
-  if (!cell) return;
-#pragma unroll
-  for (int q = 0; q < 2; q++) {
-    const int k = kb + q;
-    if (q == 1 && !two) break;
-    const int c = gidx(A.as.g, i, j, k);
-    const float dFx = fxs[q][ly][lx + 1] - fxs[q][ly][lx];
-    const float dFy = fys[q][ly + 1][lx] - fys[q][ly][lx];
-    float tn = assemble_t(A.as, i, j, k, c, dFx, dFy, fz[q + 1] - fz[q]);
-    if (A.accumulate) {
-      A.dest[c] = A.dest[c] + tn;
-    } else {
-      if (A.thterm) tn = fmaf(-A.div3d[c], A.thterm[c], tn);   // apply_thterm.wgsl
-      if (A.write_dest) A.dest[c] = tn;
-      if (A.phi) A.phi[c] = fmaf(A.dttmp, tn, A.phiA[c]);      // rk_update.wgsl
-    }
-  }
-}
-
 template <int KIND, int ST>
 static void launch_adv_t(const AdvArgs& A, cudaStream_t s) {
   const dim3 b(kAdvTX, kAdvTY, 1);
   constexpr int kz = AdvKZ<KIND>::value;
-  if (kz == 1) {
-    const dim3 gr((A.ihi - A.ilo + kAdvTX) / kAdvTX, (A.jhi - A.jlo + kAdvTY) / kAdvTY, (A.khi - A.klo + 2) / 2);
-    k_adv_fused2<KIND, ST><<<gr, b, 0, s>>>(A);
-    return;
-  }
   const dim3 gr((A.ihi - A.ilo + kAdvTX) / kAdvTX, (A.jhi - A.jlo + kAdvTY) / kAdvTY, (A.khi - A.klo + kz) / kz);
   k_adv_fused<KIND, ST><<<gr, b, 0, s>>>(A);
 }

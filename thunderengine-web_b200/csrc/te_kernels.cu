@@ -1135,6 +1135,43 @@ struct OpBuoyancyApply {
   }
 };
 
+struct OpPdefDum {
+  struct In { float s0, s, f0, f1, r0, r1; };
+  TE_OP_INTERIOR
+  static __device__ __forceinline__ int step(const KArgs& A) {
+    const int dir = A.iv[1];
+    return dir == 0 ? 1 : (dir == 1 ? A.g.sJ : A.g.sJ * A.g.sK);
+  }
+  static __device__ __forceinline__ In load(const KArgs& A, int tx, int ty, int tz) {
+    TE_OP_C(0);
+    const int st = step(A);
+    const float *TE_R sf = A.p[2], *TE_R s0 = A.p[3], *TE_R f = A.p[4], *TE_R rr = A.p[5];
+    return In{s0[c], sf[c], f[c], f[c + st], rr[c], rr[c + st]};
+  }
+  static __device__ __forceinline__ void store(const KArgs& A, int tx, int ty, int tz, const In& v) {
+    TE_OP_C(0);
+    const int dir = A.iv[1], ox = A.iv[9], oy = A.iv2[9];
+    const float *TE_R rho0 = A.p[6], *TE_R mh = A.p[7], *TE_R hm = A.p[30];
+    const float dt = A.f[8];
+    float rd = dir == 0 ? g.rdx : (dir == 1 ? g.rdy : g.rdz);
+    float base = rho0[k] * v.s0;
+    // pdef_inflow on the loaded mass fluxes (rr[c], rr[c + step])
+    bool inflow = false;
+    if (dir == 0 && ox != 0) inflow = (i == 0 && v.r0 >= 0.0f) || (i == g.nx - 1 && v.r1 <= 0.0f);
+    if (dir == 1 && oy != 0) inflow = (j == 0 && v.r0 >= 0.0f) || (j == g.ny - 1 && v.r1 <= 0.0f);
+    if (inflow) {
+      A.p[10][c] = base;
+      return;
+    }
+    float adv = (-(v.f1 - v.f0)) * rd;
+    float sdiv = (v.s * (v.r1 - v.r0)) * rd;
+    float m = dir == 0 ? hm_uh(g, hm, i) : (dir == 1 ? hm_vh(g, hm, j) : mh[k]);
+    adv = adv * m;
+    sdiv = sdiv * m;
+    A.p[10][c] = fmaf(dt, adv + sdiv, base);
+  }
+};
+
 // the __restrict__ build launches the row-vector form where a kernel has one
 #ifdef TE_KERNELS_FAST
 #define TE_ROWVEC(name, op) launch_rowvec<op>
@@ -1161,7 +1198,7 @@ static const KernelSpec kTable[] = {
     {"adv_assemble", 24, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), W(11), R(12), P(13), P(14),
                           P(15), P(16), R(17), P(30), P(18), W(19), R(27), P(24), P(25)}, false, launch_adv_assemble},
     {"rk_update", 6, {R(0), R(1), P(2), P(3), W(4), R(5)}, false, TE_ROWVEC(rk_update, OpRkUpdate)},
-    {"pdef_dum", 12, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), P(7), R(8), R(9), W(10), P(30)}, false, launch_pdef_dum},
+    {"pdef_dum", 12, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), P(7), R(8), R(9), W(10), P(30)}, false, TE_ROWVEC(pdef_dum, OpPdefDum)},
     {"pdef_apply", 18, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), P(11), P(12), P(13), R(14),
                         R(15), W(16), P(30)}, false, launch_pdef_apply},
     {"build_sadv", 4, {R(0), P(1), P(2), W(3)}, false, TE_ROWVEC(build_sadv, OpBuildSadv)},
