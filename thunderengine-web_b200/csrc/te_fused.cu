@@ -139,7 +139,7 @@ constexpr int kWorkers = kColTile * kLevels;     // 512
 constexpr int kColThreads = kWorkers + kColTile; // + the recurrence warp
 
 struct ColSmem {
-  float *cA, *cB, *A, *Bq, *s, *prev;  // [nz][32], whole column
+  float *cA, *cB, *A, *Bq, *s, *prev, *rw;  // [nz][32], whole column (rw: rrw before the substep)
   float* co;                           // [2][4][kLevels][32]: aa, bb, cc, dd per pass
 };
 
@@ -152,11 +152,12 @@ __device__ __forceinline__ ColSmem col_smem(float* base, int nz) {
   S.Bq = base + 3 * P;
   S.s = base + 4 * P;
   S.prev = base + 5 * P;
-  S.co = base + 6 * P;
+  S.rw = base + 6 * P;
+  S.co = base + 7 * P;
   return S;
 }
 
-static size_t col_smem_bytes(int nz) { return (size_t)(6 * nz + 8 * kLevels) * kColTile * sizeof(float); }
+static size_t col_smem_bytes(int nz) { return (size_t)(7 * nz + 8 * kLevels) * kColTile * sizeof(float); }
 
 // index of coefficient `term` (0 aa, 1 bb, 2 cc, 3 dd) of level slot q, lane, buffer b
 __device__ __forceinline__ int co_at(int b, int term, int q, int lane) {
@@ -166,10 +167,18 @@ __device__ __forceinline__ int co_at(int b, int term, int q, int lane) {
 __device__ __forceinline__ void workers_sync() {
   asm volatile("bar.sync 1, %0;" ::"n"(kWorkers) : "memory");
 }
+// chunk barriers 2.. (at most 14 chunks: nz <= 224): the recurrence warp arrives, the
+// workers wait
+__device__ __forceinline__ void chunk_arrive(int ch) {
+  asm volatile("bar.arrive %0, %1;" ::"r"(2 + ch), "n"(kColThreads) : "memory");
+}
+__device__ __forceinline__ void chunk_sync(int ch) {
+  asm volatile("bar.sync %0, %1;" ::"r"(2 + ch), "n"(kColThreads) : "memory");
+}
 
 // The 19 inputs of one level of one column, loaded ahead of use.
 struct LevelIn {
-  float u0, u1, v0, v1, pa0, paw, pae, pas, pan, ppten, ppterm, pk1, pk2, qk, w0, w1, pp, mm, wt;
+  float u0, u1, v0, v1, pa0, paw, pae, pas, pan, ppten, ppterm, pk1, pk2, qk, w0, w1, pp, mm, wt, rw;
 };
 
 __device__ __forceinline__ LevelIn load_level(const AcuArgs& A, int c) {
@@ -194,6 +203,7 @@ __device__ __forceinline__ LevelIn load_level(const AcuArgs& A, int c) {
   L.pp = A.pp3d[c];
   L.mm = __ldg(A.mm + c);
   L.wt = __ldg(A.wten + c);
+  L.rw = A.rrw[c];
   return L;
 }
 
@@ -240,6 +250,7 @@ __global__ void __launch_bounds__(kColThreads, 2) k_acu_column(AcuArgs A) {
           S.Bq[e] = cur.pk2 - cur.qk;
           S.prev[e] = cur.pp;
           S.s[e] = cur.pp + fk;
+          S.rw[e] = cur.rw;
           m = cur.mm;
           wt = cur.wt;
           w0 = cur.w0;
@@ -287,37 +298,55 @@ __global__ void __launch_bounds__(kColThreads, 2) k_acu_column(AcuArgs A) {
     }
     __syncthreads();
   }
-  // back substitution (recurrence warp): w(k) overwrites cA(k); w(0) = w(nz) = 0
-  if (!worker && col) {
+  // Back substitution (recurrence warp, top-down, w(k) overwrites cA(k); w(0) = 0) and the
+  // pi' update / stores of the workers overlap chunk by chunk: after the warp has the w of
+  // levels [16c, 16c + 16) it arrives on barrier 2 + c, where worker q waits before
+  // finishing level 16c + q (w(k + 1) comes from the chunk above, finished earlier).
+  const int nchunk = npass;
+  if (!worker) {
     float wk1 = wtop;
-    S.cA[(nz - 1) * kColTile + lane] = wtop;
-    for (int k = nz - 2; k >= 1; k--) {
-      const int e = k * kColTile + lane;
-      const float wk = fmaf(S.cA[e], wk1, S.cB[e]);
-      S.cA[e] = wk;
-      wk1 = wk;
+    for (int ch = nchunk - 1; ch >= 0; ch--) {
+      if (col) {
+        const int klo = ch * kLevels, khi = min(nz - 1, klo + kLevels - 1);
+        for (int k = khi; k >= klo; k--) {
+          const int e = k * kColTile + lane;
+          if (k == nz - 1) {
+            S.cA[e] = wtop;
+          } else if (k >= 1) {
+            const float wk = fmaf(S.cA[e], wk1, S.cB[e]);
+            S.cA[e] = wk;
+            wk1 = wk;
+          } else {
+            S.cA[e] = 0.0f;
+          }
+        }
+      }
+      chunk_arrive(ch);
     }
-    S.cA[lane] = 0.0f;
-  }
-  __syncthreads();
-  if (!col) return;
-  for (int k = q; k <= nz; k += kLevels + 1) {
-    const int c = c0 + k * sk;
-    if (k < nz) {
-      const int e = k * kColTile + lane;
-      const float wk = S.cA[e];
-      const float wk1 = k + 1 < nz ? S.cA[e + kColTile] : 0.0f;
-      float p = fmaf(a.alph, fmaf(wk, S.A[e], wk1 * S.Bq[e]), S.s[e]);
-      if (fabsf(p) < a.smeps) p = 0.0f;
-      A.pp3d[c] = p;
-      const float dum1 = a.kdiv * (p - S.prev[e]);
-      A.ppdw[c] = p + dum1;
-      if (A.saveX != 0) A.ppx[c] = dum1;
-      A.w[c] = wk;
-      A.rrw[c] = A.tavg > 0.0f ? fmaf(wk, a.alph, A.rrw[c]) * A.tavg : A.rrw[c] + wk;
-    } else {
+    if (col) {  // level nz: w = 0 and its accumulation
+      const int c = c0 + nz * sk;
+      const float r = A.rrw[c];
       A.w[c] = 0.0f;
-      A.rrw[c] = A.tavg > 0.0f ? fmaf(0.0f, a.alph, A.rrw[c]) * A.tavg : A.rrw[c] + 0.0f;
+      A.rrw[c] = A.tavg > 0.0f ? fmaf(0.0f, a.alph, r) * A.tavg : r + 0.0f;
+    }
+  } else {
+    for (int ch = nchunk - 1; ch >= 0; ch--) {
+      chunk_sync(ch);
+      const int k = ch * kLevels + q;
+      if (col && k < nz) {
+        const int c = c0 + k * sk, e = k * kColTile + lane;
+        const float wk = S.cA[e];
+        const float wk1 = k + 1 < nz ? S.cA[e + kColTile] : 0.0f;
+        float p = fmaf(a.alph, fmaf(wk, S.A[e], wk1 * S.Bq[e]), S.s[e]);
+        if (fabsf(p) < a.smeps) p = 0.0f;
+        A.pp3d[c] = p;
+        const float dum1 = a.kdiv * (p - S.prev[e]);
+        A.ppdw[c] = p + dum1;
+        if (A.saveX != 0) A.ppx[c] = dum1;
+        A.w[c] = wk;
+        const float r = S.rw[e];
+        A.rrw[c] = A.tavg > 0.0f ? fmaf(wk, a.alph, r) * A.tavg : r + wk;
+      }
     }
   }
 }
