@@ -16,15 +16,16 @@ struct FaceRange {
 
 // The five values of an upwind-biased stencil at face index c along stride s: on the
 // upwind side (up) c-3s .. c+s, else c+2s .. c-2s (reversed), both moved by `shift`
-// points along the axis.  The side is chosen before the reconstruction, so each face
-// evaluates one reconstruction whatever the flow direction in its warp.
+// points along the axis.  The six points of both sides are loaded before the side is
+// known (the loads do not wait for the mass flux that decides it), then the side is
+// chosen, so each face evaluates one reconstruction whatever the flow direction.
 struct Sten5 {
   float s1, s2, s3, s4, s5;
 };
 __device__ __forceinline__ Sten5 sten5(const float* a, int c, int s, bool up, int shift) {
-  const int st = up ? s : -s;
-  const int b = c + shift * s + (up ? -3 * s : 2 * s);
-  return Sten5{a[b], a[b + st], a[b + 2 * st], a[b + 3 * st], a[b + 4 * st]};
+  const int b = c + (shift - 3) * s;
+  const float v0 = a[b], v1 = a[b + s], v2 = a[b + 2 * s], v3 = a[b + 3 * s], v4 = a[b + 4 * s], v5 = a[b + 5 * s];
+  return up ? Sten5{v0, v1, v2, v3, v4} : Sten5{v5, v4, v3, v2, v1};
 }
 __device__ __forceinline__ float flx5(const Sten5& t) { return flx5(t.s1, t.s2, t.s3, t.s4, t.s5); }
 __device__ __forceinline__ float weno5(const Sten5& t, float weps) { return weno5(t.s1, t.s2, t.s3, t.s4, t.s5, weps); }
@@ -282,24 +283,48 @@ __device__ __forceinline__ float face_weno_w_z(const KArgs& A, int i, int j, int
 #undef AZ
 }
 
+// Pieces of adv_assemble (adv_assemble.wgsl:139-279), shared by the per-dispatch kernel
+// and the fused advection kernel.  assemble_dv_off: offset of the second divergence
+// value the cell's stagger averages (0 for a scalar); assemble_dv: the divergence at the
+// cell from divx[c] and divx[c - off]; assemble_core: the tendency from the advected
+// value s[c], that divergence and the flux differences.
+__device__ __forceinline__ int assemble_dv_off(const KArgs& A) {
+  const int stag = A.iv[1], st = stag < 0 ? -stag : stag;
+  return st == 2 ? 1 : (st == 3 ? A.g.sJ : (st == 4 ? A.g.sJ * A.g.sK : 0));
+}
+__device__ __forceinline__ float assemble_dv(const KArgs& A, int k, float d0, float d1) {
+  const int stag = A.iv[1], st = stag < 0 ? -stag : stag;
+  const float *c1 = A.p[15], *c2 = A.p[16];
+  if (st == 2 || st == 3) return 0.5f * (d0 + d1);
+  if (st == 4) return fmaf(c2[k], d0, c1[k] * d1);
+  return d0;
+}
+__device__ __forceinline__ float assemble_core(const KArgs& A, int i, int j, int k, float sc, float dv, float dFx,
+                                               float dFy, float dFz) {
+  const Dims& g = A.g;
+  const int stag = A.iv[1], st = stag < 0 ? -stag : stag;
+  const float *rho0 = A.p[7], *rf0 = A.p[8], *mh = A.p[9], *mf = A.p[10];
+  const float* hm = A.p[30];
+  const float mz = stag < 0 ? 1.0f : (stag == 4 ? mf[k] : mh[k]);
+  const float mx = st == 2 ? hm_uf(g, hm, i) : hm_uh(g, hm, i);
+  const float my = st == 3 ? hm_vf(g, hm, j) : hm_vh(g, hm, j);
+  const float divF = fmaf(dFz * g.rdz, mz, fmaf(dFx * g.rdx, mx, (dFy * g.rdy) * my));
+  const float rho = st == 4 ? rf0[k] : rho0[k];
+  return dcr(fmaf(sc, dv, -divF), rho);
+}
+
 // adv_assemble (adv_assemble.wgsl:139-279) at cell (i, j, k) from the flux differences:
 // returns the advective tendency t (before the accumulate/store).
 __device__ __forceinline__ float assemble_t(const KArgs& A, int i, int j, int k, int c, float dFx, float dFy, float dFz) {
   const Dims& g = A.g;
   const int stag = A.iv[1];
   const float *s = A.p[2], *divx = A.p[6];
-  const float *rho0 = A.p[7], *rf0 = A.p[8], *mh = A.p[9], *mf = A.p[10];
   const float *rru = A.p[13], *rrv = A.p[14], *c1 = A.p[15], *c2 = A.p[16];
   const int openx = A.iv[17], openy = A.iv2[17];
   const float* hm = A.p[30];
   const int sj = g.sJ, sk = g.sJ * g.sK;
   const int st = stag < 0 ? -stag : stag;
-  float mz = stag < 0 ? 1.0f : (stag == 4 ? mf[k] : mh[k]);
-  float dv;
-  if (st == 2) dv = 0.5f * (divx[c] + divx[c - 1]);
-  else if (st == 3) dv = 0.5f * (divx[c] + divx[c - sj]);
-  else if (st == 4) dv = fmaf(c2[k], divx[c], c1[k] * divx[c - sk]);
-  else dv = divx[c];
+  float dv = assemble_dv(A, k, divx[c], divx[c - assemble_dv_off(A)]);
   if (openx != 0 && st != 2) {
     bool west = i == 0, east = i == g.nx - 1;
     if (west || east) {
@@ -348,11 +373,7 @@ __device__ __forceinline__ float assemble_t(const KArgs& A, int i, int j, int k,
       }
     }
   }
-  float mx = st == 2 ? hm_uf(g, hm, i) : hm_uh(g, hm, i);
-  float my = st == 3 ? hm_vf(g, hm, j) : hm_vh(g, hm, j);
-  float divF = fmaf(dFz * g.rdz, mz, fmaf(dFx * g.rdx, mx, (dFy * g.rdy) * my));
-  float rho = st == 4 ? rf0[k] : rho0[k];
-  return dcr(fmaf(s[c], dv, -divF), rho);
+  return assemble_core(A, i, j, k, s[c], dv, dFx, dFy, dFz);
 }
 
 }  // namespace te

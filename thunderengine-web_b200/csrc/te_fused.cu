@@ -139,7 +139,7 @@ constexpr int kWorkers = kColTile * kLevels;     // 512
 constexpr int kColThreads = kWorkers + kColTile; // + the recurrence warp
 
 struct ColSmem {
-  float *cA, *cB, *A, *Bq, *s, *prev, *rw;  // [nz][32], whole column (rw: rrw before the substep)
+  float *cA, *cB, *A, *Bq, *s, *prev;  // [nz][32], whole column
   float* co;                           // [2][4][kLevels][32]: aa, bb, cc, dd per pass
 };
 
@@ -152,12 +152,11 @@ __device__ __forceinline__ ColSmem col_smem(float* base, int nz) {
   S.Bq = base + 3 * P;
   S.s = base + 4 * P;
   S.prev = base + 5 * P;
-  S.rw = base + 6 * P;
-  S.co = base + 7 * P;
+  S.co = base + 6 * P;
   return S;
 }
 
-static size_t col_smem_bytes(int nz) { return (size_t)(7 * nz + 8 * kLevels) * kColTile * sizeof(float); }
+static size_t col_smem_bytes(int nz) { return (size_t)(6 * nz + 8 * kLevels) * kColTile * sizeof(float); }
 
 // index of coefficient `term` (0 aa, 1 bb, 2 cc, 3 dd) of level slot q, lane, buffer b
 __device__ __forceinline__ int co_at(int b, int term, int q, int lane) {
@@ -167,18 +166,10 @@ __device__ __forceinline__ int co_at(int b, int term, int q, int lane) {
 __device__ __forceinline__ void workers_sync() {
   asm volatile("bar.sync 1, %0;" ::"n"(kWorkers) : "memory");
 }
-// chunk barriers 2.. (at most 14 chunks: nz <= 224): the recurrence warp arrives, the
-// workers wait
-__device__ __forceinline__ void chunk_arrive(int ch) {
-  asm volatile("bar.arrive %0, %1;" ::"r"(2 + ch), "n"(kColThreads) : "memory");
-}
-__device__ __forceinline__ void chunk_sync(int ch) {
-  asm volatile("bar.sync %0, %1;" ::"r"(2 + ch), "n"(kColThreads) : "memory");
-}
 
 // The 19 inputs of one level of one column, loaded ahead of use.
 struct LevelIn {
-  float u0, u1, v0, v1, pa0, paw, pae, pas, pan, ppten, ppterm, pk1, pk2, qk, w0, w1, pp, mm, wt, rw;
+  float u0, u1, v0, v1, pa0, paw, pae, pas, pan, ppten, ppterm, pk1, pk2, qk, w0, w1, pp, mm, wt;
 };
 
 __device__ __forceinline__ LevelIn load_level(const AcuArgs& A, int c) {
@@ -203,7 +194,6 @@ __device__ __forceinline__ LevelIn load_level(const AcuArgs& A, int c) {
   L.pp = A.pp3d[c];
   L.mm = __ldg(A.mm + c);
   L.wt = __ldg(A.wten + c);
-  L.rw = A.rrw[c];
   return L;
 }
 
@@ -250,7 +240,6 @@ __global__ void __launch_bounds__(kColThreads, 2) k_acu_column(AcuArgs A) {
           S.Bq[e] = cur.pk2 - cur.qk;
           S.prev[e] = cur.pp;
           S.s[e] = cur.pp + fk;
-          S.rw[e] = cur.rw;
           m = cur.mm;
           wt = cur.wt;
           w0 = cur.w0;
@@ -298,55 +287,37 @@ __global__ void __launch_bounds__(kColThreads, 2) k_acu_column(AcuArgs A) {
     }
     __syncthreads();
   }
-  // Back substitution (recurrence warp, top-down, w(k) overwrites cA(k); w(0) = 0) and the
-  // pi' update / stores of the workers overlap chunk by chunk: after the warp has the w of
-  // levels [16c, 16c + 16) it arrives on barrier 2 + c, where worker q waits before
-  // finishing level 16c + q (w(k + 1) comes from the chunk above, finished earlier).
-  const int nchunk = npass;
-  if (!worker) {
+  // back substitution (recurrence warp): w(k) overwrites cA(k); w(0) = w(nz) = 0
+  if (!worker && col) {
     float wk1 = wtop;
-    for (int ch = nchunk - 1; ch >= 0; ch--) {
-      if (col) {
-        const int klo = ch * kLevels, khi = min(nz - 1, klo + kLevels - 1);
-        for (int k = khi; k >= klo; k--) {
-          const int e = k * kColTile + lane;
-          if (k == nz - 1) {
-            S.cA[e] = wtop;
-          } else if (k >= 1) {
-            const float wk = fmaf(S.cA[e], wk1, S.cB[e]);
-            S.cA[e] = wk;
-            wk1 = wk;
-          } else {
-            S.cA[e] = 0.0f;
-          }
-        }
-      }
-      chunk_arrive(ch);
+    S.cA[(nz - 1) * kColTile + lane] = wtop;
+    for (int k = nz - 2; k >= 1; k--) {
+      const int e = k * kColTile + lane;
+      const float wk = fmaf(S.cA[e], wk1, S.cB[e]);
+      S.cA[e] = wk;
+      wk1 = wk;
     }
-    if (col) {  // level nz: w = 0 and its accumulation
-      const int c = c0 + nz * sk;
-      const float r = A.rrw[c];
+    S.cA[lane] = 0.0f;
+  }
+  __syncthreads();
+  if (!col) return;
+  for (int k = q; k <= nz; k += kLevels + 1) {
+    const int c = c0 + k * sk;
+    if (k < nz) {
+      const int e = k * kColTile + lane;
+      const float wk = S.cA[e];
+      const float wk1 = k + 1 < nz ? S.cA[e + kColTile] : 0.0f;
+      float p = fmaf(a.alph, fmaf(wk, S.A[e], wk1 * S.Bq[e]), S.s[e]);
+      if (fabsf(p) < a.smeps) p = 0.0f;
+      A.pp3d[c] = p;
+      const float dum1 = a.kdiv * (p - S.prev[e]);
+      A.ppdw[c] = p + dum1;
+      if (A.saveX != 0) A.ppx[c] = dum1;
+      A.w[c] = wk;
+      A.rrw[c] = A.tavg > 0.0f ? fmaf(wk, a.alph, A.rrw[c]) * A.tavg : A.rrw[c] + wk;
+    } else {
       A.w[c] = 0.0f;
-      A.rrw[c] = A.tavg > 0.0f ? fmaf(0.0f, a.alph, r) * A.tavg : r + 0.0f;
-    }
-  } else {
-    for (int ch = nchunk - 1; ch >= 0; ch--) {
-      chunk_sync(ch);
-      const int k = ch * kLevels + q;
-      if (col && k < nz) {
-        const int c = c0 + k * sk, e = k * kColTile + lane;
-        const float wk = S.cA[e];
-        const float wk1 = k + 1 < nz ? S.cA[e + kColTile] : 0.0f;
-        float p = fmaf(a.alph, fmaf(wk, S.A[e], wk1 * S.Bq[e]), S.s[e]);
-        if (fabsf(p) < a.smeps) p = 0.0f;
-        A.pp3d[c] = p;
-        const float dum1 = a.kdiv * (p - S.prev[e]);
-        A.ppdw[c] = p + dum1;
-        if (A.saveX != 0) A.ppx[c] = dum1;
-        A.w[c] = wk;
-        const float r = S.rw[e];
-        A.rrw[c] = A.tavg > 0.0f ? fmaf(wk, a.alph, r) * A.tavg : r + wk;
-      }
+      A.rrw[c] = A.tavg > 0.0f ? fmaf(0.0f, a.alph, A.rrw[c]) * A.tavg : A.rrw[c] + 0.0f;
     }
   }
 }
@@ -519,7 +490,7 @@ struct AdvKZ {
 };
 
 template <int KIND, int ST>
-__global__ void __launch_bounds__(kAdvTX* kAdvTY, AdvKZ<KIND>::value > 1 ? 6 : (KIND == kWeno ? 7 : 8)) k_adv_fused(AdvArgs A) {
+__global__ void __launch_bounds__(kAdvTX* kAdvTY, AdvKZ<KIND>::value > 1 ? 5 : 6) k_adv_fused(AdvArgs A) {
   constexpr int kAdvKZ = AdvKZ<KIND>::value;
   __shared__ float fxs[2][kAdvTY][kAdvTX + 1];
   __shared__ float fys[2][kAdvTY + 1][kAdvTX];
@@ -532,7 +503,22 @@ __global__ void __launch_bounds__(kAdvTX* kAdvTY, AdvKZ<KIND>::value > 1 ? 6 : (
   const int xr = t / (kAdvTX + 1), xq = t % (kAdvTX + 1);                       // x-face of this thread
   const int e2 = kAdvTX * kAdvTY + lx, xr2 = e2 / (kAdvTX + 1), xq2 = e2 % (kAdvTX + 1);  // 256..263, warp 0
   float fzb = cell ? adv_face<KIND, 2>(A.fz, i, j, kb + dz) : 0.0f;
+  const int dvoff = assemble_dv_off(A.as);
   for (int k = kb, b = 0; k <= ke; k++, b ^= 1) {
+    // the cell's own inputs first, so their loads overlap the face computations
+    const int c = gidx(A.as.g, i, j, k);
+    float sc = 0.0f, d0 = 0.0f, d1 = 0.0f, dst = 0.0f, dv3 = 0.0f, tht = 0.0f, pa = 0.0f;
+    if (cell) {
+      sc = A.as.p[2][c];
+      d0 = A.as.p[6][c];
+      d1 = A.as.p[6][c - dvoff];
+      if (A.accumulate) dst = A.dest[c];
+      if (A.thterm) {
+        dv3 = A.div3d[c];
+        tht = A.thterm[c];
+      }
+      if (A.phi) pa = A.phiA[c];
+    }
     if (in_range(A.rx, i0 + dx + xq, j0 + xr, k)) fxs[b][xr][xq] = adv_face<KIND, 0>(A.fx, i0 + dx + xq, j0 + xr, k);
     if (in_range(A.ry, i, j0 + dy + ly, k)) fys[b][ly][lx] = adv_face<KIND, 1>(A.fy, i, j0 + dy + ly, k);
     if (ly == 0 && lx < kAdvTY && in_range(A.rx, i0 + dx + xq2, j0 + xr2, k))
@@ -542,16 +528,17 @@ __global__ void __launch_bounds__(kAdvTX* kAdvTY, AdvKZ<KIND>::value > 1 ? 6 : (
     const float fzt = cell ? adv_face<KIND, 2>(A.fz, i, j, k + dz + 1) : 0.0f;
     __syncthreads();
     if (cell) {
-      const int c = gidx(A.as.g, i, j, k);
       const float dFx = fxs[b][ly][lx + 1] - fxs[b][ly][lx];
       const float dFy = fys[b][ly + 1][lx] - fys[b][ly][lx];
-      float tn = assemble_t(A.as, i, j, k, c, dFx, dFy, fzt - fzb);
+      // adv_assemble without its open-boundary branches (the planner fuses closed and
+      // periodic boundaries only)
+      float tn = assemble_core(A.as, i, j, k, sc, assemble_dv(A.as, k, d0, d1), dFx, dFy, fzt - fzb);
       if (A.accumulate) {
-        A.dest[c] = A.dest[c] + tn;
+        A.dest[c] = dst + tn;
       } else {
-        if (A.thterm) tn = fmaf(-A.div3d[c], A.thterm[c], tn);   // apply_thterm.wgsl
+        if (A.thterm) tn = fmaf(-dv3, tht, tn);                 // apply_thterm.wgsl
         if (A.write_dest) A.dest[c] = tn;
-        if (A.phi) A.phi[c] = fmaf(A.dttmp, tn, A.phiA[c]);      // rk_update.wgsl
+        if (A.phi) A.phi[c] = fmaf(A.dttmp, tn, pa);            // rk_update.wgsl
       }
     }
     fzb = fzt;
