@@ -490,7 +490,7 @@ struct AdvKZ {
 };
 
 template <int KIND, int ST>
-__global__ void __launch_bounds__(kAdvTX* kAdvTY, AdvKZ<KIND>::value > 1 ? 5 : 6) k_adv_fused(AdvArgs A) {
+__global__ void __launch_bounds__(kAdvTX* kAdvTY, AdvKZ<KIND>::value > 1 ? 6 : 8) k_adv_fused(AdvArgs A) {
   constexpr int kAdvKZ = AdvKZ<KIND>::value;
   __shared__ float fxs[2][kAdvTY][kAdvTX + 1];
   __shared__ float fys[2][kAdvTY + 1][kAdvTX];
