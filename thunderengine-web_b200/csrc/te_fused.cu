@@ -137,6 +137,7 @@ constexpr int kColTile = 32;
 constexpr int kLevels = 16;                      // worker warps = levels per pass
 constexpr int kWorkers = kColTile * kLevels;     // 512
 constexpr int kColThreads = kWorkers + kColTile; // + the recurrence warp
+constexpr int kEpiLevels = 6;                    // levels 0..nz per thread in the epilogue: nz < 6 * 17
 
 struct ColSmem {
   float *cA, *cB, *A, *Bq, *s, *prev;  // [nz][32], whole column
@@ -301,7 +302,18 @@ __global__ void __launch_bounds__(kColThreads, 2) k_acu_column(AcuArgs A) {
   }
   __syncthreads();
   if (!col) return;
-  for (int k = q; k <= nz; k += kLevels + 1) {
+  // pi' update and stores, levels q, q + 17, ... (at most kEpiLevels each): the rrw loads
+  // of all of a thread's levels are issued first
+  float rr[kEpiLevels];
+#pragma unroll
+  for (int n = 0; n < kEpiLevels; n++) {
+    const int k = q + n * (kLevels + 1);
+    if (k <= nz) rr[n] = A.rrw[c0 + k * sk];
+  }
+#pragma unroll
+  for (int n = 0; n < kEpiLevels; n++) {
+    const int k = q + n * (kLevels + 1);
+    if (k > nz) break;
     const int c = c0 + k * sk;
     if (k < nz) {
       const int e = k * kColTile + lane;
@@ -314,10 +326,10 @@ __global__ void __launch_bounds__(kColThreads, 2) k_acu_column(AcuArgs A) {
       A.ppdw[c] = p + dum1;
       if (A.saveX != 0) A.ppx[c] = dum1;
       A.w[c] = wk;
-      A.rrw[c] = A.tavg > 0.0f ? fmaf(wk, a.alph, A.rrw[c]) * A.tavg : A.rrw[c] + wk;
+      A.rrw[c] = A.tavg > 0.0f ? fmaf(wk, a.alph, rr[n]) * A.tavg : rr[n] + wk;
     } else {
       A.w[c] = 0.0f;
-      A.rrw[c] = A.tavg > 0.0f ? fmaf(0.0f, a.alph, A.rrw[c]) * A.tavg : A.rrw[c] + 0.0f;
+      A.rrw[c] = A.tavg > 0.0f ? fmaf(0.0f, a.alph, rr[n]) * A.tavg : rr[n] + 0.0f;
     }
   }
 }
@@ -790,7 +802,8 @@ static bool match_substep(const std::vector<Op>& ops, size_t i, FusedSegment& s,
   const Op& acc = ops[i + 6];
   if (!is_name(acc, "acoustic_accumulate")) return false;
   const Dims& g = uv.args.g;
-  if (g.nx < 1 || g.ny < 1 || g.nz < 3 || col_smem_bytes(g.nz) > 110 * 1024) return false;
+  if (g.nx < 1 || g.ny < 1 || g.nz < 3 || g.nz + 1 > kEpiLevels * (kLevels + 1) || col_smem_bytes(g.nz) > 110 * 1024)
+    return false;
   for (const Op* o : {&fp, &ws, &pp, &acc})
     if (!same_dims(g, o->args.g) || !same_acoustic(uv.args.a, o->args.a)) return false;
   // periodic (closed) lateral boundaries only
