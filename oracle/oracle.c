@@ -1319,3 +1319,137 @@ void teor_ppx_finish(uint32_t *M, const uint32_t *ARG) {
     ppx[c] = pp3d[c] + ppx[c];
   }
 }
+
+/* ------------------------------------------------------ open lateral boundaries */
+
+void teor_bc_open_x(uint32_t *M, const uint32_t *ARG) {
+  /* bc_open_x.wgsl main: zero-gradient x halos, i = -1-h <- 0 and i = last+1+h <- last
+   * (h < 3, last = nx + stagX - 1) over rows j in [-3, ny+3] and levels k <= nz */
+  Dims g = dims_at(M, B(0));
+  float *f = FPTR(1);
+  const int stagX = IVAL(2);
+  FOR_GRID {
+    int h = (int)tx, jj = (int)ty - 3, k = (int)tz;
+    if (h >= 3 || jj > g.ny + 3 || k > g.nz) continue;
+    int last = g.nx + stagX - 1;
+    f[GIDX(g, -1 - h, jj, k)] = f[GIDX(g, 0, jj, k)];
+    f[GIDX(g, last + 1 + h, jj, k)] = f[GIDX(g, last, jj, k)];
+  }
+}
+
+void teor_bc_open_y(uint32_t *M, const uint32_t *ARG) {
+  /* bc_open_y.wgsl main: the same along y, columns i in [-3, nx+3] */
+  Dims g = dims_at(M, B(0));
+  float *f = FPTR(1);
+  const int stagY = IVAL(2);
+  FOR_GRID {
+    int h = (int)tx, ii = (int)ty - 3, k = (int)tz;
+    if (h >= 3 || ii > g.nx + 3 || k > g.nz) continue;
+    int last = g.ny + stagY - 1;
+    f[GIDX(g, ii, -1 - h, k)] = f[GIDX(g, ii, 0, k)];
+    f[GIDX(g, ii, last + 1 + h, k)] = f[GIDX(g, ii, last, k)];
+  }
+}
+
+/* copysign(1e-10, x) as the reference builds it from bits */
+static inline float tiny_signed(float x) { return bitsf((fbits(1e-10f) & 0x7fffffffu) | (fbits(x) & 0x80000000u)); }
+
+/* one boundary's radiation speed at a point (radbc_ew.wgsl / radbc_ns.wgsl loop body):
+ * dx (a - b) / (dt (tiny_signed(foo) + foo)) with foo = a2 - a1 */
+static inline float radbc_speed(float dx, float a, float b, float foo, float dt) {
+  return DCR(dx * (a - b), dt * (tiny_signed(foo) + foo));
+}
+
+void teor_radbc_ew(uint32_t *M, const uint32_t *ARG) {
+  /* radbc_ew.wgsl main: per row j < ny, the level mean of the west (i = 1, clipped to
+   * [-umax, 0]) and east (i = nx-1, clipped to [0, umax]) radiation speeds of u */
+  Dims g = dims_at(M, B(0));
+  const float *ua = FPTR(1), *u3d = FPTR(2), *hm = FPTR(30);
+  const float dt = FVAL(3);
+  float *radbcw = FPTR(4), *radbce = FPTR(5);
+  FOR_GRID {
+    int j = (int)tx;
+    if (j >= g.ny) continue;
+    const float umax = 350.0f;
+    float dxw = DCR(DCR(1.0f, g.rdx), hm_uf(&g, hm, 1));
+    float dxe = DCR(DCR(1.0f, g.rdx), hm_uf(&g, hm, g.nx - 1));
+    float avgw = 0.0f, avge = 0.0f;
+    for (int k = 0; k < g.nz; k++) {
+      int c1 = GIDX(g, 1, j, k), c2 = GIDX(g, 2, j, k);
+      float foo = ua[c2] - ua[c1];
+      float cbcw = radbc_speed(dxw, ua[c1], u3d[c1], foo, dt);
+      cbcw = fmax_(fmin_(cbcw, 0.0f), -umax);
+      avgw = avgw + cbcw;
+      int ce = GIDX(g, g.nx - 1, j, k), ce2 = GIDX(g, g.nx - 2, j, k);
+      foo = ua[ce] - ua[ce2];
+      float cbce = radbc_speed(dxe, ua[ce], u3d[ce], foo, dt);
+      cbce = fmin_(fmax_(cbce, 0.0f), umax);
+      avge = avge + cbce;
+    }
+    radbcw[j] = DCR(avgw, (float)g.nz);
+    radbce[j] = DCR(avge, (float)g.nz);
+  }
+}
+
+void teor_radbc_ns(uint32_t *M, const uint32_t *ARG) {
+  /* radbc_ns.wgsl main: per column i < nx, the same for v at j = 1 (south) and
+   * j = ny-1 (north) */
+  Dims g = dims_at(M, B(0));
+  const float *va = FPTR(1), *v3d = FPTR(2), *hm = FPTR(30);
+  const float dt = FVAL(3);
+  float *radbcs = FPTR(4), *radbcn = FPTR(5);
+  FOR_GRID {
+    int i = (int)tx;
+    if (i >= g.nx) continue;
+    const float umax = 350.0f;
+    float dys = DCR(DCR(1.0f, g.rdy), hm_vf(&g, hm, 1));
+    float dyn = DCR(DCR(1.0f, g.rdy), hm_vf(&g, hm, g.ny - 1));
+    float avgs = 0.0f, avgn = 0.0f;
+    for (int k = 0; k < g.nz; k++) {
+      int c1 = GIDX(g, i, 1, k), c2 = GIDX(g, i, 2, k);
+      float foo = va[c2] - va[c1];
+      float cbcs = radbc_speed(dys, va[c1], v3d[c1], foo, dt);
+      cbcs = fmax_(fmin_(cbcs, 0.0f), -umax);
+      avgs = avgs + cbcs;
+      int cn = GIDX(g, i, g.ny - 1, k), cn2 = GIDX(g, i, g.ny - 2, k);
+      foo = va[cn] - va[cn2];
+      float cbcn = radbc_speed(dyn, va[cn], v3d[cn], foo, dt);
+      cbcn = fmin_(fmax_(cbcn, 0.0f), umax);
+      avgn = avgn + cbcn;
+    }
+    radbcs[i] = DCR(avgs, (float)g.nz);
+    radbcn[i] = DCR(avgn, (float)g.nz);
+  }
+}
+
+void teor_openbc_uv_tendency(uint32_t *M, const uint32_t *ARG) {
+  /* openbc_uv_tendency.wgsl main: on open x boundaries the u faces i = 0 and i = nx
+   * (and on open y boundaries the v faces j = 0, j = ny) advance by the radiation term
+   * u = fma(dts, fma((-c * du) * rdx, uh, uten), u), du the one-sided difference */
+  Dims g = dims_at(M, B(0));
+  Acoustic a = acoustic_at(M, B(1));
+  const float *radbcw = FPTR(2), *radbce = FPTR(3), *radbcs = FPTR(4), *radbcn = FPTR(5);
+  const float *uten = FPTR(6), *vten = FPTR(7), *hm = FPTR(30);
+  float *u3d = FPTR(8), *v3d = FPTR(9);
+  const int openx = (int32_t)M[B(10)], openy = (int32_t)M[B(10) + 1];
+  FOR_GRID {
+    int n = (int)tx, k = (int)ty;
+    if (k >= g.nz) continue;
+    if (openx != 0 && n < g.ny) {
+      int j = n;
+      int cw = GIDX(g, 0, j, k);
+      u3d[cw] = fmaf(a.dts, fmaf(((-radbcw[j]) * (u3d[cw + 1] - u3d[cw])) * g.rdx, hm_uh(&g, hm, 0), uten[cw]), u3d[cw]);
+      int ce = GIDX(g, g.nx, j, k);
+      u3d[ce] = fmaf(a.dts, fmaf(((-radbce[j]) * (u3d[ce] - u3d[ce - 1])) * g.rdx, hm_uh(&g, hm, g.nx - 1), uten[ce]),
+                     u3d[ce]);
+    }
+    if (openy != 0 && n < g.nx) {
+      int i = n, sj = g.sJ;
+      int cs = GIDX(g, i, 0, k);
+      v3d[cs] = fmaf(a.dts, fmaf(((-radbcs[i]) * (v3d[cs + sj] - v3d[cs])) * g.rdy, hm_vh(&g, hm, 0), vten[cs]), v3d[cs]);
+      int cn = GIDX(g, i, g.ny, k);
+      v3d[cn] = fmaf(a.dts, fmaf(((-radbcn[i]) * (v3d[cn] - v3d[cn - sj])) * g.rdy, hm_vh(&g, hm, g.ny - 1), vten[cn]),
+                     v3d[cn]);
+    }
+  }
+}

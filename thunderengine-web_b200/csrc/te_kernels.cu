@@ -686,6 +686,130 @@ __global__ void k_bc_periodic_y(KArgs A) {
 }
 TE_LAUNCH3(bc_periodic_y)
 
+// ------------------------------------------------------ open lateral boundaries
+
+// bc_open_x.wgsl / bc_open_y.wgsl: zero-gradient halos, -1-h <- 0 and last+1+h <- last
+// (h < 3, last = n + stagger - 1)
+__global__ void k_bc_open_x(KArgs A) {
+  TE_K3
+  float* TE_R f = A.p[1];
+  const int stagX = A.iv[2];
+  const int h = tx, jj = ty - 3, k = tz;
+  if (h >= 3 || jj > g.ny + 3 || k > g.nz) return;
+  const int last = g.nx + stagX - 1;
+  f[gidx(g, -1 - h, jj, k)] = f[gidx(g, 0, jj, k)];
+  f[gidx(g, last + 1 + h, jj, k)] = f[gidx(g, last, jj, k)];
+}
+TE_LAUNCH3(bc_open_x)
+
+__global__ void k_bc_open_y(KArgs A) {
+  TE_K3
+  float* TE_R f = A.p[1];
+  const int stagY = A.iv[2];
+  const int h = tx, ii = ty - 3, k = tz;
+  if (h >= 3 || ii > g.nx + 3 || k > g.nz) return;
+  const int last = g.ny + stagY - 1;
+  f[gidx(g, ii, -1 - h, k)] = f[gidx(g, ii, 0, k)];
+  f[gidx(g, ii, last + 1 + h, k)] = f[gidx(g, ii, last, k)];
+}
+TE_LAUNCH3(bc_open_y)
+
+// copysign(1e-10, x) as the reference forms it from bits
+__device__ __forceinline__ float tiny_signed(float x) {
+  return __uint_as_float((__float_as_uint(1e-10f) & 0x7fffffffu) | (__float_as_uint(x) & 0x80000000u));
+}
+__device__ __forceinline__ float radbc_speed(float dx, float a, float b, float foo, float dt) {
+  return dcr(dx * (a - b), dt * (tiny_signed(foo) + foo));
+}
+
+// radbc_ew.wgsl: per row j < ny, the level mean of the clipped radiation speeds of u at
+// the west (i = 1) and east (i = nx - 1) faces.  One thread per row; the level loop is
+// sequential as in the reference (the sum's rounding order).
+__global__ void k_radbc_ew(KArgs A) {
+  TE_K3
+  const float *TE_R ua = A.p[1], *TE_R u3d = A.p[2], *TE_R hm = A.p[30];
+  const float dt = A.f[3];
+  float *TE_R radbcw = A.p[4], *TE_R radbce = A.p[5];
+  const int j = tx;
+  if (j >= g.ny) return;
+  const float umax = 350.0f;
+  const float dxw = dcr(dcr(1.0f, g.rdx), hm_uf(g, hm, 1));
+  const float dxe = dcr(dcr(1.0f, g.rdx), hm_uf(g, hm, g.nx - 1));
+  float avgw = 0.0f, avge = 0.0f;
+  for (int k = 0; k < g.nz; k++) {
+    const int c1 = gidx(g, 1, j, k), c2 = gidx(g, 2, j, k);
+    float foo = ua[c2] - ua[c1];
+    float cbcw = radbc_speed(dxw, ua[c1], u3d[c1], foo, dt);
+    cbcw = wmax(wmin(cbcw, 0.0f), -umax);
+    avgw = avgw + cbcw;
+    const int ce = gidx(g, g.nx - 1, j, k), ce2 = gidx(g, g.nx - 2, j, k);
+    foo = ua[ce] - ua[ce2];
+    float cbce = radbc_speed(dxe, ua[ce], u3d[ce], foo, dt);
+    cbce = wmin(wmax(cbce, 0.0f), umax);
+    avge = avge + cbce;
+  }
+  radbcw[j] = dcr(avgw, (float)g.nz);
+  radbce[j] = dcr(avge, (float)g.nz);
+}
+TE_LAUNCH3(radbc_ew)
+
+// radbc_ns.wgsl: the same for v at the south (j = 1) and north (j = ny - 1) faces
+__global__ void k_radbc_ns(KArgs A) {
+  TE_K3
+  const float *TE_R va = A.p[1], *TE_R v3d = A.p[2], *TE_R hm = A.p[30];
+  const float dt = A.f[3];
+  float *TE_R radbcs = A.p[4], *TE_R radbcn = A.p[5];
+  const int i = tx;
+  if (i >= g.nx) return;
+  const float umax = 350.0f;
+  const float dys = dcr(dcr(1.0f, g.rdy), hm_vf(g, hm, 1));
+  const float dyn = dcr(dcr(1.0f, g.rdy), hm_vf(g, hm, g.ny - 1));
+  float avgs = 0.0f, avgn = 0.0f;
+  for (int k = 0; k < g.nz; k++) {
+    const int c1 = gidx(g, i, 1, k), c2 = gidx(g, i, 2, k);
+    float foo = va[c2] - va[c1];
+    float cbcs = radbc_speed(dys, va[c1], v3d[c1], foo, dt);
+    cbcs = wmax(wmin(cbcs, 0.0f), -umax);
+    avgs = avgs + cbcs;
+    const int cn = gidx(g, i, g.ny - 1, k), cn2 = gidx(g, i, g.ny - 2, k);
+    foo = va[cn] - va[cn2];
+    float cbcn = radbc_speed(dyn, va[cn], v3d[cn], foo, dt);
+    cbcn = wmin(wmax(cbcn, 0.0f), umax);
+    avgn = avgn + cbcn;
+  }
+  radbcs[i] = dcr(avgs, (float)g.nz);
+  radbcn[i] = dcr(avgn, (float)g.nz);
+}
+TE_LAUNCH3(radbc_ns)
+
+// openbc_uv_tendency.wgsl: on open x boundaries the u faces i = 0 and i = nx, on open y
+// boundaries the v faces j = 0 and j = ny, advance by the radiation term
+__global__ void k_openbc_uv_tendency(KArgs A) {
+  TE_K3
+  const Acoustic a = A.a;
+  const float *TE_R radbcw = A.p[2], *TE_R radbce = A.p[3], *TE_R radbcs = A.p[4], *TE_R radbcn = A.p[5];
+  const float *TE_R uten = A.p[6], *TE_R vten = A.p[7], *TE_R hm = A.p[30];
+  float *TE_R u3d = A.p[8], *TE_R v3d = A.p[9];
+  const int openx = A.iv[10], openy = A.iv2[10];
+  const int n = tx, k = ty;
+  if (k >= g.nz) return;
+  if (openx != 0 && n < g.ny) {
+    const int j = n, cw = gidx(g, 0, j, k);
+    u3d[cw] = fmaf(a.dts, fmaf(((-radbcw[j]) * (u3d[cw + 1] - u3d[cw])) * g.rdx, hm_uh(g, hm, 0), uten[cw]), u3d[cw]);
+    const int ce = gidx(g, g.nx, j, k);
+    u3d[ce] = fmaf(a.dts, fmaf(((-radbce[j]) * (u3d[ce] - u3d[ce - 1])) * g.rdx, hm_uh(g, hm, g.nx - 1), uten[ce]),
+                   u3d[ce]);
+  }
+  if (openy != 0 && n < g.nx) {
+    const int i = n, sj = g.sJ, cs = gidx(g, i, 0, k);
+    v3d[cs] = fmaf(a.dts, fmaf(((-radbcs[i]) * (v3d[cs + sj] - v3d[cs])) * g.rdy, hm_vh(g, hm, 0), vten[cs]), v3d[cs]);
+    const int cn = gidx(g, i, g.ny, k);
+    v3d[cn] = fmaf(a.dts, fmaf(((-radbcn[i]) * (v3d[cn] - v3d[cn - sj])) * g.rdy, hm_vh(g, hm, g.ny - 1), vten[cn]),
+                   v3d[cn]);
+  }
+}
+TE_LAUNCH3(openbc_uv_tendency)
+
 // -------------------------------------------------- thermodynamic glue
 
 __global__ void k_update_diagnostics_moist(KArgs A) {
@@ -1221,6 +1345,12 @@ static const KernelSpec kTable[] = {
     {"acoustic_accumulate", 9, {R(0), R(1), P(2), P(3), P(4), W(5), W(6), W(7), R(8)}, true, TE_ROWVEC(acoustic_accumulate, OpAcousticAccumulate)},
     {"bc_periodic_x", 2, {R(0), W(1)}, false, launch_bc_periodic_x},
     {"bc_periodic_y", 2, {R(0), W(1)}, false, launch_bc_periodic_y},
+    {"bc_open_x", 3, {R(0), W(1), R(2)}, false, launch_bc_open_x},
+    {"bc_open_y", 3, {R(0), W(1), R(2)}, false, launch_bc_open_y},
+    {"radbc_ew", 7, {R(0), P(1), P(2), R(3), W(4), W(5), P(30)}, false, launch_radbc_ew},
+    {"radbc_ns", 7, {R(0), P(1), P(2), R(3), W(4), W(5), P(30)}, false, launch_radbc_ns},
+    {"openbc_uv_tendency", 17, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), P(7), W(8), W(9), R(10), P(30), P(20), P(22),
+                                P(24), P(25), R(26)}, true, launch_openbc_uv_tendency},
     {"update_diagnostics_moist", 20, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), P(11), P(12),
                                       P(13), P(14), W(15), W(16), W(17), W(18), W(19)}, false, TE_ROWVEC(update_diagnostics_moist, OpUpdateDiagnosticsMoist)},
     {"pressure_tendency", 15, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), R(9), R(10), R(12), P(13), R(14), W(11)},
