@@ -1453,3 +1453,31 @@ void teor_openbc_uv_tendency(uint32_t *M, const uint32_t *ARG) {
     }
   }
 }
+
+/* ------------------------------------------------------- turbulence bookkeeping */
+
+void teor_turb_zero(uint32_t *M, const uint32_t *ARG) {
+  /* turb_zero.wgsl main: f[i + strideJ (j + strideK k)] = 0 for i < strideJ, j < strideK,
+   * k <= nz + 1 (one level above the field's nz + 1: the reference's own range) */
+  Dims g = dims_at(M, B(0));
+  float *f = FPTR(1);
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i >= g.sJ || j >= g.sK || k > g.nz + 1) continue;
+    f[i + g.sJ * (j + g.sK * k)] = 0.0f;
+  }
+}
+
+void teor_turb_add_tendency(uint32_t *M, const uint32_t *ARG) {
+  /* turb_add_tendency.wgsl main: dst = fma(scale, src, dst) over the whole field */
+  Dims g = dims_at(M, B(0));
+  const float *src = FPTR(1);
+  float *dst = FPTR(2);
+  const float scale = FVAL(3);
+  FOR_GRID {
+    int i = (int)tx - 3, j = (int)ty - 3, k = (int)tz;
+    if (i > g.nx + 3 || j > g.ny + 3 || k > g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    dst[c] = fmaf(scale, src[c], dst[c]);
+  }
+}

@@ -41,7 +41,8 @@ float te_rr_pow_cr(float x, float p);
   X(bc_periodic_x) X(bc_periodic_y) \
   X(update_diagnostics_moist) X(pressure_tendency) X(divergence3d) \
   X(update_rho_prs) X(diabatic_unapply) X(diabatic_rates) X(ppx_finish) \
-  X(bc_open_x) X(bc_open_y) X(radbc_ew) X(radbc_ns) X(openbc_uv_tendency)
+  X(bc_open_x) X(bc_open_y) X(radbc_ew) X(radbc_ns) X(openbc_uv_tendency) \
+  X(turb_zero) X(turb_add_tendency)
 TE_ORACLE_KERNELS(TE_ORACLE_KERNEL)
 
 #ifdef __cplusplus

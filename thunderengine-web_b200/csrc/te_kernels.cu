@@ -810,6 +810,28 @@ __global__ void k_openbc_uv_tendency(KArgs A) {
 }
 TE_LAUNCH3(openbc_uv_tendency)
 
+// ------------------------------------------------------- turbulence bookkeeping
+
+// turb_zero.wgsl: zero f[i + strideJ (j + strideK k)] for i < strideJ, j < strideK and
+// k <= nz + 1 (the reference's range, one level above a field's nz + 1)
+__global__ void k_turb_zero(KArgs A) {
+  TE_K3
+  float* TE_R f = A.p[1];
+  if (tx >= g.sJ || ty >= g.sK || tz > g.nz + 1) return;
+  f[tx + g.sJ * (ty + g.sK * tz)] = 0.0f;
+}
+TE_LAUNCH3(turb_zero)
+
+// turb_add_tendency.wgsl: dst = fma(scale, src, dst) over the whole field
+__global__ void k_turb_add_tendency(KArgs A) {
+  TE_K3
+  const float* TE_R src = A.p[1];
+  float* TE_R dst = A.p[2];
+  TE_WHOLE(k <= g.nz)
+  dst[c] = fmaf(A.f[3], src[c], dst[c]);
+}
+TE_LAUNCH3(turb_add_tendency)
+
 // -------------------------------------------------- thermodynamic glue
 
 __global__ void k_update_diagnostics_moist(KArgs A) {
@@ -1351,6 +1373,8 @@ static const KernelSpec kTable[] = {
     {"radbc_ns", 7, {R(0), P(1), P(2), R(3), W(4), W(5), P(30)}, false, launch_radbc_ns},
     {"openbc_uv_tendency", 17, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), P(7), W(8), W(9), R(10), P(30), P(20), P(22),
                                 P(24), P(25), R(26)}, true, launch_openbc_uv_tendency},
+    {"turb_zero", 2, {R(0), W(1)}, false, launch_turb_zero},
+    {"turb_add_tendency", 4, {R(0), P(1), W(2), R(3)}, false, launch_turb_add_tendency},
     {"update_diagnostics_moist", 20, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), P(11), P(12),
                                       P(13), P(14), W(15), W(16), W(17), W(18), W(19)}, false, TE_ROWVEC(update_diagnostics_moist, OpUpdateDiagnosticsMoist)},
     {"pressure_tendency", 15, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), R(9), R(10), R(12), P(13), R(14), W(11)},

@@ -332,6 +332,14 @@ void Plan::finalize_args(std::vector<Op>& ops) {
         A.iv2[ps.index] = (int)word(it->second + 1);
       }
     }
+    // turb_zero writes up to level nz + 1 of its binding (its own range check): the
+    // highest word the dispatch grid reaches must lie in the planned memory
+    if (o.name == "turb_zero" && A.p[1]) {
+      const uint64_t gi = std::min<uint64_t>(o.grid[0], A.g.sJ), gj = std::min<uint64_t>(o.grid[1], A.g.sK);
+      const uint64_t gk = std::min<uint64_t>(o.grid[2], (uint64_t)A.g.nz + 2);
+      const uint64_t top = o.bind.at(1) + (gi - 1) + (uint64_t)A.g.sJ * ((gj - 1) + (uint64_t)A.g.sK * (gk - 1));
+      if (gi && gj && gk && top >= mem_words) throw ApiError(TE_ERANGE, o.name + ": dispatch writes past the planned memory");
+    }
     // the __restrict__ build is valid when no written region overlaps another bound region
     bool disjoint = true;
     for (int q1 = 0; q1 < o.spec->nparams && disjoint; q1++) {
