@@ -88,6 +88,15 @@ int te_use_step(te_ctx *ctx, const char *cmds_json, size_t len);
  * its region hash to its slot (replay.js:102-115, 407-418); slots are not cleared. */
 int te_run(te_ctx *ctx, int nsteps, int with_hashes);
 
+/* No counterpart in the reference (its writes and reads are whole-queue operations):
+ * te_write_words / te_read queued on the context's stream without waiting, so that a
+ * caller driving several contexts overlaps one context's copies with another's step.
+ * The host buffer must stay valid and unchanged until te_sync returns (pinned memory
+ * lets the copy engine run concurrently); asynchronous writes must lie inside the tape
+ * buffers (not the setBytes area, whose host mirror te_write_words keeps). */
+int te_write_words_async(te_ctx *ctx, uint64_t word_off, const void *data, size_t bytes);
+int te_read_async(te_ctx *ctx, uint64_t word_off, uint64_t words, void *out);
+
 /* encodeSteps(enc, 1, withHashes, lastOp) restricted to ops [first_op, last_op]. */
 int te_run_ops(te_ctx *ctx, int first_op, int last_op, int with_hashes);
 

@@ -468,6 +468,26 @@ int te_write_words(te_ctx* ctx, uint64_t word_off, const void* data, size_t byte
   API_END(ctx)
 }
 
+int te_write_words_async(te_ctx* ctx, uint64_t word_off, const void* data, size_t bytes) {
+  API_BEGIN(ctx)
+  require_plan(ctx);
+  te::Plan& P = ctx->plan;
+  if (word_off + te::ceil_div(bytes, 4) > P.buffers_end)
+    throw te::ApiError(TE_ERANGE, "asynchronous writes must stay inside the tape buffers");
+  CU(cudaSetDevice(ctx->device));
+  CU(cudaMemcpyAsync(P.M + word_off, data, bytes, cudaMemcpyHostToDevice, ctx->plan.stream));
+  API_END(ctx)
+}
+
+int te_read_async(te_ctx* ctx, uint64_t word_off, uint64_t words, void* out) {
+  API_BEGIN(ctx)
+  require_plan(ctx);
+  if (word_off + words > ctx->plan.mem_words) throw te::ApiError(TE_ERANGE, "read past the end of memory");
+  CU(cudaSetDevice(ctx->device));
+  CU(cudaMemcpyAsync(out, ctx->plan.M + word_off, words * 4, cudaMemcpyDeviceToHost, ctx->plan.stream));
+  API_END(ctx)
+}
+
 int te_upload(te_ctx* ctx, int buf_id, const void* data, size_t bytes) {
   if (!ctx) return TE_EINVAL;
   if (!ctx->plan.M) return fail(ctx, TE_ESTATE, "te_plan has not been called");

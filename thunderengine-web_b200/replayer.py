@@ -86,6 +86,8 @@ EXPORTS = {
     'te_kernel_table_json': ([ctypes.c_char_p, ctypes.c_size_t], ctypes.c_size_t),
     'te_fused_segments': ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     'te_run_segment': ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    'te_write_words_async': ([ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_size_t], ctypes.c_int),
+    'te_read_async': ([ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p], ctypes.c_int),
     'te_w_solve_static_scratch': ([ctypes.POINTER(TeWSolveFields), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                    ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_void_p,
                                    ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
