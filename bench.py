@@ -430,8 +430,8 @@ def dispatch_bytes(d, km, nz):
 
 
 def end_to_end(r, run, init, cfg, a, world, mode, dev):
-    """The same metric through the public API with host buffers.  Every step uploads all
-    40 non-scratch fields of the arena from pinned host memory, plays the step and reads
+    """The same metric through the public API with host buffers.  Every step uploads every
+    non-scratch field of the arena (33 here) from pinned host memory, plays the step and reads
     th, qv, u, v, w, pp3d back into pinned memory.  Two replicas (the context of the
     timed run and a second one on its own stream) take the steps in turn, so one
     replica's copies overlap the other's step (te_write_words_async / te_read_async);
@@ -499,7 +499,7 @@ def end_to_end(r, run, init, cfg, a, world, mode, dev):
     return {'value': pts * steps * world / dt, 'unit': METRIC, 'h2d_bytes_per_step': len(state) * g.count * 4,
             'd2h_bytes_per_step': len(outs) * g.count * 4, 'steps': steps,
             'serial_value': pts * steps * world / dt_serial,
-            'path': 'per step: Replayer write_words_async x40 (pinned host) -> encode_steps(1) -> read_async x6 '
+            'path': 'per step: Replayer write_words_async of each non-scratch field (pinned host) -> encode_steps(1) -> read_async x6 '
                     '(pinned host); two replicas alternate steps so copies overlap the other replica\'s step; '
                     'serial_value: one context at a time with blocking copies'}
 
