@@ -358,7 +358,7 @@ def kernel_roofline(r, run, stream, mode):
 # (a size ncu captures quickly), divided by its interior points; traffic grows with the
 # points a launch processes.  Writes still held in L2 when the launch ends are not counted.
 NCU_DRAM_BYTES_PER_POINT = {
-    'acoustic_column (fused fpk+w_solve+pp+accumulate)': (112.05e6 + 13.56e6) / (160 * 160 * 80),
+    'acoustic_column (fused fpk+w_solve+pp+accumulate)': (112.06e6 + 13.74e6) / (160 * 160 * 80),
 }
 
 
