@@ -44,6 +44,16 @@ static void launch3(void (*k)(KArgs), const KArgs& A, cudaStream_t s) {
 #define TE_LAUNCH3(name) \
   static void launch_##name(const KArgs& A, cudaStream_t s) { launch3(k_##name, A, s); }
 
+// Halo kernels dispatch 3-4 threads along x (the halo depth) per row: blocks of 4 x 64
+// threads keep their warps full (the per-thread work is the same)
+static void launch_halo3(void (*k)(KArgs), const KArgs& A, cudaStream_t s) {
+  dim3 b(4, 64, 1);
+  dim3 gr((A.gx + 3) / 4, (A.gy + 63) / 64, A.gz);
+  k<<<gr, b, 0, s>>>(A);
+}
+#define TE_LAUNCH_HALO(name) \
+  static void launch_##name(const KArgs& A, cudaStream_t s) { launch_halo3(k_##name, A, s); }
+
 // Point-wise kernels in the __restrict__ build: a thread takes kRowVec dispatch threads
 // of the same (tx, ty) on consecutive levels, loads the inputs of all of them, then
 // computes and stores each (the loads of a warp stay 128-byte rows).  Op::active is the
@@ -672,7 +682,7 @@ __global__ void k_bc_periodic_x(KArgs A) {
   if (h < 3) f[gidx(g, -1 - h, jj, k)] = f[gidx(g, lo, jj, k)];
   f[gidx(g, g.nx + h, jj, k)] = f[gidx(g, hi, jj, k)];
 }
-TE_LAUNCH3(bc_periodic_x)
+TE_LAUNCH_HALO(bc_periodic_x)
 
 __global__ void k_bc_periodic_y(KArgs A) {
   TE_K3
@@ -684,7 +694,7 @@ __global__ void k_bc_periodic_y(KArgs A) {
   if (h < 3) f[gidx(g, i, -1 - h, k)] = f[gidx(g, i, lo, k)];
   f[gidx(g, i, g.ny + h, k)] = f[gidx(g, i, hi, k)];
 }
-TE_LAUNCH3(bc_periodic_y)
+TE_LAUNCH_HALO(bc_periodic_y)
 
 // ------------------------------------------------------ open lateral boundaries
 
@@ -700,7 +710,7 @@ __global__ void k_bc_open_x(KArgs A) {
   f[gidx(g, -1 - h, jj, k)] = f[gidx(g, 0, jj, k)];
   f[gidx(g, last + 1 + h, jj, k)] = f[gidx(g, last, jj, k)];
 }
-TE_LAUNCH3(bc_open_x)
+TE_LAUNCH_HALO(bc_open_x)
 
 __global__ void k_bc_open_y(KArgs A) {
   TE_K3
@@ -712,7 +722,7 @@ __global__ void k_bc_open_y(KArgs A) {
   f[gidx(g, ii, -1 - h, k)] = f[gidx(g, ii, 0, k)];
   f[gidx(g, ii, last + 1 + h, k)] = f[gidx(g, ii, last, k)];
 }
-TE_LAUNCH3(bc_open_y)
+TE_LAUNCH_HALO(bc_open_y)
 
 // copysign(1e-10, x) as the reference forms it from bits
 __device__ __forceinline__ float tiny_signed(float x) {
