@@ -24,10 +24,7 @@ struct Sten5 {
 };
 __device__ __forceinline__ Sten5 sten5(const float* a, int c, int s, bool up, int shift) {
   const int b = c + (shift - 3) * s;
-  // the kernels that call this never write the advected field (a tape binding it as
-  // their output too would race in the reference as well): the read-only cache path
-  const float v0 = __ldg(a + b), v1 = __ldg(a + b + s), v2 = __ldg(a + b + 2 * s), v3 = __ldg(a + b + 3 * s),
-              v4 = __ldg(a + b + 4 * s), v5 = __ldg(a + b + 5 * s);
+  const float v0 = a[b], v1 = a[b + s], v2 = a[b + 2 * s], v3 = a[b + 3 * s], v4 = a[b + 4 * s], v5 = a[b + 5 * s];
   return up ? Sten5{v0, v1, v2, v3, v4} : Sten5{v5, v4, v3, v2, v1};
 }
 __device__ __forceinline__ float flx5(const Sten5& t) { return flx5(t.s1, t.s2, t.s3, t.s4, t.s5); }

@@ -48,18 +48,14 @@ struct AcuArgs {
 __device__ __forceinline__ float uv_u(const AcuArgs& A, int i, int j, int c) {
   const Dims& g = A.g;
   const float tem1 = (g.rdx * 1005.7f) * 0.5f;
-  return fmaf(A.a.dts,
-              fmaf(-((tem1 * (__ldg(A.ppd + c) - __ldg(A.ppd + c - 1))) * hm_uf(g, A.hm, i)),
-                   __ldg(A.thv + c) + __ldg(A.thv + c - 1), __ldg(A.uten + c)),
+  return fmaf(A.a.dts, fmaf(-((tem1 * (A.ppd[c] - A.ppd[c - 1])) * hm_uf(g, A.hm, i)), A.thv[c] + A.thv[c - 1], A.uten[c]),
               A.u[c]);
 }
 __device__ __forceinline__ float uv_v(const AcuArgs& A, int i, int j, int c) {
   const Dims& g = A.g;
   const float tem2 = (g.rdy * 1005.7f) * 0.5f;
   const int sj = g.sJ;
-  return fmaf(A.a.dts,
-              fmaf(-((tem2 * (__ldg(A.ppd + c) - __ldg(A.ppd + c - sj))) * hm_vf(g, A.hm, j)),
-                   __ldg(A.thv + c) + __ldg(A.thv + c - sj), __ldg(A.vten + c)),
+  return fmaf(A.a.dts, fmaf(-((tem2 * (A.ppd[c] - A.ppd[c - sj])) * hm_vf(g, A.hm, j)), A.thv[c] + A.thv[c - sj], A.vten[c]),
               A.v[c]);
 }
 
