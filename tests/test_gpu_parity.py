@@ -222,3 +222,20 @@ def test_aliased_bindings_keep_program_order():
     cpu, gpu, mem = _compare(run, tape, init, nsteps=1)
     assert np.array_equal(gpu.read_hashes(), cpu.hashes[:gpu.hash_count])
     assert np.array_equal(mem, cpu.M[:gpu.buffers_end])
+
+
+def test_fused_plan_covers_the_step():
+    """The fused planner recognises every acoustic substep, the advection of every variable
+    except the stage-3 scalar WENO (whose fluxes pdef_dum reads) and the halo-fill runs;
+    a structural change that made it fall back to per-dispatch kernels shows here."""
+    from thunderengine_web_b200.replayer import TE_MODE_FUSED
+    run = timestep.Run(scenario.tiny(37, 29, 13, dx=500.0, dz=250.0, dt=3.0, nsound=8, us=25.0))
+    tape = run.tape(1)
+    gpu = helpers.gpu_replayer(tape, run.initial_buffers(), hashes=False, mode=TE_MODE_FUSED)
+    segs = gpu.fused_segments()
+    kinds = [s[0] for s in segs]
+    assert kinds.count(1) == sum(n for n, _ in run.schedule.loops)   # every acoustic substep (15)
+    assert kinds.count(3) == 14
+    assert kinds.count(2) >= 10
+    exact_ops = sum(s[2] - s[1] + 1 for s in segs if s[0] == 0)
+    assert exact_ops < gpu.num_ops // 3
