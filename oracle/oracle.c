@@ -1481,3 +1481,122 @@ void teor_turb_add_tendency(uint32_t *M, const uint32_t *ARG) {
     dst[c] = fmaf(scale, src[c], dst[c]);
   }
 }
+
+/* turbulence fluxes and TKE bookkeeping (the reference's subgrid turbulence kernels) */
+
+void teor_turb_scalar_flux_h(uint32_t *M, const uint32_t *ARG) {
+  /* turb_scalar_flux_h.wgsl main: horizontal subgrid scalar fluxes at the x and y faces
+   * fx = ((((-1/8 (rho + rho_w)) le) ((kh + kh_w) + (kh_up + kh_w,up))) (s - s_w)) rdx uf */
+  Dims g = dims_at(M, B(0));
+  const float *s = FPTR(1), *rho = FPTR(2), *khh = FPTR(3), *hm = FPTR(30);
+  const float leNum = FVAL(4);
+  float *fx = FPTR(5), *fy = FPTR(6);
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i > g.nx || j > g.ny || k >= g.nz) continue;
+    int c = GIDX(g, i, j, k), sj = g.sJ, sk = g.sJ * g.sK;
+    fx[c] = ((((((-0.125f) * (rho[c] + rho[c - 1])) * leNum) * ((khh[c] + khh[c - 1]) + (khh[c + sk] + khh[c - 1 + sk]))) *
+              (s[c] - s[c - 1])) * g.rdx) * hm_uf(&g, hm, i);
+    fy[c] = ((((((-0.125f) * (rho[c] + rho[c - sj])) * leNum) * ((khh[c] + khh[c - sj]) + (khh[c + sk] + khh[c - sj + sk]))) *
+              (s[c] - s[c - sj])) * g.rdy) * hm_vf(&g, hm, j);
+  }
+}
+
+void teor_turb_openbc_flux(uint32_t *M, const uint32_t *ARG) {
+  /* turb_openbc_flux.wgsl main: on open boundaries the edge fluxes copy their inner
+   * neighbours (x: 0 <- 1, nx <- nx-1; y: 0 <- 1, ny <- ny-1), levels k <= nz */
+  Dims g = dims_at(M, B(0));
+  float *fx = FPTR(1), *fy = FPTR(2);
+  const int openx = (int32_t)M[B(3)], openy = (int32_t)M[B(3) + 1];
+  FOR_GRID {
+    int n = (int)tx, k = (int)ty;
+    if (k > g.nz) continue;
+    if (openx != 0 && n <= g.ny) {
+      fx[GIDX(g, 0, n, k)] = fx[GIDX(g, 1, n, k)];
+      fx[GIDX(g, g.nx, n, k)] = fx[GIDX(g, g.nx - 1, n, k)];
+    }
+    if (openy != 0 && n <= g.nx) {
+      fy[GIDX(g, n, 0, k)] = fy[GIDX(g, n, 1, k)];
+      fy[GIDX(g, n, g.ny, k)] = fy[GIDX(g, n, g.ny - 1, k)];
+    }
+  }
+}
+
+void teor_turb_openbc_stress_x(uint32_t *M, const uint32_t *ARG) {
+  /* turb_openbc_stress_x.wgsl main: s11 halo columns -1 <- 0, nx <- nx-1 (rows j >= -1);
+   * s12 columns 0 <- 1, nx <- nx-1 (rows j >= 0) */
+  Dims g = dims_at(M, B(0));
+  float *s11 = FPTR(1), *s12 = FPTR(2);
+  FOR_GRID {
+    int j = (int)tx - 1, k = (int)ty;
+    if (j > g.ny || k >= g.nz) continue;
+    s11[GIDX(g, -1, j, k)] = s11[GIDX(g, 0, j, k)];
+    s11[GIDX(g, g.nx, j, k)] = s11[GIDX(g, g.nx - 1, j, k)];
+    if (j >= 0) {
+      s12[GIDX(g, 0, j, k)] = s12[GIDX(g, 1, j, k)];
+      s12[GIDX(g, g.nx, j, k)] = s12[GIDX(g, g.nx - 1, j, k)];
+    }
+  }
+}
+
+void teor_turb_openbc_stress_y(uint32_t *M, const uint32_t *ARG) {
+  /* turb_openbc_stress_y.wgsl main: the same along y for s22 and s12 */
+  Dims g = dims_at(M, B(0));
+  float *s22 = FPTR(1), *s12 = FPTR(2);
+  FOR_GRID {
+    int i = (int)tx - 1, k = (int)ty;
+    if (i > g.nx || k >= g.nz) continue;
+    s22[GIDX(g, i, -1, k)] = s22[GIDX(g, i, 0, k)];
+    s22[GIDX(g, i, g.ny, k)] = s22[GIDX(g, i, g.ny - 1, k)];
+    if (i >= 0) {
+      s12[GIDX(g, i, 0, k)] = s12[GIDX(g, i, 1, k)];
+      s12[GIDX(g, i, g.ny, k)] = s12[GIDX(g, i, g.ny - 1, k)];
+    }
+  }
+}
+
+void teor_tke_advance(uint32_t *M, const uint32_t *ARG) {
+  /* tke_advance.wgsl main: tke = fma(dttmp, tketen, tkea), flushed to 0 below 1e-10,
+   * interior w levels 1 .. nz-1 */
+  Dims g = dims_at(M, B(0));
+  const float *tkea = FPTR(1), *tketen = FPTR(2);
+  const float dttmp = FVAL(3);
+  float *tke = FPTR(4);
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz + 1;
+    if (i >= g.nx || j >= g.ny || k > g.nz - 1) continue;
+    int c = GIDX(g, i, j, k);
+    float v = fmaf(dttmp, tketen[c], tkea[c]);
+    tke[c] = v < 1e-10f ? 0.0f : v;
+  }
+}
+
+void teor_tke_sources(uint32_t *M, const uint32_t *ARG) {
+  /* tke_sources.wgsl main: tketen = fma(-khv, nm, -dissten) + epst */
+  Dims g = dims_at(M, B(0));
+  const float *khv = FPTR(1), *nm = FPTR(2), *dissten = FPTR(3), *epst = FPTR(4);
+  float *tketen = FPTR(5);
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz + 1;
+    if (i >= g.nx || j >= g.ny || k > g.nz - 1) continue;
+    int c = GIDX(g, i, j, k);
+    tketen[c] = fmaf(-khv[c], nm[c], -dissten[c]) + epst[c];
+  }
+}
+
+void teor_tke_flux_h(uint32_t *M, const uint32_t *ARG) {
+  /* tke_flux_h.wgsl main: horizontal TKE fluxes at the x and y faces of w levels 1..nz-1
+   * fx = (((((-1/4 (rf + rf_w)) 2) (km + km_w)) (t - t_w)) rdx) uf */
+  Dims g = dims_at(M, B(0));
+  const float *t = FPTR(1), *rf = FPTR(2), *kmh = FPTR(3), *hm = FPTR(30);
+  float *fx = FPTR(4), *fy = FPTR(5);
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz + 1;
+    if (i > g.nx || j > g.ny || k > g.nz - 1) continue;
+    int sj = g.sJ, c = GIDX(g, i, j, k);
+    fx[c] = ((((((-0.25f) * (rf[c] + rf[c - 1])) * 2.0f) * (kmh[c] + kmh[c - 1])) * (t[c] - t[c - 1])) * g.rdx) *
+            hm_uf(&g, hm, i);
+    fy[c] = ((((((-0.25f) * (rf[c] + rf[c - sj])) * 2.0f) * (kmh[c] + kmh[c - sj])) * (t[c] - t[c - sj])) * g.rdy) *
+            hm_vf(&g, hm, j);
+  }
+}

@@ -42,7 +42,8 @@ float te_rr_pow_cr(float x, float p);
   X(update_diagnostics_moist) X(pressure_tendency) X(divergence3d) \
   X(update_rho_prs) X(diabatic_unapply) X(diabatic_rates) X(ppx_finish) \
   X(bc_open_x) X(bc_open_y) X(radbc_ew) X(radbc_ns) X(openbc_uv_tendency) \
-  X(turb_zero) X(turb_add_tendency)
+  X(turb_zero) X(turb_add_tendency) X(turb_scalar_flux_h) X(turb_openbc_flux) \
+  X(turb_openbc_stress_x) X(turb_openbc_stress_y) X(tke_advance) X(tke_sources) X(tke_flux_h)
 TE_ORACLE_KERNELS(TE_ORACLE_KERNEL)
 
 #ifdef __cplusplus

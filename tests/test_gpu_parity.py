@@ -154,7 +154,7 @@ def test_golden_single_cell_in_scope_dispatches():
                 dirty.append((o.dst, o.n))
             else:
                 dirty.extend((off, ln) for _, off, ln in o.hashes if off is not None and ln)
-    assert ngpu >= 640   # 643 of the 718 dispatches: dynamics path, open boundaries, turbulence sums
+    assert ngpu >= 675   # 677 of the 718 dispatches: dynamics path, open boundaries, turbulence fluxes and sums
     fields = {v // 4 + cpu.base[2]: k for k, v in tape['fields'].items()}
     slot_field = {s: fields.get(off) for o in cpu.ops if o.kind == 'k' for s, off, _ in o.hashes}
     bad = [s for s in gpu_hashes if gpu_hashes[s] != int(want[s])]

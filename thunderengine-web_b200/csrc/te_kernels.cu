@@ -842,6 +842,109 @@ __global__ void k_turb_add_tendency(KArgs A) {
 }
 TE_LAUNCH3(turb_add_tendency)
 
+// turb_scalar_flux_h.wgsl: horizontal subgrid scalar fluxes at the x and y faces
+__global__ void k_turb_scalar_flux_h(KArgs A) {
+  TE_K3
+  const float *TE_R s = A.p[1], *TE_R rho = A.p[2], *TE_R khh = A.p[3], *TE_R hm = A.p[30];
+  const float leNum = A.f[4];
+  float *TE_R fx = A.p[5], *TE_R fy = A.p[6];
+  const int i = tx, j = ty, k = tz;
+  if (i > g.nx || j > g.ny || k >= g.nz) return;
+  const int c = gidx(g, i, j, k), sj = g.sJ, sk = g.sJ * g.sK;
+  fx[c] = ((((((-0.125f) * (rho[c] + rho[c - 1])) * leNum) * ((khh[c] + khh[c - 1]) + (khh[c + sk] + khh[c - 1 + sk]))) *
+            (s[c] - s[c - 1])) * g.rdx) * hm_uf(g, hm, i);
+  fy[c] = ((((((-0.125f) * (rho[c] + rho[c - sj])) * leNum) * ((khh[c] + khh[c - sj]) + (khh[c + sk] + khh[c - sj + sk]))) *
+            (s[c] - s[c - sj])) * g.rdy) * hm_vf(g, hm, j);
+}
+TE_LAUNCH3(turb_scalar_flux_h)
+
+// turb_openbc_flux.wgsl: edge fluxes copy their inner neighbours on open boundaries
+__global__ void k_turb_openbc_flux(KArgs A) {
+  TE_K3
+  float *TE_R fx = A.p[1], *TE_R fy = A.p[2];
+  const int openx = A.iv[3], openy = A.iv2[3];
+  const int n = tx, k = ty;
+  if (k > g.nz) return;
+  if (openx != 0 && n <= g.ny) {
+    fx[gidx(g, 0, n, k)] = fx[gidx(g, 1, n, k)];
+    fx[gidx(g, g.nx, n, k)] = fx[gidx(g, g.nx - 1, n, k)];
+  }
+  if (openy != 0 && n <= g.nx) {
+    fy[gidx(g, n, 0, k)] = fy[gidx(g, n, 1, k)];
+    fy[gidx(g, n, g.ny, k)] = fy[gidx(g, n, g.ny - 1, k)];
+  }
+}
+TE_LAUNCH3(turb_openbc_flux)
+
+// turb_openbc_stress_x.wgsl / _y.wgsl: edge stresses copy their inner neighbours
+__global__ void k_turb_openbc_stress_x(KArgs A) {
+  TE_K3
+  float *TE_R s11 = A.p[1], *TE_R s12 = A.p[2];
+  const int j = tx - 1, k = ty;
+  if (j > g.ny || k >= g.nz) return;
+  s11[gidx(g, -1, j, k)] = s11[gidx(g, 0, j, k)];
+  s11[gidx(g, g.nx, j, k)] = s11[gidx(g, g.nx - 1, j, k)];
+  if (j >= 0) {
+    s12[gidx(g, 0, j, k)] = s12[gidx(g, 1, j, k)];
+    s12[gidx(g, g.nx, j, k)] = s12[gidx(g, g.nx - 1, j, k)];
+  }
+}
+TE_LAUNCH3(turb_openbc_stress_x)
+
+__global__ void k_turb_openbc_stress_y(KArgs A) {
+  TE_K3
+  float *TE_R s22 = A.p[1], *TE_R s12 = A.p[2];
+  const int i = tx - 1, k = ty;
+  if (i > g.nx || k >= g.nz) return;
+  s22[gidx(g, i, -1, k)] = s22[gidx(g, i, 0, k)];
+  s22[gidx(g, i, g.ny, k)] = s22[gidx(g, i, g.ny - 1, k)];
+  if (i >= 0) {
+    s12[gidx(g, i, 0, k)] = s12[gidx(g, i, 1, k)];
+    s12[gidx(g, i, g.ny, k)] = s12[gidx(g, i, g.ny - 1, k)];
+  }
+}
+TE_LAUNCH3(turb_openbc_stress_y)
+
+// tke_advance.wgsl: tke = fma(dttmp, tketen, tkea), flushed to 0 below 1e-10
+__global__ void k_tke_advance(KArgs A) {
+  TE_K3
+  const float *TE_R tkea = A.p[1], *TE_R tketen = A.p[2];
+  float* TE_R tke = A.p[4];
+  const int i = tx, j = ty, k = tz + 1;
+  if (i >= g.nx || j >= g.ny || k > g.nz - 1) return;
+  const int c = gidx(g, i, j, k);
+  const float v = fmaf(A.f[3], tketen[c], tkea[c]);
+  tke[c] = v < 1e-10f ? 0.0f : v;
+}
+TE_LAUNCH3(tke_advance)
+
+// tke_sources.wgsl: tketen = fma(-khv, nm, -dissten) + epst
+__global__ void k_tke_sources(KArgs A) {
+  TE_K3
+  const float *TE_R khv = A.p[1], *TE_R nm = A.p[2], *TE_R dissten = A.p[3], *TE_R epst = A.p[4];
+  float* TE_R tketen = A.p[5];
+  const int i = tx, j = ty, k = tz + 1;
+  if (i >= g.nx || j >= g.ny || k > g.nz - 1) return;
+  const int c = gidx(g, i, j, k);
+  tketen[c] = fmaf(-khv[c], nm[c], -dissten[c]) + epst[c];
+}
+TE_LAUNCH3(tke_sources)
+
+// tke_flux_h.wgsl: horizontal TKE fluxes at the x and y faces of w levels 1..nz-1
+__global__ void k_tke_flux_h(KArgs A) {
+  TE_K3
+  const float *TE_R t = A.p[1], *TE_R rf = A.p[2], *TE_R kmh = A.p[3], *TE_R hm = A.p[30];
+  float *TE_R fx = A.p[4], *TE_R fy = A.p[5];
+  const int i = tx, j = ty, k = tz + 1;
+  if (i > g.nx || j > g.ny || k > g.nz - 1) return;
+  const int sj = g.sJ, c = gidx(g, i, j, k);
+  fx[c] = ((((((-0.25f) * (rf[c] + rf[c - 1])) * 2.0f) * (kmh[c] + kmh[c - 1])) * (t[c] - t[c - 1])) * g.rdx) *
+          hm_uf(g, hm, i);
+  fy[c] = ((((((-0.25f) * (rf[c] + rf[c - sj])) * 2.0f) * (kmh[c] + kmh[c - sj])) * (t[c] - t[c - sj])) * g.rdy) *
+          hm_vf(g, hm, j);
+}
+TE_LAUNCH3(tke_flux_h)
+
 // -------------------------------------------------- thermodynamic glue
 
 __global__ void k_update_diagnostics_moist(KArgs A) {
@@ -1385,6 +1488,13 @@ static const KernelSpec kTable[] = {
                                 P(24), P(25), R(26)}, true, launch_openbc_uv_tendency},
     {"turb_zero", 2, {R(0), W(1)}, false, launch_turb_zero},
     {"turb_add_tendency", 4, {R(0), P(1), W(2), R(3)}, false, launch_turb_add_tendency},
+    {"turb_scalar_flux_h", 8, {R(0), P(1), P(2), P(3), R(4), W(5), W(6), P(30)}, false, launch_turb_scalar_flux_h},
+    {"turb_openbc_flux", 4, {R(0), W(1), W(2), R(3)}, false, launch_turb_openbc_flux},
+    {"turb_openbc_stress_x", 3, {R(0), W(1), W(2)}, false, launch_turb_openbc_stress_x},
+    {"turb_openbc_stress_y", 3, {R(0), W(1), W(2)}, false, launch_turb_openbc_stress_y},
+    {"tke_advance", 5, {R(0), P(1), P(2), R(3), W(4)}, false, launch_tke_advance},
+    {"tke_sources", 6, {R(0), P(1), P(2), P(3), P(4), W(5)}, false, launch_tke_sources},
+    {"tke_flux_h", 7, {R(0), P(1), P(2), P(3), W(4), W(5), P(30)}, false, launch_tke_flux_h},
     {"update_diagnostics_moist", 20, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), P(11), P(12),
                                       P(13), P(14), W(15), W(16), W(17), W(18), W(19)}, false, TE_ROWVEC(update_diagnostics_moist, OpUpdateDiagnosticsMoist)},
     {"pressure_tendency", 15, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), R(9), R(10), R(12), P(13), R(14), W(11)},
