@@ -1600,3 +1600,268 @@ void teor_tke_flux_h(uint32_t *M, const uint32_t *ARG) {
             hm_vf(&g, hm, j);
   }
 }
+
+void teor_mp_pdefq(uint32_t *M, const uint32_t *ARG) {
+  /* mp_pdefq.wgsl main: per column, t1 = sum rho q; q below rmax set to 0; t2 = sum rho q
+   * after the clip; every q of the column scaled by (t1 + 1e-20) / (t2 + 1e-20), 1 when
+   * that ratio is negative (a column-mass-preserving positive-definite fix) */
+  Dims g = dims_at(M, B(0));
+  const float *rho = FPTR(1);
+  float *q = FPTR(2);
+  const float rmax = FVAL(3);
+  const int sk = g.sJ * g.sK;
+  const long GX = ARG[0], GY = ARG[1];
+#pragma omp parallel for collapse(2) schedule(static)
+  for (long ty = 0; ty < GY; ty++)
+    for (long tx = 0; tx < GX; tx++) {
+      int i = (int)tx, j = (int)ty;
+      if (i >= g.nx || j >= g.ny) continue;
+      const int base = GIDX(g, i, j, 0);
+      float t1 = 0.0f, t2 = 0.0f;
+      for (int k = 0; k < g.nz; k++) {
+        int c = base + k * sk;
+        t1 = fmaf(rho[c], q[c], t1);
+        if (q[c] < rmax) q[c] = 0.0f;
+        t2 = fmaf(rho[c], q[c], t2);
+      }
+      float t3 = DCR(t1 + 1e-20f, t2 + 1e-20f);
+      if (t3 < 0.0f) t3 = 1.0f;
+      for (int k = 0; k < g.nz; k++) q[base + k * sk] = q[base + k * sk] * t3;
+    }
+}
+
+/* Vertical subgrid flux of a scalar at w level kf of a column (turb_scalar_vert_implicit.wgsl
+ * lam_1 and lam_2): interior levels -khv ds/dz mf rf; the bottom and top levels follow the
+ * wall setting (w = 0: surface flux or the bcturbs == 2 inner gradient; w = 2: a prescribed
+ * flux; otherwise a drag towards the wall values y (bottom) and z (top)) */
+static float tsvi_vflux(const Dims *g, int base, int sk, int kf, const float *khv, const float *s, const float *mf,
+                        const float *rf, const float *wall, int useFlux, const float *sflux, int bcturbs) {
+  const int c = base + kf * sk;
+  if (kf == 0 || kf == g->nz) {
+    int inner = kf == 0 ? 1 : g->nz - 1;
+    if (wall[3] == 0.0f) {
+      if (kf == 0 && useFlux != 0) return sflux[base] * rf[c];
+      if (bcturbs != 2) return 0.0f;
+      int cc = base + inner * sk;
+      return ((((-khv[cc]) * (s[cc] - s[cc - sk])) * g->rdz) * mf[inner]) * rf[cc];
+    }
+    if (wall[3] == 2.0f) return (wall[0] * (kf == 0 ? wall[1] : wall[2])) * rf[c];
+    if (kf == 0) return (((((-wall[0]) * 2.0f) * (s[c] - wall[1])) * g->rdz) * mf[0]) * rf[c];
+    return (((((-wall[0]) * 2.0f) * (wall[2] - s[base + (g->nz - 1) * sk])) * g->rdz) * mf[g->nz]) * rf[c];
+  }
+  return ((((-khv[c]) * (s[c] - s[c - sk])) * g->rdz) * mf[kf]) * rf[c];
+}
+
+/* sten += ((fx/fy divergence) + turbz) rr at point c (turb_scalar_vert_implicit.wgsl lam_5) */
+static void tsvi_tend(const Dims *g, int c, int i, int j, float turbz, const float *fx, const float *fy,
+                      const float *hm, const float *rr, float *sten) {
+  float h = ((-(fx[c + 1] - fx[c])) * g->rdx) * hm_uh(g, hm, i) + ((-(fy[c + g->sJ] - fy[c])) * g->rdy) * hm_vh(g, hm, j);
+  sten[c] = fmaf(h + turbz, rr[c], sten[c]);
+}
+
+void teor_turb_scalar_vert_implicit(uint32_t *M, const uint32_t *ARG) {
+  /* turb_scalar_vert_implicit.wgsl main: subgrid tendency of a scalar, horizontal flux
+   * divergence plus either the explicit vertical flux divergence (explicitZ) or the
+   * implicit one: per column a tridiagonal Thomas solve of s_new - dt d/dz(K ds_new/dz)
+   * = s (cA, cB: forward sweep; cB ends as s_new), tendency rho (s_new - s) / dt.
+   * lam_3 / lam_4 are the coefficients khv mf rf (face above / below) mh rr. */
+  Dims g = dims_at(M, B(0));
+  const float *s = FPTR(1), *rho = FPTR(2), *rr = FPTR(3), *rf = FPTR(4), *khv = FPTR(5), *mh = FPTR(6), *mf = FPTR(7);
+  const float *fx = FPTR(8), *fy = FPTR(9), *sflux = FPTR(14), *hm = FPTR(30);
+  float *cA = FPTR(11), *cB = FPTR(12), *sten = FPTR(13);
+  const float dt = FVAL(10);
+  const int useFlux = IVAL(15), explicitZ = IVAL(16), bcturbs = IVAL(18);
+  float wall[4];
+  for (int q = 0; q < 4; q++) wall[q] = bitsf(M[B(17) + q]);
+  const int sk = g.sJ * g.sK;
+  const long GX = ARG[0], GY = ARG[1];
+#pragma omp parallel for collapse(2) schedule(static)
+  for (long ty = 0; ty < GY; ty++)
+    for (long tx = 0; tx < GX; tx++) {
+      int i = (int)tx, j = (int)ty;
+      if (i >= g.nx || j >= g.ny) continue;
+      const int base = GIDX(g, i, j, 0);
+      if (explicitZ != 0) {
+        float below = tsvi_vflux(&g, base, sk, 0, khv, s, mf, rf, wall, useFlux, sflux, bcturbs);
+        for (int k = 0; k < g.nz; k++) {
+          float above = tsvi_vflux(&g, base, sk, k + 1, khv, s, mf, rf, wall, useFlux, sflux, bcturbs);
+          tsvi_tend(&g, base + k * sk, i, j, ((-(above - below)) * g.rdz) * mh[k], fx, fy, hm, rr, sten);
+          below = above;
+        }
+        continue;
+      }
+#define LAM3(k) ((((khv[base + (k) * sk + sk] * mf[(k) + 1]) * rf[base + (k) * sk + sk]) * mh[k]) * rr[base + (k) * sk])
+#define LAM4(k) ((((khv[base + (k) * sk] * mf[k]) * rf[base + (k) * sk]) * mh[k]) * rr[base + (k) * sk])
+      const float tema = ((-dt) * g.rdz) * g.rdz, rdt = DCR(1.0f, dt), temc = dt * g.rdz;
+      {
+        float cfc = tema * LAM3(0), t = DCR(1.0f, 1.0f - cfc);
+        cA[base] = (-cfc) * t;
+        float cfd = s[base];
+        if (useFlux != 0 || bcturbs == 2) {
+          int c1 = base + sk;
+          float dumz = useFlux != 0 ? sflux[base] * rf[base]
+                                    : ((((-khv[c1]) * (s[c1] - s[base])) * g.rdz) * mf[1]) * rf[c1];
+          cfd = fmaf((temc * dumz) * mh[0], rr[base], s[base]);
+        }
+        cB[base] = cfd * t;
+      }
+      for (int k = 1; k < g.nz - 1; k++) {
+        int c = base + k * sk;
+        float cfa = tema * LAM4(k), cfc = tema * LAM3(k), cfb = (1.0f - cfa) - cfc;
+        float t = DCR(1.0f, fmaf(cfa, cA[c - sk], cfb));
+        cA[c] = (-cfc) * t;
+        cB[c] = fmaf(-cfa, cB[c - sk], s[c]) * t;
+      }
+      {
+        int kt = g.nz - 1, ct = base + kt * sk;
+        float cfa = tema * LAM4(kt), t = DCR(1.0f, fmaf(cfa, cA[ct - sk], 1.0f - cfa));
+        float cfd = s[ct];
+        if (bcturbs == 2) {
+          float dumz = ((((-khv[ct]) * (s[ct] - s[ct - sk])) * g.rdz) * mf[kt]) * rf[ct];
+          cfd = fmaf(-((temc * dumz) * mh[kt]), rr[ct], s[ct]);
+        }
+        float snew = fmaf(-cfa, cB[ct - sk], cfd) * t;
+        cB[ct] = snew;
+        tsvi_tend(&g, ct, i, j, (rho[ct] * (snew - s[ct])) * rdt, fx, fy, hm, rr, sten);
+      }
+#undef LAM3
+#undef LAM4
+      for (int k = g.nz - 2; k >= 0; k--) {
+        int c = base + k * sk;
+        float snew = fmaf(cA[c], cB[c + sk], cB[c]);
+        cB[c] = snew;
+        tsvi_tend(&g, c, i, j, (rho[c] * (snew - s[c])) * rdt, fx, fy, hm, rr, sten);
+      }
+    }
+}
+
+void teor_rayleigh_damping(uint32_t *M, const uint32_t *ARG) {
+  /* rayleigh_damping.wgsl main: tendencies -rdalpha tau (phi - phi_ref) for u, v, th
+   * (reference profiles u0/v0/th, or the level averages avg[k], avg[nz + k], avg[2 nz + k]
+   * when toAverage), and -rdalpha tauf w for w, tauf raised to the lateral sponge hdx/hdy */
+  Dims g = dims_at(M, B(0));
+  const float *u = FPTR(1), *v = FPTR(2), *w = FPTR(3), *th = FPTR(4), *u0 = FPTR(5), *v0 = FPTR(6);
+  const float *tauh = FPTR(7), *tauf = FPTR(8), *hdx = FPTR(14), *hdy = FPTR(15), *avg = FPTR(18), *th0 = FPTR(19);
+  float *uten = FPTR(10), *vten = FPTR(11), *wten = FPTR(12), *thten = FPTR(13);
+  const float rdalpha = FVAL(9);
+  const int lateral = IVAL(16), toAverage = IVAL(17);
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i > g.nx || j > g.ny || k > g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    if (k < g.nz) {
+      float t = tauh[k];
+      float ur = toAverage != 0 ? avg[k] : u0[k];
+      float vr = toAverage != 0 ? avg[g.nz + k] : v0[k];
+      if (j < g.ny) uten[c] = ((-rdalpha) * t) * (u[c] - ur);
+      if (i < g.nx) vten[c] = ((-rdalpha) * t) * (v[c] - vr);
+      if (i < g.nx && j < g.ny) {
+        float d = toAverage != 0 ? (th0[k] - avg[2 * g.nz + k]) + th[c] : th[c];
+        thten[c] = ((-rdalpha) * t) * d;
+      }
+    }
+    if (i < g.nx && j < g.ny) {
+      float tf = tauf[k];
+      if (lateral != 0 && k < g.nz) tf = fmax_(fmax_(tf, hdx[i]), hdy[j]);
+      wten[c] = ((-rdalpha) * tf) * w[c];
+    }
+  }
+}
+
+void teor_turb_rho_faces(uint32_t *M, const uint32_t *ARG) {
+  /* turb_rho_faces.wgsl main: rr = 1 / rho at levels k < nz; rf on w levels: interior
+   * c1 rho(k-1) + c2 rho(k), bottom and top extrapolated with the weights cgs / cgt
+   * (third weight only when nz >= 3); columns -2..nx+1, rows -2..ny+1 */
+  Dims g = dims_at(M, B(0));
+  const float *rho = FPTR(1), *c1 = FPTR(2), *c2 = FPTR(3);
+  float *rr = FPTR(4), *rf = FPTR(5);
+  float cgs[3], cgt[3];
+  for (int q = 0; q < 3; q++) {
+    cgs[q] = bitsf(M[B(6) + q]);
+    cgt[q] = bitsf(M[B(7) + q]);
+  }
+  const int sk = g.sJ * g.sK;
+  FOR_GRID {
+    int i = (int)tx - 2, j = (int)ty - 2, k = (int)tz;
+    if (i > g.nx + 1 || j > g.ny + 1 || k > g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    if (k < g.nz) rr[c] = DCR(1.0f, rho[c]);
+    if (k == 0) {
+      float r = fmaf(cgs[0], rho[c], cgs[1] * rho[c + sk]);
+      if (g.nz >= 3) r = fmaf(cgs[2], rho[c + 2 * sk], r);
+      rf[c] = r;
+    } else if (k == g.nz) {
+      float r = fmaf(cgt[0], rho[c - sk], cgt[1] * rho[c - 2 * sk]);
+      if (g.nz >= 3) r = fmaf(cgt[2], rho[c - 3 * sk], r);
+      rf[c] = r;
+    } else {
+      rf[c] = fmaf(c1[k], rho[c - sk], c2[k] * rho[c]);
+    }
+  }
+}
+
+void teor_turb_def_centers(uint32_t *M, const uint32_t *ARG) {
+  /* turb_def_centers.wgsl main: rho-weighted strain rates at cell centres (s11, s22, s33)
+   * and at the (i-1/2, j-1/2) edges (s12, with the four-point corner density) */
+  Dims g = dims_at(M, B(0));
+  const float *u = FPTR(1), *v = FPTR(2), *w = FPTR(3), *rho = FPTR(4), *mh = FPTR(5), *hm = FPTR(30);
+  float *s11 = FPTR(6), *s22 = FPTR(7), *s33 = FPTR(8), *s12 = FPTR(9);
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  FOR_GRID {
+    int i = (int)tx - 1, j = (int)ty - 1, k = (int)tz;
+    if (i > g.nx + 1 || j > g.ny + 1 || k >= g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    s11[c] = ((rho[c] * (u[c + 1] - u[c])) * g.rdx) * hm_uh(&g, hm, i);
+    s22[c] = ((rho[c] * (v[c + sj] - v[c])) * g.rdy) * hm_vh(&g, hm, j);
+    s33[c] = ((rho[c] * (w[c + sk] - w[c])) * g.rdz) * mh[k];
+    float rcorner = 0.25f * ((rho[c - 1 - sj] + rho[c]) + (rho[c - 1] + rho[c - sj]));
+    s12[c] = (0.5f * fmaf((u[c] - u[c - sj]) * g.rdy, hm_vf(&g, hm, j), ((v[c] - v[c - 1]) * g.rdx) * hm_uf(&g, hm, i))) * rcorner;
+  }
+}
+
+void teor_turb_def_faces(uint32_t *M, const uint32_t *ARG) {
+  /* turb_def_faces.wgsl main: strain rates s13, s23 on the w levels 1..nz-1 at the x and y
+   * faces, weighted by the face-averaged rf */
+  Dims g = dims_at(M, B(0));
+  const float *u = FPTR(1), *v = FPTR(2), *w = FPTR(3), *rf = FPTR(4), *mf = FPTR(5), *hm = FPTR(30);
+  float *s13 = FPTR(6), *s23 = FPTR(7);
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz + 1;
+    if (i > g.nx + 1 || j > g.ny + 1 || k > g.nz - 1) continue;
+    int c = GIDX(g, i, j, k);
+    float mfk = 0.5f * (mf[k] + mf[k]);
+    s13[c] = ((0.5f * fmaf((w[c] - w[c - 1]) * g.rdx, hm_uf(&g, hm, i), ((u[c] - u[c - sk]) * g.rdz) * mfk)) * 0.5f) * (rf[c - 1] + rf[c]);
+    s23[c] = ((0.5f * fmaf((w[c] - w[c - sj]) * g.rdy, hm_vf(&g, hm, j), ((v[c] - v[c - sk]) * g.rdz) * mfk)) * 0.5f) * (rf[c - sj] + rf[c]);
+  }
+}
+
+void teor_turb_def_assemble(uint32_t *M, const uint32_t *ARG) {
+  /* turb_def_assemble.wgsl main: deformation on w levels 1..nz-1, defv = 4 (t13 + t23) / rf^2,
+   * defh = (2 (t11 + t22 + t33) + 4 t12) / rf^2, with t11..t33 the squared centre rates
+   * interpolated by c1/c2 and t12, t13, t23 averaged over the surrounding edges and faces */
+  Dims g = dims_at(M, B(0));
+  const float *s11 = FPTR(1), *s22 = FPTR(2), *s33 = FPTR(3), *s12 = FPTR(4), *s13 = FPTR(5), *s23 = FPTR(6);
+  const float *c1 = FPTR(7), *c2 = FPTR(8), *rf = FPTR(9);
+  float *defv = FPTR(10), *defh = FPTR(11);
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz + 1;
+    if (i >= g.nx || j >= g.ny || k > g.nz - 1) continue;
+    int c = GIDX(g, i, j, k);
+    float a = c1[k], b = c2[k];
+#define SQ2(s) fmaf(a * s[c - sk], s[c - sk], (b * s[c]) * s[c])
+    float t11 = SQ2(s11), t22 = SQ2(s22), t33 = SQ2(s33);
+#undef SQ2
+#define PAIR(p, q) fmaf(s12[p], s12[p], s12[q] * s12[q])
+    float lo = PAIR(c - sk, c + 1 + sj - sk) + PAIR(c + sj - sk, c + 1 - sk);
+    float hi = PAIR(c, c + 1 + sj) + PAIR(c + sj, c + 1);
+#undef PAIR
+    float t12 = 0.25f * fmaf(a, lo, b * hi);
+    float t13 = 0.5f * fmaf(s13[c], s13[c], s13[c + 1] * s13[c + 1]);
+    float t23 = 0.5f * fmaf(s23[c], s23[c], s23[c + sj] * s23[c + sj]);
+    float rrf = DCR(1.0f, rf[c] * rf[c]);
+    defv[c] = (4.0f * (t13 + t23)) * rrf;
+    defh[c] = fmaf(2.0f, (t11 + t22) + t33, 4.0f * t12) * rrf;
+  }
+}

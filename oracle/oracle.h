@@ -43,7 +43,9 @@ float te_rr_pow_cr(float x, float p);
   X(update_rho_prs) X(diabatic_unapply) X(diabatic_rates) X(ppx_finish) \
   X(bc_open_x) X(bc_open_y) X(radbc_ew) X(radbc_ns) X(openbc_uv_tendency) \
   X(turb_zero) X(turb_add_tendency) X(turb_scalar_flux_h) X(turb_openbc_flux) \
-  X(turb_openbc_stress_x) X(turb_openbc_stress_y) X(tke_advance) X(tke_sources) X(tke_flux_h)
+  X(turb_openbc_stress_x) X(turb_openbc_stress_y) X(tke_advance) X(tke_sources) X(tke_flux_h) \
+  X(mp_pdefq) X(turb_scalar_vert_implicit) \
+  X(rayleigh_damping) X(turb_rho_faces) X(turb_def_centers) X(turb_def_faces) X(turb_def_assemble)
 TE_ORACLE_KERNELS(TE_ORACLE_KERNEL)
 
 #ifdef __cplusplus

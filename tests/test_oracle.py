@@ -81,3 +81,59 @@ def test_oracle_pinned_to_golden_single_cell(oracle_lib, ref_lib):
     bad = [s for s in range(want.size) if want[s] != p.hashes[s]]
     assert want.size == 1010 and len(bad) <= 40
     assert {slot_field[s] for s in bad} <= {'tend', 'fpk'}
+
+
+@pytest.mark.slow
+def test_column_kernels_on_branches_the_recording_does_not_take(oracle_lib, ref_lib):
+    """turb_scalar_vert_implicit and mp_pdefq, oracle vs the reference's kernels, on the
+    state of the recorded step at their first dispatch, with the flags of the branches the
+    recording does not take: explicit vertical fluxes, surface flux, bcturbs = 2 and the
+    three wall settings (turb_scalar_vert_implicit.wgsl lam_1), a clip threshold that
+    zeroes part of every column (mp_pdefq.wgsl), and the lateral sponge and level-average
+    references of rayleigh_damping.wgsl."""
+    import itertools
+    from oracle.player import CpuPlayer
+    tape, init, want, step1 = helpers.load_golden_scenario()
+    p = CpuPlayer(tape, helpers.kernels_meta())
+    p.plan(False)
+    for i, b in init.items():
+        p.upload(i, b)
+    fb = lambda x: int(np.float32(x).view(np.uint32))
+    vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    done = set()
+    compared = 0
+    for o in p.ops:
+        if o.kind == 'copy':
+            p.M[o.dst:o.dst + o.n] = p.M[o.src:o.src + o.n]
+            continue
+        if o.name in ('turb_scalar_vert_implicit', 'mp_pdefq', 'rayleigh_damping') and o.name not in done:
+            done.add(o.name)
+            B = lambda n: int(o.arg[4 + n])
+            sk = 127 * 127   # one level of the 120 x 120 recording (halo 3 on each side)
+            if o.name == 'rayleigh_damping':
+                variants = [{B(16): a, B(17): b} for a in (0, 1) for b in (0, 1)]
+            elif o.name == 'mp_pdefq':
+                q = p.M[B(2):B(2) + 8 * sk].view(np.float32)
+                nz_q = np.abs(q[q != 0])
+                variants = [{B(3): fb(np.median(nz_q) if nz_q.size else 1e-6)}, {B(3): fb(-1.0)}]
+            else:
+                variants = []
+                for uf, ez, bt, ww in itertools.product([0, 1], [0, 1], [1, 2], [0.0, 1.0, 2.0]):
+                    v = {B(15): uf, B(16): ez, B(18): bt}
+                    v.update({B(17) + q: fb(x) for q, x in enumerate([0.37, 301.5, 290.25, ww])})
+                    variants.append(v)
+            for v in variants:
+                E, F = p.M.copy(), p.M.copy()
+                for X in (E, F):
+                    for w, val in v.items():
+                        X[w] = val
+                    if o.name == 'turb_scalar_vert_implicit':
+                        X[B(14):B(14) + sk] = fb(0.011)
+                oracle_lib.get(o.name)(vp(E), vp(o.arg))
+                ref_lib.get(o.name)(vp(F), vp(o.arg))
+                assert np.array_equal(E, F), (o.name, v)
+                compared += 1
+        helpers.mixed(o.name)(vp(p.M), vp(o.arg))
+        if len(done) == 3:
+            break
+    assert compared == 30

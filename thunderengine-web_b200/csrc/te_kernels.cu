@@ -945,6 +945,257 @@ __global__ void k_tke_flux_h(KArgs A) {
 }
 TE_LAUNCH3(tke_flux_h)
 
+// Column kernels (one thread per (i, j) column, columns of a warp adjacent in i) share
+// the acoustic solve's launch shape.
+static void launch_columns(void (*k)(KArgs), const KArgs& A, cudaStream_t s) {
+  dim3 b(32, 4, 1);
+  dim3 gr((A.gx + 31) / 32, (A.gy + 3) / 4, 1);
+  k<<<gr, b, 0, s>>>(A);
+}
+#define TE_LAUNCH_COLUMNS(name) \
+  static void launch_##name(const KArgs& A, cudaStream_t s) { launch_columns(k_##name, A, s); }
+
+// mp_pdefq.wgsl: per column, q below rmax set to 0 and the column rescaled so that
+// sum rho q keeps its value before the clip ((t1 + 1e-20) / (t2 + 1e-20), 1 if negative)
+__global__ void k_mp_pdefq(KArgs A) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const Dims& g = A.g;
+  if (i >= A.gx || j >= A.gy || i >= g.nx || j >= g.ny) return;
+  const float* TE_R rho = A.p[1];
+  float* TE_R q = A.p[2];
+  const float rmax = A.f[3];
+  const int sk = g.sJ * g.sK, base = gidx(g, i, j, 0);
+  float t1 = 0.0f, t2 = 0.0f;
+  for (int k = 0; k < g.nz; k++) {
+    const int c = base + k * sk;
+    const float r = rho[c];
+    float v = q[c];
+    t1 = fmaf(r, v, t1);
+    if (v < rmax) {
+      v = 0.0f;
+      q[c] = 0.0f;
+    }
+    t2 = fmaf(r, v, t2);
+  }
+  float t3 = dcr(t1 + 1e-20f, t2 + 1e-20f);
+  if (t3 < 0.0f) t3 = 1.0f;
+  for (int k = 0; k < g.nz; k++) q[base + k * sk] = q[base + k * sk] * t3;
+}
+TE_LAUNCH_COLUMNS(mp_pdefq)
+
+// turb_scalar_vert_implicit.wgsl: subgrid tendency of a scalar s.  sten gains
+// ((fx, fy divergence) + turbz) rr at every level; turbz is the explicit vertical flux
+// divergence (explicitZ), or rho (s_new - s) / dt with s_new from a per-column Thomas
+// solve of the implicit vertical diffusion (cA, cB as the forward sweep; cB ends as s_new).
+struct TsviCol {
+  const Dims& g;
+  int i, j, base, sk, useFlux, bcturbs;
+  const float *TE_R s, *TE_R khv, *TE_R mf, *TE_R rf, *TE_R sflux, *TE_R fx, *TE_R fy, *TE_R hm, *TE_R rr;
+  float* TE_R sten;
+  const float* wall;
+  // vertical flux at w level kf (lam_1 / lam_2 of the reference kernel)
+  __device__ float vflux(int kf) const {
+    const int c = base + kf * sk;
+    if (kf == 0 || kf == g.nz) {
+      const int inner = kf == 0 ? 1 : g.nz - 1;
+      if (wall[3] == 0.0f) {
+        if (kf == 0 && useFlux != 0) return sflux[base] * rf[c];
+        if (bcturbs != 2) return 0.0f;
+        const int cc = base + inner * sk;
+        return ((((-khv[cc]) * (s[cc] - s[cc - sk])) * g.rdz) * mf[inner]) * rf[cc];
+      }
+      if (wall[3] == 2.0f) return (wall[0] * (kf == 0 ? wall[1] : wall[2])) * rf[c];
+      if (kf == 0) return (((((-wall[0]) * 2.0f) * (s[c] - wall[1])) * g.rdz) * mf[0]) * rf[c];
+      return (((((-wall[0]) * 2.0f) * (wall[2] - s[base + (g.nz - 1) * sk])) * g.rdz) * mf[g.nz]) * rf[c];
+    }
+    return ((((-khv[c]) * (s[c] - s[c - sk])) * g.rdz) * mf[kf]) * rf[c];
+  }
+  // sten += ((fx, fy divergence) + turbz) rr at point c (lam_5)
+  __device__ void tend(int c, float turbz) const {
+    const float h = ((-(fx[c + 1] - fx[c])) * g.rdx) * hm_uh(g, hm, i) + ((-(fy[c + g.sJ] - fy[c])) * g.rdy) * hm_vh(g, hm, j);
+    sten[c] = fmaf(h + turbz, rr[c], sten[c]);
+  }
+};
+
+__global__ void k_turb_scalar_vert_implicit(KArgs A) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const Dims& g = A.g;
+  if (i >= A.gx || j >= A.gy || i >= g.nx || j >= g.ny) return;
+  const float *TE_R s = A.p[1], *TE_R rho = A.p[2], *TE_R rr = A.p[3], *TE_R rf = A.p[4], *TE_R khv = A.p[5];
+  const float *TE_R mh = A.p[6], *TE_R mf = A.p[7];
+  float *TE_R cA = A.p[11], *TE_R cB = A.p[12];
+  const float dt = A.f[10];
+  const int sk = g.sJ * g.sK, base = gidx(g, i, j, 0);
+  const TsviCol col{g, i, j, base, sk, A.iv[15], A.iv[18], s, khv, mf, rf, A.p[14], A.p[8], A.p[9], A.p[30], rr, A.p[13], A.v4[0]};
+  if (A.iv[16] != 0) {
+    float below = col.vflux(0);
+    for (int k = 0; k < g.nz; k++) {
+      const float above = col.vflux(k + 1);
+      col.tend(base + k * sk, ((-(above - below)) * g.rdz) * mh[k]);
+      below = above;
+    }
+    return;
+  }
+  // lam_3 (coefficient of the face above level k) and lam_4 (the face below)
+  auto lam3 = [&](int k) {
+    const int c = base + k * sk;
+    return (((khv[c + sk] * mf[k + 1]) * rf[c + sk]) * mh[k]) * rr[c];
+  };
+  auto lam4 = [&](int k) {
+    const int c = base + k * sk;
+    return (((khv[c] * mf[k]) * rf[c]) * mh[k]) * rr[c];
+  };
+  const float tema = ((-dt) * g.rdz) * g.rdz, rdt = dcr(1.0f, dt), temc = dt * g.rdz;
+  const int useFlux = A.iv[15], bcturbs = A.iv[18];
+  {
+    const float cfc = tema * lam3(0), t = dcr(1.0f, 1.0f - cfc);
+    cA[base] = (-cfc) * t;
+    float cfd = s[base];
+    if (useFlux != 0 || bcturbs == 2) {
+      const int c1 = base + sk;
+      const float dumz = useFlux != 0 ? A.p[14][base] * rf[base] : ((((-khv[c1]) * (s[c1] - s[base])) * g.rdz) * mf[1]) * rf[c1];
+      cfd = fmaf((temc * dumz) * mh[0], rr[base], s[base]);
+    }
+    cB[base] = cfd * t;
+  }
+  for (int k = 1; k < g.nz - 1; k++) {
+    const int c = base + k * sk;
+    const float cfa = tema * lam4(k), cfc = tema * lam3(k), cfb = (1.0f - cfa) - cfc;
+    const float t = dcr(1.0f, fmaf(cfa, cA[c - sk], cfb));
+    cA[c] = (-cfc) * t;
+    cB[c] = fmaf(-cfa, cB[c - sk], s[c]) * t;
+  }
+  {
+    const int kt = g.nz - 1, ct = base + kt * sk;
+    const float cfa = tema * lam4(kt), t = dcr(1.0f, fmaf(cfa, cA[ct - sk], 1.0f - cfa));
+    float cfd = s[ct];
+    if (bcturbs == 2) {
+      const float dumz = ((((-khv[ct]) * (s[ct] - s[ct - sk])) * g.rdz) * mf[kt]) * rf[ct];
+      cfd = fmaf(-((temc * dumz) * mh[kt]), rr[ct], s[ct]);
+    }
+    const float snew = fmaf(-cfa, cB[ct - sk], cfd) * t;
+    cB[ct] = snew;
+    col.tend(ct, (rho[ct] * (snew - s[ct])) * rdt);
+  }
+  for (int k = g.nz - 2; k >= 0; k--) {
+    const int c = base + k * sk;
+    const float snew = fmaf(cA[c], cB[c + sk], cB[c]);
+    cB[c] = snew;
+    col.tend(c, (rho[c] * (snew - s[c])) * rdt);
+  }
+}
+TE_LAUNCH_COLUMNS(turb_scalar_vert_implicit)
+
+// rayleigh_damping.wgsl: -rdalpha tau (phi - phi_ref) for u, v, th (profiles, or level
+// averages when toAverage) and -rdalpha tauf w, tauf raised to the lateral sponge
+__global__ void k_rayleigh_damping(KArgs A) {
+  TE_K3
+  const int i = tx, j = ty, k = tz;
+  if (i > g.nx || j > g.ny || k > g.nz) return;
+  const float *TE_R u = A.p[1], *TE_R v = A.p[2], *TE_R w = A.p[3], *TE_R th = A.p[4];
+  float *TE_R uten = A.p[10], *TE_R vten = A.p[11], *TE_R wten = A.p[12], *TE_R thten = A.p[13];
+  const float rdalpha = A.f[9];
+  const int toAverage = A.iv[17];
+  const int c = gidx(g, i, j, k);
+  if (k < g.nz) {
+    const float t = A.p[7][k];
+    const float ur = toAverage != 0 ? A.p[18][k] : A.p[5][k];
+    const float vr = toAverage != 0 ? A.p[18][g.nz + k] : A.p[6][k];
+    if (j < g.ny) uten[c] = ((-rdalpha) * t) * (u[c] - ur);
+    if (i < g.nx) vten[c] = ((-rdalpha) * t) * (v[c] - vr);
+    if (i < g.nx && j < g.ny) {
+      const float d = toAverage != 0 ? (A.p[19][k] - A.p[18][2 * g.nz + k]) + th[c] : th[c];
+      thten[c] = ((-rdalpha) * t) * d;
+    }
+  }
+  if (i < g.nx && j < g.ny) {
+    float tf = A.p[8][k];
+    if (A.iv[16] != 0 && k < g.nz) tf = wmax(wmax(tf, A.p[14][i]), A.p[15][j]);
+    wten[c] = ((-rdalpha) * tf) * w[c];
+  }
+}
+TE_LAUNCH3(rayleigh_damping)
+
+// turb_rho_faces.wgsl: rr = 1 / rho (k < nz); rf on w levels, interior c1/c2 weights,
+// bottom and top extrapolated with cgs / cgt; columns -2..nx+1, rows -2..ny+1
+__global__ void k_turb_rho_faces(KArgs A) {
+  TE_K3
+  const int i = tx - 2, j = ty - 2, k = tz;
+  if (i > g.nx + 1 || j > g.ny + 1 || k > g.nz) return;
+  const float* TE_R rho = A.p[1];
+  float *TE_R rr = A.p[4], *TE_R rf = A.p[5];
+  const float *cgs = A.v4[0], *cgt = A.v4[1];
+  const int sk = g.sJ * g.sK, c = gidx(g, i, j, k);
+  if (k < g.nz) rr[c] = dcr(1.0f, rho[c]);
+  float r;
+  if (k == 0) {
+    r = fmaf(cgs[0], rho[c], cgs[1] * rho[c + sk]);
+    if (g.nz >= 3) r = fmaf(cgs[2], rho[c + 2 * sk], r);
+  } else if (k == g.nz) {
+    r = fmaf(cgt[0], rho[c - sk], cgt[1] * rho[c - 2 * sk]);
+    if (g.nz >= 3) r = fmaf(cgt[2], rho[c - 3 * sk], r);
+  } else {
+    r = fmaf(A.p[2][k], rho[c - sk], A.p[3][k] * rho[c]);
+  }
+  rf[c] = r;
+}
+TE_LAUNCH3(turb_rho_faces)
+
+// turb_def_centers.wgsl: rho-weighted strain rates s11, s22, s33 at cell centres and s12
+// at the (i-1/2, j-1/2) edges; columns -1..nx+1, rows -1..ny+1
+__global__ void k_turb_def_centers(KArgs A) {
+  TE_K3
+  const int i = tx - 1, j = ty - 1, k = tz;
+  if (i > g.nx + 1 || j > g.ny + 1 || k >= g.nz) return;
+  const float *TE_R u = A.p[1], *TE_R v = A.p[2], *TE_R w = A.p[3], *TE_R rho = A.p[4], *TE_R hm = A.p[30];
+  const int sj = g.sJ, sk = g.sJ * g.sK, c = gidx(g, i, j, k);
+  A.p[6][c] = ((rho[c] * (u[c + 1] - u[c])) * g.rdx) * hm_uh(g, hm, i);
+  A.p[7][c] = ((rho[c] * (v[c + sj] - v[c])) * g.rdy) * hm_vh(g, hm, j);
+  A.p[8][c] = ((rho[c] * (w[c + sk] - w[c])) * g.rdz) * A.p[5][k];
+  const float rcorner = 0.25f * ((rho[c - 1 - sj] + rho[c]) + (rho[c - 1] + rho[c - sj]));
+  A.p[9][c] = (0.5f * fmaf((u[c] - u[c - sj]) * g.rdy, hm_vf(g, hm, j), ((v[c] - v[c - 1]) * g.rdx) * hm_uf(g, hm, i))) * rcorner;
+}
+TE_LAUNCH3(turb_def_centers)
+
+// turb_def_faces.wgsl: s13, s23 on w levels 1..nz-1 at the x and y faces
+__global__ void k_turb_def_faces(KArgs A) {
+  TE_K3
+  const int i = tx, j = ty, k = tz + 1;
+  if (i > g.nx + 1 || j > g.ny + 1 || k > g.nz - 1) return;
+  const float *TE_R u = A.p[1], *TE_R v = A.p[2], *TE_R w = A.p[3], *TE_R rf = A.p[4], *TE_R hm = A.p[30];
+  const int sj = g.sJ, sk = g.sJ * g.sK, c = gidx(g, i, j, k);
+  const float mfk = 0.5f * (A.p[5][k] + A.p[5][k]);
+  A.p[6][c] = ((0.5f * fmaf((w[c] - w[c - 1]) * g.rdx, hm_uf(g, hm, i), ((u[c] - u[c - sk]) * g.rdz) * mfk)) * 0.5f) * (rf[c - 1] + rf[c]);
+  A.p[7][c] = ((0.5f * fmaf((w[c] - w[c - sj]) * g.rdy, hm_vf(g, hm, j), ((v[c] - v[c - sk]) * g.rdz) * mfk)) * 0.5f) * (rf[c - sj] + rf[c]);
+}
+TE_LAUNCH3(turb_def_faces)
+
+// turb_def_assemble.wgsl: defv = 4 (t13 + t23) / rf^2, defh = (2 (t11 + t22 + t33) + 4 t12)
+// / rf^2 on w levels 1..nz-1 (squared rates interpolated by c1/c2, edge/face averages)
+__global__ void k_turb_def_assemble(KArgs A) {
+  TE_K3
+  const int i = tx, j = ty, k = tz + 1;
+  if (i >= g.nx || j >= g.ny || k > g.nz - 1) return;
+  const float *TE_R s11 = A.p[1], *TE_R s22 = A.p[2], *TE_R s33 = A.p[3], *TE_R s12 = A.p[4], *TE_R s13 = A.p[5];
+  const float *TE_R s23 = A.p[6], *TE_R rf = A.p[9];
+  const int sj = g.sJ, sk = g.sJ * g.sK, c = gidx(g, i, j, k);
+  const float a = A.p[7][k], b = A.p[8][k];
+  auto sq2 = [&](const float* s) { return fmaf(a * s[c - sk], s[c - sk], (b * s[c]) * s[c]); };
+  auto pair = [&](int p, int q) { return fmaf(s12[p], s12[p], s12[q] * s12[q]); };
+  const float t11 = sq2(s11), t22 = sq2(s22), t33 = sq2(s33);
+  const float lo = pair(c - sk, c + 1 + sj - sk) + pair(c + sj - sk, c + 1 - sk);
+  const float hi = pair(c, c + 1 + sj) + pair(c + sj, c + 1);
+  const float t12 = 0.25f * fmaf(a, lo, b * hi);
+  const float t13 = 0.5f * fmaf(s13[c], s13[c], s13[c + 1] * s13[c + 1]);
+  const float t23 = 0.5f * fmaf(s23[c], s23[c], s23[c + sj] * s23[c + sj]);
+  const float rrf = dcr(1.0f, rf[c] * rf[c]);
+  A.p[10][c] = (4.0f * (t13 + t23)) * rrf;
+  A.p[11][c] = fmaf(2.0f, (t11 + t22) + t33, 4.0f * t12) * rrf;
+}
+TE_LAUNCH3(turb_def_assemble)
+
 // -------------------------------------------------- thermodynamic glue
 
 __global__ void k_update_diagnostics_moist(KArgs A) {
@@ -1495,6 +1746,13 @@ static const KernelSpec kTable[] = {
     {"tke_advance", 5, {R(0), P(1), P(2), R(3), W(4)}, false, launch_tke_advance},
     {"tke_sources", 6, {R(0), P(1), P(2), P(3), P(4), W(5)}, false, launch_tke_sources},
     {"tke_flux_h", 7, {R(0), P(1), P(2), P(3), W(4), W(5), P(30)}, false, launch_tke_flux_h},
+    {"mp_pdefq", 4, {R(0), P(1), W(2), R(3)}, false, launch_mp_pdefq},
+    {"turb_scalar_vert_implicit", 20, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), R(10), W(11), W(12), W(13), P(14), R(15), R(16), {17, kRef4, 0}, R(18), P(30)}, false, launch_turb_scalar_vert_implicit},
+    {"rayleigh_damping", 20, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), R(9), W(10), W(11), W(12), W(13), P(14), P(15), R(16), R(17), P(18), P(19)}, false, launch_rayleigh_damping},
+    {"turb_rho_faces", 8, {R(0), P(1), P(2), P(3), W(4), W(5), {6, kRef4, 0}, {7, kRef4, 0}}, false, launch_turb_rho_faces},
+    {"turb_def_centers", 11, {R(0), P(1), P(2), P(3), P(4), P(5), W(6), W(7), W(8), W(9), P(30)}, false, launch_turb_def_centers},
+    {"turb_def_faces", 9, {R(0), P(1), P(2), P(3), P(4), P(5), W(6), W(7), P(30)}, false, launch_turb_def_faces},
+    {"turb_def_assemble", 12, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), W(10), W(11)}, false, launch_turb_def_assemble},
     {"update_diagnostics_moist", 20, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), P(11), P(12),
                                       P(13), P(14), W(15), W(16), W(17), W(18), W(19)}, false, TE_ROWVEC(update_diagnostics_moist, OpUpdateDiagnosticsMoist)},
     {"pressure_tendency", 15, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), R(9), R(10), R(12), P(13), R(14), W(11)},

@@ -21,9 +21,10 @@ struct KArgs {
   float f[kMaxBind];
   int iv[kMaxBind];
   int iv2[kMaxBind];
+  float v4[2][4];  // the words of the kernel's first and second vec3/vec4 reference bindings (kRef4)
 };
 
-enum ParamKind : uint8_t { kPtr = 0, kRef = 1 };
+enum ParamKind : uint8_t { kPtr = 0, kRef = 1, kRef4 = 2 };
 
 struct ParamSpec {
   int8_t index;

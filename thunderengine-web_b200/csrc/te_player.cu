@@ -112,7 +112,7 @@ void Plan::load_kernel_meta(const char* kjson, size_t klen) {
     for (int i = 0; i < n; i++) {
       KMeta m;
       for (int q = 0; q < t[i].nparams; q++)
-        m.params.push_back({t[i].params[q].index, t[i].params[q].kind == kRef, t[i].params[q].write != 0});
+        m.params.push_back({t[i].params[q].index, t[i].params[q].kind != kPtr, t[i].params[q].write != 0});
       kmeta[t[i].name] = m;
     }
   }
@@ -317,6 +317,7 @@ void Plan::finalize_args(std::vector<Op>& ops) {
       A.a.kdiv = fl(ap + 3);
       A.a.smeps = fl(ap + 4);
     }
+    int nvec = 0;
     for (int q = 0; q < o.spec->nparams; q++) {
       const ParamSpec& ps = o.spec->params[q];
       auto it = o.bind.find(ps.index);
@@ -330,6 +331,12 @@ void Plan::finalize_args(std::vector<Op>& ops) {
         A.iv[ps.index] = (int)word(it->second);
         A.f[ps.index] = fl(it->second);
         A.iv2[ps.index] = (int)word(it->second + 1);
+        if (ps.kind == kRef4) {
+          if (nvec == 2) throw ApiError(TE_EINVAL, o.name + ": more than two vector parameter structs");
+          for (int w = 0; w < 4; w++)  // a vec3 may end the setBytes area: its fourth word reads 0
+            A.v4[nvec][w] = w < 3 || it->second + w < bytes_spare_end ? fl(it->second + w) : 0.0f;
+          nvec++;
+        }
       }
     }
     // turb_zero writes up to level nz + 1 of its binding (its own range check): the
@@ -681,7 +688,7 @@ size_t te_kernel_table_json(char* buf, size_t n) {
     for (int q = 0; q < t[i].nparams; q++) {
       if (q) s += ",";
       s += "{\"index\":" + std::to_string(t[i].params[q].index) + ",\"kind\":\"" +
-           (t[i].params[q].kind == te::kRef ? "ref" : "ptr") + "\",\"write\":" + (t[i].params[q].write ? "true" : "false") + "}";
+           (t[i].params[q].kind != te::kPtr ? "ref" : "ptr") + "\",\"write\":" + (t[i].params[q].write ? "true" : "false") + "}";
     }
     s += "]}";
   }
