@@ -1865,3 +1865,134 @@ void teor_turb_def_assemble(uint32_t *M, const uint32_t *ARG) {
     defh[c] = fmaf(2.0f, (t11 + t22) + t33, 4.0f * t12) * rrf;
   }
 }
+
+void teor_turb_gettau(uint32_t *M, const uint32_t *ARG) {
+  /* turb_gettau.wgsl main: stresses from the strain rates, t = s (kmh + kmh above) at
+   * centres, t12 with the 8-point edge average of kmh, t13 / t23 with the face sums of kmv
+   * (levels 1..nz-1, columns and rows >= 0); columns and rows -1..n */
+  Dims g = dims_at(M, B(0));
+  const float *kmh = FPTR(1), *kmv = FPTR(2);
+  float *t11 = FPTR(3), *t22 = FPTR(4), *t33 = FPTR(5), *t12 = FPTR(6), *t13 = FPTR(7), *t23 = FPTR(8);
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  FOR_GRID {
+    int i = (int)tx - 1, j = (int)ty - 1, k = (int)tz;
+    if (i > g.nx || j > g.ny || k >= g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    float tem = kmh[c] + kmh[c + sk];
+    t11[c] = t11[c] * tem;
+    t22[c] = t22[c] * tem;
+    t33[c] = t33[c] * tem;
+    int d = c + sk;
+    t12[c] = t12[c] * (0.25f * (((kmh[c - 1 - sj] + kmh[c]) + (kmh[c - 1] + kmh[c - sj])) +
+                                ((kmh[d - 1 - sj] + kmh[d]) + (kmh[d - 1] + kmh[d - sj]))));
+    if (k >= 1 && k <= g.nz - 1 && i >= 0 && j >= 0) {
+      t13[c] = t13[c] * (kmv[c - 1] + kmv[c]);
+      t23[c] = t23[c] * (kmv[c - sj] + kmv[c]);
+    }
+  }
+}
+
+/* x^y for the reference's WGSL pow builtin (turb_km_kh.wgsl), whose precision WGSL leaves
+ * to the implementation.  Evaluated as 2^(y log2 x) in binary64 with plain operations and
+ * rounded once to binary32: log2 x = e + ln(m) / ln 2 with m in [sqrt(1/2), sqrt(2)) and
+ * ln m = 2 atanh(s), s = (m - 1) / (m + 1), by its odd power series to s^23; 2^t = 2^n e^r,
+ * n = rint(t), r = (t - n) ln 2, by the Taylor series of e^r to r^14.  The binary64 error is
+ * far below half a binary32 ulp, so the result is the correctly rounded power except within
+ * that error of a rounding boundary.  The CUDA kernels evaluate the same operations. */
+float te_pow_f64(float x, float y) {
+  if (!(x > 0.0f) || x == INFINITY) return x == 0.0f ? (y > 0.0f ? 0.0f : INFINITY) : (x == INFINITY ? (y > 0.0f ? INFINITY : 0.0f) : NAN);
+  uint32_t b = fbits(x);
+  int e = (int)(b >> 23) - 127;
+  double m = (double)bitsf((b & 0x7fffffu) | 0x3f800000u);
+  if (m > 1.4142135623730951) {
+    m = m * 0.5;
+    e = e + 1;
+  }
+  double s = (m - 1.0) / (m + 1.0), s2 = s * s, p = 1.0 / 23;
+  for (int k = 21; k >= 1; k -= 2) p = p * s2 + 1.0 / k;
+  double t = (double)y * ((double)e + (2.0 * s * p) * 1.4426950408889634);
+  if (t > 128.0) return INFINITY;
+  if (t < -126.0) return 0.0f;
+  double n = nearbyint(t), r = (t - n) * 0.6931471805599453, q = 1.0;
+  for (int k = 14; k >= 1; k--) q = 1.0 + (r * (1.0 / k)) * q;
+  return (float)ldexp(q, (int)n);
+}
+
+void teor_turb_km_kh(uint32_t *M, const uint32_t *ARG) {
+  /* turb_km_kh.wgsl main: TKE closure on w levels 1..nz-1.  Grid scale (dx dy dz)^(1/3),
+   * mixing length (stability-limited by c_l sqrt(tke / N^2)), dissipation added to dissten,
+   * km = cmz sqrt(tke) len kmScale (or kmFixed), kh = km / Pr with 1/Pr = min(1 + 2 len /
+   * grid scale, 3) */
+  Dims g = dims_at(M, B(0));
+  const float *tkea = FPTR(1), *nm = FPTR(2), *mf = FPTR(3), *hm = FPTR(30);
+  float *kmh = FPTR(4), *kmv = FPTR(5), *khh = FPTR(6), *khv = FPTR(7), *lenscl = FPTR(8), *dissten = FPTR(9);
+  const float kmScale = FVAL(10), kmFixed = FVAL(11), turbfac = FVAL(12);
+  const float c_m = 0.1f, c_l = 0.8165f, ri_c = 0.25f, tke_min = 1e-10f, nm_min = 1e-06f, small_len_frac = 0.001f;
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz + 1;
+    if (i >= g.nx || j >= g.ny || k > g.nz - 1) continue;
+    int c = GIDX(g, i, j, k);
+    float cmz = fmax_(0.001f, turbfac * c_m);
+    float ce1z = ((cmz * c_l) * c_l) * (DCR(1.0f, ri_c) - 1.0f);
+    float ce2z = fmax_(0.0f, fmaf(cmz * 3.1415927f, 3.1415927f, -ce1z));
+    float dzk = DCR(DCR(1.0f, g.rdz), mf[k]);
+    float grdscl = te_pow_f64((DCR(DCR(1.0f, g.rdx), hm_uh(&g, hm, i)) * DCR(DCR(1.0f, g.rdy), hm_vh(&g, hm, j))) * dzk, 0.33333334f);
+    float rgrdscl = DCR(1.0f, grdscl);
+    float tk, len;
+    if (tkea[c] <= tke_min) {
+      tk = tke_min;
+      len = small_len_frac * grdscl;
+    } else {
+      tk = tkea[c];
+      len = grdscl;
+      if (nm[c] > nm_min) {
+        len = c_l * sqrtf(DCR(tk, nm[c]));
+        len = fmin_(len, grdscl);
+        len = fmax_(len, small_len_frac * grdscl);
+      }
+    }
+    lenscl[c] = len;
+    dissten[c] = dissten[c] + DCR((fmaf(ce2z * len, rgrdscl, ce1z) * tk) * sqrtf(tk), len);
+    float km = kmFixed > 0.0f ? kmFixed : ((cmz * sqrtf(tk)) * len) * kmScale;
+    kmh[c] = km;
+    kmv[c] = km;
+    float prinv = 3.0f;
+    if (nm[c] > nm_min) prinv = fmin_(fmaf(2.0f * len, rgrdscl, 1.0f), 3.0f);
+    khh[c] = km * prinv;
+    khv[c] = khh[c];
+  }
+}
+
+void teor_tke_epst(uint32_t *M, const uint32_t *ARG) {
+  /* tke_epst.wgsl main: shear production of TKE on w levels 1..nz-1, the stresses t_ij
+   * times the strain rates, interpolated (c1/c2) or averaged to the w point, divided by rf */
+  Dims g = dims_at(M, B(0));
+  const float *u = FPTR(1), *v = FPTR(2), *w = FPTR(3), *t11 = FPTR(4), *t12 = FPTR(5), *t13 = FPTR(6);
+  const float *t22 = FPTR(7), *t23 = FPTR(8), *t33 = FPTR(9), *rf = FPTR(10), *mh = FPTR(11), *mf = FPTR(12);
+  const float *c1 = FPTR(13), *c2 = FPTR(14), *hm = FPTR(30);
+  float *epst = FPTR(15);
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz + 1;
+    if (i >= g.nx || j >= g.ny || k > g.nz - 1) continue;
+    int c = GIDX(g, i, j, k), cd = c - sk;
+    const float uh = hm_uh(&g, hm, i), vh = hm_vh(&g, hm, j), mfk = mf[k];
+#define L1(cc) fmaf(((u[(cc) + 1] - u[cc]) * g.rdx) * uh, t11[cc], (((v[(cc) + sj] - v[cc]) * g.rdy) * vh) * t22[cc])
+#define L2(cc, ii, jj) (t12[cc] * fmaf((u[cc] - u[(cc) - sj]) * g.rdy, hm_vf(&g, hm, jj), ((v[cc] - v[(cc) - 1]) * g.rdx) * hm_uf(&g, hm, ii)))
+#define L3(cc, ii) (fmaf((w[cc] - w[(cc) - 1]) * g.rdx, hm_uf(&g, hm, ii), ((u[cc] - u[(cc) - sk]) * g.rdz) * mfk) * t13[cc])
+#define L4(cc, jj) (fmaf((w[cc] - w[(cc) - sj]) * g.rdy, hm_vf(&g, hm, jj), ((v[cc] - v[(cc) - sk]) * g.rdz) * mfk) * t23[cc])
+#define L5(cc, kk) ((((w[(cc) + sk] - w[cc]) * g.rdz) * mh[kk]) * t33[cc])
+    float e = fmaf(c1[k], L1(cd), c2[k] * L1(c));
+    float hi = (L2(c, i, j) + L2(c + 1 + sj, i + 1, j + 1)) + (L2(c + sj, i, j + 1) + L2(c + 1, i + 1, j));
+    float lo = (L2(cd, i, j) + L2(cd + 1 + sj, i + 1, j + 1)) + (L2(cd + sj, i, j + 1) + L2(cd + 1, i + 1, j));
+    e = fmaf(0.25f, fmaf(c2[k], hi, c1[k] * lo), e);
+    e = fmaf(0.5f, (L3(c, i) + L3(c + 1, i + 1)) + (L4(c, j) + L4(c + sj, j + 1)), e);
+    e = e + fmaf(c1[k], L5(cd, k - 1), c2[k] * L5(c, k));
+#undef L1
+#undef L2
+#undef L3
+#undef L4
+#undef L5
+    epst[c] = DCR(e, rf[c]);
+  }
+}

@@ -27,6 +27,8 @@ float te_weno5(float s1, float s2, float s3, float s4, float s5, float weps);
 float te_rr_pow_cr(float x, float p);
 
 #define TE_ORACLE_KERNEL(name) void teor_##name(uint32_t *M, const uint32_t *ARG);
+float te_pow_f64(float x, float y);
+
 #define TE_ORACLE_KERNELS(X) \
   X(adv_flux_x) X(adv_flux_y) X(adv_flux_z) \
   X(adv_flux_x_stag) X(adv_flux_y_stag) X(adv_flux_z_stag) \
@@ -45,7 +47,8 @@ float te_rr_pow_cr(float x, float p);
   X(turb_zero) X(turb_add_tendency) X(turb_scalar_flux_h) X(turb_openbc_flux) \
   X(turb_openbc_stress_x) X(turb_openbc_stress_y) X(tke_advance) X(tke_sources) X(tke_flux_h) \
   X(mp_pdefq) X(turb_scalar_vert_implicit) \
-  X(rayleigh_damping) X(turb_rho_faces) X(turb_def_centers) X(turb_def_faces) X(turb_def_assemble)
+  X(rayleigh_damping) X(turb_rho_faces) X(turb_def_centers) X(turb_def_faces) X(turb_def_assemble) \
+  X(turb_gettau) X(turb_km_kh) X(tke_epst)
 TE_ORACLE_KERNELS(TE_ORACLE_KERNEL)
 
 #ifdef __cplusplus

@@ -156,7 +156,7 @@ def test_golden_single_cell_in_scope_dispatches():
                 dirty.append((o.dst, o.n))
             else:
                 dirty.extend((off, ln) for _, off, ln in o.hashes if off is not None and ln)
-    assert ngpu >= 699   # 701 of the 718: dynamics, open boundaries, Rayleigh damping, most of the turbulence, pdefq
+    assert ngpu >= 702   # 704 of the 718: dynamics, open boundaries, Rayleigh damping, most of the turbulence, pdefq
     fields = {v // 4 + cpu.base[2]: k for k, v in tape['fields'].items()}
     slot_field = {s: fields.get(off) for o in cpu.ops if o.kind == 'k' for s, off, _ in o.hashes}
     bad = [s for s in gpu_hashes if gpu_hashes[s] != int(want[s])]
@@ -179,6 +179,7 @@ UNTAKEN_BRANCHES = {
                                (0, 1, 1, 1.0), (0, 1, 1, 2.0), (0, 0, 2, 1.0)]],
     'rayleigh_damping': [{16: [1], 17: [0]}, {16: [0], 17: [1]}, {16: [1], 17: [1]}],
     'mp_pdefq': [{3: [_f32(1e-5)]}, {3: [_f32(-1.0)]}],
+    'turb_km_kh': [{11: [_f32(5.0)]}, {12: [_f32(0.001)]}],
 }
 
 

@@ -46,6 +46,30 @@ def test_rr_pow_is_correctly_rounded(oracle_lib):
     assert bad <= 3
 
 
+
+def test_wgsl_pow_is_correctly_rounded(oracle_lib):
+    """te_pow_f64 (the WGSL pow builtin of turb_km_kh.wgsl) against x^y to 50 digits:
+    correctly rounded on every sample, and exact on exact cubes."""
+    from decimal import Decimal, getcontext
+    getcontext().prec = 50
+    p = oracle_lib.lib.te_pow_f64
+    p.restype = ctypes.c_float
+    p.argtypes = [ctypes.c_float, ctypes.c_float]
+
+    def nearest(x, y):
+        v = (Decimal(float(y)) * Decimal(float(x)).ln()).exp()
+        f = np.float32(float(v))
+        cands = [np.nextafter(f, np.float32(-np.inf)), f, np.nextafter(f, np.float32(np.inf))]
+        return min(cands, key=lambda c: abs(Decimal(float(c)) - v))
+
+    rng = np.random.default_rng(3)
+    xs = (10.0 ** rng.uniform(-12, 12, 1500)).astype(np.float32)
+    for y in (np.float32(0.33333334), np.float32(2.5), np.float32(-0.7)):
+        for x in xs:
+            assert p(float(x), float(y)) == nearest(x, y), (x, y)
+    assert p(8.0, 0.33333334) == 2.0 and p(1.0, 0.33333334) == 1.0 and p(0.0, 0.33333334) == 0.0
+    assert math.isnan(p(-1.0, 0.33333334))
+
 def test_oracle_equals_reference_kernels_on_synthetic_step(oracle_lib, ref_lib, kernels_meta):
     """Hand-written oracle vs the reference's own kernels: every word after 2 steps."""
     run = timestep.Run(scenario.tiny(16, 12, 10))
@@ -89,8 +113,8 @@ def test_column_kernels_on_branches_the_recording_does_not_take(oracle_lib, ref_
     state of the recorded step at their first dispatch, with the flags of the branches the
     recording does not take: explicit vertical fluxes, surface flux, bcturbs = 2 and the
     three wall settings (turb_scalar_vert_implicit.wgsl lam_1), a clip threshold that
-    zeroes part of every column (mp_pdefq.wgsl), and the lateral sponge and level-average
-    references of rayleigh_damping.wgsl."""
+    zeroes part of every column (mp_pdefq.wgsl), the lateral sponge and level-average
+    references of rayleigh_damping.wgsl, and a fixed km and the cmz floor of turb_km_kh.wgsl."""
     import itertools
     from oracle.player import CpuPlayer
     tape, init, want, step1 = helpers.load_golden_scenario()
@@ -106,12 +130,14 @@ def test_column_kernels_on_branches_the_recording_does_not_take(oracle_lib, ref_
         if o.kind == 'copy':
             p.M[o.dst:o.dst + o.n] = p.M[o.src:o.src + o.n]
             continue
-        if o.name in ('turb_scalar_vert_implicit', 'mp_pdefq', 'rayleigh_damping') and o.name not in done:
+        if o.name in ('turb_scalar_vert_implicit', 'mp_pdefq', 'rayleigh_damping', 'turb_km_kh') and o.name not in done:
             done.add(o.name)
             B = lambda n: int(o.arg[4 + n])
             sk = 127 * 127   # one level of the 120 x 120 recording (halo 3 on each side)
             if o.name == 'rayleigh_damping':
                 variants = [{B(16): a, B(17): b} for a in (0, 1) for b in (0, 1)]
+            elif o.name == 'turb_km_kh':
+                variants = [{B(11): fb(5.0)}, {B(12): fb(0.001)}]
             elif o.name == 'mp_pdefq':
                 q = p.M[B(2):B(2) + 8 * sk].view(np.float32)
                 nz_q = np.abs(q[q != 0])
@@ -134,6 +160,6 @@ def test_column_kernels_on_branches_the_recording_does_not_take(oracle_lib, ref_
                 assert np.array_equal(E, F), (o.name, v)
                 compared += 1
         helpers.mixed(o.name)(vp(p.M), vp(o.arg))
-        if len(done) == 3:
+        if len(done) == 4:
             break
-    assert compared == 30
+    assert compared == 32

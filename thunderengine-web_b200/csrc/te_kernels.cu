@@ -1196,6 +1196,109 @@ __global__ void k_turb_def_assemble(KArgs A) {
 }
 TE_LAUNCH3(turb_def_assemble)
 
+// turb_gettau.wgsl: stresses t = s (kmh + kmh above) at centres, t12 by the 8-point edge
+// average of kmh, t13 / t23 by the face sums of kmv (levels 1..nz-1, i, j >= 0); the
+// dispatch covers columns and rows -1..n
+__global__ void k_turb_gettau(KArgs A) {
+  TE_K3
+  const int i = tx - 1, j = ty - 1, k = tz;
+  if (i > g.nx || j > g.ny || k >= g.nz) return;
+  const float *TE_R kmh = A.p[1], *TE_R kmv = A.p[2];
+  float *TE_R t11 = A.p[3], *TE_R t22 = A.p[4], *TE_R t33 = A.p[5], *TE_R t12 = A.p[6];
+  const int sj = g.sJ, sk = g.sJ * g.sK, c = gidx(g, i, j, k), d = c + sk;
+  const float tem = kmh[c] + kmh[d];
+  t11[c] = t11[c] * tem;
+  t22[c] = t22[c] * tem;
+  t33[c] = t33[c] * tem;
+  t12[c] = t12[c] * (0.25f * (((kmh[c - 1 - sj] + kmh[c]) + (kmh[c - 1] + kmh[c - sj])) +
+                              ((kmh[d - 1 - sj] + kmh[d]) + (kmh[d - 1] + kmh[d - sj]))));
+  if (k >= 1 && k <= g.nz - 1 && i >= 0 && j >= 0) {
+    float *TE_R t13 = A.p[7], *TE_R t23 = A.p[8];
+    t13[c] = t13[c] * (kmv[c - 1] + kmv[c]);
+    t23[c] = t23[c] * (kmv[c - sj] + kmv[c]);
+  }
+}
+TE_LAUNCH3(turb_gettau)
+
+// turb_km_kh.wgsl: TKE closure on w levels 1..nz-1: grid scale (dx dy dz)^(1/3), mixing
+// length (limited by c_l sqrt(tke / N^2) in stable air), dissipation added to dissten,
+// km = cmz sqrt(tke) len kmScale (or kmFixed > 0), kh = km min(1 + 2 len / scale, 3)
+__global__ void k_turb_km_kh(KArgs A) {
+  TE_K3
+  const int i = tx, j = ty, k = tz + 1;
+  if (i >= g.nx || j >= g.ny || k > g.nz - 1) return;
+  const float *TE_R tkea = A.p[1], *TE_R nm = A.p[2], *TE_R hm = A.p[30];
+  float *TE_R kmh = A.p[4], *TE_R kmv = A.p[5], *TE_R khh = A.p[6], *TE_R khv = A.p[7];
+  float *TE_R lenscl = A.p[8], *TE_R dissten = A.p[9];
+  const float kmScale = A.f[10], kmFixed = A.f[11], turbfac = A.f[12];
+  const float c_m = 0.1f, c_l = 0.8165f, ri_c = 0.25f, tke_min = 1e-10f, nm_min = 1e-06f, small_len_frac = 0.001f;
+  const int c = gidx(g, i, j, k);
+  const float cmz = wmax(0.001f, turbfac * c_m);
+  const float ce1z = ((cmz * c_l) * c_l) * (dcr(1.0f, ri_c) - 1.0f);
+  const float ce2z = wmax(0.0f, fmaf(cmz * 3.1415927f, 3.1415927f, -ce1z));
+  const float dzk = dcr(dcr(1.0f, g.rdz), A.p[3][k]);
+  const float grdscl = pow_f64((dcr(dcr(1.0f, g.rdx), hm_uh(g, hm, i)) * dcr(dcr(1.0f, g.rdy), hm_vh(g, hm, j))) * dzk, 0.33333334f);
+  const float rgrdscl = dcr(1.0f, grdscl);
+  const float tka = tkea[c], nmc = nm[c];
+  float tk, len;
+  if (tka <= tke_min) {
+    tk = tke_min;
+    len = small_len_frac * grdscl;
+  } else {
+    tk = tka;
+    len = grdscl;
+    if (nmc > nm_min) {
+      len = c_l * sqrtf(dcr(tk, nmc));
+      len = wmin(len, grdscl);
+      len = wmax(len, small_len_frac * grdscl);
+    }
+  }
+  lenscl[c] = len;
+  dissten[c] = dissten[c] + dcr((fmaf(ce2z * len, rgrdscl, ce1z) * tk) * sqrtf(tk), len);
+  const float km = kmFixed > 0.0f ? kmFixed : ((cmz * sqrtf(tk)) * len) * kmScale;
+  kmh[c] = km;
+  kmv[c] = km;
+  float prinv = 3.0f;
+  if (nm[c] > nm_min) prinv = wmin(fmaf(2.0f * len, rgrdscl, 1.0f), 3.0f);
+  khh[c] = km * prinv;
+  khv[c] = khh[c];
+}
+TE_LAUNCH3(turb_km_kh)
+
+// tke_epst.wgsl: shear production on w levels 1..nz-1, stresses times strain rates
+// interpolated (c1/c2) or averaged to the w point, divided by rf
+__global__ void k_tke_epst(KArgs A) {
+  TE_K3
+  const int i = tx, j = ty, k = tz + 1;
+  if (i >= g.nx || j >= g.ny || k > g.nz - 1) return;
+  const float *TE_R u = A.p[1], *TE_R v = A.p[2], *TE_R w = A.p[3], *TE_R t11 = A.p[4], *TE_R t12 = A.p[5];
+  const float *TE_R t13 = A.p[6], *TE_R t22 = A.p[7], *TE_R t23 = A.p[8], *TE_R t33 = A.p[9], *TE_R rf = A.p[10];
+  const float *TE_R mh = A.p[11], *TE_R hm = A.p[30];
+  const int sj = g.sJ, sk = g.sJ * g.sK, c = gidx(g, i, j, k), cd = c - sk;
+  const float uh = hm_uh(g, hm, i), vh = hm_vh(g, hm, j), mfk = A.p[12][k], c1 = A.p[13][k], c2 = A.p[14][k];
+  auto l1 = [&](int cc) {
+    return fmaf(((u[cc + 1] - u[cc]) * g.rdx) * uh, t11[cc], (((v[cc + sj] - v[cc]) * g.rdy) * vh) * t22[cc]);
+  };
+  auto l2 = [&](int cc, int ii, int jj) {
+    return t12[cc] * fmaf((u[cc] - u[cc - sj]) * g.rdy, hm_vf(g, hm, jj), ((v[cc] - v[cc - 1]) * g.rdx) * hm_uf(g, hm, ii));
+  };
+  auto l3 = [&](int cc, int ii) {
+    return fmaf((w[cc] - w[cc - 1]) * g.rdx, hm_uf(g, hm, ii), ((u[cc] - u[cc - sk]) * g.rdz) * mfk) * t13[cc];
+  };
+  auto l4 = [&](int cc, int jj) {
+    return fmaf((w[cc] - w[cc - sj]) * g.rdy, hm_vf(g, hm, jj), ((v[cc] - v[cc - sk]) * g.rdz) * mfk) * t23[cc];
+  };
+  auto l5 = [&](int cc, int kk) { return (((w[cc + sk] - w[cc]) * g.rdz) * mh[kk]) * t33[cc]; };
+  float e = fmaf(c1, l1(cd), c2 * l1(c));
+  const float hi = (l2(c, i, j) + l2(c + 1 + sj, i + 1, j + 1)) + (l2(c + sj, i, j + 1) + l2(c + 1, i + 1, j));
+  const float lo = (l2(cd, i, j) + l2(cd + 1 + sj, i + 1, j + 1)) + (l2(cd + sj, i, j + 1) + l2(cd + 1, i + 1, j));
+  e = fmaf(0.25f, fmaf(c2, hi, c1 * lo), e);
+  e = fmaf(0.5f, (l3(c, i) + l3(c + 1, i + 1)) + (l4(c, j) + l4(c + sj, j + 1)), e);
+  e = e + fmaf(c1, l5(cd, k - 1), c2 * l5(c, k));
+  A.p[15][c] = dcr(e, rf[c]);
+}
+TE_LAUNCH3(tke_epst)
+
 // -------------------------------------------------- thermodynamic glue
 
 __global__ void k_update_diagnostics_moist(KArgs A) {
@@ -1753,6 +1856,9 @@ static const KernelSpec kTable[] = {
     {"turb_def_centers", 11, {R(0), P(1), P(2), P(3), P(4), P(5), W(6), W(7), W(8), W(9), P(30)}, false, launch_turb_def_centers},
     {"turb_def_faces", 9, {R(0), P(1), P(2), P(3), P(4), P(5), W(6), W(7), P(30)}, false, launch_turb_def_faces},
     {"turb_def_assemble", 12, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), W(10), W(11)}, false, launch_turb_def_assemble},
+    {"turb_gettau", 10, {R(0), P(1), P(2), W(3), W(4), W(5), W(6), W(7), W(8), P(30)}, false, launch_turb_gettau},
+    {"turb_km_kh", 14, {R(0), P(1), P(2), P(3), W(4), W(5), W(6), W(7), W(8), W(9), R(10), R(11), R(12), P(30)}, false, launch_turb_km_kh},
+    {"tke_epst", 17, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), P(11), P(12), P(13), P(14), W(15), P(30)}, false, launch_tke_epst},
     {"update_diagnostics_moist", 20, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), P(11), P(12),
                                       P(13), P(14), W(15), W(16), W(17), W(18), W(19)}, false, TE_ROWVEC(update_diagnostics_moist, OpUpdateDiagnosticsMoist)},
     {"pressure_tendency", 15, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), R(9), R(10), R(12), P(13), R(14), W(11)},

@@ -34,6 +34,37 @@ __device__ __forceinline__ float dcr(float a, float b) { return a / b; }
 __device__ __forceinline__ float wmin(float a, float b) { return (b < a || a != a) ? b : a; }
 __device__ __forceinline__ float wmax(float a, float b) { return (a < b || a != a) ? b : a; }
 
+// x^y for the reference's WGSL pow builtin, whose precision WGSL leaves to the
+// implementation: 2^(y log2 x) in binary64 with plain operations, rounded once to binary32.
+// log2 x = e + ln(m) / ln 2 with m in [sqrt(1/2), sqrt(2)) and ln m = 2 atanh(s),
+// s = (m - 1) / (m + 1), by its odd power series to s^23; 2^t = 2^n e^r, n = rint(t),
+// r = (t - n) ln 2, by the Taylor series of e^r to r^14.  The binary64 error is far below
+// half a binary32 ulp: the correctly rounded power except within that error of a rounding
+// boundary.  The same operations in the same order on every device (no contraction).
+__device__ __forceinline__ float pow_f64(float x, float y) {
+  if (!(x > 0.0f) || x == INFINITY)
+    return x == 0.0f ? (y > 0.0f ? 0.0f : INFINITY) : (x == INFINITY ? (y > 0.0f ? INFINITY : 0.0f) : NAN);
+  const uint32_t b = __float_as_uint(x);
+  int e = (int)(b >> 23) - 127;
+  double m = (double)__uint_as_float((b & 0x7fffffu) | 0x3f800000u);
+  if (m > 1.4142135623730951) {
+    m = m * 0.5;
+    e = e + 1;
+  }
+  const double s = (m - 1.0) / (m + 1.0), s2 = s * s;
+  double p = 1.0 / 23;
+#pragma unroll
+  for (int k = 21; k >= 1; k -= 2) p = p * s2 + 1.0 / k;
+  const double t = (double)y * ((double)e + (2.0 * s * p) * 1.4426950408889634);
+  if (t > 128.0) return INFINITY;
+  if (t < -126.0) return 0.0f;
+  const double n = rint(t), r = (t - n) * 0.6931471805599453;
+  double q = 1.0;
+#pragma unroll
+  for (int k = 14; k >= 1; k--) q = 1.0 + (r * (1.0 / k)) * q;
+  return (float)ldexp(q, (int)n);
+}
+
 // Quotients of constants, rounded once (the reference writes e.g. div_cr(13.0, 12.0)).
 #define TE_C1312 (13.0f / 12.0f)
 #define TE_C2_60 (2.0f / 60.0f)
