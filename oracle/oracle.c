@@ -1892,30 +1892,52 @@ void teor_turb_gettau(uint32_t *M, const uint32_t *ARG) {
   }
 }
 
-/* x^y for the reference's WGSL pow builtin (turb_km_kh.wgsl), whose precision WGSL leaves
- * to the implementation.  Evaluated as 2^(y log2 x) in binary64 with plain operations and
- * rounded once to binary32: log2 x = e + ln(m) / ln 2 with m in [sqrt(1/2), sqrt(2)) and
- * ln m = 2 atanh(s), s = (m - 1) / (m + 1), by its odd power series to s^23; 2^t = 2^n e^r,
- * n = rint(t), r = (t - n) ln 2, by the Taylor series of e^r to r^14.  The binary64 error is
- * far below half a binary32 ulp, so the result is the correctly rounded power except within
- * that error of a rounding boundary.  The CUDA kernels evaluate the same operations. */
-float te_pow_f64(float x, float y) {
-  if (!(x > 0.0f) || x == INFINITY) return x == 0.0f ? (y > 0.0f ? 0.0f : INFINITY) : (x == INFINITY ? (y > 0.0f ? INFINITY : 0.0f) : NAN);
+/* The reference's WGSL pow, exp and log builtins (turb_km_kh.wgsl, turb_nm.wgsl,
+ * turb_dissipative_heating.wgsl), whose precision WGSL leaves to the implementation, are
+ * evaluated in binary64 with plain operations and rounded once to binary32:
+ *   ln x = e ln 2 + 2 atanh(s) for x = 2^e m, m in [sqrt(1/2), sqrt(2)), s = (m - 1) / (m + 1),
+ *          atanh by its odd power series to s^23;
+ *   2^t  = 2^n e^r, n = rint(t), r = (t - n) ln 2, e^r by its Taylor series to r^14;
+ *   x^y = 2^(y log2 x), e^x = 2^(x / ln 2).
+ * The binary64 error is far below half a binary32 ulp, so each is the correctly rounded
+ * value except within that error of a rounding boundary.  The CUDA kernels evaluate the
+ * same operations in the same order. */
+static double ln_mantissa(float x, int *e) {   /* x > 0 normal: returns ln(m), sets e */
   uint32_t b = fbits(x);
-  int e = (int)(b >> 23) - 127;
   double m = (double)bitsf((b & 0x7fffffu) | 0x3f800000u);
+  *e = (int)(b >> 23) - 127;
   if (m > 1.4142135623730951) {
     m = m * 0.5;
-    e = e + 1;
+    *e = *e + 1;
   }
   double s = (m - 1.0) / (m + 1.0), s2 = s * s, p = 1.0 / 23;
   for (int k = 21; k >= 1; k -= 2) p = p * s2 + 1.0 / k;
-  double t = (double)y * ((double)e + (2.0 * s * p) * 1.4426950408889634);
+  return 2.0 * s * p;
+}
+static float exp2_rounded(double t) {
   if (t > 128.0) return INFINITY;
   if (t < -126.0) return 0.0f;
   double n = nearbyint(t), r = (t - n) * 0.6931471805599453, q = 1.0;
   for (int k = 14; k >= 1; k--) q = 1.0 + (r * (1.0 / k)) * q;
   return (float)ldexp(q, (int)n);
+}
+float te_pow_f64(float x, float y) {
+  if (!(x > 0.0f) || x == INFINITY) return x == 0.0f ? (y > 0.0f ? 0.0f : INFINITY) : (x == INFINITY ? (y > 0.0f ? INFINITY : 0.0f) : NAN);
+  int e;
+  double lm = ln_mantissa(x, &e);
+  return exp2_rounded((double)y * ((double)e + lm * 1.4426950408889634));
+}
+float te_exp_f64(float x) {
+  if (x != x) return x;
+  return exp2_rounded((double)x * 1.4426950408889634);
+}
+float te_log_f64(float x) {
+  if (x != x || x < 0.0f) return NAN;
+  if (x == 0.0f) return -INFINITY;
+  if (x == INFINITY) return INFINITY;
+  int e;
+  double lm = ln_mantissa(x, &e);
+  return (float)((double)e * 0.6931471805599453 + lm);
 }
 
 void teor_turb_km_kh(uint32_t *M, const uint32_t *ARG) {
@@ -1994,5 +2016,211 @@ void teor_tke_epst(uint32_t *M, const uint32_t *ARG) {
 #undef L4
 #undef L5
     epst[c] = DCR(e, rf[c]);
+  }
+}
+
+/* turb_nm.wgsl f_rr_log_cr: the reference's correctly rounded log (two-float log, summed);
+ * non-positive, infinite and NaN arguments take the log builtin's special values */
+static float rr_log_cr(float x) {
+  if (!(x > 0.0f) || x == INFINITY) return x == 0.0f ? -INFINITY : (x == INFINITY ? INFINITY : NAN);
+  F2 a = rr_log_ff(x);
+  return a.x + a.y;
+}
+
+/* saturation mixing ratios over liquid (f_mp_rslf) and ice (f_mp_rsif), turb_nm.wgsl */
+static float mp_rs(float p, float t, float a, float b) {
+  float es = 611.2f * te_exp_f64(DCR(a * (t - 273.15f), t - b));
+  es = fmin_(es, p * 0.5f);
+  return DCR(DCR(287.04f, 461.5f) * es, p - es);
+}
+
+void teor_turb_nm(uint32_t *M, const uint32_t *ARG) {
+  /* turb_nm.wgsl main: squared Brunt-Vaisala frequency on w levels 1..nz-1.  Dry: g dln(th)/dz.
+   * Moist: g dln(thv)/dz, or in saturated air (liquid above 0 C, ice below -40 C, a linear
+   * blend between) the moist-adiabatic form of lam_1; sat marks saturated points */
+  Dims g = dims_at(M, B(0));
+  const float *thPert = FPTR(1), *ppPert = FPTR(2), *th0 = FPTR(3), *pi0 = FPTR(4), *prs = FPTR(5);
+  const float *qv = FPTR(6), *qc = FPTR(7), *qr = FPTR(8), *qi = FPTR(9), *qs = FPTR(10), *qg = FPTR(11);
+  const float *c1 = FPTR(12), *c2 = FPTR(13), *mf = FPTR(14);
+  float *nm = FPTR(15), *sat = FPTR(17);
+  const int moist = IVAL(16), wantSat = IVAL(18);
+  const float rd = 287.04f, rv = 461.5f, cp = 1005.7f, cpv = 1870.0f, cpl = 4190.0f, cpi = 2106.0f;
+  const float lv1 = 3134708.0f, lv2 = 2320.0f, ls1 = 2898463.5f, ls2 = 236.0f, nmsat = 1e-10f, gAcc = 9.81f;
+  const int sk = g.sJ * g.sK;
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz + 1;
+    if (i >= g.nx || j >= g.ny || k > g.nz - 1) continue;
+    int c = GIDX(g, i, j, k), d = c - sk;
+    if (wantSat != 0) sat[c] = 0.0f;
+    float eps = DCR(rd, rv), reps = DCR(rv, rd);
+    float thA = th0[k - 1] + thPert[d], thB = th0[k] + thPert[c];
+    if (moist == 0) {
+      nm[c] = ((rr_log_cr(DCR(thB, thA)) * gAcc) * g.rdz) * mf[k];
+      continue;
+    }
+    float piA = pi0[k - 1] + ppPert[d], piB = pi0[k] + ppPert[c];
+    float tA = thA * piA, tB = thB * piB;
+    float qtA = ((((qv[d] + qc[d]) + qr[d]) + qi[d]) + qs[d]) + qg[d];
+    float qtB = ((((qv[c] + qc[c]) + qr[c]) + qi[c]) + qs[c]) + qg[c];
+    float qciA = (qv[d] + qc[d]) + qi[d], qciB = (qv[c] + qc[c]) + qi[c];
+    float thvA = DCR(thA * fmaf(reps, qv[d], 1.0f), 1.0f + qtA);
+    float thvB = DCR(thB * fmaf(reps, qv[c], 1.0f), 1.0f + qtB);
+    float rmf = g.rdz * mf[k];
+    float dlnT = rr_log_cr(DCR(tB, tA)) * rmf;
+    float dlnQt = rr_log_cr(DCR(1.0f + qtB, 1.0f + qtA)) * rmf;
+    float out = (gAcc * rr_log_cr(DCR(thvB, thvA))) * rmf;
+    float a = c1[k], b = c2[k];
+    float pavg = fmaf(a, prs[d], b * prs[c]), tavg = fmaf(a, tA, b * tB);
+    float qtavg = fmaf(a, qtA, b * qtB), qciavg = fmaf(a, qciA, b * qciB);
+    /* lam_1: moist-adiabatic N^2 for saturation ratio qvs, latent heat lh, dqvs/dT drdt */
+#define LAM1(qvs, lh, drdt, cpml)                                                                    \
+  (gAcc * fmaf(dlnT + DCR(DCR((gAcc * (1.0f + qtavg)) * (1.0f + DCR((lh) * (qvs), rd * tavg)),          \
+                              fmaf((lh), (drdt), (cpml))), tavg),                                      \
+               1.0f + DCR(tavg * (drdt), eps + (qvs)), -dlnQt))
+    const float al = 17.67f, bl = 29.65f, ai = 21.874557f, bi = 7.66f;
+    if (tavg >= 273.15f) {
+      float qvs = mp_rs(pavg, tavg, al, bl);
+      float ql = fmax_(qciavg - qvs, 0.0f);
+      if (ql > nmsat) {
+        if (wantSat != 0) sat[c] = 1.0f;
+        float qvl = fmax_(qciavg - ql, 0.0f);
+        float cpml = fmaf(cpl, ql, fmaf(cpv, qvl, cp));
+        float lh = fmaf(-lv2, tavg, lv1);
+        float drdt = DCR((al * (273.15f - bl)) * qvs, (tavg - bl) * (tavg - bl));
+        out = LAM1(qvs, lh, drdt, cpml);
+      }
+    } else if (tavg <= 233.15f) {
+      float qvs = mp_rs(pavg, tavg, ai, bi);
+      float qice = fmax_(qciavg - qvs, 0.0f);
+      if (qice > nmsat) {
+        if (wantSat != 0) sat[c] = 1.0f;
+        float qvl = fmax_(qciavg - qice, 0.0f);
+        float cpml = fmaf(cpi, qice, fmaf(cpv, qvl, cp));
+        float lh = fmaf(-ls2, tavg, ls1);
+        float drdt = DCR((ai * (273.15f - bi)) * qvs, (tavg - bi) * (tavg - bi));
+        out = LAM1(qvs, lh, drdt, cpml);
+      }
+    } else {
+      float ff = DCR(tavg - 233.15f, 273.15f - 233.15f);
+      float qvsl = mp_rs(pavg, tavg, al, bl), qvsi = mp_rs(pavg, tavg, ai, bi);
+      float qvs = fmaf(ff, qvsl, (1.0f - ff) * qvsi);
+      float qice = fmax_(0.0f, (1.0f - ff) * (qciavg - qvs));
+      float ql = fmax_(0.0f, ff * (qciavg - qvs));
+      if (ql + qice > nmsat) {
+        if (wantSat != 0) sat[c] = 1.0f;
+        float qvl = fmax_(0.0f, (qciavg - ql) - qice);
+        float cpml = fmaf(cpi, qice, fmaf(cpl, ql, fmaf(cpv, qvl, cp)));
+        float lhl = fmaf(-lv2, tavg, lv1);
+        float drdtl = DCR((al * (273.15f - bl)) * qvsl, (tavg - bl) * (tavg - bl));
+        float nml = LAM1(qvsl, lhl, drdtl, cpml);
+        float lhi = fmaf(-ls2, tavg, ls1);
+        float drdti = DCR((ai * (273.15f - bi)) * qvsi, (tavg - bi) * (tavg - bi));
+        float nmi = LAM1(qvsi, lhi, drdti, cpml);
+        out = fmaf(ff, nml, (1.0f - ff) * nmi);
+      }
+    }
+#undef LAM1
+    nm[c] = out;
+  }
+}
+
+void teor_turb_sfcstress(uint32_t *M, const uint32_t *ARG) {
+  /* turb_sfcstress.wgsl main: boundary stresses t13, t23 per column (i <= nx, j <= ny).
+   * Top (level nz): no-slip drag, or a copy of level nz-1.  Bottom (level 0) by mode:
+   * 0 copy of level 1; 4 no-slip drag; 2 constant drag coefficient 0.001229 with the
+   * surface wind speed s1 (plane 2 of sfc); 3 the drag against the domain-mean wind
+   * (planes 14..16 at the origin, lam_1); otherwise u*^2 w1 / max(s1, 0.01) (lam_2) */
+  Dims g = dims_at(M, B(0));
+  const float *sfc = FPTR(1), *rf = FPTR(2), *u = FPTR(6), *v = FPTR(7), *kmv = FPTR(9), *mf = FPTR(11);
+  float *t13 = FPTR(3), *t23 = FPTR(4);
+  const int mode = IVAL(5), topNoSlip = IVAL(10);
+  const float mx = bitsf(M[B(8)]), my = bitsf(M[B(8) + 1]);
+  const int plane = g.sJ * g.sK, sj = g.sJ;
+  const long GX = ARG[0], GY = ARG[1];
+#pragma omp parallel for collapse(2) schedule(static)
+  for (long ty = 0; ty < GY; ty++)
+    for (long tx = 0; tx < GX; tx++) {
+      int i = (int)tx, j = (int)ty;
+      if (i > g.nx || j > g.ny) continue;
+      int ct = GIDX(g, i, j, g.nz);
+      if (topNoSlip != 0) {
+        int cu = ct - plane;
+        float mft = 0.5f * (mf[g.nz] + mf[g.nz]);
+        t13[ct] = ((((((-2.0f) * (u[cu] + mx)) * g.rdz) * mft) * 0.5f) * (rf[ct - 1] + rf[ct])) * 0.5f * (kmv[cu - 1] + kmv[cu]);
+        t23[ct] = ((((((-2.0f) * (v[cu] + my)) * g.rdz) * mft) * 0.5f) * (rf[ct - sj] + rf[ct])) * 0.5f * (kmv[cu - sj] + kmv[cu]);
+      } else {
+        t13[ct] = t13[ct - plane];
+        t23[ct] = t23[ct - plane];
+      }
+      int c = GIDX(g, i, j, 0);
+      if (mode == 0) {
+        t13[c] = t13[c + plane];
+        t23[c] = t23[c + plane];
+      } else if (mode == 4) {
+        float mfb = 0.5f * (mf[0] + mf[0]);
+        t13[c] = ((((((2.0f * (u[c] + mx)) * g.rdz) * mfb) * 0.5f) * (rf[c - 1] + rf[c])) * 0.5f) * (kmv[c - 1 + plane] + kmv[c + plane]);
+        t23[c] = ((((((2.0f * (v[c] + my)) * g.rdz) * mfb) * 0.5f) * (rf[c - sj] + rf[c])) * 0.5f) * (kmv[c - sj + plane] + kmv[c + plane]);
+      } else if (mode == 2) {
+        float s1w = sfc[2 * plane + GIDX(g, i - 1, j, 0)], s1c = sfc[2 * plane + c], s1s = sfc[2 * plane + GIDX(g, i, j - 1, 0)];
+        t13[c] = ((((0.001229f * 0.5f) * (s1w + s1c)) * (u[c] + mx)) * 0.5f) * (rf[c - 1] + rf[c]);
+        t23[c] = ((((0.001229f * 0.5f) * (s1s + s1c)) * (v[c] + my)) * 0.5f) * (rf[c - sj] + rf[c]);
+      } else if (mode == 3) {
+        int o0 = GIDX(g, 0, 0, 0);
+        float au = sfc[14 * plane + o0], av = sfc[15 * plane + o0], as = sfc[16 * plane + o0];
+        float den = fmax_(0.0001f, as * sqrtf(fmaf(au, au, av * av)));
+#define L1(ii, jj, comp)                                                                                  \
+  DCR((sfc[3 * plane + GIDX(g, ii, jj, 0)] * sfc[3 * plane + GIDX(g, ii, jj, 0)]) *                        \
+          fmaf(sfc[2 * plane + GIDX(g, ii, jj, 0)], (comp) == 0 ? au : av,                                 \
+               as * (sfc[(comp) * plane + GIDX(g, ii, jj, 0)] - ((comp) == 0 ? au : av))),                 \
+      den)
+        t13[c] = (0.25f * (L1(i - 1, j, 0) + L1(i, j, 0))) * (rf[c - 1] + rf[c]);
+        t23[c] = (0.25f * (L1(i, j - 1, 1) + L1(i, j, 1))) * (rf[c - sj] + rf[c]);
+#undef L1
+      } else {
+#define L2(ii, jj, comp)                                                                                  \
+  DCR((sfc[3 * plane + GIDX(g, ii, jj, 0)] * sfc[3 * plane + GIDX(g, ii, jj, 0)]) *                        \
+          sfc[(comp) * plane + GIDX(g, ii, jj, 0)],                                                        \
+      fmax_(sfc[2 * plane + GIDX(g, ii, jj, 0)], 0.01f))
+        t13[c] = (0.25f * (L2(i - 1, j, 0) + L2(i, j, 0))) * (rf[c - 1] + rf[c]);
+        t23[c] = (0.25f * (L2(i, j - 1, 1) + L2(i, j, 1))) * (rf[c - sj] + rf[c]);
+#undef L2
+      }
+    }
+}
+
+void teor_turb_dissipative_heating(uint32_t *M, const uint32_t *ARG) {
+  /* turb_dissipative_heating.wgsl main: thten += eps / (cp_m/cv_m... pi): the dissipation
+   * averaged to the cell centre (at the surface with bbc3, u*^3 ln((dz1 + z0) / z0) / (k dz1)),
+   * divided by cp pi (dry) or (cp/cv) cv_m pi (moist) */
+  Dims g = dims_at(M, B(0));
+  const float *dissten = FPTR(1), *pi0 = FPTR(2), *ppi = FPTR(3), *qv = FPTR(4), *qc = FPTR(5), *qr = FPTR(6);
+  const float *qi = FPTR(7), *qs = FPTR(8), *qg = FPTR(9), *sfc = FPTR(12);
+  float *thten = FPTR(10);
+  const uint32_t pw = B(11);
+  const int moist = (int32_t)M[pw], bbc3 = (int32_t)M[pw + 1], zntField = (int32_t)M[pw + 4];
+  const float znt = bitsf(M[pw + 2]), dz1 = bitsf(M[pw + 3]);
+  const float cpd = 1005.7f, rd = 287.04f, cpv = 1870.0f, rv = 461.5f, karman = 0.4f;
+  const int sk = g.sJ * g.sK;
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    float cv = cpd - rd, cvv = cpv - rv, cpl = 4190.0f, cpi = 2106.0f, cpdcv = DCR(cpd, cv);
+    float epsd;
+    if (k == 0 && bbc3 != 0) {
+      float ust = sfc[3 * sk + GIDX(g, i, j, 0)];
+      float z0 = zntField != 0 ? sfc[4 * sk + GIDX(g, i, j, 0)] : znt;
+      epsd = DCR(((ust * ust) * ust) * te_log_f64(DCR(dz1 + z0, z0)), karman * dz1);
+    } else {
+      epsd = 0.5f * (dissten[c] + dissten[c + sk]);
+    }
+    float pi = pi0[k] + ppi[c], dheat;
+    if (moist != 0) {
+      float cvm = fmaf(cpi, (qi[c] + qs[c]) + qg[c], fmaf(cpl, qc[c] + qr[c], fmaf(cvv, qv[c], cv)));
+      dheat = DCR(epsd, (cpdcv * cvm) * pi);
+    } else {
+      dheat = DCR(epsd, cpd * pi);
+    }
+    thten[c] = thten[c] + dheat;
   }
 }

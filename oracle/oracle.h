@@ -28,6 +28,8 @@ float te_rr_pow_cr(float x, float p);
 
 #define TE_ORACLE_KERNEL(name) void teor_##name(uint32_t *M, const uint32_t *ARG);
 float te_pow_f64(float x, float y);
+float te_exp_f64(float x);
+float te_log_f64(float x);
 
 #define TE_ORACLE_KERNELS(X) \
   X(adv_flux_x) X(adv_flux_y) X(adv_flux_z) \
@@ -48,7 +50,8 @@ float te_pow_f64(float x, float y);
   X(turb_openbc_stress_x) X(turb_openbc_stress_y) X(tke_advance) X(tke_sources) X(tke_flux_h) \
   X(mp_pdefq) X(turb_scalar_vert_implicit) \
   X(rayleigh_damping) X(turb_rho_faces) X(turb_def_centers) X(turb_def_faces) X(turb_def_assemble) \
-  X(turb_gettau) X(turb_km_kh) X(tke_epst)
+  X(turb_gettau) X(turb_km_kh) X(tke_epst) \
+  X(turb_nm) X(turb_sfcstress) X(turb_dissipative_heating)
 TE_ORACLE_KERNELS(TE_ORACLE_KERNEL)
 
 #ifdef __cplusplus

@@ -114,3 +114,39 @@ def load_golden_scenario(name='single_cell'):
     with open(os.path.join(d, 'step1.json')) as fh:
         step1 = {int(k): v for k, v in json.load(fh).items()}
     return tape, init, hashes, step1
+
+
+def f32_word(x):
+    return int(np.float32(x).view(np.uint32))
+
+
+# Branches the recorded single_cell step does not take: per kernel, cases of
+# {binding: words written over the start of that binding's parameter struct}.
+_W = f32_word
+UNTAKEN_BRANCHES = {
+    'turb_scalar_vert_implicit': [
+        {15: [uf], 16: [ez], 18: [bt], 17: [_W(0.37), _W(301.5), _W(290.25), _W(ww)]}
+        for uf, ez, bt, ww in [(1, 0, 1, 0.0), (0, 0, 2, 0.0), (1, 1, 1, 0.0), (0, 1, 2, 0.0),
+                               (0, 1, 1, 1.0), (0, 1, 1, 2.0), (0, 0, 2, 1.0), (0, 0, 1, 2.0)]],
+    'rayleigh_damping': [{16: [1], 17: [0]}, {16: [0], 17: [1]}, {16: [1], 17: [1]}],
+    'mp_pdefq': [{3: [_W(1e-5)]}, {3: [_W(-1.0)]}],
+    'turb_km_kh': [{11: [_W(5.0)]}, {12: [_W(0.001)]}],
+    'turb_nm': [{16: [0]}, {18: [1]}, {16: [0], 18: [1]}],
+    'turb_sfcstress': [{5: [m], 10: [top], 8: [_W(1.5), _W(-0.5)]}
+                       for m, top in [(0, 1), (1, 0), (2, 0), (3, 1), (4, 0), (4, 1)]],
+    'turb_dissipative_heating': [{11: [moist, 1, _W(0.1), _W(500.0), zf]}
+                                 for moist, zf in [(1, 0), (1, 1), (0, 0), (0, 1)]] + [{11: [0]}],
+}
+# (binding, planes of one level each) filled with seeded positive values before those
+# cases, so that the branches read surface data that is not all zero
+BRANCH_FILLS = {'turb_scalar_vert_implicit': (14, 1), 'turb_sfcstress': (1, 17),
+                'turb_dissipative_heating': (12, 17)}
+
+
+def fill_for_branches(name, bind, mem, plane):
+    """Seeded surface data for the UNTAKEN_BRANCHES cases of `name` (in place)."""
+    if name not in BRANCH_FILLS:
+        return
+    idx, planes = BRANCH_FILLS[name]
+    vals = np.random.default_rng(7).uniform(0.05, 2.0, planes * plane).astype(np.float32)
+    mem[bind[idx]:bind[idx] + planes * plane] = vals.view(np.uint32)

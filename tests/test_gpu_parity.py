@@ -156,7 +156,7 @@ def test_golden_single_cell_in_scope_dispatches():
                 dirty.append((o.dst, o.n))
             else:
                 dirty.extend((off, ln) for _, off, ln in o.hashes if off is not None and ln)
-    assert ngpu >= 702   # 704 of the 718: dynamics, open boundaries, Rayleigh damping, most of the turbulence, pdefq
+    assert ngpu >= 705   # 707 of the 718: dynamics, open boundaries, Rayleigh damping, most of the turbulence, pdefq
     fields = {v // 4 + cpu.base[2]: k for k, v in tape['fields'].items()}
     slot_field = {s: fields.get(off) for o in cpu.ops if o.kind == 'k' for s, off, _ in o.hashes}
     bad = [s for s in gpu_hashes if gpu_hashes[s] != int(want[s])]
@@ -166,28 +166,11 @@ def test_golden_single_cell_in_scope_dispatches():
 
 
 
-def _f32(x):
-    return int(np.float32(x).view(np.uint32))
-
-
-# (kernel, {binding: words written over the start of its setBytes payload}); the recorded
-# single_cell step takes none of these branches
-UNTAKEN_BRANCHES = {
-    'turb_scalar_vert_implicit': [
-        {15: [uf], 16: [ez], 18: [bt], 17: [_f32(0.37), _f32(301.5), _f32(290.25), _f32(ww)]}
-        for uf, ez, bt, ww in [(1, 0, 1, 0.0), (0, 0, 2, 0.0), (1, 1, 1, 0.0), (0, 1, 2, 0.0),
-                               (0, 1, 1, 1.0), (0, 1, 1, 2.0), (0, 0, 2, 1.0)]],
-    'rayleigh_damping': [{16: [1], 17: [0]}, {16: [0], 17: [1]}, {16: [1], 17: [1]}],
-    'mp_pdefq': [{3: [_f32(1e-5)]}, {3: [_f32(-1.0)]}],
-    'turb_km_kh': [{11: [_f32(5.0)]}, {12: [_f32(0.001)]}],
-}
-
-
 def test_branches_the_recording_does_not_take():
     """Kernels of the recorded single_cell step, each at its first dispatch, with the
-    parameter structs of the branches the recording does not take, set through use_step
-    (the reference's useStep rewrites changed setBytes payloads): the GPU's written regions
-    equal the oracle's."""
+    parameter structs of the branches the recording does not take (helpers.UNTAKEN_BRANCHES),
+    set through use_step (the reference's useStep rewrites changed setBytes payloads): the
+    GPU's written regions equal the oracle's."""
     import base64
     from oracle.player import CpuPlayer
     from thunderengine_web_b200.replayer import Replayer
@@ -203,15 +186,18 @@ def test_branches_the_recording_does_not_take():
     r.plan(False)
     r.build()
     cmds0 = tape['steps'][0]
-    todo = dict(UNTAKEN_BRANCHES)
+    todo = dict(helpers.UNTAKEN_BRANCHES)
     checked = 0
     for oi, o in enumerate(cpu.ops):
         if o.kind == 'copy':
             cpu.M[o.dst:o.dst + o.n] = cpu.M[o.src:o.src + o.n]
             continue
-        for changes in todo.pop(o.name, []):
+        cases = todo.pop(o.name, [])
+        gd = o.bind[0] if cases else 0
+        for changes in cases:
             cmds = list(cmds0)
             E = cpu.M.copy()
+            helpers.fill_for_branches(o.name, o.bind, E, int(E[gd + 3]) * int(E[gd + 4]))
             for n, words in changes.items():
                 ci = max(c for c in range(o.index) if cmds0[c]['op'] == 'bytes' and cmds0[c]['index'] == n)
                 raw = bytearray(base64.b64decode(cmds0[ci]['data']))
@@ -231,7 +217,7 @@ def test_branches_the_recording_does_not_take():
         helpers.mixed(o.name)(cpu.M.ctypes.data_as(ctypes.c_void_p), o.arg.ctypes.data_as(ctypes.c_void_p))
         if not todo:
             break
-    assert checked == sum(len(v) for v in UNTAKEN_BRANCHES.values())
+    assert checked == sum(len(v) for v in helpers.UNTAKEN_BRANCHES.values())
 
 
 STEP_SCRATCH = set(helpers.SCRATCH)

@@ -107,59 +107,53 @@ def test_oracle_pinned_to_golden_single_cell(oracle_lib, ref_lib):
     assert {slot_field[s] for s in bad} <= {'tend', 'fpk'}
 
 
+# kernels whose result passes through a WGSL exp/log/pow of data-dependent arguments
+ROUNDING_BUILTINS = {'turb_dissipative_heating', 'turb_nm', 'turb_km_kh'}
+
+
 @pytest.mark.slow
-def test_column_kernels_on_branches_the_recording_does_not_take(oracle_lib, ref_lib):
-    """turb_scalar_vert_implicit and mp_pdefq, oracle vs the reference's kernels, on the
-    state of the recorded step at their first dispatch, with the flags of the branches the
-    recording does not take: explicit vertical fluxes, surface flux, bcturbs = 2 and the
-    three wall settings (turb_scalar_vert_implicit.wgsl lam_1), a clip threshold that
-    zeroes part of every column (mp_pdefq.wgsl), the lateral sponge and level-average
-    references of rayleigh_damping.wgsl, and a fixed km and the cmz floor of turb_km_kh.wgsl."""
-    import itertools
+def test_kernels_on_branches_the_recording_does_not_take(oracle_lib, ref_lib):
+    """Oracle vs the reference's kernels on the branches the recorded single_cell step does
+    not take (helpers.UNTAKEN_BRANCHES: implicit/explicit vertical diffusion with its wall
+    and surface-flux settings, pdefq clip thresholds, Rayleigh sponge and level averages,
+    fixed km, dry and saturated N^2, every surface-stress mode, surface dissipation),
+    each from the state of the recorded step at the kernel's first dispatch."""
     from oracle.player import CpuPlayer
     tape, init, want, step1 = helpers.load_golden_scenario()
     p = CpuPlayer(tape, helpers.kernels_meta())
     p.plan(False)
     for i, b in init.items():
         p.upload(i, b)
-    fb = lambda x: int(np.float32(x).view(np.uint32))
     vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
-    done = set()
+    todo = dict(helpers.UNTAKEN_BRANCHES)
     compared = 0
     for o in p.ops:
         if o.kind == 'copy':
             p.M[o.dst:o.dst + o.n] = p.M[o.src:o.src + o.n]
             continue
-        if o.name in ('turb_scalar_vert_implicit', 'mp_pdefq', 'rayleigh_damping', 'turb_km_kh') and o.name not in done:
-            done.add(o.name)
-            B = lambda n: int(o.arg[4 + n])
-            sk = 127 * 127   # one level of the 120 x 120 recording (halo 3 on each side)
-            if o.name == 'rayleigh_damping':
-                variants = [{B(16): a, B(17): b} for a in (0, 1) for b in (0, 1)]
-            elif o.name == 'turb_km_kh':
-                variants = [{B(11): fb(5.0)}, {B(12): fb(0.001)}]
-            elif o.name == 'mp_pdefq':
-                q = p.M[B(2):B(2) + 8 * sk].view(np.float32)
-                nz_q = np.abs(q[q != 0])
-                variants = [{B(3): fb(np.median(nz_q) if nz_q.size else 1e-6)}, {B(3): fb(-1.0)}]
+        cases = todo.pop(o.name, [])
+        gd = o.bind[0] if cases else 0
+        for changes in cases:
+            E = p.M.copy()
+            helpers.fill_for_branches(o.name, o.bind, E, int(E[gd + 3]) * int(E[gd + 4]))
+            for n, words in changes.items():
+                E[o.bind[n]:o.bind[n] + len(words)] = words
+            F = E.copy()
+            oracle_lib.get(o.name)(vp(E), vp(o.arg))
+            ref_lib.get(o.name)(vp(F), vp(o.arg))
+            diff = np.nonzero(E != F)[0]
+            if o.name in ROUNDING_BUILTINS and diff.size:
+                # WGSL leaves the precision of exp/log/pow to the implementation: the oracle
+                # rounds them correctly, the reference build calls the C library's binary32
+                # functions, which miss the correctly rounded result for a few arguments in
+                # 10^4; at those points the one-ulp difference, carried through the rest of
+                # the kernel's arithmetic, may reach a few ulps of the output, nothing else may
+                ulps = np.abs(E[diff].view(np.int32).astype(np.int64) - F[diff].view(np.int32).astype(np.int64))
+                assert ulps.max() <= 4 and diff.size <= 0.002 * o.grid[0] * o.grid[1] * o.grid[2], (o.name, changes)
             else:
-                variants = []
-                for uf, ez, bt, ww in itertools.product([0, 1], [0, 1], [1, 2], [0.0, 1.0, 2.0]):
-                    v = {B(15): uf, B(16): ez, B(18): bt}
-                    v.update({B(17) + q: fb(x) for q, x in enumerate([0.37, 301.5, 290.25, ww])})
-                    variants.append(v)
-            for v in variants:
-                E, F = p.M.copy(), p.M.copy()
-                for X in (E, F):
-                    for w, val in v.items():
-                        X[w] = val
-                    if o.name == 'turb_scalar_vert_implicit':
-                        X[B(14):B(14) + sk] = fb(0.011)
-                oracle_lib.get(o.name)(vp(E), vp(o.arg))
-                ref_lib.get(o.name)(vp(F), vp(o.arg))
-                assert np.array_equal(E, F), (o.name, v)
-                compared += 1
+                assert diff.size == 0, (o.name, changes)
+            compared += 1
         helpers.mixed(o.name)(vp(p.M), vp(o.arg))
-        if len(done) == 4:
+        if not todo:
             break
-    assert compared == 32
+    assert compared == sum(len(v) for v in helpers.UNTAKEN_BRANCHES.values())

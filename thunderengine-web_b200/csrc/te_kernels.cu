@@ -1028,7 +1028,7 @@ __global__ void k_turb_scalar_vert_implicit(KArgs A) {
   float *TE_R cA = A.p[11], *TE_R cB = A.p[12];
   const float dt = A.f[10];
   const int sk = g.sJ * g.sK, base = gidx(g, i, j, 0);
-  const TsviCol col{g, i, j, base, sk, A.iv[15], A.iv[18], s, khv, mf, rf, A.p[14], A.p[8], A.p[9], A.p[30], rr, A.p[13], A.v4[0]};
+  const TsviCol col{g, i, j, base, sk, A.iv[15], A.iv[18], s, khv, mf, rf, A.p[14], A.p[8], A.p[9], A.p[30], rr, A.p[13], A.sw[0]};
   if (A.iv[16] != 0) {
     float below = col.vflux(0);
     for (int k = 0; k < g.nz; k++) {
@@ -1126,7 +1126,7 @@ __global__ void k_turb_rho_faces(KArgs A) {
   if (i > g.nx + 1 || j > g.ny + 1 || k > g.nz) return;
   const float* TE_R rho = A.p[1];
   float *TE_R rr = A.p[4], *TE_R rf = A.p[5];
-  const float *cgs = A.v4[0], *cgt = A.v4[1];
+  const float *cgs = A.sw[0], *cgt = A.sw[1];
   const int sk = g.sJ * g.sK, c = gidx(g, i, j, k);
   if (k < g.nz) rr[c] = dcr(1.0f, rho[c]);
   float r;
@@ -1298,6 +1298,194 @@ __global__ void k_tke_epst(KArgs A) {
   A.p[15][c] = dcr(e, rf[c]);
 }
 TE_LAUNCH3(tke_epst)
+
+// saturation mixing ratio over liquid (a, b = 17.67, 29.65: f_mp_rslf) or ice (21.874557,
+// 7.66: f_mp_rsif), turb_nm.wgsl
+__device__ __forceinline__ float mp_rs(float p, float t, float a, float b) {
+  float es = 611.2f * exp_f64(dcr(a * (t - 273.15f), t - b));
+  es = wmin(es, p * 0.5f);
+  return dcr(dcr(287.04f, 461.5f) * es, p - es);
+}
+
+// turb_nm.wgsl: squared Brunt-Vaisala frequency on w levels 1..nz-1.  Dry: g dln(th)/dz;
+// moist: g dln(thv)/dz, or in saturated air (liquid above 0 C, ice below -40 C, a linear
+// blend between) the moist-adiabatic form (lam_1); sat marks saturated points
+__global__ void k_turb_nm(KArgs A) {
+  TE_K3
+  const int i = tx, j = ty, k = tz + 1;
+  if (i >= g.nx || j >= g.ny || k > g.nz - 1) return;
+  const float *TE_R thPert = A.p[1], *TE_R ppPert = A.p[2], *TE_R th0 = A.p[3], *TE_R pi0 = A.p[4], *TE_R prs = A.p[5];
+  const float *TE_R qv = A.p[6], *TE_R qc = A.p[7], *TE_R qr = A.p[8], *TE_R qi = A.p[9], *TE_R qs = A.p[10], *TE_R qg = A.p[11];
+  const float *TE_R mf = A.p[14];
+  float *TE_R nm = A.p[15], *TE_R sat = A.p[17];
+  const int moist = A.iv[16], wantSat = A.iv[18];
+  const float rd = 287.04f, rv = 461.5f, cp = 1005.7f, cpv = 1870.0f, cpl = 4190.0f, cpi = 2106.0f;
+  const float lv1 = 3134708.0f, lv2 = 2320.0f, ls1 = 2898463.5f, ls2 = 236.0f, nmsat = 1e-10f, gAcc = 9.81f;
+  const float al = 17.67f, bl = 29.65f, ai = 21.874557f, bi = 7.66f;
+  const int sk = g.sJ * g.sK, c = gidx(g, i, j, k), d = c - sk;
+  if (wantSat != 0) sat[c] = 0.0f;
+  const float eps = dcr(rd, rv), reps = dcr(rv, rd);
+  const float thA = th0[k - 1] + thPert[d], thB = th0[k] + thPert[c];
+  if (moist == 0) {
+    nm[c] = ((rr_log_cr(dcr(thB, thA)) * gAcc) * g.rdz) * mf[k];
+    return;
+  }
+  const float piA = pi0[k - 1] + ppPert[d], piB = pi0[k] + ppPert[c];
+  const float tA = thA * piA, tB = thB * piB;
+  const float qtA = ((((qv[d] + qc[d]) + qr[d]) + qi[d]) + qs[d]) + qg[d];
+  const float qtB = ((((qv[c] + qc[c]) + qr[c]) + qi[c]) + qs[c]) + qg[c];
+  const float qciA = (qv[d] + qc[d]) + qi[d], qciB = (qv[c] + qc[c]) + qi[c];
+  const float thvA = dcr(thA * fmaf(reps, qv[d], 1.0f), 1.0f + qtA);
+  const float thvB = dcr(thB * fmaf(reps, qv[c], 1.0f), 1.0f + qtB);
+  const float rmf = g.rdz * mf[k];
+  const float dlnT = rr_log_cr(dcr(tB, tA)) * rmf;
+  const float dlnQt = rr_log_cr(dcr(1.0f + qtB, 1.0f + qtA)) * rmf;
+  float out = (gAcc * rr_log_cr(dcr(thvB, thvA))) * rmf;
+  const float a = A.p[12][k], b = A.p[13][k];
+  const float pavg = fmaf(a, prs[d], b * prs[c]), tavg = fmaf(a, tA, b * tB);
+  const float qtavg = fmaf(a, qtA, b * qtB), qciavg = fmaf(a, qciA, b * qciB);
+  // lam_1: moist-adiabatic N^2 for saturation ratio qvs, latent heat lh, dqvs/dT drdt
+  auto lam1 = [&](float qvs, float lh, float drdt, float cpml) {
+    const float gamma = dcr((gAcc * (1.0f + qtavg)) * (1.0f + dcr(lh * qvs, rd * tavg)), fmaf(lh, drdt, cpml));
+    return gAcc * fmaf(dlnT + dcr(gamma, tavg), 1.0f + dcr(tavg * drdt, eps + qvs), -dlnQt);
+  };
+  if (tavg >= 273.15f) {
+    const float qvs = mp_rs(pavg, tavg, al, bl);
+    const float ql = wmax(qciavg - qvs, 0.0f);
+    if (ql > nmsat) {
+      if (wantSat != 0) sat[c] = 1.0f;
+      const float qvl = wmax(qciavg - ql, 0.0f);
+      const float cpml = fmaf(cpl, ql, fmaf(cpv, qvl, cp));
+      const float lh = fmaf(-lv2, tavg, lv1);
+      const float drdt = dcr((al * (273.15f - bl)) * qvs, (tavg - bl) * (tavg - bl));
+      out = lam1(qvs, lh, drdt, cpml);
+    }
+  } else if (tavg <= 233.15f) {
+    const float qvs = mp_rs(pavg, tavg, ai, bi);
+    const float qice = wmax(qciavg - qvs, 0.0f);
+    if (qice > nmsat) {
+      if (wantSat != 0) sat[c] = 1.0f;
+      const float qvl = wmax(qciavg - qice, 0.0f);
+      const float cpml = fmaf(cpi, qice, fmaf(cpv, qvl, cp));
+      const float lh = fmaf(-ls2, tavg, ls1);
+      const float drdt = dcr((ai * (273.15f - bi)) * qvs, (tavg - bi) * (tavg - bi));
+      out = lam1(qvs, lh, drdt, cpml);
+    }
+  } else {
+    const float ff = dcr(tavg - 233.15f, 273.15f - 233.15f);
+    const float qvsl = mp_rs(pavg, tavg, al, bl), qvsi = mp_rs(pavg, tavg, ai, bi);
+    const float qvs = fmaf(ff, qvsl, (1.0f - ff) * qvsi);
+    const float qice = wmax(0.0f, (1.0f - ff) * (qciavg - qvs));
+    const float ql = wmax(0.0f, ff * (qciavg - qvs));
+    if (ql + qice > nmsat) {
+      if (wantSat != 0) sat[c] = 1.0f;
+      const float qvl = wmax(0.0f, (qciavg - ql) - qice);
+      const float cpml = fmaf(cpi, qice, fmaf(cpl, ql, fmaf(cpv, qvl, cp)));
+      const float lhl = fmaf(-lv2, tavg, lv1);
+      const float drdtl = dcr((al * (273.15f - bl)) * qvsl, (tavg - bl) * (tavg - bl));
+      const float nml = lam1(qvsl, lhl, drdtl, cpml);
+      const float lhi = fmaf(-ls2, tavg, ls1);
+      const float drdti = dcr((ai * (273.15f - bi)) * qvsi, (tavg - bi) * (tavg - bi));
+      const float nmi = lam1(qvsi, lhi, drdti, cpml);
+      out = fmaf(ff, nml, (1.0f - ff) * nmi);
+    }
+  }
+  nm[c] = out;
+}
+TE_LAUNCH3(turb_nm)
+
+// turb_sfcstress.wgsl: boundary stresses t13, t23 per column (i <= nx, j <= ny).  Top:
+// no-slip drag or a copy of level nz-1.  Bottom by mode: 0 copy of level 1; 4 no-slip drag;
+// 2 drag coefficient 0.001229 with the surface wind speed (plane 2 of sfc); 3 drag against
+// the domain-mean wind (planes 14..16 at the origin, lam_1); else u*^2 w1 / max(s1, 0.01)
+__global__ void k_turb_sfcstress(KArgs A) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const Dims& g = A.g;
+  if (i >= A.gx || j >= A.gy || i > g.nx || j > g.ny) return;
+  const float *TE_R sfc = A.p[1], *TE_R rf = A.p[2], *TE_R u = A.p[6], *TE_R v = A.p[7], *TE_R kmv = A.p[9];
+  const float *TE_R mf = A.p[11];
+  float *TE_R t13 = A.p[3], *TE_R t23 = A.p[4];
+  const int mode = A.iv[5];
+  const float mx = A.f[8], my = __int_as_float(A.iv2[8]);
+  const int plane = g.sJ * g.sK, sj = g.sJ;
+  const int ct = gidx(g, i, j, g.nz);
+  if (A.iv[10] != 0) {
+    const int cu = ct - plane;
+    const float mft = 0.5f * (mf[g.nz] + mf[g.nz]);
+    t13[ct] = ((((((-2.0f) * (u[cu] + mx)) * g.rdz) * mft) * 0.5f) * (rf[ct - 1] + rf[ct])) * 0.5f * (kmv[cu - 1] + kmv[cu]);
+    t23[ct] = ((((((-2.0f) * (v[cu] + my)) * g.rdz) * mft) * 0.5f) * (rf[ct - sj] + rf[ct])) * 0.5f * (kmv[cu - sj] + kmv[cu]);
+  } else {
+    t13[ct] = t13[ct - plane];
+    t23[ct] = t23[ct - plane];
+  }
+  const int c = gidx(g, i, j, 0);
+  if (mode == 0) {
+    t13[c] = t13[c + plane];
+    t23[c] = t23[c + plane];
+  } else if (mode == 4) {
+    const float mfb = 0.5f * (mf[0] + mf[0]);
+    t13[c] = ((((((2.0f * (u[c] + mx)) * g.rdz) * mfb) * 0.5f) * (rf[c - 1] + rf[c])) * 0.5f) * (kmv[c - 1 + plane] + kmv[c + plane]);
+    t23[c] = ((((((2.0f * (v[c] + my)) * g.rdz) * mfb) * 0.5f) * (rf[c - sj] + rf[c])) * 0.5f) * (kmv[c - sj + plane] + kmv[c + plane]);
+  } else if (mode == 2) {
+    const float s1w = sfc[2 * plane + c - 1], s1c = sfc[2 * plane + c], s1s = sfc[2 * plane + c - sj];
+    t13[c] = ((((0.001229f * 0.5f) * (s1w + s1c)) * (u[c] + mx)) * 0.5f) * (rf[c - 1] + rf[c]);
+    t23[c] = ((((0.001229f * 0.5f) * (s1s + s1c)) * (v[c] + my)) * 0.5f) * (rf[c - sj] + rf[c]);
+  } else if (mode == 3) {
+    const int o0 = gidx(g, 0, 0, 0);
+    const float au = sfc[14 * plane + o0], av = sfc[15 * plane + o0], as = sfc[16 * plane + o0];
+    const float den = wmax(0.0001f, as * sqrtf(fmaf(au, au, av * av)));
+    auto lam1 = [&](int q, int comp) {
+      const float us = sfc[3 * plane + q], am = comp == 0 ? au : av;
+      return dcr((us * us) * fmaf(sfc[2 * plane + q], am, as * (sfc[comp * plane + q] - am)), den);
+    };
+    t13[c] = (0.25f * (lam1(c - 1, 0) + lam1(c, 0))) * (rf[c - 1] + rf[c]);
+    t23[c] = (0.25f * (lam1(c - sj, 1) + lam1(c, 1))) * (rf[c - sj] + rf[c]);
+  } else {
+    auto lam2 = [&](int q, int comp) {
+      const float us = sfc[3 * plane + q];
+      return dcr((us * us) * sfc[comp * plane + q], wmax(sfc[2 * plane + q], 0.01f));
+    };
+    t13[c] = (0.25f * (lam2(c - 1, 0) + lam2(c, 0))) * (rf[c - 1] + rf[c]);
+    t23[c] = (0.25f * (lam2(c - sj, 1) + lam2(c, 1))) * (rf[c - sj] + rf[c]);
+  }
+}
+static void launch_turb_sfcstress(const KArgs& A, cudaStream_t s) { launch_columns(k_turb_sfcstress, A, s); }
+
+// turb_dissipative_heating.wgsl: thten += dissipation / (cp pi) (dry) or / ((cp/cv) cv_m pi)
+// (moist); the dissipation averaged to the cell centre, at the surface with bbc3
+// u*^3 ln((dz1 + z0) / z0) / (k dz1)
+__global__ void k_turb_dissipative_heating(KArgs A) {
+  TE_K3
+  const int i = tx, j = ty, k = tz;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  const float *TE_R dissten = A.p[1], *TE_R ppi = A.p[3], *TE_R sfc = A.p[12];
+  float* TE_R thten = A.p[10];
+  const float* pw = A.sw[0];
+  const int moist = __float_as_int(pw[0]), bbc3 = __float_as_int(pw[1]), zntField = __float_as_int(pw[4]);
+  const float znt = pw[2], dz1 = pw[3];
+  const float cpd = 1005.7f, rd = 287.04f, cpv = 1870.0f, rv = 461.5f, karman = 0.4f;
+  const int sk = g.sJ * g.sK, c = gidx(g, i, j, k);
+  const float cv = cpd - rd, cvv = cpv - rv, cpl = 4190.0f, cpi = 2106.0f, cpdcv = dcr(cpd, cv);
+  float epsd;
+  if (k == 0 && bbc3 != 0) {
+    const float ust = sfc[3 * sk + c];
+    const float z0 = zntField != 0 ? sfc[4 * sk + c] : znt;
+    epsd = dcr(((ust * ust) * ust) * log_f64(dcr(dz1 + z0, z0)), karman * dz1);
+  } else {
+    epsd = 0.5f * (dissten[c] + dissten[c + sk]);
+  }
+  const float pi = A.p[2][k] + ppi[c];
+  float dheat;
+  if (moist != 0) {
+    const float cvm = fmaf(cpi, (A.p[7][c] + A.p[8][c]) + A.p[9][c], fmaf(cpl, A.p[5][c] + A.p[6][c], fmaf(cvv, A.p[4][c], cv)));
+    dheat = dcr(epsd, (cpdcv * cvm) * pi);
+  } else {
+    dheat = dcr(epsd, cpd * pi);
+  }
+  thten[c] = thten[c] + dheat;
+}
+TE_LAUNCH3(turb_dissipative_heating)
 
 // -------------------------------------------------- thermodynamic glue
 
@@ -1850,15 +2038,18 @@ static const KernelSpec kTable[] = {
     {"tke_sources", 6, {R(0), P(1), P(2), P(3), P(4), W(5)}, false, launch_tke_sources},
     {"tke_flux_h", 7, {R(0), P(1), P(2), P(3), W(4), W(5), P(30)}, false, launch_tke_flux_h},
     {"mp_pdefq", 4, {R(0), P(1), W(2), R(3)}, false, launch_mp_pdefq},
-    {"turb_scalar_vert_implicit", 20, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), R(10), W(11), W(12), W(13), P(14), R(15), R(16), {17, kRef4, 0}, R(18), P(30)}, false, launch_turb_scalar_vert_implicit},
+    {"turb_scalar_vert_implicit", 20, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), R(10), W(11), W(12), W(13), P(14), R(15), R(16), {17, kRefS, 0}, R(18), P(30)}, false, launch_turb_scalar_vert_implicit},
     {"rayleigh_damping", 20, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), R(9), W(10), W(11), W(12), W(13), P(14), P(15), R(16), R(17), P(18), P(19)}, false, launch_rayleigh_damping},
-    {"turb_rho_faces", 8, {R(0), P(1), P(2), P(3), W(4), W(5), {6, kRef4, 0}, {7, kRef4, 0}}, false, launch_turb_rho_faces},
+    {"turb_rho_faces", 8, {R(0), P(1), P(2), P(3), W(4), W(5), {6, kRefS, 0}, {7, kRefS, 0}}, false, launch_turb_rho_faces},
     {"turb_def_centers", 11, {R(0), P(1), P(2), P(3), P(4), P(5), W(6), W(7), W(8), W(9), P(30)}, false, launch_turb_def_centers},
     {"turb_def_faces", 9, {R(0), P(1), P(2), P(3), P(4), P(5), W(6), W(7), P(30)}, false, launch_turb_def_faces},
     {"turb_def_assemble", 12, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), W(10), W(11)}, false, launch_turb_def_assemble},
     {"turb_gettau", 10, {R(0), P(1), P(2), W(3), W(4), W(5), W(6), W(7), W(8), P(30)}, false, launch_turb_gettau},
     {"turb_km_kh", 14, {R(0), P(1), P(2), P(3), W(4), W(5), W(6), W(7), W(8), W(9), R(10), R(11), R(12), P(30)}, false, launch_turb_km_kh},
     {"tke_epst", 17, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), P(11), P(12), P(13), P(14), W(15), P(30)}, false, launch_tke_epst},
+    {"turb_nm", 19, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), P(11), P(12), P(13), P(14), W(15), R(16), W(17), R(18)}, false, launch_turb_nm},
+    {"turb_sfcstress", 13, {R(0), P(1), P(2), W(3), W(4), R(5), P(6), P(7), R(8), P(9), R(10), P(11), P(30)}, false, launch_turb_sfcstress},
+    {"turb_dissipative_heating", 13, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), W(10), {11, kRefS, 0}, P(12)}, false, launch_turb_dissipative_heating},
     {"update_diagnostics_moist", 20, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), P(11), P(12),
                                       P(13), P(14), W(15), W(16), W(17), W(18), W(19)}, false, TE_ROWVEC(update_diagnostics_moist, OpUpdateDiagnosticsMoist)},
     {"pressure_tendency", 15, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), R(9), R(10), R(12), P(13), R(14), W(11)},

@@ -21,10 +21,10 @@ struct KArgs {
   float f[kMaxBind];
   int iv[kMaxBind];
   int iv2[kMaxBind];
-  float v4[2][4];  // the words of the kernel's first and second vec3/vec4 reference bindings (kRef4)
+  float sw[2][8];  // the first 8 words of the kernel's first and second struct bindings (kRefS)
 };
 
-enum ParamKind : uint8_t { kPtr = 0, kRef = 1, kRef4 = 2 };
+enum ParamKind : uint8_t { kPtr = 0, kRef = 1, kRefS = 2 };
 
 struct ParamSpec {
   int8_t index;

@@ -34,19 +34,19 @@ __device__ __forceinline__ float dcr(float a, float b) { return a / b; }
 __device__ __forceinline__ float wmin(float a, float b) { return (b < a || a != a) ? b : a; }
 __device__ __forceinline__ float wmax(float a, float b) { return (a < b || a != a) ? b : a; }
 
-// x^y for the reference's WGSL pow builtin, whose precision WGSL leaves to the
-// implementation: 2^(y log2 x) in binary64 with plain operations, rounded once to binary32.
-// log2 x = e + ln(m) / ln 2 with m in [sqrt(1/2), sqrt(2)) and ln m = 2 atanh(s),
-// s = (m - 1) / (m + 1), by its odd power series to s^23; 2^t = 2^n e^r, n = rint(t),
-// r = (t - n) ln 2, by the Taylor series of e^r to r^14.  The binary64 error is far below
-// half a binary32 ulp: the correctly rounded power except within that error of a rounding
-// boundary.  The same operations in the same order on every device (no contraction).
-__device__ __forceinline__ float pow_f64(float x, float y) {
-  if (!(x > 0.0f) || x == INFINITY)
-    return x == 0.0f ? (y > 0.0f ? 0.0f : INFINITY) : (x == INFINITY ? (y > 0.0f ? INFINITY : 0.0f) : NAN);
+// The reference's WGSL pow, exp and log builtins, whose precision WGSL leaves to the
+// implementation, evaluated in binary64 with plain operations and rounded once to binary32:
+//   ln x = e ln 2 + 2 atanh(s) for x = 2^e m, m in [sqrt(1/2), sqrt(2)), s = (m - 1) / (m + 1),
+//          atanh by its odd power series to s^23;
+//   2^t  = 2^n e^r, n = rint(t), r = (t - n) ln 2, e^r by its Taylor series to r^14;
+//   x^y = 2^(y log2 x), e^x = 2^(x / ln 2).
+// The binary64 error is far below half a binary32 ulp: each is the correctly rounded value
+// except within that error of a rounding boundary.  The same operations in the same order
+// on every device (no contraction).
+__device__ __forceinline__ double ln_mantissa(float x, int& e) {  // x > 0 normal
   const uint32_t b = __float_as_uint(x);
-  int e = (int)(b >> 23) - 127;
   double m = (double)__uint_as_float((b & 0x7fffffu) | 0x3f800000u);
+  e = (int)(b >> 23) - 127;
   if (m > 1.4142135623730951) {
     m = m * 0.5;
     e = e + 1;
@@ -55,7 +55,9 @@ __device__ __forceinline__ float pow_f64(float x, float y) {
   double p = 1.0 / 23;
 #pragma unroll
   for (int k = 21; k >= 1; k -= 2) p = p * s2 + 1.0 / k;
-  const double t = (double)y * ((double)e + (2.0 * s * p) * 1.4426950408889634);
+  return 2.0 * s * p;
+}
+__device__ __forceinline__ float exp2_rounded(double t) {
   if (t > 128.0) return INFINITY;
   if (t < -126.0) return 0.0f;
   const double n = rint(t), r = (t - n) * 0.6931471805599453;
@@ -63,6 +65,25 @@ __device__ __forceinline__ float pow_f64(float x, float y) {
 #pragma unroll
   for (int k = 14; k >= 1; k--) q = 1.0 + (r * (1.0 / k)) * q;
   return (float)ldexp(q, (int)n);
+}
+__device__ __forceinline__ float pow_f64(float x, float y) {
+  if (!(x > 0.0f) || x == INFINITY)
+    return x == 0.0f ? (y > 0.0f ? 0.0f : INFINITY) : (x == INFINITY ? (y > 0.0f ? INFINITY : 0.0f) : NAN);
+  int e;
+  const double lm = ln_mantissa(x, e);
+  return exp2_rounded((double)y * ((double)e + lm * 1.4426950408889634));
+}
+__device__ __forceinline__ float exp_f64(float x) {
+  if (x != x) return x;
+  return exp2_rounded((double)x * 1.4426950408889634);
+}
+__device__ __forceinline__ float log_f64(float x) {
+  if (x != x || x < 0.0f) return NAN;
+  if (x == 0.0f) return -INFINITY;
+  if (x == INFINITY) return INFINITY;
+  int e;
+  const double lm = ln_mantissa(x, e);
+  return (float)((double)e * 0.6931471805599453 + lm);
 }
 
 // Quotients of constants, rounded once (the reference writes e.g. div_cr(13.0, 12.0)).
@@ -201,6 +222,14 @@ __device__ __forceinline__ F2 rr_log_ff(float x) {
 
 // exp of a two-float argument: k = round(y / ln2), Taylor series of the remainder,
 // final rounding to nearest fixed up by the residual.
+// f_rr_log_cr (turb_nm.wgsl): the two-float log summed; non-positive, infinite and NaN
+// arguments take the log builtin's special values
+__device__ __forceinline__ float rr_log_cr(float x) {
+  if (!(x > 0.0f) || x == INFINITY) return x == 0.0f ? -INFINITY : (x == INFINITY ? INFINITY : NAN);
+  const F2 a = rr_log_ff(x);
+  return a.x + a.y;
+}
+
 __device__ __forceinline__ float rr_exp_ff(F2 y) {
   const float ln2h = 0.69314575f, ln2m = 1.4285906e-06f, ln2l = 1.6198487e-11f;
   float k = rintf(dcr(y.x, 0.6931472f));

@@ -331,10 +331,10 @@ void Plan::finalize_args(std::vector<Op>& ops) {
         A.iv[ps.index] = (int)word(it->second);
         A.f[ps.index] = fl(it->second);
         A.iv2[ps.index] = (int)word(it->second + 1);
-        if (ps.kind == kRef4) {
-          if (nvec == 2) throw ApiError(TE_EINVAL, o.name + ": more than two vector parameter structs");
-          for (int w = 0; w < 4; w++)  // a vec3 may end the setBytes area: its fourth word reads 0
-            A.v4[nvec][w] = w < 3 || it->second + w < bytes_spare_end ? fl(it->second + w) : 0.0f;
+        if (ps.kind == kRefS) {
+          if (nvec == 2) throw ApiError(TE_EINVAL, o.name + ": more than two struct parameters read by words");
+          for (int w = 0; w < 8; w++)  // words past the end of the setBytes area read 0
+            A.sw[nvec][w] = it->second + w < bytes_spare_end ? fl(it->second + w) : 0.0f;
           nvec++;
         }
       }
