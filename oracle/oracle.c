@@ -2224,3 +2224,189 @@ void teor_turb_dissipative_heating(uint32_t *M, const uint32_t *ARG) {
     thten[c] = thten[c] + dheat;
   }
 }
+
+/* turb_u_tendency.wgsl / turb_v_tendency.wgsl main (axis 0: u, axis 1: v; the v kernel is
+ * the u kernel with x and y exchanged): subgrid momentum tendency.  Horizontal stress
+ * divergence (zero on open edges) plus either the explicit vertical one or, per column, an
+ * implicit vertical diffusion solved by a Thomas sweep (cA, cB; cB ends as the new
+ * velocity), its tendency rho (new - old) / dt, and the dw/dx (dw/dy) cross term dwd */
+static void turb_uv_tendency(uint32_t *M, const uint32_t *ARG, int axis) {
+  Dims g = dims_at(M, B(0));
+  const float *X = FPTR(1), *w = FPTR(2), *rho = FPTR(3), *rf = FPTR(4), *kmv = FPTR(5);
+  const float *A1 = FPTR(6), *A2 = FPTR(7), *A3 = FPTR(8), *mh = FPTR(9), *mf = FPTR(10), *hm = FPTR(30);
+  float *cA = FPTR(12), *cB = FPTR(13), *dwd = FPTR(14), *ten = FPTR(15);
+  const float dt = FVAL(11);
+  const int openx = (int32_t)M[B(16)], openy = (int32_t)M[B(16) + 1], explicitZ = IVAL(17);
+  const int sj = g.sJ, sk = g.sJ * g.sK, s = axis == 0 ? 1 : sj;
+  const long GX = ARG[0], GY = ARG[1];
+#pragma omp parallel for collapse(2) schedule(static)
+  for (long ty = 0; ty < GY; ty++)
+    for (long tx = 0; tx < GX; tx++) {
+      int i = (int)tx, j = (int)ty;
+      if (axis == 0 ? (i > g.nx || j >= g.ny) : (i >= g.nx || j > g.ny)) continue;
+      int zeroX = openx != 0 && (i == 0 || i == (axis == 0 ? g.nx : g.nx - 1));
+      int zeroY = openy != 0 && (j == 0 || j == (axis == 0 ? g.ny - 1 : g.ny));
+      const int base = GIDX(g, i, j, 0);
+#define HORIZ(c)                                                                                         \
+  ((zeroX ? 0.0f : axis == 0 ? ((A1[c] - A1[(c) - 1]) * g.rdx) * hm_uf(&g, hm, i)                        \
+                             : ((A1[(c) + 1] - A1[c]) * g.rdx) * hm_uh(&g, hm, i)) +                     \
+   (zeroY ? 0.0f : axis == 0 ? ((A2[(c) + sj] - A2[c]) * g.rdy) * hm_vh(&g, hm, j)                       \
+                             : ((A2[c] - A2[(c) - sj]) * g.rdy) * hm_vf(&g, hm, j)))
+#define RINV(k) DCR(1.0f, 0.5f * (rho[base + (k) * sk - s] + rho[base + (k) * sk]))
+      if (explicitZ != 0) {
+        for (int k = 0; k < g.nz; k++) {
+          int c = base + k * sk;
+          float turbz = (((A3[c + sk] - A3[c]) * g.rdz) * 0.5f) * (mh[k] + mh[k]);
+          ten[c] = ten[c] + DCR(HORIZ(c) + turbz, 0.5f * (rho[c - s] + rho[c]));
+        }
+        continue;
+      }
+      const float tema = (((-0.0625f) * dt) * g.rdz) * g.rdz, temc = (0.5f * dt) * g.rdz, rdt = DCR(0.5f, dt);
+      for (int k = 0; k <= g.nz; k++) {
+        int c = base + k * sk;
+        float dwx = axis == 0 ? ((w[c] - w[c - 1]) * g.rdx) * hm_uf(&g, hm, i) : ((w[c] - w[c - sj]) * g.rdy) * hm_vf(&g, hm, j);
+        dwd[c] = ((dwx * 0.25f) * (kmv[c - s] + kmv[c])) * (rf[c - s] + rf[c]);
+      }
+      /* lam_1: coefficient of the face at level lev for the cell at level k */
+#define LAM1(k, lev) \
+  ((((kmv[base + (lev) * sk - s] + kmv[base + (lev) * sk]) * (mf[lev] + mf[lev])) * (rf[base + (lev) * sk - s] + rf[base + (lev) * sk])) * ((mh[k] + mh[k]) * RINV(k)))
+      {
+        float cfc = tema * LAM1(0, 1), cfb = 1.0f - cfc;
+        float cfd = fmaf(-((temc * A3[base]) * (mh[0] + mh[0])), RINV(0), X[base]);
+        float t = DCR(1.0f, cfb);
+        cA[base] = (-cfc) * t;
+        cB[base] = cfd * t;
+      }
+      for (int k = 1; k < g.nz - 1; k++) {
+        int c = base + k * sk;
+        float cfa = tema * LAM1(k, k), cfc = tema * LAM1(k, k + 1), cfb = (1.0f - cfa) - cfc;
+        float t = DCR(1.0f, fmaf(cfa, cA[c - sk], cfb));
+        cA[c] = (-cfc) * t;
+        cB[c] = fmaf(-cfa, cB[c - sk], X[c]) * t;
+      }
+      {
+        int kt = g.nz - 1, ct = base + kt * sk;
+        float cfa = tema * LAM1(kt, kt), cfb = 1.0f - cfa;
+        float cfd = fmaf((temc * A3[base + g.nz * sk]) * (mh[kt] + mh[kt]), RINV(kt), X[ct]);
+        float t = DCR(1.0f, fmaf(cfa, cA[ct - sk], cfb));
+        cB[ct] = fmaf(-cfa, cB[ct - sk], cfd) * t;
+      }
+#undef LAM1
+      for (int k = g.nz - 2; k >= 0; k--) {
+        int c = base + k * sk;
+        cB[c] = fmaf(cA[c], cB[c + sk], cB[c]);
+      }
+      for (int k = 0; k < g.nz; k++) {
+        int c = base + k * sk;
+        float turbz = ((rho[c - s] + rho[c]) * (cB[c] - X[c])) * rdt;
+        turbz = fmaf(((dwd[c + sk] - dwd[c]) * g.rdz) * 0.5f, mh[k] + mh[k], turbz);
+        ten[c] = fmaf(HORIZ(c) + turbz, RINV(k), ten[c]);
+      }
+#undef HORIZ
+#undef RINV
+    }
+}
+void teor_turb_u_tendency(uint32_t *M, const uint32_t *ARG) { turb_uv_tendency(M, ARG, 0); }
+void teor_turb_v_tendency(uint32_t *M, const uint32_t *ARG) { turb_uv_tendency(M, ARG, 1); }
+
+/* turb_w_tendency.wgsl and tke_transport.wgsl main (tke = 1): tendency of a w-level
+ * quantity q (w, or TKE) on levels 1..nz-1.  Horizontal divergence (w: of the stresses
+ * t13, t23; TKE: of -fx, -fy), zero on open edges, plus the explicit vertical divergence
+ * or, per column, the implicit vertical diffusion (Thomas sweep over levels 1..nz-1 with
+ * the boundary fluxes folded into the right-hand side), tendency rf (new - old) / dt */
+static void turb_wlevel_tendency(uint32_t *M, const uint32_t *ARG, int tke) {
+  Dims g = dims_at(M, B(0));
+  const float *q, *rho, *rf, *kmh, *kmv = 0, *h1, *h2, *t33 = 0, *mh, *mf, *hm = FPTR(30);
+  float *cA, *cB, *ten;
+  float dt;
+  int ob;
+  if (tke) {
+    q = FPTR(1); rho = FPTR(2); rf = FPTR(3); kmh = FPTR(4); kmv = FPTR(5); mh = FPTR(6); mf = FPTR(7);
+    dt = FVAL(8); cA = FPTR(9); cB = FPTR(10); h1 = FPTR(11); h2 = FPTR(12); ten = FPTR(13); ob = 14;
+  } else {
+    q = FPTR(1); rho = FPTR(2); rf = FPTR(3); kmh = FPTR(4); h1 = FPTR(5); h2 = FPTR(6); t33 = FPTR(7);
+    mh = FPTR(8); mf = FPTR(9); dt = FVAL(10); cA = FPTR(11); cB = FPTR(12); ten = FPTR(13); ob = 14;
+  }
+  const int openx = (int32_t)M[B(ob)], openy = (int32_t)M[B(ob) + 1], explicitZ = IVAL(ob + 1);
+  const int sj = g.sJ, sk = g.sJ * g.sK;
+  const long GX = ARG[0], GY = ARG[1];
+#pragma omp parallel for collapse(2) schedule(static)
+  for (long ty = 0; ty < GY; ty++)
+    for (long tx = 0; tx < GX; tx++) {
+      int i = (int)tx, j = (int)ty;
+      if (i >= g.nx || j >= g.ny) continue;
+      int zeroX = openx != 0 && (i == 0 || i == g.nx - 1), zeroY = openy != 0 && (j == 0 || j == g.ny - 1);
+      const int base = GIDX(g, i, j, 0);
+#define HORIZ(c)                                                                                          \
+  ((zeroX ? 0.0f : tke ? ((-(h1[(c) + 1] - h1[c])) * g.rdx) * hm_uh(&g, hm, i) : ((h1[(c) + 1] - h1[c]) * g.rdx) * hm_uh(&g, hm, i)) + \
+   (zeroY ? 0.0f : tke ? ((-(h2[(c) + sj] - h2[c])) * g.rdy) * hm_vh(&g, hm, j) : ((h2[(c) + sj] - h2[c]) * g.rdy) * hm_vh(&g, hm, j)))
+      /* TKE vertical flux at cell level k (lam_1 of tke_transport.wgsl) */
+#define TFLUX(k) \
+  (((((-(kmv[base + (k) * sk] + kmv[base + (k) * sk + sk])) * (q[base + (k) * sk + sk] - q[base + (k) * sk])) * g.rdz) * mh[k]) * rho[base + (k) * sk])
+      if (explicitZ != 0) {
+        float below = tke ? TFLUX(0) : 0.0f;
+        for (int k = 1; k < g.nz; k++) {
+          int c = base + k * sk;
+          float turbz;
+          if (tke) {
+            float here = TFLUX(k);
+            turbz = ((-(here - below)) * g.rdz) * mf[k];
+            below = here;
+          } else {
+            turbz = ((t33[c] - t33[c - sk]) * g.rdz) * mf[k];
+          }
+          ten[c] = ten[c] + DCR(HORIZ(c) + turbz, rf[c]);
+        }
+        continue;
+      }
+      const float tema = (((-1.0f) * dt) * g.rdz) * g.rdz, temc = dt * g.rdz, rdt = DCR(1.0f, dt);
+      /* coefficients of the faces above (UP) and below (DN) w level k */
+#define MFR(k) DCR(mf[k], rf[base + (k) * sk])
+#define UP(k) ((((kmh[base + (k) * sk] + kmh[base + (k) * sk + sk]) * mh[k]) * rho[base + (k) * sk]) * MFR(k))
+#define DN(k) ((((kmh[base + (k) * sk - sk] + kmh[base + (k) * sk]) * mh[(k) - 1]) * rho[base + (k) * sk - sk]) * MFR(k))
+      {
+        int c = base + sk;
+        float cfc = tema * UP(1), cfb = 1.0f - cfc, cfd;
+        if (tke)
+          cfd = fmaf(temc * ((((-(kmv[c - sk] + kmv[c])) * (q[c] - q[c - sk])) * g.rdz) * mh[0]) * rho[c - sk], MFR(1), q[c]);
+        else
+          cfd = fmaf(-(temc * t33[c - sk]), MFR(1), q[c]);
+        float t = DCR(1.0f, cfb);
+        cA[c] = (-cfc) * t;
+        cB[c] = cfd * t;
+      }
+      for (int k = 2; k < g.nz - 1; k++) {
+        int c = base + k * sk;
+        float cfa = tema * DN(k), cfc = tema * UP(k), cfb = (1.0f - cfa) - cfc;
+        float t = DCR(1.0f, fmaf(cfa, cA[c - sk], cfb));
+        cA[c] = (-cfc) * t;
+        cB[c] = fmaf(-cfa, cB[c - sk], q[c]) * t;
+      }
+      {
+        int kt = g.nz - 1, ct = base + kt * sk;
+        float cfa = tema * DN(kt), cfb = 1.0f - cfa, cfd;
+        if (tke)
+          cfd = fmaf(-(temc * (((((-(kmv[ct] + kmv[ct + sk])) * (q[ct + sk] - q[ct])) * g.rdz) * mh[kt]) * rho[ct])), MFR(kt), q[ct]);
+        else
+          cfd = fmaf(temc * t33[ct], MFR(kt), q[ct]);
+        float t = DCR(1.0f, fmaf(cfa, cA[ct - sk], cfb));
+        cB[ct] = fmaf(-cfa, cB[ct - sk], cfd) * t;
+      }
+#undef UP
+#undef DN
+#undef MFR
+#undef TFLUX
+      for (int k = g.nz - 2; k >= 1; k--) {
+        int c = base + k * sk;
+        cB[c] = fmaf(cA[c], cB[c + sk], cB[c]);
+      }
+      for (int k = 1; k < g.nz; k++) {
+        int c = base + k * sk;
+        float turbz = (rf[c] * (cB[c] - q[c])) * rdt;
+        ten[c] = ten[c] + DCR(HORIZ(c) + turbz, rf[c]);
+      }
+#undef HORIZ
+    }
+}
+void teor_turb_w_tendency(uint32_t *M, const uint32_t *ARG) { turb_wlevel_tendency(M, ARG, 0); }
+void teor_tke_transport(uint32_t *M, const uint32_t *ARG) { turb_wlevel_tendency(M, ARG, 1); }

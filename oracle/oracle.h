@@ -51,7 +51,8 @@ float te_log_f64(float x);
   X(mp_pdefq) X(turb_scalar_vert_implicit) \
   X(rayleigh_damping) X(turb_rho_faces) X(turb_def_centers) X(turb_def_faces) X(turb_def_assemble) \
   X(turb_gettau) X(turb_km_kh) X(tke_epst) \
-  X(turb_nm) X(turb_sfcstress) X(turb_dissipative_heating)
+  X(turb_nm) X(turb_sfcstress) X(turb_dissipative_heating) \
+  X(turb_u_tendency) X(turb_v_tendency) X(turb_w_tendency) X(tke_transport)
 TE_ORACLE_KERNELS(TE_ORACLE_KERNEL)
 
 #ifdef __cplusplus

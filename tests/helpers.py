@@ -136,6 +136,10 @@ UNTAKEN_BRANCHES = {
                        for m, top in [(0, 1), (1, 0), (2, 0), (3, 1), (4, 0), (4, 1)]],
     'turb_dissipative_heating': [{11: [moist, 1, _W(0.1), _W(500.0), zf]}
                                  for moist, zf in [(1, 0), (1, 1), (0, 0), (0, 1)]] + [{11: [0]}],
+    'turb_u_tendency': [{17: [1]}, {16: [0, 0]}, {16: [0, 1], 17: [1]}],
+    'turb_v_tendency': [{17: [1]}, {16: [0, 0]}, {16: [1, 0], 17: [1]}],
+    'turb_w_tendency': [{15: [1]}, {14: [0, 0]}, {14: [0, 1], 15: [1]}],
+    'tke_transport': [{15: [1]}, {14: [0, 0]}, {14: [1, 0], 15: [1]}],
 }
 # (binding, planes of one level each) filled with seeded positive values before those
 # cases, so that the branches read surface data that is not all zero

@@ -156,7 +156,7 @@ def test_golden_single_cell_in_scope_dispatches():
                 dirty.append((o.dst, o.n))
             else:
                 dirty.extend((off, ln) for _, off, ln in o.hashes if off is not None and ln)
-    assert ngpu >= 705   # 707 of the 718: dynamics, open boundaries, Rayleigh damping, most of the turbulence, pdefq
+    assert ngpu >= 709   # 711 of the 718: dynamics, open boundaries, Rayleigh damping, turbulence, pdefq
     fields = {v // 4 + cpu.base[2]: k for k, v in tape['fields'].items()}
     slot_field = {s: fields.get(off) for o in cpu.ops if o.kind == 'k' for s, off, _ in o.hashes}
     bad = [s for s in gpu_hashes if gpu_hashes[s] != int(want[s])]

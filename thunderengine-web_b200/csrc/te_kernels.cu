@@ -1487,6 +1487,180 @@ __global__ void k_turb_dissipative_heating(KArgs A) {
 }
 TE_LAUNCH3(turb_dissipative_heating)
 
+// turb_u_tendency.wgsl (AX 0) and turb_v_tendency.wgsl (AX 1, x and y exchanged): subgrid
+// momentum tendency per column.  Horizontal stress divergence (zero on open edges) plus
+// the explicit vertical divergence, or an implicit vertical diffusion by a Thomas sweep
+// (cA, cB; cB ends as the new velocity) with tendency rho (new - old) / dt and the dw/dx
+// (dw/dy) cross term dwd.  s is the offset of the staggered neighbour (1 or strideJ).
+template <int AX>
+__global__ void k_turb_uv_tendency(KArgs A) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const Dims& g = A.g;
+  if (i >= A.gx || j >= A.gy) return;
+  if (AX == 0 ? (i > g.nx || j >= g.ny) : (i >= g.nx || j > g.ny)) return;
+  const float *TE_R X = A.p[1], *TE_R w = A.p[2], *TE_R rho = A.p[3], *TE_R rf = A.p[4], *TE_R kmv = A.p[5];
+  const float *TE_R A1 = A.p[6], *TE_R A2 = A.p[7], *TE_R A3 = A.p[8], *TE_R mh = A.p[9], *TE_R mf = A.p[10];
+  const float* TE_R hm = A.p[30];
+  float *TE_R cA = A.p[12], *TE_R cB = A.p[13], *TE_R dwd = A.p[14], *TE_R ten = A.p[15];
+  const float dt = A.f[11];
+  const bool zeroX = A.iv[16] != 0 && (i == 0 || i == (AX == 0 ? g.nx : g.nx - 1));
+  const bool zeroY = A.iv2[16] != 0 && (j == 0 || j == (AX == 0 ? g.ny - 1 : g.ny));
+  const int sj = g.sJ, sk = g.sJ * g.sK, s = AX == 0 ? 1 : sj, base = gidx(g, i, j, 0);
+  auto horiz = [&](int c) {
+    const float tx = zeroX ? 0.0f
+                           : (AX == 0 ? ((A1[c] - A1[c - 1]) * g.rdx) * hm_uf(g, hm, i) : ((A1[c + 1] - A1[c]) * g.rdx) * hm_uh(g, hm, i));
+    const float ty = zeroY ? 0.0f
+                           : (AX == 0 ? ((A2[c + sj] - A2[c]) * g.rdy) * hm_vh(g, hm, j) : ((A2[c] - A2[c - sj]) * g.rdy) * hm_vf(g, hm, j));
+    return tx + ty;
+  };
+  auto rinv = [&](int k) { return dcr(1.0f, 0.5f * (rho[base + k * sk - s] + rho[base + k * sk])); };
+  if (A.iv[17] != 0) {
+    for (int k = 0; k < g.nz; k++) {
+      const int c = base + k * sk;
+      const float turbz = (((A3[c + sk] - A3[c]) * g.rdz) * 0.5f) * (mh[k] + mh[k]);
+      ten[c] = ten[c] + dcr(horiz(c) + turbz, 0.5f * (rho[c - s] + rho[c]));
+    }
+    return;
+  }
+  const float tema = (((-0.0625f) * dt) * g.rdz) * g.rdz, temc = (0.5f * dt) * g.rdz, rdt = dcr(0.5f, dt);
+  for (int k = 0; k <= g.nz; k++) {
+    const int c = base + k * sk;
+    const float dwx = AX == 0 ? ((w[c] - w[c - 1]) * g.rdx) * hm_uf(g, hm, i) : ((w[c] - w[c - sj]) * g.rdy) * hm_vf(g, hm, j);
+    dwd[c] = ((dwx * 0.25f) * (kmv[c - s] + kmv[c])) * (rf[c - s] + rf[c]);
+  }
+  // lam_1: coefficient of the face at level lev for the cell at level k
+  auto lam1 = [&](int k, int lev) {
+    const int cl = base + lev * sk;
+    return (((kmv[cl - s] + kmv[cl]) * (mf[lev] + mf[lev])) * (rf[cl - s] + rf[cl])) * ((mh[k] + mh[k]) * rinv(k));
+  };
+  {
+    const float cfc = tema * lam1(0, 1), cfb = 1.0f - cfc;
+    const float cfd = fmaf(-((temc * A3[base]) * (mh[0] + mh[0])), rinv(0), X[base]);
+    const float t = dcr(1.0f, cfb);
+    cA[base] = (-cfc) * t;
+    cB[base] = cfd * t;
+  }
+  for (int k = 1; k < g.nz - 1; k++) {
+    const int c = base + k * sk;
+    const float cfa = tema * lam1(k, k), cfc = tema * lam1(k, k + 1), cfb = (1.0f - cfa) - cfc;
+    const float t = dcr(1.0f, fmaf(cfa, cA[c - sk], cfb));
+    cA[c] = (-cfc) * t;
+    cB[c] = fmaf(-cfa, cB[c - sk], X[c]) * t;
+  }
+  {
+    const int kt = g.nz - 1, ct = base + kt * sk;
+    const float cfa = tema * lam1(kt, kt), cfb = 1.0f - cfa;
+    const float cfd = fmaf((temc * A3[base + g.nz * sk]) * (mh[kt] + mh[kt]), rinv(kt), X[ct]);
+    const float t = dcr(1.0f, fmaf(cfa, cA[ct - sk], cfb));
+    cB[ct] = fmaf(-cfa, cB[ct - sk], cfd) * t;
+  }
+  for (int k = g.nz - 2; k >= 0; k--) {
+    const int c = base + k * sk;
+    cB[c] = fmaf(cA[c], cB[c + sk], cB[c]);
+  }
+  for (int k = 0; k < g.nz; k++) {
+    const int c = base + k * sk;
+    float turbz = ((rho[c - s] + rho[c]) * (cB[c] - X[c])) * rdt;
+    turbz = fmaf(((dwd[c + sk] - dwd[c]) * g.rdz) * 0.5f, mh[k] + mh[k], turbz);
+    ten[c] = fmaf(horiz(c) + turbz, rinv(k), ten[c]);
+  }
+}
+static void launch_turb_u_tendency(const KArgs& A, cudaStream_t s) { launch_columns(k_turb_uv_tendency<0>, A, s); }
+static void launch_turb_v_tendency(const KArgs& A, cudaStream_t s) { launch_columns(k_turb_uv_tendency<1>, A, s); }
+
+// turb_w_tendency.wgsl (TKE 0) and tke_transport.wgsl (TKE 1): tendency of a w-level
+// quantity q on levels 1..nz-1 per column.  Horizontal divergence (w: of t13, t23; TKE: of
+// -fx, -fy), zero on open edges, plus the explicit vertical divergence or the implicit
+// vertical diffusion (Thomas sweep over levels 1..nz-1, boundary fluxes folded into the
+// right-hand side), tendency rf (new - old) / dt.
+template <int TKE>
+__global__ void k_turb_wlevel(KArgs A) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const Dims& g = A.g;
+  if (i >= A.gx || j >= A.gy || i >= g.nx || j >= g.ny) return;
+  const float *TE_R q = A.p[1], *TE_R rho = A.p[2], *TE_R rf = A.p[3], *TE_R kmh = A.p[4];
+  const float *TE_R kmv = TKE ? A.p[5] : nullptr, *TE_R h1 = TKE ? A.p[11] : A.p[5], *TE_R h2 = TKE ? A.p[12] : A.p[6];
+  const float *TE_R t33 = TKE ? nullptr : A.p[7], *TE_R mh = TKE ? A.p[6] : A.p[8], *TE_R mf = TKE ? A.p[7] : A.p[9];
+  const float* TE_R hm = A.p[30];
+  float *TE_R cA = TKE ? A.p[9] : A.p[11], *TE_R cB = TKE ? A.p[10] : A.p[12], *TE_R ten = A.p[13];
+  const float dt = TKE ? A.f[8] : A.f[10];
+  const bool zeroX = A.iv[14] != 0 && (i == 0 || i == g.nx - 1), zeroY = A.iv2[14] != 0 && (j == 0 || j == g.ny - 1);
+  const int sj = g.sJ, sk = g.sJ * g.sK, base = gidx(g, i, j, 0);
+  auto horiz = [&](int c) {
+    const float tx = zeroX ? 0.0f : (TKE ? ((-(h1[c + 1] - h1[c])) * g.rdx) * hm_uh(g, hm, i) : ((h1[c + 1] - h1[c]) * g.rdx) * hm_uh(g, hm, i));
+    const float ty = zeroY ? 0.0f : (TKE ? ((-(h2[c + sj] - h2[c])) * g.rdy) * hm_vh(g, hm, j) : ((h2[c + sj] - h2[c]) * g.rdy) * hm_vh(g, hm, j));
+    return tx + ty;
+  };
+  // TKE vertical flux at cell level k (lam_1 of tke_transport.wgsl)
+  auto tflux = [&](int k) {
+    const int c = base + k * sk;
+    return ((((-(kmv[c] + kmv[c + sk])) * (q[c + sk] - q[c])) * g.rdz) * mh[k]) * rho[c];
+  };
+  if (A.iv[15] != 0) {
+    float below = TKE ? tflux(0) : 0.0f;
+    for (int k = 1; k < g.nz; k++) {
+      const int c = base + k * sk;
+      float turbz;
+      if (TKE) {
+        const float here = tflux(k);
+        turbz = ((-(here - below)) * g.rdz) * mf[k];
+        below = here;
+      } else {
+        turbz = ((t33[c] - t33[c - sk]) * g.rdz) * mf[k];
+      }
+      ten[c] = ten[c] + dcr(horiz(c) + turbz, rf[c]);
+    }
+    return;
+  }
+  const float tema = (((-1.0f) * dt) * g.rdz) * g.rdz, temc = dt * g.rdz, rdt = dcr(1.0f, dt);
+  auto mfr = [&](int k) { return dcr(mf[k], rf[base + k * sk]); };
+  auto up = [&](int k) {
+    const int c = base + k * sk;
+    return (((kmh[c] + kmh[c + sk]) * mh[k]) * rho[c]) * mfr(k);
+  };
+  auto dn = [&](int k) {
+    const int c = base + k * sk;
+    return (((kmh[c - sk] + kmh[c]) * mh[k - 1]) * rho[c - sk]) * mfr(k);
+  };
+  {
+    const int c = base + sk;
+    const float cfc = tema * up(1), cfb = 1.0f - cfc;
+    const float cfd = TKE ? fmaf(temc * ((((-(kmv[c - sk] + kmv[c])) * (q[c] - q[c - sk])) * g.rdz) * mh[0]) * rho[c - sk], mfr(1), q[c])
+                          : fmaf(-(temc * t33[c - sk]), mfr(1), q[c]);
+    const float t = dcr(1.0f, cfb);
+    cA[c] = (-cfc) * t;
+    cB[c] = cfd * t;
+  }
+  for (int k = 2; k < g.nz - 1; k++) {
+    const int c = base + k * sk;
+    const float cfa = tema * dn(k), cfc = tema * up(k), cfb = (1.0f - cfa) - cfc;
+    const float t = dcr(1.0f, fmaf(cfa, cA[c - sk], cfb));
+    cA[c] = (-cfc) * t;
+    cB[c] = fmaf(-cfa, cB[c - sk], q[c]) * t;
+  }
+  {
+    const int kt = g.nz - 1, ct = base + kt * sk;
+    const float cfa = tema * dn(kt), cfb = 1.0f - cfa;
+    const float cfd = TKE ? fmaf(-(temc * (((((-(kmv[ct] + kmv[ct + sk])) * (q[ct + sk] - q[ct])) * g.rdz) * mh[kt]) * rho[ct])), mfr(kt), q[ct])
+                          : fmaf(temc * t33[ct], mfr(kt), q[ct]);
+    const float t = dcr(1.0f, fmaf(cfa, cA[ct - sk], cfb));
+    cB[ct] = fmaf(-cfa, cB[ct - sk], cfd) * t;
+  }
+  for (int k = g.nz - 2; k >= 1; k--) {
+    const int c = base + k * sk;
+    cB[c] = fmaf(cA[c], cB[c + sk], cB[c]);
+  }
+  for (int k = 1; k < g.nz; k++) {
+    const int c = base + k * sk;
+    const float turbz = (rf[c] * (cB[c] - q[c])) * rdt;
+    ten[c] = ten[c] + dcr(horiz(c) + turbz, rf[c]);
+  }
+}
+static void launch_turb_w_tendency(const KArgs& A, cudaStream_t s) { launch_columns(k_turb_wlevel<0>, A, s); }
+static void launch_tke_transport(const KArgs& A, cudaStream_t s) { launch_columns(k_turb_wlevel<1>, A, s); }
+
 // -------------------------------------------------- thermodynamic glue
 
 __global__ void k_update_diagnostics_moist(KArgs A) {
@@ -2050,6 +2224,10 @@ static const KernelSpec kTable[] = {
     {"turb_nm", 19, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), P(11), P(12), P(13), P(14), W(15), R(16), W(17), R(18)}, false, launch_turb_nm},
     {"turb_sfcstress", 13, {R(0), P(1), P(2), W(3), W(4), R(5), P(6), P(7), R(8), P(9), R(10), P(11), P(30)}, false, launch_turb_sfcstress},
     {"turb_dissipative_heating", 13, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), W(10), {11, kRefS, 0}, P(12)}, false, launch_turb_dissipative_heating},
+    {"turb_u_tendency", 19, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), R(11), W(12), W(13), W(14), W(15), R(16), R(17), P(30)}, false, launch_turb_u_tendency},
+    {"turb_v_tendency", 19, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), R(11), W(12), W(13), W(14), W(15), R(16), R(17), P(30)}, false, launch_turb_v_tendency},
+    {"turb_w_tendency", 17, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), R(10), W(11), W(12), W(13), R(14), R(15), P(30)}, false, launch_turb_w_tendency},
+    {"tke_transport", 17, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), R(8), W(9), W(10), W(11), W(12), W(13), R(14), R(15), P(30)}, false, launch_tke_transport},
     {"update_diagnostics_moist", 20, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), P(11), P(12),
                                       P(13), P(14), W(15), W(16), W(17), W(18), W(19)}, false, TE_ROWVEC(update_diagnostics_moist, OpUpdateDiagnosticsMoist)},
     {"pressure_tendency", 15, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), R(9), R(10), R(12), P(13), R(14), W(11)},
