@@ -2410,3 +2410,130 @@ static void turb_wlevel_tendency(uint32_t *M, const uint32_t *ARG, int tke) {
 }
 void teor_turb_w_tendency(uint32_t *M, const uint32_t *ARG) { turb_wlevel_tendency(M, ARG, 0); }
 void teor_tke_transport(uint32_t *M, const uint32_t *ARG) { turb_wlevel_tendency(M, ARG, 1); }
+
+/* two-float accumulation of the mass sums (f_df_add / f_df_add_pair, mass_row_sums.wgsl):
+ * acc.x + x by an error-free sum, the error accumulated in acc.y */
+static inline void df_add(F2 *acc, float x) {
+  float s = acc->x + x, bb = s - acc->x;
+  float err = (acc->x - (s - bb)) + (x - bb);
+  acc->x = s;
+  acc->y = acc->y + err;
+}
+static inline void df_add_pair(F2 *acc, float vx, float vy) {
+  df_add(acc, vx);
+  acc->y = acc->y + vy;
+}
+
+void teor_mass_row_sums(uint32_t *M, const uint32_t *ARG) {
+  /* mass_row_sums.wgsl main: per (j, k) row, the two-float sums over i of the cell mass
+   * rho / (uh vh mh) (rows1) and of pi0 + pp3d (rows2), stored at (k strideK + j) pairs */
+  Dims g = dims_at(M, B(0));
+  const float *rho = FPTR(1), *pi0 = FPTR(2), *pp3d = FPTR(3), *mh = FPTR(4), *hm = FPTR(30);
+  float *rows1 = FPTR(5), *rows2 = FPTR(6);
+  const long GX = ARG[0], GY = ARG[1];
+#pragma omp parallel for collapse(2) schedule(static)
+  for (long ty = 0; ty < GY; ty++)
+    for (long tx = 0; tx < GX; tx++) {
+      int j = (int)tx, k = (int)ty;
+      if (j >= g.ny || k >= g.nz) continue;
+      F2 s1 = {0.0f, 0.0f}, s2 = {0.0f, 0.0f};
+      float rvh = DCR(1.0f, hm_vh(&g, hm, j));
+      for (int i = 0; i < g.nx; i++) {
+        int c = GIDX(g, i, j, k);
+        float rmh = DCR(1.0f, mh[k]);
+        df_add(&s1, ((rho[c] * DCR(1.0f, hm_uh(&g, hm, i))) * rvh) * rmh);
+        df_add(&s2, pi0[k] + pp3d[c]);
+      }
+      long o = 2L * ((long)k * g.sK + j);
+      rows1[o] = s1.x;
+      rows1[o + 1] = s1.y;
+      rows2[o] = s2.x;
+      rows2[o + 1] = s2.y;
+    }
+}
+
+void teor_mass_level_sums(uint32_t *M, const uint32_t *ARG) {
+  /* mass_level_sums.wgsl main: per level k, the two-float sums over j of the row pairs */
+  Dims g = dims_at(M, B(0));
+  const float *rows1 = FPTR(1), *rows2 = FPTR(2);
+  float *levels1 = FPTR(3), *levels2 = FPTR(4);
+  const long GX = ARG[0];
+#pragma omp parallel for schedule(static)
+  for (long tx = 0; tx < GX; tx++) {
+    int k = (int)tx;
+    if (k >= g.nz) continue;
+    F2 s1 = {0.0f, 0.0f}, s2 = {0.0f, 0.0f};
+    for (int j = 0; j < g.ny; j++) {
+      long o = 2L * ((long)k * g.sK + j);
+      df_add_pair(&s1, rows1[o], rows1[o + 1]);
+      df_add_pair(&s2, rows2[o], rows2[o + 1]);
+    }
+    levels1[2 * k] = s1.x;
+    levels1[2 * k + 1] = s1.y;
+    levels2[2 * k] = s2.x;
+    levels2[2 * k + 1] = s2.y;
+  }
+}
+
+void teor_mass_reference_init(uint32_t *M, const uint32_t *ARG) {
+  /* mass_reference_init.wgsl main: on its first run (ref[2] == 0) thread 0 stores the total
+   * mass (two-float sum of the level sums) as the reference and sets ref[2] = 1 */
+  Dims g = dims_at(M, B(0));
+  const float *levels1 = FPTR(1);
+  float *ref = FPTR(2);
+  if (ARG[0] == 0 || ref[2] != 0.0f) return;
+  F2 s = {0.0f, 0.0f};
+  for (int k = 0; k < g.nz; k++) df_add_pair(&s, levels1[2 * k], levels1[2 * k + 1]);
+  ref[0] = s.x;
+  ref[1] = s.y;
+  ref[2] = 1.0f;
+}
+
+/* (1 + r)^a - 1 (f_powm1, mass_correction_apply.wgsl): the WGSL pow for |r| > 0.05, else
+ * its third-order expansion */
+static float powm1(float r, float a) {
+  if (fabsf(r) > 0.05f) return te_pow_f64(1.0f + r, a) - 1.0f;
+  return r * fmaf(r, fmaf(a * (a - 1.0f), 0.5f, DCR(((r * a) * (a - 1.0f)) * (a - 2.0f), 6.0f)), a);
+}
+
+void teor_mass_correction_apply(uint32_t *M, const uint32_t *ARG) {
+  /* mass_correction_apply.wgsl main: the relative mass change r against the reference,
+   * turned into a uniform pi' correction tem = ((1 + r)^(rd/cv) - 1) sum(pi) / (nx ny nz),
+   * added to pp3d; prs and rho recomputed from the corrected pi; thread (0,0,0) records
+   * tem, the mass, the pi sum, r and the mass's low part in out[0..4] */
+  Dims g = dims_at(M, B(0));
+  const float *levels1 = FPTR(2), *levels2 = FPTR(3), *ref = FPTR(4), *thPert = FPTR(5);
+  const float *th0 = FPTR(7), *pi0 = FPTR(8), *qv = FPTR(9);
+  float *pp3d = FPTR(6), *prs = FPTR(10), *rho = FPTR(11), *out = FPTR(12);
+  const int moist = IVAL(1);
+  const float rd = 287.04f, cp = 1005.7f, rv = 461.5f, p00 = 1e+05f;
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) continue;
+    F2 m2 = {0.0f, 0.0f}, pp2 = {0.0f, 0.0f};
+    for (int kk = 0; kk < g.nz; kk++) {
+      df_add_pair(&m2, levels1[2 * kk], levels1[2 * kk + 1]);
+      df_add_pair(&pp2, levels2[2 * kk], levels2[2 * kk + 1]);
+    }
+    float rddcv = DCR(rd, cp - rd);
+    float r = DCR((ref[0] - m2.x) + (ref[1] - m2.y), m2.x);
+    float p2 = pp2.x + pp2.y;
+    float tem = DCR(powm1(r, rddcv) * p2, (float)((g.nx * g.ny) * g.nz));
+    if (i == 0 && j == 0 && k == 0) {
+      out[0] = tem;
+      out[1] = m2.x;
+      out[2] = p2;
+      out[3] = r;
+      out[4] = m2.y;
+    }
+    int c = GIDX(g, i, j, k);
+    float pp = pp3d[c] + tem;
+    pp3d[c] = pp;
+    float cpdrd = DCR(cp, rd);
+    float pi = pi0[k] + pp, th = th0[k] + thPert[c];
+    float p = p00 * te_rr_pow_cr(pi, cpdrd);
+    prs[c] = p;
+    float rmix = moist != 0 ? fmaf(fmax_(0.0f, qv[c]), rv, rd) : rd;
+    rho[c] = DCR(p, (th * pi) * rmix);
+  }
+}

@@ -121,7 +121,8 @@ def f32_word(x):
 
 
 # Branches the recorded single_cell step does not take: per kernel, cases of
-# {binding: words written over the start of that binding's parameter struct}.
+# {binding: words written over the start of that binding's parameter struct}; a key
+# ('at', binding, offset) writes buffer words at that offset of a pointer binding instead.
 _W = f32_word
 UNTAKEN_BRANCHES = {
     'turb_scalar_vert_implicit': [
@@ -140,6 +141,9 @@ UNTAKEN_BRANCHES = {
     'turb_v_tendency': [{17: [1]}, {16: [0, 0]}, {16: [1, 0], 17: [1]}],
     'turb_w_tendency': [{15: [1]}, {14: [0, 0]}, {14: [0, 1], 15: [1]}],
     'tke_transport': [{15: [1]}, {14: [0, 0]}, {14: [1, 0], 15: [1]}],
+    'mass_reference_init': [{('at', 2, 2): [_W(1.0)]}],
+    # the recorded total mass is 2.75e5: these references make r = 0.45 and -0.27
+    'mass_correction_apply': [{1: [0]}, {('at', 4, 0): [_W(4.0e5)]}, {('at', 4, 0): [_W(2.0e5)], 1: [0]}],
 }
 # (binding, planes of one level each) filled with seeded positive values before those
 # cases, so that the branches read surface data that is not all zero

@@ -1661,6 +1661,121 @@ __global__ void k_turb_wlevel(KArgs A) {
 static void launch_turb_w_tendency(const KArgs& A, cudaStream_t s) { launch_columns(k_turb_wlevel<0>, A, s); }
 static void launch_tke_transport(const KArgs& A, cudaStream_t s) { launch_columns(k_turb_wlevel<1>, A, s); }
 
+// Two-float accumulation of the mass sums (f_df_add / f_df_add_pair, mass_row_sums.wgsl):
+// acc.x + x by an error-free sum, the error accumulated in acc.y.  The sums run in the
+// reference's order (one thread per row, level or total), so the results are its words.
+__device__ __forceinline__ void df_add(F2& acc, float x) {
+  const float s = acc.x + x, bb = s - acc.x;
+  const float err = (acc.x - (s - bb)) + (x - bb);
+  acc.x = s;
+  acc.y = acc.y + err;
+}
+__device__ __forceinline__ void df_add_pair(F2& acc, float vx, float vy) {
+  df_add(acc, vx);
+  acc.y = acc.y + vy;
+}
+
+// mass_row_sums.wgsl: per (j, k) row the sums over i of rho / (uh vh mh) (rows1) and of
+// pi0 + pp3d (rows2), stored as pairs at k strideK + j
+__global__ void k_mass_row_sums(KArgs A) {
+  TE_K3
+  const int j = tx, k = ty;
+  if (j >= g.ny || k >= g.nz) return;
+  const float *TE_R rho = A.p[1], *TE_R pp3d = A.p[3], *TE_R hm = A.p[30];
+  const float pik = A.p[2][k], mhk = A.p[4][k];
+  F2 s1{0.0f, 0.0f}, s2{0.0f, 0.0f};
+  const float rvh = dcr(1.0f, hm_vh(g, hm, j));
+  for (int i = 0; i < g.nx; i++) {
+    const int c = gidx(g, i, j, k);
+    const float rmh = dcr(1.0f, mhk);
+    df_add(s1, ((rho[c] * dcr(1.0f, hm_uh(g, hm, i))) * rvh) * rmh);
+    df_add(s2, pik + pp3d[c]);
+  }
+  const long o = 2L * ((long)k * g.sK + j);
+  A.p[5][o] = s1.x;
+  A.p[5][o + 1] = s1.y;
+  A.p[6][o] = s2.x;
+  A.p[6][o + 1] = s2.y;
+}
+TE_LAUNCH3(mass_row_sums)
+
+// mass_level_sums.wgsl: per level the sums over j of the row pairs
+__global__ void k_mass_level_sums(KArgs A) {
+  TE_K3
+  const int k = tx;
+  if (ty != 0 || k >= g.nz) return;
+  const float *TE_R rows1 = A.p[1], *TE_R rows2 = A.p[2];
+  F2 s1{0.0f, 0.0f}, s2{0.0f, 0.0f};
+  for (int j = 0; j < g.ny; j++) {
+    const long o = 2L * ((long)k * g.sK + j);
+    df_add_pair(s1, rows1[o], rows1[o + 1]);
+    df_add_pair(s2, rows2[o], rows2[o + 1]);
+  }
+  A.p[3][2 * k] = s1.x;
+  A.p[3][2 * k + 1] = s1.y;
+  A.p[4][2 * k] = s2.x;
+  A.p[4][2 * k + 1] = s2.y;
+}
+TE_LAUNCH3(mass_level_sums)
+
+// mass_reference_init.wgsl: on its first run (ref[2] == 0) thread 0 stores the total mass
+// (the sum of the level pairs) as the reference and sets ref[2] = 1
+__global__ void k_mass_reference_init(KArgs A) {
+  TE_K3
+  if (tx != 0 || ty != 0) return;
+  const float* TE_R levels1 = A.p[1];
+  float* TE_R ref = A.p[2];
+  if (ref[2] != 0.0f) return;
+  F2 s{0.0f, 0.0f};
+  for (int k = 0; k < g.nz; k++) df_add_pair(s, levels1[2 * k], levels1[2 * k + 1]);
+  ref[0] = s.x;
+  ref[1] = s.y;
+  ref[2] = 1.0f;
+}
+TE_LAUNCH3(mass_reference_init)
+
+// mass_correction_apply.wgsl: relative mass change r against the reference turned into a
+// uniform pi' correction tem = ((1 + r)^(rd/cv) - 1) sum(pi) / (nx ny nz) (f_powm1: the pow
+// builtin for |r| > 0.05, else its third-order expansion), added to pp3d; prs and rho from
+// the corrected pi; thread (0,0,0) records tem, the mass, the pi sum, r and the mass's low part
+__global__ void k_mass_correction_apply(KArgs A) {
+  TE_K3
+  const int i = tx, j = ty, k = tz;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  const float *TE_R levels1 = A.p[2], *TE_R levels2 = A.p[3], *TE_R ref = A.p[4], *TE_R thPert = A.p[5];
+  float *TE_R pp3d = A.p[6], *TE_R prs = A.p[10], *TE_R rho = A.p[11];
+  const float rd = 287.04f, cp = 1005.7f, rv = 461.5f, p00 = 1e+05f;
+  F2 m2{0.0f, 0.0f}, pp2{0.0f, 0.0f};
+  for (int kk = 0; kk < g.nz; kk++) {
+    df_add_pair(m2, levels1[2 * kk], levels1[2 * kk + 1]);
+    df_add_pair(pp2, levels2[2 * kk], levels2[2 * kk + 1]);
+  }
+  const float rddcv = dcr(rd, cp - rd);
+  const float r = dcr((ref[0] - m2.x) + (ref[1] - m2.y), m2.x);
+  const float p2 = pp2.x + pp2.y;
+  const float pm1 = fabsf(r) > 0.05f ? pow_f64(1.0f + r, rddcv) - 1.0f
+                                     : r * fmaf(r, fmaf(rddcv * (rddcv - 1.0f), 0.5f, dcr(((r * rddcv) * (rddcv - 1.0f)) * (rddcv - 2.0f), 6.0f)), rddcv);
+  const float tem = dcr(pm1 * p2, (float)((g.nx * g.ny) * g.nz));
+  if (i == 0 && j == 0 && k == 0) {
+    float* out = A.p[12];
+    out[0] = tem;
+    out[1] = m2.x;
+    out[2] = p2;
+    out[3] = r;
+    out[4] = m2.y;
+  }
+  const int c = gidx(g, i, j, k);
+  const float pp = pp3d[c] + tem;
+  pp3d[c] = pp;
+  const float cpdrd = dcr(cp, rd);
+  const float pi = A.p[8][k] + pp, th = A.p[7][k] + thPert[c];
+  const float p = p00 * rr_pow_cr(pi, cpdrd);
+  prs[c] = p;
+  const float rmix = A.iv[1] != 0 ? fmaf(wmax(0.0f, A.p[9][c]), rv, rd) : rd;
+  rho[c] = dcr(p, (th * pi) * rmix);
+}
+TE_LAUNCH3(mass_correction_apply)
+
 // -------------------------------------------------- thermodynamic glue
 
 __global__ void k_update_diagnostics_moist(KArgs A) {
@@ -2228,6 +2343,10 @@ static const KernelSpec kTable[] = {
     {"turb_v_tendency", 19, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), R(11), W(12), W(13), W(14), W(15), R(16), R(17), P(30)}, false, launch_turb_v_tendency},
     {"turb_w_tendency", 17, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), R(10), W(11), W(12), W(13), R(14), R(15), P(30)}, false, launch_turb_w_tendency},
     {"tke_transport", 17, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), R(8), W(9), W(10), W(11), W(12), W(13), R(14), R(15), P(30)}, false, launch_tke_transport},
+    {"mass_row_sums", 8, {R(0), P(1), P(2), P(3), P(4), W(5), W(6), P(30)}, false, launch_mass_row_sums},
+    {"mass_level_sums", 5, {R(0), P(1), P(2), W(3), W(4)}, false, launch_mass_level_sums},
+    {"mass_reference_init", 3, {R(0), P(1), W(2)}, false, launch_mass_reference_init},
+    {"mass_correction_apply", 13, {R(0), R(1), P(2), P(3), P(4), P(5), W(6), P(7), P(8), P(9), W(10), W(11), W(12)}, false, launch_mass_correction_apply},
     {"update_diagnostics_moist", 20, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), P(11), P(12),
                                       P(13), P(14), W(15), W(16), W(17), W(18), W(19)}, false, TE_ROWVEC(update_diagnostics_moist, OpUpdateDiagnosticsMoist)},
     {"pressure_tendency", 15, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), R(9), R(10), R(12), P(13), R(14), W(11)},
