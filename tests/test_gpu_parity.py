@@ -103,15 +103,26 @@ def test_unknown_kernel_is_an_error_at_plan_or_run():
         r2.encode_steps(1, with_hashes=True)
 
 
-def test_golden_single_cell_in_scope_dispatches():
-    """Recorded single_cell step 1: every in-scope dispatch runs on the GPU (the others on
-    the CPU reference build); region hashes and buffer FNVs are compared with the
-    recording.  Scratch tend/fpk hashes are exempt as the reference documents."""
+# Recorded scenarios and whether the oracle reproduces the recording itself.  On the
+# horizontally stretched grid the grid scale (dx dy dz)^(1/3) of turb_km_kh.wgsl takes many
+# values, and at some of them the recording's pow builtin (whose precision WGSL leaves to
+# the implementation) is not the correctly rounded power; from that dispatch on the
+# recording is not reproducible bit for bit, so there the GPU is checked against the
+# oracle dispatch by dispatch only.
+GOLDEN_SCENARIOS = {'single_cell': True, 'squall_line': True, 'supercell_stretched': False}
+
+
+@pytest.mark.parametrize('scen', list(GOLDEN_SCENARIOS))
+def test_golden_in_scope_dispatches(scen):
+    """A recorded step 1: every dispatch with a CUDA kernel runs on the GPU (the others on
+    the CPU reference build), its region hashes equal to the oracle's; where the oracle
+    reproduces the recording, region hashes and buffer FNVs are also compared with the
+    recording (scratch tend/fpk hashes exempt, as the reference documents)."""
     ref = helpers.reference()
     if ref is None:
         pytest.skip('oracle/_ref not built')
     from oracle.player import CpuPlayer, fnv1a
-    tape, init, want, step1 = helpers.load_golden_scenario()
+    tape, init, want, step1 = helpers.load_golden_scenario(scen)
     km = helpers.kernels_meta()
     cpu = CpuPlayer(tape, km)
     cpu.plan(True)
@@ -156,7 +167,10 @@ def test_golden_single_cell_in_scope_dispatches():
                 dirty.append((o.dst, o.n))
             else:
                 dirty.extend((off, ln) for _, off, ln in o.hashes if off is not None and ln)
-    assert ngpu >= 713   # 715 of the 718: all but the Morrison microphysics column
+    # every dispatch but the Morrison microphysics column (morr_prep, morr_column, morr_post)
+    assert ngpu == sum(1 for o in cpu.ops if o.kind == 'k') - 3
+    if not GOLDEN_SCENARIOS[scen]:
+        return
     fields = {v // 4 + cpu.base[2]: k for k, v in tape['fields'].items()}
     slot_field = {s: fields.get(off) for o in cpu.ops if o.kind == 'k' for s, off, _ in o.hashes}
     bad = [s for s in gpu_hashes if gpu_hashes[s] != int(want[s])]
