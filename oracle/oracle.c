@@ -2537,3 +2537,43 @@ void teor_mass_correction_apply(uint32_t *M, const uint32_t *ARG) {
     rho[c] = DCR(p, (th * pi) * rmix);
   }
 }
+
+void teor_morr_prep(uint32_t *M, const uint32_t *ARG) {
+  /* morr_prep.wgsl main: temperature T = (th0 + th) (pi0 + pp) and a copy qv0 of qv before
+   * the microphysics column */
+  Dims g = dims_at(M, B(0));
+  const float *th0 = FPTR(1), *pi0 = FPTR(2), *th = FPTR(3), *pp = FPTR(4), *qv = FPTR(5);
+  float *T = FPTR(6), *qv0 = FPTR(7);
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    T[c] = (th0[k] + th[c]) * (pi0[k] + pp[c]);
+    qv0[c] = qv[c];
+  }
+}
+
+void teor_morr_post(uint32_t *M, const uint32_t *ARG) {
+  /* morr_post.wgsl main: where the column changed T (by >= 1e-4) or qv (by >= 1e-14),
+   * pressure from the equation of state, pi' from it (the reference's correctly rounded
+   * pow) and th from T and the new pi */
+  Dims g = dims_at(M, B(0));
+  const float *th0 = FPTR(1), *pi0 = FPTR(2), *rho = FPTR(3), *T = FPTR(4), *qv0 = FPTR(5), *qv = FPTR(6);
+  float *th = FPTR(7), *pp = FPTR(8), *prs = FPTR(9);
+  const float rd = 287.04f, cp = 1005.7f, rv = 461.5f;
+  FOR_GRID {
+    int i = (int)tx, j = (int)ty, k = (int)tz;
+    if (i >= g.nx || j >= g.ny || k >= g.nz) continue;
+    int c = GIDX(g, i, j, k);
+    float rp00 = DCR(1.0f, 1e+05f), rovcp = DCR(rd, cp);
+    float told = (th0[k] + th[c]) * (pi0[k] + pp[c]);
+    float t = T[c], q = qv[c];
+    if (fabsf(t - told) >= 0.0001f || fabsf(q - qv0[c]) >= 1e-14f) {
+      float p = (rho[c] * fmaf(rv, q, rd)) * t;
+      float ppn = te_rr_pow_cr(p * rp00, rovcp) - pi0[k];
+      prs[c] = p;
+      pp[c] = ppn;
+      th[c] = DCR(t, pi0[k] + ppn) - th0[k];
+    }
+  }
+}

@@ -53,7 +53,8 @@ float te_log_f64(float x);
   X(turb_gettau) X(turb_km_kh) X(tke_epst) \
   X(turb_nm) X(turb_sfcstress) X(turb_dissipative_heating) \
   X(turb_u_tendency) X(turb_v_tendency) X(turb_w_tendency) X(tke_transport) \
-  X(mass_row_sums) X(mass_level_sums) X(mass_reference_init) X(mass_correction_apply)
+  X(mass_row_sums) X(mass_level_sums) X(mass_reference_init) X(mass_correction_apply) \
+  X(morr_prep) X(morr_post)
 TE_ORACLE_KERNELS(TE_ORACLE_KERNEL)
 
 #ifdef __cplusplus

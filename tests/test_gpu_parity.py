@@ -167,8 +167,8 @@ def test_golden_in_scope_dispatches(scen):
                 dirty.append((o.dst, o.n))
             else:
                 dirty.extend((off, ln) for _, off, ln in o.hashes if off is not None and ln)
-    # every dispatch but the Morrison microphysics column (morr_prep, morr_column, morr_post)
-    assert ngpu == sum(1 for o in cpu.ops if o.kind == 'k') - 3
+    # every dispatch but the Morrison microphysics column (morr_column)
+    assert ngpu == sum(1 for o in cpu.ops if o.kind == 'k') - 1
     if not GOLDEN_SCENARIOS[scen]:
         return
     fields = {v // 4 + cpu.base[2]: k for k, v in tape['fields'].items()}

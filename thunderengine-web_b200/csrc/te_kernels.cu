@@ -1776,6 +1776,42 @@ __global__ void k_mass_correction_apply(KArgs A) {
 }
 TE_LAUNCH3(mass_correction_apply)
 
+// morr_prep.wgsl: temperature T = (th0 + th)(pi0 + pp) and a copy qv0 of qv before the
+// microphysics column
+__global__ void k_morr_prep(KArgs A) {
+  TE_K3
+  const int i = tx, j = ty, k = tz;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  const int c = gidx(g, i, j, k);
+  A.p[6][c] = (A.p[1][k] + A.p[3][c]) * (A.p[2][k] + A.p[4][c]);
+  A.p[7][c] = A.p[5][c];
+}
+TE_LAUNCH3(morr_prep)
+
+// morr_post.wgsl: where the column changed T (by >= 1e-4) or qv (by >= 1e-14), pressure
+// from the equation of state, pi' from it (the reference's correctly rounded pow) and th
+__global__ void k_morr_post(KArgs A) {
+  TE_K3
+  const int i = tx, j = ty, k = tz;
+  if (i >= g.nx || j >= g.ny || k >= g.nz) return;
+  const float *TE_R th0 = A.p[1], *TE_R pi0 = A.p[2], *TE_R rho = A.p[3], *TE_R T = A.p[4], *TE_R qv0 = A.p[5];
+  const float* TE_R qv = A.p[6];
+  float *TE_R th = A.p[7], *TE_R pp = A.p[8], *TE_R prs = A.p[9];
+  const float rd = 287.04f, cp = 1005.7f, rv = 461.5f;
+  const int c = gidx(g, i, j, k);
+  const float rp00 = dcr(1.0f, 1e+05f), rovcp = dcr(rd, cp);
+  const float told = (th0[k] + th[c]) * (pi0[k] + pp[c]);
+  const float t = T[c], q = qv[c];
+  if (fabsf(t - told) >= 0.0001f || fabsf(q - qv0[c]) >= 1e-14f) {
+    const float p = (rho[c] * fmaf(rv, q, rd)) * t;
+    const float ppn = rr_pow_cr(p * rp00, rovcp) - pi0[k];
+    prs[c] = p;
+    pp[c] = ppn;
+    th[c] = dcr(t, pi0[k] + ppn) - th0[k];
+  }
+}
+TE_LAUNCH3(morr_post)
+
 // -------------------------------------------------- thermodynamic glue
 
 __global__ void k_update_diagnostics_moist(KArgs A) {
@@ -2262,6 +2298,20 @@ struct OpPdefDum {
   }
 };
 
+struct OpMorrPrep {
+  struct In { float th, pp, qv; };
+  TE_OP_INTERIOR
+  static __device__ __forceinline__ In load(const KArgs& A, int tx, int ty, int tz) {
+    TE_OP_C(0);
+    return In{A.p[3][c], A.p[4][c], A.p[5][c]};
+  }
+  static __device__ __forceinline__ void store(const KArgs& A, int tx, int ty, int tz, const In& v) {
+    TE_OP_C(0);
+    A.p[6][c] = (A.p[1][k] + v.th) * (A.p[2][k] + v.pp);
+    A.p[7][c] = v.qv;
+  }
+};
+
 // the __restrict__ build launches the row-vector form where a kernel has one
 #ifdef TE_KERNELS_FAST
 #define TE_ROWVEC(name, op) launch_rowvec<op>
@@ -2347,6 +2397,8 @@ static const KernelSpec kTable[] = {
     {"mass_level_sums", 5, {R(0), P(1), P(2), W(3), W(4)}, false, launch_mass_level_sums},
     {"mass_reference_init", 3, {R(0), P(1), W(2)}, false, launch_mass_reference_init},
     {"mass_correction_apply", 13, {R(0), R(1), P(2), P(3), P(4), P(5), W(6), P(7), P(8), P(9), W(10), W(11), W(12)}, false, launch_mass_correction_apply},
+    {"morr_prep", 8, {R(0), P(1), P(2), P(3), P(4), P(5), W(6), W(7)}, false, TE_ROWVEC(morr_prep, OpMorrPrep)},
+    {"morr_post", 10, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), W(7), W(8), W(9)}, false, launch_morr_post},
     {"update_diagnostics_moist", 20, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), P(11), P(12),
                                       P(13), P(14), W(15), W(16), W(17), W(18), W(19)}, false, TE_ROWVEC(update_diagnostics_moist, OpUpdateDiagnosticsMoist)},
     {"pressure_tendency", 15, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), R(9), R(10), R(12), P(13), R(14), W(11)},
