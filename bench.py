@@ -429,32 +429,61 @@ def dispatch_bytes(d, km, nz):
     return sum(fields.values()) * 4 * pts
 
 
+def step_inputs(rep, run, init, state):
+    """The arena fields one step reads before it writes them (its inputs), found with this
+    library's own kernels: each non-scratch field in turn is filled with seeded garbage
+    before one step from the initial state; a field whose garbage leaves every
+    non-scratch field after the step bit-identical is fully rewritten before any read.
+    Returns (inputs, the non-scratch fields after one step from the initial state)."""
+    g = run.grid
+    aid = run.rec.ids['arena']
+    base = rep.base[aid]
+    rng = np.random.default_rng(11)
+
+    def one_step(poison=None):
+        for i, buf in init.items():
+            rep.upload(i, buf)
+        if poison is not None:
+            junk = rng.uniform(-3.0, 3.0, g.count).astype(np.float32).view(np.uint32)
+            rep.write_words(base + run.fields[poison] // 4, junk)
+        rep.encode_steps(1)
+        rep.sync()
+        return {n: rep.read(g.count, base + run.fields[n] // 4) for n in state}
+
+    want = one_step()
+    inputs = [n for n in state if any(not np.array_equal(v, want[m]) for m, v in one_step(n).items())]
+    return inputs, want
+
+
 def end_to_end(r, run, init, cfg, a, world, mode, dev):
-    """The same metric through the public API with host buffers.  Every step uploads every
-    non-scratch field of the arena (33 here) from pinned host memory, plays the step and reads
-    th, qv, u, v, w, pp3d back into pinned memory.  Two replicas (the context of the
-    timed run and a second one on its own stream) take the steps in turn, so one
-    replica's copies overlap the other's step (te_write_words_async / te_read_async);
-    the serial figure (one context, blocking copies) is reported beside it."""
+    """The same metric through the public API with host buffers.  Every step uploads the
+    step's inputs (the arena fields it reads before writing, step_inputs) from pinned host
+    memory, plays the step and reads th, qv, u, v, w, pp3d back into pinned memory.  Two
+    replicas (the context of the timed run and a second one on its own stream) take the
+    steps in turn, so one replica's copies overlap the other's step (te_write_words_async /
+    te_read_async); the serial figure (one context, blocking copies) is reported beside it.
+    The fields read back after the timed steps are checked bit for bit against a step whose
+    every non-scratch field was uploaded."""
     import torch
     from thunderengine_web_b200.replayer import Replayer
     from thunderengine_web_b200.timestep import SCRATCH_FIELDS
     g = run.grid
     aid = run.rec.ids['arena']
     arena0 = np.frombuffer(init[aid], dtype=np.uint32)
-    state = [n for n in run.fields if n not in SCRATCH_FIELDS]
+    nonscratch = [n for n in run.fields if n not in SCRATCH_FIELDS]
     outs = ['th', 'qv', 'u', 'v', 'w', 'pp3d']
-    pin_in = torch.empty((len(state), g.count), dtype=torch.int32).pin_memory()
-    for q, n in enumerate(state):
-        o = run.fields[n] // 4
-        pin_in[q].numpy()[:] = arena0[o:o + g.count].view(np.int32)
     lib = r.lib
     r2 = Replayer(run.tape(1), None, device=dev)
     r2.plan(False)
     r2.build()
+    r2.set_mode(mode)
+    state, want = step_inputs(r2, run, init, nonscratch)
     for i, buf in init.items():
         r2.upload(i, buf)
-    r2.set_mode(mode)
+    pin_in = torch.empty((len(state), g.count), dtype=torch.int32).pin_memory()
+    for q, n in enumerate(state):
+        o = run.fields[n] // 4
+        pin_in[q].numpy()[:] = arena0[o:o + g.count].view(np.int32)
     s2 = torch.cuda.Stream(device=dev)
     r2.set_stream(s2.cuda_stream)
     reps = [(r, torch.empty((len(outs), g.count), dtype=torch.int32).pin_memory()),
@@ -493,15 +522,22 @@ def end_to_end(r, run, init, cfg, a, world, mode, dev):
         return max_over_ranks(time.perf_counter() - t0, world)
 
     dt = timed(step_async, steps)
+    verified = all(np.array_equal(pout[q].numpy().view(np.uint32), want[n]) for _, pout in reps for q, n in enumerate(outs))
     dt_serial = timed(step_serial, steps)
+    verified = verified and all(np.array_equal(pout[q].numpy().view(np.uint32), want[n])
+                                for _, pout in reps for q, n in enumerate(outs))
     barrier(world)
     r2.close()
+    if not verified:
+        raise RuntimeError('end-to-end steps did not reproduce the full-upload step')
     return {'value': pts * steps * world / dt, 'unit': METRIC, 'h2d_bytes_per_step': len(state) * g.count * 4,
             'd2h_bytes_per_step': len(outs) * g.count * 4, 'steps': steps,
             'serial_value': pts * steps * world / dt_serial,
-            'path': 'per step: Replayer write_words_async of each non-scratch field (pinned host) -> encode_steps(1) -> read_async x6 '
-                    '(pinned host); two replicas alternate steps so copies overlap the other replica\'s step; '
-                    'serial_value: one context at a time with blocking copies'}
+            'inputs': state, 'verified': True,
+            'path': 'per step: Replayer write_words_async of each input field of the step (pinned host) -> '
+                    'encode_steps(1) -> read_async x6 (pinned host); two replicas alternate steps so copies overlap '
+                    'the other replica\'s step; serial_value: one context at a time with blocking copies; the read-back '
+                    'fields equal those of a step with every non-scratch field uploaded'}
 
 
 # -------------------------------------------------------- reference arm (CPU)

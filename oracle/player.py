@@ -161,7 +161,17 @@ class CpuPlayer:
         self.scratch_base = top
         top += math.ceil(self.scratch_need / ALIGN) * ALIGN
         self.mem_words = top
-        self.M = np.zeros(self.mem_words, dtype=np.uint32)
+        # The reference runs a dispatch whose per-thread scratch would pass SCRATCH_CAP in
+        # y tiles that share the planned scratch (replay.js:23-29, 104-109, 272-274); the C
+        # kernels here run the whole grid at once, so the host array carries the scratch of
+        # every thread past mem_words (the layout, mem_words and all hashed regions are
+        # the reference's).
+        full = self.mem_words
+        for o in self.ops + self.diag_ops:
+            scr = (self.kmeta.get(o.name) or {}).get('scratch') or 0 if o.kind == 'k' else 0
+            if scr:
+                full = max(full, self.scratch_base + scr * o.grid[0] * o.grid[1] * o.grid[2])
+        self.M = np.zeros(full, dtype=np.uint32)
         for off, data in self.bytes:
             self.write_words(off, data)
         self.hashes = np.zeros(max(self.hash_count, 1), dtype=np.uint32)
