@@ -84,10 +84,21 @@ static inline f32 W_sqrt(f32 a) { return sqrtf(a); }
 static inline f32 W_floor(f32 a) { return floorf(a); }
 static inline f32 W_round(f32 a) { return nearbyintf(a); }
 static inline f32 W_trunc(f32 a) { return truncf(a); }
+#ifdef TE_REF_F64_BUILTINS
+// WGSL leaves the precision of exp/log/pow to the implementation: this variant evaluates
+// them like the CUDA kernels (binary64, rounded once; oracle.c te_*_f64)
+extern "C" float te_exp_f64(float x);
+extern "C" float te_log_f64(float x);
+extern "C" float te_pow_f64(float x, float y);
+static inline f32 W_exp(f32 a) { return te_exp_f64(a); }
+static inline f32 W_log(f32 a) { return te_log_f64(a); }
+static inline f32 W_pow(f32 a, f32 b) { return te_pow_f64(a, b); }
+#else
 static inline f32 W_exp(f32 a) { return expf(a); }
 static inline f32 W_log(f32 a) { return logf(a); }
-static inline f32 W_log2(f32 a) { return log2f(a); }
 static inline f32 W_pow(f32 a, f32 b) { return powf(a, b); }
+#endif
+static inline f32 W_log2(f32 a) { return log2f(a); }
 static inline f32 W_sin(f32 a) { return sinf(a); }
 static inline f32 W_atan(f32 a) { return atanf(a); }
 static inline f32 W_atan2(f32 a, f32 b) { return atan2f(a, b); }

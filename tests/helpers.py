@@ -10,6 +10,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(ROOT, 'tests', 'golden')
 ORACLE_SO = os.path.join(ROOT, 'oracle', 'liboracle.so')
 REF_SO = os.path.join(ROOT, 'oracle', '_ref', 'libteref.so')
+REF64_SO = os.path.join(ROOT, 'oracle', '_ref', 'libteref64.so')
 
 # Scratch fields of a step (timestep.js:334-337 Fields.scratchFields): their contents
 # between dispatches are not part of the step's result.
@@ -18,6 +19,7 @@ SCRATCH = ['rru', 'rrv', 'rrw', 'fx', 'fy', 'fz', 'tend', 'divx', 'qk', 'pk1', '
 
 _ORACLE = None
 _REF = None
+_REF64 = None
 
 
 def oracle():
@@ -47,6 +49,19 @@ def reference():
 def kernels_meta():
     with open(os.path.join(GOLDEN, 'kernels.json')) as fh:
         return json.load(fh)
+
+
+def reference64():
+    """The reference's kernels that call WGSL exp/log/pow, with those evaluated in binary64
+    like the CUDA kernels (oracle/_ref/libteref64.so), or None."""
+    global _REF64
+    if _REF64 is None:
+        if not os.path.exists(REF64_SO):
+            return None
+        oracle()
+        from oracle.player import KernelSet
+        _REF64 = KernelSet(REF64_SO, 'teref_')
+    return _REF64
 
 
 def mixed(name):
