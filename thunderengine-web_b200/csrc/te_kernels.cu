@@ -38,7 +38,7 @@ namespace fast {
 static void launch3(void (*k)(KArgs), const KArgs& A, cudaStream_t s) {
   dim3 b(32, 4, 1);
   dim3 gr((A.gx + 31) / 32, (A.gy + 3) / 4, A.gz);
-  k<<<gr, b, 0, s>>>(A);
+  launch_pdl(k, dim3(gr), dim3(b), 0, s, A);
 }
 
 #define TE_LAUNCH3(name) \
@@ -49,7 +49,7 @@ static void launch3(void (*k)(KArgs), const KArgs& A, cudaStream_t s) {
 static void launch_halo3(void (*k)(KArgs), const KArgs& A, cudaStream_t s) {
   dim3 b(4, 64, 1);
   dim3 gr((A.gx + 3) / 4, (A.gy + 63) / 64, A.gz);
-  k<<<gr, b, 0, s>>>(A);
+  launch_pdl(k, dim3(gr), dim3(b), 0, s, A);
 }
 #define TE_LAUNCH_HALO(name) \
   static void launch_##name(const KArgs& A, cudaStream_t s) { launch_halo3(k_##name, A, s); }
@@ -64,6 +64,7 @@ enum { kRowVec = 4 };
 
 template <class Op>
 __global__ void __launch_bounds__(128) k_rowvec(KArgs A) {
+  grid_dep_wait();
   const int tx = blockIdx.x * blockDim.x + threadIdx.x;
   const int ty = blockIdx.y * blockDim.y + threadIdx.y;
   const int tz0 = blockIdx.z * kRowVec;
@@ -84,7 +85,7 @@ template <class Op>
 static void launch_rowvec(const KArgs& A, cudaStream_t s) {
   dim3 b(32, 4, 1);
   dim3 gr((A.gx + 31) / 32, (A.gy + 3) / 4, (A.gz + kRowVec - 1) / kRowVec);
-  k_rowvec<Op><<<gr, b, 0, s>>>(A);
+  launch_pdl(k_rowvec<Op>, dim3(gr), dim3(b), 0, s, A);
 }
 
 // ------------------------------------------------------------------ fluxes
@@ -94,6 +95,7 @@ static void launch_rowvec(const KArgs& A, cudaStream_t s) {
 // adv_flux_x / adv_flux_y: f = rr * flx5(upwind stencil)
 template <int DIR>
 __global__ void k_flux_lin_h(KArgs A) {
+  grid_dep_wait();
   TE_K3
   int i = tx, j = ty, k = tz;
   if (DIR == 0 ? (i > g.nx || j >= g.ny || k >= g.nz) : (i >= g.nx || j > g.ny || k >= g.nz)) return;
@@ -103,6 +105,7 @@ static void launch_adv_flux_x(const KArgs& A, cudaStream_t s) { launch3(k_flux_l
 static void launch_adv_flux_y(const KArgs& A, cudaStream_t s) { launch3(k_flux_lin_h<1>, A, s); }
 
 __global__ void k_adv_flux_z(KArgs A) {
+  grid_dep_wait();
   TE_K3
   int i = tx, j = ty, k = tz;
   if (i >= g.nx || j >= g.ny || k > g.nz) return;
@@ -114,6 +117,7 @@ TE_LAUNCH3(adv_flux_z)
 // adv_flux_x_stag / adv_flux_y_stag (momentum, RK stages 1-2)
 template <int DIR>
 __global__ void k_flux_stag_h(KArgs A) {
+  grid_dep_wait();
   TE_K3
   int i = tx - 1, j = ty - 1, k = tz;
   if (i > g.nx || j > g.ny || k >= g.nz) return;
@@ -123,6 +127,7 @@ static void launch_adv_flux_x_stag(const KArgs& A, cudaStream_t s) { launch3(k_f
 static void launch_adv_flux_y_stag(const KArgs& A, cudaStream_t s) { launch3(k_flux_stag_h<1>, A, s); }
 
 __global__ void k_adv_flux_z_stag(KArgs A) {
+  grid_dep_wait();
   TE_K3
   int i = tx, j = ty, k = tz;
   if (i > g.nx || j > g.ny || k > g.nz) return;
@@ -133,6 +138,7 @@ TE_LAUNCH3(adv_flux_z_stag)
 // adv_flux_x_weno / adv_flux_y_weno (scalars, positive-definite gate)
 template <int DIR>
 __global__ void k_flux_weno_h(KArgs A) {
+  grid_dep_wait();
   TE_K3
   int i = tx, j = ty, k = tz;
   if (DIR == 0 ? (i > g.nx || j >= g.ny || k >= g.nz) : (i >= g.nx || j > g.ny || k >= g.nz)) return;
@@ -142,6 +148,7 @@ static void launch_adv_flux_x_weno(const KArgs& A, cudaStream_t s) { launch3(k_f
 static void launch_adv_flux_y_weno(const KArgs& A, cudaStream_t s) { launch3(k_flux_weno_h<1>, A, s); }
 
 __global__ void k_adv_flux_z_weno(KArgs A) {
+  grid_dep_wait();
   TE_K3
   int i = tx, j = ty, k = tz;
   if (i >= g.nx || j >= g.ny || k > g.nz) return;
@@ -153,6 +160,7 @@ TE_LAUNCH3(adv_flux_z_weno)
 // adv_flux_x_weno_uv / adv_flux_y_weno_uv (u, v momentum, RK stage 3)
 template <int DIR>
 __global__ void k_flux_weno_uv_h(KArgs A) {
+  grid_dep_wait();
   TE_K3
   int i = tx - 1, j = ty - 1, k = tz;
   if (i > g.nx || j > g.ny || k >= g.nz) return;
@@ -162,6 +170,7 @@ static void launch_adv_flux_x_weno_uv(const KArgs& A, cudaStream_t s) { launch3(
 static void launch_adv_flux_y_weno_uv(const KArgs& A, cudaStream_t s) { launch3(k_flux_weno_uv_h<1>, A, s); }
 
 __global__ void k_adv_flux_z_weno_uv(KArgs A) {
+  grid_dep_wait();
   TE_K3
   int i = tx, j = ty, k = tz;
   if (i > g.nx || j > g.ny || k > g.nz) return;
@@ -172,6 +181,7 @@ TE_LAUNCH3(adv_flux_z_weno_uv)
 // adv_flux_x_weno_w / adv_flux_y_weno_w (w momentum, RK stage 3)
 template <int DIR>
 __global__ void k_flux_weno_w_h(KArgs A) {
+  grid_dep_wait();
   TE_K3
   int i = tx - 1, j = ty - 1, k = tz;
   if (i < 0 || j < 0 || i > g.nx || j > g.ny || k >= g.nz) return;
@@ -181,6 +191,7 @@ static void launch_adv_flux_x_weno_w(const KArgs& A, cudaStream_t s) { launch3(k
 static void launch_adv_flux_y_weno_w(const KArgs& A, cudaStream_t s) { launch3(k_flux_weno_w_h<1>, A, s); }
 
 __global__ void k_adv_flux_z_weno_w(KArgs A) {
+  grid_dep_wait();
   TE_K3
   int i = tx, j = ty, k = tz;
   if (i > g.nx || j > g.ny || k > g.nz) return;
@@ -191,6 +202,7 @@ TE_LAUNCH3(adv_flux_z_weno_w)
 // ------------------------------------------------------------ assembly
 
 __global__ void k_adv_assemble(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const int stag = A.iv[1];
   const float *TE_R fx = A.p[3], *TE_R fy = A.p[4], *TE_R fz = A.p[5];
@@ -215,6 +227,7 @@ __global__ void k_adv_assemble(KArgs A) {
 TE_LAUNCH3(adv_assemble)
 
 __global__ void k_rk_update(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const int stag = A.iv[1];
   const float *TE_R phiA = A.p[2], *TE_R tend = A.p[3];
@@ -241,6 +254,7 @@ __device__ __forceinline__ bool pdef_inflow(const Dims& g, int dir, int i, int j
 }
 
 __global__ void k_pdef_dum(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const int dir = A.iv[1];
   const float *TE_R s = A.p[2], *TE_R s0 = A.p[3], *TE_R f = A.p[4], *TE_R rr = A.p[5], *TE_R rho0 = A.p[6], *TE_R mh = A.p[7];
@@ -295,6 +309,7 @@ __device__ __forceinline__ float pdef_mass(float dm2, float dm1, float d0, float
 }
 
 __global__ void k_pdef_apply(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const float *TE_R s = A.p[1], *TE_R s0 = A.p[2], *TE_R fx = A.p[3], *TE_R fy = A.p[4], *TE_R fz = A.p[5];
   const float *TE_R rru = A.p[6], *TE_R rrv = A.p[7], *TE_R rrw = A.p[8], *TE_R dumx = A.p[9], *TE_R dumy = A.p[10], *TE_R dumz = A.p[11];
@@ -348,6 +363,7 @@ TE_LAUNCH3(pdef_apply)
   int c = gidx(g, i, j, k);
 
 __global__ void k_build_sadv(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const float *TE_R th0 = A.p[1], *TE_R thp = A.p[2];
   float* TE_R sadv = A.p[3];
@@ -357,6 +373,7 @@ __global__ void k_build_sadv(KArgs A) {
 TE_LAUNCH3(build_sadv)
 
 __global__ void k_massflux_from_state(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const float *TE_R u = A.p[1], *TE_R v = A.p[2], *TE_R w = A.p[3], *TE_R rho0 = A.p[4], *TE_R rf0 = A.p[5];
   float *TE_R rru = A.p[6], *TE_R rrv = A.p[7], *TE_R rrw = A.p[8];
@@ -370,6 +387,7 @@ __global__ void k_massflux_from_state(KArgs A) {
 TE_LAUNCH3(massflux_from_state)
 
 __global__ void k_div_massflux(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const float *TE_R rru = A.p[1], *TE_R rrv = A.p[2], *TE_R rrw = A.p[3], *TE_R mh = A.p[4];
   float* TE_R divx = A.p[5];
@@ -407,6 +425,7 @@ struct OpDivMassflux {  // div_massflux as a row-vector op (same operations)
 };
 
 __global__ void k_velocity_to_massflux(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const float *TE_R rho0 = A.p[1], *TE_R rf0 = A.p[2];
   float *TE_R rru = A.p[3], *TE_R rrv = A.p[4], *TE_R rrw = A.p[5];
@@ -446,6 +465,7 @@ struct OpVelocityToMassflux {  // velocity_to_massflux as a row-vector op
 };
 
 __global__ void k_stage_state_reset(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const float *TE_R ua = A.p[1], *TE_R va = A.p[2], *TE_R wa = A.p[3], *TE_R ppi = A.p[4];
   float *TE_R u = A.p[5], *TE_R v = A.p[6], *TE_R w = A.p[7], *TE_R pp3d = A.p[8], *TE_R ppd = A.p[9];
@@ -460,6 +480,7 @@ __global__ void k_stage_state_reset(KArgs A) {
 TE_LAUNCH3(stage_state_reset)
 
 __global__ void k_stage_tendency_reset(KArgs A) {
+  grid_dep_wait();
   TE_K3
   float *TE_R uten = A.p[1], *TE_R vten = A.p[2], *TE_R wten = A.p[3];
   TE_WHOLE(k <= g.nz)
@@ -470,6 +491,7 @@ __global__ void k_stage_tendency_reset(KArgs A) {
 TE_LAUNCH3(stage_tendency_reset)
 
 __global__ void k_buoyancy_apply(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const float *TE_R buoy = A.p[1], *TE_R c1 = A.p[2], *TE_R c2 = A.p[3];
   float* TE_R wten = A.p[4];
@@ -482,6 +504,7 @@ __global__ void k_buoyancy_apply(KArgs A) {
 TE_LAUNCH3(buoyancy_apply)
 
 __global__ void k_apply_thterm(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const float *TE_R div = A.p[1], *TE_R thterm = A.p[2];
   float* TE_R tend = A.p[3];
@@ -495,6 +518,7 @@ TE_LAUNCH3(apply_thterm)
 // ------------------------------------------------------ acoustic substep
 
 __global__ void k_acoustic_prepare(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const Acoustic a = A.a;
   const float *TE_R ppterm = A.p[2], *TE_R piadv = A.p[3], *TE_R thv = A.p[4], *TE_R rr0 = A.p[5], *TE_R rf0 = A.p[6];
@@ -524,6 +548,7 @@ __global__ void k_acoustic_prepare(KArgs A) {
 TE_LAUNCH3(acoustic_prepare)
 
 __global__ void k_acoustic_begin(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const float* TE_R w = A.p[2];
   float *TE_R rru = A.p[3], *TE_R rrv = A.p[4], *TE_R rrw = A.p[5];
@@ -535,6 +560,7 @@ __global__ void k_acoustic_begin(KArgs A) {
 TE_LAUNCH3(acoustic_begin)
 
 __global__ void k_acoustic_uv(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const Acoustic a = A.a;
   const float *TE_R ppd = A.p[2], *TE_R thv = A.p[3], *TE_R uten = A.p[4], *TE_R vten = A.p[5];
@@ -556,6 +582,7 @@ __global__ void k_acoustic_uv(KArgs A) {
 TE_LAUNCH3(acoustic_uv)
 
 __global__ void k_acoustic_fpk(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const Acoustic a = A.a;
   const float *TE_R u = A.p[2], *TE_R v = A.p[3], *TE_R w = A.p[4], *TE_R piadv = A.p[5], *TE_R ppten = A.p[6], *TE_R ppterm = A.p[7];
@@ -579,6 +606,7 @@ TE_LAUNCH3(acoustic_fpk)
 // Vertically implicit w-pi' solve: one column per thread, columns of a warp adjacent
 // in i (coalesced), the Thomas recurrence sequential in k as in the reference.
 __global__ void k_acoustic_w_solve(KArgs A) {
+  grid_dep_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const Dims& g = A.g;
@@ -629,10 +657,11 @@ __global__ void k_acoustic_w_solve(KArgs A) {
 static void launch_acoustic_w_solve(const KArgs& A, cudaStream_t s) {
   dim3 b(32, 4, 1);
   dim3 gr((A.gx + 31) / 32, (A.gy + 3) / 4, 1);
-  k_acoustic_w_solve<<<gr, b, 0, s>>>(A);
+  launch_pdl(k_acoustic_w_solve, dim3(gr), dim3(b), 0, s, A);
 }
 
 __global__ void k_acoustic_pp(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const Acoustic a = A.a;
   const float *TE_R w = A.p[2], *TE_R pk1 = A.p[3], *TE_R pk2 = A.p[4], *TE_R qk = A.p[5], *TE_R fpk = A.p[6];
@@ -653,6 +682,7 @@ __global__ void k_acoustic_pp(KArgs A) {
 TE_LAUNCH3(acoustic_pp)
 
 __global__ void k_acoustic_accumulate(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const float *TE_R u = A.p[2], *TE_R v = A.p[3], *TE_R w = A.p[4];
   float *TE_R rru = A.p[5], *TE_R rrv = A.p[6], *TE_R rrw = A.p[7];
@@ -673,6 +703,7 @@ TE_LAUNCH3(acoustic_accumulate)
 // ------------------------------------------------------- periodic halos
 
 __global__ void k_bc_periodic_x(KArgs A) {
+  grid_dep_wait();
   TE_K3
   float* TE_R f = A.p[1];
   int h = tx, jj = ty - 3, k = tz;
@@ -685,6 +716,7 @@ __global__ void k_bc_periodic_x(KArgs A) {
 TE_LAUNCH_HALO(bc_periodic_x)
 
 __global__ void k_bc_periodic_y(KArgs A) {
+  grid_dep_wait();
   TE_K3
   float* TE_R f = A.p[1];
   int h = tx, i = ty - 3, k = tz;
@@ -701,6 +733,7 @@ TE_LAUNCH_HALO(bc_periodic_y)
 // bc_open_x.wgsl / bc_open_y.wgsl: zero-gradient halos, -1-h <- 0 and last+1+h <- last
 // (h < 3, last = n + stagger - 1)
 __global__ void k_bc_open_x(KArgs A) {
+  grid_dep_wait();
   TE_K3
   float* TE_R f = A.p[1];
   const int stagX = A.iv[2];
@@ -713,6 +746,7 @@ __global__ void k_bc_open_x(KArgs A) {
 TE_LAUNCH_HALO(bc_open_x)
 
 __global__ void k_bc_open_y(KArgs A) {
+  grid_dep_wait();
   TE_K3
   float* TE_R f = A.p[1];
   const int stagY = A.iv[2];
@@ -736,6 +770,7 @@ __device__ __forceinline__ float radbc_speed(float dx, float a, float b, float f
 // the west (i = 1) and east (i = nx - 1) faces.  One thread per row; the level loop is
 // sequential as in the reference (the sum's rounding order).
 __global__ void k_radbc_ew(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const float *TE_R ua = A.p[1], *TE_R u3d = A.p[2], *TE_R hm = A.p[30];
   const float dt = A.f[3];
@@ -765,6 +800,7 @@ TE_LAUNCH3(radbc_ew)
 
 // radbc_ns.wgsl: the same for v at the south (j = 1) and north (j = ny - 1) faces
 __global__ void k_radbc_ns(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const float *TE_R va = A.p[1], *TE_R v3d = A.p[2], *TE_R hm = A.p[30];
   const float dt = A.f[3];
@@ -795,6 +831,7 @@ TE_LAUNCH3(radbc_ns)
 // openbc_uv_tendency.wgsl: on open x boundaries the u faces i = 0 and i = nx, on open y
 // boundaries the v faces j = 0 and j = ny, advance by the radiation term
 __global__ void k_openbc_uv_tendency(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const Acoustic a = A.a;
   const float *TE_R radbcw = A.p[2], *TE_R radbce = A.p[3], *TE_R radbcs = A.p[4], *TE_R radbcn = A.p[5];
@@ -825,6 +862,7 @@ TE_LAUNCH3(openbc_uv_tendency)
 // turb_zero.wgsl: zero f[i + strideJ (j + strideK k)] for i < strideJ, j < strideK and
 // k <= nz + 1 (the reference's range, one level above a field's nz + 1)
 __global__ void k_turb_zero(KArgs A) {
+  grid_dep_wait();
   TE_K3
   float* TE_R f = A.p[1];
   if (tx >= g.sJ || ty >= g.sK || tz > g.nz + 1) return;
@@ -834,6 +872,7 @@ TE_LAUNCH3(turb_zero)
 
 // turb_add_tendency.wgsl: dst = fma(scale, src, dst) over the whole field
 __global__ void k_turb_add_tendency(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const float* TE_R src = A.p[1];
   float* TE_R dst = A.p[2];
@@ -844,6 +883,7 @@ TE_LAUNCH3(turb_add_tendency)
 
 // turb_scalar_flux_h.wgsl: horizontal subgrid scalar fluxes at the x and y faces
 __global__ void k_turb_scalar_flux_h(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const float *TE_R s = A.p[1], *TE_R rho = A.p[2], *TE_R khh = A.p[3], *TE_R hm = A.p[30];
   const float leNum = A.f[4];
@@ -860,6 +900,7 @@ TE_LAUNCH3(turb_scalar_flux_h)
 
 // turb_openbc_flux.wgsl: edge fluxes copy their inner neighbours on open boundaries
 __global__ void k_turb_openbc_flux(KArgs A) {
+  grid_dep_wait();
   TE_K3
   float *TE_R fx = A.p[1], *TE_R fy = A.p[2];
   const int openx = A.iv[3], openy = A.iv2[3];
@@ -878,6 +919,7 @@ TE_LAUNCH3(turb_openbc_flux)
 
 // turb_openbc_stress_x.wgsl / _y.wgsl: edge stresses copy their inner neighbours
 __global__ void k_turb_openbc_stress_x(KArgs A) {
+  grid_dep_wait();
   TE_K3
   float *TE_R s11 = A.p[1], *TE_R s12 = A.p[2];
   const int j = tx - 1, k = ty;
@@ -892,6 +934,7 @@ __global__ void k_turb_openbc_stress_x(KArgs A) {
 TE_LAUNCH3(turb_openbc_stress_x)
 
 __global__ void k_turb_openbc_stress_y(KArgs A) {
+  grid_dep_wait();
   TE_K3
   float *TE_R s22 = A.p[1], *TE_R s12 = A.p[2];
   const int i = tx - 1, k = ty;
@@ -907,6 +950,7 @@ TE_LAUNCH3(turb_openbc_stress_y)
 
 // tke_advance.wgsl: tke = fma(dttmp, tketen, tkea), flushed to 0 below 1e-10
 __global__ void k_tke_advance(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const float *TE_R tkea = A.p[1], *TE_R tketen = A.p[2];
   float* TE_R tke = A.p[4];
@@ -920,6 +964,7 @@ TE_LAUNCH3(tke_advance)
 
 // tke_sources.wgsl: tketen = fma(-khv, nm, -dissten) + epst
 __global__ void k_tke_sources(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const float *TE_R khv = A.p[1], *TE_R nm = A.p[2], *TE_R dissten = A.p[3], *TE_R epst = A.p[4];
   float* TE_R tketen = A.p[5];
@@ -932,6 +977,7 @@ TE_LAUNCH3(tke_sources)
 
 // tke_flux_h.wgsl: horizontal TKE fluxes at the x and y faces of w levels 1..nz-1
 __global__ void k_tke_flux_h(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const float *TE_R t = A.p[1], *TE_R rf = A.p[2], *TE_R kmh = A.p[3], *TE_R hm = A.p[30];
   float *TE_R fx = A.p[4], *TE_R fy = A.p[5];
@@ -950,7 +996,7 @@ TE_LAUNCH3(tke_flux_h)
 static void launch_columns(void (*k)(KArgs), const KArgs& A, cudaStream_t s) {
   dim3 b(32, 4, 1);
   dim3 gr((A.gx + 31) / 32, (A.gy + 3) / 4, 1);
-  k<<<gr, b, 0, s>>>(A);
+  launch_pdl(k, dim3(gr), dim3(b), 0, s, A);
 }
 #define TE_LAUNCH_COLUMNS(name) \
   static void launch_##name(const KArgs& A, cudaStream_t s) { launch_columns(k_##name, A, s); }
@@ -958,6 +1004,7 @@ static void launch_columns(void (*k)(KArgs), const KArgs& A, cudaStream_t s) {
 // mp_pdefq.wgsl: per column, q below rmax set to 0 and the column rescaled so that
 // sum rho q keeps its value before the clip ((t1 + 1e-20) / (t2 + 1e-20), 1 if negative)
 __global__ void k_mp_pdefq(KArgs A) {
+  grid_dep_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const Dims& g = A.g;
@@ -1019,6 +1066,7 @@ struct TsviCol {
 };
 
 __global__ void k_turb_scalar_vert_implicit(KArgs A) {
+  grid_dep_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const Dims& g = A.g;
@@ -1091,6 +1139,7 @@ TE_LAUNCH_COLUMNS(turb_scalar_vert_implicit)
 // rayleigh_damping.wgsl: -rdalpha tau (phi - phi_ref) for u, v, th (profiles, or level
 // averages when toAverage) and -rdalpha tauf w, tauf raised to the lateral sponge
 __global__ void k_rayleigh_damping(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const int i = tx, j = ty, k = tz;
   if (i > g.nx || j > g.ny || k > g.nz) return;
@@ -1121,6 +1170,7 @@ TE_LAUNCH3(rayleigh_damping)
 // turb_rho_faces.wgsl: rr = 1 / rho (k < nz); rf on w levels, interior c1/c2 weights,
 // bottom and top extrapolated with cgs / cgt; columns -2..nx+1, rows -2..ny+1
 __global__ void k_turb_rho_faces(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const int i = tx - 2, j = ty - 2, k = tz;
   if (i > g.nx + 1 || j > g.ny + 1 || k > g.nz) return;
@@ -1146,6 +1196,7 @@ TE_LAUNCH3(turb_rho_faces)
 // turb_def_centers.wgsl: rho-weighted strain rates s11, s22, s33 at cell centres and s12
 // at the (i-1/2, j-1/2) edges; columns -1..nx+1, rows -1..ny+1
 __global__ void k_turb_def_centers(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const int i = tx - 1, j = ty - 1, k = tz;
   if (i > g.nx + 1 || j > g.ny + 1 || k >= g.nz) return;
@@ -1161,6 +1212,7 @@ TE_LAUNCH3(turb_def_centers)
 
 // turb_def_faces.wgsl: s13, s23 on w levels 1..nz-1 at the x and y faces
 __global__ void k_turb_def_faces(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const int i = tx, j = ty, k = tz + 1;
   if (i > g.nx + 1 || j > g.ny + 1 || k > g.nz - 1) return;
@@ -1175,6 +1227,7 @@ TE_LAUNCH3(turb_def_faces)
 // turb_def_assemble.wgsl: defv = 4 (t13 + t23) / rf^2, defh = (2 (t11 + t22 + t33) + 4 t12)
 // / rf^2 on w levels 1..nz-1 (squared rates interpolated by c1/c2, edge/face averages)
 __global__ void k_turb_def_assemble(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const int i = tx, j = ty, k = tz + 1;
   if (i >= g.nx || j >= g.ny || k > g.nz - 1) return;
@@ -1200,6 +1253,7 @@ TE_LAUNCH3(turb_def_assemble)
 // average of kmh, t13 / t23 by the face sums of kmv (levels 1..nz-1, i, j >= 0); the
 // dispatch covers columns and rows -1..n
 __global__ void k_turb_gettau(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const int i = tx - 1, j = ty - 1, k = tz;
   if (i > g.nx || j > g.ny || k >= g.nz) return;
@@ -1224,6 +1278,7 @@ TE_LAUNCH3(turb_gettau)
 // length (limited by c_l sqrt(tke / N^2) in stable air), dissipation added to dissten,
 // km = cmz sqrt(tke) len kmScale (or kmFixed > 0), kh = km min(1 + 2 len / scale, 3)
 __global__ void k_turb_km_kh(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const int i = tx, j = ty, k = tz + 1;
   if (i >= g.nx || j >= g.ny || k > g.nz - 1) return;
@@ -1268,6 +1323,7 @@ TE_LAUNCH3(turb_km_kh)
 // tke_epst.wgsl: shear production on w levels 1..nz-1, stresses times strain rates
 // interpolated (c1/c2) or averaged to the w point, divided by rf
 __global__ void k_tke_epst(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const int i = tx, j = ty, k = tz + 1;
   if (i >= g.nx || j >= g.ny || k > g.nz - 1) return;
@@ -1311,6 +1367,7 @@ __device__ __forceinline__ float mp_rs(float p, float t, float a, float b) {
 // moist: g dln(thv)/dz, or in saturated air (liquid above 0 C, ice below -40 C, a linear
 // blend between) the moist-adiabatic form (lam_1); sat marks saturated points
 __global__ void k_turb_nm(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const int i = tx, j = ty, k = tz + 1;
   if (i >= g.nx || j >= g.ny || k > g.nz - 1) return;
@@ -1399,6 +1456,7 @@ TE_LAUNCH3(turb_nm)
 // 2 drag coefficient 0.001229 with the surface wind speed (plane 2 of sfc); 3 drag against
 // the domain-mean wind (planes 14..16 at the origin, lam_1); else u*^2 w1 / max(s1, 0.01)
 __global__ void k_turb_sfcstress(KArgs A) {
+  grid_dep_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const Dims& g = A.g;
@@ -1456,6 +1514,7 @@ static void launch_turb_sfcstress(const KArgs& A, cudaStream_t s) { launch_colum
 // (moist); the dissipation averaged to the cell centre, at the surface with bbc3
 // u*^3 ln((dz1 + z0) / z0) / (k dz1)
 __global__ void k_turb_dissipative_heating(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const int i = tx, j = ty, k = tz;
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
@@ -1494,6 +1553,7 @@ TE_LAUNCH3(turb_dissipative_heating)
 // (dw/dy) cross term dwd.  s is the offset of the staggered neighbour (1 or strideJ).
 template <int AX>
 __global__ void k_turb_uv_tendency(KArgs A) {
+  grid_dep_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const Dims& g = A.g;
@@ -1576,6 +1636,7 @@ static void launch_turb_v_tendency(const KArgs& A, cudaStream_t s) { launch_colu
 // right-hand side), tendency rf (new - old) / dt.
 template <int TKE>
 __global__ void k_turb_wlevel(KArgs A) {
+  grid_dep_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const Dims& g = A.g;
@@ -1678,6 +1739,7 @@ __device__ __forceinline__ void df_add_pair(F2& acc, float vx, float vy) {
 // mass_row_sums.wgsl: per (j, k) row the sums over i of rho / (uh vh mh) (rows1) and of
 // pi0 + pp3d (rows2), stored as pairs at k strideK + j
 __global__ void k_mass_row_sums(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const int j = tx, k = ty;
   if (j >= g.ny || k >= g.nz) return;
@@ -1701,6 +1763,7 @@ TE_LAUNCH3(mass_row_sums)
 
 // mass_level_sums.wgsl: per level the sums over j of the row pairs
 __global__ void k_mass_level_sums(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const int k = tx;
   if (ty != 0 || k >= g.nz) return;
@@ -1721,6 +1784,7 @@ TE_LAUNCH3(mass_level_sums)
 // mass_reference_init.wgsl: on its first run (ref[2] == 0) thread 0 stores the total mass
 // (the sum of the level pairs) as the reference and sets ref[2] = 1
 __global__ void k_mass_reference_init(KArgs A) {
+  grid_dep_wait();
   TE_K3
   if (tx != 0 || ty != 0) return;
   const float* TE_R levels1 = A.p[1];
@@ -1739,6 +1803,7 @@ TE_LAUNCH3(mass_reference_init)
 // builtin for |r| > 0.05, else its third-order expansion), added to pp3d; prs and rho from
 // the corrected pi; thread (0,0,0) records tem, the mass, the pi sum, r and the mass's low part
 __global__ void k_mass_correction_apply(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const int i = tx, j = ty, k = tz;
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
@@ -1779,6 +1844,7 @@ TE_LAUNCH3(mass_correction_apply)
 // morr_prep.wgsl: temperature T = (th0 + th)(pi0 + pp) and a copy qv0 of qv before the
 // microphysics column
 __global__ void k_morr_prep(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const int i = tx, j = ty, k = tz;
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
@@ -1791,6 +1857,7 @@ TE_LAUNCH3(morr_prep)
 // morr_post.wgsl: where the column changed T (by >= 1e-4) or qv (by >= 1e-14), pressure
 // from the equation of state, pi' from it (the reference's correctly rounded pow) and th
 __global__ void k_morr_post(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const int i = tx, j = ty, k = tz;
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
@@ -1815,6 +1882,7 @@ TE_LAUNCH3(morr_post)
 // -------------------------------------------------- thermodynamic glue
 
 __global__ void k_update_diagnostics_moist(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const float *TE_R thp = A.p[1], *TE_R ppp = A.p[2], *TE_R th0 = A.p[3], *TE_R pi0 = A.p[4], *TE_R qv0 = A.p[5], *TE_R qc0 = A.p[6];
   const float *TE_R qi0 = A.p[7], *TE_R rth0 = A.p[8], *TE_R qv = A.p[9], *TE_R qc = A.p[10], *TE_R qr = A.p[11], *TE_R qi = A.p[12];
@@ -1844,6 +1912,7 @@ __global__ void k_update_diagnostics_moist(KArgs A) {
 TE_LAUNCH3(update_diagnostics_moist)
 
 __global__ void k_pressure_tendency(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const float *TE_R th = A.p[1], *TE_R qv = A.p[2], *TE_R rho = A.p[3], *TE_R ppi = A.p[4], *TE_R thten = A.p[5], *TE_R qpten = A.p[6];
   const float *TE_R th0 = A.p[7], *TE_R pi0 = A.p[8];
@@ -1886,6 +1955,7 @@ __global__ void k_pressure_tendency(KArgs A) {
 TE_LAUNCH3(pressure_tendency)
 
 __global__ void k_divergence3d(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const float *TE_R u = A.p[1], *TE_R v = A.p[2], *TE_R w = A.p[3], *TE_R mh = A.p[4];
   float* TE_R div = A.p[5];
@@ -1901,6 +1971,7 @@ __global__ void k_divergence3d(KArgs A) {
 TE_LAUNCH3(divergence3d)
 
 __global__ void k_update_rho_prs(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const int moist = A.iv[1];
   const float *TE_R thp = A.p[2], *TE_R ppp = A.p[3], *TE_R th0 = A.p[4], *TE_R pi0 = A.p[5], *TE_R qv = A.p[6];
@@ -1919,6 +1990,7 @@ __global__ void k_update_rho_prs(KArgs A) {
 TE_LAUNCH3(update_rho_prs)
 
 __global__ void k_diabatic_unapply(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const float dt = A.f[1];
   float *TE_R pp3d = A.p[2], *TE_R th = A.p[3], *TE_R qv = A.p[4], *TE_R qc = A.p[5];
@@ -1943,6 +2015,7 @@ __global__ void k_diabatic_unapply(KArgs A) {
 TE_LAUNCH3(diabatic_unapply)
 
 __global__ void k_diabatic_rates(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const float dt = A.f[1];
   const float *TE_R pp3d = A.p[2], *TE_R th = A.p[3], *TE_R qv = A.p[4], *TE_R qc = A.p[5];
@@ -1959,6 +2032,7 @@ __global__ void k_diabatic_rates(KArgs A) {
 TE_LAUNCH3(diabatic_rates)
 
 __global__ void k_ppx_finish(KArgs A) {
+  grid_dep_wait();
   TE_K3
   const float* TE_R pp3d = A.p[1];
   float* TE_R ppx = A.p[2];
