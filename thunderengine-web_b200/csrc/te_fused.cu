@@ -67,7 +67,6 @@ __device__ __forceinline__ float uv_v(const AcuArgs& A, int i, int j, int c) {
 constexpr int kUvLevels = 2;
 
 __global__ void __launch_bounds__(256) k_acu_uv(AcuArgs A) {
-  grid_dep_wait();
   const Dims& g = A.g;
   const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x) - 3;
   const int j = (int)(blockIdx.y * blockDim.y + threadIdx.y) - 3;
@@ -213,7 +212,6 @@ __device__ __forceinline__ float fpk_of(const AcuArgs& A, const LevelIn& L, floa
 }
 
 __global__ void __launch_bounds__(kColThreads, 2) k_acu_column(AcuArgs A) {
-  grid_dep_wait();
   extern __shared__ float smem[];
   const Dims& g = A.g;
   const Acoustic& a = A.a;
@@ -344,7 +342,7 @@ static void launch_acu_column(const AcuArgs& A, cudaStream_t s) {
     configured = (int)bytes;
   }
   dim3 b(kColThreads), gr((A.g.nx + kColTile - 1) / kColTile, A.g.ny);
-  launch_pdl(k_acu_column, dim3(gr), dim3(b), bytes, s, A);
+  launch_kernel(k_acu_column, dim3(gr), dim3(b), bytes, s, A);
 }
 
 // ------------------------------------------------------------ periodic halos
@@ -372,7 +370,6 @@ constexpr int kHaloX = 7;
 constexpr int kHaloLevels = 3;  // levels per thread: their loads are issued together
 
 __global__ void __launch_bounds__(256) k_halo_periodic(HaloArgs H) {
-  grid_dep_wait();
   const Dims& g = H.g;
   const int k0 = blockIdx.y * kHaloLevels;
   const int sk = g.sJ * g.sK;
@@ -439,7 +436,7 @@ __global__ void __launch_bounds__(256) k_halo_periodic(HaloArgs H) {
 static void launch_halo(const HaloArgs& H, cudaStream_t s) {
   const int xblocks = (H.g.sK + 7) / 8, yblocks = (kHaloX * H.g.nx + 255) / 256;
   dim3 b(256), gr(xblocks + yblocks, (H.g.nz + kHaloLevels) / kHaloLevels);
-  launch_pdl(k_halo_periodic, dim3(gr), dim3(b), 0, s, H);
+  launch_kernel(k_halo_periodic, dim3(gr), dim3(b), 0, s, H);
 }
 
 // ------------------------------------------------------------ planner helpers
@@ -506,7 +503,6 @@ struct AdvKZ {
 
 template <int KIND, int ST>
 __global__ void __launch_bounds__(kAdvTX* kAdvTY, AdvKZ<KIND>::value > 1 ? 6 : 8) k_adv_fused(AdvArgs A) {
-  grid_dep_wait();
   constexpr int kAdvKZ = AdvKZ<KIND>::value;
   __shared__ float fxs[2][kAdvTY][kAdvTX + 1];
   __shared__ float fys[2][kAdvTY + 1][kAdvTX];
@@ -566,7 +562,7 @@ static void launch_adv_t(const AdvArgs& A, cudaStream_t s) {
   const dim3 b(kAdvTX, kAdvTY, 1);
   constexpr int kz = AdvKZ<KIND>::value;
   const dim3 gr((A.ihi - A.ilo + kAdvTX) / kAdvTX, (A.jhi - A.jlo + kAdvTY) / kAdvTY, (A.khi - A.klo + kz) / kz);
-  launch_pdl(k_adv_fused<KIND, ST>, dim3(gr), dim3(b), 0, s, A);
+  launch_kernel(k_adv_fused<KIND, ST>, dim3(gr), dim3(b), 0, s, A);
 }
 
 static void launch_adv(const AdvArgs& A, int kind, int st, cudaStream_t s) {
@@ -966,7 +962,7 @@ void FusedStep::launch_segment(Plan& P, std::vector<Op>& ops, int seg, int part)
     const Dims& g = A.g;
     if (part < 0 || part == 0) {
       dim3 b(32, 8, 1), gr((g.sJ + 31) / 32, (g.sK + 7) / 8, (g.nz + kUvLevels) / kUvLevels);
-      launch_pdl(k_acu_uv, dim3(gr), dim3(b), 0, P.stream, A);
+      launch_kernel(k_acu_uv, dim3(gr), dim3(b), 0, P.stream, A);
     }
     if (part < 0 || part == 1) launch_acu_column(A, P.stream);
     if (part < 0 || part == 2) {

@@ -38,7 +38,7 @@ namespace fast {
 static void launch3(void (*k)(KArgs), const KArgs& A, cudaStream_t s) {
   dim3 b(32, 4, 1);
   dim3 gr((A.gx + 31) / 32, (A.gy + 3) / 4, A.gz);
-  launch_pdl(k, dim3(gr), dim3(b), 0, s, A);
+  launch_kernel(k, dim3(gr), dim3(b), 0, s, A);
 }
 
 #define TE_LAUNCH3(name) \
@@ -49,7 +49,7 @@ static void launch3(void (*k)(KArgs), const KArgs& A, cudaStream_t s) {
 static void launch_halo3(void (*k)(KArgs), const KArgs& A, cudaStream_t s) {
   dim3 b(4, 64, 1);
   dim3 gr((A.gx + 3) / 4, (A.gy + 63) / 64, A.gz);
-  launch_pdl(k, dim3(gr), dim3(b), 0, s, A);
+  launch_kernel(k, dim3(gr), dim3(b), 0, s, A);
 }
 #define TE_LAUNCH_HALO(name) \
   static void launch_##name(const KArgs& A, cudaStream_t s) { launch_halo3(k_##name, A, s); }
@@ -64,7 +64,6 @@ enum { kRowVec = 4 };
 
 template <class Op>
 __global__ void __launch_bounds__(128) k_rowvec(KArgs A) {
-  grid_dep_wait();
   const int tx = blockIdx.x * blockDim.x + threadIdx.x;
   const int ty = blockIdx.y * blockDim.y + threadIdx.y;
   const int tz0 = blockIdx.z * kRowVec;
@@ -85,7 +84,7 @@ template <class Op>
 static void launch_rowvec(const KArgs& A, cudaStream_t s) {
   dim3 b(32, 4, 1);
   dim3 gr((A.gx + 31) / 32, (A.gy + 3) / 4, (A.gz + kRowVec - 1) / kRowVec);
-  launch_pdl(k_rowvec<Op>, dim3(gr), dim3(b), 0, s, A);
+  launch_kernel(k_rowvec<Op>, dim3(gr), dim3(b), 0, s, A);
 }
 
 // ------------------------------------------------------------------ fluxes
@@ -95,7 +94,6 @@ static void launch_rowvec(const KArgs& A, cudaStream_t s) {
 // adv_flux_x / adv_flux_y: f = rr * flx5(upwind stencil)
 template <int DIR>
 __global__ void k_flux_lin_h(KArgs A) {
-  grid_dep_wait();
   TE_K3
   int i = tx, j = ty, k = tz;
   if (DIR == 0 ? (i > g.nx || j >= g.ny || k >= g.nz) : (i >= g.nx || j > g.ny || k >= g.nz)) return;
@@ -105,7 +103,6 @@ static void launch_adv_flux_x(const KArgs& A, cudaStream_t s) { launch3(k_flux_l
 static void launch_adv_flux_y(const KArgs& A, cudaStream_t s) { launch3(k_flux_lin_h<1>, A, s); }
 
 __global__ void k_adv_flux_z(KArgs A) {
-  grid_dep_wait();
   TE_K3
   int i = tx, j = ty, k = tz;
   if (i >= g.nx || j >= g.ny || k > g.nz) return;
@@ -117,7 +114,6 @@ TE_LAUNCH3(adv_flux_z)
 // adv_flux_x_stag / adv_flux_y_stag (momentum, RK stages 1-2)
 template <int DIR>
 __global__ void k_flux_stag_h(KArgs A) {
-  grid_dep_wait();
   TE_K3
   int i = tx - 1, j = ty - 1, k = tz;
   if (i > g.nx || j > g.ny || k >= g.nz) return;
@@ -127,7 +123,6 @@ static void launch_adv_flux_x_stag(const KArgs& A, cudaStream_t s) { launch3(k_f
 static void launch_adv_flux_y_stag(const KArgs& A, cudaStream_t s) { launch3(k_flux_stag_h<1>, A, s); }
 
 __global__ void k_adv_flux_z_stag(KArgs A) {
-  grid_dep_wait();
   TE_K3
   int i = tx, j = ty, k = tz;
   if (i > g.nx || j > g.ny || k > g.nz) return;
@@ -138,7 +133,6 @@ TE_LAUNCH3(adv_flux_z_stag)
 // adv_flux_x_weno / adv_flux_y_weno (scalars, positive-definite gate)
 template <int DIR>
 __global__ void k_flux_weno_h(KArgs A) {
-  grid_dep_wait();
   TE_K3
   int i = tx, j = ty, k = tz;
   if (DIR == 0 ? (i > g.nx || j >= g.ny || k >= g.nz) : (i >= g.nx || j > g.ny || k >= g.nz)) return;
@@ -148,7 +142,6 @@ static void launch_adv_flux_x_weno(const KArgs& A, cudaStream_t s) { launch3(k_f
 static void launch_adv_flux_y_weno(const KArgs& A, cudaStream_t s) { launch3(k_flux_weno_h<1>, A, s); }
 
 __global__ void k_adv_flux_z_weno(KArgs A) {
-  grid_dep_wait();
   TE_K3
   int i = tx, j = ty, k = tz;
   if (i >= g.nx || j >= g.ny || k > g.nz) return;
@@ -160,7 +153,6 @@ TE_LAUNCH3(adv_flux_z_weno)
 // adv_flux_x_weno_uv / adv_flux_y_weno_uv (u, v momentum, RK stage 3)
 template <int DIR>
 __global__ void k_flux_weno_uv_h(KArgs A) {
-  grid_dep_wait();
   TE_K3
   int i = tx - 1, j = ty - 1, k = tz;
   if (i > g.nx || j > g.ny || k >= g.nz) return;
@@ -170,7 +162,6 @@ static void launch_adv_flux_x_weno_uv(const KArgs& A, cudaStream_t s) { launch3(
 static void launch_adv_flux_y_weno_uv(const KArgs& A, cudaStream_t s) { launch3(k_flux_weno_uv_h<1>, A, s); }
 
 __global__ void k_adv_flux_z_weno_uv(KArgs A) {
-  grid_dep_wait();
   TE_K3
   int i = tx, j = ty, k = tz;
   if (i > g.nx || j > g.ny || k > g.nz) return;
@@ -181,7 +172,6 @@ TE_LAUNCH3(adv_flux_z_weno_uv)
 // adv_flux_x_weno_w / adv_flux_y_weno_w (w momentum, RK stage 3)
 template <int DIR>
 __global__ void k_flux_weno_w_h(KArgs A) {
-  grid_dep_wait();
   TE_K3
   int i = tx - 1, j = ty - 1, k = tz;
   if (i < 0 || j < 0 || i > g.nx || j > g.ny || k >= g.nz) return;
@@ -191,7 +181,6 @@ static void launch_adv_flux_x_weno_w(const KArgs& A, cudaStream_t s) { launch3(k
 static void launch_adv_flux_y_weno_w(const KArgs& A, cudaStream_t s) { launch3(k_flux_weno_w_h<1>, A, s); }
 
 __global__ void k_adv_flux_z_weno_w(KArgs A) {
-  grid_dep_wait();
   TE_K3
   int i = tx, j = ty, k = tz;
   if (i > g.nx || j > g.ny || k > g.nz) return;
@@ -202,7 +191,6 @@ TE_LAUNCH3(adv_flux_z_weno_w)
 // ------------------------------------------------------------ assembly
 
 __global__ void k_adv_assemble(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const int stag = A.iv[1];
   const float *TE_R fx = A.p[3], *TE_R fy = A.p[4], *TE_R fz = A.p[5];
@@ -227,7 +215,6 @@ __global__ void k_adv_assemble(KArgs A) {
 TE_LAUNCH3(adv_assemble)
 
 __global__ void k_rk_update(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const int stag = A.iv[1];
   const float *TE_R phiA = A.p[2], *TE_R tend = A.p[3];
@@ -254,7 +241,6 @@ __device__ __forceinline__ bool pdef_inflow(const Dims& g, int dir, int i, int j
 }
 
 __global__ void k_pdef_dum(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const int dir = A.iv[1];
   const float *TE_R s = A.p[2], *TE_R s0 = A.p[3], *TE_R f = A.p[4], *TE_R rr = A.p[5], *TE_R rho0 = A.p[6], *TE_R mh = A.p[7];
@@ -309,7 +295,6 @@ __device__ __forceinline__ float pdef_mass(float dm2, float dm1, float d0, float
 }
 
 __global__ void k_pdef_apply(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const float *TE_R s = A.p[1], *TE_R s0 = A.p[2], *TE_R fx = A.p[3], *TE_R fy = A.p[4], *TE_R fz = A.p[5];
   const float *TE_R rru = A.p[6], *TE_R rrv = A.p[7], *TE_R rrw = A.p[8], *TE_R dumx = A.p[9], *TE_R dumy = A.p[10], *TE_R dumz = A.p[11];
@@ -363,7 +348,6 @@ TE_LAUNCH3(pdef_apply)
   int c = gidx(g, i, j, k);
 
 __global__ void k_build_sadv(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const float *TE_R th0 = A.p[1], *TE_R thp = A.p[2];
   float* TE_R sadv = A.p[3];
@@ -373,7 +357,6 @@ __global__ void k_build_sadv(KArgs A) {
 TE_LAUNCH3(build_sadv)
 
 __global__ void k_massflux_from_state(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const float *TE_R u = A.p[1], *TE_R v = A.p[2], *TE_R w = A.p[3], *TE_R rho0 = A.p[4], *TE_R rf0 = A.p[5];
   float *TE_R rru = A.p[6], *TE_R rrv = A.p[7], *TE_R rrw = A.p[8];
@@ -387,7 +370,6 @@ __global__ void k_massflux_from_state(KArgs A) {
 TE_LAUNCH3(massflux_from_state)
 
 __global__ void k_div_massflux(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const float *TE_R rru = A.p[1], *TE_R rrv = A.p[2], *TE_R rrw = A.p[3], *TE_R mh = A.p[4];
   float* TE_R divx = A.p[5];
@@ -425,7 +407,6 @@ struct OpDivMassflux {  // div_massflux as a row-vector op (same operations)
 };
 
 __global__ void k_velocity_to_massflux(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const float *TE_R rho0 = A.p[1], *TE_R rf0 = A.p[2];
   float *TE_R rru = A.p[3], *TE_R rrv = A.p[4], *TE_R rrw = A.p[5];
@@ -465,7 +446,6 @@ struct OpVelocityToMassflux {  // velocity_to_massflux as a row-vector op
 };
 
 __global__ void k_stage_state_reset(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const float *TE_R ua = A.p[1], *TE_R va = A.p[2], *TE_R wa = A.p[3], *TE_R ppi = A.p[4];
   float *TE_R u = A.p[5], *TE_R v = A.p[6], *TE_R w = A.p[7], *TE_R pp3d = A.p[8], *TE_R ppd = A.p[9];
@@ -480,7 +460,6 @@ __global__ void k_stage_state_reset(KArgs A) {
 TE_LAUNCH3(stage_state_reset)
 
 __global__ void k_stage_tendency_reset(KArgs A) {
-  grid_dep_wait();
   TE_K3
   float *TE_R uten = A.p[1], *TE_R vten = A.p[2], *TE_R wten = A.p[3];
   TE_WHOLE(k <= g.nz)
@@ -491,7 +470,6 @@ __global__ void k_stage_tendency_reset(KArgs A) {
 TE_LAUNCH3(stage_tendency_reset)
 
 __global__ void k_buoyancy_apply(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const float *TE_R buoy = A.p[1], *TE_R c1 = A.p[2], *TE_R c2 = A.p[3];
   float* TE_R wten = A.p[4];
@@ -504,7 +482,6 @@ __global__ void k_buoyancy_apply(KArgs A) {
 TE_LAUNCH3(buoyancy_apply)
 
 __global__ void k_apply_thterm(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const float *TE_R div = A.p[1], *TE_R thterm = A.p[2];
   float* TE_R tend = A.p[3];
@@ -518,7 +495,6 @@ TE_LAUNCH3(apply_thterm)
 // ------------------------------------------------------ acoustic substep
 
 __global__ void k_acoustic_prepare(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const Acoustic a = A.a;
   const float *TE_R ppterm = A.p[2], *TE_R piadv = A.p[3], *TE_R thv = A.p[4], *TE_R rr0 = A.p[5], *TE_R rf0 = A.p[6];
@@ -548,7 +524,6 @@ __global__ void k_acoustic_prepare(KArgs A) {
 TE_LAUNCH3(acoustic_prepare)
 
 __global__ void k_acoustic_begin(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const float* TE_R w = A.p[2];
   float *TE_R rru = A.p[3], *TE_R rrv = A.p[4], *TE_R rrw = A.p[5];
@@ -560,7 +535,6 @@ __global__ void k_acoustic_begin(KArgs A) {
 TE_LAUNCH3(acoustic_begin)
 
 __global__ void k_acoustic_uv(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const Acoustic a = A.a;
   const float *TE_R ppd = A.p[2], *TE_R thv = A.p[3], *TE_R uten = A.p[4], *TE_R vten = A.p[5];
@@ -582,7 +556,6 @@ __global__ void k_acoustic_uv(KArgs A) {
 TE_LAUNCH3(acoustic_uv)
 
 __global__ void k_acoustic_fpk(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const Acoustic a = A.a;
   const float *TE_R u = A.p[2], *TE_R v = A.p[3], *TE_R w = A.p[4], *TE_R piadv = A.p[5], *TE_R ppten = A.p[6], *TE_R ppterm = A.p[7];
@@ -606,7 +579,6 @@ TE_LAUNCH3(acoustic_fpk)
 // Vertically implicit w-pi' solve: one column per thread, columns of a warp adjacent
 // in i (coalesced), the Thomas recurrence sequential in k as in the reference.
 __global__ void k_acoustic_w_solve(KArgs A) {
-  grid_dep_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const Dims& g = A.g;
@@ -657,11 +629,10 @@ __global__ void k_acoustic_w_solve(KArgs A) {
 static void launch_acoustic_w_solve(const KArgs& A, cudaStream_t s) {
   dim3 b(32, 4, 1);
   dim3 gr((A.gx + 31) / 32, (A.gy + 3) / 4, 1);
-  launch_pdl(k_acoustic_w_solve, dim3(gr), dim3(b), 0, s, A);
+  launch_kernel(k_acoustic_w_solve, dim3(gr), dim3(b), 0, s, A);
 }
 
 __global__ void k_acoustic_pp(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const Acoustic a = A.a;
   const float *TE_R w = A.p[2], *TE_R pk1 = A.p[3], *TE_R pk2 = A.p[4], *TE_R qk = A.p[5], *TE_R fpk = A.p[6];
@@ -682,7 +653,6 @@ __global__ void k_acoustic_pp(KArgs A) {
 TE_LAUNCH3(acoustic_pp)
 
 __global__ void k_acoustic_accumulate(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const float *TE_R u = A.p[2], *TE_R v = A.p[3], *TE_R w = A.p[4];
   float *TE_R rru = A.p[5], *TE_R rrv = A.p[6], *TE_R rrw = A.p[7];
@@ -703,7 +673,6 @@ TE_LAUNCH3(acoustic_accumulate)
 // ------------------------------------------------------- periodic halos
 
 __global__ void k_bc_periodic_x(KArgs A) {
-  grid_dep_wait();
   TE_K3
   float* TE_R f = A.p[1];
   int h = tx, jj = ty - 3, k = tz;
@@ -716,7 +685,6 @@ __global__ void k_bc_periodic_x(KArgs A) {
 TE_LAUNCH_HALO(bc_periodic_x)
 
 __global__ void k_bc_periodic_y(KArgs A) {
-  grid_dep_wait();
   TE_K3
   float* TE_R f = A.p[1];
   int h = tx, i = ty - 3, k = tz;
@@ -733,7 +701,6 @@ TE_LAUNCH_HALO(bc_periodic_y)
 // bc_open_x.wgsl / bc_open_y.wgsl: zero-gradient halos, -1-h <- 0 and last+1+h <- last
 // (h < 3, last = n + stagger - 1)
 __global__ void k_bc_open_x(KArgs A) {
-  grid_dep_wait();
   TE_K3
   float* TE_R f = A.p[1];
   const int stagX = A.iv[2];
@@ -746,7 +713,6 @@ __global__ void k_bc_open_x(KArgs A) {
 TE_LAUNCH_HALO(bc_open_x)
 
 __global__ void k_bc_open_y(KArgs A) {
-  grid_dep_wait();
   TE_K3
   float* TE_R f = A.p[1];
   const int stagY = A.iv[2];
@@ -770,7 +736,6 @@ __device__ __forceinline__ float radbc_speed(float dx, float a, float b, float f
 // the west (i = 1) and east (i = nx - 1) faces.  One thread per row; the level loop is
 // sequential as in the reference (the sum's rounding order).
 __global__ void k_radbc_ew(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const float *TE_R ua = A.p[1], *TE_R u3d = A.p[2], *TE_R hm = A.p[30];
   const float dt = A.f[3];
@@ -800,7 +765,6 @@ TE_LAUNCH3(radbc_ew)
 
 // radbc_ns.wgsl: the same for v at the south (j = 1) and north (j = ny - 1) faces
 __global__ void k_radbc_ns(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const float *TE_R va = A.p[1], *TE_R v3d = A.p[2], *TE_R hm = A.p[30];
   const float dt = A.f[3];
@@ -831,7 +795,6 @@ TE_LAUNCH3(radbc_ns)
 // openbc_uv_tendency.wgsl: on open x boundaries the u faces i = 0 and i = nx, on open y
 // boundaries the v faces j = 0 and j = ny, advance by the radiation term
 __global__ void k_openbc_uv_tendency(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const Acoustic a = A.a;
   const float *TE_R radbcw = A.p[2], *TE_R radbce = A.p[3], *TE_R radbcs = A.p[4], *TE_R radbcn = A.p[5];
@@ -862,7 +825,6 @@ TE_LAUNCH3(openbc_uv_tendency)
 // turb_zero.wgsl: zero f[i + strideJ (j + strideK k)] for i < strideJ, j < strideK and
 // k <= nz + 1 (the reference's range, one level above a field's nz + 1)
 __global__ void k_turb_zero(KArgs A) {
-  grid_dep_wait();
   TE_K3
   float* TE_R f = A.p[1];
   if (tx >= g.sJ || ty >= g.sK || tz > g.nz + 1) return;
@@ -872,7 +834,6 @@ TE_LAUNCH3(turb_zero)
 
 // turb_add_tendency.wgsl: dst = fma(scale, src, dst) over the whole field
 __global__ void k_turb_add_tendency(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const float* TE_R src = A.p[1];
   float* TE_R dst = A.p[2];
@@ -883,7 +844,6 @@ TE_LAUNCH3(turb_add_tendency)
 
 // turb_scalar_flux_h.wgsl: horizontal subgrid scalar fluxes at the x and y faces
 __global__ void k_turb_scalar_flux_h(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const float *TE_R s = A.p[1], *TE_R rho = A.p[2], *TE_R khh = A.p[3], *TE_R hm = A.p[30];
   const float leNum = A.f[4];
@@ -900,7 +860,6 @@ TE_LAUNCH3(turb_scalar_flux_h)
 
 // turb_openbc_flux.wgsl: edge fluxes copy their inner neighbours on open boundaries
 __global__ void k_turb_openbc_flux(KArgs A) {
-  grid_dep_wait();
   TE_K3
   float *TE_R fx = A.p[1], *TE_R fy = A.p[2];
   const int openx = A.iv[3], openy = A.iv2[3];
@@ -919,7 +878,6 @@ TE_LAUNCH3(turb_openbc_flux)
 
 // turb_openbc_stress_x.wgsl / _y.wgsl: edge stresses copy their inner neighbours
 __global__ void k_turb_openbc_stress_x(KArgs A) {
-  grid_dep_wait();
   TE_K3
   float *TE_R s11 = A.p[1], *TE_R s12 = A.p[2];
   const int j = tx - 1, k = ty;
@@ -934,7 +892,6 @@ __global__ void k_turb_openbc_stress_x(KArgs A) {
 TE_LAUNCH3(turb_openbc_stress_x)
 
 __global__ void k_turb_openbc_stress_y(KArgs A) {
-  grid_dep_wait();
   TE_K3
   float *TE_R s22 = A.p[1], *TE_R s12 = A.p[2];
   const int i = tx - 1, k = ty;
@@ -950,7 +907,6 @@ TE_LAUNCH3(turb_openbc_stress_y)
 
 // tke_advance.wgsl: tke = fma(dttmp, tketen, tkea), flushed to 0 below 1e-10
 __global__ void k_tke_advance(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const float *TE_R tkea = A.p[1], *TE_R tketen = A.p[2];
   float* TE_R tke = A.p[4];
@@ -964,7 +920,6 @@ TE_LAUNCH3(tke_advance)
 
 // tke_sources.wgsl: tketen = fma(-khv, nm, -dissten) + epst
 __global__ void k_tke_sources(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const float *TE_R khv = A.p[1], *TE_R nm = A.p[2], *TE_R dissten = A.p[3], *TE_R epst = A.p[4];
   float* TE_R tketen = A.p[5];
@@ -977,7 +932,6 @@ TE_LAUNCH3(tke_sources)
 
 // tke_flux_h.wgsl: horizontal TKE fluxes at the x and y faces of w levels 1..nz-1
 __global__ void k_tke_flux_h(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const float *TE_R t = A.p[1], *TE_R rf = A.p[2], *TE_R kmh = A.p[3], *TE_R hm = A.p[30];
   float *TE_R fx = A.p[4], *TE_R fy = A.p[5];
@@ -996,7 +950,7 @@ TE_LAUNCH3(tke_flux_h)
 static void launch_columns(void (*k)(KArgs), const KArgs& A, cudaStream_t s) {
   dim3 b(32, 4, 1);
   dim3 gr((A.gx + 31) / 32, (A.gy + 3) / 4, 1);
-  launch_pdl(k, dim3(gr), dim3(b), 0, s, A);
+  launch_kernel(k, dim3(gr), dim3(b), 0, s, A);
 }
 #define TE_LAUNCH_COLUMNS(name) \
   static void launch_##name(const KArgs& A, cudaStream_t s) { launch_columns(k_##name, A, s); }
@@ -1004,7 +958,6 @@ static void launch_columns(void (*k)(KArgs), const KArgs& A, cudaStream_t s) {
 // mp_pdefq.wgsl: per column, q below rmax set to 0 and the column rescaled so that
 // sum rho q keeps its value before the clip ((t1 + 1e-20) / (t2 + 1e-20), 1 if negative)
 __global__ void k_mp_pdefq(KArgs A) {
-  grid_dep_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const Dims& g = A.g;
@@ -1029,7 +982,9 @@ __global__ void k_mp_pdefq(KArgs A) {
   if (t3 < 0.0f) t3 = 1.0f;
   for (int k = 0; k < g.nz; k++) q[base + k * sk] = q[base + k * sk] * t3;
 }
+#ifndef TE_KERNELS_FAST
 TE_LAUNCH_COLUMNS(mp_pdefq)
+#endif
 
 // turb_scalar_vert_implicit.wgsl: subgrid tendency of a scalar s.  sten gains
 // ((fx, fy divergence) + turbz) rr at every level; turbz is the explicit vertical flux
@@ -1066,7 +1021,6 @@ struct TsviCol {
 };
 
 __global__ void k_turb_scalar_vert_implicit(KArgs A) {
-  grid_dep_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const Dims& g = A.g;
@@ -1134,12 +1088,195 @@ __global__ void k_turb_scalar_vert_implicit(KArgs A) {
     col.tend(c, (rho[c] * (snew - s[c])) * rdt);
   }
 }
+#ifdef TE_KERNELS_FAST
+// Column solves in the __restrict__ build (no bound region overlaps another): a block per
+// 32 columns.  Its 8 warps build the tridiagonal rows of all levels in parallel (warp w:
+// levels w, w + 8, ...; lanes on consecutive columns), one warp runs the Thomas sweep and
+// back-substitution of the 32 columns from shared memory (coop_thomas), and the 8 warps
+// then form the tendencies level-parallel.  Every value is computed by the operations of
+// the one-thread-per-column kernel, and the recurrence in its order, so every written word
+// is the same; the one-thread-per-column kernels walk 40-80 dependent levels per column.
+enum { kCoopCols = 32, kCoopWarps = 8 };
+
+// Thomas sweep over levels klo..khi of a block's 32 columns.  Row k: sA = sub-diagonal
+// coefficient (k > klo), sC = super-diagonal (k < khi), sD = right-hand side; the diagonal
+// is 1 - sA - sC as the reference forms it.  Writes the forward coefficient cA (levels
+// klo..khi-1) and the solution into cB (levels klo..khi), in memory and in scA / scB.
+__device__ __forceinline__ void coop_thomas(const float* sA, const float* sC, const float* sD, float* scA, float* scB,
+                                            int klo, int khi, int lane, float* TE_R cA, float* TE_R cB, int base, int sk) {
+  int e = klo * kCoopCols + lane;
+  float t = dcr(1.0f, 1.0f - sC[e]);
+  float a = (-sC[e]) * t, b = sD[e] * t;
+  scA[e] = a;
+  scB[e] = b;
+  cA[base + klo * sk] = a;
+  for (int k = klo + 1; k < khi; k++) {
+    e = k * kCoopCols + lane;
+    const float cfa = sA[e], cfc = sC[e];
+    t = dcr(1.0f, fmaf(cfa, a, (1.0f - cfa) - cfc));
+    a = (-cfc) * t;
+    b = fmaf(-cfa, b, sD[e]) * t;
+    scA[e] = a;
+    scB[e] = b;
+    cA[base + k * sk] = a;
+  }
+  e = khi * kCoopCols + lane;
+  const float cfa = sA[e];
+  t = dcr(1.0f, fmaf(cfa, a, 1.0f - cfa));
+  b = fmaf(-cfa, b, sD[e]) * t;
+  scB[e] = b;
+  cB[base + khi * sk] = b;
+  for (int k = khi - 1; k >= klo; k--) {
+    e = k * kCoopCols + lane;
+    b = fmaf(scA[e], b, scB[e]);
+    scB[e] = b;
+    cB[base + k * sk] = b;
+  }
+}
+
+struct CoopCol {
+  int lane, wq, i, j, base, sk;
+  bool on;
+  float *sA, *sC, *sD, *scA, *scB;
+};
+
+// the block's column (lane): cx x cy columns of the dispatch, x fastest
+__device__ __forceinline__ CoopCol coop_col(const KArgs& A, float* smem, int cx, int cy) {
+  CoopCol q;
+  const Dims& g = A.g;
+  const int nz = g.nz;
+  q.lane = threadIdx.x & 31;
+  q.wq = threadIdx.x >> 5;
+  const int col = blockIdx.x * kCoopCols + q.lane;
+  q.i = col % cx;
+  q.j = col / cx;
+  q.on = col < cx * cy && q.i < A.gx && q.j < A.gy;
+  q.sk = g.sJ * g.sK;
+  q.base = gidx(g, q.on ? q.i : 0, q.on ? q.j : 0, 0);
+  q.sA = smem;
+  q.sC = smem + nz * kCoopCols;
+  q.sD = smem + 2 * nz * kCoopCols;
+  q.scA = smem + 3 * nz * kCoopCols;
+  q.scB = smem + 4 * nz * kCoopCols;
+  return q;
+}
+
+static size_t coop_bytes(int nz) { return (size_t)5 * nz * kCoopCols * sizeof(float); }
+
+template <class K>
+static void launch_coop(K kernel, const KArgs& A, cudaStream_t st, int cx, int cy) {
+  const size_t bytes = coop_bytes(A.g.nz);
+  if (A.gx <= 0 || A.gy <= 0 || A.gz <= 0) return;
+  if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  launch_kernel(kernel, dim3((cx * cy + kCoopCols - 1) / kCoopCols), dim3(kCoopCols * kCoopWarps), bytes, st, A);
+}
+
+// mp_pdefq: the column sums run by one warp from shared memory in the reference's order,
+// the clipped and rescaled q stored level-parallel
+__global__ void __launch_bounds__(kCoopCols * kCoopWarps) k_pdefq_coop(KArgs A) {
+  extern __shared__ float tsm[];
+  const Dims& g = A.g;
+  const int nz = g.nz;
+  const CoopCol cq = coop_col(A, tsm, g.nx, g.ny);
+  const float* TE_R rho = A.p[1];
+  float* TE_R q = A.p[2];
+  const float rmax = A.f[3];
+  if (cq.on)
+    for (int k = cq.wq; k < nz; k += kCoopWarps) {
+      const int c = cq.base + k * cq.sk, e = k * kCoopCols + cq.lane;
+      cq.sA[e] = rho[c];
+      cq.sC[e] = q[c];
+    }
+  __syncthreads();
+  if (cq.wq == 0 && cq.on) {
+    float t1 = 0.0f, t2 = 0.0f;
+    for (int k = 0; k < nz; k++) {
+      const int e = k * kCoopCols + cq.lane;
+      const float r = cq.sA[e];
+      float v = cq.sC[e];
+      t1 = fmaf(r, v, t1);
+      if (v < rmax) {
+        v = 0.0f;
+        cq.sC[e] = 0.0f;
+      }
+      t2 = fmaf(r, v, t2);
+    }
+    float t3 = dcr(t1 + 1e-20f, t2 + 1e-20f);
+    if (t3 < 0.0f) t3 = 1.0f;
+    cq.sD[cq.lane] = t3;
+  }
+  __syncthreads();
+  if (!cq.on) return;
+  const float t3 = cq.sD[cq.lane];
+  for (int k = cq.wq; k < nz; k += kCoopWarps) q[cq.base + k * cq.sk] = cq.sC[k * kCoopCols + cq.lane] * t3;
+}
+
+static void launch_mp_pdefq(const KArgs& A, cudaStream_t st) {
+  if (A.g.nz < 1 || coop_bytes(A.g.nz) > 200 * 1024) {
+    launch_columns(k_mp_pdefq, A, st);
+    return;
+  }
+  launch_coop(k_pdefq_coop, A, st, A.g.nx, A.g.ny);
+}
+
+// turb_scalar_vert_implicit, implicit branch
+__global__ void __launch_bounds__(kCoopCols * kCoopWarps) k_tsvi_coop(KArgs A) {
+  extern __shared__ float tsm[];
+  const Dims& g = A.g;
+  const int nz = g.nz;
+  const CoopCol q = coop_col(A, tsm, g.nx, g.ny);
+  const int sk = q.sk, base = q.base;
+  const float *TE_R s = A.p[1], *TE_R rho = A.p[2], *TE_R rr = A.p[3], *TE_R rf = A.p[4], *TE_R khv = A.p[5];
+  const float *TE_R mh = A.p[6], *TE_R mf = A.p[7];
+  const float dt = A.f[10];
+  const int useFlux = A.iv[15], bcturbs = A.iv[18];
+  const float tema = ((-dt) * g.rdz) * g.rdz, temc = dt * g.rdz;
+  if (q.on)
+    for (int k = q.wq; k < nz; k += kCoopWarps) {
+      const int c = base + k * sk, e = k * kCoopCols + q.lane;
+      if (k < nz - 1) q.sC[e] = tema * ((((khv[c + sk] * mf[k + 1]) * rf[c + sk]) * mh[k]) * rr[c]);
+      if (k > 0) q.sA[e] = tema * ((((khv[c] * mf[k]) * rf[c]) * mh[k]) * rr[c]);
+      float d = s[c];
+      if (k == 0 && (useFlux != 0 || bcturbs == 2)) {
+        const int c1 = base + sk;
+        const float dumz = useFlux != 0 ? A.p[14][base] * rf[base] : ((((-khv[c1]) * (s[c1] - s[base])) * g.rdz) * mf[1]) * rf[c1];
+        d = fmaf((temc * dumz) * mh[0], rr[base], s[base]);
+      } else if (k == nz - 1 && bcturbs == 2) {
+        const float dumz = ((((-khv[c]) * (s[c] - s[c - sk])) * g.rdz) * mf[k]) * rf[c];
+        d = fmaf(-((temc * dumz) * mh[k]), rr[c], s[c]);
+      }
+      q.sD[e] = d;
+    }
+  __syncthreads();
+  if (q.wq == 0 && q.on) coop_thomas(q.sA, q.sC, q.sD, q.scA, q.scB, 0, nz - 1, q.lane, A.p[11], A.p[12], base, sk);
+  __syncthreads();
+  if (!q.on) return;
+  const float rdt = dcr(1.0f, dt);
+  const float uh = hm_uh(g, A.p[30], q.i), vh = hm_vh(g, A.p[30], q.j);
+  const float *TE_R fx = A.p[8], *TE_R fy = A.p[9];
+  float* TE_R sten = A.p[13];
+  for (int k = q.wq; k < nz; k += kCoopWarps) {
+    const int c = base + k * sk;
+    const float snew = q.scB[k * kCoopCols + q.lane];
+    const float h = ((-(fx[c + 1] - fx[c])) * g.rdx) * uh + ((-(fy[c + g.sJ] - fy[c])) * g.rdy) * vh;
+    sten[c] = fmaf(h + (rho[c] * (snew - s[c])) * rdt, rr[c], sten[c]);
+  }
+}
+
+static void launch_turb_scalar_vert_implicit(const KArgs& A, cudaStream_t st) {
+  if (A.iv[16] != 0 || A.g.nz < 2 || coop_bytes(A.g.nz) > 200 * 1024) {  // explicit branch, degenerate columns
+    launch_columns(k_turb_scalar_vert_implicit, A, st);
+    return;
+  }
+  launch_coop(k_tsvi_coop, A, st, A.g.nx, A.g.ny);
+}
+#else
 TE_LAUNCH_COLUMNS(turb_scalar_vert_implicit)
+#endif
 
 // rayleigh_damping.wgsl: -rdalpha tau (phi - phi_ref) for u, v, th (profiles, or level
 // averages when toAverage) and -rdalpha tauf w, tauf raised to the lateral sponge
 __global__ void k_rayleigh_damping(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const int i = tx, j = ty, k = tz;
   if (i > g.nx || j > g.ny || k > g.nz) return;
@@ -1170,7 +1307,6 @@ TE_LAUNCH3(rayleigh_damping)
 // turb_rho_faces.wgsl: rr = 1 / rho (k < nz); rf on w levels, interior c1/c2 weights,
 // bottom and top extrapolated with cgs / cgt; columns -2..nx+1, rows -2..ny+1
 __global__ void k_turb_rho_faces(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const int i = tx - 2, j = ty - 2, k = tz;
   if (i > g.nx + 1 || j > g.ny + 1 || k > g.nz) return;
@@ -1196,7 +1332,6 @@ TE_LAUNCH3(turb_rho_faces)
 // turb_def_centers.wgsl: rho-weighted strain rates s11, s22, s33 at cell centres and s12
 // at the (i-1/2, j-1/2) edges; columns -1..nx+1, rows -1..ny+1
 __global__ void k_turb_def_centers(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const int i = tx - 1, j = ty - 1, k = tz;
   if (i > g.nx + 1 || j > g.ny + 1 || k >= g.nz) return;
@@ -1212,7 +1347,6 @@ TE_LAUNCH3(turb_def_centers)
 
 // turb_def_faces.wgsl: s13, s23 on w levels 1..nz-1 at the x and y faces
 __global__ void k_turb_def_faces(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const int i = tx, j = ty, k = tz + 1;
   if (i > g.nx + 1 || j > g.ny + 1 || k > g.nz - 1) return;
@@ -1227,7 +1361,6 @@ TE_LAUNCH3(turb_def_faces)
 // turb_def_assemble.wgsl: defv = 4 (t13 + t23) / rf^2, defh = (2 (t11 + t22 + t33) + 4 t12)
 // / rf^2 on w levels 1..nz-1 (squared rates interpolated by c1/c2, edge/face averages)
 __global__ void k_turb_def_assemble(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const int i = tx, j = ty, k = tz + 1;
   if (i >= g.nx || j >= g.ny || k > g.nz - 1) return;
@@ -1253,7 +1386,6 @@ TE_LAUNCH3(turb_def_assemble)
 // average of kmh, t13 / t23 by the face sums of kmv (levels 1..nz-1, i, j >= 0); the
 // dispatch covers columns and rows -1..n
 __global__ void k_turb_gettau(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const int i = tx - 1, j = ty - 1, k = tz;
   if (i > g.nx || j > g.ny || k >= g.nz) return;
@@ -1278,7 +1410,6 @@ TE_LAUNCH3(turb_gettau)
 // length (limited by c_l sqrt(tke / N^2) in stable air), dissipation added to dissten,
 // km = cmz sqrt(tke) len kmScale (or kmFixed > 0), kh = km min(1 + 2 len / scale, 3)
 __global__ void k_turb_km_kh(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const int i = tx, j = ty, k = tz + 1;
   if (i >= g.nx || j >= g.ny || k > g.nz - 1) return;
@@ -1323,7 +1454,6 @@ TE_LAUNCH3(turb_km_kh)
 // tke_epst.wgsl: shear production on w levels 1..nz-1, stresses times strain rates
 // interpolated (c1/c2) or averaged to the w point, divided by rf
 __global__ void k_tke_epst(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const int i = tx, j = ty, k = tz + 1;
   if (i >= g.nx || j >= g.ny || k > g.nz - 1) return;
@@ -1367,7 +1497,6 @@ __device__ __forceinline__ float mp_rs(float p, float t, float a, float b) {
 // moist: g dln(thv)/dz, or in saturated air (liquid above 0 C, ice below -40 C, a linear
 // blend between) the moist-adiabatic form (lam_1); sat marks saturated points
 __global__ void k_turb_nm(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const int i = tx, j = ty, k = tz + 1;
   if (i >= g.nx || j >= g.ny || k > g.nz - 1) return;
@@ -1456,7 +1585,6 @@ TE_LAUNCH3(turb_nm)
 // 2 drag coefficient 0.001229 with the surface wind speed (plane 2 of sfc); 3 drag against
 // the domain-mean wind (planes 14..16 at the origin, lam_1); else u*^2 w1 / max(s1, 0.01)
 __global__ void k_turb_sfcstress(KArgs A) {
-  grid_dep_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const Dims& g = A.g;
@@ -1514,7 +1642,6 @@ static void launch_turb_sfcstress(const KArgs& A, cudaStream_t s) { launch_colum
 // (moist); the dissipation averaged to the cell centre, at the surface with bbc3
 // u*^3 ln((dz1 + z0) / z0) / (k dz1)
 __global__ void k_turb_dissipative_heating(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const int i = tx, j = ty, k = tz;
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
@@ -1553,7 +1680,6 @@ TE_LAUNCH3(turb_dissipative_heating)
 // (dw/dy) cross term dwd.  s is the offset of the staggered neighbour (1 or strideJ).
 template <int AX>
 __global__ void k_turb_uv_tendency(KArgs A) {
-  grid_dep_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const Dims& g = A.g;
@@ -1626,8 +1752,76 @@ __global__ void k_turb_uv_tendency(KArgs A) {
     ten[c] = fmaf(horiz(c) + turbz, rinv(k), ten[c]);
   }
 }
+#ifdef TE_KERNELS_FAST
+// implicit branch of turb_u_tendency / turb_v_tendency, a block per 32 columns (coop_thomas)
+template <int AX>
+__global__ void __launch_bounds__(kCoopCols * kCoopWarps) k_turb_uv_coop(KArgs A) {
+  extern __shared__ float tsm[];
+  const Dims& g = A.g;
+  const int nz = g.nz;
+  const CoopCol q = coop_col(A, tsm, g.nx + (AX == 0), g.ny + (AX == 1));
+  const int i = q.i, j = q.j;
+  const bool on = q.on;
+  const float *TE_R X = A.p[1], *TE_R w = A.p[2], *TE_R rho = A.p[3], *TE_R rf = A.p[4], *TE_R kmv = A.p[5];
+  const float *TE_R A1 = A.p[6], *TE_R A2 = A.p[7], *TE_R A3 = A.p[8], *TE_R mh = A.p[9], *TE_R mf = A.p[10];
+  const float* TE_R hm = A.p[30];
+  float *TE_R dwd = A.p[14], *TE_R ten = A.p[15];
+  const float dt = A.f[11];
+  const int sj = g.sJ, sk = q.sk, s = AX == 0 ? 1 : sj, base = q.base;
+  const float tema = (((-0.0625f) * dt) * g.rdz) * g.rdz, temc = (0.5f * dt) * g.rdz;
+  auto rinv = [&](int k) { return dcr(1.0f, 0.5f * (rho[base + k * sk - s] + rho[base + k * sk])); };
+  auto lam1 = [&](int k, int lev) {
+    const int cl = base + lev * sk;
+    return (((kmv[cl - s] + kmv[cl]) * (mf[lev] + mf[lev])) * (rf[cl - s] + rf[cl])) * ((mh[k] + mh[k]) * rinv(k));
+  };
+  if (on) {
+    for (int k = q.wq; k <= nz; k += kCoopWarps) {
+      const int c = base + k * sk;
+      const float dwx = AX == 0 ? ((w[c] - w[c - 1]) * g.rdx) * hm_uf(g, hm, i) : ((w[c] - w[c - sj]) * g.rdy) * hm_vf(g, hm, j);
+      dwd[c] = ((dwx * 0.25f) * (kmv[c - s] + kmv[c])) * (rf[c - s] + rf[c]);
+      if (k == nz) continue;
+      const int e = k * kCoopCols + q.lane;
+      if (k < nz - 1) q.sC[e] = tema * lam1(k, k + 1);
+      if (k > 0) q.sA[e] = tema * lam1(k, k);
+      float d = X[c];
+      if (k == 0) d = fmaf(-((temc * A3[base]) * (mh[0] + mh[0])), rinv(0), X[base]);
+      else if (k == nz - 1) d = fmaf((temc * A3[base + nz * sk]) * (mh[k] + mh[k]), rinv(k), X[c]);
+      q.sD[e] = d;
+    }
+  }
+  __syncthreads();
+  if (q.wq == 0 && on) coop_thomas(q.sA, q.sC, q.sD, q.scA, q.scB, 0, nz - 1, q.lane, A.p[12], A.p[13], base, sk);
+  __syncthreads();
+  if (!on) return;
+  const bool zeroX = A.iv[16] != 0 && (i == 0 || i == (AX == 0 ? g.nx : g.nx - 1));
+  const bool zeroY = A.iv2[16] != 0 && (j == 0 || j == (AX == 0 ? g.ny - 1 : g.ny));
+  const float rdt = dcr(0.5f, dt);
+  for (int k = q.wq; k < nz; k += kCoopWarps) {
+    const int c = base + k * sk;
+    const float tx = zeroX ? 0.0f
+                           : (AX == 0 ? ((A1[c] - A1[c - 1]) * g.rdx) * hm_uf(g, hm, i) : ((A1[c + 1] - A1[c]) * g.rdx) * hm_uh(g, hm, i));
+    const float ty = zeroY ? 0.0f
+                           : (AX == 0 ? ((A2[c + sj] - A2[c]) * g.rdy) * hm_vh(g, hm, j) : ((A2[c] - A2[c - sj]) * g.rdy) * hm_vf(g, hm, j));
+    float turbz = ((rho[c - s] + rho[c]) * (q.scB[k * kCoopCols + q.lane] - X[c])) * rdt;
+    turbz = fmaf(((dwd[c + sk] - dwd[c]) * g.rdz) * 0.5f, mh[k] + mh[k], turbz);
+    ten[c] = fmaf((tx + ty) + turbz, rinv(k), ten[c]);
+  }
+}
+
+template <int AX>
+static void launch_turb_uv(const KArgs& A, cudaStream_t st) {
+  if (A.iv[17] != 0 || A.g.nz < 2 || coop_bytes(A.g.nz) > 200 * 1024) {
+    launch_columns(k_turb_uv_tendency<AX>, A, st);
+    return;
+  }
+  launch_coop(k_turb_uv_coop<AX>, A, st, A.g.nx + (AX == 0), A.g.ny + (AX == 1));
+}
+static void launch_turb_u_tendency(const KArgs& A, cudaStream_t s) { launch_turb_uv<0>(A, s); }
+static void launch_turb_v_tendency(const KArgs& A, cudaStream_t s) { launch_turb_uv<1>(A, s); }
+#else
 static void launch_turb_u_tendency(const KArgs& A, cudaStream_t s) { launch_columns(k_turb_uv_tendency<0>, A, s); }
 static void launch_turb_v_tendency(const KArgs& A, cudaStream_t s) { launch_columns(k_turb_uv_tendency<1>, A, s); }
+#endif
 
 // turb_w_tendency.wgsl (TKE 0) and tke_transport.wgsl (TKE 1): tendency of a w-level
 // quantity q on levels 1..nz-1 per column.  Horizontal divergence (w: of t13, t23; TKE: of
@@ -1636,7 +1830,6 @@ static void launch_turb_v_tendency(const KArgs& A, cudaStream_t s) { launch_colu
 // right-hand side), tendency rf (new - old) / dt.
 template <int TKE>
 __global__ void k_turb_wlevel(KArgs A) {
-  grid_dep_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const Dims& g = A.g;
@@ -1719,8 +1912,69 @@ __global__ void k_turb_wlevel(KArgs A) {
     ten[c] = ten[c] + dcr(horiz(c) + turbz, rf[c]);
   }
 }
+#ifdef TE_KERNELS_FAST
+// implicit branch of turb_w_tendency (TKE 0) / tke_transport (TKE 1) over w levels
+// 1..nz-1, a block per 32 columns (coop_thomas)
+template <int TKE>
+__global__ void __launch_bounds__(kCoopCols * kCoopWarps) k_turb_wlevel_coop(KArgs A) {
+  extern __shared__ float tsm[];
+  const Dims& g = A.g;
+  const int nz = g.nz;
+  const CoopCol cq = coop_col(A, tsm, g.nx, g.ny);
+  const int i = cq.i, j = cq.j, sj = g.sJ, sk = cq.sk, base = cq.base;
+  const float *TE_R q = A.p[1], *TE_R rho = A.p[2], *TE_R rf = A.p[3], *TE_R kmh = A.p[4];
+  const float *TE_R kmv = TKE ? A.p[5] : nullptr, *TE_R h1 = TKE ? A.p[11] : A.p[5], *TE_R h2 = TKE ? A.p[12] : A.p[6];
+  const float *TE_R t33 = TKE ? nullptr : A.p[7], *TE_R mh = TKE ? A.p[6] : A.p[8], *TE_R mf = TKE ? A.p[7] : A.p[9];
+  const float* TE_R hm = A.p[30];
+  float* TE_R ten = A.p[13];
+  const float dt = TKE ? A.f[8] : A.f[10];
+  const float tema = (((-1.0f) * dt) * g.rdz) * g.rdz, temc = dt * g.rdz;
+  auto mfr = [&](int k) { return dcr(mf[k], rf[base + k * sk]); };
+  if (cq.on)
+    for (int k = 1 + cq.wq; k <= nz - 1; k += kCoopWarps) {
+      const int c = base + k * sk, e = k * kCoopCols + cq.lane;
+      if (k < nz - 1) cq.sC[e] = tema * ((((kmh[c] + kmh[c + sk]) * mh[k]) * rho[c]) * mfr(k));
+      if (k > 1) cq.sA[e] = tema * ((((kmh[c - sk] + kmh[c]) * mh[k - 1]) * rho[c - sk]) * mfr(k));
+      float d = q[c];
+      if (k == 1)
+        d = TKE ? fmaf(temc * ((((-(kmv[c - sk] + kmv[c])) * (q[c] - q[c - sk])) * g.rdz) * mh[0]) * rho[c - sk], mfr(1), q[c])
+                : fmaf(-(temc * t33[c - sk]), mfr(1), q[c]);
+      else if (k == nz - 1)
+        d = TKE ? fmaf(-(temc * (((((-(kmv[c] + kmv[c + sk])) * (q[c + sk] - q[c])) * g.rdz) * mh[k]) * rho[c])), mfr(k), q[c])
+                : fmaf(temc * t33[c], mfr(k), q[c]);
+      cq.sD[e] = d;
+    }
+  __syncthreads();
+  float* TE_R cA = TKE ? A.p[9] : A.p[11];
+  float* TE_R cB = TKE ? A.p[10] : A.p[12];
+  if (cq.wq == 0 && cq.on) coop_thomas(cq.sA, cq.sC, cq.sD, cq.scA, cq.scB, 1, nz - 1, cq.lane, cA, cB, base, sk);
+  __syncthreads();
+  if (!cq.on) return;
+  const bool zeroX = A.iv[14] != 0 && (i == 0 || i == g.nx - 1), zeroY = A.iv2[14] != 0 && (j == 0 || j == g.ny - 1);
+  const float rdt = dcr(1.0f, dt);
+  for (int k = 1 + cq.wq; k <= nz - 1; k += kCoopWarps) {
+    const int c = base + k * sk;
+    const float tx = zeroX ? 0.0f : (TKE ? ((-(h1[c + 1] - h1[c])) * g.rdx) * hm_uh(g, hm, i) : ((h1[c + 1] - h1[c]) * g.rdx) * hm_uh(g, hm, i));
+    const float ty = zeroY ? 0.0f : (TKE ? ((-(h2[c + sj] - h2[c])) * g.rdy) * hm_vh(g, hm, j) : ((h2[c + sj] - h2[c]) * g.rdy) * hm_vh(g, hm, j));
+    const float turbz = (rf[c] * (cq.scB[k * kCoopCols + cq.lane] - q[c])) * rdt;
+    ten[c] = ten[c] + dcr((tx + ty) + turbz, rf[c]);
+  }
+}
+
+template <int TKE>
+static void launch_turb_wlevel(const KArgs& A, cudaStream_t st) {
+  if (A.iv[15] != 0 || A.g.nz < 3 || coop_bytes(A.g.nz) > 200 * 1024) {
+    launch_columns(k_turb_wlevel<TKE>, A, st);
+    return;
+  }
+  launch_coop(k_turb_wlevel_coop<TKE>, A, st, A.g.nx, A.g.ny);
+}
+static void launch_turb_w_tendency(const KArgs& A, cudaStream_t s) { launch_turb_wlevel<0>(A, s); }
+static void launch_tke_transport(const KArgs& A, cudaStream_t s) { launch_turb_wlevel<1>(A, s); }
+#else
 static void launch_turb_w_tendency(const KArgs& A, cudaStream_t s) { launch_columns(k_turb_wlevel<0>, A, s); }
 static void launch_tke_transport(const KArgs& A, cudaStream_t s) { launch_columns(k_turb_wlevel<1>, A, s); }
+#endif
 
 // Two-float accumulation of the mass sums (f_df_add / f_df_add_pair, mass_row_sums.wgsl):
 // acc.x + x by an error-free sum, the error accumulated in acc.y.  The sums run in the
@@ -1739,7 +1993,6 @@ __device__ __forceinline__ void df_add_pair(F2& acc, float vx, float vy) {
 // mass_row_sums.wgsl: per (j, k) row the sums over i of rho / (uh vh mh) (rows1) and of
 // pi0 + pp3d (rows2), stored as pairs at k strideK + j
 __global__ void k_mass_row_sums(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const int j = tx, k = ty;
   if (j >= g.ny || k >= g.nz) return;
@@ -1763,7 +2016,6 @@ TE_LAUNCH3(mass_row_sums)
 
 // mass_level_sums.wgsl: per level the sums over j of the row pairs
 __global__ void k_mass_level_sums(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const int k = tx;
   if (ty != 0 || k >= g.nz) return;
@@ -1784,7 +2036,6 @@ TE_LAUNCH3(mass_level_sums)
 // mass_reference_init.wgsl: on its first run (ref[2] == 0) thread 0 stores the total mass
 // (the sum of the level pairs) as the reference and sets ref[2] = 1
 __global__ void k_mass_reference_init(KArgs A) {
-  grid_dep_wait();
   TE_K3
   if (tx != 0 || ty != 0) return;
   const float* TE_R levels1 = A.p[1];
@@ -1803,7 +2054,6 @@ TE_LAUNCH3(mass_reference_init)
 // builtin for |r| > 0.05, else its third-order expansion), added to pp3d; prs and rho from
 // the corrected pi; thread (0,0,0) records tem, the mass, the pi sum, r and the mass's low part
 __global__ void k_mass_correction_apply(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const int i = tx, j = ty, k = tz;
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
@@ -1844,7 +2094,6 @@ TE_LAUNCH3(mass_correction_apply)
 // morr_prep.wgsl: temperature T = (th0 + th)(pi0 + pp) and a copy qv0 of qv before the
 // microphysics column
 __global__ void k_morr_prep(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const int i = tx, j = ty, k = tz;
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
@@ -1857,7 +2106,6 @@ TE_LAUNCH3(morr_prep)
 // morr_post.wgsl: where the column changed T (by >= 1e-4) or qv (by >= 1e-14), pressure
 // from the equation of state, pi' from it (the reference's correctly rounded pow) and th
 __global__ void k_morr_post(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const int i = tx, j = ty, k = tz;
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
@@ -1882,7 +2130,6 @@ TE_LAUNCH3(morr_post)
 // -------------------------------------------------- thermodynamic glue
 
 __global__ void k_update_diagnostics_moist(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const float *TE_R thp = A.p[1], *TE_R ppp = A.p[2], *TE_R th0 = A.p[3], *TE_R pi0 = A.p[4], *TE_R qv0 = A.p[5], *TE_R qc0 = A.p[6];
   const float *TE_R qi0 = A.p[7], *TE_R rth0 = A.p[8], *TE_R qv = A.p[9], *TE_R qc = A.p[10], *TE_R qr = A.p[11], *TE_R qi = A.p[12];
@@ -1912,7 +2159,6 @@ __global__ void k_update_diagnostics_moist(KArgs A) {
 TE_LAUNCH3(update_diagnostics_moist)
 
 __global__ void k_pressure_tendency(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const float *TE_R th = A.p[1], *TE_R qv = A.p[2], *TE_R rho = A.p[3], *TE_R ppi = A.p[4], *TE_R thten = A.p[5], *TE_R qpten = A.p[6];
   const float *TE_R th0 = A.p[7], *TE_R pi0 = A.p[8];
@@ -1955,7 +2201,6 @@ __global__ void k_pressure_tendency(KArgs A) {
 TE_LAUNCH3(pressure_tendency)
 
 __global__ void k_divergence3d(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const float *TE_R u = A.p[1], *TE_R v = A.p[2], *TE_R w = A.p[3], *TE_R mh = A.p[4];
   float* TE_R div = A.p[5];
@@ -1971,7 +2216,6 @@ __global__ void k_divergence3d(KArgs A) {
 TE_LAUNCH3(divergence3d)
 
 __global__ void k_update_rho_prs(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const int moist = A.iv[1];
   const float *TE_R thp = A.p[2], *TE_R ppp = A.p[3], *TE_R th0 = A.p[4], *TE_R pi0 = A.p[5], *TE_R qv = A.p[6];
@@ -1990,7 +2234,6 @@ __global__ void k_update_rho_prs(KArgs A) {
 TE_LAUNCH3(update_rho_prs)
 
 __global__ void k_diabatic_unapply(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const float dt = A.f[1];
   float *TE_R pp3d = A.p[2], *TE_R th = A.p[3], *TE_R qv = A.p[4], *TE_R qc = A.p[5];
@@ -2015,7 +2258,6 @@ __global__ void k_diabatic_unapply(KArgs A) {
 TE_LAUNCH3(diabatic_unapply)
 
 __global__ void k_diabatic_rates(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const float dt = A.f[1];
   const float *TE_R pp3d = A.p[2], *TE_R th = A.p[3], *TE_R qv = A.p[4], *TE_R qc = A.p[5];
@@ -2032,7 +2274,6 @@ __global__ void k_diabatic_rates(KArgs A) {
 TE_LAUNCH3(diabatic_rates)
 
 __global__ void k_ppx_finish(KArgs A) {
-  grid_dep_wait();
   TE_K3
   const float* TE_R pp3d = A.p[1];
   float* TE_R ppx = A.p[2];

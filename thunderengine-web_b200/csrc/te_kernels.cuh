@@ -42,21 +42,15 @@ struct KernelSpec {
   LaunchFn launch;
 };
 
-// Launches kernel k with the programmatic-stream-serialization attribute (see
-// grid_dep_wait): inside a captured step graph the launch becomes a programmatic edge, so
-// the next grid is scheduled while the previous one drains.
+// Launches kernel k on stream s (cudaLaunchKernelEx: one call for every kernel of the
+// library, dynamic shared memory included).
 template <typename... P, typename... Args>
-inline cudaError_t launch_pdl(void (*k)(P...), dim3 gr, dim3 b, size_t smem, cudaStream_t s, Args... a) {
+inline cudaError_t launch_kernel(void (*k)(P...), dim3 gr, dim3 b, size_t smem, cudaStream_t s, Args... a) {
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = gr;
   cfg.blockDim = b;
   cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
   return cudaLaunchKernelEx(&cfg, k, a...);
 }
 

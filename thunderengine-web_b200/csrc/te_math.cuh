@@ -29,16 +29,6 @@ __host__ __device__ __forceinline__ int gidx(const Dims& g, int i, int j, int k)
 // quotient, and the 2^64 pre-scaling of tiny numerators cancels exactly.
 __device__ __forceinline__ float dcr(float a, float b) { return a / b; }
 
-// Programmatic dependent launch (sm_90+): every kernel of the library begins with this
-// wait, which returns once the previous kernel on the stream has completed and its writes
-// are visible; kernels launched with launch_pdl may therefore be scheduled while that
-// kernel drains, and stream order is kept.  Without the launch attribute it returns at once.
-__device__ __forceinline__ void grid_dep_wait() {
-#ifdef __CUDA_ARCH__
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-#endif
-}
-
 // WGSL min/max on f32: min(a,b) = b if b < a else a; max(a,b) = b if a < b else a;
 // a NaN operand yields the other one (fixes the sign of zero on +0/-0 ties).
 __device__ __forceinline__ float wmin(float a, float b) { return (b < a || a != a) ? b : a; }

@@ -66,7 +66,6 @@ static std::string signature(const JValue& cmds) {
 }
 
 __global__ void k_region_hash(const uint32_t* __restrict__ M, uint64_t off, uint64_t len, uint32_t* H, uint32_t slot) {
-  grid_dep_wait();
   // Reference region hash (replay.js:407-418): sum over i of mix(M[off+i] ^ i*0x9E3779B1).
   uint32_t s = 0;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -750,7 +749,7 @@ void Plan::launch_exact(std::vector<Op>& ops, int first, int last, bool hashes) 
     if (hashes) {
       for (auto& h : o.hashes) {
         if (!h.bound || !h.len) continue;
-        launch_pdl(k_region_hash, dim3(64), dim3(256), 0, stream, M, h.off, h.len, H, h.slot);
+        launch_kernel(k_region_hash, dim3(64), dim3(256), 0, stream, M, h.off, h.len, H, h.slot);
       }
     }
   }
