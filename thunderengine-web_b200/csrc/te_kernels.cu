@@ -626,11 +626,14 @@ __global__ void k_acoustic_w_solve(KArgs A) {
     w[c] = fmaf(cA[c], w[c + sk], cB[c]);
   }
 }
-static void launch_acoustic_w_solve(const KArgs& A, cudaStream_t s) {
+static void launch_acoustic_w_solve_columns(const KArgs& A, cudaStream_t s) {
   dim3 b(32, 4, 1);
   dim3 gr((A.gx + 31) / 32, (A.gy + 3) / 4, 1);
   launch_kernel(k_acoustic_w_solve, dim3(gr), dim3(b), 0, s, A);
 }
+#ifndef TE_KERNELS_FAST
+static void launch_acoustic_w_solve(const KArgs& A, cudaStream_t s) { launch_acoustic_w_solve_columns(A, s); }
+#endif
 
 __global__ void k_acoustic_pp(KArgs A) {
   TE_K3
@@ -1217,6 +1220,81 @@ static void launch_mp_pdefq(const KArgs& A, cudaStream_t st) {
     return;
   }
   launch_coop(k_pdefq_coop, A, st, A.g.nx, A.g.ny);
+}
+
+// acoustic_w_solve: the rows (aa, bb, cc, dd of every w level) level-parallel, the
+// Thomas sweep and back-substitution of the 32 columns by one warp from shared memory
+__global__ void __launch_bounds__(kCoopCols * kCoopWarps) k_wsolve_coop(KArgs A) {
+  extern __shared__ float tsm[];
+  const Dims& g = A.g;
+  const int nz = g.nz;
+  const CoopCol q = coop_col(A, tsm, g.nx, g.ny);
+  float* sB = tsm + 5 * nz * kCoopCols;
+  const Acoustic a = A.a;
+  const float asq = a.alph * a.alph;
+  const float *TE_R pk1 = A.p[2], *TE_R pk2 = A.p[3], *TE_R qk = A.p[4], *TE_R mm = A.p[5], *TE_R fpk = A.p[6];
+  const float *TE_R wten = A.p[7], *TE_R pp3d = A.p[8];
+  float *TE_R w = A.p[9], *TE_R cA = A.p[10], *TE_R cB = A.p[11];
+  const int sk = q.sk, base = q.base;
+  if (q.on)
+    for (int k = 1 + q.wq; k <= nz - 1; k += kCoopWarps) {
+      const int c = base + k * sk, cm = c - sk, e = k * kCoopCols + q.lane;
+      const float m = mm[c];
+      q.sA[e] = (-asq) * (m * (pk1[cm] + qk[cm]));
+      q.sC[e] = (-asq) * ((-m) * (pk2[c] - qk[c]));
+      sB[e] = fmaf(-asq, m * ((-(pk1[c] + qk[c])) + (pk2[cm] - qk[cm])), 1.0f);
+      const float fw = fmaf(a.dts, wten[c], a.beta * ((-m) * (pp3d[c] - pp3d[cm])));
+      q.sD[e] = fmaf(a.alph, (-m) * ((pp3d[c] + fpk[c]) - (pp3d[cm] + fpk[cm])), w[c] + fw);
+    }
+  __syncthreads();
+  if (q.wq != 0 || !q.on) return;
+  const int ln = q.lane;
+  w[base] = 0.0f;
+  w[base + nz * sk] = 0.0f;
+  int e = kCoopCols + ln;
+  float r = dcr(1.0f, sB[e]);
+  float ca = (-q.sC[e]) * r, cb = q.sD[e] * r;
+  q.scA[e] = ca;
+  q.scB[e] = cb;
+  cA[base + sk] = ca;
+  cB[base + sk] = cb;
+  for (int k = 2; k < nz - 1; k++) {
+    e = k * kCoopCols + ln;
+    const float aa = q.sA[e];
+    r = dcr(1.0f, fmaf(aa, ca, sB[e]));
+    ca = (-q.sC[e]) * r;
+    cb = fmaf(-aa, cb, q.sD[e]) * r;
+    q.scA[e] = ca;
+    q.scB[e] = cb;
+    cA[base + k * sk] = ca;
+    cB[base + k * sk] = cb;
+  }
+  e = (nz - 1) * kCoopCols + ln;
+  const float aa = q.sA[e];
+  r = dcr(1.0f, fmaf(aa, ca, sB[e]));
+  float wk = fmaf(-aa, cb, q.sD[e]) * r;
+  w[base + (nz - 1) * sk] = wk;
+  for (int k = nz - 2; k >= 1; k--) {
+    e = k * kCoopCols + ln;
+    wk = fmaf(q.scA[e], wk, q.scB[e]);
+    w[base + k * sk] = wk;
+  }
+}
+
+static void launch_acoustic_w_solve(const KArgs& A, cudaStream_t st) {
+  const int nz = A.g.nz;
+  const size_t bytes = (size_t)6 * nz * kCoopCols * sizeof(float);
+  if (nz < 3 || bytes > 200 * 1024) {
+    launch_acoustic_w_solve_columns(A, st);
+    return;
+  }
+  if (A.gx <= 0 || A.gy <= 0) return;
+  static size_t configured = 0;
+  if (bytes > 48 * 1024 && bytes > configured) {
+    cudaFuncSetAttribute(k_wsolve_coop, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    configured = bytes;
+  }
+  launch_kernel(k_wsolve_coop, dim3((A.g.nx * A.g.ny + kCoopCols - 1) / kCoopCols), dim3(kCoopCols * kCoopWarps), bytes, st, A);
 }
 
 // turb_scalar_vert_implicit, implicit branch
