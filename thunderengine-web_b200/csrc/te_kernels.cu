@@ -764,7 +764,9 @@ __global__ void k_radbc_ew(KArgs A) {
   radbcw[j] = dcr(avgw, (float)g.nz);
   radbce[j] = dcr(avge, (float)g.nz);
 }
+#ifndef TE_KERNELS_FAST
 TE_LAUNCH3(radbc_ew)
+#endif
 
 // radbc_ns.wgsl: the same for v at the south (j = 1) and north (j = ny - 1) faces
 __global__ void k_radbc_ns(KArgs A) {
@@ -793,7 +795,61 @@ __global__ void k_radbc_ns(KArgs A) {
   radbcs[i] = dcr(avgs, (float)g.nz);
   radbcn[i] = dcr(avgn, (float)g.nz);
 }
+#ifndef TE_KERNELS_FAST
 TE_LAUNCH3(radbc_ns)
+#endif
+
+enum { kLineWarps = 8 };
+
+#ifdef TE_KERNELS_FAST
+// Line sums in the __restrict__ build: a warp per line.  Its lanes evaluate the terms of 32
+// consecutive levels (or columns) at a time, and every lane adds them in the reference's
+// order, taking each term from the lane that computed it (__shfl_sync), so the sum is the
+// one-thread-per-line kernel's; those kernels ran 40-4800 threads.
+
+// radbc_ew (NS 0: line j, the u columns i = 1, 2 and nx - 1, nx - 2) and radbc_ns (NS 1:
+// line i, the v rows j = 1, 2 and ny - 1, ny - 2)
+template <int NS>
+__global__ void __launch_bounds__(32 * kLineWarps) k_radbc_warp(KArgs A) {
+  const Dims& g = A.g;
+  const int lane = threadIdx.x & 31, line = blockIdx.x * kLineWarps + (threadIdx.x >> 5);
+  if (line >= A.gx || A.gy <= 0 || A.gz <= 0 || line >= (NS ? g.nx : g.ny)) return;
+  const float *TE_R a3 = A.p[1], *TE_R b3 = A.p[2], *TE_R hm = A.p[30];
+  const float dt = A.f[3];
+  const float umax = 350.0f;
+  const float d0 = NS ? dcr(dcr(1.0f, g.rdy), hm_vf(g, hm, 1)) : dcr(dcr(1.0f, g.rdx), hm_uf(g, hm, 1));
+  const float d1 = NS ? dcr(dcr(1.0f, g.rdy), hm_vf(g, hm, g.ny - 1)) : dcr(dcr(1.0f, g.rdx), hm_uf(g, hm, g.nx - 1));
+  float avg0 = 0.0f, avg1 = 0.0f;
+  for (int k0 = 0; k0 < g.nz; k0 += 32) {
+    const int k = k0 + lane;
+    float t0 = 0.0f, t1 = 0.0f;
+    if (k < g.nz) {
+      const int c1 = NS ? gidx(g, line, 1, k) : gidx(g, 1, line, k), c2 = NS ? gidx(g, line, 2, k) : gidx(g, 2, line, k);
+      t0 = radbc_speed(d0, a3[c1], b3[c1], a3[c2] - a3[c1], dt);
+      t0 = wmax(wmin(t0, 0.0f), -umax);
+      const int e1 = NS ? gidx(g, line, g.ny - 1, k) : gidx(g, g.nx - 1, line, k);
+      const int e2 = NS ? gidx(g, line, g.ny - 2, k) : gidx(g, g.nx - 2, line, k);
+      t1 = radbc_speed(d1, a3[e1], b3[e1], a3[e1] - a3[e2], dt);
+      t1 = wmin(wmax(t1, 0.0f), umax);
+    }
+    const int n = min(32, g.nz - k0);
+    for (int l = 0; l < n; l++) {
+      avg0 = avg0 + __shfl_sync(0xffffffffu, t0, l);
+      avg1 = avg1 + __shfl_sync(0xffffffffu, t1, l);
+    }
+  }
+  if (lane == 0) {
+    A.p[4][line] = dcr(avg0, (float)g.nz);
+    A.p[5][line] = dcr(avg1, (float)g.nz);
+  }
+}
+static void launch_radbc_ew(const KArgs& A, cudaStream_t s) {
+  if (A.gx > 0) launch_kernel(k_radbc_warp<0>, dim3((A.gx + kLineWarps - 1) / kLineWarps), dim3(32 * kLineWarps), 0, s, A);
+}
+static void launch_radbc_ns(const KArgs& A, cudaStream_t s) {
+  if (A.gx > 0) launch_kernel(k_radbc_warp<1>, dim3((A.gx + kLineWarps - 1) / kLineWarps), dim3(32 * kLineWarps), 0, s, A);
+}
+#endif
 
 // openbc_uv_tendency.wgsl: on open x boundaries the u faces i = 0 and i = nx, on open y
 // boundaries the v faces j = 0 and j = ny, advance by the radiation term
@@ -2056,7 +2112,8 @@ static void launch_tke_transport(const KArgs& A, cudaStream_t s) { launch_column
 
 // Two-float accumulation of the mass sums (f_df_add / f_df_add_pair, mass_row_sums.wgsl):
 // acc.x + x by an error-free sum, the error accumulated in acc.y.  The sums run in the
-// reference's order (one thread per row, level or total), so the results are its words.
+// reference's order (row by row in i, level by level in j, total in k), so the results
+// are its words.
 __device__ __forceinline__ void df_add(F2& acc, float x) {
   const float s = acc.x + x, bb = s - acc.x;
   const float err = (acc.x - (s - bb)) + (x - bb);
@@ -2068,48 +2125,78 @@ __device__ __forceinline__ void df_add_pair(F2& acc, float vx, float vy) {
   acc.y = acc.y + vy;
 }
 
-// mass_row_sums.wgsl: per (j, k) row the sums over i of rho / (uh vh mh) (rows1) and of
-// pi0 + pp3d (rows2), stored as pairs at k strideK + j
-__global__ void k_mass_row_sums(KArgs A) {
-  TE_K3
-  const int j = tx, k = ty;
-  if (j >= g.ny || k >= g.nz) return;
+// mass_row_sums with a warp per (j, k) row: the lanes form 32 consecutive terms, every
+// lane accumulates them in order of i (two-float sums are order-dependent).  A row's
+// inputs are all read before lane 0 writes its two pairs, in the reference's order, so
+// this form serves aliased bindings too.
+__global__ void __launch_bounds__(32 * kLineWarps) k_mass_rows_warp(KArgs A) {
+  const Dims& g = A.g;
+  const int lane = threadIdx.x & 31, j = blockIdx.x * kLineWarps + (threadIdx.x >> 5), k = blockIdx.y;
+  if (j >= A.gx || k >= A.gy || A.gz <= 0 || j >= g.ny || k >= g.nz) return;
   const float *TE_R rho = A.p[1], *TE_R pp3d = A.p[3], *TE_R hm = A.p[30];
   const float pik = A.p[2][k], mhk = A.p[4][k];
-  F2 s1{0.0f, 0.0f}, s2{0.0f, 0.0f};
   const float rvh = dcr(1.0f, hm_vh(g, hm, j));
-  for (int i = 0; i < g.nx; i++) {
-    const int c = gidx(g, i, j, k);
-    const float rmh = dcr(1.0f, mhk);
-    df_add(s1, ((rho[c] * dcr(1.0f, hm_uh(g, hm, i))) * rvh) * rmh);
-    df_add(s2, pik + pp3d[c]);
+  F2 s1{0.0f, 0.0f}, s2{0.0f, 0.0f};
+  for (int i0 = 0; i0 < g.nx; i0 += 32) {
+    const int i = i0 + lane;
+    float w = 0.0f, p = 0.0f;
+    if (i < g.nx) {
+      const int c = gidx(g, i, j, k);
+      w = ((rho[c] * dcr(1.0f, hm_uh(g, hm, i))) * rvh) * dcr(1.0f, mhk);
+      p = pik + pp3d[c];
+    }
+    const int n = min(32, g.nx - i0);
+    for (int l = 0; l < n; l++) {
+      df_add(s1, __shfl_sync(0xffffffffu, w, l));
+      df_add(s2, __shfl_sync(0xffffffffu, p, l));
+    }
   }
-  const long o = 2L * ((long)k * g.sK + j);
-  A.p[5][o] = s1.x;
-  A.p[5][o + 1] = s1.y;
-  A.p[6][o] = s2.x;
-  A.p[6][o + 1] = s2.y;
+  if (lane == 0) {
+    const long o = 2L * ((long)k * g.sK + j);
+    A.p[5][o] = s1.x;
+    A.p[5][o + 1] = s1.y;
+    A.p[6][o] = s2.x;
+    A.p[6][o + 1] = s2.y;
+  }
 }
-TE_LAUNCH3(mass_row_sums)
+static void launch_mass_row_sums(const KArgs& A, cudaStream_t s) {
+  if (A.gx > 0 && A.gy > 0)
+    launch_kernel(k_mass_rows_warp, dim3((A.gx + kLineWarps - 1) / kLineWarps, A.gy), dim3(32 * kLineWarps), 0, s, A);
+}
 
-// mass_level_sums.wgsl: per level the sums over j of the row pairs
-__global__ void k_mass_level_sums(KArgs A) {
-  TE_K3
-  const int k = tx;
-  if (ty != 0 || k >= g.nz) return;
+// mass_level_sums with a warp per level, the row pairs added in order of j
+__global__ void __launch_bounds__(32 * kLineWarps) k_mass_levels_warp(KArgs A) {
+  const Dims& g = A.g;
+  const int lane = threadIdx.x & 31, k = blockIdx.x * kLineWarps + (threadIdx.x >> 5);
+  if (k >= A.gx || A.gy <= 0 || A.gz <= 0 || k >= g.nz) return;
   const float *TE_R rows1 = A.p[1], *TE_R rows2 = A.p[2];
   F2 s1{0.0f, 0.0f}, s2{0.0f, 0.0f};
-  for (int j = 0; j < g.ny; j++) {
-    const long o = 2L * ((long)k * g.sK + j);
-    df_add_pair(s1, rows1[o], rows1[o + 1]);
-    df_add_pair(s2, rows2[o], rows2[o + 1]);
+  for (int j0 = 0; j0 < g.ny; j0 += 32) {
+    const int j = j0 + lane;
+    float a0 = 0.0f, a1 = 0.0f, b0 = 0.0f, b1 = 0.0f;
+    if (j < g.ny) {
+      const long o = 2L * ((long)k * g.sK + j);
+      a0 = rows1[o];
+      a1 = rows1[o + 1];
+      b0 = rows2[o];
+      b1 = rows2[o + 1];
+    }
+    const int n = min(32, g.ny - j0);
+    for (int l = 0; l < n; l++) {
+      df_add_pair(s1, __shfl_sync(0xffffffffu, a0, l), __shfl_sync(0xffffffffu, a1, l));
+      df_add_pair(s2, __shfl_sync(0xffffffffu, b0, l), __shfl_sync(0xffffffffu, b1, l));
+    }
   }
-  A.p[3][2 * k] = s1.x;
-  A.p[3][2 * k + 1] = s1.y;
-  A.p[4][2 * k] = s2.x;
-  A.p[4][2 * k + 1] = s2.y;
+  if (lane == 0) {
+    A.p[3][2 * k] = s1.x;
+    A.p[3][2 * k + 1] = s1.y;
+    A.p[4][2 * k] = s2.x;
+    A.p[4][2 * k + 1] = s2.y;
+  }
 }
-TE_LAUNCH3(mass_level_sums)
+static void launch_mass_level_sums(const KArgs& A, cudaStream_t s) {
+  if (A.gx > 0) launch_kernel(k_mass_levels_warp, dim3((A.gx + kLineWarps - 1) / kLineWarps), dim3(32 * kLineWarps), 0, s, A);
+}
 
 // mass_reference_init.wgsl: on its first run (ref[2] == 0) thread 0 stores the total mass
 // (the sum of the level pairs) as the reference and sets ref[2] = 1
