@@ -1160,7 +1160,8 @@ enum { kCoopCols = 32, kCoopWarps = 8 };
 // Thomas sweep over levels klo..khi of a block's 32 columns.  Row k: sA = sub-diagonal
 // coefficient (k > klo), sC = super-diagonal (k < khi), sD = right-hand side; the diagonal
 // is 1 - sA - sC as the reference forms it.  Writes the forward coefficient cA (levels
-// klo..khi-1) and the solution into cB (levels klo..khi), in memory and in scA / scB.
+// klo..khi-1) and the solution into cB (levels klo..khi), in memory and in scA / scB,
+// which may be sC / sD themselves (each row is read before its slot is rewritten).
 __device__ __forceinline__ void coop_thomas(const float* sA, const float* sC, const float* sD, float* scA, float* scB,
                                             int klo, int khi, int lane, float* TE_R cA, float* TE_R cB, int base, int sk) {
   int e = klo * kCoopCols + lane;
@@ -1215,12 +1216,12 @@ __device__ __forceinline__ CoopCol coop_col(const KArgs& A, float* smem, int cx,
   q.sA = smem;
   q.sC = smem + nz * kCoopCols;
   q.sD = smem + 2 * nz * kCoopCols;
-  q.scA = smem + 3 * nz * kCoopCols;
-  q.scB = smem + 4 * nz * kCoopCols;
+  q.scA = q.sC;  // the forward sweep overwrites each row's sC / sD after reading them
+  q.scB = q.sD;
   return q;
 }
 
-static size_t coop_bytes(int nz) { return (size_t)5 * nz * kCoopCols * sizeof(float); }
+static size_t coop_bytes(int nz) { return (size_t)3 * nz * kCoopCols * sizeof(float); }
 
 template <class K>
 static void launch_coop(K kernel, const KArgs& A, cudaStream_t st, int cx, int cy) {
@@ -1285,7 +1286,7 @@ __global__ void __launch_bounds__(kCoopCols * kCoopWarps) k_wsolve_coop(KArgs A)
   const Dims& g = A.g;
   const int nz = g.nz;
   const CoopCol q = coop_col(A, tsm, g.nx, g.ny);
-  float* sB = tsm + 5 * nz * kCoopCols;
+  float* sB = tsm + 3 * nz * kCoopCols;
   const Acoustic a = A.a;
   const float asq = a.alph * a.alph;
   const float *TE_R pk1 = A.p[2], *TE_R pk2 = A.p[3], *TE_R qk = A.p[4], *TE_R mm = A.p[5], *TE_R fpk = A.p[6];
@@ -1293,6 +1294,7 @@ __global__ void __launch_bounds__(kCoopCols * kCoopWarps) k_wsolve_coop(KArgs A)
   float *TE_R w = A.p[9], *TE_R cA = A.p[10], *TE_R cB = A.p[11];
   const int sk = q.sk, base = q.base;
   if (q.on)
+#pragma unroll 2
     for (int k = 1 + q.wq; k <= nz - 1; k += kCoopWarps) {
       const int c = base + k * sk, cm = c - sk, e = k * kCoopCols + q.lane;
       const float m = mm[c];
@@ -1339,7 +1341,7 @@ __global__ void __launch_bounds__(kCoopCols * kCoopWarps) k_wsolve_coop(KArgs A)
 
 static void launch_acoustic_w_solve(const KArgs& A, cudaStream_t st) {
   const int nz = A.g.nz;
-  const size_t bytes = (size_t)6 * nz * kCoopCols * sizeof(float);
+  const size_t bytes = (size_t)4 * nz * kCoopCols * sizeof(float);
   if (nz < 3 || bytes > 200 * 1024) {
     launch_acoustic_w_solve_columns(A, st);
     return;
@@ -1366,6 +1368,7 @@ __global__ void __launch_bounds__(kCoopCols * kCoopWarps) k_tsvi_coop(KArgs A) {
   const int useFlux = A.iv[15], bcturbs = A.iv[18];
   const float tema = ((-dt) * g.rdz) * g.rdz, temc = dt * g.rdz;
   if (q.on)
+#pragma unroll 2
     for (int k = q.wq; k < nz; k += kCoopWarps) {
       const int c = base + k * sk, e = k * kCoopCols + q.lane;
       if (k < nz - 1) q.sC[e] = tema * ((((khv[c + sk] * mf[k + 1]) * rf[c + sk]) * mh[k]) * rr[c]);
@@ -1909,6 +1912,7 @@ __global__ void __launch_bounds__(kCoopCols * kCoopWarps) k_turb_uv_coop(KArgs A
     return (((kmv[cl - s] + kmv[cl]) * (mf[lev] + mf[lev])) * (rf[cl - s] + rf[cl])) * ((mh[k] + mh[k]) * rinv(k));
   };
   if (on) {
+#pragma unroll 2
     for (int k = q.wq; k <= nz; k += kCoopWarps) {
       const int c = base + k * sk;
       const float dwx = AX == 0 ? ((w[c] - w[c - 1]) * g.rdx) * hm_uf(g, hm, i) : ((w[c] - w[c - sj]) * g.rdy) * hm_vf(g, hm, j);
@@ -2065,6 +2069,7 @@ __global__ void __launch_bounds__(kCoopCols * kCoopWarps) k_turb_wlevel_coop(KAr
   const float tema = (((-1.0f) * dt) * g.rdz) * g.rdz, temc = dt * g.rdz;
   auto mfr = [&](int k) { return dcr(mf[k], rf[base + k * sk]); };
   if (cq.on)
+#pragma unroll 2
     for (int k = 1 + cq.wq; k <= nz - 1; k += kCoopWarps) {
       const int c = base + k * sk, e = k * kCoopCols + cq.lane;
       if (k < nz - 1) cq.sC[e] = tema * ((((kmh[c] + kmh[c + sk]) * mh[k]) * rho[c]) * mfr(k));
