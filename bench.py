@@ -95,7 +95,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.device), '--query-gpu=' + self.Q,
-                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                          '--format=csv,noheader,nounits', '-lms', '50'],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -175,6 +175,7 @@ def cpu_baseline_sample(budget_s=10.0):
     t0 = time.perf_counter()
     p.run(kern)                      # warm-up step
     t_one = time.perf_counter() - t0
+    after_one = p.M.copy()           # the state after one step: the parity check of the GPU step
     nsteps = max(1, min(20, int(budget_s / max(t_one, 1e-3))))
     t0 = time.perf_counter()
     for _ in range(nsteps):
@@ -185,7 +186,26 @@ def cpu_baseline_sample(budget_s=10.0):
             'sample': '%d large step(s) of the 256x256x80 workload after one warm-up step, %s kernels, '
                       'OpenMP over the dispatch grid on all host cores' % (
                           nsteps, "the reference's WGSL translated to C++" if kind == 'reference' else 'oracle'),
-            'seconds': dt}
+            'seconds': dt, '_after_one_step': after_one}
+
+
+def parity_vs_cpu(r, run, init, cpu_mem, kind):
+    """One large step of the benchmarked workload on the GPU (the mode being measured)
+    against the same step on the host (the reference kernels, or the oracle): every
+    non-scratch arena field compared word for word."""
+    from thunderengine_web_b200.timestep import SCRATCH_FIELDS
+    for i, b in init.items():
+        r.upload(i, b)
+    r.encode_steps(1)
+    r.sync()
+    g = run.grid
+    aid = run.rec.ids['arena']
+    base = r.base[aid]
+    names = [n for n in run.fields if n not in SCRATCH_FIELDS]
+    bad = [n for n in names if not np.array_equal(r.read(g.count, base + run.fields[n] // 4),
+                                                  cpu_mem[base + run.fields[n] // 4:base + run.fields[n] // 4 + g.count])]
+    return {'against': "the reference's kernels on the host (oracle/_ref)" if kind == 'reference' else 'the oracle',
+            'steps': 1, 'fields_compared': len(names), 'fields_differing': bad, 'bit_exact': not bad}
 
 
 # ---------------------------------------------------------------- our arm
@@ -237,8 +257,10 @@ def run_ours(a, rank, world, local):
     # fields from pinned memory, plays the step, reads the prognostic fields back
     e2e = None if a.no_e2e else end_to_end(r, run, init, cfg, a, world, mode, dev)
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline_sample()
+        parity = parity_vs_cpu(r, run, init, cpu.pop('_after_one_step'), cpu['kind'])
     ops = r.num_ops
     if roof is not None:
         launches = roof.pop('_launches_per_step')
@@ -254,6 +276,7 @@ def run_ours(a, rank, world, local):
                        tape_ops_per_step=ops,
                        l2='inputs larger than L2: %.2f GB arena per replica' % (run.arena_bytes / 1e9)),
         'roofline': roof, 'cpu_baseline': cpu, 'e2e': e2e, 'gpu_launches': launches * a.steps, 'clocks': clocks,
+        'parity': parity,
     }
     if rank == 0:
         print(json.dumps(out))
@@ -293,8 +316,10 @@ def kernel_roofline(r, run, stream, mode):
             pts_whole = g.count
             pts = g.nx * g.ny * g.nz
             stats['acoustic_uv_accumulate (fused)'] = [timed(lambda: r.run_segment(q, 0)), len(acu), 12 * 4 * pts_whole]
+            # the timed launch is a stage-3 substep: reads u, v, w, piadv, ppten, ppterm, pk1,
+            # pk2, qk, mm, wten, pp3d, rrw; writes w, pp3d, ppd, rrw and ppx (stages 1-2: no ppx)
             stats['acoustic_column (fused fpk+w_solve+pp+accumulate)'] = [timed(lambda: r.run_segment(q, 1)), len(acu),
-                                                                          19 * 4 * pts]
+                                                                          18 * 4 * pts]
             stats['halo_periodic x4 (fused)'] = [timed(lambda: r.run_segment(q, 2)), len(acu),
                                                  4 * 2 * 4 * 7 * (g.strideK + g.nx) * (g.nz + 1)]
         if halo:
@@ -573,8 +598,10 @@ def run_reference(a, rank, world):
     big = cfg
     out = {'metric': METRIC, 'value': v, 'unit': METRIC, 'n_gpus': world, 'steps': a.steps, 'warmup': a.warmup,
            'ms_per_step': dt / a.steps * 1e3, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
-           'dtype': 'f32', 'data': 'synthetic', 'impl': 'reference',
-           'config': dict(big.as_dict(), grid_points=pts),
+           'dtype': 'f32', 'data': 'synthetic (Weisman-Klemp sounding, 2 K bubble, seeded noise)', 'impl': 'reference',
+           'config': dict(big.as_dict(), grid_points=pts, mode=a.mode, parallelism='replicas x%d' % world,
+                          tape_ops_per_step=sum(1 for c in tape['steps'][0] if c['op'] in ('dispatch', 'copy')),
+                          l2='inputs larger than L2: %.2f GB arena per replica' % (run.arena_bytes / 1e9)),
            'cpu_baseline': {'value': v, 'unit': METRIC, 'cores': os.cpu_count(), 'kind': kind,
                             'sample': 'each step = one large step of the 256x256x80 workload on all host cores'},
            'e2e': {'value': v, 'unit': METRIC, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}

@@ -163,13 +163,15 @@ typedef struct te_wsolve_fields {
  * same w as the tape kernel acoustic_w_solve (bit for bit) but keeps the Thomas
  * coefficients, which the tape writes to the arena fields cA and cB, in a fixed 64 MiB
  * array inside this library; it allocates nothing.
- *   - Limit: nx * ny * (nz - 2) <= 8,388,608 (256 x 256 columns up to nz = 130); larger
- *     grids, nz < 3 or a NULL field return TE_ERANGE / TE_EINVAL with a message in `err`
- *     (`err_len` bytes, may be NULL) and launch nothing.
+ *   - Limit: nx * ny * (nz - 2) <= 8,388,608 (256 x 256 columns up to nz = 130) and
+ *     ny <= 262,140; larger grids, nz < 3 or a NULL field return TE_ERANGE / TE_EINVAL
+ *     with a message in `err` (`err_len` bytes, may be NULL) and launch nothing.
  *   - Every GPU that loads the library holds the 64 MiB until the process exits.
  *   - Runs on the current CUDA device, on `cuda_stream` (NULL = legacy default stream),
- *     asynchronously.  The first call on a device looks up the array's device address;
- *     make that first call before any stream capture.
+ *     asynchronously, in the device's primary context (the CUDA runtime's).  The first
+ *     call on a device looks up the array's device address and keeps it for the life of
+ *     the process; make that first call before any stream capture, and do not call
+ *     again after cudaDeviceReset on that device.
  *   - Nothing in the array has to start at zero: each column's coefficients are written
  *     before they are read.  All calls share the array, so calls that may overlap on the
  *     GPU (different streams, or different host threads) race: order them. */

@@ -313,3 +313,71 @@ def test_fused_plan_covers_the_step():
     assert kinds.count(2) >= 10
     exact_ops = sum(s[2] - s[1] + 1 for s in segs if s[0] == 0)
     assert exact_ops < gpu.num_ops // 3
+
+
+# ---------------------------------------------------------------- the benchmarked configuration
+
+def _nonscratch_mismatches(run, mem_a, mem_b, base):
+    bad = []
+    for name in run.fields:
+        if name in STEP_SCRATCH:
+            continue
+        a = helpers.field_view(mem_a, run, base, name).view(np.uint32)
+        b = helpers.field_view(mem_b, run, base, name).view(np.uint32)
+        if not np.array_equal(a, b):
+            bad.append((name, int(np.count_nonzero(a != b))))
+    return bad
+
+
+def test_headline_config_one_step_exact_and_fused_vs_oracle():
+    """256x256x80, dt 3 s, nsound 8 (15 acoustic substeps, 5 passes of the fused column
+    kernel, every epilogue slot up to level 80): one large step in exact mode equals the
+    oracle in every memory word, and in fused mode in every non-scratch field."""
+    from thunderengine_web_b200.replayer import TE_MODE_FUSED
+    run = timestep.Run(scenario.AT_SCALE)
+    tape = run.tape(1)
+    init = run.initial_buffers()
+    cpu = helpers.cpu_run(tape, init, nsteps=1, hashes=False)
+    gpu = helpers.gpu_replayer(tape, init, hashes=False)
+    gpu.encode_steps(1)
+    mem = gpu.read(gpu.buffers_end)
+    base = gpu.base[run.rec.ids['arena']]
+    diff = np.nonzero(mem != cpu.M[:gpu.buffers_end])[0]
+    assert diff.size == 0, 'exact mode: %d words differ, first at %d' % (diff.size, diff[0])
+    gpu.close()
+    del mem
+    fz = helpers.gpu_replayer(tape, init, hashes=False, mode=TE_MODE_FUSED)
+    fz.encode_steps(1)
+    mem = fz.read(fz.buffers_end)
+    assert not _nonscratch_mismatches(run, mem, cpu.M, base)
+    assert np.array_equal(mem[:base], cpu.M[:base])
+    fz.close()
+
+
+@pytest.mark.parametrize('nz', [80, 100])
+def test_fused_tall_columns_vs_oracle(nz):
+    """Narrow grids with the benchmark's depth and deeper: the fused column kernel's
+    epilogue slots 3-5 (levels 51..101) and 5-7 passes of 16 levels, three steps."""
+    _fused_vs_oracle(scenario.tiny(24, 20, nz, dx=500.0, dz=250.0, dt=3.0, nsound=8, us=25.0), nsteps=3)
+
+
+def test_headline_config_fused_equals_exact_over_20_steps():
+    """20 large steps at 256x256x80 in fused and in exact mode on the GPU: every
+    non-scratch field bit-identical."""
+    from thunderengine_web_b200.replayer import TE_MODE_FUSED
+    run = timestep.Run(scenario.AT_SCALE)
+    tape = run.tape(1)
+    init = run.initial_buffers()
+    ex = helpers.gpu_replayer(tape, init, hashes=False)
+    ex.encode_steps(20)
+    mem_ex = ex.read(ex.buffers_end)
+    base = ex.base[run.rec.ids['arena']]
+    ex.close()
+    fz = helpers.gpu_replayer(tape, init, hashes=False, mode=TE_MODE_FUSED)
+    fz.encode_steps(20)
+    mem_fz = fz.read(fz.buffers_end)
+    fz.close()
+    assert not _nonscratch_mismatches(run, mem_fz, mem_ex, base)
+    # the state moved: the comparison is not of two untouched arenas
+    th0 = helpers.field_view(np.frombuffer(init[run.rec.ids['arena']], dtype=np.uint32), run, 0, 'w')
+    assert not np.array_equal(helpers.field_view(mem_ex, run, base, 'w').view(np.uint32), th0)

@@ -34,14 +34,20 @@ def test_oversize_grid_is_rejected_before_any_device_work():
     assert b'scratch' in err.value and b'8388608' in err.value
     rc = lib.te_w_solve_static_scratch(ctypes.byref(f), 16, 16, 2, 1.0, 0.6, 0.4, None, err, 256)
     assert rc == -1                          # TE_EINVAL: nz < 3
+    rc = lib.te_w_solve_static_scratch(ctypes.byref(f), 1, 300000, 3, 1.0, 0.6, 0.4, None, err, 256)
+    assert rc == -5 and b'262140' in err.value   # more rows than one launch covers
 
 
+# 37x29x13: odd sizes; 33x5x3: the shallowest column (no middle forward level, the top
+# level reads the coefficients of level 1) on a row count that is not a multiple of the
+# launch's 4 rows per block
 @pytest.mark.gpu
-def test_static_scratch_solve_matches_the_tape_kernel_twice():
+@pytest.mark.parametrize('nx,ny,nz', [(37, 29, 13), (33, 5, 3)])
+def test_static_scratch_solve_matches_the_tape_kernel_twice(nx, ny, nz):
     import torch
     from thunderengine_web_b200 import scenario, timestep
     from thunderengine_web_b200.replayer import TeWSolveFields
-    run = timestep.Run(scenario.tiny(37, 29, 13, dx=500.0, dz=250.0, dt=3.0, nsound=8, us=25.0))
+    run = timestep.Run(scenario.tiny(nx, ny, nz, dx=500.0, dz=250.0, dt=3.0, nsound=8, us=25.0))
     tape = run.tape(1)
     r = helpers.gpu_replayer(tape, run.initial_buffers(), hashes=False)
     solves = [q for q in range(r.num_ops) if r.op_name(q) == 'acoustic_w_solve'][:2]

@@ -335,12 +335,8 @@ __global__ void __launch_bounds__(kColThreads, 2) k_acu_column(AcuArgs A) {
 }
 
 static void launch_acu_column(const AcuArgs& A, cudaStream_t s) {
-  static int configured = -1;
   const size_t bytes = col_smem_bytes(A.g.nz);
-  if ((int)bytes > configured) {
-    cudaFuncSetAttribute(k_acu_column, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    configured = (int)bytes;
-  }
+  if (opt_in_smem((const void*)k_acu_column, bytes) != cudaSuccess) return;  // error left pending
   dim3 b(kColThreads), gr((A.g.nx + kColTile - 1) / kColTile, A.g.ny);
   launch_kernel(k_acu_column, dim3(gr), dim3(b), bytes, s, A);
 }

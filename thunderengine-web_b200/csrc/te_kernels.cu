@@ -1227,7 +1227,7 @@ template <class K>
 static void launch_coop(K kernel, const KArgs& A, cudaStream_t st, int cx, int cy) {
   const size_t bytes = coop_bytes(A.g.nz);
   if (A.gx <= 0 || A.gy <= 0 || A.gz <= 0) return;
-  if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (opt_in_smem((const void*)kernel, bytes) != cudaSuccess) return;  // error left pending for the player
   launch_kernel(kernel, dim3((cx * cy + kCoopCols - 1) / kCoopCols), dim3(kCoopCols * kCoopWarps), bytes, st, A);
 }
 
@@ -1347,11 +1347,7 @@ static void launch_acoustic_w_solve(const KArgs& A, cudaStream_t st) {
     return;
   }
   if (A.gx <= 0 || A.gy <= 0) return;
-  static size_t configured = 0;
-  if (bytes > 48 * 1024 && bytes > configured) {
-    cudaFuncSetAttribute(k_wsolve_coop, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    configured = bytes;
-  }
+  if (opt_in_smem((const void*)k_wsolve_coop, bytes) != cudaSuccess) return;  // error left pending
   launch_kernel(k_wsolve_coop, dim3((A.g.nx * A.g.ny + kCoopCols - 1) / kCoopCols), dim3(kCoopCols * kCoopWarps), bytes, st, A);
 }
 

@@ -54,6 +54,12 @@ inline cudaError_t launch_kernel(void (*k)(P...), dim3 gr, dim3 b, size_t smem, 
   return cudaLaunchKernelEx(&cfg, k, a...);
 }
 
+// Opts kernel `k` into `bytes` of dynamic shared memory on the CURRENT device.  The
+// attribute belongs to the device, so it is set once per (kernel, device) — a process
+// with contexts on several GPUs sets it on each — under a lock.  On failure the CUDA
+// error stays pending for the caller's cudaGetLastError check and is also returned.
+cudaError_t opt_in_smem(const void* k, size_t bytes);
+
 // All kernels this library implements (te_kernels.cu).
 const KernelSpec* kernel_table(int* count);
 const KernelSpec* find_kernel(const char* name);

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -36,6 +37,21 @@ struct ApiError : std::runtime_error {
   } while (0)
 
 static uint64_t ceil_div(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
+
+cudaError_t opt_in_smem(const void* k, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> done;  // (kernel, device) -> bytes set
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& have = done[std::make_pair(k, dev)];
+  if (have >= bytes) return cudaSuccess;
+  e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) have = bytes;
+  return e;
+}
 
 // Step structure without setBytes data (replay.js:31): commands minus barriers, bytes
 // replaced by their index and encoded length.

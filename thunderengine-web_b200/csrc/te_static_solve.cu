@@ -102,6 +102,11 @@ extern "C" int te_w_solve_static_scratch(const te_wsolve_fields* f, int nx, int 
                   nx, ny, nz, need, kScratchFloats, kScratchFloats / 2);
     return fail(err, err_len, TE_ERANGE, msg);
   }
+  if (ny > 4 * 65535) {
+    char msg[160];
+    std::snprintf(msg, sizeof msg, "te_w_solve_static_scratch: ny = %d exceeds the launch limit of 262140 rows", ny);
+    return fail(err, err_len, TE_ERANGE, msg);
+  }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
     return fail(err, err_len, TE_ECUDA, "te_w_solve_static_scratch: no usable current CUDA device");
@@ -110,7 +115,9 @@ extern "C" int te_w_solve_static_scratch(const te_wsolve_fields* f, int nx, int 
     std::lock_guard<std::mutex> lock(g_mu);
     if (!g_scratch[dev]) {
       // first call on this device: translate the array's host-side name into its device
-      // address (the host symbol itself is not a device pointer)
+      // address (the host symbol itself is not a device pointer).  The address belongs to
+      // the device's primary context, the one the CUDA runtime uses; it stays valid until
+      // that context is destroyed (cudaDeviceReset), after which this cache is stale.
       void* p = nullptr;
       const cudaError_t e = cudaGetSymbolAddress(&p, kScratch);
       if (e != cudaSuccess) {
