@@ -39,6 +39,7 @@ def parse():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-roofline', action='store_true', help='skip the per-kernel timing pass')
+    ap.add_argument('--no-fp64', action='store_true', help='skip the error statement against the binary64 oracle')
     ap.add_argument('--workload', default='at_scale', choices=['at_scale', 'medium', 'small'],
                     help='at_scale = 256x256x80 (the benchmark); medium = 160x160x80 with the same '
                          'physics, for profiler captures; small = 64x64x40')
@@ -208,6 +209,55 @@ def parity_vs_cpu(r, run, init, cpu_mem, kind):
             'steps': 1, 'fields_compared': len(names), 'fields_differing': bad, 'bit_exact': not bad}
 
 
+PROGNOSTIC = ('th', 'qv', 'u', 'v', 'w', 'pp3d')
+
+
+def interior(a, g):
+    return a.reshape(g.nz + 1, g.strideK, g.strideJ)[:g.nz, 3:3 + g.ny, 3:3 + g.nx]
+
+
+def fp64_error(r, run, init, checkpoints=(1, 20)):
+    """Error of the binary32 step against the binary64 twin of the oracle
+    (oracle/liboracle64.so: the same kernels evaluated in binary64) after each number of
+    large steps in ``checkpoints``, from the same initial state: per prognostic field the
+    largest absolute error over the interior points and that divided by the largest
+    |value| of the binary64 field (normwise relative error).  The binary32 states are
+    the GPU's (this library, the mode being measured)."""
+    from tests import helpers
+    from oracle.player import CpuPlayer64
+    g = run.grid
+    aid = run.rec.ids['arena']
+    p = CpuPlayer64(run.tape(1), helpers.kernels_meta())
+    p.plan()
+    for i, b in init.items():
+        p.upload(i, b)
+    p.values_from_words()
+    for i, b in init.items():
+        r.upload(i, b)
+    base = r.base[aid]
+    assert base == p.base[aid]
+    out, done, t0 = {}, 0, time.perf_counter()
+    for n in checkpoints:
+        r.encode_steps(n - done)
+        r.sync()
+        p.run64(n - done)
+        done = n
+        per = {}
+        for f in PROGNOSTIC:
+            o = base + run.fields[f] // 4
+            a = interior(r.read(g.count, o).view(np.float32), g).astype(np.float64)
+            b = interior(p.field64(o, g.count), g)
+            err = float(np.abs(a - b).max())
+            scale = float(np.abs(b).max())
+            per[f] = {'max_abs': err, 'max_rel': err / scale if scale > 0 else None}
+        out['after_%d_steps' % n] = per
+    out['reference'] = ('the binary64 twin of the oracle (same kernels, same order, binary64 arithmetic, '
+                        'binary32 constants), from the same initial state')
+    out['max_rel_definition'] = 'max |f32 - f64| / max |f64| over the interior points of the field'
+    out['seconds'] = time.perf_counter() - t0
+    return out
+
+
 # ---------------------------------------------------------------- our arm
 
 def run_ours(a, rank, world, local):
@@ -258,9 +308,11 @@ def run_ours(a, rank, world, local):
     e2e = None if a.no_e2e else end_to_end(r, run, init, cfg, a, world, mode, dev)
     cpu = None
     parity = None
+    f64err = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline_sample()
         parity = parity_vs_cpu(r, run, init, cpu.pop('_after_one_step'), cpu['kind'])
+        f64err = None if a.no_fp64 else fp64_error(r, run, init)
     ops = r.num_ops
     if roof is not None:
         launches = roof.pop('_launches_per_step')
@@ -276,7 +328,7 @@ def run_ours(a, rank, world, local):
                        tape_ops_per_step=ops,
                        l2='inputs larger than L2: %.2f GB arena per replica' % (run.arena_bytes / 1e9)),
         'roofline': roof, 'cpu_baseline': cpu, 'e2e': e2e, 'gpu_launches': launches * a.steps, 'clocks': clocks,
-        'parity': parity,
+        'parity': parity, 'fp64_error': f64err,
     }
     if rank == 0:
         print(json.dumps(out))

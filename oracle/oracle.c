@@ -84,6 +84,33 @@ float te_sqrt_cr(float x) {
   return sqrt_core(x);
 }
 
+#ifdef TE_ORACLE_F64
+/* Binary64 twin (oracle/oracle64.c compiles this file with TE_ORACLE_F64): every
+ * kernel below evaluates the same formulas in binary64.  Field values live in a double
+ * array parallel to the word memory (te64_D, set by te64_bind); parameter structs are
+ * still read from the words.  Division and square root are the binary64 operations;
+ * fma is the binary64 fma; the reference's two-float pow becomes pow().  Constants keep
+ * the binary32 values the step is defined with. */
+double *te64_D;
+void te64_bind(double *D) { te64_D = D; }
+#undef DCR
+#define DCR(a, b) ((double)(a) / (double)(b))
+#define float double
+#define fmaf fma
+#define fabsf fabs
+#define sqrtf sqrt
+#define powf pow
+#define nearbyintf nearbyint
+#define ldexpf ldexp
+#define frexpf frexp
+#define te_sqrt_cr sqrt
+#define te_weno5 te64_weno5
+#define te_rr_pow_cr te64_rr_pow_cr
+#define te_pow_f64 pow
+#define te_exp_f64 exp
+#define te_log_f64 log
+#endif
+
 /* WGSL min/max on f32: min(a, b) is b if b < a, else a; max(a, b) is b if a < b,
  * else a; a NaN operand yields the other one.  This fixes the sign of a zero result
  * when the operands are +0 and -0. */
@@ -127,7 +154,11 @@ static Acoustic acoustic_at(const uint32_t *M, uint32_t off) {
 }
 
 #define B(n) (ARG[4 + (n)])
+#ifdef TE_ORACLE_F64
+#define FPTR(n) (te64_D + B(n))
+#else
 #define FPTR(n) ((float *)(M + B(n)))
+#endif
 #define FVAL(n) (bitsf(M[B(n)]))
 #define IVAL(n) ((int32_t)M[B(n)])
 #define GIDX(g, i, j, k) (((i) + 3) + (g).sJ * (((j) + 3) + (g).sK * (k)))
@@ -1181,6 +1212,9 @@ static float rr_exp_ff(F2 y) {
   return ldexpf(res, (int)k);
 }
 float te_rr_pow_cr(float x, float p) {
+#ifdef TE_ORACLE_F64
+  if (1) return pow(x, p);
+#endif
   if (!(x > 0.0f) || (fbits(x) & 0x7fffffffu) == 0x7f800000u) return powf(x, p);
   F2 L = rr_log_ff(x);
   float yh = L.x * p;
@@ -1902,6 +1936,7 @@ void teor_turb_gettau(uint32_t *M, const uint32_t *ARG) {
  * The binary64 error is far below half a binary32 ulp, so each is the correctly rounded
  * value except within that error of a rounding boundary.  The CUDA kernels evaluate the
  * same operations in the same order. */
+#ifndef TE_ORACLE_F64
 static double ln_mantissa(float x, int *e) {   /* x > 0 normal: returns ln(m), sets e */
   uint32_t b = fbits(x);
   double m = (double)bitsf((b & 0x7fffffu) | 0x3f800000u);
@@ -1939,6 +1974,7 @@ float te_log_f64(float x) {
   double lm = ln_mantissa(x, &e);
   return (float)((double)e * 0.6931471805599453 + lm);
 }
+#endif /* !TE_ORACLE_F64 */
 
 void teor_turb_km_kh(uint32_t *M, const uint32_t *ARG) {
   /* turb_km_kh.wgsl main: TKE closure on w levels 1..nz-1.  Grid scale (dx dy dz)^(1/3),

@@ -349,3 +349,47 @@ def load_tape(scen_dir):
 def load_kernels_meta(path):
     with open(path) as fh:
         return json.load(fh)
+
+
+class CpuPlayer64(CpuPlayer):
+    """The same player over the binary64 twin of the oracle (liboracle64.so): a double
+    array ``D`` beside the word memory holds every field value; kernels read parameter
+    structs from ``M`` and field values from ``D``.  ``values_from_words()`` widens the
+    uploaded binary32 words into ``D``; ``field64(off, n)`` reads values back."""
+
+    def __init__(self, tape, kernels_meta, lib_path=None):
+        super().__init__(tape, kernels_meta)
+        self.lib64 = ctypes.CDLL(lib_path or os.path.join(HERE, 'liboracle64.so'))
+        self.lib64.te64_bind.argtypes = [ctypes.c_void_p]
+        self.lib64.te64_bind.restype = None
+        self.kernels64 = {}
+
+    def plan(self, with_hashes=False):
+        super().plan(False)
+        self.D = np.zeros(self.M.size, dtype=np.float64)
+
+    def values_from_words(self):
+        self.D[:] = self.M.view(np.float32)
+
+    def kernel(self, name):
+        f = self.kernels64.get(name)
+        if f is None:
+            f = getattr(self.lib64, 'teor_' + name)
+            f.restype = None
+            f.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+            self.kernels64[name] = f
+        return f
+
+    def run64(self, nsteps=1):
+        self.lib64.te64_bind(self.D.ctypes.data_as(ctypes.c_void_p))
+        mp = self.M.ctypes.data_as(ctypes.c_void_p)
+        for _ in range(nsteps):
+            for o in self.ops:
+                if o.kind == 'copy':
+                    self.D[o.dst:o.dst + o.n] = self.D[o.src:o.src + o.n]
+                    self.M[o.dst:o.dst + o.n] = self.M[o.src:o.src + o.n]
+                else:
+                    self.kernel(o.name)(mp, o.arg.ctypes.data_as(ctypes.c_void_p))
+
+    def field64(self, off, n):
+        return self.D[off:off + n]
