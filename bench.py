@@ -83,54 +83,95 @@ def max_over_ranks(x, world):
 # --------------------------------------------------------------------- clocks
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
-    Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,'
-         'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
-         'clocks_event_reasons.sw_power_cap')
+    """SM clock and clock-event (throttle) reasons sampled during the timed region: NVML
+    polled every 5 ms from a thread (read-only queries), or nvidia-smi at 50 ms when
+    NVML is unavailable."""
+    NAMES = ('hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap')
 
     def __init__(self, device):
         self.device = device
+        self.samples = []          # (sm_mhz, max_mhz, set of reason names)
+        self.stop_flag = threading.Event()
+        self.t = None
+        self.nvml = None
         self.proc = None
-        self.lines = []
+
+    def _handle(self, nv):
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.device)
+            bus = '%08x:%02x:%02x.0' % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            return nv.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.device)
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.device), '--query-gpu=' + self.Q,
+            import pynvml as nv
+            nv.nvmlInit()
+            h = self._handle(nv)
+            bits = {'hw_slowdown': nv.nvmlClocksEventReasonHwSlowdown,
+                    'hw_thermal_slowdown': nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    'sw_thermal_slowdown': nv.nvmlClocksEventReasonSwThermalSlowdown,
+                    'sw_power_cap': nv.nvmlClocksEventReasonSwPowerCap}
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+
+            def poll():
+                while not self.stop_flag.is_set():
+                    sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                    r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((float(sm), float(mx), {n for n, b in bits.items() if r & b}))
+                    time.sleep(0.005)
+            self.nvml = nv
+            self.t = threading.Thread(target=poll, daemon=True)
+            self.t.start()
+            return
+        except Exception:
+            self.nvml = None
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.device), '--query-gpu=clocks.sm,clocks.max.sm,'
+                                          'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+                                          'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap',
                                           '--format=csv,noheader,nounits', '-lms', '50'],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+
+            def read():
+                for line in self.proc.stdout:
+                    parts = [p.strip() for p in line.split(',')]
+                    try:
+                        self.samples.append((float(parts[0]), float(parts[1]),
+                                             {n for n, v in zip(self.NAMES, parts[2:6]) if v.lower() == 'active'}))
+                    except (ValueError, IndexError):
+                        pass
+            self.t = threading.Thread(target=read, daemon=True)
             self.t.start()
         except Exception:
             self.proc = None
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def wait_first(self, timeout=5.0):
+        """Block until the sampler has its first sample, so the timed region is covered."""
+        t0 = time.time()
+        while not self.samples and time.time() - t0 < timeout and (self.t is not None):
+            time.sleep(0.002)
 
     def stop(self):
-        if not self.proc:
-            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['nvidia-smi unavailable']}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        sm, mx, reasons = [], None, set()
-        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(',')]
-            if len(parts) < 9:
-                continue
+        self.stop_flag.set()
+        if self.proc:
+            self.proc.terminate()
             try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, parts[5:9]):
-                if v.lower() == 'active':
-                    reasons.add(n)
-        return {'sm_mhz': statistics.median(sm) if sm else None, 'sm_max_mhz': mx, 'reasons': sorted(reasons),
-                'samples': len(sm)}
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.t is not None:
+            self.t.join(timeout=2)
+        if not self.samples:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['no clock samples'], 'samples': 0}
+        reasons = set()
+        for _, _, r in self.samples:
+            reasons |= r
+        return {'sm_mhz': statistics.median(x[0] for x in self.samples), 'sm_max_mhz': self.samples[-1][1],
+                'reasons': sorted(reasons), 'samples': len(self.samples),
+                'source': 'NVML, 5 ms polling' if self.nvml else 'nvidia-smi, 50 ms polling'}
 
 
 # ------------------------------------------------------------------ workload
@@ -286,6 +327,7 @@ def run_ours(a, rank, world, local):
     torch.cuda.synchronize()
     sampler = ClockSampler(dev)
     sampler.start()
+    sampler.wait_first()
     barrier(world)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
