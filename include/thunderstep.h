@@ -149,6 +149,32 @@ size_t te_kernel_table_json(char *buf, size_t n);
 /* Region hash of `words` host words with the reference formula (replay.js:407-418). */
 uint32_t te_region_hash_host(const uint32_t *words, uint64_t n);
 
+/* ---- Discrete adjoint of a step (no counterpart in the reference; the forward/backward
+ * pair behind a torch.autograd.Function-shaped host interface).  The adjoint memory has
+ * the layout of the word memory: the adjoint of the value at word w is the float at word
+ * w.  Supported steps are those whose every kernel has an adjoint operator: the
+ * dynamics-core step (WENO / upwind advection of th', u, v, w, the acoustic substeps and
+ * the buoyancy coupling, thermodynamic coefficients held fixed); other kernels fail with
+ * TE_ENOKERNEL.
+ *
+ * te_adjoint_forward: runs `nsteps` steps of the active step from the current memory,
+ *   copying the tape buffers every `checkpoint_every` steps (device memory:
+ *   ceil(nsteps / checkpoint_every) copies of the tape buffers, plus an undo log of
+ *   `checkpoint_every` steps: every region each op writes), and clears the adjoint memory.
+ * te_adjoint_backward: with the adjoint memory holding d(cost)/d(state after the last
+ *   step) (set with te_adjoint_write_words), replaces it by d(cost)/d(state before the
+ *   first step) and returns memory to that first state.  Each block of checkpoint_every
+ *   steps is replayed once from its checkpoint with the undo log, then walked in reverse
+ *   op by op. */
+int te_adjoint_forward(te_ctx *ctx, int nsteps, int checkpoint_every);
+int te_adjoint_backward(te_ctx *ctx);
+int te_adjoint_write_words(te_ctx *ctx, uint64_t word_off, const void *data, size_t bytes);
+int te_adjoint_read(te_ctx *ctx, uint64_t word_off, uint64_t words, void *out);
+int te_adjoint_zero(te_ctx *ctx);
+int te_adjoint_device_ptr(te_ctx *ctx, uint64_t word_off, void **out);
+/* Device bytes held by the adjoint state (adjoint memory, checkpoints, undo log). */
+int te_adjoint_memory(te_ctx *ctx, uint64_t *bytes);
+
 /* Fields of one vertically implicit w-pi' column solve: device pointers to the start of
  * each field (index 0 = point (i, j, k) = (-3, -3, 0) of the halo-3 layout, strideJ =
  * nx + 7, strideK = ny + 7). */

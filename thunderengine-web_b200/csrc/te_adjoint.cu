@@ -1,0 +1,457 @@
+// Discrete adjoint of a planned step (te_adjoint_* in include/thunderstep.h).
+//
+// The forward (te_adjoint_forward) runs N steps of the active step, keeping a copy of the
+// tape buffers every K steps (checkpoints).  The backward (te_adjoint_backward) walks the
+// blocks of K steps from the last: it restores the block's checkpoint and replays its steps
+// op by op, saving every region an op is about to write into an undo log; then it walks the
+// block's ops in reverse, restoring each op's written regions (so memory holds the values
+// before the op) and running the op's adjoint operator (te_adjoint.cuh), which turns the
+// adjoints of the values after the op into the adjoints of the values before it.  At the
+// end memory holds the state of step 0 and the adjoint memory the gradient with respect
+// to it.  Each block position has its own CUDA graph for the logged replay and for the
+// reverse walk, so a step costs two graph launches.
+//
+// The adjoint memory has the layout of the player's word memory: the adjoint of the value
+// at word w is the float at word w.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/thunderstep.h"
+#include "te_adjoint.cuh"
+#include "te_kernels.cuh"
+#include "te_player.hpp"
+
+namespace te {
+namespace adj {
+
+struct AccDevice {
+  __device__ static void add(float* p, float v) { atomicAdd(p, v); }
+};
+
+#define TE_ADJ_OP(Name, call)                                                           \
+  struct Name {                                                                         \
+    __device__ static void run(const AdjArgs<float>& A, int tx, int ty, int tz) { call; } \
+  };
+
+TE_ADJ_OP(OpFluxX, (adj_flux_lin_h<float, AccDevice>(A, tx, ty, tz, 0)))
+TE_ADJ_OP(OpFluxY, (adj_flux_lin_h<float, AccDevice>(A, tx, ty, tz, 1)))
+TE_ADJ_OP(OpFluxZ, (adj_flux_lin_z<float, AccDevice>(A, tx, ty, tz)))
+TE_ADJ_OP(OpStagX, (adj_flux_stag_h<float, AccDevice>(A, tx, ty, tz, 0)))
+TE_ADJ_OP(OpStagY, (adj_flux_stag_h<float, AccDevice>(A, tx, ty, tz, 1)))
+TE_ADJ_OP(OpStagZ, (adj_flux_stag_z<float, AccDevice>(A, tx, ty, tz)))
+TE_ADJ_OP(OpWenoX, (adj_flux_weno_h<float, AccDevice>(A, tx, ty, tz, 0)))
+TE_ADJ_OP(OpWenoY, (adj_flux_weno_h<float, AccDevice>(A, tx, ty, tz, 1)))
+TE_ADJ_OP(OpWenoZ, (adj_flux_weno_z<float, AccDevice>(A, tx, ty, tz)))
+TE_ADJ_OP(OpWenoUvX, (adj_flux_weno_uv_h<float, AccDevice>(A, tx, ty, tz, 0)))
+TE_ADJ_OP(OpWenoUvY, (adj_flux_weno_uv_h<float, AccDevice>(A, tx, ty, tz, 1)))
+TE_ADJ_OP(OpWenoUvZ, (adj_flux_weno_uv_z<float, AccDevice>(A, tx, ty, tz)))
+TE_ADJ_OP(OpWenoWX, (adj_flux_weno_w_h<float, AccDevice>(A, tx, ty, tz, 0)))
+TE_ADJ_OP(OpWenoWY, (adj_flux_weno_w_h<float, AccDevice>(A, tx, ty, tz, 1)))
+TE_ADJ_OP(OpWenoWZ, (adj_flux_weno_w_z<float, AccDevice>(A, tx, ty, tz)))
+TE_ADJ_OP(OpAssemble, (adj_assemble<float, AccDevice>(A, tx, ty, tz)))
+TE_ADJ_OP(OpRk, (adj_rk_update<float, AccDevice>(A, tx, ty, tz)))
+TE_ADJ_OP(OpThterm, (adj_apply_thterm<float, AccDevice>(A, tx, ty, tz)))
+TE_ADJ_OP(OpBuoy, (adj_buoyancy_apply<float, AccDevice>(A, tx, ty, tz)))
+TE_ADJ_OP(OpDiag, (adj_update_diagnostics_moist<float, AccDevice>(A, tx, ty, tz)))
+TE_ADJ_OP(OpTendReset, (adj_stage_tendency_reset<float, AccDevice>(A, tx, ty, tz)))
+TE_ADJ_OP(OpMassflux, (adj_massflux_from_state<float, AccDevice>(A, tx, ty, tz)))
+TE_ADJ_OP(OpDivMassflux, (adj_div_massflux<float, AccDevice>(A, tx, ty, tz)))
+TE_ADJ_OP(OpDiv3d, (adj_divergence3d<float, AccDevice>(A, tx, ty, tz)))
+TE_ADJ_OP(OpVelMassflux, (adj_velocity_to_massflux<float, AccDevice>(A, tx, ty, tz)))
+TE_ADJ_OP(OpSadv, (adj_build_sadv<float, AccDevice>(A, tx, ty, tz)))
+TE_ADJ_OP(OpStateReset, (adj_stage_state_reset<float, AccDevice>(A, tx, ty, tz)))
+TE_ADJ_OP(OpBegin, (adj_acoustic_begin<float, AccDevice>(A, tx, ty, tz)))
+TE_ADJ_OP(OpPrepare, (adj_acoustic_prepare<float, AccDevice>(A, tx, ty, tz)))
+TE_ADJ_OP(OpUv, (adj_acoustic_uv<float, AccDevice>(A, tx, ty, tz)))
+TE_ADJ_OP(OpFpk, (adj_acoustic_fpk<float, AccDevice>(A, tx, ty, tz)))
+TE_ADJ_OP(OpPp, (adj_acoustic_pp<float, AccDevice>(A, tx, ty, tz)))
+TE_ADJ_OP(OpAccum, (adj_acoustic_accumulate<float, AccDevice>(A, tx, ty, tz)))
+TE_ADJ_OP(OpHaloX, (adj_bc_periodic<float, AccDevice>(A, tx, ty, tz, 0)))
+TE_ADJ_OP(OpHaloY, (adj_bc_periodic<float, AccDevice>(A, tx, ty, tz, 1)))
+TE_ADJ_OP(OpPpxFinish, (adj_ppx_finish<float, AccDevice>(A, tx, ty, tz)))
+TE_ADJ_OP(OpWSolve, (adj_acoustic_w_solve<float, AccDevice>(A, tx, ty, tz)))
+
+// One thread per dispatch thread of the forward op (its grid in threads).
+template <class Op>
+__global__ void __launch_bounds__(128) k_adj(AdjArgs<float> A) {
+  const int tx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ty = blockIdx.y * blockDim.y + threadIdx.y;
+  const int tz = blockIdx.z;
+  if (tx >= A.gx || ty >= A.gy || tz >= A.gz) return;
+  Op::run(A, tx, ty, tz);
+}
+
+typedef void (*AdjLaunch)(const AdjArgs<float>&, cudaStream_t);
+
+template <class Op>
+static void launch_adj(const AdjArgs<float>& A, cudaStream_t s) {
+  if (A.gx <= 0 || A.gy <= 0 || A.gz <= 0) return;
+  launch_kernel(k_adj<Op>, dim3((A.gx + 31) / 32, (A.gy + 3) / 4, A.gz), dim3(32, 4, 1), 0, s, A);
+}
+
+struct AdjEntry {
+  const char* name;
+  AdjLaunch launch;
+};
+
+static const AdjEntry kAdjTable[] = {
+    {"adv_flux_x", launch_adj<OpFluxX>},
+    {"adv_flux_y", launch_adj<OpFluxY>},
+    {"adv_flux_z", launch_adj<OpFluxZ>},
+    {"adv_flux_x_stag", launch_adj<OpStagX>},
+    {"adv_flux_y_stag", launch_adj<OpStagY>},
+    {"adv_flux_z_stag", launch_adj<OpStagZ>},
+    {"adv_flux_x_weno", launch_adj<OpWenoX>},
+    {"adv_flux_y_weno", launch_adj<OpWenoY>},
+    {"adv_flux_z_weno", launch_adj<OpWenoZ>},
+    {"adv_flux_x_weno_uv", launch_adj<OpWenoUvX>},
+    {"adv_flux_y_weno_uv", launch_adj<OpWenoUvY>},
+    {"adv_flux_z_weno_uv", launch_adj<OpWenoUvZ>},
+    {"adv_flux_x_weno_w", launch_adj<OpWenoWX>},
+    {"adv_flux_y_weno_w", launch_adj<OpWenoWY>},
+    {"adv_flux_z_weno_w", launch_adj<OpWenoWZ>},
+    {"adv_assemble", launch_adj<OpAssemble>},
+    {"rk_update", launch_adj<OpRk>},
+    {"apply_thterm", launch_adj<OpThterm>},
+    {"buoyancy_apply", launch_adj<OpBuoy>},
+    {"update_diagnostics_moist", launch_adj<OpDiag>},
+    {"stage_tendency_reset", launch_adj<OpTendReset>},
+    {"massflux_from_state", launch_adj<OpMassflux>},
+    {"div_massflux", launch_adj<OpDivMassflux>},
+    {"divergence3d", launch_adj<OpDiv3d>},
+    {"velocity_to_massflux", launch_adj<OpVelMassflux>},
+    {"build_sadv", launch_adj<OpSadv>},
+    {"stage_state_reset", launch_adj<OpStateReset>},
+    {"acoustic_begin", launch_adj<OpBegin>},
+    {"acoustic_prepare", launch_adj<OpPrepare>},
+    {"acoustic_uv", launch_adj<OpUv>},
+    {"acoustic_fpk", launch_adj<OpFpk>},
+    {"acoustic_pp", launch_adj<OpPp>},
+    {"acoustic_accumulate", launch_adj<OpAccum>},
+    {"bc_periodic_x", launch_adj<OpHaloX>},
+    {"bc_periodic_y", launch_adj<OpHaloY>},
+    {"ppx_finish", launch_adj<OpPpxFinish>},
+    {"acoustic_w_solve", launch_adj<OpWSolve>},
+};
+
+static AdjLaunch find_adjoint(const std::string& name) {
+  for (const AdjEntry& e : kAdjTable)
+    if (name == e.name) return e.launch;
+  return nullptr;
+}
+
+// adjoint of a copy dst <- src (disjoint ranges): lambda_src += lambda_dst, lambda_dst = 0
+__global__ void k_adj_copy(float* L, uint64_t src, uint64_t dst, uint64_t n) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const float x = L[dst + i];
+    L[dst + i] = 0.0f;
+    L[src + i] += x;
+  }
+}
+
+}  // namespace adj
+
+struct Region {
+  uint64_t off, len;  // words
+};
+
+struct AdjointState {
+  float* L = nullptr;  // adjoint memory, mem_words floats
+  std::vector<uint32_t*> ckpt;
+  uint64_t ckpt_words = 0;
+  int nsteps = 0, every = 0;
+  const Step* step = nullptr;  // the step the tables below were built for
+  std::vector<std::vector<Region>> regions;  // per op: the regions it writes
+  std::vector<adj::AdjArgs<float>> args;     // per op
+  std::vector<adj::AdjLaunch> launch;        // per op (nullptr for copies)
+  uint64_t step_undo_words = 0;
+  uint32_t* undo = nullptr;
+  uint64_t undo_cap = 0;  // words
+  std::vector<cudaGraphExec_t> fwd_graph, rev_graph;  // per position in a block
+
+  void drop_graphs() {
+    for (auto g : fwd_graph)
+      if (g) cudaGraphExecDestroy(g);
+    for (auto g : rev_graph)
+      if (g) cudaGraphExecDestroy(g);
+    fwd_graph.clear();
+    rev_graph.clear();
+  }
+};
+
+void release_adjoint(Plan& P) {
+  AdjointState* S = P.adjoint;
+  if (!S) return;
+  S->drop_graphs();
+  for (auto p : S->ckpt) cudaFree(p);
+  if (S->L) cudaFree(S->L);
+  if (S->undo) cudaFree(S->undo);
+  delete S;
+  P.adjoint = nullptr;
+}
+
+namespace {
+
+struct AdjError : std::runtime_error {
+  int code;
+  AdjError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define ACU(x)                                                                                  \
+  do {                                                                                          \
+    cudaError_t e_ = (x);                                                                       \
+    if (e_ != cudaSuccess) throw te::AdjError(TE_ECUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+AdjointState& state(Plan& P) {
+  if (!P.adjoint) P.adjoint = new AdjointState();
+  return *P.adjoint;
+}
+
+// Per-op tables of the active step: written regions, adjoint arguments and operators.
+void build_tables(Plan& P, AdjointState& S) {
+  if (S.step == P.active && !S.args.empty()) return;
+  S.drop_graphs();
+  const std::vector<Op>& ops = P.active->ops;
+  S.regions.assign(ops.size(), {});
+  S.args.assign(ops.size(), adj::AdjArgs<float>());
+  S.launch.assign(ops.size(), nullptr);
+  S.step_undo_words = 0;
+  const uint32_t* M = P.M;
+  for (size_t i = 0; i < ops.size(); i++) {
+    const Op& o = ops[i];
+    if (o.copy) {
+      S.regions[i].push_back({o.dst, o.n});
+      S.step_undo_words += o.n;
+      continue;
+    }
+    if (!o.spec) throw AdjError(TE_ENOKERNEL, "no CUDA kernel for " + o.name);
+    S.launch[i] = adj::find_adjoint(o.name);
+    if (!S.launch[i]) throw AdjError(TE_ENOKERNEL, "no adjoint operator for " + o.name);
+    for (int q = 0; q < o.spec->nparams; q++) {
+      const ParamSpec& ps = o.spec->params[q];
+      if (ps.kind != kPtr || !ps.write) continue;
+      auto it = o.bind.find(ps.index);
+      if (it == o.bind.end()) continue;
+      const uint64_t len = P.region_len(it->second);
+      S.regions[i].push_back({it->second, len});
+      S.step_undo_words += len;
+    }
+    adj::AdjArgs<float>& a = S.args[i];
+    std::memset(&a, 0, sizeof a);
+    a.g = o.args.g;
+    a.a = o.args.a;
+    a.gx = o.args.gx;
+    a.gy = o.args.gy;
+    a.gz = o.args.gz;
+    for (int n = 0; n < adj::kMaxBindA && n < kMaxBind; n++) {
+      a.p[n] = o.args.p[n];
+      a.l[n] = o.args.p[n] ? S.L + (reinterpret_cast<const uint32_t*>(o.args.p[n]) - M) : nullptr;
+      a.f[n] = o.args.f[n];
+      a.iv[n] = o.args.iv[n];
+      a.iv2[n] = o.args.iv2[n];
+    }
+  }
+  S.step = P.active;
+}
+
+// Replays the active step op by op, saving each op's written regions at log + cursor.
+void logged_step(Plan& P, AdjointState& S, uint32_t* log) {
+  std::vector<Op>& ops = P.active->ops;
+  uint64_t cur = 0;
+  for (size_t i = 0; i < ops.size(); i++) {
+    for (const Region& r : S.regions[i]) {
+      ACU(cudaMemcpyAsync(log + cur, P.M + r.off, r.len * 4, cudaMemcpyDeviceToDevice, P.stream));
+      cur += r.len;
+    }
+    P.launch_exact(ops, (int)i, (int)i, false);
+  }
+}
+
+// Walks the active step's ops in reverse: restore the op's written regions, run its adjoint.
+void reverse_step(Plan& P, AdjointState& S, const uint32_t* log) {
+  std::vector<Op>& ops = P.active->ops;
+  uint64_t cur = S.step_undo_words;
+  for (size_t ii = ops.size(); ii-- > 0;) {
+    const Op& o = ops[ii];
+    for (size_t q = S.regions[ii].size(); q-- > 0;) {
+      const Region& r = S.regions[ii][q];
+      cur -= r.len;
+      ACU(cudaMemcpyAsync(P.M + r.off, log + cur, r.len * 4, cudaMemcpyDeviceToDevice, P.stream));
+    }
+    if (o.copy) {
+      const int blocks = (int)std::min<uint64_t>(1024, (o.n + 255) / 256);
+      launch_kernel(adj::k_adj_copy, dim3(blocks), dim3(256), 0, P.stream, S.L, o.src, o.dst, o.n);
+    } else {
+      S.launch[ii](S.args[ii], P.stream);
+    }
+  }
+}
+
+template <class F>
+cudaGraphExec_t capture(cudaStream_t s, F body) {
+  cudaGraph_t graph = nullptr;
+  ACU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  try {
+    body();
+  } catch (...) {
+    cudaStreamEndCapture(s, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  ACU(cudaStreamEndCapture(s, &graph));
+  cudaGraphExec_t ex = nullptr;
+  const cudaError_t e = cudaGraphInstantiate(&ex, graph, 0);
+  cudaGraphDestroy(graph);
+  ACU(e);
+  return ex;
+}
+
+int fail(te_ctx* ctx, int code, const std::string& m) {
+  ctx->err = m;
+  return code;
+}
+
+}  // namespace
+}  // namespace te
+
+#define ADJ_BEGIN(ctx) \
+  if (!ctx) return TE_EINVAL; \
+  try {
+#define ADJ_END(ctx)                                                        \
+  }                                                                         \
+  catch (const te::AdjError& e) { return te::fail(ctx, e.code, e.what()); } \
+  catch (const std::exception& e) { return te::fail(ctx, TE_EINVAL, e.what()); } \
+  return TE_OK;
+
+extern "C" {
+
+int te_adjoint_forward(te_ctx* ctx, int nsteps, int checkpoint_every) {
+  ADJ_BEGIN(ctx)
+  te::Plan& P = ctx->plan;
+  if (!P.M) throw te::AdjError(TE_ESTATE, "te_plan has not been called");
+  if (nsteps < 1 || checkpoint_every < 1) throw te::AdjError(TE_EINVAL, "nsteps and checkpoint_every must be >= 1");
+  ACU(cudaSetDevice(ctx->device));
+  te::AdjointState& S = te::state(P);
+  if (!S.L) {
+    ACU(cudaMalloc(&S.L, P.mem_words * 4));
+  }
+  ACU(cudaMemsetAsync(S.L, 0, P.mem_words * 4, P.stream));
+  te::build_tables(P, S);
+  const int nck = (nsteps + checkpoint_every - 1) / checkpoint_every;
+  S.ckpt_words = P.buffers_end;
+  while ((int)S.ckpt.size() < nck) {
+    uint32_t* p = nullptr;
+    ACU(cudaMalloc(&p, S.ckpt_words * 4));
+    S.ckpt.push_back(p);
+  }
+  const uint64_t need = (uint64_t)checkpoint_every * S.step_undo_words;
+  if (need > S.undo_cap) {
+    if (S.undo) cudaFree(S.undo);
+    S.undo = nullptr;
+    S.undo_cap = 0;
+    ACU(cudaMalloc(&S.undo, need * 4));
+    S.undo_cap = need;
+  }
+  if (S.every != checkpoint_every) S.drop_graphs();
+  S.every = checkpoint_every;
+  S.nsteps = nsteps;
+  for (int s = 0; s < nsteps; s++) {
+    if (s % checkpoint_every == 0)
+      ACU(cudaMemcpyAsync(S.ckpt[s / checkpoint_every], P.M, S.ckpt_words * 4, cudaMemcpyDeviceToDevice, P.stream));
+    P.launch_step_graph();
+  }
+  ACU(cudaGetLastError());
+  ADJ_END(ctx)
+}
+
+int te_adjoint_backward(te_ctx* ctx) {
+  ADJ_BEGIN(ctx)
+  te::Plan& P = ctx->plan;
+  te::AdjointState* Sp = P.adjoint;
+  if (!P.M || !Sp || Sp->nsteps < 1) throw te::AdjError(TE_ESTATE, "te_adjoint_forward has not been called");
+  te::AdjointState& S = *Sp;
+  ACU(cudaSetDevice(ctx->device));
+  te::build_tables(P, S);
+  const int K = S.every;
+  if ((uint64_t)K * S.step_undo_words > S.undo_cap) throw te::AdjError(TE_ESTATE, "step changed since te_adjoint_forward");
+  if ((int)S.fwd_graph.size() != K) {
+    S.drop_graphs();
+    S.fwd_graph.assign(K, nullptr);
+    S.rev_graph.assign(K, nullptr);
+  }
+  const int nb = (S.nsteps + K - 1) / K;
+  for (int b = nb - 1; b >= 0; b--) {
+    const int s0 = b * K, s1 = std::min(s0 + K, S.nsteps);
+    ACU(cudaMemcpyAsync(P.M, S.ckpt[b], S.ckpt_words * 4, cudaMemcpyDeviceToDevice, P.stream));
+    for (int s = s0; s < s1; s++) {
+      const int j = s - s0;
+      if (!S.fwd_graph[j])
+        S.fwd_graph[j] = te::capture(P.stream, [&] { te::logged_step(P, S, S.undo + (uint64_t)j * S.step_undo_words); });
+      ACU(cudaGraphLaunch(S.fwd_graph[j], P.stream));
+    }
+    for (int s = s1 - 1; s >= s0; s--) {
+      const int j = s - s0;
+      if (!S.rev_graph[j])
+        S.rev_graph[j] = te::capture(P.stream, [&] { te::reverse_step(P, S, S.undo + (uint64_t)j * S.step_undo_words); });
+      ACU(cudaGraphLaunch(S.rev_graph[j], P.stream));
+    }
+  }
+  ACU(cudaGetLastError());
+  ADJ_END(ctx)
+}
+
+int te_adjoint_write_words(te_ctx* ctx, uint64_t word_off, const void* data, size_t bytes) {
+  ADJ_BEGIN(ctx)
+  te::Plan& P = ctx->plan;
+  if (!P.adjoint || !P.adjoint->L) throw te::AdjError(TE_ESTATE, "te_adjoint_forward has not been called");
+  if (word_off + (bytes + 3) / 4 > P.mem_words) throw te::AdjError(TE_ERANGE, "write past the end of memory");
+  ACU(cudaSetDevice(ctx->device));
+  ACU(cudaMemcpyAsync(P.adjoint->L + word_off, data, bytes, cudaMemcpyHostToDevice, P.stream));
+  ACU(cudaStreamSynchronize(P.stream));
+  ADJ_END(ctx)
+}
+
+int te_adjoint_read(te_ctx* ctx, uint64_t word_off, uint64_t words, void* out) {
+  ADJ_BEGIN(ctx)
+  te::Plan& P = ctx->plan;
+  if (!P.adjoint || !P.adjoint->L) throw te::AdjError(TE_ESTATE, "te_adjoint_forward has not been called");
+  if (word_off + words > P.mem_words) throw te::AdjError(TE_ERANGE, "read past the end of memory");
+  ACU(cudaSetDevice(ctx->device));
+  ACU(cudaMemcpyAsync(out, P.adjoint->L + word_off, words * 4, cudaMemcpyDeviceToHost, P.stream));
+  ACU(cudaStreamSynchronize(P.stream));
+  ADJ_END(ctx)
+}
+
+int te_adjoint_zero(te_ctx* ctx) {
+  ADJ_BEGIN(ctx)
+  te::Plan& P = ctx->plan;
+  if (!P.adjoint || !P.adjoint->L) throw te::AdjError(TE_ESTATE, "te_adjoint_forward has not been called");
+  ACU(cudaSetDevice(ctx->device));
+  ACU(cudaMemsetAsync(P.adjoint->L, 0, P.mem_words * 4, P.stream));
+  ADJ_END(ctx)
+}
+
+int te_adjoint_device_ptr(te_ctx* ctx, uint64_t word_off, void** out) {
+  ADJ_BEGIN(ctx)
+  te::Plan& P = ctx->plan;
+  if (!P.adjoint || !P.adjoint->L) throw te::AdjError(TE_ESTATE, "te_adjoint_forward has not been called");
+  if (word_off >= P.mem_words) throw te::AdjError(TE_ERANGE, "offset outside memory");
+  *out = P.adjoint->L + word_off;
+  ADJ_END(ctx)
+}
+
+int te_adjoint_memory(te_ctx* ctx, uint64_t* bytes) {
+  ADJ_BEGIN(ctx)
+  te::Plan& P = ctx->plan;
+  const te::AdjointState* S = P.adjoint;
+  *bytes = S ? (S->L ? P.mem_words * 4 : 0) + S->ckpt.size() * S->ckpt_words * 4 + S->undo_cap * 4 : 0;
+  ADJ_END(ctx)
+}
+
+}  // extern "C"

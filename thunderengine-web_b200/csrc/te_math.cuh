@@ -8,20 +8,10 @@
 #pragma once
 #include <cstdint>
 
+#include "te_dims.cuh"
+
 namespace te {
 
-struct Dims {
-  int nx, ny, nz, sJ, sK;
-  float rdx, rdy, rdz;
-};
-
-struct Acoustic {
-  float dts, alph, beta, kdiv, smeps;
-};
-
-__host__ __device__ __forceinline__ int gidx(const Dims& g, int i, int j, int k) {
-  return (i + 3) + g.sJ * ((j + 3) + g.sK * k);
-}
 
 // Correctly rounded quotient.  The reference's div_cr returns the correctly rounded
 // quotient in the normal range and the plain quotient for zero, huge, NaN and tiny

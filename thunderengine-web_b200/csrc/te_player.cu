@@ -100,13 +100,6 @@ __global__ void k_region_hash(const uint32_t* __restrict__ M, uint64_t off, uint
 
 using namespace te;
 
-struct te_ctx {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  std::string err;
-  Plan plan;
-};
-
 namespace te {
 
 // ------------------------------------------------------------------ planning
@@ -802,6 +795,7 @@ void Plan::launch_step_graph() {
 }
 
 void Plan::release() {
+  release_adjoint(*this);
   invalidate_graphs();
   fused.release();
   if (M) cudaFree(M);

@@ -53,6 +53,8 @@ struct BufInfo {
   bool arena;
 };
 
+struct AdjointState;  // te_adjoint.cu
+
 struct Plan {
   cudaStream_t stream = nullptr;
   int mode = 0;
@@ -76,6 +78,7 @@ struct Plan {
   cudaGraphExec_t graph_exec = nullptr;
   FusedStep fused;
   bool fused_dirty = true;
+  AdjointState* adjoint = nullptr;  // checkpoints, undo log and adjoint memory of te_adjoint_*
 
   void load_kernel_meta(const char* kjson, size_t klen);
   std::map<int, uint64_t> layout_bytes(const JValue& cmds);
@@ -89,4 +92,14 @@ struct Plan {
   void release();
 };
 
+void release_adjoint(Plan& P);  // te_adjoint.cu
+
 }  // namespace te
+
+// One player context (include/thunderstep.h te_ctx).
+struct te_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  te::Plan plan;
+};

@@ -88,6 +88,13 @@ EXPORTS = {
     'te_run_segment': ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     'te_write_words_async': ([ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_size_t], ctypes.c_int),
     'te_read_async': ([ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p], ctypes.c_int),
+    'te_adjoint_forward': ([ctypes.c_void_p, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    'te_adjoint_backward': ([ctypes.c_void_p], ctypes.c_int),
+    'te_adjoint_write_words': ([ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_size_t], ctypes.c_int),
+    'te_adjoint_read': ([ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p], ctypes.c_int),
+    'te_adjoint_zero': ([ctypes.c_void_p], ctypes.c_int),
+    'te_adjoint_device_ptr': ([ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    'te_adjoint_memory': ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
     'te_w_solve_static_scratch': ([ctypes.POINTER(TeWSolveFields), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                    ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_void_p,
                                    ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
@@ -245,6 +252,34 @@ class Replayer:
 
     def run_segment(self, seg, part=-1):
         self._check(self.lib.te_run_segment(self.h, int(seg), int(part)))
+
+    # ---- discrete adjoint (te_adjoint_*; no counterpart in the reference)
+    def adjoint_forward(self, nsteps, checkpoint_every):
+        """Runs nsteps steps keeping checkpoints every checkpoint_every steps; clears the
+        adjoint memory."""
+        self._check(self.lib.te_adjoint_forward(self.h, int(nsteps), int(checkpoint_every)))
+
+    def adjoint_backward(self):
+        """Adjoint memory: d(cost)/d(final state) -> d(cost)/d(initial state); memory
+        returns to the initial state."""
+        self._check(self.lib.te_adjoint_backward(self.h))
+
+    def adjoint_write_words(self, off, data):
+        a = np.ascontiguousarray(np.asarray(data))
+        self._check(self.lib.te_adjoint_write_words(self.h, int(off), a.ctypes.data, a.nbytes))
+
+    def adjoint_read(self, words, off_words=0):
+        out = np.empty(int(words), dtype=np.float32)
+        self._check(self.lib.te_adjoint_read(self.h, int(off_words), int(words), out.ctypes.data))
+        return out
+
+    def adjoint_zero(self):
+        self._check(self.lib.te_adjoint_zero(self.h))
+
+    def adjoint_memory(self):
+        n = ctypes.c_uint64()
+        self._check(self.lib.te_adjoint_memory(self.h, ctypes.byref(n)))
+        return n.value
 
     def sync(self):
         self._check(self.lib.te_sync(self.h))

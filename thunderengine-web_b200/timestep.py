@@ -112,6 +112,11 @@ SCRATCH_FIELDS = ['rru', 'rrv', 'rrw', 'fx', 'fy', 'fz', 'tend', 'divx', 'qk', '
                   'cB', 'sadv']
 
 
+# Sink fields of the dynamics-core step: update_diagnostics_moist writes its thv, ppterm,
+# piadv and thterm here, so those coefficients keep their window-start values.
+CORE_SINKS = ['xthv', 'xppterm', 'xpiadv', 'xthterm']
+
+
 class Run:
     """A synthetic run: grid, profiles, arena and the encoder state (driver.buildRun).
 
@@ -120,15 +125,16 @@ class Run:
     a moist step bind it (timestep.js:1473-1479).
     """
 
-    def __init__(self, cfg, weno_momentum=True):
+    def __init__(self, cfg, weno_momentum=True, core=False):
         self.cfg = cfg
+        self.core = core
         self.grid = sc.Grid(cfg.nx, cfg.ny, cfg.nz, cfg.dx, cfg.dy, cfg.dz)
         self.prof = sc.profiles(cfg)
         self.dt = f(cfg.dt)
         self.schedule = AcousticSchedule(cfg.nsound, self.dt)
         self.weno_scalars = True
         self.weno_momentum = weno_momentum
-        names = sorted(set(STATE_FIELDS_MOIST + SCRATCH_FIELDS), key=lambda s: s.encode())
+        names = sorted(set(STATE_FIELDS_MOIST + SCRATCH_FIELDS + (CORE_SINKS if core else [])), key=lambda s: s.encode())
         g = self.grid
         self.fields = {n: i * g.field_stride for i, n in enumerate(names)}
         self.arena_bytes = g.field_stride * len(names)
@@ -169,8 +175,21 @@ class Run:
         a = self.acoustic
         return pack('fffff', [a['dts'], a['alph'], a['beta'], a['kdiv'], a['smeps']])
 
-    def encode(self):
-        """Commands of one large step."""
+    def encode(self, core=False):
+        """Commands of one large step.
+
+        ``core=True`` encodes the dynamics-core step that the discrete adjoint
+        differentiates: the same kernels and order, with the thermodynamic fields held at
+        their values when the window starts - no pressure_tendency (ppten fixed),
+        update_diagnostics_moist writing thv, ppterm, piadv and thterm to sink fields
+        (only its buoyancy is live), so acoustic_prepare forms each stage's implicit
+        coefficients from fixed fields and that stage's dts - and without the moisture
+        and diabatic kernels (qv advection and its pdef correction, diabatic_*,
+        update_rho_prs).  The state it advances is th', u, v, w, pi' (pp3d, ppi, ppx).
+        Needs a Run made with core=True.
+        """
+        if core and not self.core:
+            raise ValueError('the dynamics-core step needs Run(..., core=True) (its sink fields)')
         cmds = []
         rec = self.rec
         g = self.grid
@@ -232,7 +251,8 @@ class Run:
             by(I1(0), 12)
             fld('qvten_t', 13)
             by(I1(1), 14)
-        enc('pressure_tendency', full, TG3, False, pt)
+        if not core:
+            enc('pressure_tendency', full, TG3, False, pt)
 
         for nrk in range(3):
             dttmp_v = f(dt / (3 - nrk))
@@ -245,7 +265,8 @@ class Run:
                     buf(n, i + 3)
                 for i, n in enumerate(['qv', 'qc', 'qr', 'qi', 'qs', 'qg']):
                     fld('qv' if n == 'qv' else 'qzero', i + 9)
-                for i, n in enumerate(['thv', 'ppterm', 'piadv', 'thterm', 'buoy']):
+                outs = CORE_SINKS + ['buoy'] if core else ['thv', 'ppterm', 'piadv', 'thterm', 'buoy']
+                for i, n in enumerate(outs):
                     fld(n, i + 15)
             enc('update_diagnostics_moist', whole, TG3, False, diag)
 
@@ -442,6 +463,8 @@ class Run:
             # 5. scalar advection (timestep.js:2115-2127)
             enc('build_sadv', whole, TG3, False, lambda: (buf('th0', 1), fld('th', 2), fld('sadv', 3)))
             advect('sadv', state='th')
+            if core:
+                continue
             advect('qv')
             if nrk == 2:
                 dtb = F1(dt)
@@ -452,23 +475,26 @@ class Run:
                     lambda: (by(I1(1), 1), fld('th', 2), fld('pp3d', 3), buf('th0', 4), buf('pi0', 5), fld('qv', 6),
                              fld('prs', 7), fld('rho', 8)))
         dtb = F1(dt)
-        enc('diabatic_rates', full, TG3, False,
-            lambda: (by(dtb, 1), [fld(n, i + 2) for i, n in
-                                  enumerate(['pp3d', 'th', 'qv', 'qc', 'qpten', 'qtten', 'qvten', 'qcten'])]))
+        if not core:
+            enc('diabatic_rates', full, TG3, False,
+                lambda: (by(dtb, 1), [fld(n, i + 2) for i, n in
+                                      enumerate(['pp3d', 'th', 'qv', 'qc', 'qpten', 'qtten', 'qvten', 'qcten'])]))
         enc('ppx_finish', full, TG3, False, lambda: (fld('pp3d', 1), fld('ppx', 2)))
         halo_fill('ppx')
         cmds.append({'op': 'end'})
         # state swap (timestep.js:766-774)
         nbytes = g.count * 4
         aid = rec.id('arena')
-        for src, dst in [('th', 'th_a'), ('qv', 'qv_a'), ('u', 'u_a'), ('v', 'v_a'), ('w', 'w_a'), ('pp3d', 'ppi')]:
+        swaps = [('th', 'th_a'), ('qv', 'qv_a'), ('u', 'u_a'), ('v', 'v_a'), ('w', 'w_a'), ('pp3d', 'ppi')]
+        for src, dst in [sw for sw in swaps if not (core and sw[0] == 'qv')]:
             cmds.append({'op': 'copy', 'src': aid, 'srcOffset': self.fields[src], 'dst': aid,
                          'dstOffset': self.fields[dst], 'size': nbytes})
         return cmds
 
-    def tape(self, nsteps=1):
-        """Tape in the reference format (driver.js:62-74)."""
-        steps = [self.encode() for _ in range(max(1, nsteps))]
+    def tape(self, nsteps=1, core=False):
+        """Tape in the reference format (driver.js:62-74); ``core`` selects the
+        dynamics-core step (see encode)."""
+        steps = [self.encode(core=core) for _ in range(max(1, nsteps))]
         g = self.grid
         buffers = [{'id': i, 'length': self.buffer_length(n), 'label': n, 'arena': n == 'arena'}
                    for i, n in enumerate(self.rec.buffers)]
