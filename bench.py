@@ -40,6 +40,9 @@ def parse():
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-roofline', action='store_true', help='skip the per-kernel timing pass')
     ap.add_argument('--no-fp64', action='store_true', help='skip the error statement against the binary64 oracle')
+    ap.add_argument('--no-adjoint', action='store_true', help='skip the adjoint window (128x128x64, 60 steps)')
+    ap.add_argument('--no-ensemble', action='store_true', help='skip the 64-member uneven ensemble')
+    ap.add_argument('--ensemble-members', type=int, default=64)
     ap.add_argument('--workload', default='at_scale', choices=['at_scale', 'medium', 'small'],
                     help='at_scale = 256x256x80 (the benchmark); medium = 160x160x80 with the same '
                          'physics, for profiler captures; small = 64x64x40')
@@ -299,6 +302,127 @@ def fp64_error(r, run, init, checkpoints=(1, 20)):
     return out
 
 
+def adjoint_leg(dev, nx=128, ny=128, nz=64, steps=60, every=10):
+    """The adjoint configuration: a window of `steps` dynamics-core steps at nx x ny x nz
+    (physics of the 256x256x80 workload) with checkpoints every `every` steps, cost
+    J = sum of w^2 dx dy dz at the end.  Times, with CUDA events on the window's stream:
+    the plain window (graph replay of the step), the forward with checkpoints and the
+    backward (replay of each block with the undo log + the reverse walk)."""
+    import torch
+    from thunderengine_web_b200 import scenario, timestep
+    from thunderengine_web_b200.adjoint import CoreWindow
+    from thunderengine_web_b200.replayer import Replayer
+    cfg = scenario.tiny(nx, ny, nz, dx=500.0, dz=250.0, dt=3.0, nsound=8, us=25.0)
+    run = timestep.Run(cfg, core=True)
+    tape = run.tape(1)
+    r = Replayer(tape, None, device=dev)
+    r.plan(False)
+    r.build()
+    for i, b in run.initial_buffers().items():
+        r.upload(i, b)
+    r.encode_steps(1)  # the window starts after one regular step
+    r.sync()
+    init = {b['id']: r.read(b['length'] // 4, r.base[b['id']]).tobytes() for b in tape['buffers']}
+    r.close()
+    win = CoreWindow(run, init, steps, checkpoint_every=every, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    win.r.set_stream(stream.cuda_stream)
+    g = run.grid
+    arena = np.frombuffer(init[run.rec.ids['arena']], dtype=np.float32)
+    ctl = [arena[run.fields[n] // 4:run.fields[n] // 4 + g.count].reshape(g.nz + 1, g.strideK, g.strideJ)
+           [:g.nz, 3:3 + g.ny, 3:3 + g.nx] for n in ('th', 'u', 'v')]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3, out
+
+    win.r.encode_steps(2)
+    t_plain, _ = timed(lambda: win.r.encode_steps(steps))
+    w = win.forward(*ctl)
+    dV = g.dx * g.dy * g.dz
+    gw = 2.0 * w.astype(np.float64) * dV
+    win.backward(gw)  # captures the block graphs
+    t_fwd, w = timed(lambda: win.forward(*ctl))
+    lw = np.zeros((g.nz + 1, g.strideK, g.strideJ), dtype=np.float32)
+    lw[1:g.nz, 3:3 + g.ny, 3:3 + g.nx] = 2.0 * w.astype(np.float64) * dV
+    win.r.adjoint_zero()
+    win.r.adjoint_write_words(win.base + run.fields['w'] // 4, lw.ravel())
+    t_bwd, _ = timed(lambda: win.r.adjoint_backward())
+    pts = g.nx * g.ny * g.nz
+    out = {'grid': [nx, ny, nz], 'window_steps': steps, 'checkpoint_every': every, 'cost': 'sum of w^2 dx dy dz at the end',
+           'control': "th', u, v at the start", 'dtype': 'f32',
+           'value': pts * steps / t_bwd, 'unit': 'grid-pt-steps/s (adjoint: backward with recompute)',
+           'forward_value': pts * steps / t_plain, 'backward_s': t_bwd, 'plain_window_s': t_plain,
+           'forward_with_checkpoints_s': t_fwd, 'backward_over_forward': t_bwd / t_plain,
+           'device_bytes': win.r.adjoint_memory(),
+           'timing': 'CUDA events on the window stream; forward = graph replay of the dynamics-core step'}
+    win.close()
+    return out
+
+
+def ensemble_leg(dev, n=64, steps=50, warmup=2):
+    """The batched-ensemble configuration: `n` members of uneven grids from 64x64x40 to
+    192x192x64 (seeded sizes, CAPE, shear, dt 3/6 s, nsound 6..8), fused mode, block
+    shapes autotuned per member.  member-steps/s of one ensemble graph launch per large
+    step against looping the plain step member by member on one stream."""
+    import torch
+    from thunderengine_web_b200 import scenario, timestep
+    from thunderengine_web_b200.replayer import Ensemble, Replayer, TE_MODE_FUSED
+    cfgs = scenario.ensemble(n, seed=7, steps=steps)
+    stream = torch.cuda.Stream(device=dev)
+    reps, tuned, pts = [], 0, 0
+    for cfg in cfgs:
+        run = timestep.Run(cfg)
+        r = Replayer(run.tape(1), None, device=dev)
+        r.plan(False)
+        r.build()
+        for i, b in run.initial_buffers().items():
+            r.upload(i, b)
+        r.set_mode(TE_MODE_FUSED)
+        tuned += r.autotune(reps=2)
+        r.set_stream(stream.cuda_stream)
+        reps.append(r)
+        pts += cfg.nx * cfg.ny * cfg.nz
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # looping the plain step: every member's step graph, one member after another
+    for _ in range(warmup):
+        for r in reps:
+            r.encode_steps(1)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        for r in reps:
+            r.encode_steps(1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_loop = e0.elapsed_time(e1) / 1e3
+    ens = Ensemble(reps)
+    es = torch.cuda.ExternalStream(ens.stream(), device=dev)
+    ens.run(warmup)
+    ens.sync()
+    e0.record(es)
+    ens.run(steps)
+    e1.record(es)
+    torch.cuda.synchronize()
+    t_ens = e0.elapsed_time(e1) / 1e3
+    ens.close()
+    mem = sum(r.mem_words for r in reps) * 4
+    for r in reps:
+        r.close()
+    return {'members': n, 'steps': steps, 'value': n * steps / t_ens, 'unit': 'member-steps/s',
+            'loop_value': n * steps / t_loop, 'speedup_vs_loop': t_loop / t_ens,
+            'grid_pt_steps_per_s': pts * steps / t_ens, 'grid_points_total': pts,
+            'substeps_per_step': sorted({timestep.AcousticSchedule(c.nsound, timestep.f(c.dt)).total for c in cfgs}),
+            'autotuned_ops': tuned, 'device_bytes': mem, 'mode': 'fused',
+            'how': 'one graph launch per large step (every member a child graph, no edges between members) vs '
+                   'each member\'s step graph launched in turn on one stream; CUDA events'}
+
+
 # ---------------------------------------------------------------- our arm
 
 def run_ours(a, rank, world, local):
@@ -351,6 +475,8 @@ def run_ours(a, rank, world, local):
     cpu = None
     parity = None
     f64err = None
+    adjoint = None if (a.no_adjoint or rank != 0) else adjoint_leg(dev)
+    ens = None if (a.no_ensemble or rank != 0) else ensemble_leg(dev, a.ensemble_members)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline_sample()
         parity = parity_vs_cpu(r, run, init, cpu.pop('_after_one_step'), cpu['kind'])
@@ -370,7 +496,7 @@ def run_ours(a, rank, world, local):
                        tape_ops_per_step=ops,
                        l2='inputs larger than L2: %.2f GB arena per replica' % (run.arena_bytes / 1e9)),
         'roofline': roof, 'cpu_baseline': cpu, 'e2e': e2e, 'gpu_launches': launches * a.steps, 'clocks': clocks,
-        'parity': parity, 'fp64_error': f64err,
+        'parity': parity, 'fp64_error': f64err, 'adjoint': adjoint, 'ensemble': ens,
     }
     if rank == 0:
         print(json.dumps(out))

@@ -175,6 +175,28 @@ int te_adjoint_device_ptr(te_ctx *ctx, uint64_t word_off, void **out);
 /* Device bytes held by the adjoint state (adjoint memory, checkpoints, undo log). */
 int te_adjoint_memory(te_ctx *ctx, uint64_t *bytes);
 
+/* ---- Launch-shape autotuner (no counterpart in the reference).  Times every candidate
+ * thread-block shape of each per-dispatch op of the active step whose launcher takes its
+ * block from the op (`reps` launches each, CUDA events on the context's stream), keeps a
+ * shape only when it beats the default 32 x 4 by more than 3 %, and restores memory
+ * afterwards.  *tuned_ops (may be NULL) receives the number of ops that changed shape. */
+int te_autotune(te_ctx *ctx, int reps, int *tuned_ops);
+
+/* ---- Ensembles (no counterpart in the reference): independent planned contexts on one
+ * device, of any grid size, time step and substep count, advanced together.  Each
+ * member's step (in the member's mode at creation) becomes a child graph of one
+ * ensemble graph without edges between members; te_ensemble_run launches it once per
+ * large step on the ensemble's own stream, so the members' kernels run concurrently.
+ * Members must not be stepped through their own contexts while an ensemble run is in
+ * flight; te_ensemble_sync waits for it. */
+typedef struct te_ensemble te_ensemble;
+int te_ensemble_create(te_ctx *const *members, int n, te_ensemble **out);
+int te_ensemble_run(te_ensemble *ens, int nsteps);
+int te_ensemble_stream(te_ensemble *ens, void **cuda_stream);
+int te_ensemble_sync(te_ensemble *ens);
+const char *te_ensemble_last_error(te_ensemble *ens);
+void te_ensemble_destroy(te_ensemble *ens);
+
 /* Fields of one vertically implicit w-pi' column solve: device pointers to the start of
  * each field (index 0 = point (i, j, k) = (-3, -3, 0) of the halo-3 layout, strideJ =
  * nx + 7, strideK = ny + 7). */

@@ -39,8 +39,15 @@ def adjoint_lib():
 
 
 class CpuAdjoint64:
-    def __init__(self, tape, kernels_meta, init):
+    """``linearize='f64'``: the forward and the states the adjoint operators see are the
+    binary64 twin's.  ``linearize='f32'``: they are the binary32 oracle's (the trajectory
+    the GPU follows bit for bit), widened to binary64 for the adjoint operators - the
+    binary64 adjoint around the GPU's own trajectory."""
+
+    def __init__(self, tape, kernels_meta, init, linearize='f64', kernels32=None):
         self.km = kernels_meta
+        self.f32 = linearize == 'f32'
+        self.k32 = kernels32
         self.p = CpuPlayer64(tape, kernels_meta)
         self.p.plan()
         for i, b in init.items():
@@ -70,6 +77,30 @@ class CpuAdjoint64:
     def D(self):
         return self.p.D
 
+    def _step(self):
+        """One forward step of the chosen trajectory (D mirrors M in binary32 mode)."""
+        if self.f32:
+            p = self.p
+            mp = p.M.ctypes.data_as(ctypes.c_void_p)
+            for o in p.ops:
+                if o.kind == 'copy':
+                    p.M[o.dst:o.dst + o.n] = p.M[o.src:o.src + o.n]
+                else:
+                    self.k32(o.name)(mp, o.arg.ctypes.data_as(ctypes.c_void_p))
+            p.D[:] = p.M.view(np.float32)
+        else:
+            self.p.run64(1)
+
+    def _state(self):
+        return (self.p.M.copy(), self.p.D.copy()) if self.f32 else self.p.D.copy()
+
+    def _set_state(self, st):
+        if self.f32:
+            self.p.M[:] = st[0]
+            self.p.D[:] = st[1]
+        else:
+            self.p.D[:] = st
+
     def forward(self, nsteps, checkpoint_every=None):
         """Runs nsteps steps from the current state, keeping the start state of every
         `checkpoint_every`-th step (every step by default)."""
@@ -78,18 +109,18 @@ class CpuAdjoint64:
         self.ckpt = {}
         for s in range(nsteps):
             if s % self.every == 0:
-                self.ckpt[s] = self.p.D.copy()
-            self.p.run64(1)
+                self.ckpt[s] = self._state()
+            self._step()
 
     def _step_starts(self, b):
         """Start states of the steps of block b, replayed from its checkpoint."""
         s0, s1 = b * self.every, min((b + 1) * self.every, self.nsteps)
-        self.p.D[:] = self.ckpt[s0]
+        self._set_state(self.ckpt[s0])
         out = []
         for s in range(s0, s1):
-            out.append(self.p.D.copy())
+            out.append(self._state())
             if s + 1 < s1:
-                self.p.run64(1)
+                self._step()
         return out
 
     def backward(self, L):
@@ -110,19 +141,27 @@ class CpuAdjoint64:
 
     def _reverse_step(self, start, L, mp, dp, lp):
         p = self.p
-        p.D[:] = start
+        self._set_state(start)
         log = []
         for o, (mask, acu, regions) in zip(p.ops, self.info):
-            log.append([p.D[off:off + n].copy() for off, n in regions])
+            log.append([(p.D[off:off + n].copy(), p.M[off:off + n].copy() if self.f32 else None)
+                        for off, n in regions])
             if o.kind == 'copy':
                 p.D[o.dst:o.dst + o.n] = p.D[o.src:o.src + o.n]
+                p.M[o.dst:o.dst + o.n] = p.M[o.src:o.src + o.n]
+            elif self.f32:
+                self.k32(o.name)(mp, o.arg.ctypes.data_as(ctypes.c_void_p))
+                for off, n in regions:
+                    p.D[off:off + n] = p.M[off:off + n].view(np.float32)
             else:
                 p.kernel(o.name)(mp, o.arg.ctypes.data_as(ctypes.c_void_p))
         for oi in range(len(p.ops) - 1, -1, -1):
             o = p.ops[oi]
             mask, acu, regions = self.info[oi]
-            for (off, n), saved in zip(regions, log[oi]):
+            for (off, n), (saved, saved32) in zip(regions, log[oi]):
                 p.D[off:off + n] = saved
+                if saved32 is not None:
+                    p.M[off:off + n] = saved32
             if o.kind == 'copy':
                 x = L[o.dst:o.dst + o.n].copy()
                 L[o.dst:o.dst + o.n] = 0.0

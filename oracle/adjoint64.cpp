@@ -29,6 +29,10 @@ struct AccHost {
 #pragma omp atomic
     *p += v;
   }
+  static inline void add(float *p, float v) {
+#pragma omp atomic
+    *p += v;
+  }
 };
 
 inline float wordf(uint32_t w) {
@@ -113,23 +117,84 @@ const Entry kTable[] = {
     {"acoustic_w_solve", runner<adj_acoustic_w_solve<double, AccHost>>()},
 };
 
-}  // namespace
-
-extern "C" {
-
-int teadj_has(const char *name) {
-  for (const Entry &e : kTable)
-    if (!std::strcmp(e.name, name)) return 1;
-  return 0;
+template <void (*Fn)(const AdjArgs<float> &, int, int, int)>
+void loop32(const AdjArgs<float> &A) {
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int tz = 0; tz < A.gz; tz++)
+    for (int ty = 0; ty < A.gy; ty++)
+      for (int tx = 0; tx < A.gx; tx++) Fn(A, tx, ty, tz);
 }
 
-int teadj_run(const char *name, const uint32_t *M, double *D, double *L, const uint32_t *ARG, uint64_t ptr_mask,
-              int acoustic) {
-  Runner run = nullptr;
-  for (const Entry &e : kTable)
-    if (!std::strcmp(e.name, name)) run = e.run;
-  if (!run) return -1;
-  AdjArgs<double> A;
+
+typedef void (*Runner32)(const AdjArgs<float> &);
+
+template <void (*Fn)(const AdjArgs<float> &, int, int, int)>
+Runner32 runner32() {
+  return loop32<Fn>;
+}
+
+void fx32(const AdjArgs<float> &A, int x, int y, int z) { adj_flux_lin_h<float, AccHost>(A, x, y, z, 0); }
+void fy32(const AdjArgs<float> &A, int x, int y, int z) { adj_flux_lin_h<float, AccHost>(A, x, y, z, 1); }
+void sx32(const AdjArgs<float> &A, int x, int y, int z) { adj_flux_stag_h<float, AccHost>(A, x, y, z, 0); }
+void sy32(const AdjArgs<float> &A, int x, int y, int z) { adj_flux_stag_h<float, AccHost>(A, x, y, z, 1); }
+void wx32(const AdjArgs<float> &A, int x, int y, int z) { adj_flux_weno_h<float, AccHost>(A, x, y, z, 0); }
+void wy32(const AdjArgs<float> &A, int x, int y, int z) { adj_flux_weno_h<float, AccHost>(A, x, y, z, 1); }
+void uvx32(const AdjArgs<float> &A, int x, int y, int z) { adj_flux_weno_uv_h<float, AccHost>(A, x, y, z, 0); }
+void uvy32(const AdjArgs<float> &A, int x, int y, int z) { adj_flux_weno_uv_h<float, AccHost>(A, x, y, z, 1); }
+void wwx32(const AdjArgs<float> &A, int x, int y, int z) { adj_flux_weno_w_h<float, AccHost>(A, x, y, z, 0); }
+void wwy32(const AdjArgs<float> &A, int x, int y, int z) { adj_flux_weno_w_h<float, AccHost>(A, x, y, z, 1); }
+void hx32(const AdjArgs<float> &A, int x, int y, int z) { adj_bc_periodic<float, AccHost>(A, x, y, z, 0); }
+void hy32(const AdjArgs<float> &A, int x, int y, int z) { adj_bc_periodic<float, AccHost>(A, x, y, z, 1); }
+
+struct Entry32 {
+  const char *name;
+  Runner32 run;
+};
+
+const Entry32 kTable32[] = {
+    {"adv_flux_x", runner32<fx32>()},
+    {"adv_flux_y", runner32<fy32>()},
+    {"adv_flux_z", runner32<adj_flux_lin_z<float, AccHost>>()},
+    {"adv_flux_x_stag", runner32<sx32>()},
+    {"adv_flux_y_stag", runner32<sy32>()},
+    {"adv_flux_z_stag", runner32<adj_flux_stag_z<float, AccHost>>()},
+    {"adv_flux_x_weno", runner32<wx32>()},
+    {"adv_flux_y_weno", runner32<wy32>()},
+    {"adv_flux_z_weno", runner32<adj_flux_weno_z<float, AccHost>>()},
+    {"adv_flux_x_weno_uv", runner32<uvx32>()},
+    {"adv_flux_y_weno_uv", runner32<uvy32>()},
+    {"adv_flux_z_weno_uv", runner32<adj_flux_weno_uv_z<float, AccHost>>()},
+    {"adv_flux_x_weno_w", runner32<wwx32>()},
+    {"adv_flux_y_weno_w", runner32<wwy32>()},
+    {"adv_flux_z_weno_w", runner32<adj_flux_weno_w_z<float, AccHost>>()},
+    {"adv_assemble", runner32<adj_assemble<float, AccHost>>()},
+    {"rk_update", runner32<adj_rk_update<float, AccHost>>()},
+    {"apply_thterm", runner32<adj_apply_thterm<float, AccHost>>()},
+    {"buoyancy_apply", runner32<adj_buoyancy_apply<float, AccHost>>()},
+    {"update_diagnostics_moist", runner32<adj_update_diagnostics_moist<float, AccHost>>()},
+    {"stage_tendency_reset", runner32<adj_stage_tendency_reset<float, AccHost>>()},
+    {"massflux_from_state", runner32<adj_massflux_from_state<float, AccHost>>()},
+    {"div_massflux", runner32<adj_div_massflux<float, AccHost>>()},
+    {"divergence3d", runner32<adj_divergence3d<float, AccHost>>()},
+    {"velocity_to_massflux", runner32<adj_velocity_to_massflux<float, AccHost>>()},
+    {"build_sadv", runner32<adj_build_sadv<float, AccHost>>()},
+    {"stage_state_reset", runner32<adj_stage_state_reset<float, AccHost>>()},
+    {"acoustic_begin", runner32<adj_acoustic_begin<float, AccHost>>()},
+    {"acoustic_prepare", runner32<adj_acoustic_prepare<float, AccHost>>()},
+    {"acoustic_uv", runner32<adj_acoustic_uv<float, AccHost>>()},
+    {"acoustic_fpk", runner32<adj_acoustic_fpk<float, AccHost>>()},
+    {"acoustic_pp", runner32<adj_acoustic_pp<float, AccHost>>()},
+    {"acoustic_accumulate", runner32<adj_acoustic_accumulate<float, AccHost>>()},
+    {"bc_periodic_x", runner32<hx32>()},
+    {"bc_periodic_y", runner32<hy32>()},
+    {"ppx_finish", runner32<adj_ppx_finish<float, AccHost>>()},
+    {"acoustic_w_solve", runner32<adj_acoustic_w_solve<float, AccHost>>()},
+};
+
+}  // namespace
+
+template <class R>
+static void decode(AdjArgs<R> &A, const uint32_t *M, R *D, R *L, const uint32_t *ARG, uint64_t ptr_mask, int acoustic) {
   std::memset(&A, 0, sizeof A);
   A.gx = (int)ARG[0];
   A.gy = (int)ARG[1];
@@ -162,8 +227,40 @@ int teadj_run(const char *name, const uint32_t *M, double *D, double *L, const u
       A.iv2[n] = (int)M[off + 1];
     }
   }
+}
+
+extern "C" {
+
+int teadj_has(const char *name) {
+  for (const Entry &e : kTable)
+    if (!std::strcmp(e.name, name)) return 1;
+  return 0;
+}
+
+/* the binary32 instantiation (test infrastructure: the GPU's arithmetic on the host, over
+ * the binary32 memory itself): values are the words of M read as floats */
+int teadj_run32(const char *name, uint32_t *M, float *L, const uint32_t *ARG, uint64_t ptr_mask, int acoustic) {
+  Runner32 run = nullptr;
+  for (const Entry32 &e : kTable32)
+    if (!std::strcmp(e.name, name)) run = e.run;
+  if (!run) return -1;
+  AdjArgs<float> A;
+  decode<float>(A, M, reinterpret_cast<float *>(M), L, ARG, ptr_mask, acoustic);
+  run(A);
+  return 0;
+}
+
+int teadj_run(const char *name, const uint32_t *M, double *D, double *L, const uint32_t *ARG, uint64_t ptr_mask,
+              int acoustic) {
+  Runner run = nullptr;
+  for (const Entry &e : kTable)
+    if (!std::strcmp(e.name, name)) run = e.run;
+  if (!run) return -1;
+  AdjArgs<double> A;
+  decode<double>(A, M, D, L, ARG, ptr_mask, acoustic);
   run(A);
   return 0;
 }
 
 }  // extern "C"
+

@@ -1101,6 +1101,71 @@ void teor_bc_periodic_y(uint32_t *M, const uint32_t *ARG) {
 
 /* ------------------------------------------------------ thermodynamic glue */
 
+void teor_update_diagnostics(uint32_t *M, const uint32_t *ARG) {
+  /* update_diagnostics.wgsl main (dry step): thv = th0 + th', piadv = pi, ppterm = pi rd/(cp-rd),
+   * buoy = (g th') / th0 */
+  Dims g = dims_at(M, B(0));
+  const float *thp = FPTR(1), *ppp = FPTR(2), *th0 = FPTR(3), *pi0 = FPTR(4), *rth0 = FPTR(8);
+  float *thv = FPTR(5), *ppterm = FPTR(6), *piadv = FPTR(7), *buoy = FPTR(9);
+  FOR_WHOLE(k < g.nz)
+    float rd = 287.04f, cp = 1005.7f;
+    float rddcv = DCR(rd, cp - rd);
+    float pi = pi0[k] + ppp[c];
+    thv[c] = th0[k] + thp[c];
+    piadv[c] = pi;
+    ppterm[c] = pi * rddcv;
+    buoy[c] = (9.81f * thp[c]) * rth0[k];
+  }
+}
+
+void teor_stability_max(uint32_t *M, const uint32_t *ARG) {
+  /* stability_max.wgsl main: max over interior points of the squared Courant number and of
+   * the diffusion number (bit patterns of non-negative floats, atomicMax into out[0..1]) */
+  Dims g = dims_at(M, B(0));
+  const uint32_t pw = B(1);
+  const float dtdx = bitsf(M[pw]), dtdy = bitsf(M[pw + 1]), dtdz = bitsf(M[pw + 2]);
+  const float ksdx = bitsf(M[pw + 3]), ksdy = bitsf(M[pw + 4]);
+  const int twoD = (int)M[pw + 5], withKs = (int)M[pw + 6];
+  const float *u = FPTR(2), *v = FPTR(3), *w = FPTR(4), *mh = FPTR(5), *kmh = FPTR(6), *kmv = FPTR(7), *khh = FPTR(8);
+  const float *hm = FPTR(30);
+  uint32_t *out = M + B(9);
+  const long GX = ARG[0], GY = ARG[1], GZ = ARG[2];
+  uint32_t cbmax = 0, kbmax = 0;
+  for (long tz = 0; tz < GZ; tz++)
+    for (long ty = 0; ty < GY; ty++)
+      for (long tx = 0; tx < GX; tx++) {
+        int i = (int)tx, j = (int)ty, k = (int)tz;
+        if (i >= g.nx || j >= g.ny || k >= g.nz) continue;
+        int c = GIDX(g, i, j, k);
+        float uh = hm_uh(&g, hm, i), vh = hm_vh(&g, hm, j);
+        float x = ((u[c] + u[GIDX(g, i + 1, j, k)]) * dtdx) * uh;
+        float z = ((w[c] + w[GIDX(g, i, j, k + 1)]) * dtdz) * mh[k];
+        float c2, m = 0.0f;
+        if (twoD != 0) c2 = fmaf(x, x, z * z);
+        else {
+          float y = ((v[c] + v[GIDX(g, i, j + 1, k)]) * dtdy) * vh;
+          c2 = fmaf(z, z, fmaf(x, x, y * y));
+        }
+        if (withKs != 0 && k >= 1) {
+          float K[3] = {kmh[c], khh[c], kmv[c]};
+          for (int n = 0; n < 3; n++) {
+            float a = ((K[n] * ksdx) * uh) * uh;
+            float t;
+            if (twoD != 0) t = a;
+            else {
+              float b = ((K[n] * ksdy) * vh) * vh;
+              t = fmaf(a, a, b * b);
+            }
+            m = fmax_(m, t);
+          }
+        }
+        if (fbits(c2) > cbmax) cbmax = fbits(c2);
+        if (fbits(m) > kbmax) kbmax = fbits(m);
+      }
+  if (cbmax > out[0]) out[0] = cbmax;
+  if (kbmax > out[1]) out[1] = kbmax;
+}
+
 void teor_update_diagnostics_moist(uint32_t *M, const uint32_t *ARG) {
   /* update_diagnostics_moist.wgsl main: thv, piadv, ppterm, thterm, buoy */
   Dims g = dims_at(M, B(0));

@@ -43,7 +43,7 @@ float te_log_f64(float x);
   X(acoustic_prepare) X(acoustic_begin) X(acoustic_uv) X(acoustic_fpk) \
   X(acoustic_w_solve) X(acoustic_pp) X(acoustic_accumulate) \
   X(bc_periodic_x) X(bc_periodic_y) \
-  X(update_diagnostics_moist) X(pressure_tendency) X(divergence3d) \
+  X(update_diagnostics) X(stability_max) X(update_diagnostics_moist) X(pressure_tendency) X(divergence3d) \
   X(update_rho_prs) X(diabatic_unapply) X(diabatic_rates) X(ppx_finish) \
   X(bc_open_x) X(bc_open_y) X(radbc_ew) X(radbc_ns) X(openbc_uv_tendency) \
   X(turb_zero) X(turb_add_tendency) X(turb_scalar_flux_h) X(turb_openbc_flux) \

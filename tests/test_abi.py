@@ -43,7 +43,7 @@ def test_kernel_table_is_the_reference_abi():
     lib.te_kernel_table_json(buf, n + 1)
     table = json.loads(buf.value.decode())
     ref = helpers.kernels_meta()
-    assert len(table) == 80
+    assert len(table) == 82
     for name, k in table.items():
         want = [(p['index'], p['kind'], bool(p['write'])) for p in ref[name]['params']]
         got = [(p['index'], p['kind'], bool(p['write'])) for p in k['params']]

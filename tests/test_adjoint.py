@@ -42,14 +42,16 @@ def _fd(run, init, ctl, d, eps, nsteps):
     return (vals[0] - vals[1]) / (2 * eps)
 
 
-def _cpu_gradient(run, init, nsteps):
+def _cpu_gradient(run, init, nsteps, linearize='f64'):
     from oracle.adjoint import Control, CpuAdjoint64, cost_w2, seed_w2
-    A = CpuAdjoint64(run.tape(1, core=True), helpers.kernels_meta(), init)
+    A = CpuAdjoint64(run.tape(1, core=True), helpers.kernels_meta(), init, linearize=linearize,
+                     kernels32=helpers.oracle().get)
     base = A.p.base[run.rec.ids['arena']]
     A.forward(nsteps)
+    J = cost_w2(run, A.D, base)  # before backward, which returns memory to the start state
     L = A.backward(seed_w2(run, A.D, base, A.D.size))
     ctl = Control(run, base)
-    return ctl, ctl.gradient(L), cost_w2(run, A.D, base)
+    return ctl, ctl.gradient(L), J
 
 
 def test_every_core_kernel_has_an_adjoint_operator():
@@ -116,11 +118,14 @@ def _controls(run, init):
 @pytest.mark.gpu
 def test_gpu_adjoint_matches_binary64_adjoint_and_differences():
     """24x20x16, 4 core steps, checkpoints every 2: the GPU's binary32 gradient against the
-    binary64 adjoint (relative 2-norm error per control field) and against binary64
-    central differences along seeded directions."""
+    binary64 adjoint around the same (binary32) trajectory (relative 2-norm error per
+    control field), and its directional derivatives against binary64 central differences
+    of the binary64 step along seeded directions (the two trajectories differ by rounding,
+    which the WENO weights' derivatives amplify where stencil values are nearly equal)."""
     run, init = _window_start(24, 20, 16)
     g = run.grid
-    ctl, grad64, J = _cpu_gradient(run, init, 4)
+    # the binary64 adjoint around the binary32 trajectory, which the GPU follows bit for bit
+    ctl, grad64, J = _cpu_gradient(run, init, 4, linearize='f32')
     win = _gpu_window(run, init, 4, 2)
     th, u, v = _controls(run, init)
     w = win.forward(th, u, v)
@@ -130,15 +135,18 @@ def test_gpu_adjoint_matches_binary64_adjoint_and_differences():
     gth, gu, gv = win.backward(2.0 * w.astype(np.float64) * dV)
     grad32 = np.concatenate([gth.ravel(), gu.ravel(), gv.ravel()]).astype(np.float64)
     n = g.nz * g.ny * g.nx
-    for q in range(3):
-        a, b = grad32[q * n:(q + 1) * n], grad64[q * n:(q + 1) * n]
-        assert np.linalg.norm(a - b) <= 1e-3 * np.linalg.norm(b), q
+    errs = [float(np.linalg.norm(grad32[q * n:(q + 1) * n] - grad64[q * n:(q + 1) * n]) /
+                  np.linalg.norm(grad64[q * n:(q + 1) * n])) for q in range(3)]
+    assert max(errs) <= 1e-5, errs
     rng = np.random.default_rng(9)
+    rel = []
     for _ in range(2):
         d = rng.standard_normal(ctl.size)
         d /= np.linalg.norm(d)
         fd = _fd(run, init, ctl, d, 1e-5, 4)
-        assert abs(float(grad32 @ d) - fd) <= 1e-3 * abs(fd)
+        rel.append(abs(float(grad32 @ d) - fd) / abs(fd))
+    assert max(rel) <= 1e-3, (errs, rel)
+    print('gradient error against the binary64 adjoint per field', errs, 'directional', rel)
     win.close()
 
 

@@ -5,7 +5,8 @@
 // blocks of K steps from the last: it restores the block's checkpoint and replays its steps
 // op by op, saving every region an op is about to write into an undo log; then it walks the
 // block's ops in reverse, restoring each op's written regions (so memory holds the values
-// before the op) and running the op's adjoint operator (te_adjoint.cuh), which turns the
+// before the op, in every field an adjoint operator reads; regions of the others are not
+// logged) and running the op's adjoint operator (te_adjoint.cuh), which turns the
 // adjoints of the values after the op into the adjoints of the values before it.  At the
 // end memory holds the state of step 0 and the adjoint memory the gradient with respect
 // to it.  Each block position has its own CUDA graph for the logged replay and for the
@@ -17,6 +18,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <set>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -94,54 +96,153 @@ static void launch_adj(const AdjArgs<float>& A, cudaStream_t s) {
   launch_kernel(k_adj<Op>, dim3((A.gx + 31) / 32, (A.gy + 3) / 4, A.gz), dim3(32, 4, 1), 0, s, A);
 }
 
+// Per kernel: the adjoint operator and the bindings whose values BEFORE the op the
+// operator reads (bit n = binding n).  Only fields some operator of the step reads need
+// their overwritten values kept in the undo log.
+// The halo operators' dispatch has 4 threads along x (the halo depth) per row: blocks of
+// 4 x 32 (k_adj is compiled for 128 threads) keep every thread of a block busy.
+template <class Op>
+static void launch_adj_halo(const AdjArgs<float>& A, cudaStream_t s) {
+  if (A.gx <= 0 || A.gy <= 0 || A.gz <= 0) return;
+  launch_kernel(k_adj<Op>, dim3((A.gx + 3) / 4, (A.gy + 31) / 32, A.gz), dim3(4, 32, 1), 0, s, A);
+}
+
+// acoustic_w_solve, a block per 32 columns (lanes on consecutive i) and 8 warps: the rows
+// of the transposed system T^T mu = lambda_w of all levels are formed level-parallel into
+// shared memory, one warp runs the Thomas sweep of the 32 columns, and the 8 warps
+// distribute mu level-parallel (each level's adjoint updates come from rows k and k + 1
+// of its own column: no atomics).  The same operations as adj_acoustic_w_solve.
+constexpr int kAdjCols = 32, kAdjWarps = 8;
+
+__global__ void __launch_bounds__(kAdjCols * kAdjWarps) k_adj_wsolve_coop(AdjArgs<float> A) {
+  extern __shared__ float asm_[];
+  const Dims& g = A.g;
+  const int nz = g.nz, sk = g.sJ * g.sK;
+  const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+  const int col = blockIdx.x * kAdjCols + lane;
+  const bool on = col < g.nx * g.ny;
+  const int c0 = gidx(g, on ? col % g.nx : 0, on ? col / g.nx : 0, 0);
+  float* sSub = asm_;
+  float* sDia = asm_ + nz * kAdjCols;
+  float* sSup = asm_ + 2 * nz * kAdjCols;
+  float* sRhs = asm_ + 3 * nz * kAdjCols;
+  const float *pk1 = A.p[2], *pk2 = A.p[3], *qk = A.p[4], *mm = A.p[5];
+  float *lfpk = A.l[6], *lwten = A.l[7], *lpp = A.l[8], *lw = A.l[9], *lcA = A.l[10], *lcB = A.l[11];
+  const float alph = A.a.alph, beta = A.a.beta, dts = A.a.dts, asq = alph * alph;
+  if (on)
+    for (int k = 1 + wq; k <= nz - 1; k += kAdjWarps) {
+      const int c = c0 + k * sk, e = k * kAdjCols + lane;
+      const float Ak = pk1[c] + qk[c], Bk = pk2[c] - qk[c];
+      const float Am = pk1[c - sk] + qk[c - sk], Bm = pk2[c - sk] - qk[c - sk];
+      const float m = mm[c];
+      sDia[e] = fmaf(-asq, m * ((-Ak) + Bm), 1.0f);
+      sSub[e] = k > 1 ? (-asq) * ((-mm[c - sk]) * Bm) : 0.0f;          // cc(k - 1)
+      sSup[e] = k < nz - 1 ? (-asq) * (mm[c + sk] * Ak) : 0.0f;         // aa(k + 1)
+      sRhs[e] = lw[c];
+    }
+  __syncthreads();
+  if (wq == 0 && on) {
+    float cp = 0.0f, dp = 0.0f;
+    for (int k = 1; k <= nz - 1; k++) {
+      const int e = k * kAdjCols + lane;
+      const float sub = sSub[e];
+      const float den = sDia[e] - sub * cp;
+      cp = sSup[e] / den;
+      dp = (sRhs[e] - sub * dp) / den;
+      sSup[e] = cp;
+      sRhs[e] = dp;
+    }
+    float mu = 0.0f;
+    for (int k = nz - 1; k >= 1; k--) {
+      const int e = k * kAdjCols + lane;
+      mu = sRhs[e] - sSup[e] * mu;
+      sRhs[e] = mu;
+    }
+  }
+  __syncthreads();
+  if (!on) return;
+  for (int k = wq; k <= nz; k += kAdjWarps) {
+    const int c = c0 + k * sk;
+    const float mu = (k >= 1 && k <= nz - 1) ? sRhs[k * kAdjCols + lane] : 0.0f;
+    const float mu1 = (k + 1 <= nz - 1) ? sRhs[(k + 1) * kAdjCols + lane] : 0.0f;
+    const float m = k <= nz - 1 ? mm[c] : 0.0f;
+    const float m1 = k + 1 <= nz - 1 ? mm[c + sk] : 0.0f;
+    if (k <= nz - 1) {
+      lwten[c] += dts * mu;
+      lpp[c] += mu * (beta * (-m) + alph * (-m)) - mu1 * (beta * (-m1) + alph * (-m1));
+      lfpk[c] += mu * (alph * (-m)) - mu1 * (alph * (-m1));
+    }
+    lw[c] = mu;
+    lcA[c] = 0.0f;
+    lcB[c] = 0.0f;
+  }
+}
+
+static void launch_adj_wsolve(const AdjArgs<float>& A, cudaStream_t s) {
+  const int nz = A.g.nz;
+  const size_t bytes = (size_t)4 * nz * kAdjCols * sizeof(float);
+  if (nz < 3 || bytes > 200 * 1024) {
+    launch_adj<OpWSolve>(A, s);
+    return;
+  }
+  if (A.gx <= 0 || A.gy <= 0) return;
+  if (opt_in_smem((const void*)k_adj_wsolve_coop, bytes) != cudaSuccess) return;  // error left pending
+  launch_kernel(k_adj_wsolve_coop, dim3((A.g.nx * A.g.ny + kAdjCols - 1) / kAdjCols), dim3(kAdjCols * kAdjWarps),
+                bytes, s, A);
+}
+
 struct AdjEntry {
   const char* name;
   AdjLaunch launch;
+  uint64_t reads;
 };
 
+#define B1(n) (uint64_t(1) << (n))
 static const AdjEntry kAdjTable[] = {
-    {"adv_flux_x", launch_adj<OpFluxX>},
-    {"adv_flux_y", launch_adj<OpFluxY>},
-    {"adv_flux_z", launch_adj<OpFluxZ>},
-    {"adv_flux_x_stag", launch_adj<OpStagX>},
-    {"adv_flux_y_stag", launch_adj<OpStagY>},
-    {"adv_flux_z_stag", launch_adj<OpStagZ>},
-    {"adv_flux_x_weno", launch_adj<OpWenoX>},
-    {"adv_flux_y_weno", launch_adj<OpWenoY>},
-    {"adv_flux_z_weno", launch_adj<OpWenoZ>},
-    {"adv_flux_x_weno_uv", launch_adj<OpWenoUvX>},
-    {"adv_flux_y_weno_uv", launch_adj<OpWenoUvY>},
-    {"adv_flux_z_weno_uv", launch_adj<OpWenoUvZ>},
-    {"adv_flux_x_weno_w", launch_adj<OpWenoWX>},
-    {"adv_flux_y_weno_w", launch_adj<OpWenoWY>},
-    {"adv_flux_z_weno_w", launch_adj<OpWenoWZ>},
-    {"adv_assemble", launch_adj<OpAssemble>},
-    {"rk_update", launch_adj<OpRk>},
-    {"apply_thterm", launch_adj<OpThterm>},
-    {"buoyancy_apply", launch_adj<OpBuoy>},
-    {"update_diagnostics_moist", launch_adj<OpDiag>},
-    {"stage_tendency_reset", launch_adj<OpTendReset>},
-    {"massflux_from_state", launch_adj<OpMassflux>},
-    {"div_massflux", launch_adj<OpDivMassflux>},
-    {"divergence3d", launch_adj<OpDiv3d>},
-    {"velocity_to_massflux", launch_adj<OpVelMassflux>},
-    {"build_sadv", launch_adj<OpSadv>},
-    {"stage_state_reset", launch_adj<OpStateReset>},
-    {"acoustic_begin", launch_adj<OpBegin>},
-    {"acoustic_prepare", launch_adj<OpPrepare>},
-    {"acoustic_uv", launch_adj<OpUv>},
-    {"acoustic_fpk", launch_adj<OpFpk>},
-    {"acoustic_pp", launch_adj<OpPp>},
-    {"acoustic_accumulate", launch_adj<OpAccum>},
-    {"bc_periodic_x", launch_adj<OpHaloX>},
-    {"bc_periodic_y", launch_adj<OpHaloY>},
-    {"ppx_finish", launch_adj<OpPpxFinish>},
-    {"acoustic_w_solve", launch_adj<OpWSolve>},
+    {"adv_flux_x", launch_adj<OpFluxX>, B1(1) | B1(2)},
+    {"adv_flux_y", launch_adj<OpFluxY>, B1(1) | B1(2)},
+    {"adv_flux_z", launch_adj<OpFluxZ>, B1(1) | B1(2) | B1(3) | B1(4)},
+    {"adv_flux_x_stag", launch_adj<OpStagX>, B1(2) | B1(3) | B1(4) | B1(7)},
+    {"adv_flux_y_stag", launch_adj<OpStagY>, B1(2) | B1(3) | B1(4) | B1(7)},
+    {"adv_flux_z_stag", launch_adj<OpStagZ>, B1(2) | B1(5) | B1(6) | B1(7)},
+    {"adv_flux_x_weno", launch_adj<OpWenoX>, B1(1) | B1(2)},
+    {"adv_flux_y_weno", launch_adj<OpWenoY>, B1(1) | B1(2)},
+    {"adv_flux_z_weno", launch_adj<OpWenoZ>, B1(1) | B1(2) | B1(3) | B1(4)},
+    {"adv_flux_x_weno_uv", launch_adj<OpWenoUvX>, B1(2) | B1(3)},
+    {"adv_flux_y_weno_uv", launch_adj<OpWenoUvY>, B1(2) | B1(3)},
+    {"adv_flux_z_weno_uv", launch_adj<OpWenoUvZ>, B1(2) | B1(3) | B1(4) | B1(5)},
+    {"adv_flux_x_weno_w", launch_adj<OpWenoWX>, B1(1) | B1(2) | B1(3)},
+    {"adv_flux_y_weno_w", launch_adj<OpWenoWY>, B1(1) | B1(2) | B1(3)},
+    {"adv_flux_z_weno_w", launch_adj<OpWenoWZ>, B1(1) | B1(2)},
+    {"adv_assemble", launch_adj<OpAssemble>, B1(2) | B1(6) | B1(7) | B1(8) | B1(9) | B1(10) | B1(15) | B1(16) | B1(30)},
+    {"rk_update", launch_adj<OpRk>, 0},
+    {"apply_thterm", launch_adj<OpThterm>, B1(1) | B1(2)},
+    {"buoyancy_apply", launch_adj<OpBuoy>, B1(2) | B1(3)},
+    {"update_diagnostics_moist", launch_adj<OpDiag>,
+     B1(3) | B1(4) | B1(8) | B1(9) | B1(10) | B1(11) | B1(12) | B1(13) | B1(14)},
+    {"stage_tendency_reset", launch_adj<OpTendReset>, 0},
+    {"massflux_from_state", launch_adj<OpMassflux>, B1(4) | B1(5)},
+    {"div_massflux", launch_adj<OpDivMassflux>, B1(4) | B1(30)},
+    {"divergence3d", launch_adj<OpDiv3d>, B1(1) | B1(2) | B1(3) | B1(4) | B1(30)},
+    {"velocity_to_massflux", launch_adj<OpVelMassflux>, B1(1) | B1(2)},
+    {"build_sadv", launch_adj<OpSadv>, 0},
+    {"stage_state_reset", launch_adj<OpStateReset>, 0},
+    {"acoustic_begin", launch_adj<OpBegin>, 0},
+    {"acoustic_prepare", launch_adj<OpPrepare>, 0},
+    {"acoustic_uv", launch_adj<OpUv>, B1(2) | B1(3) | B1(30)},
+    {"acoustic_fpk", launch_adj<OpFpk>, B1(2) | B1(3) | B1(5) | B1(7) | B1(8) | B1(9) | B1(10) | B1(30)},
+    {"acoustic_pp", launch_adj<OpPp>, B1(2) | B1(3) | B1(4) | B1(5) | B1(6) | B1(7)},
+    {"acoustic_accumulate", launch_adj<OpAccum>, 0},
+    {"bc_periodic_x", launch_adj_halo<OpHaloX>, 0},
+    {"bc_periodic_y", launch_adj_halo<OpHaloY>, 0},
+    {"ppx_finish", launch_adj<OpPpxFinish>, 0},
+    {"acoustic_w_solve", launch_adj_wsolve, B1(2) | B1(3) | B1(4) | B1(5)},
 };
+#undef B1
 
-static AdjLaunch find_adjoint(const std::string& name) {
+static const AdjEntry* find_adjoint(const std::string& name) {
   for (const AdjEntry& e : kAdjTable)
-    if (name == e.name) return e.launch;
+    if (name == e.name) return &e;
   return nullptr;
 }
 
@@ -156,8 +257,10 @@ __global__ void k_adj_copy(float* L, uint64_t src, uint64_t dst, uint64_t n) {
 
 }  // namespace adj
 
+// A written region in words: `rows` rows of `width` words, `pitch` words apart.
 struct Region {
-  uint64_t off, len;  // words
+  uint64_t off, width, pitch, rows;
+  uint64_t size() const { return width * rows; }
 };
 
 struct AdjointState {
@@ -223,23 +326,49 @@ void build_tables(Plan& P, AdjointState& S) {
   S.launch.assign(ops.size(), nullptr);
   S.step_undo_words = 0;
   const uint32_t* M = P.M;
+  // the memory regions whose values before an op some adjoint operator reads
+  std::set<uint64_t> read;
+  for (const Op& o : ops) {
+    if (o.copy) continue;
+    if (!o.spec) throw AdjError(TE_ENOKERNEL, "no CUDA kernel for " + o.name);
+    const adj::AdjEntry* e = adj::find_adjoint(o.name);
+    if (!e) throw AdjError(TE_ENOKERNEL, "no adjoint operator for " + o.name);
+    for (auto& kv : o.bind)
+      if (kv.first < 64 && (e->reads >> kv.first & 1u)) read.insert(kv.second);
+  }
   for (size_t i = 0; i < ops.size(); i++) {
     const Op& o = ops[i];
     if (o.copy) {
-      S.regions[i].push_back({o.dst, o.n});
-      S.step_undo_words += o.n;
+      if (read.count(o.dst)) {
+        S.regions[i].push_back({o.dst, o.n, o.n, 1});
+        S.step_undo_words += o.n;
+      }
       continue;
     }
-    if (!o.spec) throw AdjError(TE_ENOKERNEL, "no CUDA kernel for " + o.name);
-    S.launch[i] = adj::find_adjoint(o.name);
-    if (!S.launch[i]) throw AdjError(TE_ENOKERNEL, "no adjoint operator for " + o.name);
+    S.launch[i] = adj::find_adjoint(o.name)->launch;
+    const bool halo_x = o.name == "bc_periodic_x", halo_y = o.name == "bc_periodic_y";
     for (int q = 0; q < o.spec->nparams; q++) {
       const ParamSpec& ps = o.spec->params[q];
       if (ps.kind != kPtr || !ps.write) continue;
       auto it = o.bind.find(ps.index);
-      if (it == o.bind.end()) continue;
-      const uint64_t len = P.region_len(it->second);
-      S.regions[i].push_back({it->second, len});
+      if (it == o.bind.end() || !read.count(it->second)) continue;
+      const uint64_t f0 = it->second;
+      const Dims& g = o.args.g;
+      if (halo_x || halo_y) {
+        // the halo points only: 3 columns (rows) below the interior and 4 above
+        const uint64_t sJ = g.sJ, sK = g.sK, lv = (uint64_t)g.nz + 1;
+        if (halo_x) {
+          S.regions[i].push_back({f0, 3, sJ, sK * lv});
+          S.regions[i].push_back({f0 + (uint64_t)g.nx + 3, 4, sJ, sK * lv});
+        } else {
+          S.regions[i].push_back({f0, 3 * sJ, sJ * sK, lv});
+          S.regions[i].push_back({f0 + ((uint64_t)g.ny + 3) * sJ, 4 * sJ, sJ * sK, lv});
+        }
+        S.step_undo_words += S.regions[i][S.regions[i].size() - 2].size() + S.regions[i].back().size();
+        continue;
+      }
+      const uint64_t len = P.region_len(f0);
+      S.regions[i].push_back({f0, len, len, 1});
       S.step_undo_words += len;
     }
     adj::AdjArgs<float>& a = S.args[i];
@@ -266,8 +395,9 @@ void logged_step(Plan& P, AdjointState& S, uint32_t* log) {
   uint64_t cur = 0;
   for (size_t i = 0; i < ops.size(); i++) {
     for (const Region& r : S.regions[i]) {
-      ACU(cudaMemcpyAsync(log + cur, P.M + r.off, r.len * 4, cudaMemcpyDeviceToDevice, P.stream));
-      cur += r.len;
+      ACU(cudaMemcpy2DAsync(log + cur, r.width * 4, P.M + r.off, r.pitch * 4, r.width * 4, r.rows,
+                            cudaMemcpyDeviceToDevice, P.stream));
+      cur += r.size();
     }
     P.launch_exact(ops, (int)i, (int)i, false);
   }
@@ -281,8 +411,9 @@ void reverse_step(Plan& P, AdjointState& S, const uint32_t* log) {
     const Op& o = ops[ii];
     for (size_t q = S.regions[ii].size(); q-- > 0;) {
       const Region& r = S.regions[ii][q];
-      cur -= r.len;
-      ACU(cudaMemcpyAsync(P.M + r.off, log + cur, r.len * 4, cudaMemcpyDeviceToDevice, P.stream));
+      cur -= r.size();
+      ACU(cudaMemcpy2DAsync(P.M + r.off, r.pitch * 4, log + cur, r.width * 4, r.width * 4, r.rows,
+                            cudaMemcpyDeviceToDevice, P.stream));
     }
     if (o.copy) {
       const int blocks = (int)std::min<uint64_t>(1024, (o.n + 255) / 256);
@@ -402,6 +533,9 @@ int te_adjoint_backward(te_ctx* ctx) {
       ACU(cudaGraphLaunch(S.rev_graph[j], P.stream));
     }
   }
+  // fields that no adjoint operator reads are not logged: memory returns to the start
+  // state from its checkpoint
+  ACU(cudaMemcpyAsync(P.M, S.ckpt[0], S.ckpt_words * 4, cudaMemcpyDeviceToDevice, P.stream));
   ACU(cudaGetLastError());
   ADJ_END(ctx)
 }

@@ -242,23 +242,22 @@ struct Face {
 
 // Loads the 7-point window around c along stride d; offsets whose coordinate `pos + o`
 // leaves [lo, hi] (the halo-3 field) are not read and enter as constants.
-template <class R>
-TE_HD void load_face(Face<R>& F, const R* a, int c, int d, int pos, int lo, int hi) {
+template <class Q, class R>
+TE_HD void load_face(Face<Q>& F, const R* a, int c, int d, int pos, int lo, int hi) {
 #pragma unroll
   for (int o = -3; o <= 3; o++)
-    F.s[o + 3] = (pos + o >= lo && pos + o <= hi) ? Face<R>::T::seed(a[c + o * d], o + 3) : typename Face<R>::T(R(0));
+    F.s[o + 3] = (pos + o >= lo && pos + o <= hi) ? Face<Q>::T::seed(Q(a[c + o * d]), o + 3) : typename Face<Q>::T(Q(0));
 }
 
 // Adds lam * d(flux)/d(input) to the adjoints of the inputs: field `la` at c + o d, mass
 // fluxes lm0 at c + m0off and lm1 at c + m1off (either may be null).
-template <class R, class Acc>
-TE_HD void scatter_face(const typename Face<R>::T& f, R lam, R* la, int c, int d, R* lm0, int m0off, R* lm1,
-                        int m1off) {
+template <class R, class Acc, class TT>
+TE_HD void scatter_face(const TT& f, R lam, R* la, int c, int d, R* lm0, int m0off, R* lm1, int m1off) {
 #pragma unroll
   for (int o = -3; o <= 3; o++)
-    if (f.d[o + 3] != R(0)) Acc::add(&la[c + o * d], lam * f.d[o + 3]);
-  if (lm0 && f.d[7] != R(0)) Acc::add(&lm0[c + m0off], lam * f.d[7]);
-  if (lm1 && f.d[8] != R(0)) Acc::add(&lm1[c + m1off], lam * f.d[8]);
+    if (f.d[o + 3] != 0) Acc::add(&la[c + o * d], lam * R(f.d[o + 3]));
+  if (lm0 && f.d[7] != 0) Acc::add(&lm0[c + m0off], lam * R(f.d[7]));
+  if (lm1 && f.d[8] != 0) Acc::add(&lm1[c + m1off], lam * R(f.d[8]));
 }
 
 #define S(o) F.s[(o) + 3]
@@ -266,6 +265,7 @@ TE_HD void scatter_face(const typename Face<R>::T& f, R lam, R* la, int c, int d
 // adv_flux_x / adv_flux_y (adv_flux_x.wgsl main): f = rr flx5(upwind stencil)
 template <class R, class Acc>
 TE_HD void adj_flux_lin_h(const AdjArgs<R>& A, int tx, int ty, int tz, int dir) {
+  typedef double Q;  // the face Jacobian in binary64 whatever R is
   const Dims& g = A.g;
   const int i = tx, j = ty, k = tz;
   if (dir == 0 ? (i > g.nx || j >= g.ny || k >= g.nz) : (i >= g.nx || j > g.ny || k >= g.nz)) return;
@@ -273,18 +273,19 @@ TE_HD void adj_flux_lin_h(const AdjArgs<R>& A, int tx, int ty, int tz, int dir) 
   const R lam = A.l[3][c];
   A.l[3][c] = R(0);
   if (lam == R(0)) return;
-  Face<R> F;
+  Face<Q> F;
   load_face(F, A.p[1], c, d, dir == 0 ? i : j, -3, dir == 0 ? g.nx + 3 : g.ny + 3);
-  typedef typename Face<R>::T T;
-  const T rr = T::seed(A.p[2][c], 7);
-  const T f = rr.v >= R(0) ? rr * g_flx5<T, R>(S(-3), S(-2), S(-1), S(0), S(1))
-                           : rr * g_flx5<T, R>(S(2), S(1), S(0), S(-1), S(-2));
+  typedef typename Face<Q>::T T;
+  const T rr = T::seed(Q(A.p[2][c]), 7);
+  const T f = rr.v >= 0 ? rr * g_flx5<T, Q>(S(-3), S(-2), S(-1), S(0), S(1))
+                           : rr * g_flx5<T, Q>(S(2), S(1), S(0), S(-1), S(-2));
   scatter_face<R, Acc>(f, lam, A.l[1], c, d, A.l[2], 0, (R*)nullptr, 0);
 }
 
 // adv_flux_z (adv_flux_z.wgsl main)
 template <class R, class Acc>
 TE_HD void adj_flux_lin_z(const AdjArgs<R>& A, int tx, int ty, int tz) {
+  typedef double Q;  // the face Jacobian in binary64 whatever R is
   const Dims& g = A.g;
   const int i = tx, j = ty, k = tz;
   if (i >= g.nx || j >= g.ny || k > g.nz) return;
@@ -293,18 +294,18 @@ TE_HD void adj_flux_lin_z(const AdjArgs<R>& A, int tx, int ty, int tz) {
   A.l[5][c] = R(0);
   if (k == 0 || k == g.nz || lam == R(0)) return;
   const R *c1 = A.p[3], *c2 = A.p[4];
-  Face<R> F;
-  typedef typename Face<R>::T T;
+  Face<Q> F;
+  typedef typename Face<Q>::T T;
 #pragma unroll
-  for (int o = -3; o <= 3; o++) F.s[o + 3] = (k + o >= 0 && k + o <= g.nz) ? T::seed(A.p[1][c + o * sk], o + 3) : T(R(0));
-  const T w = T::seed(A.p[2][c], 7);
-  const bool up = w.v >= R(0);
+  for (int o = -3; o <= 3; o++) F.s[o + 3] = (k + o >= 0 && k + o <= g.nz) ? T::seed(Q(A.p[1][c + o * sk]), o + 3) : T(Q(0));
+  const T w = T::seed(Q(A.p[2][c]), 7);
+  const bool up = w.v >= 0;
   T f;
-  if (k == 1) f = up ? gfma(T(c1[k]), S(-1), c2[k] * S(0)) : g_flx3<T, R>(S(1), S(0), S(-1));
-  else if (k == 2) f = up ? g_flx3<T, R>(S(-2), S(-1), S(0)) : g_flx5<T, R>(S(2), S(1), S(0), S(-1), S(-2));
-  else if (k == g.nz - 2) f = up ? g_flx5<T, R>(S(-3), S(-2), S(-1), S(0), S(1)) : g_flx3<T, R>(S(1), S(0), S(-1));
-  else if (k == g.nz - 1) f = up ? g_flx3<T, R>(S(-2), S(-1), S(0)) : gfma(T(c1[k]), S(-1), c2[k] * S(0));
-  else f = up ? g_flx5<T, R>(S(-3), S(-2), S(-1), S(0), S(1)) : g_flx5<T, R>(S(2), S(1), S(0), S(-1), S(-2));
+  if (k == 1) f = up ? gfma(T(Q(c1[k])), S(-1), Q(c2[k]) * S(0)) : g_flx3<T, Q>(S(1), S(0), S(-1));
+  else if (k == 2) f = up ? g_flx3<T, Q>(S(-2), S(-1), S(0)) : g_flx5<T, Q>(S(2), S(1), S(0), S(-1), S(-2));
+  else if (k == g.nz - 2) f = up ? g_flx5<T, Q>(S(-3), S(-2), S(-1), S(0), S(1)) : g_flx3<T, Q>(S(1), S(0), S(-1));
+  else if (k == g.nz - 1) f = up ? g_flx3<T, Q>(S(-2), S(-1), S(0)) : gfma(T(Q(c1[k])), S(-1), Q(c2[k]) * S(0));
+  else f = up ? g_flx5<T, Q>(S(-3), S(-2), S(-1), S(0), S(1)) : g_flx5<T, Q>(S(2), S(1), S(0), S(-1), S(-2));
   f = w * f;
   scatter_face<R, Acc>(f, lam, A.l[1], c, sk, A.l[2], 0, (R*)nullptr, 0);
 }
@@ -324,6 +325,7 @@ TE_HD T weno5_up(const Face<R>& F, bool up, bool shifted, R weps) {
 // adv_flux_x_stag / adv_flux_y_stag (adv_flux_x_stag.wgsl main)
 template <class R, class Acc>
 TE_HD void adj_flux_stag_h(const AdjArgs<R>& A, int tx, int ty, int tz, int dir) {
+  typedef double Q;  // the face Jacobian in binary64 whatever R is
   const Dims& g = A.g;
   const int i = tx - 1, j = ty - 1, k = tz;
   if (i > g.nx || j > g.ny || k >= g.nz) return;
@@ -336,12 +338,12 @@ TE_HD void adj_flux_stag_h(const AdjArgs<R>& A, int tx, int ty, int tz, int dir)
   const R* rr = A.p[rb];
   R* lr = A.l[rb];
   const int d = dir == 0 ? 1 : sj;
-  Face<R> F;
+  Face<Q> F;
   load_face(F, A.p[2], c, d, dir == 0 ? i : j, -3, dir == 0 ? g.nx + 3 : g.ny + 3);
-  typedef typename Face<R>::T T;
+  typedef typename Face<Q>::T T;
   int off1 = 0;
   T m;
-  const T r0 = T::seed(rr[c], 7);
+  const T r0 = T::seed(Q(rr[c]), 7);
   if (dir == 0) {
     if (stag == 2) off1 = 1;
     else if (stag == 3) off1 = -sj;
@@ -351,19 +353,20 @@ TE_HD void adj_flux_stag_h(const AdjArgs<R>& A, int tx, int ty, int tz, int dir)
     else if (stag == 3) off1 = sj;
     else if (stag == 4) off1 = -sk;
   }
-  if (stag == 2 || stag == 3) m = R(0.5) * (r0 + T::seed(rr[c + off1], 8));
+  if (stag == 2 || stag == 3) m = Q(0.5) * (r0 + T::seed(Q(rr[c + off1]), 8));
   else if (stag == 4) {
-    const R cc2 = A.p[7][k];
-    m = gfma(T(cc2), r0, (R(1) - cc2) * T::seed(rr[c + off1], 8));
+    const Q cc2 = A.p[7][k];
+    m = gfma(T(cc2), r0, (Q(1) - cc2) * T::seed(Q(rr[c + off1]), 8));
   } else m = r0;
   const bool shifted = dir == 0 ? stag == 2 : stag == 3;
-  const T f = m * flx5_up<T, R>(F, m.v >= R(0), shifted);
+  const T f = m * flx5_up<T, Q>(F, m.v >= 0, shifted);
   scatter_face<R, Acc>(f, lam, A.l[2], c, d, lr, 0, off1 ? lr : (R*)nullptr, off1);
 }
 
 // adv_flux_z_stag (adv_flux_z_stag.wgsl main)
 template <class R, class Acc>
 TE_HD void adj_flux_stag_z(const AdjArgs<R>& A, int tx, int ty, int tz) {
+  typedef double Q;  // the face Jacobian in binary64 whatever R is
   const Dims& g = A.g;
   const int i = tx, j = ty, k = tz;
   if (i > g.nx || j > g.ny || k > g.nz) return;
@@ -375,37 +378,37 @@ TE_HD void adj_flux_stag_z(const AdjArgs<R>& A, int tx, int ty, int tz) {
   if (stag == 4 ? k > g.nz - 1 : (k == 0 || k == g.nz)) return;
   const R *rrw = A.p[5], *c1 = A.p[6], *c2 = A.p[7];
   R* lw = A.l[5];
-  typedef typename Face<R>::T T;
-  Face<R> F;
+  typedef typename Face<Q>::T T;
+  Face<Q> F;
 #pragma unroll
-  for (int o = -3; o <= 3; o++) F.s[o + 3] = (k + o >= 0 && k + o <= g.nz) ? T::seed(A.p[2][c + o * sk], o + 3) : T(R(0));
+  for (int o = -3; o <= 3; o++) F.s[o + 3] = (k + o >= 0 && k + o <= g.nz) ? T::seed(Q(A.p[2][c + o * sk]), o + 3) : T(Q(0));
   int off1;
   T m;
-  const T r0 = T::seed(rrw[c], 7);
+  const T r0 = T::seed(Q(rrw[c]), 7);
   if (stag == 2) {
     off1 = -1;
-    m = R(0.5) * (r0 + T::seed(rrw[c - 1], 8));
+    m = Q(0.5) * (r0 + T::seed(Q(rrw[c - 1]), 8));
   } else if (stag == 3) {
     off1 = -sj;
-    m = R(0.5) * (r0 + T::seed(rrw[c - sj], 8));
+    m = Q(0.5) * (r0 + T::seed(Q(rrw[c - sj]), 8));
   } else {
     off1 = sk;
-    m = R(0.5) * (r0 + (k < g.nz ? T::seed(rrw[c + sk], 8) : T(R(0))));
+    m = Q(0.5) * (r0 + (k < g.nz ? T::seed(Q(rrw[c + sk]), 8) : T(Q(0))));
   }
-  const bool up = m.v >= R(0);
+  const bool up = m.v >= 0;
   T f;
   if (stag == 4) {
-    if (k == 0) f = up ? R(0.5) * (S(0) + S(1)) : g_flx3<T, R>(S(2), S(1), S(0));
-    else if (k == 1) f = up ? g_flx3<T, R>(S(-1), S(0), S(1)) : g_flx5<T, R>(S(3), S(2), S(1), S(0), S(-1));
-    else if (k == g.nz - 2) f = up ? g_flx5<T, R>(S(-2), S(-1), S(0), S(1), S(2)) : g_flx3<T, R>(S(2), S(1), S(0));
-    else if (k == g.nz - 1) f = up ? g_flx3<T, R>(S(-1), S(0), S(1)) : R(0.5) * (S(0) + S(1));
-    else f = up ? g_flx5<T, R>(S(-2), S(-1), S(0), S(1), S(2)) : g_flx5<T, R>(S(3), S(2), S(1), S(0), S(-1));
+    if (k == 0) f = up ? Q(0.5) * (S(0) + S(1)) : g_flx3<T, Q>(S(2), S(1), S(0));
+    else if (k == 1) f = up ? g_flx3<T, Q>(S(-1), S(0), S(1)) : g_flx5<T, Q>(S(3), S(2), S(1), S(0), S(-1));
+    else if (k == g.nz - 2) f = up ? g_flx5<T, Q>(S(-2), S(-1), S(0), S(1), S(2)) : g_flx3<T, Q>(S(2), S(1), S(0));
+    else if (k == g.nz - 1) f = up ? g_flx3<T, Q>(S(-1), S(0), S(1)) : Q(0.5) * (S(0) + S(1));
+    else f = up ? g_flx5<T, Q>(S(-2), S(-1), S(0), S(1), S(2)) : g_flx5<T, Q>(S(3), S(2), S(1), S(0), S(-1));
   } else {
-    if (k == 1) f = up ? gfma(T(c1[k]), S(-1), c2[k] * S(0)) : g_flx3<T, R>(S(1), S(0), S(-1));
-    else if (k == 2) f = up ? g_flx3<T, R>(S(-2), S(-1), S(0)) : g_flx5<T, R>(S(2), S(1), S(0), S(-1), S(-2));
-    else if (k == g.nz - 2) f = up ? g_flx5<T, R>(S(-3), S(-2), S(-1), S(0), S(1)) : g_flx3<T, R>(S(1), S(0), S(-1));
-    else if (k == g.nz - 1) f = up ? g_flx3<T, R>(S(-2), S(-1), S(0)) : gfma(T(c1[k]), S(-1), c2[k] * S(0));
-    else f = up ? g_flx5<T, R>(S(-3), S(-2), S(-1), S(0), S(1)) : g_flx5<T, R>(S(2), S(1), S(0), S(-1), S(-2));
+    if (k == 1) f = up ? gfma(T(Q(c1[k])), S(-1), Q(c2[k]) * S(0)) : g_flx3<T, Q>(S(1), S(0), S(-1));
+    else if (k == 2) f = up ? g_flx3<T, Q>(S(-2), S(-1), S(0)) : g_flx5<T, Q>(S(2), S(1), S(0), S(-1), S(-2));
+    else if (k == g.nz - 2) f = up ? g_flx5<T, Q>(S(-3), S(-2), S(-1), S(0), S(1)) : g_flx3<T, Q>(S(1), S(0), S(-1));
+    else if (k == g.nz - 1) f = up ? g_flx3<T, Q>(S(-2), S(-1), S(0)) : gfma(T(Q(c1[k])), S(-1), Q(c2[k]) * S(0));
+    else f = up ? g_flx5<T, Q>(S(-3), S(-2), S(-1), S(0), S(1)) : g_flx5<T, Q>(S(2), S(1), S(0), S(-1), S(-2));
   }
   f = m * f;
   scatter_face<R, Acc>(f, lam, A.l[2], c, sk, lw, 0, lw, off1);
@@ -426,6 +429,7 @@ TE_HD bool pdef_ok(R s1, R s2, R s3, R s4, R s5, R weps, bool pdef) {
 // adv_flux_x_weno / adv_flux_y_weno (scalars)
 template <class R, class Acc>
 TE_HD void adj_flux_weno_h(const AdjArgs<R>& A, int tx, int ty, int tz, int dir) {
+  typedef double Q;  // the face Jacobian in binary64 whatever R is
   const Dims& g = A.g;
   const int i = tx, j = ty, k = tz;
   if (dir == 0 ? (i > g.nx || j >= g.ny || k >= g.nz) : (i >= g.nx || j > g.ny || k >= g.nz)) return;
@@ -433,23 +437,24 @@ TE_HD void adj_flux_weno_h(const AdjArgs<R>& A, int tx, int ty, int tz, int dir)
   const R lam = A.l[5][c];
   A.l[5][c] = R(0);
   if (lam == R(0)) return;
-  const R weps = (R)A.f[3];
+  const Q weps = (Q)A.f[3];
   const bool pdef = A.iv[4] == 1;
-  Face<R> F;
+  Face<Q> F;
   load_face(F, A.p[1], c, d, dir == 0 ? i : j, -3, dir == 0 ? g.nx + 3 : g.ny + 3);
-  typedef typename Face<R>::T T;
-  const T rr = T::seed(A.p[2][c], 7);
-  const bool up = rr.v >= R(0);
+  typedef typename Face<Q>::T T;
+  const T rr = T::seed(Q(A.p[2][c]), 7);
+  const bool up = rr.v >= 0;
   const T s1 = up ? S(-3) : S(2), s2 = up ? S(-2) : S(1), s3 = up ? S(-1) : S(0), s4 = up ? S(0) : S(-1),
           s5 = up ? S(1) : S(-2);
-  if (!pdef_ok(s1.v, s2.v, s3.v, s4.v, s5.v, weps, pdef)) return;
-  const T f = rr * g_weno5<T, R>(s1, s2, s3, s4, s5, weps);
+  if (!pdef_ok<Q>(s1.v, s2.v, s3.v, s4.v, s5.v, weps, pdef)) return;
+  const T f = rr * g_weno5<T, Q>(s1, s2, s3, s4, s5, weps);
   scatter_face<R, Acc>(f, lam, A.l[1], c, d, A.l[2], 0, (R*)nullptr, 0);
 }
 
 // adv_flux_z_weno (scalars; face kf = k + 1)
 template <class R, class Acc>
 TE_HD void adj_flux_weno_z(const AdjArgs<R>& A, int tx, int ty, int tz) {
+  typedef double Q;  // the face Jacobian in binary64 whatever R is
   const Dims& g = A.g;
   const int i = tx, j = ty, kf = tz + 1;
   if (i >= g.nx || j >= g.ny || kf > g.nz + 1) return;
@@ -459,32 +464,32 @@ TE_HD void adj_flux_weno_z(const AdjArgs<R>& A, int tx, int ty, int tz) {
   A.l[8][c] = R(0);
   if (kf == 1 || kf == g.nz + 1 || lam == R(0)) return;
   const R *c1 = A.p[3], *c2 = A.p[4];
-  const R weps = (R)A.f[5];
+  const Q weps = (Q)A.f[5];
   const bool pdefweno = A.iv[7] == 1;
-  typedef typename Face<R>::T T;
-  Face<R> F;
+  typedef typename Face<Q>::T T;
+  Face<Q> F;
 #pragma unroll
-  for (int o = -3; o <= 3; o++) F.s[o + 3] = (k + o >= 0 && k + o <= g.nz) ? T::seed(A.p[1][c + o * sk], o + 3) : T(R(0));
-  const T w = T::seed(A.p[2][c], 7);
+  for (int o = -3; o <= 3; o++) F.s[o + 3] = (k + o >= 0 && k + o <= g.nz) ? T::seed(Q(A.p[1][c + o * sk]), o + 3) : T(Q(0));
+  const T w = T::seed(Q(A.p[2][c]), 7);
   T f;
   bool have = false;
   if (kf == 2) {
-    f = w.v >= R(0) ? gfma(T(c1[k]), S(-1), c2[k] * S(0)) : g_upstrpd<T, R>(S(1), S(0), S(-1), weps);
+    f = w.v >= 0 ? gfma(T(Q(c1[k])), S(-1), Q(c2[k]) * S(0)) : g_upstrpd<T, Q>(S(1), S(0), S(-1), weps);
     have = true;
   } else if (kf == nk) {
-    f = w.v > R(0) ? g_upstrpd<T, R>(S(-2), S(-1), S(0), weps) : gfma(T(c1[k]), S(-1), c2[k] * S(0));
+    f = w.v > 0 ? g_upstrpd<T, Q>(S(-2), S(-1), S(0), weps) : gfma(T(Q(c1[k])), S(-1), Q(c2[k]) * S(0));
     have = true;
   }
   if (!have) {
-    const bool up = w.v >= R(0);
+    const bool up = w.v >= 0;
     const T s1 = up ? S(-3) : S(2), s2 = up ? S(-2) : S(1), s3 = up ? S(-1) : S(0), s4 = up ? S(0) : S(-1),
             s5 = up ? S(1) : S(-2);
     if (pdefweno) {
-      bool doit = pdef_ok(s1.v, s2.v, s3.v, s4.v, s5.v, weps, true);
-      if (kf == 3 && w.v > R(0)) doit = false;
-      if (kf == nk - 1 && w.v < R(0)) doit = false;
+      bool doit = pdef_ok<Q>(s1.v, s2.v, s3.v, s4.v, s5.v, weps, true);
+      if (kf == 3 && w.v > 0) doit = false;
+      if (kf == nk - 1 && w.v < 0) doit = false;
       if (doit) {
-        f = g_weno5<T, R>(s1, s2, s3, s4, s5, weps);
+        f = g_weno5<T, Q>(s1, s2, s3, s4, s5, weps);
         have = true;
       } else if (kf != 3 && kf != nk - 1) {
         return;  // flux 0
@@ -492,10 +497,10 @@ TE_HD void adj_flux_weno_z(const AdjArgs<R>& A, int tx, int ty, int tz) {
     }
     if (!have) {
       if (kf == 3)
-        f = w.v >= R(0) ? g_upstrpd<T, R>(S(-2), S(-1), S(0), weps) : g_weno5<T, R>(S(2), S(1), S(0), S(-1), S(-2), weps);
+        f = w.v >= 0 ? g_upstrpd<T, Q>(S(-2), S(-1), S(0), weps) : g_weno5<T, Q>(S(2), S(1), S(0), S(-1), S(-2), weps);
       else if (kf == nk - 1)
-        f = w.v >= R(0) ? g_weno5<T, R>(S(-3), S(-2), S(-1), S(0), S(1), weps) : g_upstrpd<T, R>(S(1), S(0), S(-1), weps);
-      else f = g_weno5<T, R>(s1, s2, s3, s4, s5, weps);
+        f = w.v >= 0 ? g_weno5<T, Q>(S(-3), S(-2), S(-1), S(0), S(1), weps) : g_upstrpd<T, Q>(S(1), S(0), S(-1), weps);
+      else f = g_weno5<T, Q>(s1, s2, s3, s4, s5, weps);
     }
   }
   f = w * f;
@@ -505,6 +510,7 @@ TE_HD void adj_flux_weno_z(const AdjArgs<R>& A, int tx, int ty, int tz) {
 // adv_flux_x_weno_uv / adv_flux_y_weno_uv (u, v momentum)
 template <class R, class Acc>
 TE_HD void adj_flux_weno_uv_h(const AdjArgs<R>& A, int tx, int ty, int tz, int dir) {
+  typedef double Q;  // the face Jacobian in binary64 whatever R is
   const Dims& g = A.g;
   const int i = tx - 1, j = ty - 1, k = tz;
   if (i > g.nx || j > g.ny || k >= g.nz) return;
@@ -513,25 +519,26 @@ TE_HD void adj_flux_weno_uv_h(const AdjArgs<R>& A, int tx, int ty, int tz, int d
   const R lam = A.l[5][c];
   A.l[5][c] = R(0);
   if (lam == R(0)) return;
-  const R weps = (R)A.f[4];
+  const Q weps = (Q)A.f[4];
   const R* rr = A.p[3];
   R* lr = A.l[3];
-  typedef typename Face<R>::T T;
-  Face<R> F;
+  typedef typename Face<Q>::T T;
+  Face<Q> F;
   const int d = dir == 0 ? 1 : sj;
   load_face(F, A.p[2], c, d, dir == 0 ? i : j, -3, dir == 0 ? g.nx + 3 : g.ny + 3);
   int off1;
   if (dir == 0) off1 = stag == 2 ? 1 : -sj;
   else off1 = stag == 2 ? -1 : sj;
-  const T m = R(0.5) * (T::seed(rr[c], 7) + T::seed(rr[c + off1], 8));
+  const T m = Q(0.5) * (T::seed(Q(rr[c]), 7) + T::seed(Q(rr[c + off1]), 8));
   const bool shifted = dir == 0 ? stag == 2 : stag == 3;
-  const T f = m * weno5_up<T, R>(F, m.v >= R(0), shifted, weps);
+  const T f = m * weno5_up<T, Q>(F, m.v >= 0, shifted, weps);
   scatter_face<R, Acc>(f, lam, A.l[2], c, d, lr, 0, lr, off1);
 }
 
 // adv_flux_z_weno_uv
 template <class R, class Acc>
 TE_HD void adj_flux_weno_uv_z(const AdjArgs<R>& A, int tx, int ty, int tz) {
+  typedef double Q;  // the face Jacobian in binary64 whatever R is
   const Dims& g = A.g;
   const int i = tx, j = ty, k = tz;
   if (i > g.nx || j > g.ny || k > g.nz) return;
@@ -542,22 +549,22 @@ TE_HD void adj_flux_weno_uv_z(const AdjArgs<R>& A, int tx, int ty, int tz) {
   if (k == 0 || k == g.nz || lam == R(0)) return;
   const R *rrw = A.p[3], *c1 = A.p[4], *c2 = A.p[5];
   R* lw = A.l[3];
-  const R weps = (R)A.f[6];
-  typedef typename Face<R>::T T;
-  Face<R> F;
+  const Q weps = (Q)A.f[6];
+  typedef typename Face<Q>::T T;
+  Face<Q> F;
 #pragma unroll
-  for (int o = -3; o <= 3; o++) F.s[o + 3] = (k + o >= 0 && k + o <= g.nz) ? T::seed(A.p[2][c + o * sk], o + 3) : T(R(0));
+  for (int o = -3; o <= 3; o++) F.s[o + 3] = (k + o >= 0 && k + o <= g.nz) ? T::seed(Q(A.p[2][c + o * sk]), o + 3) : T(Q(0));
   const int off1 = stag == 2 ? -1 : -sj;
-  const T m = R(0.5) * (T::seed(rrw[c], 7) + T::seed(rrw[c + off1], 8));
-  const bool up = m.v >= R(0);
+  const T m = Q(0.5) * (T::seed(Q(rrw[c]), 7) + T::seed(Q(rrw[c + off1]), 8));
+  const bool up = m.v >= 0;
   T f;
-  if (k == 1) f = up ? gfma(T(c1[k]), S(-1), c2[k] * S(0)) : g_upstrpd<T, R>(S(1), S(0), S(-1), weps);
-  else if (k == 2) f = up ? g_upstrpd<T, R>(S(-2), S(-1), S(0), weps) : g_weno5<T, R>(S(2), S(1), S(0), S(-1), S(-2), weps);
+  if (k == 1) f = up ? gfma(T(Q(c1[k])), S(-1), Q(c2[k]) * S(0)) : g_upstrpd<T, Q>(S(1), S(0), S(-1), weps);
+  else if (k == 2) f = up ? g_upstrpd<T, Q>(S(-2), S(-1), S(0), weps) : g_weno5<T, Q>(S(2), S(1), S(0), S(-1), S(-2), weps);
   else if (k == g.nz - 2)
-    f = up ? g_weno5<T, R>(S(-3), S(-2), S(-1), S(0), S(1), weps) : g_upstrpd<T, R>(S(1), S(0), S(-1), weps);
-  else if (k == g.nz - 1) f = up ? g_upstrpd<T, R>(S(-2), S(-1), S(0), weps) : gfma(T(c1[k]), S(-1), c2[k] * S(0));
+    f = up ? g_weno5<T, Q>(S(-3), S(-2), S(-1), S(0), S(1), weps) : g_upstrpd<T, Q>(S(1), S(0), S(-1), weps);
+  else if (k == g.nz - 1) f = up ? g_upstrpd<T, Q>(S(-2), S(-1), S(0), weps) : gfma(T(Q(c1[k])), S(-1), Q(c2[k]) * S(0));
   else
-    f = up ? g_weno5<T, R>(S(-3), S(-2), S(-1), S(0), S(1), weps) : g_weno5<T, R>(S(2), S(1), S(0), S(-1), S(-2), weps);
+    f = up ? g_weno5<T, Q>(S(-3), S(-2), S(-1), S(0), S(1), weps) : g_weno5<T, Q>(S(2), S(1), S(0), S(-1), S(-2), weps);
   f = m * f;
   scatter_face<R, Acc>(f, lam, A.l[2], c, sk, lw, 0, lw, off1);
 }
@@ -565,6 +572,7 @@ TE_HD void adj_flux_weno_uv_z(const AdjArgs<R>& A, int tx, int ty, int tz) {
 // adv_flux_x_weno_w / adv_flux_y_weno_w (w momentum)
 template <class R, class Acc>
 TE_HD void adj_flux_weno_w_h(const AdjArgs<R>& A, int tx, int ty, int tz, int dir) {
+  typedef double Q;  // the face Jacobian in binary64 whatever R is
   const Dims& g = A.g;
   const int i = tx - 1, j = ty - 1, k = tz;
   if (i < 0 || j < 0 || i > g.nx || j > g.ny || k >= g.nz) return;
@@ -572,23 +580,24 @@ TE_HD void adj_flux_weno_w_h(const AdjArgs<R>& A, int tx, int ty, int tz, int di
   const R lam = A.l[5][c];
   A.l[5][c] = R(0);
   if (k == 0 || lam == R(0)) return;
-  const R weps = (R)A.f[4];
+  const Q weps = (Q)A.f[4];
   const R* rr = A.p[2];
   R* lr = A.l[2];
-  const R cc2 = A.p[3][k], cc1 = R(1) - cc2;
-  typedef typename Face<R>::T T;
-  Face<R> F;
+  const Q cc2 = A.p[3][k], cc1 = Q(1) - cc2;
+  typedef typename Face<Q>::T T;
+  Face<Q> F;
   const int d = dir == 0 ? 1 : g.sJ;
   load_face(F, A.p[1], c, d, dir == 0 ? i : j, -3, dir == 0 ? g.nx + 3 : g.ny + 3);
-  const T ub = gfma(T(cc2), T::seed(rr[c], 7), cc1 * T::seed(rr[c - sk], 8));
-  const T f = ub.v >= R(0) ? ub * g_weno5<T, R>(S(-3), S(-2), S(-1), S(0), S(1), weps)
-                           : ub * g_weno5<T, R>(S(2), S(1), S(0), S(-1), S(-2), weps);
+  const T ub = gfma(T(cc2), T::seed(Q(rr[c]), 7), cc1 * T::seed(Q(rr[c - sk]), 8));
+  const T f = ub.v >= 0 ? ub * g_weno5<T, Q>(S(-3), S(-2), S(-1), S(0), S(1), weps)
+                           : ub * g_weno5<T, Q>(S(2), S(1), S(0), S(-1), S(-2), weps);
   scatter_face<R, Acc>(f, lam, A.l[1], c, d, lr, 0, lr, -sk);
 }
 
 // adv_flux_z_weno_w: w flux at cell centres
 template <class R, class Acc>
 TE_HD void adj_flux_weno_w_z(const AdjArgs<R>& A, int tx, int ty, int tz) {
+  typedef double Q;  // the face Jacobian in binary64 whatever R is
   const Dims& g = A.g;
   const int i = tx, j = ty, k = tz, nz = g.nz;
   if (i > g.nx || j > g.ny || k > g.nz) return;
@@ -596,24 +605,24 @@ TE_HD void adj_flux_weno_w_z(const AdjArgs<R>& A, int tx, int ty, int tz) {
   const R lam = A.l[4][c];
   A.l[4][c] = R(0);
   if (k > g.nz - 1 || lam == R(0)) return;
-  const R weps = (R)A.f[3];
+  const Q weps = (Q)A.f[3];
   const R* rrw = A.p[2];
   R* lw = A.l[2];
-  typedef typename Face<R>::T T;
-  Face<R> F;
+  typedef typename Face<Q>::T T;
+  Face<Q> F;
 #pragma unroll
-  for (int o = -3; o <= 3; o++) F.s[o + 3] = (k + o >= 0 && k + o <= g.nz) ? T::seed(A.p[1][c + o * sk], o + 3) : T(R(0));
-  const T wb = R(0.5) * (T::seed(rrw[c], 7) + T::seed(rrw[c + sk], 8));
+  for (int o = -3; o <= 3; o++) F.s[o + 3] = (k + o >= 0 && k + o <= g.nz) ? T::seed(Q(A.p[1][c + o * sk]), o + 3) : T(Q(0));
+  const T wb = Q(0.5) * (T::seed(Q(rrw[c]), 7) + T::seed(Q(rrw[c + sk]), 8));
   T f;
-  if (k == 0) f = wb.v >= R(0) ? R(0.5) * (S(0) + S(1)) : g_upstrpd<T, R>(S(2), S(1), S(0), weps);
-  else if (k == nz - 1) f = wb.v > R(0) ? g_upstrpd<T, R>(S(-1), S(0), S(1), weps) : R(0.5) * (S(0) + S(1));
+  if (k == 0) f = wb.v >= 0 ? Q(0.5) * (S(0) + S(1)) : g_upstrpd<T, Q>(S(2), S(1), S(0), weps);
+  else if (k == nz - 1) f = wb.v > 0 ? g_upstrpd<T, Q>(S(-1), S(0), S(1), weps) : Q(0.5) * (S(0) + S(1));
   else if (k == 1)
-    f = wb.v >= R(0) ? g_upstrpd<T, R>(S(-1), S(0), S(1), weps) : g_weno5<T, R>(S(3), S(2), S(1), S(0), S(-1), weps);
+    f = wb.v >= 0 ? g_upstrpd<T, Q>(S(-1), S(0), S(1), weps) : g_weno5<T, Q>(S(3), S(2), S(1), S(0), S(-1), weps);
   else if (k == nz - 2)
-    f = wb.v > R(0) ? g_weno5<T, R>(S(-2), S(-1), S(0), S(1), S(2), weps) : g_upstrpd<T, R>(S(2), S(1), S(0), weps);
+    f = wb.v > 0 ? g_weno5<T, Q>(S(-2), S(-1), S(0), S(1), S(2), weps) : g_upstrpd<T, Q>(S(2), S(1), S(0), weps);
   else
-    f = wb.v >= R(0) ? g_weno5<T, R>(S(-2), S(-1), S(0), S(1), S(2), weps)
-                     : g_weno5<T, R>(S(3), S(2), S(1), S(0), S(-1), weps);
+    f = wb.v >= 0 ? g_weno5<T, Q>(S(-2), S(-1), S(0), S(1), S(2), weps)
+                     : g_weno5<T, Q>(S(3), S(2), S(1), S(0), S(-1), weps);
   f = wb * f;
   scatter_face<R, Acc>(f, lam, A.l[1], c, sk, lw, 0, lw, sk);
 }
@@ -754,7 +763,6 @@ TE_HD void adj_update_diagnostics_moist(const AdjArgs<R>& A, int tx, int ty, int
   const R cpli = rfma(cpl, liq > R(0) ? liq : R(0), cpi * (ice > R(0) ? ice : R(0)));
   const R cpm = rfma(cpv, qvv, cp) + cpli;
   const R cvm = R(1) / (rfma(cvv, qvv, cv) + cpli);
-  const R th = th0[k] + A.p[1][c];
   R lth = R(0), lpi = R(0);
   R* L15 = A.l[15];
   R* L16 = A.l[16];
@@ -771,7 +779,6 @@ TE_HD void adj_update_diagnostics_moist(const AdjArgs<R>& A, int tx, int ty, int
   L18[c] = R(0);
   lth += L19[c] * (gacc * rth0[k]);
   L19[c] = R(0);
-  (void)th;
   Acc::add(&A.l[1][c], lth);
   Acc::add(&A.l[2][c], lpi);
 }

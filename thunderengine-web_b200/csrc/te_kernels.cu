@@ -36,8 +36,8 @@ namespace fast {
   (void)g;
 
 static void launch3(void (*k)(KArgs), const KArgs& A, cudaStream_t s) {
-  dim3 b(32, 4, 1);
-  dim3 gr((A.gx + 31) / 32, (A.gy + 3) / 4, A.gz);
+  const dim3 b = tile_of(A);
+  dim3 gr((A.gx + b.x - 1) / b.x, (A.gy + b.y - 1) / b.y, A.gz);
   launch_kernel(k, dim3(gr), dim3(b), 0, s, A);
 }
 
@@ -82,8 +82,8 @@ __global__ void __launch_bounds__(128) k_rowvec(KArgs A) {
 
 template <class Op>
 static void launch_rowvec(const KArgs& A, cudaStream_t s) {
-  dim3 b(32, 4, 1);
-  dim3 gr((A.gx + 31) / 32, (A.gy + 3) / 4, (A.gz + kRowVec - 1) / kRowVec);
+  const dim3 b = tile_of(A);
+  dim3 gr((A.gx + b.x - 1) / b.x, (A.gy + b.y - 1) / b.y, (A.gz + kRowVec - 1) / kRowVec);
   launch_kernel(k_rowvec<Op>, dim3(gr), dim3(b), 0, s, A);
 }
 
@@ -2324,6 +2324,85 @@ __global__ void k_update_diagnostics_moist(KArgs A) {
 }
 TE_LAUNCH3(update_diagnostics_moist)
 
+// update_diagnostics (update_diagnostics.wgsl main; encoded timestep.js:1548-1556): the dry
+// step's thv = th0 + th', piadv = pi0 + pi', ppterm = pi rd / (cp - rd), buoy = g th' / th0
+__global__ void k_update_diagnostics(KArgs A) {
+  TE_K3
+  const float *TE_R thp = A.p[1], *TE_R ppp = A.p[2], *TE_R th0 = A.p[3], *TE_R pi0 = A.p[4], *TE_R rth0 = A.p[8];
+  float *TE_R thv = A.p[5], *TE_R ppterm = A.p[6], *TE_R piadv = A.p[7], *TE_R buoy = A.p[9];
+  TE_WHOLE(k < g.nz)
+  const float rd = 287.04f, cp = 1005.7f;
+  const float rddcv = dcr(rd, cp - rd);
+  const float pi = pi0[k] + ppp[c];
+  thv[c] = th0[k] + thp[c];
+  piadv[c] = pi;
+  ppterm[c] = pi * rddcv;
+  buoy[c] = (9.81f * thp[c]) * rth0[k];
+}
+TE_LAUNCH3(update_diagnostics)
+
+// stability_max (stability_max.wgsl main; encoded timestep.js:742-762): per interior point
+// the squared advective Courant number c2 = x^2 + y^2 + z^2 (x = (u + u_e) dt/2dx uh, ...)
+// and, with the eddy viscosities (withKs, k >= 1), the largest diffusion number m; the
+// bit patterns (non-negative floats order like their u32 words) reach out[0], out[1] by
+// atomic max.  A warp forms its maxima first, so one atomic per warp and word.
+__global__ void k_stability_max(KArgs A) {
+  const int tx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ty = blockIdx.y * blockDim.y + threadIdx.y;
+  const int tz = blockIdx.z;
+  const Dims& g = A.g;
+  const float dtdx = A.sw[0][0], dtdy = A.sw[0][1], dtdz = A.sw[0][2], ksdx = A.sw[0][3], ksdy = A.sw[0][4];
+  const int twoD = __float_as_int(A.sw[0][5]), withKs = __float_as_int(A.sw[0][6]);
+  const float *TE_R u = A.p[2], *TE_R v = A.p[3], *TE_R w = A.p[4], *TE_R mh = A.p[5];
+  const float *TE_R kmh = A.p[6], *TE_R kmv = A.p[7], *TE_R khh = A.p[8], *TE_R hm = A.p[30];
+  const int i = tx, j = ty, k = tz;
+  const bool inside = tx < A.gx && ty < A.gy && tz < A.gz && i < g.nx && j < g.ny && k < g.nz;
+  float c2 = 0.0f, m = 0.0f;
+  if (inside) {
+    const int c = gidx(g, i, j, k);
+    const float uh = hm_uh(g, hm, i), vh = hm_vh(g, hm, j);
+    const float x = ((u[c] + u[gidx(g, i + 1, j, k)]) * dtdx) * uh;
+    const float z = ((w[c] + w[gidx(g, i, j, k + 1)]) * dtdz) * mh[k];
+    if (twoD != 0) {
+      c2 = fmaf(x, x, z * z);
+    } else {
+      const float y = ((v[c] + v[gidx(g, i, j + 1, k)]) * dtdy) * vh;
+      c2 = fmaf(z, z, fmaf(x, x, y * y));
+    }
+    if (withKs != 0 && k >= 1) {
+      const float K[3] = {kmh[c], khh[c], kmv[c]};
+#pragma unroll
+      for (int n = 0; n < 3; n++) {
+        const float a = ((K[n] * ksdx) * uh) * uh;
+        float t;
+        if (twoD != 0) {
+          t = a;
+        } else {
+          const float b = ((K[n] * ksdy) * vh) * vh;
+          t = fmaf(a, a, b * b);
+        }
+        m = wmax(m, t);
+      }
+    }
+  }
+  unsigned cb = __float_as_uint(c2), kb = __float_as_uint(m);
+  for (int o = 16; o > 0; o >>= 1) {
+    cb = max(cb, __shfl_xor_sync(0xffffffffu, cb, o));
+    kb = max(kb, __shfl_xor_sync(0xffffffffu, kb, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    unsigned* out = reinterpret_cast<unsigned*>(A.p[9]);
+    atomicMax(out, cb);
+    atomicMax(out + 1, kb);
+  }
+}
+static void launch_stability_max(const KArgs& A, cudaStream_t s) {
+  // blocks of 32 x 4: every warp is one full row of 32 threads, as the shuffle reduction needs
+  dim3 b(32, 4, 1);
+  dim3 gr((A.gx + 31) / 32, (A.gy + 3) / 4, A.gz);
+  launch_kernel(k_stability_max, dim3(gr), dim3(b), 0, s, A);
+}
+
 __global__ void k_pressure_tendency(KArgs A) {
   TE_K3
   const float *TE_R th = A.p[1], *TE_R qv = A.p[2], *TE_R rho = A.p[3], *TE_R ppi = A.p[4], *TE_R thten = A.p[5], *TE_R qpten = A.p[6];
@@ -2880,6 +2959,8 @@ static const KernelSpec kTable[] = {
     {"mass_correction_apply", 13, {R(0), R(1), P(2), P(3), P(4), P(5), W(6), P(7), P(8), P(9), W(10), W(11), W(12)}, false, launch_mass_correction_apply},
     {"morr_prep", 8, {R(0), P(1), P(2), P(3), P(4), P(5), W(6), W(7)}, false, TE_ROWVEC(morr_prep, OpMorrPrep)},
     {"morr_post", 10, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), W(7), W(8), W(9)}, false, launch_morr_post},
+    {"update_diagnostics", 10, {R(0), P(1), P(2), P(3), P(4), W(5), W(6), W(7), P(8), W(9)}, false, launch_update_diagnostics},
+    {"stability_max", 11, {R(0), {1, kRefS, 0}, P(2), P(3), P(4), P(5), P(6), P(7), P(8), W(9), P(30)}, false, launch_stability_max},
     {"update_diagnostics_moist", 20, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), P(11), P(12),
                                       P(13), P(14), W(15), W(16), W(17), W(18), W(19)}, false, TE_ROWVEC(update_diagnostics_moist, OpUpdateDiagnosticsMoist)},
     {"pressure_tendency", 15, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), R(9), R(10), R(12), P(13), R(14), W(11)},

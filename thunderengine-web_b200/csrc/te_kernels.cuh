@@ -22,7 +22,11 @@ struct KArgs {
   int iv[kMaxBind];
   int iv2[kMaxBind];
   float sw[2][8];  // the first 8 words of the kernel's first and second struct bindings (kRefS)
+  short bx, by;    // thread-block shape of the generic launchers (0: 32 x 4), set by te_autotune
 };
+
+// Thread-block shape of a generic launch: the op's tuned shape, else 32 x 4.
+inline dim3 tile_of(const KArgs& A) { return dim3(A.bx > 0 ? A.bx : 32, A.by > 0 ? A.by : 4, 1); }
 
 enum ParamKind : uint8_t { kPtr = 0, kRef = 1, kRefS = 2 };
 

@@ -280,6 +280,8 @@ void Plan::finalize_args(std::vector<Op>& ops) {
     if (o.copy || !o.spec) continue;
     KArgs& A = o.args;
     std::memset(&A, 0, sizeof(A));
+    A.bx = o.tile[0];
+    A.by = o.tile[1];
     A.gx = o.grid[0];
     A.gy = o.grid[1];
     A.gz = o.grid[2];
@@ -770,23 +772,28 @@ void Plan::invalidate_graphs() {
   fused_dirty = true;
 }
 
+cudaGraph_t Plan::capture_step() {
+  if (mode == TE_MODE_FUSED && fused_dirty) {
+    fused.build(*this, active->ops);
+    fused_dirty = false;
+  }
+  cudaGraph_t graph = nullptr;
+  CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+  try {
+    if (mode == TE_MODE_FUSED) fused.launch(*this, active->ops);
+    else launch_exact(active->ops, 0, (int)active->ops.size() - 1, false);
+  } catch (...) {
+    cudaStreamEndCapture(stream, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  CU(cudaStreamEndCapture(stream, &graph));
+  return graph;
+}
+
 void Plan::launch_step_graph() {
   if (!graph_exec) {
-    if (mode == TE_MODE_FUSED && fused_dirty) {
-      fused.build(*this, active->ops);
-      fused_dirty = false;
-    }
-    cudaGraph_t graph = nullptr;
-    CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-    try {
-      if (mode == TE_MODE_FUSED) fused.launch(*this, active->ops);
-      else launch_exact(active->ops, 0, (int)active->ops.size() - 1, false);
-    } catch (...) {
-      cudaStreamEndCapture(stream, &graph);
-      if (graph) cudaGraphDestroy(graph);
-      throw;
-    }
-    CU(cudaStreamEndCapture(stream, &graph));
+    cudaGraph_t graph = capture_step();
     cudaError_t e = cudaGraphInstantiate(&graph_exec, graph, 0);
     cudaGraphDestroy(graph);
     CU(e);

@@ -30,6 +30,7 @@ struct Op {
   std::map<int, uint64_t> bind;  // binding index -> memory word offset
   std::vector<HashReq> hashes;
   KArgs args;
+  short tile[2] = {0, 0};  // thread-block shape chosen by te_autotune (0: the launcher's default)
 };
 
 struct Step {
@@ -88,6 +89,7 @@ struct Plan {
   void finalize_args(std::vector<Op>& ops);
   void launch_exact(std::vector<Op>& ops, int first, int last, bool hashes);
   void launch_step_graph();
+  cudaGraph_t capture_step();  // the active step (current mode) as a graph, not instantiated
   void invalidate_graphs();
   void release();
 };

@@ -95,6 +95,14 @@ EXPORTS = {
     'te_adjoint_zero': ([ctypes.c_void_p], ctypes.c_int),
     'te_adjoint_device_ptr': ([ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     'te_adjoint_memory': ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
+    'te_autotune': ([ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    'te_ensemble_create': ([ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)],
+                           ctypes.c_int),
+    'te_ensemble_run': ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    'te_ensemble_stream': ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    'te_ensemble_sync': ([ctypes.c_void_p], ctypes.c_int),
+    'te_ensemble_last_error': ([ctypes.c_void_p], ctypes.c_char_p),
+    'te_ensemble_destroy': ([ctypes.c_void_p], None),
     'te_w_solve_static_scratch': ([ctypes.POINTER(TeWSolveFields), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                    ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_void_p,
                                    ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
@@ -253,6 +261,13 @@ class Replayer:
     def run_segment(self, seg, part=-1):
         self._check(self.lib.te_run_segment(self.h, int(seg), int(part)))
 
+    def autotune(self, reps=5):
+        """Picks the thread-block shape of each per-dispatch op (te_autotune); returns the
+        number of ops whose shape changed.  Memory is left as it was."""
+        n = ctypes.c_int()
+        self._check(self.lib.te_autotune(self.h, int(reps), ctypes.byref(n)))
+        return n.value
+
     # ---- discrete adjoint (te_adjoint_*; no counterpart in the reference)
     def adjoint_forward(self, nsteps, checkpoint_every):
         """Runs nsteps steps keeping checkpoints every checkpoint_every steps; clears the
@@ -283,3 +298,47 @@ class Replayer:
 
     def sync(self):
         self._check(self.lib.te_sync(self.h))
+
+
+class Ensemble:
+    """Independent Replayers on one device advanced together (te_ensemble_*; no
+    counterpart in the reference): one graph launch per large step runs every member's
+    step, the members' kernels concurrently."""
+
+    def __init__(self, members):
+        self.lib = load_library()
+        self.members = list(members)
+        arr = (ctypes.c_void_p * len(self.members))(*[m.h.value if hasattr(m.h, "value") else m.h for m in self.members])
+        h = ctypes.c_void_p()
+        rc = self.lib.te_ensemble_create(arr, len(self.members), ctypes.byref(h))
+        self.h = h
+        if rc != 0:
+            msg = self.lib.te_ensemble_last_error(h).decode() if h.value else 'te_ensemble_create failed'
+            self.close()
+            raise RuntimeError('thunderstep error %d: %s' % (rc, msg))
+
+    def _check(self, rc):
+        if rc != 0:
+            raise RuntimeError('thunderstep error %d: %s' % (rc, self.lib.te_ensemble_last_error(self.h).decode()))
+
+    def run(self, nsteps=1):
+        self._check(self.lib.te_ensemble_run(self.h, int(nsteps)))
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        self._check(self.lib.te_ensemble_stream(self.h, ctypes.byref(s)))
+        return s.value
+
+    def sync(self):
+        self._check(self.lib.te_ensemble_sync(self.h))
+
+    def close(self):
+        if getattr(self, 'h', None) is not None and self.h.value:
+            self.lib.te_ensemble_destroy(self.h)
+        self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

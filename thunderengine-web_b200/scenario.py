@@ -21,6 +21,7 @@ functions are used.
 * Arena fill: scenario.js:234-296; step profiles rho0/rr0/rf0/th0/pi0/qv0
   (scenario.js:122-136).
 """
+import functools
 import math
 
 import numpy as np
@@ -214,8 +215,9 @@ class Config:
     """One synthetic run: grid, time step, acoustic substeps and perturbation."""
 
     def __init__(self, name, nx, ny, nz, dx, dz, dt, nsound, us, steps, amplitude=2.0, noise=0.1, seed=1,
-                 bubbles=None):
+                 bubbles=None, qv_pbl=0.014):
         self.name = name
+        self.qv_pbl = float(qv_pbl)
         self.nx, self.ny, self.nz = nx, ny, nz
         self.dx = self.dy = float(dx)
         self.dz = float(dz)
@@ -243,10 +245,11 @@ def tiny(nx=12, ny=10, nz=8, dx=1000.0, dz=500.0, dt=6.0, nsound=6, us=20.0):
     return Config('cm1-dyn-%dx%dx%d' % (nx, ny, nz), nx, ny, nz, dx, dz, dt, nsound, us, 1)
 
 
-def profiles(cfg):
-    """Vertical profiles handed to the step (scenario.js:122-136)."""
+def profiles(cfg, dry=False):
+    """Vertical profiles handed to the step (scenario.js:122-136); ``dry``: no water vapour
+    (the sounding's moisture cap set to 0)."""
     vg = VerticalGrid(cfg.nz, cfg.dz)
-    base = weisman_klemp(vg.zh)
+    base = weisman_klemp(vg.zh, qv_pbl=0.0 if dry else getattr(cfg, 'qv_pbl', 0.014))
     nz = cfg.nz
     rho0 = base['rho0']
     cgs, cgt = vg.surface, vg.top
@@ -304,7 +307,8 @@ def fill_arena(cfg, grid, prof, arena, fields):
     for name in ('th', 'th_a'):
         view(name)[:nz] = th
     for name in ('qv', 'qv_a'):
-        view(name)[:nz] = qv0[:, None, None]
+        if name in fields:   # a dry run has no moisture fields
+            view(name)[:nz] = qv0[:, None, None]
     for name in ('u', 'u_a'):
         view(name)[:nz] = u0[:, None, None]
     p = np.array([f(p00 * np.power(pi0[k], cpdrd)) for k in range(nz)], F)
@@ -322,3 +326,101 @@ def periodic_halos(a, nx, ny):
     a[:, :, nx + h:nx + 2 * h + 1] = a[:, :, h:2 * h + 1]
     a[:, :h, :] = a[:, ny:ny + h, :]
     a[:, ny + h:ny + 2 * h + 1, :] = a[:, h:2 * h + 1, :]
+
+
+# ---------------------------------------------------------------- ensembles
+
+def cape(qv_pbl=0.014, dz=100.0, ztop=16000.0):
+    """Surface-parcel CAPE (J/kg) of the Weisman-Klemp sounding with boundary-layer
+    moisture capped at ``qv_pbl``: the parcel rises dry-adiabatically, then
+    pseudo-adiabatically (condensate removed, saturation adjustment by Newton steps),
+    CAPE = sum of g (thv_parcel - thv_env) / thv_env dz where positive.  Binary64, on a
+    fine column of its own (dz), independent of any model grid."""
+    zh = np.arange(0.5 * dz, ztop, dz)
+    b = weisman_klemp(zh.astype(F), qv_pbl=qv_pbl)
+    th_env = b['th0'].astype(np.float64)
+    qv_env = b['qv0'].astype(np.float64)
+    pi = b['pi0'].astype(np.float64)
+    prs = b['prs0'].astype(np.float64)
+    cp, rd, rv, lv = CP, RD, RV, 2.501e6
+    eps = RD / RV
+
+    def qsat(p, t):
+        es = 611.2 * np.exp(17.67 * (t - 273.15) / (t - 29.65))
+        es = min(es, 0.5 * p)
+        return eps * es / (p - es)
+
+    t = th_env[0] * pi[0]
+    qv = qv_env[0]
+    total = 0.0
+    for k in range(1, len(zh)):
+        t = t - G / cp * (zh[k] - zh[k - 1])        # dry ascent over the step
+        for _ in range(20):                         # condense the excess (pseudo-adiabatic)
+            qs = qsat(prs[k], t)
+            if qv <= qs:
+                break
+            dq = (qv - qs) / (1.0 + lv * lv * qs / (cp * rv * t * t))
+            qv -= dq
+            t += lv / cp * dq
+        thv_p = t / pi[k] * (1.0 + qv / eps) / (1.0 + qv)
+        thv_e = th_env[k] * (1.0 + qv_env[k] / eps) / (1.0 + qv_env[k])
+        buoy = G * (thv_p - thv_e) / thv_e
+        if buoy > 0:
+            total += buoy * (zh[k] - zh[k - 1])
+    return total
+
+
+_CAPE_TABLE = None
+
+
+def _cape_table():
+    """CAPE of moisture caps 0.0100, 0.0102, ..., 0.0200 (monotone; computed once)."""
+    global _CAPE_TABLE
+    if _CAPE_TABLE is None:
+        q = np.linspace(0.010, 0.020, 51)
+        _CAPE_TABLE = (q, np.array([cape(x) for x in q]))
+    return _CAPE_TABLE
+
+
+@functools.lru_cache(maxsize=None)
+def qv_pbl_for_cape(target):
+    """The boundary-layer moisture cap whose sounding has CAPE ``target``: bracketed in
+    the table, then refined by bisection on the sounding itself."""
+    q, c = _cape_table()
+    k = int(np.clip(np.searchsorted(c, target), 1, len(q) - 1))
+    lo, hi = q[k - 1], q[k]
+    for _ in range(8):
+        mid = 0.5 * (lo + hi)
+        if cape(mid) < target:
+            lo = mid
+        else:
+            hi = mid
+    return 0.5 * (lo + hi)
+
+
+def ensemble(n=64, seed=7, steps=50):
+    """Members of the batched-ensemble workload: grids drawn from 64x64x40 to 192x192x64
+    (nx, ny multiples of 8, nz multiple of 4), dx = 500 m with dt = 3 s or dx = 1000 m with
+    dt = 6 s, nsound 6..8, shear Us ~ U[10, 30] m/s, CAPE ~ U[1000, 4000] J/kg through the
+    boundary-layer moisture cap, each with its own noise seed."""
+    rng = np.random.default_rng(seed)
+    out = []
+    caps = {}
+    for m in range(n):
+        nx = int(rng.integers(8, 25)) * 8
+        ny = int(rng.integers(8, 25)) * 8
+        nz = int(rng.integers(10, 17)) * 4
+        fine = bool(rng.integers(0, 2))
+        dx, dt = (500.0, 3.0) if fine else (1000.0, 6.0)
+        dz = 16000.0 / nz if not fine else 12000.0 / nz
+        nsound = int(rng.integers(6, 9))
+        us = float(rng.uniform(10.0, 30.0))
+        target = float(rng.uniform(1000.0, 4000.0))
+        key = round(target, -2)
+        if key not in caps:
+            caps[key] = qv_pbl_for_cape(key)
+        cfg = Config('member%02d-%dx%dx%d' % (m, nx, ny, nz), nx, ny, nz, dx, dz, dt, nsound, us, steps,
+                     seed=1 + m, qv_pbl=caps[key])
+        cfg.cape = key
+        out.append(cfg)
+    return out

@@ -79,6 +79,84 @@ class AcousticSchedule:
         return sum(c for c, _ in self.loops)
 
 
+class AdaptiveTimeStep:
+    """The adaptive time step of the reference's driver (web/core/adaptive.js, CM1
+    getnewdt misclibs.F:543-742 and dtsmall :750-847): after each large step the host
+    reads cflmax and ksmax from the 8-byte stability buffer (stability_max), picks the next
+    dt (limited to a 10 % increase, CFL 1, the diffusion limit and 2 dtl) and its acoustic
+    substep count.  Arithmetic as the reference: binary32 where it rounds with fround,
+    binary64 elsewhere.  Output clocks (tape, stat, ...) are not modelled: every clock
+    frequency is absent, which is the reference's behaviour for a run without output."""
+    MAX_NSOUND = 192
+
+    def __init__(self, dtl, min_horizontal_spacing, two_dimensional=False, min_vertical_spacing=None,
+                 ks_check=True):
+        self.dtl = f(dtl)
+        self.ks_check = ks_check
+        self.dtsm = self.small_step(min_horizontal_spacing, min_vertical_spacing, two_dimensional)
+        self.ks_limit = f(0.18) if two_dimensional else f(f(0.18) / f(2.0))
+        self.dbldt = float(self.dtl)
+        self.dt = self.dtl
+        self.dtlast = self.dt
+        self.nsound = 0
+        self.cflmax = 0.0
+        self.ksmax = 0.0
+
+    @staticmethod
+    def small_step(dh, dv=None, two_d=False):
+        """AcousticSchedule.smallStep (config.js:239-243)."""
+        if dv is None:
+            return f(f(f(0.60) * f(dh)) / f(360.0))
+        m = f(min(dh, dv))
+        return f(f((f(0.60) if two_d else f(0.50)) * m) / f(360.0))
+
+    def start(self, cflmax, ksmax):
+        self.getnewdt(cflmax, ksmax)
+
+    def end_step(self, cflmax, ksmax):
+        self.getnewdt(cflmax, ksmax)
+
+    def getnewdt(self, c_in, k_in):
+        cfl_limit, max_change = f(1.00), f(0.10)
+        self.dtlast = self.dt
+        cfl = f(max(c_in, f(1.0e-10)))
+        ks = f(k_in)
+        if cfl > cfl_limit:
+            self.dbldt = self.dbldt * f(cfl_limit / cfl)
+        else:
+            self.dbldt = self.dbldt * min(f(f(1.0) + max_change), f(cfl_limit / cfl))
+        if self.ks_check and (ks * self.dbldt / self.dt) > self.ks_limit:
+            self.dbldt = min(self.dbldt, f(f(self.dt * self.ks_limit) / max(f(1.0e-10), ks)))
+        self.dbldt = min(self.dbldt, f(f(2.0) * self.dtl))
+        self.dt = f(self.dbldt)
+        self.dtsmall()
+        tem = f(self.dt / self.dtlast)
+        self.cflmax = f(cfl * tem)
+        self.ksmax = f(ks * tem)
+
+    def dtsmall(self):
+        x = self.dbldt / self.dtsm
+        n = max(int(math.copysign(1, x) * round_half_away(abs(x))), 4)
+        if n % 2 != 0:
+            n += 1
+        if self.dbldt / f(n) > self.dtsm:
+            n += 2
+        if n > self.MAX_NSOUND:
+            n = self.MAX_NSOUND
+            self.dbldt = f(f(n) * self.dtsm)
+            self.dt = f(self.dbldt)
+        self.nsound = n
+
+
+def stability_from_words(words, two_dimensional=False):
+    """cflmax, ksmax from the 2 words of the stability buffer (adaptive.js:104-110): the
+    kernel reduces squares, the square root is taken here."""
+    fl = np.asarray(words, dtype=np.uint32).view(np.float32)
+    cfl = f(math.sqrt(float(fl[0])))
+    ks = float(fl[1]) if two_dimensional else f(math.sqrt(float(fl[1])))
+    return cfl, ks
+
+
 def weno_epsilon(name):
     """timestep.js:387-392"""
     eps = f(1.0e-18)
@@ -108,6 +186,10 @@ STATE_FIELDS_MOIST = ['th', 'qv', 'u', 'v', 'w', 'th_a', 'qv_a', 'u_a', 'v_a', '
                       'ppterm', 'piadv', 'thv', 'pp3d', 'ppi', 'ppd', 'ppx', 'uten', 'vten', 'wten', 'ppten',
                       'buoy', 'prs', 'rho', 'thterm', 'div3d', 'qpten', 'qtten', 'qvten', 'qcten', 'qvten_t',
                       'qc', 'qzero']
+# the dry step's state (Fields.stateFields, timestep.js:324-332, with scalars = [th])
+STATE_FIELDS_DRY = ['th', 'u', 'v', 'w', 'th_a', 'u_a', 'v_a', 'w_a',
+                    'ppterm', 'piadv', 'thv', 'pp3d', 'ppi', 'ppd', 'ppx', 'uten', 'vten', 'wten', 'ppten',
+                    'buoy', 'prs', 'rho']
 SCRATCH_FIELDS = ['rru', 'rrv', 'rrw', 'fx', 'fy', 'fz', 'tend', 'divx', 'qk', 'pk1', 'pk2', 'mm', 'fpk', 'cA',
                   'cB', 'sadv']
 
@@ -125,16 +207,21 @@ class Run:
     a moist step bind it (timestep.js:1473-1479).
     """
 
-    def __init__(self, cfg, weno_momentum=True, core=False):
+    def __init__(self, cfg, weno_momentum=True, core=False, moist=True, adaptive=False):
         self.cfg = cfg
         self.core = core
+        self.moist = moist
+        self.adaptive = adaptive
+        if core and not moist:
+            raise ValueError('the dynamics-core step is defined on the moist step')
         self.grid = sc.Grid(cfg.nx, cfg.ny, cfg.nz, cfg.dx, cfg.dy, cfg.dz)
-        self.prof = sc.profiles(cfg)
+        self.prof = sc.profiles(cfg, dry=not moist)
         self.dt = f(cfg.dt)
         self.schedule = AcousticSchedule(cfg.nsound, self.dt)
         self.weno_scalars = True
         self.weno_momentum = weno_momentum
-        names = sorted(set(STATE_FIELDS_MOIST + SCRATCH_FIELDS + (CORE_SINKS if core else [])), key=lambda s: s.encode())
+        state = STATE_FIELDS_MOIST if moist else STATE_FIELDS_DRY
+        names = sorted(set(state + SCRATCH_FIELDS + (CORE_SINKS if core else [])), key=lambda s: s.encode())
         g = self.grid
         self.fields = {n: i * g.field_stride for i, n in enumerate(names)}
         self.arena_bytes = g.field_stride * len(names)
@@ -146,6 +233,8 @@ class Run:
             'th0': self.prof['th0'], 'pi0': self.prof['pi0'], 'rth0': self.prof['rth0'],
             'qv0': self.prof['qv0'], 'qc0': self.prof['qc0'], 'qi0': self.prof['qi0'],
         }
+        if adaptive:
+            self.host['stability'] = np.zeros(2, F)   # cflmax^2, ksmax bits (timestep.js:706-709)
         self.rec = Recorder()
         self.acoustic = dict(dts=f(0.1), alph=f(0.6), beta=f(1.0 - f(0.6)), kdiv=f(0.1), smeps=f(0.0))
 
@@ -238,19 +327,21 @@ class Run:
             enc('div_massflux', whole, TG3, False, b)
 
         # pressure tendency (timestep.js:1507-1531)
+        moist = self.moist
+
         def pt():
-            for i, n in enumerate(['th_a', 'qv_a', 'rho', 'ppi']):
+            for i, n in enumerate(['th_a', 'qv_a' if moist else 'th_a', 'rho', 'ppi']):
                 fld(n, i + 1)
             fld('ppten', 5)
-            fld('qpten', 6)
+            fld('qpten' if moist else 'ppten', 6)
             buf('th0', 7)
             buf('pi0', 8)
             by(F1(dt), 9)
             by(I1(0), 10)
             fld('ppten', 11)
             by(I1(0), 12)
-            fld('qvten_t', 13)
-            by(I1(1), 14)
+            fld('qvten_t' if moist else 'ppten', 13)
+            by(I1(1 if moist else 0), 14)
         if not core:
             enc('pressure_tendency', full, TG3, False, pt)
 
@@ -268,7 +359,19 @@ class Run:
                 outs = CORE_SINKS + ['buoy'] if core else ['thv', 'ppterm', 'piadv', 'thterm', 'buoy']
                 for i, n in enumerate(outs):
                     fld(n, i + 15)
-            enc('update_diagnostics_moist', whole, TG3, False, diag)
+            def diag_dry():
+                fld('th', 1)
+                fld('pp3d', 2)
+                buf('th0', 3)
+                buf('pi0', 4)
+                for i, n in enumerate(['thv', 'ppterm', 'piadv']):
+                    fld(n, i + 5)
+                buf('rth0', 8)
+                fld('buoy', 9)
+            if moist:
+                enc('update_diagnostics_moist', whole, TG3, False, diag)
+            else:
+                enc('update_diagnostics', whole, TG3, False, diag_dry)
 
             def rst():
                 for i, n in enumerate(['uten', 'vten', 'wten']):
@@ -369,7 +472,7 @@ class Run:
                             fld(n, i + 1)
                         buf('rho0', 12); buf('mh', 13); by(dttmp, 14); by(open_, 15); fld('tend', 16)
                     enc('pdef_apply', asm, TG3, False, bq)
-                if target == 'th':
+                if target == 'th' and moist:
                     enc('apply_thterm', full, TG3, False,
                         lambda: (fld('div3d', 1), fld('thterm', 2), fld('tend', 3)))
                 enc('rk_update', asm, TG3, False,
@@ -454,8 +557,9 @@ class Run:
                 halo_fill('v')
                 halo_fill('w')
             halo_fill('pp3d')
-            enc('divergence3d', full, TG3, False,
-                lambda: ([fld(n, i + 1) for i, n in enumerate(['rru', 'rrv', 'rrw'])], buf('mh', 4), fld('div3d', 5)))
+            if moist:
+                enc('divergence3d', full, TG3, False,
+                    lambda: ([fld(n, i + 1) for i, n in enumerate(['rru', 'rrv', 'rrw'])], buf('mh', 4), fld('div3d', 5)))
             # 4. averaged velocities -> mass fluxes (timestep.js:2102-2113)
             enc('velocity_to_massflux', whole, TG3, False,
                 lambda: (buf('rho0', 1), buf('rf0', 2), [fld(n, i + 3) for i, n in enumerate(['rru', 'rrv', 'rrw'])]))
@@ -465,8 +569,13 @@ class Run:
             advect('sadv', state='th')
             if core:
                 continue
-            advect('qv')
-            if nrk == 2:
+            if moist:
+                advect('qv')
+            if nrk == 2 and not moist:
+                enc('update_rho_prs', full, TG3, False,
+                    lambda: (by(I1(0), 1), fld('th', 2), fld('pp3d', 3), buf('th0', 4), buf('pi0', 5), fld('th', 6),
+                             fld('prs', 7), fld('rho', 8)))
+            elif nrk == 2:
                 dtb = F1(dt)
                 enc('diabatic_unapply', full, TG3, False,
                     lambda: (by(dtb, 1), [fld(n, i + 2) for i, n in
@@ -475,21 +584,42 @@ class Run:
                     lambda: (by(I1(1), 1), fld('th', 2), fld('pp3d', 3), buf('th0', 4), buf('pi0', 5), fld('qv', 6),
                              fld('prs', 7), fld('rho', 8)))
         dtb = F1(dt)
-        if not core:
+        if not core and moist:
             enc('diabatic_rates', full, TG3, False,
                 lambda: (by(dtb, 1), [fld(n, i + 2) for i, n in
                                       enumerate(['pp3d', 'th', 'qv', 'qc', 'qpten', 'qtten', 'qvten', 'qcten'])]))
         enc('ppx_finish', full, TG3, False, lambda: (fld('pp3d', 1), fld('ppx', 2)))
         halo_fill('ppx')
+        if self.adaptive:
+            # the stability reduction for the adaptive time step (timestep.js:742-762, 2193)
+            d = f(dt)
+            sp = pack('fffffii', [f(f(F(0.5) * d) * f(1.0 / g.dx)), f(f(F(0.5) * d) * f(1.0 / g.dy)),
+                                  f(f(F(0.5) * d) * f(1.0 / g.dz)), f(f(d * f(1.0 / g.dx)) * f(1.0 / g.dx)),
+                                  f(f(d * f(1.0 / g.dy)) * f(1.0 / g.dy)), 0, 0])
+
+            def stab():
+                by(sp, 1)
+                for i, n in enumerate(['u', 'v', 'w']):
+                    fld(n, i + 2)
+                buf('mh', 5)
+                for i in range(3):
+                    fld('u', 6 + i)
+                buf('stability', 9)
+            enc('stability_max', full, TG3, False, stab)
         cmds.append({'op': 'end'})
         # state swap (timestep.js:766-774)
         nbytes = g.count * 4
         aid = rec.id('arena')
         swaps = [('th', 'th_a'), ('qv', 'qv_a'), ('u', 'u_a'), ('v', 'v_a'), ('w', 'w_a'), ('pp3d', 'ppi')]
-        for src, dst in [sw for sw in swaps if not (core and sw[0] == 'qv')]:
+        for src, dst in [sw for sw in swaps if not ((core or not moist) and sw[0] == 'qv')]:
             cmds.append({'op': 'copy', 'src': aid, 'srcOffset': self.fields[src], 'dst': aid,
                          'dstOffset': self.fields[dst], 'size': nbytes})
         return cmds
+
+    def set_time_step(self, dt, nsound):
+        """TimeStep.setTimeStep (timestep.js:711-716): the next encode() uses dt, nsound."""
+        self.dt = f(dt)
+        self.schedule = AcousticSchedule(int(nsound), self.dt)
 
     def tape(self, nsteps=1, core=False):
         """Tape in the reference format (driver.js:62-74); ``core`` selects the
