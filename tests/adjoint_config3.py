@@ -9,8 +9,9 @@ pytest); two parts, so that the binary64 work runs on any host:
 `gpu` writes DIR/grad32.npy (the concatenated th', u, v gradient), DIR/gpu.json (J, the
 timing of the plain window, the forward with checkpoints and the backward, device memory).
 `check` computes the binary64 adjoint of the same window (oracle/libadjoint64.so over
-the binary64 twin, checkpoints every 10) and binary64 central differences of J along 16
-seeded unit directions (eps = 1e-3, and 1e-5 on the first 4), and writes DIR/check.json.
+the binary64 twin, checkpoints every 10), the binary64 adjoint around the binary32
+trajectory (the one the GPU follows), binary64 central differences of J along 16 seeded
+unit directions (eps = 1e-3, and 1e-5 on the first 4), and writes DIR/check.json.
 
 Physics as the 256x256x80 workload (dx = 500 m, dz = 250 m, dt = 3 s, nsound 8,
 Us = 25 m/s); the window starts after one regular large step of the synthetic supercell
@@ -106,12 +107,20 @@ def part_check(out, ndir=16):
     g64 = ctl.gradient(L)
     t_adj = time.perf_counter() - t0
     del A, L
+    # the binary64 adjoint around the binary32 trajectory (the GPU's, bit for bit)
+    A = CpuAdjoint64(ctape, km, init, linearize='f32', kernels32=helpers.oracle().get)
+    A.forward(STEPS, EVERY)
+    g64on32 = ctl.gradient(A.backward(seed_w2(run, A.D, base, A.D.size)))
+    del A
     g32 = np.load(os.path.join(out, 'grad32.npy')).astype(np.float64)
     with open(os.path.join(out, 'gpu.json')) as fh:
         gpu = json.load(fh)
     n = NX * NY * NZ
-    field_err = {f: float(np.linalg.norm(g32[q * n:(q + 1) * n] - g64[q * n:(q + 1) * n]) /
-                           np.linalg.norm(g64[q * n:(q + 1) * n])) for q, f in enumerate(('th', 'u', 'v'))}
+    def rel(a, b):
+        return {f: float(np.linalg.norm(a[q * n:(q + 1) * n] - b[q * n:(q + 1) * n]) /
+                         np.linalg.norm(b[q * n:(q + 1) * n])) for q, f in enumerate(('th', 'u', 'v'))}
+    field_err = rel(g32, g64on32)
+    traj_err = rel(g64on32, g64)
 
     def J_of(d, eps):
         p = CpuPlayer64(ctape, km)
@@ -129,7 +138,7 @@ def part_check(out, ndir=16):
     for q in range(ndir):
         d = rng.standard_normal(ctl.size)
         d /= np.linalg.norm(d)
-        row = {'adjoint32': float(g32 @ d), 'adjoint64': float(g64 @ d)}
+        row = {'adjoint32': float(g32 @ d), 'adjoint64': float(g64 @ d), 'adjoint64_on_f32': float(g64on32 @ d)}
         for eps in ((1e-3, 1e-5) if q < 4 else (1e-3,)):
             fd = (J_of(d, eps) - J_of(d, -eps)) / (2 * eps)
             row['fd_%g' % eps] = fd
@@ -138,10 +147,12 @@ def part_check(out, ndir=16):
         dirs.append(row)
         print(json.dumps(row), flush=True)
     res = {'grid': [NX, NY, NZ], 'steps': STEPS, 'checkpoint_every': EVERY, 'J32': gpu['J'], 'J64': J64,
-           'grad32_vs_grad64_rel_2norm': field_err, 'directions': dirs,
+           'grad32_vs_grad64_same_trajectory_rel_2norm': field_err,
+           'grad64_f32_trajectory_vs_f64_trajectory_rel_2norm': traj_err, 'directions': dirs,
            'max_rel32_eps1e-3': max(r['rel32_0.001'] for r in dirs),
            'max_rel64_eps1e-3': max(r['rel64_0.001'] for r in dirs),
            'max_rel32_eps1e-5': max(r['rel32_1e-05'] for r in dirs if 'rel32_1e-05' in r),
+           'max_rel64_eps1e-5': max(r['rel64_1e-05'] for r in dirs if 'rel64_1e-05' in r),
            'cpu_adjoint_s': t_adj, 'fd_s': time.perf_counter() - t0}
     with open(os.path.join(out, 'check.json'), 'w') as fh:
         json.dump(res, fh, indent=1)

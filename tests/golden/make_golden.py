@@ -1,7 +1,7 @@
 """Copy the reference's golden recordings used by the parity tests into tests/golden/.
 
-Run in a checkout that has the reference at REF (default /root/reference):
-    python tests/golden/make_golden.py [REF]
+Run with the reference checkout given as an argument or in TE_REFERENCE:
+    python tests/golden/make_golden.py REF
 Copies, unchanged:
   data/kernels/kernels.json        kernel parameter ABI (binding index, ptr/ref, write)
 and for each of the scenarios single_cell (120x120x40), squall_line (300x60x40, periodic
@@ -17,7 +17,7 @@ import os
 import shutil
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('TE_REFERENCE', '')
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -25,6 +25,8 @@ SCENARIOS = ('single_cell', 'squall_line', 'supercell_stretched')
 
 
 def main():
+    if not REF or not os.path.isdir(os.path.join(REF, 'data')):
+        sys.exit('usage: make_golden.py REF (the reference checkout; or set TE_REFERENCE)')
     shutil.copy(os.path.join(REF, 'data/kernels/kernels.json'), os.path.join(OUT, 'kernels.json'))
     for scen in SCENARIOS:
         src = os.path.join(REF, 'data', scen)

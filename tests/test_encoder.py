@@ -86,3 +86,71 @@ def test_initial_arena_is_periodic_and_bubble_centred():
     assert np.array_equal(th[:g.nz, :, :h], th[:g.nz, :, g.nx:g.nx + h])
     assert np.array_equal(th[:g.nz, :h, :], th[:g.nz, g.ny:g.ny + h, :])
     assert th.max() > 1.5      # 2 K bubble
+
+
+def _dispatches(cmds, fields=None):
+    """(kernel, grid, workgroup, {binding: setBytes payload}, {binding: arena field}) per
+    dispatch of a command stream."""
+    by_off = {v: k for k, v in (fields or {}).items()}
+    out, pipe, byts, bufs = [], None, {}, {}
+    for c in cmds:
+        if c['op'] == 'pipe':
+            pipe, byts, bufs = c['name'], {}, {}
+        elif c['op'] == 'bytes':
+            byts[c['index']] = c['data']
+        elif c['op'] == 'buf':
+            bufs[c['index']] = by_off.get(c['offset'])
+        elif c['op'] == 'dispatch':
+            out.append((pipe, list(c['grid']), list(c['tg']), dict(byts), dict(bufs)))
+    return out
+
+
+# ops of the recording that exist for its open lateral boundaries (and the periodic halo
+# fills that replace them here), and the setBytes payloads that carry the open flags
+OPEN_BC = ('bc_open_x', 'bc_open_y', 'radbc_ew', 'radbc_ns', 'openbc_uv_tendency', 'bc_periodic_x', 'bc_periodic_y')
+OPEN_FLAGS = {'acoustic_uv': {8}, 'adv_assemble': {17}}
+
+
+def _segment(ops, first, names):
+    """The dispatches from `first` whose kernel is in `names`, in order, up to the next
+    dispatch of `first`'s kernel (one acoustic substep / one advection call)."""
+    out = []
+    for o in ops[first:]:
+        if out and o[0] == ops[first][0] and len(out) > 1:
+            break
+        if o[0] in OPEN_BC:
+            continue
+        if o[0] not in names:
+            break
+        out.append(o)
+    return out
+
+
+def test_substep_and_advection_commands_equal_the_recording():
+    """The command stream of the first acoustic substep and of the stage-1 advection of
+    u, v and w equals the reference's recorded single_cell step (120x120x40, dt 6 s,
+    4 substeps, timestep.js:1997-2060 and 1629-1900): kernel order, dispatch grids,
+    workgroup sizes and every setBytes payload, with the recording's open-boundary
+    kernels and open flags set aside (this encoder writes periodic boundaries)."""
+    golden, _, _, _ = helpers.load_golden_scenario('single_cell')
+    rec = _dispatches(golden['steps'][0])
+    run = timestep.Run(scenario.tiny(120, 120, 40, dx=1000.0, dz=500.0, dt=6.0, nsound=4))
+    mine = _dispatches(run.encode())
+    substep = ('acoustic_uv', 'acoustic_fpk', 'acoustic_w_solve', 'acoustic_pp', 'acoustic_accumulate')
+    advect = ('adv_flux_x_stag', 'adv_flux_y_stag', 'adv_flux_z_stag', 'adv_assemble')
+
+    def first(ops, name):
+        return next(q for q, o in enumerate(ops) if o[0] == name)
+
+    for names, start in ((substep, 'acoustic_uv'), (advect, 'adv_flux_x_stag')):
+        a = [o for o in _segment(rec, first(rec, start), names)]
+        b = [o for o in _segment(mine, first(mine, start), names)]
+        if start == 'adv_flux_x_stag':   # u, v and w: three calls of four kernels
+            a = [o for o in rec[first(rec, start):] if o[0] in names][:12]
+            b = [o for o in mine[first(mine, start):] if o[0] in names][:12]
+        assert [o[0] for o in a] == [o[0] for o in b] and len(a) >= 4
+        for x, y in zip(a, b):
+            assert x[1] == y[1] and x[2] == y[2], (x[0], x[1], y[1], x[2], y[2])
+            skip = OPEN_FLAGS.get(x[0], set())
+            assert {k: v for k, v in x[3].items() if k not in skip} == \
+                   {k: v for k, v in y[3].items() if k not in skip}, x[0]

@@ -158,6 +158,11 @@ TE_DUAL gmax(const Dual<N, R>& a, const Dual<N, R>& b) { return (a.v < b.v || a.
 TE_DUAL gabs(const Dual<N, R>& a) { return a.v < R(0) ? -a : a; }
 #undef TE_DUAL
 
+// An adjoint update of the thread's own point: no other thread of the op touches it, so a
+// plain add (the point-wise operators below use it; stencil operators go through Acc).
+template <class R>
+TE_HD void own(R* p, R v) { *p += v; }
+
 // ------------------------------------------------------------ face reconstructions
 // The forward formulas of te_flux.cuh / te_math.cuh (adv_flux_x.wgsl:106-143,
 // adv_flux_z.wgsl:106-113, adv_flux_x_weno.wgsl:106-151, adv_flux_z_weno.wgsl:111-120)
@@ -710,8 +715,8 @@ TE_HD void adj_rk_update(const AdjArgs<R>& A, int tx, int ty, int tz) {
   const int c = gidx(g, i, j, k);
   const R lp = A.l[4][c];
   A.l[4][c] = R(0);
-  Acc::add(&A.l[2][c], lp);
-  Acc::add(&A.l[3][c], (R)A.f[5] * lp);
+  own(&A.l[2][c], lp);
+  own(&A.l[3][c], (R)A.f[5] * lp);
 }
 
 // apply_thterm: tend = fma(-div, thterm, tend)
@@ -722,8 +727,7 @@ TE_HD void adj_apply_thterm(const AdjArgs<R>& A, int tx, int ty, int tz) {
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
   const int c = gidx(g, i, j, k);
   const R lt = A.l[3][c];
-  Acc::add(&A.l[1][c], -A.p[2][c] * lt);
-  Acc::add(&A.l[2][c], -A.p[1][c] * lt);
+  own(&A.l[1][c], -A.p[2][c] * lt);  // thterm is a constant of the core step
 }
 
 // buoyancy_apply: wten += c1 buoy(k-1) + c2 buoy(k) on interior faces
@@ -779,8 +783,8 @@ TE_HD void adj_update_diagnostics_moist(const AdjArgs<R>& A, int tx, int ty, int
   L18[c] = R(0);
   lth += L19[c] * (gacc * rth0[k]);
   L19[c] = R(0);
-  Acc::add(&A.l[1][c], lth);
-  Acc::add(&A.l[2][c], lpi);
+  own(&A.l[1][c], lth);
+  own(&A.l[2][c], lpi);
 }
 
 // stage_tendency_reset: uten = vten = wten = 0
@@ -798,12 +802,12 @@ TE_HD void adj_massflux_from_state(const AdjArgs<R>& A, int tx, int ty, int tz) 
   TE_ADJ_WHOLE(k <= g.nz)
   const R *rho0 = A.p[4], *rf0 = A.p[5];
   if (k < g.nz) {
-    Acc::add(&A.l[1][c], rho0[k] * A.l[6][c]);
-    Acc::add(&A.l[2][c], rho0[k] * A.l[7][c]);
+    own(&A.l[1][c], rho0[k] * A.l[6][c]);
+    own(&A.l[2][c], rho0[k] * A.l[7][c]);
     A.l[6][c] = R(0);
     A.l[7][c] = R(0);
   }
-  if (k != 0 && k != g.nz) Acc::add(&A.l[3][c], rf0[k] * A.l[8][c]);
+  if (k != 0 && k != g.nz) own(&A.l[3][c], rf0[k] * A.l[8][c]);
   A.l[8][c] = R(0);
 }
 
@@ -866,7 +870,7 @@ TE_HD void adj_velocity_to_massflux(const AdjArgs<R>& A, int tx, int ty, int tz)
 template <class R, class Acc>
 TE_HD void adj_build_sadv(const AdjArgs<R>& A, int tx, int ty, int tz) {
   TE_ADJ_WHOLE(k < g.nz)
-  Acc::add(&A.l[2][c], A.l[3][c]);
+  own(&A.l[2][c], A.l[3][c]);
   A.l[3][c] = R(0);
 }
 
@@ -874,11 +878,11 @@ TE_HD void adj_build_sadv(const AdjArgs<R>& A, int tx, int ty, int tz) {
 template <class R, class Acc>
 TE_HD void adj_stage_state_reset(const AdjArgs<R>& A, int tx, int ty, int tz) {
   TE_ADJ_WHOLE(k <= g.nz)
-  Acc::add(&A.l[1][c], A.l[5][c]);
-  Acc::add(&A.l[2][c], A.l[6][c]);
-  Acc::add(&A.l[3][c], A.l[7][c]);
-  Acc::add(&A.l[4][c], A.l[8][c]);
-  Acc::add(&A.l[10][c], A.l[9][c]);
+  own(&A.l[1][c], A.l[5][c]);
+  own(&A.l[2][c], A.l[6][c]);
+  own(&A.l[3][c], A.l[7][c]);
+  own(&A.l[4][c], A.l[8][c]);
+  own(&A.l[10][c], A.l[9][c]);
   A.l[5][c] = R(0);
   A.l[6][c] = R(0);
   A.l[7][c] = R(0);
@@ -907,7 +911,7 @@ TE_HD void adj_acoustic_begin(const AdjArgs<R>& A, int tx, int ty, int tz) {
   TE_ADJ_WHOLE(k <= g.nz)
   A.l[3][c] = R(0);
   A.l[4][c] = R(0);
-  Acc::add(&A.l[2][c], (R)A.a.beta * A.l[5][c]);
+  own(&A.l[2][c], (R)A.a.beta * A.l[5][c]);
   A.l[5][c] = R(0);
 }
 
@@ -919,37 +923,33 @@ TE_HD void adj_acoustic_uv(const AdjArgs<R>& A, int tx, int ty, int tz) {
   if (i > g.nx || j > g.ny || k >= g.nz) return;
   const int c = gidx(g, i, j, k), sj = g.sJ;
   const int ox = A.iv[8], oy = A.iv2[8];
-  const R *ppd = A.p[2], *thv = A.p[3], *hm = A.p[30];
+  const R *thv = A.p[3], *hm = A.p[30];
   const R dts = (R)A.a.dts, cp = R(1005.7f);
   const R tem1 = ((R)g.rdx * cp) * R(0.5), tem2 = ((R)g.rdy * cp) * R(0.5);
   const bool uEdge = ox != 0 && (i == 0 || i == g.nx);
   const bool vEdge = oy != 0 && (j == 0 || j == g.ny);
+  // u' = u + dts (uten - tem1 uf (thv + thv_w) (ppd - ppd_w)); thv is a constant of the
+  // core step (no adjoint); u and uten updated at the thread's own point
+  R gc = R(0);
   if (!uEdge) {
-    const R lu = A.l[6][c];  // u in place: d u'/d u = 1
+    const R lu = A.l[6][c];
     if (lu != R(0)) {
-      const R uf = hm_uf_(g, hm, i);
-      const R X = -((tem1 * (ppd[c] - ppd[c - 1])) * uf), Y = thv[c] + thv[c - 1];
-      const R gp = lu * dts * Y * (-(tem1 * uf));
-      Acc::add(&A.l[2][c], gp);
+      const R gp = lu * dts * (thv[c] + thv[c - 1]) * (-(tem1 * hm_uf_(g, hm, i)));
+      gc += gp;
       Acc::add(&A.l[2][c - 1], -gp);
-      Acc::add(&A.l[3][c], lu * dts * X);
-      Acc::add(&A.l[3][c - 1], lu * dts * X);
-      Acc::add(&A.l[4][c], lu * dts);
+      own(&A.l[4][c], lu * dts);
     }
   }
   if (!vEdge) {
     const R lv = A.l[7][c];
     if (lv != R(0)) {
-      const R vf = hm_vf_(g, hm, j);
-      const R X = -((tem2 * (ppd[c] - ppd[c - sj])) * vf), Y = thv[c] + thv[c - sj];
-      const R gp = lv * dts * Y * (-(tem2 * vf));
-      Acc::add(&A.l[2][c], gp);
+      const R gp = lv * dts * (thv[c] + thv[c - sj]) * (-(tem2 * hm_vf_(g, hm, j)));
+      gc += gp;
       Acc::add(&A.l[2][c - sj], -gp);
-      Acc::add(&A.l[3][c], lv * dts * X);
-      Acc::add(&A.l[3][c - sj], lv * dts * X);
-      Acc::add(&A.l[5][c], lv * dts);
+      own(&A.l[5][c], lv * dts);
     }
   }
+  if (gc != R(0)) Acc::add(&A.l[2][c], gc);
 }
 
 // acoustic_fpk (acoustic_fpk.wgsl:167-207): the explicit pi' forcing from u, v, w (pk1,
@@ -972,7 +972,7 @@ TE_HD void adj_acoustic_fpk(const AdjArgs<R>& A, int tx, int ty, int tz) {
   const bool clipped = rabs(div) < (R)A.a.smeps;
   Acc::add(&A.l[4][c], lf * beta * (pk1[c] + qk[c]));
   Acc::add(&A.l[4][c + sk], lf * beta * (pk2[c] - qk[c]));
-  Acc::add(&A.l[6][c], lf * dts);  // ppten
+  own(&A.l[6][c], lf * dts);  // ppten, read at the thread's own point only
   const R ldiv = clipped ? R(0) : lf * dts * (-ppterm[c]);
   const R lu1 = ldiv * (R)g.rdx * uh - lf * (piadv[c + 1] - piadv[c]) * temx * uh;
   const R lu0 = -ldiv * (R)g.rdx * uh - lf * (piadv[c] - piadv[c - 1]) * temx * uh;
@@ -1020,13 +1020,13 @@ TE_HD void adj_acoustic_accumulate(const AdjArgs<R>& A, int tx, int ty, int tz) 
     A.l[5][c] = lu * tavg;
     A.l[6][c] = lv * tavg;
     A.l[7][c] = lw * tavg;
-    Acc::add(&A.l[2][c], lu * tavg);
-    Acc::add(&A.l[3][c], lv * tavg);
-    Acc::add(&A.l[4][c], lw * tavg * (R)A.a.alph);
+    own(&A.l[2][c], lu * tavg);
+    own(&A.l[3][c], lv * tavg);
+    own(&A.l[4][c], lw * tavg * (R)A.a.alph);
   } else {
-    Acc::add(&A.l[2][c], lu);
-    Acc::add(&A.l[3][c], lv);
-    Acc::add(&A.l[4][c], lw);
+    own(&A.l[2][c], lu);
+    own(&A.l[3][c], lv);
+    own(&A.l[4][c], lw);
   }
 }
 
@@ -1040,20 +1040,25 @@ TE_HD void adj_bc_periodic(const AdjArgs<R>& A, int tx, int ty, int tz, int dir)
   const int lo = (((-1 - h) % n) + n) % n;
   const int hi = (((n + h) % n) + n) % n;
   R* lf = A.l[1];
+  // with n >= 7 the 7 source points of a row are distinct (h and n - 1 - h): each is
+  // updated by one thread, so a plain add; narrower domains need the atomic
+  const bool distinct = n >= 7;
   // the forward writes the low halo, then the high one: the adjoint takes them in reverse
   {
     const int dst = dir == 0 ? gidx(g, n + h, t, k) : gidx(g, t, n + h, k);
     const int src = dir == 0 ? gidx(g, hi, t, k) : gidx(g, t, hi, k);
     const R x = lf[dst];
     lf[dst] = R(0);
-    Acc::add(&lf[src], x);
+    if (distinct) own(&lf[src], x);
+    else Acc::add(&lf[src], x);
   }
   if (h < 3) {
     const int dst = dir == 0 ? gidx(g, -1 - h, t, k) : gidx(g, t, -1 - h, k);
     const int src = dir == 0 ? gidx(g, lo, t, k) : gidx(g, t, lo, k);
     const R x = lf[dst];
     lf[dst] = R(0);
-    Acc::add(&lf[src], x);
+    if (distinct) own(&lf[src], x);
+    else Acc::add(&lf[src], x);
   }
 }
 
@@ -1064,7 +1069,7 @@ TE_HD void adj_ppx_finish(const AdjArgs<R>& A, int tx, int ty, int tz) {
   const int i = tx, j = ty, k = tz;
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
   const int c = gidx(g, i, j, k);
-  Acc::add(&A.l[1][c], A.l[2][c]);
+  own(&A.l[1][c], A.l[2][c]);
 }
 
 // acoustic_w_solve (acoustic_w_solve.wgsl:124-212), one column per dispatch thread.
