@@ -381,3 +381,45 @@ def test_headline_config_fused_equals_exact_over_20_steps():
     # the state moved: the comparison is not of two untouched arenas
     th0 = helpers.field_view(np.frombuffer(init[run.rec.ids['arena']], dtype=np.uint32), run, 0, 'w')
     assert not np.array_equal(helpers.field_view(mem_ex, run, base, 'w').view(np.uint32), th0)
+
+
+def test_large_domain_step_fused_equals_exact():
+    """1024x1024x100 (dx 250 m, dt 1.5 s, nsound 8, three-bubble line): ~21 GB of arena,
+    word offsets past 2^32.  One step in fused and in exact mode: every non-scratch field
+    bit-identical, finite, and the state moved."""
+    import psutil
+    from thunderengine_web_b200.replayer import Replayer, TE_MODE_FUSED
+    if psutil.virtual_memory().available < 64 << 30:
+        pytest.skip('needs 64 GB of host memory for the initial arena')
+    run = timestep.Run(scenario.LARGE)
+    tape = run.tape(1)
+    arena = run.initial_arena()
+    aid = run.rec.ids['arena']
+    reps = []
+    for mode in (0, TE_MODE_FUSED):
+        r = Replayer(tape, None)
+        r.plan(False)
+        r.build()
+        assert r.mem_words > 1 << 32
+        for b in tape['buffers']:
+            if b['id'] != aid:
+                r.upload(b['id'], run.buffer_bytes(b['label']))
+        r.write_words(r.base[aid], arena)
+        r.set_mode(mode)
+        r.encode_steps(1)
+        r.sync()
+        reps.append(r)
+    g = run.grid
+    base = reps[0].base[aid]
+    for name in run.fields:
+        if name in STEP_SCRATCH:
+            continue
+        off = base + run.fields[name] // 4
+        a = reps[0].read(g.count, off)
+        b = reps[1].read(g.count, off)
+        assert np.array_equal(a, b), name
+        assert np.isfinite(a.view(np.float32)).all(), name
+    w = reps[0].read(g.count, base + run.fields['w'] // 4).view(np.float32)
+    assert np.abs(w).max() > 0
+    for r in reps:
+        r.close()

@@ -238,6 +238,11 @@ class Config:
 # The synthetic workloads: small CPU-runnable case and the at-scale case.
 SMALL = Config('cm1-dyn-64x64x40', 64, 64, 40, 1000.0, 500.0, 6.0, 6, 20.0, 50)
 AT_SCALE = Config('cm1-dyn-256x256x80', 256, 256, 80, 500.0, 250.0, 3.0, 8, 25.0, 100)
+# the large domain: 1024 x 1024 x 100 at dx = 250 m (dz = 200 m), dt = 1.5 s, nsound 8,
+# a line of three bubbles 30 km apart in y (the BubbleLine spacing, base.js:522-539),
+# domain-centred; ~21 GB of arena, memory offsets past 2^32 words
+LARGE = Config('cm1-dyn-1024x1024x100', 1024, 1024, 100, 250.0, 200.0, 1.5, 8, 25.0, 20,
+               bubbles=[(0.0, -30000.0), (0.0, 0.0), (0.0, 30000.0)])
 
 
 def tiny(nx=12, ny=10, nz=8, dx=1000.0, dz=500.0, dt=6.0, nsound=6, us=20.0):
