@@ -123,50 +123,46 @@ __device__ __forceinline__ float fpk_at(const AcuArgs& A, int i, int j, int c, c
 }
 
 // K2: a CTA owns 32 interior columns (i0..i0+31, row j) and runs their implicit w-pi'
-// solve with warp specialisation.  Warps 0-15 (workers, one level each per pass of 16
-// levels) load the 19 inputs of their level, form fpk
-// (acoustic_fpk.wgsl:167-207) and the tridiagonal coefficients aa, bb, cc, dd of the level
-// (lam_1, acoustic_w_solve.wgsl:124-139) into a double-buffered pass store.  Warp 16 (one
-// lane per column) runs the sequential Thomas forward recurrence on the previous pass
-// while the workers prepare the next one, then back-substitutes w.  Finally all warps
-// apply the pi' update (acoustic_pp.wgsl:131-167), store w and accumulate rrw
-// (acoustic_accumulate.wgsl:129-158) for levels 0..nz.  Every value is produced by the
-// same binary32 operations as the per-dispatch kernels; sums the reference forms twice
-// (pk1+qk, pp3d+fpk, ...) are formed once here with the same rounding.
+// solve with warp specialisation.  kLevels worker warps (one level each per pass) load
+// the 19 inputs of their level, form fpk (acoustic_fpk.wgsl:167-207) and the tridiagonal
+// coefficients aa, bb, cc, dd of the level (lam_1, acoustic_w_solve.wgsl:124-139) into a
+// double-buffered pass store; the recurrence warp (one lane per column) runs the
+// sequential Thomas forward recurrence over the previous pass while the workers prepare
+// the next one, then back-substitutes w.  Shared memory holds only cA, cB and
+// s = pi' + fpk for the whole column (3 nz floats per column): the level-(k-1) values
+// the coefficients need come through a per-pass exchange store, and the pi' update
+// (acoustic_pp.wgsl:131-167) re-reads pk1, qk, pk2 and pi' — those loads, with rrw, are
+// issued before the back substitution so that their latency overlaps it.  Finally the
+// workers store pi', ppd, ppx, w and accumulate rrw (acoustic_accumulate.wgsl:129-158)
+// for levels 0..nz.  Every value is produced by the same binary32 operations as the
+// per-dispatch kernels; sums the reference forms twice (pk1+qk, pp3d+fpk, ...) are formed
+// with the same rounding each time.
+//
+// Sized for three resident CTAs per SM (416 threads, 52 KB of shared memory at nz = 80):
+// more columns in flight hide the per-pass load latency better than a deeper pass.
 constexpr int kColTile = 32;
-constexpr int kLevels = 16;                      // worker warps = levels per pass
-constexpr int kWorkers = kColTile * kLevels;     // 512
+constexpr int kLevels = 12;                      // worker warps = levels per pass
+constexpr int kWorkers = kColTile * kLevels;     // 384
 constexpr int kColThreads = kWorkers + kColTile; // + the recurrence warp
-constexpr int kEpiLevels = 6;                    // levels 0..nz per thread in the epilogue: nz < 6 * 17
+constexpr int kEpiChunk = 7;                     // epilogue levels per worker per chunk
 
-struct ColSmem {
-  float *cA, *cB, *A, *Bq, *s, *prev;  // [nz][32], whole column
-  float* co;                           // [2][4][kLevels][32]: aa, bb, cc, dd per pass
-};
+// [nz][32] cA, cB, s; [2][4][kLevels][32] aa, bb, cc, dd per pass; [2][3][kLevels][32]
+// the exchange store (pk1 + qk, pk2 - qk, pi') per pass
+static size_t col_smem_bytes(int nz) { return (size_t)(3 * nz + 14 * kLevels) * kColTile * sizeof(float); }
 
-__device__ __forceinline__ ColSmem col_smem(float* base, int nz) {
-  ColSmem S;
-  const int P = nz * kColTile;
-  S.cA = base;
-  S.cB = base + P;
-  S.A = base + 2 * P;
-  S.Bq = base + 3 * P;
-  S.s = base + 4 * P;
-  S.prev = base + 5 * P;
-  S.co = base + 6 * P;
-  return S;
-}
-
-static size_t col_smem_bytes(int nz) { return (size_t)(6 * nz + 8 * kLevels) * kColTile * sizeof(float); }
-
-// index of coefficient `term` (0 aa, 1 bb, 2 cc, 3 dd) of level slot q, lane, buffer b
 __device__ __forceinline__ int co_at(int b, int term, int q, int lane) {
   return ((b * 4 + term) * kLevels + q) * kColTile + lane;
+}
+__device__ __forceinline__ int xs_at(int b, int term, int q, int lane) {
+  return ((b * 3 + term) * kLevels + q) * kColTile + lane;
 }
 
 __device__ __forceinline__ void workers_sync() {
   asm volatile("bar.sync 1, %0;" ::"n"(kWorkers) : "memory");
 }
+// The CTA-wide barrier; workers and the recurrence warp reach it from separate code paths
+// (whole warps each), the same number of times.
+__device__ __forceinline__ void block_sync() { asm volatile("bar.sync 0;" ::: "memory"); }
 
 // The 19 inputs of one level of one column, loaded ahead of use.
 struct LevelIn {
@@ -211,125 +207,224 @@ __device__ __forceinline__ float fpk_of(const AcuArgs& A, const LevelIn& L, floa
   return fmaf(a.beta, fmaf(L.w0, L.pk1 + L.qk, L.w1 * (L.pk2 - L.qk)), fmaf(a.dts, fmaf(-L.ppterm, div, L.ppten), advPi));
 }
 
-__global__ void __launch_bounds__(kColThreads, 2) k_acu_column(AcuArgs A) {
+// Forward recurrence over one pass of kLevels levels (acoustic_w_solve.wgsl:150-190): the
+// coefficients of four levels are read from the pass store before the chain reaches them.
+__device__ __forceinline__ void forward_pass(const float* co, float* cA, float* cB, int pp, int nz, int lane, float& cAm,
+                                             float& cBm, float& wtop) {
+  const int b = pp & 1, base = pp * kLevels;
+  float ca[4], cb[4], cc[4], cd[4];
+#pragma unroll
+  for (int t = 0; t < 4; t++) {
+    ca[t] = co[co_at(b, 0, t, lane)];
+    cb[t] = co[co_at(b, 1, t, lane)];
+    cc[t] = co[co_at(b, 2, t, lane)];
+    cd[t] = co[co_at(b, 3, t, lane)];
+  }
+#pragma unroll
+  for (int g4 = 0; g4 < kLevels / 4; g4++) {
+    float na[4], nb[4], nc[4], nd[4];
+    if (g4 + 1 < kLevels / 4) {
+#pragma unroll
+      for (int t = 0; t < 4; t++) {
+        const int qq = 4 * (g4 + 1) + t;
+        na[t] = co[co_at(b, 0, qq, lane)];
+        nb[t] = co[co_at(b, 1, qq, lane)];
+        nc[t] = co[co_at(b, 2, qq, lane)];
+        nd[t] = co[co_at(b, 3, qq, lane)];
+      }
+    }
+    float oA[4], oB[4];
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      const int kk = base + 4 * g4 + t;
+      if (kk == 1) {
+        const float r = dcr(1.0f, cb[t]);
+        cAm = (-cc[t]) * r;
+        cBm = cd[t] * r;
+      } else if (kk >= 2 && kk < nz - 1) {
+        const float r = dcr(1.0f, fmaf(ca[t], cAm, cb[t]));
+        const float cAk = (-cc[t]) * r, cBk = fmaf(-ca[t], cBm, cd[t]) * r;
+        cAm = cAk;
+        cBm = cBk;
+      } else if (kk == nz - 1) {
+        const float r = dcr(1.0f, fmaf(ca[t], cAm, cb[t]));
+        wtop = fmaf(-ca[t], cBm, cd[t]) * r;
+      }
+      oA[t] = cAm;
+      oB[t] = cBm;
+    }
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      const int kk = base + 4 * g4 + t;
+      if (kk >= 1 && kk < nz - 1) {
+        cA[kk * kColTile + lane] = oA[t];
+        cB[kk * kColTile + lane] = oB[t];
+      }
+    }
+    if (g4 + 1 < kLevels / 4) {
+#pragma unroll
+      for (int t = 0; t < 4; t++) {
+        ca[t] = na[t];
+        cb[t] = nb[t];
+        cc[t] = nc[t];
+        cd[t] = nd[t];
+      }
+    }
+  }
+}
+
+// Back substitution: w(k) overwrites cA(k); w(0) = w(nz) = 0.  Eight levels of cA, cB are
+// read ahead of the chain.
+__device__ __forceinline__ void back_substitute(float* cA, const float* cB, int nz, int lane, float wtop) {
+  float wk1 = wtop;
+  cA[(nz - 1) * kColTile + lane] = wtop;
+  for (int k0 = nz - 2; k0 >= 1; k0 -= 8) {
+    float xa[8], xb[8], wv[8];
+#pragma unroll
+    for (int t = 0; t < 8; t++) {
+      const int k = k0 - t;
+      if (k >= 1) {
+        xa[t] = cA[k * kColTile + lane];
+        xb[t] = cB[k * kColTile + lane];
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < 8; t++) {
+      if (k0 - t >= 1) {
+        wv[t] = fmaf(xa[t], wk1, xb[t]);
+        wk1 = wv[t];
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < 8; t++) {
+      const int k = k0 - t;
+      if (k >= 1) cA[k * kColTile + lane] = wv[t];
+    }
+  }
+  cA[lane] = 0.0f;
+}
+
+// The pi' update inputs of a worker's epilogue levels k0, k0 + kLevels, ...
+struct EpiIn {
+  float rr[kEpiChunk], pk1[kEpiChunk], qk[kEpiChunk], pk2[kEpiChunk], pp[kEpiChunk];
+};
+
+__device__ __forceinline__ void load_epi(const AcuArgs& A, EpiIn& E, int c0, int k0, int nz, int sk) {
+#pragma unroll
+  for (int t = 0; t < kEpiChunk; t++) {
+    const int k = k0 + t * kLevels;
+    if (k <= nz) {
+      const int c = c0 + k * sk;
+      E.rr[t] = A.rrw[c];
+      if (k < nz) {
+        E.pk1[t] = __ldg(A.pk1 + c);
+        E.qk[t] = __ldg(A.qk + c);
+        E.pk2[t] = __ldg(A.pk2 + c);
+        E.pp[t] = A.pp3d[c];
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kColThreads, 3) k_acu_column(AcuArgs A) {
   extern __shared__ float smem[];
   const Dims& g = A.g;
   const Acoustic& a = A.a;
   const int nz = g.nz;
-  const ColSmem S = col_smem(smem, nz);
+  float* cA = smem;
+  float* cB = smem + nz * kColTile;
+  float* sS = smem + 2 * nz * kColTile;
+  float* co = smem + 3 * nz * kColTile;
+  float* xs = co + 8 * kLevels * kColTile;
   const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
-  const bool worker = q < kLevels;
   const int i = blockIdx.x * kColTile + lane;
   const int j = blockIdx.y;
   const bool col = i < g.nx;
   const int sk = g.sJ * g.sK;
   const int c0 = gidx(g, col ? i : 0, j, 0);
-  const float asq = a.alph * a.alph;
   const int npass = (nz + kLevels - 1) / kLevels;
-  float cAm = 0.0f, cBm = 0.0f, wtop = 0.0f;  // recurrence state (warp kLevels)
+  if (q == kLevels) {
+    // recurrence warp: pass p - 1 while the workers prepare pass p, then the last pass
+    // and the back substitution
+    float cAm = 0.0f, cBm = 0.0f, wtop = 0.0f;
+    for (int p = 0; p < npass; p++) {
+      if (p >= 1 && col) forward_pass(co, cA, cB, p - 1, nz, lane, cAm, cBm, wtop);
+      block_sync();
+    }
+    if (col) {
+      forward_pass(co, cA, cB, npass - 1, nz, lane, cAm, cBm, wtop);
+      back_substitute(cA, cB, nz, lane, wtop);
+    }
+    block_sync();
+    return;
+  }
+  const float asq = a.alph * a.alph;
   const float uh = hm_uh(g, A.hm, col ? i : 0), vh = hm_vh(g, A.hm, j);
-  for (int p = 0; p <= npass; p++) {
-    if (worker) {
-      if (p < npass) {
-        const int k = p * kLevels + q;
-        float m = 0.0f, wt = 0.0f, w0 = 0.0f;
-        if (col && k < nz) {
-          const LevelIn cur = load_level(A, c0 + k * sk);
-          const float fk = fpk_of(A, cur, uh, vh);
-          const int e = k * kColTile + lane;
-          S.A[e] = cur.pk1 + cur.qk;
-          S.Bq[e] = cur.pk2 - cur.qk;
-          S.prev[e] = cur.pp;
-          S.s[e] = cur.pp + fk;
-          m = cur.mm;
-          wt = cur.wt;
-          w0 = cur.w0;
-        }
-        workers_sync();
-        if (col && k < nz && k >= 1) {
-          const int e = k * kColTile + lane, em = e - kColTile;
-          const int b = p & 1;
-          S.co[co_at(b, 0, q, lane)] = (-asq) * (m * S.A[em]);
-          S.co[co_at(b, 2, q, lane)] = (-asq) * ((-m) * S.Bq[e]);
-          S.co[co_at(b, 1, q, lane)] = fmaf(-asq, m * ((-S.A[e]) + S.Bq[em]), 1.0f);
-          const float fw = fmaf(a.dts, wt, a.beta * ((-m) * (S.prev[e] - S.prev[em])));
-          S.co[co_at(b, 3, q, lane)] = fmaf(a.alph, (-m) * (S.s[e] - S.s[em]), w0 + fw);
-        }
-      }
-    } else if (p >= 1 && col) {
-      // forward recurrence over the previous pass (acoustic_w_solve.wgsl:150-190)
-      const int b = (p - 1) & 1;
-      for (int qq = 0; qq < kLevels; qq++) {
-        const int kk = (p - 1) * kLevels + qq;
-        if (kk >= nz) break;
-        if (kk == 0) continue;
-        const int e = kk * kColTile + lane;
-        const float aa = S.co[co_at(b, 0, qq, lane)], bb = S.co[co_at(b, 1, qq, lane)];
-        const float cc = S.co[co_at(b, 2, qq, lane)], dd = S.co[co_at(b, 3, qq, lane)];
-        if (kk == 1) {
-          const float r = dcr(1.0f, bb);
-          cAm = (-cc) * r;
-          cBm = dd * r;
-          S.cA[e] = cAm;
-          S.cB[e] = cBm;
-        } else if (kk < nz - 1) {
-          const float r = dcr(1.0f, fmaf(aa, cAm, bb));
-          const float cAk = (-cc) * r;
-          const float cBk = fmaf(-aa, cBm, dd) * r;
-          cAm = cAk;
-          cBm = cBk;
-          S.cA[e] = cAk;
-          S.cB[e] = cBk;
-        } else {
-          const float r = dcr(1.0f, fmaf(aa, cAm, bb));
-          wtop = fmaf(-aa, cBm, dd) * r;
-        }
-      }
+  for (int p = 0; p < npass; p++) {
+    const int k = p * kLevels + q;
+    const bool ok = col && k < nz;
+    const int b = p & 1;
+    float m = 0.0f, wt = 0.0f, w0 = 0.0f, vA = 0.0f, vB = 0.0f, vP = 0.0f, vS = 0.0f;
+    if (ok) {
+      const LevelIn cur = load_level(A, c0 + k * sk);
+      const float fk = fpk_of(A, cur, uh, vh);
+      vA = cur.pk1 + cur.qk;
+      vB = cur.pk2 - cur.qk;
+      vP = cur.pp;
+      vS = cur.pp + fk;
+      sS[k * kColTile + lane] = vS;
+      xs[xs_at(b, 0, q, lane)] = vA;
+      xs[xs_at(b, 1, q, lane)] = vB;
+      xs[xs_at(b, 2, q, lane)] = vP;
+      m = cur.mm;
+      wt = cur.wt;
+      w0 = cur.w0;
     }
-    __syncthreads();
-  }
-  // back substitution (recurrence warp): w(k) overwrites cA(k); w(0) = w(nz) = 0
-  if (!worker && col) {
-    float wk1 = wtop;
-    S.cA[(nz - 1) * kColTile + lane] = wtop;
-    for (int k = nz - 2; k >= 1; k--) {
-      const int e = k * kColTile + lane;
-      const float wk = fmaf(S.cA[e], wk1, S.cB[e]);
-      S.cA[e] = wk;
-      wk1 = wk;
+    workers_sync();
+    if (ok && k >= 1) {
+      // level k - 1: the previous warp of this pass, or the last warp of the previous one
+      const int bp = q > 0 ? b : b ^ 1, qp = q > 0 ? q - 1 : kLevels - 1;
+      const float pA = xs[xs_at(bp, 0, qp, lane)], pB = xs[xs_at(bp, 1, qp, lane)], pP = xs[xs_at(bp, 2, qp, lane)];
+      const float pS = sS[(k - 1) * kColTile + lane];
+      co[co_at(b, 0, q, lane)] = (-asq) * (m * pA);
+      co[co_at(b, 2, q, lane)] = (-asq) * ((-m) * vB);
+      co[co_at(b, 1, q, lane)] = fmaf(-asq, m * ((-vA) + pB), 1.0f);
+      const float fw = fmaf(a.dts, wt, a.beta * ((-m) * (vP - pP)));
+      co[co_at(b, 3, q, lane)] = fmaf(a.alph, (-m) * (vS - pS), w0 + fw);
     }
-    S.cA[lane] = 0.0f;
+    block_sync();
   }
-  __syncthreads();
+  // the epilogue's first loads fly during the last forward pass and the back substitution
+  EpiIn E;
+  if (col) load_epi(A, E, c0, q, nz, sk);
+  block_sync();
   if (!col) return;
-  // pi' update and stores, levels q, q + 17, ... (at most kEpiLevels each): the rrw loads
-  // of all of a thread's levels are issued first
-  float rr[kEpiLevels];
+  // pi' update and stores, levels q, q + kLevels, ... (acoustic_pp.wgsl:131-167,
+  // acoustic_accumulate.wgsl:129-158)
+  for (int k0 = q; k0 <= nz; k0 += kEpiChunk * kLevels) {
+    if (k0 != q) load_epi(A, E, c0, k0, nz, sk);
 #pragma unroll
-  for (int n = 0; n < kEpiLevels; n++) {
-    const int k = q + n * (kLevels + 1);
-    if (k <= nz) rr[n] = A.rrw[c0 + k * sk];
-  }
-#pragma unroll
-  for (int n = 0; n < kEpiLevels; n++) {
-    const int k = q + n * (kLevels + 1);
-    if (k > nz) break;
-    const int c = c0 + k * sk;
-    if (k < nz) {
-      const int e = k * kColTile + lane;
-      const float wk = S.cA[e];
-      const float wk1 = k + 1 < nz ? S.cA[e + kColTile] : 0.0f;
-      float p = fmaf(a.alph, fmaf(wk, S.A[e], wk1 * S.Bq[e]), S.s[e]);
-      if (fabsf(p) < a.smeps) p = 0.0f;
-      A.pp3d[c] = p;
-      const float dum1 = a.kdiv * (p - S.prev[e]);
-      A.ppdw[c] = p + dum1;
-      if (A.saveX != 0) A.ppx[c] = dum1;
-      A.w[c] = wk;
-      A.rrw[c] = A.tavg > 0.0f ? fmaf(wk, a.alph, rr[n]) * A.tavg : rr[n] + wk;
-    } else {
-      A.w[c] = 0.0f;
-      A.rrw[c] = A.tavg > 0.0f ? fmaf(0.0f, a.alph, rr[n]) * A.tavg : rr[n] + 0.0f;
+    for (int t = 0; t < kEpiChunk; t++) {
+      const int k = k0 + t * kLevels;
+      if (k > nz) break;
+      const int c = c0 + k * sk;
+      if (k < nz) {
+        const int e = k * kColTile + lane;
+        const float vA = E.pk1[t] + E.qk[t], vB = E.pk2[t] - E.qk[t];
+        const float wk = cA[e];
+        const float wk1 = k + 1 < nz ? cA[e + kColTile] : 0.0f;
+        float p = fmaf(a.alph, fmaf(wk, vA, wk1 * vB), sS[e]);
+        if (fabsf(p) < a.smeps) p = 0.0f;
+        A.pp3d[c] = p;
+        const float dum1 = a.kdiv * (p - E.pp[t]);
+        A.ppdw[c] = p + dum1;
+        if (A.saveX != 0) A.ppx[c] = dum1;
+        A.w[c] = wk;
+        A.rrw[c] = A.tavg > 0.0f ? fmaf(wk, a.alph, E.rr[t]) * A.tavg : E.rr[t] + wk;
+      } else {
+        A.w[c] = 0.0f;
+        A.rrw[c] = A.tavg > 0.0f ? fmaf(0.0f, a.alph, E.rr[t]) * A.tavg : E.rr[t] + 0.0f;
+      }
     }
   }
 }
@@ -798,7 +893,7 @@ static bool match_substep(const std::vector<Op>& ops, size_t i, FusedSegment& s,
   const Op& acc = ops[i + 6];
   if (!is_name(acc, "acoustic_accumulate")) return false;
   const Dims& g = uv.args.g;
-  if (g.nx < 1 || g.ny < 1 || g.nz < 3 || g.nz + 1 > kEpiLevels * (kLevels + 1) || col_smem_bytes(g.nz) > 110 * 1024)
+  if (g.nx < 1 || g.ny < 1 || g.nz < 3 || col_smem_bytes(g.nz) > 200 * 1024)
     return false;
   for (const Op* o : {&fp, &ws, &pp, &acc})
     if (!same_dims(g, o->args.g) || !same_acoustic(uv.args.a, o->args.a)) return false;
