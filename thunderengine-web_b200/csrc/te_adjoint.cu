@@ -132,8 +132,8 @@ __global__ void __launch_bounds__(kAdjCols * kAdjWarps) k_adj_wsolve_coop(AdjArg
   if (on)
     for (int k = 1 + wq; k <= nz - 1; k += kAdjWarps) {
       const int c = c0 + k * sk, e = k * kAdjCols + lane;
-      const float Ak = pk1[c] + qk[c], Bk = pk2[c] - qk[c];
-      const float Am = pk1[c - sk] + qk[c - sk], Bm = pk2[c - sk] - qk[c - sk];
+      const float Ak = pk1[c] + qk[c];
+      const float Bm = pk2[c - sk] - qk[c - sk];
       const float m = mm[c];
       sDia[e] = fmaf(-asq, m * ((-Ak) + Bm), 1.0f);
       sSub[e] = k > 1 ? (-asq) * ((-mm[c - sk]) * Bm) : 0.0f;          // cc(k - 1)

@@ -41,25 +41,34 @@ __device__ __forceinline__ float weno5_upwind(const float* a, int c, int s, bool
 // Horizontal faces come in two forms: face_X_h_at reads the advected field's stencil
 // through (a, ca, sa) - values a[ca + n * sa] along the face's axis - so that a caller
 // may stage the field elsewhere (shared memory); face_X_h reads it from the tape field.
+//
+// The *_c forms take the face's linear index c (and the grid g it was formed on) from
+// the caller, so that a caller that walks many faces forms each index once; stagger
+// dependent forms take the stagger as a template argument SG (0: read it from the
+// bindings).  Every form evaluates the same operations as the reference kernel.
 template <int DIR>
-__device__ __forceinline__ float face_lin_h_at(const KArgs& A, int i, int j, int k, const float* a, int ca, int sa) {
-  const Dims& g = A.g;
+__device__ __forceinline__ float face_lin_h_c(const KArgs& A, int c, const float* a, int ca, int sa) {
   const float* rr = A.p[2];
-  int c = gidx(g, i, j, k);
   float u = rr[c];
   float f = flx5(sten5(a, ca, sa, u >= 0.0f, 0));
   return u * f;
+}
+template <int DIR>
+__device__ __forceinline__ float face_lin_h_at(const KArgs& A, int i, int j, int k, const float* a, int ca, int sa) {
+  return face_lin_h_c<DIR>(A, gidx(A.g, i, j, k), a, ca, sa);
 }
 template <int DIR>
 __device__ __forceinline__ float face_lin_h(const KArgs& A, int i, int j, int k) {
   return face_lin_h_at<DIR>(A, i, j, k, A.p[1], gidx(A.g, i, j, k), DIR == 0 ? 1 : A.g.sJ);
 }
 
-__device__ __forceinline__ float face_lin_z(const KArgs& A, int i, int j, int k) {
-  const Dims& g = A.g;
+__device__ __forceinline__ float face_lin_z_c(const KArgs& A, const Dims& g, int c, int k) {
   const float *s = A.p[1], *rrw = A.p[2], *c1 = A.p[3], *c2 = A.p[4];
   const int sk = g.sJ * g.sK;
-  int c = gidx(g, i, j, k);
+  if (k > 2 && k < g.nz - 2) {  // the interior stencil, tested first (the common case)
+    float w = rrw[c];
+    return w * flx5(sten5(s, c, sk, w >= 0.0f, 0));
+  }
   if (k == 0 || k == g.nz) {
     return 0.0f;
   }
@@ -73,14 +82,15 @@ __device__ __forceinline__ float face_lin_z(const KArgs& A, int i, int j, int k)
   else f = flx5(sten5(s, c, sk, up, 0));
   return w * f;
 }
+__device__ __forceinline__ float face_lin_z(const KArgs& A, int i, int j, int k) {
+  return face_lin_z_c(A, A.g, gidx(A.g, i, j, k), k);
+}
 
-template <int DIR>
-__device__ __forceinline__ float face_stag_h_at(const KArgs& A, int i, int j, int k, const float* a, int ca, int sa) {
-  const Dims& g = A.g;
-  const int stag = A.iv[1];
+template <int DIR, int SG = 0>
+__device__ __forceinline__ float face_stag_h_c(const KArgs& A, const Dims& g, int c, int k, const float* a, int ca, int sa) {
+  const int stag = SG ? SG : A.iv[1];
   const float *rr = DIR == 0 ? A.p[3] : A.p[4], *c2 = A.p[7];
   const int sj = g.sJ, sk = g.sJ * g.sK;
-  int c = gidx(g, i, j, k);
   if (stag == 4 && k == 0) {
     return 0.0f;
   }
@@ -100,22 +110,28 @@ __device__ __forceinline__ float face_stag_h_at(const KArgs& A, int i, int j, in
   }
 }
 template <int DIR>
+__device__ __forceinline__ float face_stag_h_at(const KArgs& A, int i, int j, int k, const float* a, int ca, int sa) {
+  return face_stag_h_c<DIR>(A, A.g, gidx(A.g, i, j, k), k, a, ca, sa);
+}
+template <int DIR>
 __device__ __forceinline__ float face_stag_h(const KArgs& A, int i, int j, int k) {
   return face_stag_h_at<DIR>(A, i, j, k, A.p[2], gidx(A.g, i, j, k), DIR == 0 ? 1 : A.g.sJ);
 }
 
-__device__ __forceinline__ float face_stag_z(const KArgs& A, int i, int j, int k) {
-  const Dims& g = A.g;
-  const int stag = A.iv[1];
+template <int SG = 0>
+__device__ __forceinline__ float face_stag_z_c(const KArgs& A, const Dims& g, int c, int k) {
+  const int stag = SG ? SG : A.iv[1];
   const float *a = A.p[2], *rrw = A.p[5], *c1 = A.p[6], *c2 = A.p[7];
   const int sj = g.sJ, sk = g.sJ * g.sK;
-  int c = gidx(g, i, j, k);
   float m;
   if (stag == 2) m = 0.5f * (rrw[c] + rrw[c - 1]);
   else if (stag == 3) m = 0.5f * (rrw[c] + rrw[c - sj]);
   else m = 0.5f * (rrw[c] + (k < g.nz ? rrw[c + sk] : 0.0f));
   bool up = m >= 0.0f;
   float f;
+  // the interior stencils, tested first (the common case)
+  if (stag == 4 && k >= 2 && k < g.nz - 2) return m * flx5(sten5(a, c, sk, up, 1));
+  if (stag != 4 && k > 2 && k < g.nz - 2) return m * flx5(sten5(a, c, sk, up, 0));
   if (stag == 4) {
     if (k > g.nz - 1) {
       return 0.0f;
@@ -137,36 +153,47 @@ __device__ __forceinline__ float face_stag_z(const KArgs& A, int i, int j, int k
   }
   return m * f;
 }
+__device__ __forceinline__ float face_stag_z(const KArgs& A, int i, int j, int k) {
+  return face_stag_z_c(A, A.g, gidx(A.g, i, j, k), k);
+}
 
 template <int DIR>
-__device__ __forceinline__ float face_weno_h_at(const KArgs& A, int i, int j, int k, const float* a, int ca, int sa) {
-  const Dims& g = A.g;
+__device__ __forceinline__ float face_weno_h_c(const KArgs& A, int c, const float* a, int ca, int sa) {
   const float* rr = A.p[2];
   const float weps = A.f[3];
   const int pdef = A.iv[4];
-  int c = gidx(g, i, j, k);
   float r = rr[c];
   const Sten5 t = sten5(a, ca, sa, r >= 0.0f, 0);
   bool ok = pdef != 1 || weno_pdef_ok(t.s1, t.s2, t.s3, t.s4, t.s5, weps);
   return ok ? r * weno5(t, weps) : 0.0f;
 }
 template <int DIR>
+__device__ __forceinline__ float face_weno_h_at(const KArgs& A, int i, int j, int k, const float* a, int ca, int sa) {
+  return face_weno_h_c<DIR>(A, gidx(A.g, i, j, k), a, ca, sa);
+}
+template <int DIR>
 __device__ __forceinline__ float face_weno_h(const KArgs& A, int i, int j, int k) {
   return face_weno_h_at<DIR>(A, i, j, k, A.p[1], gidx(A.g, i, j, k), DIR == 0 ? 1 : A.g.sJ);
 }
 
-__device__ __forceinline__ float face_weno_z(const KArgs& A, int i, int j, int k) {
-  const Dims& g = A.g;
+__device__ __forceinline__ float face_weno_z_c(const KArgs& A, const Dims& g, int c, int k) {
   const int kf = k + 1;
   const float *a = A.p[1], *rrw = A.p[2], *c1 = A.p[3], *c2 = A.p[4];
   const float weps = A.f[5];
   const int pdefweno = A.iv[7];
   const int sk = g.sJ * g.sK, nk = g.nz;
-  int c = gidx(g, i, j, k);
+#define AZ(o) a[c + (o) * sk]
+  if (kf > 3 && kf < nk - 1) {  // the interior stencil, tested first (the common case)
+    const float w = rrw[c];
+    float s1, s2, s3, s4, s5;
+    if (w >= 0.0f) { s1 = AZ(-3); s2 = AZ(-2); s3 = AZ(-1); s4 = AZ(0); s5 = AZ(1); }
+    else { s1 = AZ(2); s2 = AZ(1); s3 = AZ(0); s4 = AZ(-1); s5 = AZ(-2); }
+    if (pdefweno == 1 && !weno_pdef_ok(s1, s2, s3, s4, s5, weps)) return 0.0f;
+    return w * weno5(s1, s2, s3, s4, s5, weps);
+  }
   if (kf == 1 || kf == g.nz + 1) {
     return 0.0f;
   }
-#define AZ(o) a[c + (o) * sk]
   float w = rrw[c];
   if (kf == 2) {
     return w >= 0.0f ? w * fmaf(c1[k], AZ(-1), c2[k] * AZ(0)) : w * upstrpd(AZ(1), AZ(0), AZ(-1), weps);
@@ -197,15 +224,16 @@ __device__ __forceinline__ float face_weno_z(const KArgs& A, int i, int j, int k
   return w * weno5(s1, s2, s3, s4, s5, weps);
 #undef AZ
 }
+__device__ __forceinline__ float face_weno_z(const KArgs& A, int i, int j, int k) {
+  return face_weno_z_c(A, A.g, gidx(A.g, i, j, k), k);
+}
 
-template <int DIR>
-__device__ __forceinline__ float face_weno_uv_h_at(const KArgs& A, int i, int j, int k, const float* a, int ca, int sa) {
-  const Dims& g = A.g;
-  const int stag = A.iv[1];
+template <int DIR, int SG = 0>
+__device__ __forceinline__ float face_weno_uv_h_c(const KArgs& A, const Dims& g, int c, const float* a, int ca, int sa) {
+  const int stag = SG ? SG : A.iv[1];
   const float* rr = A.p[3];
   const float weps = A.f[4];
   const int sj = g.sJ;
-  int c = gidx(g, i, j, k);
   if (DIR == 0) {
     float m = stag == 2 ? 0.5f * (rr[c] + rr[c + 1]) : 0.5f * (rr[c] + rr[c - sj]);
     return m * weno5_upwind(a, ca, sa, m >= 0.0f, stag == 2, weps);
@@ -215,17 +243,24 @@ __device__ __forceinline__ float face_weno_uv_h_at(const KArgs& A, int i, int j,
   }
 }
 template <int DIR>
+__device__ __forceinline__ float face_weno_uv_h_at(const KArgs& A, int i, int j, int k, const float* a, int ca, int sa) {
+  return face_weno_uv_h_c<DIR>(A, A.g, gidx(A.g, i, j, k), a, ca, sa);
+}
+template <int DIR>
 __device__ __forceinline__ float face_weno_uv_h(const KArgs& A, int i, int j, int k) {
   return face_weno_uv_h_at<DIR>(A, i, j, k, A.p[2], gidx(A.g, i, j, k), DIR == 0 ? 1 : A.g.sJ);
 }
 
-__device__ __forceinline__ float face_weno_uv_z(const KArgs& A, int i, int j, int k) {
-  const Dims& g = A.g;
-  const int stag = A.iv[1];
+template <int SG = 0>
+__device__ __forceinline__ float face_weno_uv_z_c(const KArgs& A, const Dims& g, int c, int k) {
+  const int stag = SG ? SG : A.iv[1];
   const float *a = A.p[2], *rrw = A.p[3], *c1 = A.p[4], *c2 = A.p[5];
   const float weps = A.f[6];
   const int sj = g.sJ, sk = g.sJ * g.sK;
-  int c = gidx(g, i, j, k);
+  if (k > 2 && k < g.nz - 2) {  // the interior stencil, tested first (the common case)
+    const float m = stag == 2 ? 0.5f * (rrw[c] + rrw[c - 1]) : 0.5f * (rrw[c] + rrw[c - sj]);
+    return m * weno5(sten5(a, c, sk, m >= 0.0f, 0), weps);
+  }
   if (k == 0 || k == g.nz) {
     return 0.0f;
   }
@@ -241,14 +276,15 @@ __device__ __forceinline__ float face_weno_uv_z(const KArgs& A, int i, int j, in
   return m * f;
 #undef AZ
 }
+__device__ __forceinline__ float face_weno_uv_z(const KArgs& A, int i, int j, int k) {
+  return face_weno_uv_z_c(A, A.g, gidx(A.g, i, j, k), k);
+}
 
 template <int DIR>
-__device__ __forceinline__ float face_weno_w_h_at(const KArgs& A, int i, int j, int k, const float* a, int ca, int sa) {
-  const Dims& g = A.g;
+__device__ __forceinline__ float face_weno_w_h_c(const KArgs& A, const Dims& g, int c, int k, const float* a, int ca, int sa) {
   const float *rr = A.p[2], *c2 = A.p[3];
   const float weps = A.f[4];
   const int sk = g.sJ * g.sK;
-  int c = gidx(g, i, j, k);
   if (k == 0) {
     return 0.0f;
   }
@@ -258,16 +294,22 @@ __device__ __forceinline__ float face_weno_w_h_at(const KArgs& A, int i, int j, 
   return ub * weno5(sten5(a, ca, sa, ub >= 0.0f, 0), weps);
 }
 template <int DIR>
+__device__ __forceinline__ float face_weno_w_h_at(const KArgs& A, int i, int j, int k, const float* a, int ca, int sa) {
+  return face_weno_w_h_c<DIR>(A, A.g, gidx(A.g, i, j, k), k, a, ca, sa);
+}
+template <int DIR>
 __device__ __forceinline__ float face_weno_w_h(const KArgs& A, int i, int j, int k) {
   return face_weno_w_h_at<DIR>(A, i, j, k, A.p[1], gidx(A.g, i, j, k), DIR == 0 ? 1 : A.g.sJ);
 }
 
-__device__ __forceinline__ float face_weno_w_z(const KArgs& A, int i, int j, int k) {
-  const Dims& g = A.g;
+__device__ __forceinline__ float face_weno_w_z_c(const KArgs& A, const Dims& g, int c, int k) {
   const float *a = A.p[1], *rrw = A.p[2];
   const float weps = A.f[3];
   const int sk = g.sJ * g.sK, nz = g.nz;
-  int c = gidx(g, i, j, k);
+  if (k >= 2 && k < nz - 2) {  // the interior stencil, tested first (the common case)
+    const float wb = 0.5f * (rrw[c] + rrw[c + sk]);
+    return wb * weno5(sten5(a, c, sk, wb >= 0.0f, 1), weps);
+  }
   if (k > g.nz - 1) {
     return 0.0f;
   }
@@ -282,27 +324,33 @@ __device__ __forceinline__ float face_weno_w_z(const KArgs& A, int i, int j, int
   return wb * f;
 #undef AZ
 }
+__device__ __forceinline__ float face_weno_w_z(const KArgs& A, int i, int j, int k) {
+  return face_weno_w_z_c(A, A.g, gidx(A.g, i, j, k), k);
+}
 
 // Pieces of adv_assemble (adv_assemble.wgsl:139-279), shared by the per-dispatch kernel
 // and the fused advection kernel.  assemble_dv_off: offset of the second divergence
 // value the cell's stagger averages (0 for a scalar); assemble_dv: the divergence at the
 // cell from divx[c] and divx[c - off]; assemble_core: the tendency from the advected
 // value s[c], that divergence and the flux differences.
+template <int SG = 0>
 __device__ __forceinline__ int assemble_dv_off(const KArgs& A) {
-  const int stag = A.iv[1], st = stag < 0 ? -stag : stag;
+  const int stag = SG ? SG : A.iv[1], st = stag < 0 ? -stag : stag;
   return st == 2 ? 1 : (st == 3 ? A.g.sJ : (st == 4 ? A.g.sJ * A.g.sK : 0));
 }
+template <int SG = 0>
 __device__ __forceinline__ float assemble_dv(const KArgs& A, int k, float d0, float d1) {
-  const int stag = A.iv[1], st = stag < 0 ? -stag : stag;
+  const int stag = SG ? SG : A.iv[1], st = stag < 0 ? -stag : stag;
   const float *c1 = A.p[15], *c2 = A.p[16];
   if (st == 2 || st == 3) return 0.5f * (d0 + d1);
   if (st == 4) return fmaf(c2[k], d0, c1[k] * d1);
   return d0;
 }
+template <int SG = 0>
 __device__ __forceinline__ float assemble_core(const KArgs& A, int i, int j, int k, float sc, float dv, float dFx,
                                                float dFy, float dFz) {
   const Dims& g = A.g;
-  const int stag = A.iv[1], st = stag < 0 ? -stag : stag;
+  const int stag = SG ? SG : A.iv[1], st = stag < 0 ? -stag : stag;
   const float *rho0 = A.p[7], *rf0 = A.p[8], *mh = A.p[9], *mf = A.p[10];
   const float* hm = A.p[30];
   const float mz = stag < 0 ? 1.0f : (stag == 4 ? mf[k] : mh[k]);

@@ -564,17 +564,24 @@ struct AdvArgs {
   float dttmp;
 };
 
-template <int KIND, int DIR>
-__device__ __forceinline__ float adv_face(const KArgs& A, int i, int j, int k) {
-  if (KIND == kLin) return DIR == 2 ? face_lin_z(A, i, j, k) : face_lin_h<DIR>(A, i, j, k);
-  if (KIND == kStag) return DIR == 2 ? face_stag_z(A, i, j, k) : face_stag_h<DIR>(A, i, j, k);
-  if (KIND == kWeno) return DIR == 2 ? face_weno_z(A, i, j, k) : face_weno_h<DIR>(A, i, j, k);
-  if (KIND == kWenoUV) return DIR == 2 ? face_weno_uv_z(A, i, j, k) : face_weno_uv_h<DIR>(A, i, j, k);
-  return DIR == 2 ? face_weno_w_z(A, i, j, k) : face_weno_w_h<DIR>(A, i, j, k);
+// Face (i, j, k) of direction DIR whose linear index c on the common grid g is known.
+template <int KIND, int DIR, int ST>
+__device__ __forceinline__ float adv_face(const KArgs& A, const Dims& g, int c, int k) {
+  const int sa = DIR == 0 ? 1 : g.sJ;
+  if (KIND == kLin) return DIR == 2 ? face_lin_z_c(A, g, c, k) : face_lin_h_c<DIR>(A, c, A.p[1], c, sa);
+  if (KIND == kStag) return DIR == 2 ? face_stag_z_c<ST>(A, g, c, k) : face_stag_h_c<DIR, ST>(A, g, c, k, A.p[2], c, sa);
+  if (KIND == kWeno) return DIR == 2 ? face_weno_z_c(A, g, c, k) : face_weno_h_c<DIR>(A, c, A.p[1], c, sa);
+  if (KIND == kWenoUV)
+    return DIR == 2 ? face_weno_uv_z_c<ST>(A, g, c, k) : face_weno_uv_h_c<DIR, ST>(A, g, c, A.p[2], c, sa);
+  return DIR == 2 ? face_weno_w_z_c(A, g, c, k) : face_weno_w_h_c<DIR>(A, g, c, k, A.p[1], c, sa);
 }
 
 __device__ __forceinline__ bool in_range(const FaceRange& r, int i, int j, int k) {
   return i >= r.ilo && i <= r.ihi && j >= r.jlo && j <= r.jhi && k >= r.klo && k <= r.khi;
+}
+// the box [i0, i1] x [j0, j1] x [k0, k1] lies inside r
+__device__ __forceinline__ bool box_in(const FaceRange& r, int i0, int i1, int j0, int j1, int k0, int k1) {
+  return i0 >= r.ilo && i1 <= r.ihi && j0 >= r.jlo && j1 <= r.jhi && k0 >= r.klo && k1 <= r.khi;
 }
 
 constexpr int kAdvTX = 32, kAdvTY = 8;
@@ -586,30 +593,37 @@ constexpr int kAdvTX = 32, kAdvTY = 8;
 // (double-buffered, one barrier per level; the faces beyond 256 by warps 0 and 1), and
 // each cell computes the z-face above it, reusing the one below from the level before.
 // KZ = 4 where the z-face is a WENO reconstruction (momentum WENO: the saved face pays
-// for the shorter grid); KZ = 1 (most parallel) where faces are cheap.
+// for the shorter grid); KZ = 1 (most parallel) where faces are cheap.  Every index is
+// formed once per thread on the assembly's grid (the four dispatches share it) and
+// advanced by a level stride; a tile whose faces and cells all lie inside the dispatch
+// ranges (all but the edge tiles) skips the per-face range tests.
 template <int KIND>
 struct AdvKZ {
   static constexpr int value = KIND == kWenoUV || KIND == kWenoW ? 4 : 1;
 };
 
-template <int KIND, int ST>
-__global__ void __launch_bounds__(kAdvTX* kAdvTY, AdvKZ<KIND>::value > 1 ? 6 : 8) k_adv_fused(AdvArgs A) {
+template <int KIND, int ST, bool FULL>
+__device__ __forceinline__ void adv_tile(const AdvArgs& A, float (*fxs)[kAdvTY][kAdvTX + 1], float (*fys)[kAdvTY + 1][kAdvTX]) {
   constexpr int kAdvKZ = AdvKZ<KIND>::value;
-  __shared__ float fxs[2][kAdvTY][kAdvTX + 1];
-  __shared__ float fys[2][kAdvTY + 1][kAdvTX];
   constexpr int dx = ST == 2 ? -1 : 0, dy = ST == 3 ? -1 : 0, dz = ST == 4 ? -1 : 0;
+  const Dims& g = A.as.g;
+  const int sk = g.sJ * g.sK;
   const int lx = threadIdx.x, ly = threadIdx.y, t = ly * kAdvTX + lx;
   const int i0 = A.ilo + (int)blockIdx.x * kAdvTX, j0 = A.jlo + (int)blockIdx.y * kAdvTY;
   const int i = i0 + lx, j = j0 + ly;
   const int kb = A.klo + (int)blockIdx.z * kAdvKZ, ke = min(A.khi, kb + kAdvKZ - 1);
-  const bool cell = i <= A.ihi && j <= A.jhi;
+  const bool cell = FULL || (i <= A.ihi && j <= A.jhi);
   const int xr = t / (kAdvTX + 1), xq = t % (kAdvTX + 1);                       // x-face of this thread
   const int e2 = kAdvTX * kAdvTY + lx, xr2 = e2 / (kAdvTX + 1), xq2 = e2 % (kAdvTX + 1);  // 256..263, warp 0
-  float fzb = cell ? adv_face<KIND, 2>(A.fz, i, j, kb + dz) : 0.0f;
-  const int dvoff = assemble_dv_off(A.as);
+  // level-0 indices: the cell, its x-face, y-face and the extra faces of warps 0 and 1
+  const int cc0 = gidx(g, i, j, 0);
+  const int cx0 = gidx(g, i0 + dx + xq, j0 + xr, 0), cy0 = gidx(g, i, j0 + dy + ly, 0);
+  const int cx20 = gidx(g, i0 + dx + xq2, j0 + xr2, 0), cy20 = gidx(g, i, j0 + dy + kAdvTY, 0);
+  float fzb = cell ? adv_face<KIND, 2, ST>(A.fz, g, cc0 + (kb + dz) * sk, kb + dz) : 0.0f;
+  const int dvoff = assemble_dv_off<ST>(A.as);
   for (int k = kb, b = 0; k <= ke; k++, b ^= 1) {
     // the cell's own inputs first, so their loads overlap the face computations
-    const int c = gidx(A.as.g, i, j, k);
+    const int c = cc0 + k * sk;
     float sc = 0.0f, d0 = 0.0f, d1 = 0.0f, dst = 0.0f, dv3 = 0.0f, tht = 0.0f, pa = 0.0f;
     if (cell) {
       sc = A.as.p[2][c];
@@ -622,20 +636,21 @@ __global__ void __launch_bounds__(kAdvTX* kAdvTY, AdvKZ<KIND>::value > 1 ? 6 : 8
       }
       if (A.phi) pa = A.phiA[c];
     }
-    if (in_range(A.rx, i0 + dx + xq, j0 + xr, k)) fxs[b][xr][xq] = adv_face<KIND, 0>(A.fx, i0 + dx + xq, j0 + xr, k);
-    if (in_range(A.ry, i, j0 + dy + ly, k)) fys[b][ly][lx] = adv_face<KIND, 1>(A.fy, i, j0 + dy + ly, k);
-    if (ly == 0 && lx < kAdvTY && in_range(A.rx, i0 + dx + xq2, j0 + xr2, k))
-      fxs[b][xr2][xq2] = adv_face<KIND, 0>(A.fx, i0 + dx + xq2, j0 + xr2, k);
-    if (ly == 1 && in_range(A.ry, i, j0 + dy + kAdvTY, k))
-      fys[b][kAdvTY][lx] = adv_face<KIND, 1>(A.fy, i, j0 + dy + kAdvTY, k);
-    const float fzt = cell ? adv_face<KIND, 2>(A.fz, i, j, k + dz + 1) : 0.0f;
+    const int ko = k * sk;
+    if (FULL || in_range(A.rx, i0 + dx + xq, j0 + xr, k)) fxs[b][xr][xq] = adv_face<KIND, 0, ST>(A.fx, g, cx0 + ko, k);
+    if (FULL || in_range(A.ry, i, j0 + dy + ly, k)) fys[b][ly][lx] = adv_face<KIND, 1, ST>(A.fy, g, cy0 + ko, k);
+    if (ly == 0 && lx < kAdvTY && (FULL || in_range(A.rx, i0 + dx + xq2, j0 + xr2, k)))
+      fxs[b][xr2][xq2] = adv_face<KIND, 0, ST>(A.fx, g, cx20 + ko, k);
+    if (ly == 1 && (FULL || in_range(A.ry, i, j0 + dy + kAdvTY, k)))
+      fys[b][kAdvTY][lx] = adv_face<KIND, 1, ST>(A.fy, g, cy20 + ko, k);
+    const float fzt = cell ? adv_face<KIND, 2, ST>(A.fz, g, c + (dz + 1) * sk, k + dz + 1) : 0.0f;
     __syncthreads();
     if (cell) {
       const float dFx = fxs[b][ly][lx + 1] - fxs[b][ly][lx];
       const float dFy = fys[b][ly + 1][lx] - fys[b][ly][lx];
       // adv_assemble without its open-boundary branches (the planner fuses closed and
       // periodic boundaries only)
-      float tn = assemble_core(A.as, i, j, k, sc, assemble_dv(A.as, k, d0, d1), dFx, dFy, fzt - fzb);
+      float tn = assemble_core<ST>(A.as, i, j, k, sc, assemble_dv<ST>(A.as, k, d0, d1), dFx, dFy, fzt - fzb);
       if (A.accumulate) {
         A.dest[c] = dst + tn;
       } else {
@@ -646,6 +661,23 @@ __global__ void __launch_bounds__(kAdvTX* kAdvTY, AdvKZ<KIND>::value > 1 ? 6 : 8
     }
     fzb = fzt;
   }
+}
+
+template <int KIND, int ST>
+__global__ void __launch_bounds__(kAdvTX* kAdvTY, AdvKZ<KIND>::value > 1 ? 6 : 8) k_adv_fused(AdvArgs A) {
+  constexpr int kAdvKZ = AdvKZ<KIND>::value;
+  constexpr int dx = ST == 2 ? -1 : 0, dy = ST == 3 ? -1 : 0, dz = ST == 4 ? -1 : 0;
+  __shared__ float fxs[2][kAdvTY][kAdvTX + 1];
+  __shared__ float fys[2][kAdvTY + 1][kAdvTX];
+  const int i0 = A.ilo + (int)blockIdx.x * kAdvTX, j0 = A.jlo + (int)blockIdx.y * kAdvTY;
+  const int kb = A.klo + (int)blockIdx.z * kAdvKZ, ke = min(A.khi, kb + kAdvKZ - 1);
+  const int i1 = i0 + kAdvTX - 1, j1 = j0 + kAdvTY - 1;
+  const bool full = i1 <= A.ihi && j1 <= A.jhi && box_in(A.rx, i0 + dx, i1 + dx + 1, j0, j1, kb, ke) &&
+                    box_in(A.ry, i0, i1, j0 + dy, j1 + dy + 1, kb, ke) && box_in(A.rz, i0, i1, j0, j1, kb + dz, ke + dz + 1);
+  if (full)
+    adv_tile<KIND, ST, true>(A, fxs, fys);
+  else
+    adv_tile<KIND, ST, false>(A, fxs, fys);
 }
 
 template <int KIND, int ST>
