@@ -347,7 +347,9 @@ def adjoint_leg(dev, nx=128, ny=128, nz=64, steps=60, every=10):
     dV = g.dx * g.dy * g.dz
     gw = 2.0 * w.astype(np.float64) * dV
     win.backward(gw)  # captures the block graphs
-    t_fwd, w = timed(lambda: win.forward(*ctl))
+    win.load(*ctl)
+    t_fwd, _ = timed(win.run_forward)
+    w = win.read_w()
     lw = np.zeros((g.nz + 1, g.strideK, g.strideJ), dtype=np.float32)
     lw[1:g.nz, 3:3 + g.ny, 3:3 + g.nx] = 2.0 * w.astype(np.float64) * dV
     win.r.adjoint_zero()
@@ -589,8 +591,8 @@ def kernel_roofline(r, run, stream, mode):
                                                      else 'fallback 6650 GB/s'),
             'algorithmic_bytes_per_launch': byts, 'launch_ms': ms,
             'traffic': dram * g.nx * g.ny * g.nz if dram else None,
-            'traffic_source': ('ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on the 160x160x80 '
-                               'workload, scaled by interior points' if dram else None),
+            'traffic_source': ('ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on the 256x256x80 '
+                               'workload, per interior point, times this run\'s interior points' if dram else None),
             'share_of_step': shares[0][1], 'sum_of_kernel_ms_per_step': tot,
             'top_kernels': [[n, round(sv, 4), round(stats[n][0], 4), stats[n][1],
                              round(stats[n][2] / (stats[n][0] / 1e3) / 1e9, 1)] for n, sv in shares[:10]],
@@ -599,11 +601,11 @@ def kernel_roofline(r, run, stream, mode):
 
 
 # DRAM bytes per interior point of one launch of the dominant kernels: one ncu capture
-# (dram__bytes_read.sum + dram__bytes_write.sum) of the kernel on the 160x160x80 workload
-# (a size ncu captures quickly), divided by its interior points; traffic grows with the
-# points a launch processes.  Writes still held in L2 when the launch ends are not counted.
+# (dram__bytes_read.sum + dram__bytes_write.sum, a one-pass metric set) of the kernel on
+# the 256x256x80 workload, divided by its interior points; traffic grows with the points
+# a launch processes.  Writes still held in L2 when the launch ends are not counted.
 NCU_DRAM_BYTES_PER_POINT = {
-    'acoustic_column (fused fpk+w_solve+pp+accumulate)': (112.06e6 + 13.74e6) / (160 * 160 * 80),
+    'acoustic_column (fused fpk+w_solve+pp+accumulate)': (286.53e6 + 84.02e6) / (256 * 256 * 80),
 }
 
 

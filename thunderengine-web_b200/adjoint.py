@@ -75,6 +75,12 @@ class CoreWindow:
         """Sets the start state from the controls (numpy or torch, shape (nz, ny, nx)),
         runs the window keeping checkpoints and returns w at the end, shape
         (nz - 1, ny, nx), float32 numpy."""
+        self.load(th, u, v)
+        self.run_forward()
+        return self.read_w()
+
+    def load(self, th, u, v):
+        """Uploads the start state with the controls th', u, v (no steps run)."""
         g = self.g
         arena = self.arena0.copy()
         for name, x in zip(FIELDS, (th, u, v)):
@@ -87,7 +93,14 @@ class CoreWindow:
             if i != self.aid:
                 self.r.upload(i, b)
         self.r.upload(self.aid, arena.tobytes())
+
+    def run_forward(self):
+        """The window from the loaded start state, keeping checkpoints (device work only)."""
         self.r.adjoint_forward(self.nsteps, self.every)
+
+    def read_w(self):
+        """w at the end of the window, shape (nz - 1, ny, nx)."""
+        g = self.g
         w = self.r.read(g.count, self.base + self.run.fields['w'] // 4).view(np.float32)
         return w.reshape(g.nz + 1, g.strideK, g.strideJ)[1:g.nz, 3:3 + g.ny, 3:3 + g.nx].copy()
 

@@ -597,9 +597,35 @@ constexpr int kAdvTX = 32, kAdvTY = 8;
 // formed once per thread on the assembly's grid (the four dispatches share it) and
 // advanced by a level stride; a tile whose faces and cells all lie inside the dispatch
 // ranges (all but the edge tiles) skips the per-face range tests.
+#ifndef TE_ADV_KZ_FAST
+#define TE_ADV_KZ_FAST 1   // levels per CTA, linear and staggered-linear kinds
+#endif
+#ifndef TE_ADV_KZ_WENO
+#define TE_ADV_KZ_WENO 1   // levels per CTA, scalar WENO
+#endif
+#ifndef TE_ADV_KZ_WENO_MOM
+#define TE_ADV_KZ_WENO_MOM 4   // levels per CTA, momentum WENO
+#endif
+#ifndef TE_ADV_MINB_FAST
+#define TE_ADV_MINB_FAST 8   // resident CTAs per SM the register budget is sized for
+#endif
+#ifndef TE_ADV_MINB_WENO
+#define TE_ADV_MINB_WENO 8
+#endif
+#ifndef TE_ADV_MINB_WENO_MOM
+#define TE_ADV_MINB_WENO_MOM 6
+#endif
 template <int KIND>
 struct AdvKZ {
-  static constexpr int value = KIND == kWenoUV || KIND == kWenoW ? 4 : 1;
+  static constexpr int value = KIND == kWenoUV || KIND == kWenoW ? TE_ADV_KZ_WENO_MOM
+                               : KIND == kWeno                   ? TE_ADV_KZ_WENO
+                                                                 : TE_ADV_KZ_FAST;
+};
+template <int KIND>
+struct AdvMinBlocks {
+  static constexpr int value = KIND == kLin || KIND == kStag ? TE_ADV_MINB_FAST
+                               : KIND == kWeno                 ? TE_ADV_MINB_WENO
+                                                               : TE_ADV_MINB_WENO_MOM;
 };
 
 template <int KIND, int ST, bool FULL>
@@ -664,7 +690,7 @@ __device__ __forceinline__ void adv_tile(const AdvArgs& A, float (*fxs)[kAdvTY][
 }
 
 template <int KIND, int ST>
-__global__ void __launch_bounds__(kAdvTX* kAdvTY, AdvKZ<KIND>::value > 1 ? 6 : 8) k_adv_fused(AdvArgs A) {
+__global__ void __launch_bounds__(kAdvTX* kAdvTY, AdvMinBlocks<KIND>::value) k_adv_fused(AdvArgs A) {
   constexpr int kAdvKZ = AdvKZ<KIND>::value;
   constexpr int dx = ST == 2 ? -1 : 0, dy = ST == 3 ? -1 : 0, dz = ST == 4 ? -1 : 0;
   __shared__ float fxs[2][kAdvTY][kAdvTX + 1];
