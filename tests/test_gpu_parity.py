@@ -275,6 +275,23 @@ def test_fused_mode_odd_sizes_nsound8():
     _fused_vs_oracle(scenario.tiny(37, 29, 13, dx=500.0, dz=250.0, dt=3.0, nsound=8, us=25.0), nsteps=2)
 
 
+@pytest.mark.parametrize('dims', [(37, 29, 13), (64, 40, 24)])
+def test_aligned_rows_exact_and_fused_vs_oracle(dims):
+    """Rows padded to a multiple of 32 floats (the reference's alignRows layout: every row
+    starts on a 128-byte boundary): the per-dispatch step equals the oracle word for word,
+    the fused step on every non-scratch field, and the padding columns stay untouched."""
+    nx, ny, nz = dims
+    cfg = scenario.tiny(nx, ny, nz, dx=500.0, dz=250.0, dt=3.0, nsound=8, us=25.0, align_rows=True)
+    run = timestep.Run(cfg)
+    assert run.grid.strideJ % 32 == 0 and run.grid.strideJ > nx + 7
+    tape = run.tape(1)
+    init = run.initial_buffers()
+    cpu, gpu, mem = _compare(run, tape, init, nsteps=2, hashes=False)
+    assert np.array_equal(mem, cpu.M[:gpu.buffers_end])
+    gpu.close()
+    _fused_vs_oracle(cfg, nsteps=2)
+
+
 def test_aliased_bindings_keep_program_order():
     """A tape may bind one field to several parameters of a dispatch.  Here
     stage_state_reset reads v's source from the u it has just written (va := u), so a

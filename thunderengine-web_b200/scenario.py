@@ -7,7 +7,8 @@ reference computes some base-state values with its own copies of the upstream li
 is judged step by step on identical inputs, so numpy's float32 transcendental
 functions are used.
 
-* Grid layout: halo 3, ``strideJ = nx + 7``, ``strideK = ny + 7``,
+* Grid layout: halo 3, ``strideJ = nx + 7`` (or, with ``align_rows``, rounded up to a
+  multiple of 32 so that every row starts on a 128-byte boundary), ``strideK = ny + 7``,
   ``count = strideJ * strideK * (nz + 1)`` (web/core/grid.js:181-199); arena fields at
   ``n * fieldStride`` with fieldStride = count * 4 rounded up to 256 B
   (grid.js:322-331); ``hmetric`` = 9 strideJ + 3 strideK floats (grid.js:200-214).
@@ -40,12 +41,16 @@ def f(x):
 
 
 class Grid:
-    """Uniform horizontal grid in the reference's arena layout (grid.js:181-199)."""
+    """Uniform horizontal grid in the reference's arena layout (grid.js:181-199).
+    ``align_rows``: the row pitch rounded up to 32 floats (the reference's ``alignRows``
+    option, grid.js:184-191); the padding columns past i = nx + 3 belong to no point."""
 
-    def __init__(self, nx, ny, nz, dx, dy, dz):
+    def __init__(self, nx, ny, nz, dx, dy, dz, align_rows=False):
         self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
         self.dx, self.dy, self.dz = float(dx), float(dy), float(dz)
-        self.strideJ = self.nx + 1 + 2 * HALO
+        self.align_rows = bool(align_rows)
+        raw = self.nx + 1 + 2 * HALO
+        self.strideJ = (raw + 31) // 32 * 32 if self.align_rows else raw
         self.strideK = self.ny + 1 + 2 * HALO
         self.count = self.strideJ * self.strideK * (self.nz + 1)
         self.field_stride = int(math.ceil(self.count * 4 / 256) * 256)
@@ -67,11 +72,14 @@ class Grid:
         v = np.ones(9 * sJ + 3 * sK, dtype=F)
         xf, xh = self.axis(self.nx, self.dx)
         yf, _ = self.axis(self.ny, self.dy)
-        v[2 * sJ + 2 * sK:2 * sJ + 2 * sK + sJ] = xf[:sJ].astype(F)
-        v[3 * sJ + 2 * sK:3 * sJ + 3 * sK] = yf[:sK].astype(F)
+        # each plane takes its axis' values where it has them and keeps 1 beyond
+        # (grid.js:200-214), which matters with aligned rows only
+        x, y, h = xf[:sJ].astype(F), yf[:sK].astype(F), xh[:sJ].astype(F)
+        v[2 * sJ + 2 * sK:2 * sJ + 2 * sK + len(x)] = x
+        v[3 * sJ + 2 * sK:3 * sJ + 2 * sK + len(y)] = y
         base = 3 * sJ + 3 * sK
-        v[base + 4 * sJ:base + 5 * sJ] = 0.0          # rxh: 0 when not axisymmetric
-        v[base + 5 * sJ:base + 6 * sJ] = xh[:sJ].astype(F)
+        v[base + 4 * sJ:base + 4 * sJ + len(x)] = 0.0          # rxh: 0 when not axisymmetric
+        v[base + 5 * sJ:base + 5 * sJ + len(h)] = h
         return v
 
 
@@ -215,8 +223,9 @@ class Config:
     """One synthetic run: grid, time step, acoustic substeps and perturbation."""
 
     def __init__(self, name, nx, ny, nz, dx, dz, dt, nsound, us, steps, amplitude=2.0, noise=0.1, seed=1,
-                 bubbles=None, qv_pbl=0.014):
+                 bubbles=None, qv_pbl=0.014, align_rows=False):
         self.name = name
+        self.align_rows = bool(align_rows)
         self.qv_pbl = float(qv_pbl)
         self.nx, self.ny, self.nz = nx, ny, nz
         self.dx = self.dy = float(dx)
@@ -245,9 +254,9 @@ LARGE = Config('cm1-dyn-1024x1024x100', 1024, 1024, 100, 250.0, 200.0, 1.5, 8, 2
                bubbles=[(0.0, -30000.0), (0.0, 0.0), (0.0, 30000.0)])
 
 
-def tiny(nx=12, ny=10, nz=8, dx=1000.0, dz=500.0, dt=6.0, nsound=6, us=20.0):
+def tiny(nx=12, ny=10, nz=8, dx=1000.0, dz=500.0, dt=6.0, nsound=6, us=20.0, align_rows=False):
     """A few-thousand-point case for fast oracle comparisons."""
-    return Config('cm1-dyn-%dx%dx%d' % (nx, ny, nz), nx, ny, nz, dx, dz, dt, nsound, us, 1)
+    return Config('cm1-dyn-%dx%dx%d' % (nx, ny, nz), nx, ny, nz, dx, dz, dt, nsound, us, 1, align_rows=align_rows)
 
 
 def profiles(cfg, dry=False):
@@ -279,6 +288,7 @@ def fill_arena(cfg, grid, prof, arena, fields):
     """Initial arena (scenario.js:234-296) with bubble + noise, halos periodic."""
     nx, ny, nz = grid.nx, grid.ny, grid.nz
     sJ, sK = grid.strideJ, grid.strideK
+    W = nx + 1 + 2 * HALO   # the columns of points; with aligned rows the rest is padding, left 0
     xf, xh = grid.axis(nx, grid.dx)
     yf, yh = grid.axis(ny, grid.dy)
     vg = prof['vg']
@@ -289,13 +299,13 @@ def fill_arena(cfg, grid, prof, arena, fields):
 
     def view(name):
         off = fields[name] // 4
-        return arena[off:off + grid.count].reshape(nz + 1, sK, sJ)
+        return arena[off:off + grid.count].reshape(nz + 1, sK, sJ)[:, :, :W]
 
     # bubble (+ noise on interior points, then periodic halos)
-    X = xh[None, None, :sJ]
+    X = xh[None, None, :W]
     Y = yh[None, :sK, None]
     Z = vg.zh.astype(np.float64)[:, None, None]
-    tha = np.zeros((nz, sK, sJ), np.float64)
+    tha = np.zeros((nz, sK, W), np.float64)
     for (ox, oy) in cfg.bubbles:
         bx = (X - ox) / 10000.0
         by = (Y - oy) / 10000.0

@@ -214,7 +214,8 @@ class Run:
         self.adaptive = adaptive
         if core and not moist:
             raise ValueError('the dynamics-core step is defined on the moist step')
-        self.grid = sc.Grid(cfg.nx, cfg.ny, cfg.nz, cfg.dx, cfg.dy, cfg.dz)
+        self.grid = sc.Grid(cfg.nx, cfg.ny, cfg.nz, cfg.dx, cfg.dy, cfg.dz,
+                            align_rows=getattr(cfg, 'align_rows', False))
         self.prof = sc.profiles(cfg, dry=not moist)
         self.dt = f(cfg.dt)
         self.schedule = AcousticSchedule(cfg.nsound, self.dt)
