@@ -149,6 +149,14 @@ size_t te_kernel_table_json(char *buf, size_t n);
 /* Region hash of `words` host words with the reference formula (replay.js:407-418). */
 uint32_t te_region_hash_host(const uint32_t *words, uint64_t n);
 
+/* Self-check of the library's own arithmetic (no counterpart in the reference): raises
+ * every binary32 bit pattern in [lo, hi) to the power p by the short binary64 route that
+ * update_rho_prs uses and by the two-float route of the reference's f_rr_pow_cr
+ * (update_rho_prs.wgsl), on the current CUDA device, and returns how many results differ
+ * and the lowest differing pattern (0xffffffff if none).  Synchronous; allocates 16 bytes
+ * of device memory for the counters. */
+int te_check_pow(float p, uint32_t lo, uint32_t hi, uint64_t *mismatches, uint32_t *first_bad);
+
 /* ---- Discrete adjoint of a step (no counterpart in the reference; the forward/backward
  * pair behind a torch.autograd.Function-shaped host interface).  The adjoint memory has
  * the layout of the word memory: the adjoint of the value at word w is the float at word

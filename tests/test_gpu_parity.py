@@ -440,3 +440,17 @@ def test_large_domain_step_fused_equals_exact():
     assert np.abs(w).max() > 0
     for r in reps:
         r.close()
+
+
+def test_fast_power_route_equals_two_float_power_everywhere():
+    """update_rho_prs raises the Exner function to cp/rd by a binary64 route that falls
+    back to the reference's two-float power near rounding boundaries.  On every
+    non-negative binary32 pattern (finite, infinite and NaN included) both routes give the
+    same bits."""
+    from thunderengine_web_b200 import replayer
+    lib = replayer.load_library()
+    cpdrd = float(np.float32(1005.7) / np.float32(287.04))
+    bad = ctypes.c_uint64(0)
+    first = ctypes.c_uint32(0)
+    assert lib.te_check_pow(cpdrd, 0, 0x80000000, ctypes.byref(bad), ctypes.byref(first)) == 0
+    assert bad.value == 0, 'first differing pattern 0x%08x' % first.value

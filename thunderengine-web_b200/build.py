@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, 'csrc')
 LIB = os.path.join(HERE, 'libthunderstep.so')
 SOURCES = ['te_player.cu', 'te_kernels.cu', 'te_kernels_fast.cu', 'te_fused.cu', 'te_static_solve.cu',
-           'te_adjoint.cu', 'te_ensemble.cu']
+           'te_adjoint.cu', 'te_ensemble.cu', 'te_selfcheck.cu']
 NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
 FLAGS = ['-gencode', 'arch=compute_100a,code=sm_100a', '-O3', '-lineinfo', '-std=c++17',
          '-ftz=true', '-prec-div=true', '-prec-sqrt=true', '-fmad=false',

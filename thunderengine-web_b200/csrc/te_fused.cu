@@ -104,6 +104,78 @@ __global__ void __launch_bounds__(256) k_acu_uv(AcuArgs A) {
   }
 }
 
+// Exact unsigned division by a divisor d >= 2 fixed for a launch: q = floor(n * m / 2^64)
+// with m = floor(2^64 / d) + 1 equals floor(n / d) for every n < 2^32 (the error term
+// n (m - 2^64/d) / 2^64 is below 2^-32, less than the distance 1/d from n/d to the
+// next integer).
+struct FastDiv {
+  unsigned long long m;
+  unsigned d;
+};
+static FastDiv fast_div(unsigned d) { return FastDiv{~0ull / d + 1ull, d}; }
+__device__ __forceinline__ unsigned fdiv(unsigned n, const FastDiv& f) { return (unsigned)__umul64hi(n, f.m); }
+
+#ifndef TE_UV_LINEAR
+#define TE_UV_LINEAR 1
+#endif
+// K1 with the points of the field numbered by their linear index c (the field's word
+// offset): thread t takes c = t and c = t + S (S a multiple of 32), so every warp reads and
+// writes whole aligned 128-byte lines of each field; (i, j, k) follow from c by exact
+// division.  Row padding of aligned-row layouts (x > nx + 6) belongs to no point.
+__global__ void __launch_bounds__(256) k_acu_uv_lin(AcuArgs A, FastDiv dJ, FastDiv dK, unsigned S, unsigned total) {
+  const Dims& g = A.g;
+  const unsigned t = blockIdx.x * 256u + threadIdx.x;
+  if (t >= S) return;  // every point is some thread's t or t + S
+  float un[kUvLevels], vn[kUvLevels], ru[kUvLevels], rv[kUvLevels];
+  bool on[kUvLevels], upd[kUvLevels];
+#pragma unroll
+  for (int q = 0; q < kUvLevels; q++) {
+    const unsigned c = t + q * S;
+    const unsigned kk = fdiv(c, dK);                 // level (dK: sJ * sK)
+    const unsigned r = c - kk * dK.d;
+    const unsigned jj = fdiv(r, dJ);                 // row (dJ: sJ)
+    const int x = (int)(r - jj * dJ.d);
+    const int i = x - 3, j = (int)jj - 3, k = (int)kk;
+    on[q] = c < total && x <= g.nx + 6 && j <= g.ny + 3;
+    upd[q] = on[q] && i >= 0 && j >= 0 && i <= g.nx && j <= g.ny && k < g.nz;
+    if (on[q]) {
+      un[q] = upd[q] ? uv_u(A, i, j, (int)c) : A.u[c];
+      vn[q] = upd[q] ? uv_v(A, i, j, (int)c) : A.v[c];
+      ru[q] = A.rru[c];
+      rv[q] = A.rrv[c];
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < kUvLevels; q++) {
+    if (!on[q]) continue;
+    const unsigned c = t + q * S;
+    if (upd[q]) {
+      A.u[c] = un[q];
+      A.v[c] = vn[q];
+    }
+    if (A.tavg > 0.0f) {
+      A.rru[c] = (ru[q] + un[q]) * A.tavg;
+      A.rrv[c] = (rv[q] + vn[q]) * A.tavg;
+    } else {
+      A.rru[c] = ru[q] + un[q];
+      A.rrv[c] = rv[q] + vn[q];
+    }
+  }
+}
+
+static void launch_acu_uv(const AcuArgs& A, cudaStream_t s) {
+  const Dims& g = A.g;
+#if TE_UV_LINEAR
+  const unsigned total = (unsigned)g.sJ * (unsigned)g.sK * (unsigned)(g.nz + 1);
+  const unsigned S = ((total + kUvLevels - 1) / kUvLevels + 31u) / 32u * 32u;
+  launch_kernel(k_acu_uv_lin, dim3((S + 255u) / 256u), dim3(256), 0, s, A, fast_div((unsigned)g.sJ),
+                fast_div((unsigned)g.sJ * (unsigned)g.sK), S, total);
+#else
+  dim3 b(32, 8, 1), gr((g.sJ + 31) / 32, (g.sK + 7) / 8, (g.nz + kUvLevels) / kUvLevels);
+  launch_kernel(k_acu_uv, dim3(gr), dim3(b), 0, s, A);
+#endif
+}
+
 // ------------------------------------------------------------ acoustic K2
 
 // Explicit pi' forcing at an interior point (acoustic_fpk.wgsl:167-207).
@@ -140,11 +212,20 @@ __device__ __forceinline__ float fpk_at(const AcuArgs& A, int i, int j, int c, c
 //
 // Sized for three resident CTAs per SM (416 threads, 52 KB of shared memory at nz = 80):
 // more columns in flight hide the per-pass load latency better than a deeper pass.
+#ifndef TE_COL_LEVELS
+#define TE_COL_LEVELS 12   // worker warps = levels per pass
+#endif
+#ifndef TE_COL_MINB
+#define TE_COL_MINB 3      // resident CTAs per SM the register budget is sized for
+#endif
+#ifndef TE_COL_EPI
+#define TE_COL_EPI 7       // epilogue levels per worker per chunk
+#endif
 constexpr int kColTile = 32;
-constexpr int kLevels = 12;                      // worker warps = levels per pass
+constexpr int kLevels = TE_COL_LEVELS;
 constexpr int kWorkers = kColTile * kLevels;     // 384
 constexpr int kColThreads = kWorkers + kColTile; // + the recurrence warp
-constexpr int kEpiChunk = 7;                     // epilogue levels per worker per chunk
+constexpr int kEpiChunk = TE_COL_EPI;
 
 // [nz][32] cA, cB, s; [2][4][kLevels][32] aa, bb, cc, dd per pass; [2][3][kLevels][32]
 // the exchange store (pk1 + qk, pk2 - qk, pi') per pass
@@ -326,7 +407,7 @@ __device__ __forceinline__ void load_epi(const AcuArgs& A, EpiIn& E, int c0, int
   }
 }
 
-__global__ void __launch_bounds__(kColThreads, 3) k_acu_column(AcuArgs A) {
+__global__ void __launch_bounds__(kColThreads, TE_COL_MINB) k_acu_column(AcuArgs A) {
   extern __shared__ float smem[];
   const Dims& g = A.g;
   const Acoustic& a = A.a;
@@ -1109,10 +1190,7 @@ void FusedStep::launch_segment(Plan& P, std::vector<Op>& ops, int seg, int part)
   } else {
     const AcuArgs& A = D.acu[s.aux[0]];
     const Dims& g = A.g;
-    if (part < 0 || part == 0) {
-      dim3 b(32, 8, 1), gr((g.sJ + 31) / 32, (g.sK + 7) / 8, (g.nz + kUvLevels) / kUvLevels);
-      launch_kernel(k_acu_uv, dim3(gr), dim3(b), 0, P.stream, A);
-    }
+    if (part < 0 || part == 0) launch_acu_uv(A, P.stream);
     if (part < 0 || part == 1) launch_acu_column(A, P.stream);
     if (part < 0 || part == 2) {
       HaloArgs H;

@@ -445,6 +445,47 @@ struct OpVelocityToMassflux {  // velocity_to_massflux as a row-vector op
   }
 };
 
+// Words of one field when the dispatch covers every point of a field (halos and level nz
+// included, TE_WHOLE(k <= nz)) and the layout has no row padding, so that the points are
+// the field's first sJ * sK * (nz + 1) words, in order; 0 otherwise.  Kernels that copy or
+// clear whole fields then walk them as aligned 16-byte vectors (whole 32-byte sectors; the
+// per-point form leaves the sectors at row ends half-written by two warps).
+static unsigned long long whole_field_words(const KArgs& A, const int* fields, int n) {
+  const Dims& g = A.g;
+  const unsigned long long words = (unsigned long long)g.sJ * g.sK * (g.nz + 1);
+  if (!(g.sJ == g.nx + 7 && g.sK == g.ny + 7 && A.gx >= g.nx + 7 && A.gy >= g.ny + 7 && A.gz >= g.nz + 1)) return 0;
+  if (words >= (1ull << 32)) return 0;
+  for (int q = 0; q < n; q++)
+    if ((reinterpret_cast<uintptr_t>(A.p[fields[q]]) & 15) != 0) return 0;
+  return words;
+}
+
+// stage_state_reset over whole fields: dst[n] = src[n] for the five (src, dst) pairs.
+__global__ void k_stage_state_reset_v4(KArgs A, unsigned words) {
+  const unsigned q = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned n4 = words / 4;
+  const float *TE_R s0 = A.p[1], *TE_R s1 = A.p[2], *TE_R s2 = A.p[3], *TE_R s3 = A.p[4], *TE_R s4 = A.p[10];
+  float *TE_R d0 = A.p[5], *TE_R d1 = A.p[6], *TE_R d2 = A.p[7], *TE_R d3 = A.p[8], *TE_R d4 = A.p[9];
+  if (q < n4) {
+    const float4 a = reinterpret_cast<const float4*>(s0)[q], b = reinterpret_cast<const float4*>(s1)[q];
+    const float4 c = reinterpret_cast<const float4*>(s2)[q], d = reinterpret_cast<const float4*>(s3)[q];
+    const float4 e = reinterpret_cast<const float4*>(s4)[q];
+    reinterpret_cast<float4*>(d0)[q] = a;
+    reinterpret_cast<float4*>(d1)[q] = b;
+    reinterpret_cast<float4*>(d2)[q] = c;
+    reinterpret_cast<float4*>(d3)[q] = d;
+    reinterpret_cast<float4*>(d4)[q] = e;
+  }
+  if (q < words - 4 * n4) {
+    const unsigned w = 4 * n4 + q;
+    d0[w] = s0[w];
+    d1[w] = s1[w];
+    d2[w] = s2[w];
+    d3[w] = s3[w];
+    d4[w] = s4[w];
+  }
+}
+
 __global__ void k_stage_state_reset(KArgs A) {
   TE_K3
   const float *TE_R ua = A.p[1], *TE_R va = A.p[2], *TE_R wa = A.p[3], *TE_R ppi = A.p[4];
@@ -457,7 +498,24 @@ __global__ void k_stage_state_reset(KArgs A) {
   pp3d[c] = ppi[c];
   ppd[c] = ppx[c];
 }
-TE_LAUNCH3(stage_state_reset)
+
+static void launch_stage_state_reset(const KArgs& A, cudaStream_t s) {
+  // the vector form loads all five sources before it stores: only for disjoint bindings
+  // (the __restrict__ build), where that order cannot change a result
+  static const int fields[10] = {1, 2, 3, 4, 5, 6, 7, 8, 9, 10};
+#ifdef TE_KERNELS_FAST
+  const unsigned long long words = whole_field_words(A, fields, 10);
+#else
+  const unsigned long long words = 0;
+  (void)fields;
+#endif
+  if (words) {
+    const unsigned n4 = (unsigned)(words / 4);
+    launch_kernel(k_stage_state_reset_v4, dim3((n4 + 255) / 256), dim3(256), 0, s, A, (unsigned)words);
+  } else {
+    launch3(k_stage_state_reset, A, s);
+  }
+}
 
 __global__ void k_stage_tendency_reset(KArgs A) {
   TE_K3
@@ -467,7 +525,35 @@ __global__ void k_stage_tendency_reset(KArgs A) {
   vten[c] = 0.0f;
   wten[c] = 0.0f;
 }
-TE_LAUNCH3(stage_tendency_reset)
+
+// The same zeros over whole fields (whole_field_words): 16-byte stores, then the last
+// words % 4 words one by one.
+__global__ void k_stage_tendency_reset_v4(float* TE_R a, float* TE_R b, float* TE_R c, unsigned words) {
+  const unsigned q = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned n4 = words / 4;
+  if (q < n4) {
+    const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    reinterpret_cast<float4*>(a)[q] = z;
+    reinterpret_cast<float4*>(b)[q] = z;
+    reinterpret_cast<float4*>(c)[q] = z;
+  }
+  if (q < words - 4 * n4) {
+    a[4 * n4 + q] = 0.0f;
+    b[4 * n4 + q] = 0.0f;
+    c[4 * n4 + q] = 0.0f;
+  }
+}
+
+static void launch_stage_tendency_reset(const KArgs& A, cudaStream_t s) {
+  static const int fields[3] = {1, 2, 3};
+  const unsigned long long words = whole_field_words(A, fields, 3);
+  if (words) {
+    const unsigned n4 = (unsigned)(words / 4);
+    launch_kernel(k_stage_tendency_reset_v4, dim3((n4 + 255) / 256), dim3(256), 0, s, A.p[1], A.p[2], A.p[3], (unsigned)words);
+  } else {
+    launch3(k_stage_tendency_reset, A, s);
+  }
+}
 
 __global__ void k_buoyancy_apply(KArgs A) {
   TE_K3
@@ -2471,7 +2557,7 @@ __global__ void k_update_rho_prs(KArgs A) {
   float cpdrd = dcr(1005.7f, 287.04f);
   float pi = pi0[k] + ppp[c];
   float th = th0[k] + thp[c];
-  float p = 1e5f * rr_pow_cr(pi, cpdrd);
+  float p = 1e5f * rr_pow_fast(pi, cpdrd);
   prs[c] = p;
   float rmix = moist != 0 ? fmaf(wmax(0.0f, qv[c]), 461.5f, 287.04f) : 287.04f;
   rho[c] = dcr(p, (th * pi) * rmix);

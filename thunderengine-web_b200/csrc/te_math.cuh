@@ -257,4 +257,35 @@ __device__ __forceinline__ float rr_pow_cr(float x, float p) {
   return rr_exp_ff(quick_two_sum(yh, fmaf(L.y, p, fmaf(L.x, p, -yh))));
 }
 
+// rr_pow_cr(x, p) by a shorter route where the answer is not in doubt.  The reference's
+// two-float power rounds a nearly exact x^p to the nearest binary32; here x^p is formed in
+// binary64 (ln_mantissa above, p log2 x, then 2^t = 2^n e^r with e^r by its Taylor series
+// to r^14; relative error below 2^-46) and rounded to the nearest binary32 f.  Unless that
+// binary64 value lies within 2^-42 (relative) of a rounding boundary of f, both routes
+// round the same real number the same way and give f; near a boundary, and for x outside
+// [2^-6, 2^6) (over all 2^31 patterns with p = cp/rd the two routes differ at 3 inputs,
+// the lowest 0x2e8000db, near 2^-34, where the two-float logarithm works with large
+// magnitudes), rr_pow_cr itself runs.  For the exponents the kernels use, te_check_pow compares the two routes
+// on every binary32 x.
+__device__ __forceinline__ float rr_pow_fast(float x, float p) {
+  if (__float_as_uint(x) - 0x3c800000u >= 0x06000000u) return rr_pow_cr(x, p);  // x outside [2^-6, 2^6)
+  int e;
+  const double lm = ln_mantissa(x, e);
+  const double t = (double)p * ((double)e + lm * 1.4426950408889634);
+  if (!(t > -125.0 && t < 125.0)) return rr_pow_cr(x, p);
+  const double n = rint(t), r = (t - n) * 0.6931471805599453;
+  double q = 1.0;
+#pragma unroll
+  for (int k = 14; k >= 1; k--) q = 1.0 + (r * (1.0 / k)) * q;
+  const double y = q * __longlong_as_double((long long)((int)n + 1023) << 52);
+  const float f = (float)y;
+  const uint32_t fb = __float_as_uint(f);
+  const double fd = (double)f;
+  const double lo = 0.5 * (fd + (double)__uint_as_float(fb - 1u));  // the boundaries of f
+  const double hi = 0.5 * (fd + (double)__uint_as_float(fb + 1u));
+  const double tol = y * 0x1p-42;
+  if (y - lo < tol || hi - y < tol) return rr_pow_cr(x, p);
+  return f;
+}
+
 }  // namespace te

@@ -82,6 +82,8 @@ EXPORTS = {
     'te_destroy': ([ctypes.c_void_p], None),
     'te_last_error': ([ctypes.c_void_p], ctypes.c_char_p),
     'te_region_hash_host': ([ctypes.c_void_p, ctypes.c_uint64], ctypes.c_uint32),
+    'te_check_pow': ([ctypes.c_float, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64),
+                      ctypes.POINTER(ctypes.c_uint32)], ctypes.c_int),
     'te_set_stream': ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     'te_kernel_table_json': ([ctypes.c_char_p, ctypes.c_size_t], ctypes.c_size_t),
     'te_fused_segments': ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
