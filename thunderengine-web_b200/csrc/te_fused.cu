@@ -59,51 +59,6 @@ __device__ __forceinline__ float uv_v(const AcuArgs& A, int i, int j, int c) {
               A.v[c]);
 }
 
-// K1: every point of the field (halos and k = nz included, as acoustic_accumulate):
-// u, v updated where acoustic_uv updates them, then rru += u, rrv += v (averaged on the
-// last substep, acoustic_accumulate.wgsl:129-158).  A thread takes kUvLevels levels of
-// one (i, j) and issues all their loads before its first store (the points are
-// distinct, so nothing it stores is read by it or by another thread).
-constexpr int kUvLevels = 2;
-
-__global__ void __launch_bounds__(256) k_acu_uv(AcuArgs A) {
-  const Dims& g = A.g;
-  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x) - 3;
-  const int j = (int)(blockIdx.y * blockDim.y + threadIdx.y) - 3;
-  const int k0 = blockIdx.z * kUvLevels;
-  if (i > g.nx + 3 || j > g.ny + 3) return;
-  const bool upd = i >= 0 && j >= 0 && i <= g.nx && j <= g.ny;
-  const int sk = g.sJ * g.sK;
-  float un[kUvLevels], vn[kUvLevels], ru[kUvLevels], rv[kUvLevels];
-#pragma unroll
-  for (int q = 0; q < kUvLevels; q++) {
-    const int k = k0 + q;
-    if (k > g.nz) break;
-    const int c = gidx(g, i, j, 0) + k * sk;
-    un[q] = upd && k < g.nz ? uv_u(A, i, j, c) : A.u[c];
-    vn[q] = upd && k < g.nz ? uv_v(A, i, j, c) : A.v[c];
-    ru[q] = A.rru[c];
-    rv[q] = A.rrv[c];
-  }
-#pragma unroll
-  for (int q = 0; q < kUvLevels; q++) {
-    const int k = k0 + q;
-    if (k > g.nz) break;
-    const int c = gidx(g, i, j, 0) + k * sk;
-    if (upd && k < g.nz) {
-      A.u[c] = un[q];
-      A.v[c] = vn[q];
-    }
-    if (A.tavg > 0.0f) {
-      A.rru[c] = (ru[q] + un[q]) * A.tavg;
-      A.rrv[c] = (rv[q] + vn[q]) * A.tavg;
-    } else {
-      A.rru[c] = ru[q] + un[q];
-      A.rrv[c] = rv[q] + vn[q];
-    }
-  }
-}
-
 // Exact unsigned division by a divisor d >= 2 fixed for a launch: q = floor(n * m / 2^64)
 // with m = floor(2^64 / d) + 1 equals floor(n / d) for every n < 2^32 (the error term
 // n (m - 2^64/d) / 2^64 is below 2^-32, less than the distance 1/d from n/d to the
@@ -115,17 +70,25 @@ struct FastDiv {
 static FastDiv fast_div(unsigned d) { return FastDiv{~0ull / d + 1ull, d}; }
 __device__ __forceinline__ unsigned fdiv(unsigned n, const FastDiv& f) { return (unsigned)__umul64hi(n, f.m); }
 
-#ifndef TE_UV_LINEAR
-#define TE_UV_LINEAR 1
+// K1: every point of the field (halos and k = nz included, as acoustic_accumulate):
+// u, v updated where acoustic_uv updates them, then rru += u, rrv += v (averaged on the
+// last substep, acoustic_accumulate.wgsl:129-158).  The points are numbered by their
+// linear index c (the field's word offset) and thread t takes c = t + q S, q < kUvLevels
+// (S a multiple of 32), so every warp reads and writes whole aligned 128-byte lines of
+// each field rather than a row segment straddling two (measured at 256x256x80: 51.5 us
+// per launch against 57.8 us for 32 x 8 blocks of two levels per thread); (i, j, k)
+// follow from c by exact division.  A thread issues all its loads before its first store
+// (the points are distinct, so nothing it stores is read by it or by another thread).
+// Row padding of aligned-row layouts (x > nx + 6) belongs to no point.
+#ifndef TE_UV_POINTS
+#define TE_UV_POINTS 1   // points per thread (2 and 4 measured slower)
 #endif
-// K1 with the points of the field numbered by their linear index c (the field's word
-// offset): thread t takes c = t and c = t + S (S a multiple of 32), so every warp reads and
-// writes whole aligned 128-byte lines of each field; (i, j, k) follow from c by exact
-// division.  Row padding of aligned-row layouts (x > nx + 6) belongs to no point.
+constexpr int kUvLevels = TE_UV_POINTS;
+
 __global__ void __launch_bounds__(256) k_acu_uv_lin(AcuArgs A, FastDiv dJ, FastDiv dK, unsigned S, unsigned total) {
   const Dims& g = A.g;
   const unsigned t = blockIdx.x * 256u + threadIdx.x;
-  if (t >= S) return;  // every point is some thread's t or t + S
+  if (t >= S) return;  // every point is some thread's t + q S
   float un[kUvLevels], vn[kUvLevels], ru[kUvLevels], rv[kUvLevels];
   bool on[kUvLevels], upd[kUvLevels];
 #pragma unroll
@@ -165,15 +128,10 @@ __global__ void __launch_bounds__(256) k_acu_uv_lin(AcuArgs A, FastDiv dJ, FastD
 
 static void launch_acu_uv(const AcuArgs& A, cudaStream_t s) {
   const Dims& g = A.g;
-#if TE_UV_LINEAR
   const unsigned total = (unsigned)g.sJ * (unsigned)g.sK * (unsigned)(g.nz + 1);
   const unsigned S = ((total + kUvLevels - 1) / kUvLevels + 31u) / 32u * 32u;
   launch_kernel(k_acu_uv_lin, dim3((S + 255u) / 256u), dim3(256), 0, s, A, fast_div((unsigned)g.sJ),
                 fast_div((unsigned)g.sJ * (unsigned)g.sK), S, total);
-#else
-  dim3 b(32, 8, 1), gr((g.sJ + 31) / 32, (g.sK + 7) / 8, (g.nz + kUvLevels) / kUvLevels);
-  launch_kernel(k_acu_uv, dim3(gr), dim3(b), 0, s, A);
-#endif
 }
 
 // ------------------------------------------------------------ acoustic K2

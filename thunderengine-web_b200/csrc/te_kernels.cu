@@ -2958,6 +2958,43 @@ struct OpMorrPrep {
   }
 };
 
+#ifdef TE_KERNELS_FAST
+// acoustic_begin over whole fields (whole_field_words): rru = rrv = 0, rrw = beta w, as
+// 16-byte vectors (disjoint bindings only: the vector loads w before any store)
+__global__ void k_acoustic_begin_v4(KArgs A, unsigned words) {
+  const unsigned q = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned n4 = words / 4;
+  const float beta = A.a.beta;
+  const float* TE_R w = A.p[2];
+  float *TE_R ru = A.p[3], *TE_R rv = A.p[4], *TE_R rw = A.p[5];
+  if (q < n4) {
+    const float4 x = reinterpret_cast<const float4*>(w)[q];
+    const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    reinterpret_cast<float4*>(ru)[q] = z;
+    reinterpret_cast<float4*>(rv)[q] = z;
+    reinterpret_cast<float4*>(rw)[q] = make_float4(x.x * beta, x.y * beta, x.z * beta, x.w * beta);
+  }
+  if (q < words - 4 * n4) {
+    const unsigned e = 4 * n4 + q;
+    const float x = w[e];
+    ru[e] = 0.0f;
+    rv[e] = 0.0f;
+    rw[e] = x * beta;
+  }
+}
+
+static void launch_acoustic_begin_whole(const KArgs& A, cudaStream_t s) {
+  static const int fields[4] = {2, 3, 4, 5};
+  const unsigned long long words = whole_field_words(A, fields, 4);
+  if (words) {
+    const unsigned n4 = (unsigned)(words / 4);
+    launch_kernel(k_acoustic_begin_v4, dim3((n4 + 255) / 256), dim3(256), 0, s, A, (unsigned)words);
+  } else {
+    launch_rowvec<OpAcousticBegin>(A, s);
+  }
+}
+#endif
+
 // the __restrict__ build launches the row-vector form where a kernel has one
 #ifdef TE_KERNELS_FAST
 #define TE_ROWVEC(name, op) launch_rowvec<op>
@@ -2998,7 +3035,11 @@ static const KernelSpec kTable[] = {
     {"apply_thterm", 4, {R(0), P(1), P(2), W(3)}, false, TE_ROWVEC(apply_thterm, OpApplyThterm)},
     {"acoustic_prepare", 17, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), W(11), W(12), W(13),
                               W(14), P(24), P(25)}, true, TE_ROWVEC(acoustic_prepare, OpAcousticPrepare)},
-    {"acoustic_begin", 6, {R(0), R(1), P(2), W(3), W(4), W(5)}, true, TE_ROWVEC(acoustic_begin, OpAcousticBegin)},
+#ifdef TE_KERNELS_FAST
+    {"acoustic_begin", 6, {R(0), R(1), P(2), W(3), W(4), W(5)}, true, launch_acoustic_begin_whole},
+#else
+    {"acoustic_begin", 6, {R(0), R(1), P(2), W(3), W(4), W(5)}, true, launch_acoustic_begin},
+#endif
     {"acoustic_uv", 13, {R(0), R(1), P(2), P(3), P(4), P(5), W(6), W(7), R(8), P(30), P(21), P(23), P(25)}, true, launch_acoustic_uv},
     {"acoustic_fpk", 19, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), W(11), P(30), P(15), P(16),
                           P(17), P(24), P(25), R(26)}, true, launch_acoustic_fpk},
