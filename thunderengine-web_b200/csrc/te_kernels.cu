@@ -8,6 +8,7 @@
 // hashes; the fused step kernels (te_fused.cu) are checked against them.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 
 #include "te_flux.cuh"
@@ -445,15 +446,15 @@ struct OpVelocityToMassflux {  // velocity_to_massflux as a row-vector op
   }
 };
 
-// Words of one field when the dispatch covers every point of a field (halos and level nz
-// included, TE_WHOLE(k <= nz)) and the layout has no row padding, so that the points are
-// the field's first sJ * sK * (nz + 1) words, in order; 0 otherwise.  Kernels that copy or
+// Words of one field when the dispatch covers every point of the first `levels` levels of
+// a field, halos included (TE_WHOLE(k < levels)), and the layout has no row padding, so
+// that the points are the field's first sJ * sK * levels words, in order; 0 otherwise.  Kernels that copy or
 // clear whole fields then walk them as aligned 16-byte vectors (whole 32-byte sectors; the
 // per-point form leaves the sectors at row ends half-written by two warps).
-static unsigned long long whole_field_words(const KArgs& A, const int* fields, int n) {
+static unsigned long long whole_field_words(const KArgs& A, const int* fields, int n, int levels) {
   const Dims& g = A.g;
-  const unsigned long long words = (unsigned long long)g.sJ * g.sK * (g.nz + 1);
-  if (!(g.sJ == g.nx + 7 && g.sK == g.ny + 7 && A.gx >= g.nx + 7 && A.gy >= g.ny + 7 && A.gz >= g.nz + 1)) return 0;
+  const unsigned long long words = (unsigned long long)g.sJ * g.sK * levels;
+  if (!(g.sJ == g.nx + 7 && g.sK == g.ny + 7 && A.gx >= g.nx + 7 && A.gy >= g.ny + 7 && A.gz >= levels)) return 0;
   if (words >= (1ull << 32)) return 0;
   for (int q = 0; q < n; q++)
     if ((reinterpret_cast<uintptr_t>(A.p[fields[q]]) & 15) != 0) return 0;
@@ -504,7 +505,7 @@ static void launch_stage_state_reset(const KArgs& A, cudaStream_t s) {
   // (the __restrict__ build), where that order cannot change a result
   static const int fields[10] = {1, 2, 3, 4, 5, 6, 7, 8, 9, 10};
 #ifdef TE_KERNELS_FAST
-  const unsigned long long words = whole_field_words(A, fields, 10);
+  const unsigned long long words = whole_field_words(A, fields, 10, A.g.nz + 1);
 #else
   const unsigned long long words = 0;
   (void)fields;
@@ -546,7 +547,7 @@ __global__ void k_stage_tendency_reset_v4(float* TE_R a, float* TE_R b, float* T
 
 static void launch_stage_tendency_reset(const KArgs& A, cudaStream_t s) {
   static const int fields[3] = {1, 2, 3};
-  const unsigned long long words = whole_field_words(A, fields, 3);
+  const unsigned long long words = whole_field_words(A, fields, 3, A.g.nz + 1);
   if (words) {
     const unsigned n4 = (unsigned)(words / 4);
     launch_kernel(k_stage_tendency_reset_v4, dim3((n4 + 255) / 256), dim3(256), 0, s, A.p[1], A.p[2], A.p[3], (unsigned)words);
@@ -2723,6 +2724,16 @@ struct OpUpdateDiagnosticsMoist {
   }
   static __device__ __forceinline__ void store(const KArgs& A, int tx, int ty, int tz, const In& v) {
     TE_OP_C(3);
+    float o[5];
+    point(A, k, v, o);
+    A.p[15][c] = o[0];
+    A.p[17][c] = o[2];
+    A.p[16][c] = o[1];
+    A.p[18][c] = o[3];
+    A.p[19][c] = o[4];
+  }
+  // thv, ppterm, pi, thterm, buoy (bindings 15..19) of one point at level k
+  static __device__ __forceinline__ void point(const KArgs& A, int k, const In& v, float* o) {
     const float *TE_R th0 = A.p[3], *TE_R pi0 = A.p[4], *TE_R qv0 = A.p[5], *TE_R qc0 = A.p[6];
     const float *TE_R qi0 = A.p[7], *TE_R rth0 = A.p[8];
     const float rd = 287.04f, rv = 461.5f, cp = 1005.7f, cv = 718.66003f, cpv = 1870.0f, cvv = 1408.5f;
@@ -2739,11 +2750,11 @@ struct OpUpdateDiagnosticsMoist {
     float pi = pi0[k] + v.ppp;
     float cpm = fmaf(cpv, qvv, cp) + cpli;
     float cvm = dcr(1.0f, fmaf(cvv, qvv, cv) + cpli);
-    A.p[15][c] = dcr(th * fmaf(reps, qvv, 1.0f), (1.0f + qvv) + qli);
-    A.p[17][c] = pi;
-    A.p[16][c] = ((pi * rovcp) * cpm) * cvm;
-    A.p[18][c] = (th * fmaf(-rovcp, cpm, fmaf(rv, qvv, rd))) * cvm;
-    A.p[19][c] = gacc * (fmaf(v.thp, rth0[k], repsm1 * (qvv - qv0[k])) - ((qli - qc0[k]) - qi0[k]));
+    o[0] = dcr(th * fmaf(reps, qvv, 1.0f), (1.0f + qvv) + qli);
+    o[2] = pi;
+    o[1] = ((pi * rovcp) * cpm) * cvm;
+    o[3] = (th * fmaf(-rovcp, cpm, fmaf(rv, qvv, rd))) * cvm;
+    o[4] = gacc * (fmaf(v.thp, rth0[k], repsm1 * (qvv - qv0[k])) - ((qli - qc0[k]) - qi0[k]));
   }
 };
 
@@ -2959,6 +2970,102 @@ struct OpMorrPrep {
 };
 
 #ifdef TE_KERNELS_FAST
+// update_diagnostics_moist over whole fields (whole_field_words, levels 0..nz-1): the eight
+// inputs and five outputs of four consecutive words as 16-byte vectors, each word's level
+// from its offset; the arithmetic of OpUpdateDiagnosticsMoist::point word by word.
+__global__ void k_update_diagnostics_moist_v4(KArgs A, unsigned words, unsigned sk) {
+  const unsigned q = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned n4 = words / 4;
+  static constexpr int in_f[8] = {1, 2, 9, 10, 11, 12, 13, 14};
+  using Op = OpUpdateDiagnosticsMoist;
+  if (q < n4) {
+    float4 a[8];
+#pragma unroll
+    for (int f = 0; f < 8; f++) a[f] = reinterpret_cast<const float4*>(A.p[in_f[f]])[q];
+    float4 o4[5];
+    const unsigned c0 = 4 * q, k0 = c0 / sk;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const int k = (int)(c0 + e >= (k0 + 1) * sk ? k0 + 1 : k0);
+      const Op::In v{reinterpret_cast<const float*>(&a[0])[e], reinterpret_cast<const float*>(&a[1])[e],
+                     reinterpret_cast<const float*>(&a[2])[e], reinterpret_cast<const float*>(&a[3])[e],
+                     reinterpret_cast<const float*>(&a[4])[e], reinterpret_cast<const float*>(&a[5])[e],
+                     reinterpret_cast<const float*>(&a[6])[e], reinterpret_cast<const float*>(&a[7])[e]};
+      float o[5];
+      Op::point(A, k, v, o);
+#pragma unroll
+      for (int f = 0; f < 5; f++) reinterpret_cast<float*>(&o4[f])[e] = o[f];
+    }
+#pragma unroll
+    for (int f = 0; f < 5; f++) reinterpret_cast<float4*>(A.p[15 + f])[q] = o4[f];
+  }
+  if (q < words - 4 * n4) {
+    const unsigned c = 4 * n4 + q;
+    const Op::In v{A.p[1][c], A.p[2][c], A.p[9][c], A.p[10][c], A.p[11][c], A.p[12][c], A.p[13][c], A.p[14][c]};
+    float o[5];
+    Op::point(A, (int)(c / sk), v, o);
+#pragma unroll
+    for (int f = 0; f < 5; f++) A.p[15 + f][c] = o[f];
+  }
+}
+
+static void launch_update_diagnostics_moist_whole(const KArgs& A, cudaStream_t s) {
+  static const int fields[13] = {1, 2, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19};
+  const unsigned long long words = whole_field_words(A, fields, 13, A.g.nz);
+  if (words) {
+    const unsigned n4 = (unsigned)(words / 4);
+    launch_kernel(k_update_diagnostics_moist_v4, dim3((n4 + 255) / 256), dim3(256), 0, s, A, (unsigned)words,
+                  (unsigned)(A.g.sJ * A.g.sK));
+  } else {
+    launch_rowvec<OpUpdateDiagnosticsMoist>(A, s);
+  }
+}
+
+// massflux_from_state over whole fields: levels 0..nz-1 of rru = rho0 u, rrv = rho0 v,
+// rrw = rf0 w (0 at level 0) as 16-byte vectors, each word's level from its offset; level
+// nz of rrw is 0 (rru, rrv have no level nz and are not written there).
+__global__ void k_massflux_from_state_v4(KArgs A, unsigned words, unsigned sk) {
+  const unsigned q = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned n4 = words / 4;
+  const float *TE_R rho0 = A.p[4], *TE_R rf0 = A.p[5];
+  if (q < n4) {
+    const float4 u = reinterpret_cast<const float4*>(A.p[1])[q], v = reinterpret_cast<const float4*>(A.p[2])[q];
+    const float4 w = reinterpret_cast<const float4*>(A.p[3])[q];
+    float4 ru, rv, rw;
+    const unsigned c0 = 4 * q, k0 = c0 / sk;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const int k = (int)(c0 + e >= (k0 + 1) * sk ? k0 + 1 : k0);
+      reinterpret_cast<float*>(&ru)[e] = rho0[k] * reinterpret_cast<const float*>(&u)[e];
+      reinterpret_cast<float*>(&rv)[e] = rho0[k] * reinterpret_cast<const float*>(&v)[e];
+      reinterpret_cast<float*>(&rw)[e] = k == 0 ? 0.0f : rf0[k] * reinterpret_cast<const float*>(&w)[e];
+    }
+    reinterpret_cast<float4*>(A.p[6])[q] = ru;
+    reinterpret_cast<float4*>(A.p[7])[q] = rv;
+    reinterpret_cast<float4*>(A.p[8])[q] = rw;
+  }
+  if (q < words - 4 * n4) {
+    const unsigned c = 4 * n4 + q;
+    const int k = (int)(c / sk);
+    A.p[6][c] = rho0[k] * A.p[1][c];
+    A.p[7][c] = rho0[k] * A.p[2][c];
+    A.p[8][c] = k == 0 ? 0.0f : rf0[k] * A.p[3][c];
+  }
+  if (q < sk) A.p[8][words + q] = 0.0f;
+}
+
+static void launch_massflux_from_state_whole(const KArgs& A, cudaStream_t s) {
+  static const int fields[6] = {1, 2, 3, 6, 7, 8};
+  const unsigned long long all = whole_field_words(A, fields, 6, A.g.nz + 1);
+  if (all) {
+    const unsigned sk = (unsigned)(A.g.sJ * A.g.sK), words = (unsigned)(all - sk);
+    const unsigned n = std::max(words / 4, sk);
+    launch_kernel(k_massflux_from_state_v4, dim3((n + 255) / 256), dim3(256), 0, s, A, words, sk);
+  } else {
+    launch_rowvec<OpMassfluxFromState>(A, s);
+  }
+}
+
 // acoustic_begin over whole fields (whole_field_words): rru = rrv = 0, rrw = beta w, as
 // 16-byte vectors (disjoint bindings only: the vector loads w before any store)
 __global__ void k_acoustic_begin_v4(KArgs A, unsigned words) {
@@ -2985,7 +3092,7 @@ __global__ void k_acoustic_begin_v4(KArgs A, unsigned words) {
 
 static void launch_acoustic_begin_whole(const KArgs& A, cudaStream_t s) {
   static const int fields[4] = {2, 3, 4, 5};
-  const unsigned long long words = whole_field_words(A, fields, 4);
+  const unsigned long long words = whole_field_words(A, fields, 4, A.g.nz + 1);
   if (words) {
     const unsigned n4 = (unsigned)(words / 4);
     launch_kernel(k_acoustic_begin_v4, dim3((n4 + 255) / 256), dim3(256), 0, s, A, (unsigned)words);
@@ -3025,7 +3132,11 @@ static const KernelSpec kTable[] = {
     {"pdef_apply", 18, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), P(11), P(12), P(13), R(14),
                         R(15), W(16), P(30)}, false, launch_pdef_apply},
     {"build_sadv", 4, {R(0), P(1), P(2), W(3)}, false, TE_ROWVEC(build_sadv, OpBuildSadv)},
-    {"massflux_from_state", 10, {R(0), P(1), P(2), P(3), P(4), P(5), W(6), W(7), W(8), P(24)}, false, TE_ROWVEC(massflux_from_state, OpMassfluxFromState)},
+#ifdef TE_KERNELS_FAST
+    {"massflux_from_state", 10, {R(0), P(1), P(2), P(3), P(4), P(5), W(6), W(7), W(8), P(24)}, false, launch_massflux_from_state_whole},
+#else
+    {"massflux_from_state", 10, {R(0), P(1), P(2), P(3), P(4), P(5), W(6), W(7), W(8), P(24)}, false, launch_massflux_from_state},
+#endif
     {"div_massflux", 8, {R(0), P(1), P(2), P(3), P(4), W(5), P(30), P(25)}, false, TE_ROWVEC(div_massflux, OpDivMassflux)},
     {"velocity_to_massflux", 7, {R(0), P(1), P(2), W(3), W(4), W(5), P(24)}, false,
      TE_ROWVEC(velocity_to_massflux, OpVelocityToMassflux)},
@@ -3088,8 +3199,13 @@ static const KernelSpec kTable[] = {
     {"morr_post", 10, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), W(7), W(8), W(9)}, false, launch_morr_post},
     {"update_diagnostics", 10, {R(0), P(1), P(2), P(3), P(4), W(5), W(6), W(7), P(8), W(9)}, false, launch_update_diagnostics},
     {"stability_max", 11, {R(0), {1, kRefS, 0}, P(2), P(3), P(4), P(5), P(6), P(7), P(8), W(9), P(30)}, false, launch_stability_max},
+#ifdef TE_KERNELS_FAST
     {"update_diagnostics_moist", 20, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), P(11), P(12),
-                                      P(13), P(14), W(15), W(16), W(17), W(18), W(19)}, false, TE_ROWVEC(update_diagnostics_moist, OpUpdateDiagnosticsMoist)},
+                                      P(13), P(14), W(15), W(16), W(17), W(18), W(19)}, false, launch_update_diagnostics_moist_whole},
+#else
+    {"update_diagnostics_moist", 20, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), P(11), P(12),
+                                      P(13), P(14), W(15), W(16), W(17), W(18), W(19)}, false, launch_update_diagnostics_moist},
+#endif
     {"pressure_tendency", 15, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), R(9), R(10), R(12), P(13), R(14), W(11)},
      false, launch_pressure_tendency},
     {"divergence3d", 7, {R(0), P(1), P(2), P(3), P(4), W(5), P(30)}, false, TE_ROWVEC(divergence3d, OpDivergence3d)},
