@@ -317,8 +317,9 @@ def test_aliased_bindings_keep_program_order():
 
 def test_fused_plan_covers_the_step():
     """The fused planner recognises every acoustic substep, the advection of every variable
-    except the stage-3 scalar WENO (whose fluxes pdef_dum reads) and the halo-fill runs;
-    a structural change that made it fall back to per-dispatch kernels shows here."""
+    (the stage-3 scalar WENO one storing the fluxes pdef_dum and pdef_apply read) and the
+    halo-fill runs; a structural change that made it fall back to per-dispatch kernels
+    shows here."""
     from thunderengine_web_b200.replayer import TE_MODE_FUSED
     run = timestep.Run(scenario.tiny(37, 29, 13, dx=500.0, dz=250.0, dt=3.0, nsound=8, us=25.0))
     tape = run.tape(1)
@@ -326,7 +327,7 @@ def test_fused_plan_covers_the_step():
     segs = gpu.fused_segments()
     kinds = [s[0] for s in segs]
     assert kinds.count(1) == sum(n for n, _ in run.schedule.loops)   # every acoustic substep (15)
-    assert kinds.count(3) == 14
+    assert kinds.count(3) == 15
     assert kinds.count(2) >= 10
     exact_ops = sum(s[2] - s[1] + 1 for s in segs if s[0] == 0)
     assert exact_ops < gpu.num_ops // 3

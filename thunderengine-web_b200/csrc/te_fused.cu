@@ -588,7 +588,9 @@ static bool same_acoustic(const Acoustic& a, const Acoustic& b) {
 // Advection of one variable (timestep.js:1629-1900): the three face-flux dispatches and
 // adv_assemble, optionally followed by apply_thterm and rk_update, as one kernel.  The
 // per-face arithmetic is face_* of te_flux.cuh and the assembly assemble_t, i.e. the
-// per-dispatch kernels' own code; the fx, fy, fz fields are neither written nor read.
+// per-dispatch kernels' own code; the fx, fy, fz fields are never read, and written only
+// where a later op of the step reads them (then every face the flux dispatches write is
+// stored once, by the tile that computes it).
 enum FaceKind { kLin = 0, kStag, kWeno, kWenoUV, kWenoW };
 
 struct AdvArgs {
@@ -601,6 +603,7 @@ struct AdvArgs {
   const float* phiA;                 // rk_update (null if not fused)
   float* phi;
   float dttmp;
+  float *fxo, *fyo, *fzo;            // flux outputs when a later op reads them (else null)
 };
 
 // Face (i, j, k) of direction DIR whose linear index c on the common grid g is known.
@@ -702,13 +705,33 @@ __device__ __forceinline__ void adv_tile(const AdvArgs& A, float (*fxs)[kAdvTY][
       if (A.phi) pa = A.phiA[c];
     }
     const int ko = k * sk;
-    if (FULL || in_range(A.rx, i0 + dx + xq, j0 + xr, k)) fxs[b][xr][xq] = adv_face<KIND, 0, ST>(A.fx, g, cx0 + ko, k);
-    if (FULL || in_range(A.ry, i, j0 + dy + ly, k)) fys[b][ly][lx] = adv_face<KIND, 1, ST>(A.fy, g, cy0 + ko, k);
-    if (ly == 0 && lx < kAdvTY && (FULL || in_range(A.rx, i0 + dx + xq2, j0 + xr2, k)))
-      fxs[b][xr2][xq2] = adv_face<KIND, 0, ST>(A.fx, g, cx20 + ko, k);
-    if (ly == 1 && (FULL || in_range(A.ry, i, j0 + dy + kAdvTY, k)))
-      fys[b][kAdvTY][lx] = adv_face<KIND, 1, ST>(A.fy, g, cy20 + ko, k);
+    // a tile stores the faces it shares with the next tile only when there is none
+    const bool last_x = i0 + kAdvTX > A.ihi, last_y = j0 + kAdvTY > A.jhi;
+    if (FULL || in_range(A.rx, i0 + dx + xq, j0 + xr, k)) {
+      const float f = adv_face<KIND, 0, ST>(A.fx, g, cx0 + ko, k);
+      fxs[b][xr][xq] = f;
+      if (A.fxo && (xq < kAdvTX || last_x)) A.fxo[cx0 + ko] = f;
+    }
+    if (FULL || in_range(A.ry, i, j0 + dy + ly, k)) {
+      const float f = adv_face<KIND, 1, ST>(A.fy, g, cy0 + ko, k);
+      fys[b][ly][lx] = f;
+      if (A.fyo) A.fyo[cy0 + ko] = f;
+    }
+    if (ly == 0 && lx < kAdvTY && (FULL || in_range(A.rx, i0 + dx + xq2, j0 + xr2, k))) {
+      const float f = adv_face<KIND, 0, ST>(A.fx, g, cx20 + ko, k);
+      fxs[b][xr2][xq2] = f;
+      if (A.fxo && (xq2 < kAdvTX || last_x)) A.fxo[cx20 + ko] = f;
+    }
+    if (ly == 1 && (FULL || in_range(A.ry, i, j0 + dy + kAdvTY, k))) {
+      const float f = adv_face<KIND, 1, ST>(A.fy, g, cy20 + ko, k);
+      fys[b][kAdvTY][lx] = f;
+      if (A.fyo && last_y) A.fyo[cy20 + ko] = f;
+    }
     const float fzt = cell ? adv_face<KIND, 2, ST>(A.fz, g, c + (dz + 1) * sk, k + dz + 1) : 0.0f;
+    if (A.fzo && cell) {
+      A.fzo[c + (dz + 1) * sk] = fzt;
+      if (k == A.klo) A.fzo[c + dz * sk] = fzb;  // the lowest face of the column
+    }
     __syncthreads();
     if (cell) {
       const float dFx = fxs[b][ly][lx + 1] - fxs[b][ly][lx];
@@ -954,8 +977,32 @@ static bool match_advect(const std::vector<Op>& ops, size_t i, uint32_t* M, Fuse
     if (A.thterm && !A.phi) return false;  // apply_thterm only together with its rk_update
     if (A.phi) A.write_dest = dead_after(ops, (int)i, last, A.dest, M) ? 0 : 1;
   }
-  for (float* f : {fx, fy, fz})
-    if (!dead_after(ops, (int)i, last, f, M)) return false;
+  bool live = false;
+  for (float* f : {fx, fy, fz}) live |= !dead_after(ops, (int)i, last, f, M);
+  if (live) {
+    // a later op reads the fluxes: the kernel stores them, which is the flux dispatches'
+    // result only if they write exactly the faces the tiles compute and read none of them
+    if (!(A.rx.ilo == A.ilo + dx && A.rx.ihi == A.ihi + dx + 1 && A.rx.jlo == A.jlo && A.rx.jhi == A.jhi &&
+          A.rx.klo == A.klo && A.rx.khi == A.khi))
+      return false;
+    if (!(A.ry.ilo == A.ilo && A.ry.ihi == A.ihi && A.ry.jlo == A.jlo + dy && A.ry.jhi == A.jhi + dy + 1 &&
+          A.ry.klo == A.klo && A.ry.khi == A.khi))
+      return false;
+    if (!(A.rz.ilo == A.ilo && A.rz.ihi == A.ihi && A.rz.jlo == A.jlo && A.rz.jhi == A.jhi &&
+          A.rz.klo == A.klo + dz && A.rz.khi == A.khi + dz + 1))
+      return false;
+    for (float* f : {fx, fy, fz}) {
+      for (int b = 0; b < kMaxBind; b++) {
+        if ((b != fs->out_h && A.fx.p[b] == f) || (b != fs->out_h && A.fy.p[b] == f) || (b != fs->out_z && A.fz.p[b] == f))
+          return false;
+        if (b != 3 && b != 4 && b != 5 && b != 11 && b != 19 && A.as.p[b] == f) return false;
+      }
+      if (f == A.dest || f == A.phi || f == A.phiA || f == A.div3d || f == A.thterm) return false;
+    }
+    A.fxo = fx;
+    A.fyo = fy;
+    A.fzo = fz;
+  }
   s.kind = kAdvect;
   s.first = (int)i;
   s.last = last;

@@ -3066,6 +3066,39 @@ static void launch_massflux_from_state_whole(const KArgs& A, cudaStream_t s) {
   }
 }
 
+// build_sadv over whole fields (levels 0..nz-1): sadv = (th0[k] - 300) + th', 16-byte vectors
+__global__ void k_build_sadv_v4(KArgs A, unsigned words, unsigned sk) {
+  const unsigned q = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned n4 = words / 4;
+  const float* TE_R th0 = A.p[1];
+  if (q < n4) {
+    const float4 t = reinterpret_cast<const float4*>(A.p[2])[q];
+    float4 o;
+    const unsigned c0 = 4 * q, k0 = c0 / sk;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const int k = (int)(c0 + e >= (k0 + 1) * sk ? k0 + 1 : k0);
+      reinterpret_cast<float*>(&o)[e] = (th0[k] - 300.0f) + reinterpret_cast<const float*>(&t)[e];
+    }
+    reinterpret_cast<float4*>(A.p[3])[q] = o;
+  }
+  if (q < words - 4 * n4) {
+    const unsigned c = 4 * n4 + q;
+    A.p[3][c] = (th0[c / sk] - 300.0f) + A.p[2][c];
+  }
+}
+
+static void launch_build_sadv_whole(const KArgs& A, cudaStream_t s) {
+  static const int fields[2] = {2, 3};
+  const unsigned long long words = whole_field_words(A, fields, 2, A.g.nz);
+  if (words) {
+    const unsigned n4 = (unsigned)(words / 4);
+    launch_kernel(k_build_sadv_v4, dim3((n4 + 255) / 256), dim3(256), 0, s, A, (unsigned)words, (unsigned)(A.g.sJ * A.g.sK));
+  } else {
+    launch_rowvec<OpBuildSadv>(A, s);
+  }
+}
+
 // acoustic_begin over whole fields (whole_field_words): rru = rrv = 0, rrw = beta w, as
 // 16-byte vectors (disjoint bindings only: the vector loads w before any store)
 __global__ void k_acoustic_begin_v4(KArgs A, unsigned words) {
@@ -3131,7 +3164,11 @@ static const KernelSpec kTable[] = {
     {"pdef_dum", 12, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), P(7), R(8), R(9), W(10), P(30)}, false, TE_ROWVEC(pdef_dum, OpPdefDum)},
     {"pdef_apply", 18, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), P(11), P(12), P(13), R(14),
                         R(15), W(16), P(30)}, false, launch_pdef_apply},
-    {"build_sadv", 4, {R(0), P(1), P(2), W(3)}, false, TE_ROWVEC(build_sadv, OpBuildSadv)},
+#ifdef TE_KERNELS_FAST
+    {"build_sadv", 4, {R(0), P(1), P(2), W(3)}, false, launch_build_sadv_whole},
+#else
+    {"build_sadv", 4, {R(0), P(1), P(2), W(3)}, false, launch_build_sadv},
+#endif
 #ifdef TE_KERNELS_FAST
     {"massflux_from_state", 10, {R(0), P(1), P(2), P(3), P(4), P(5), W(6), W(7), W(8), P(24)}, false, launch_massflux_from_state_whole},
 #else
