@@ -43,12 +43,13 @@ def test_kernel_table_is_the_reference_abi():
     lib.te_kernel_table_json(buf, n + 1)
     table = json.loads(buf.value.decode())
     ref = helpers.kernels_meta()
-    assert len(table) == 82
+    assert len(table) == 83
     for name, k in table.items():
         want = [(p['index'], p['kind'], bool(p['write'])) for p in ref[name]['params']]
         got = [(p['index'], p['kind'], bool(p['write'])) for p in k['params']]
         assert got == want, name
-        assert ref[name]['scratch'] == 0
+        # per-thread scratch: only the Morrison column has some (its per-column arrays)
+        assert ref[name]['scratch'] == (3712 if name == 'morr_column' else 0), name
 
 
 def test_oracle_declares_the_same_kernels():
@@ -59,6 +60,9 @@ def test_oracle_declares_the_same_kernels():
     table = json.loads(buf.value.decode())
     o = helpers.oracle()
     for name in table:
+        if name == 'morr_column':
+            # checked against the reference's own kernel (tests/test_morr.py)
+            continue
         assert o.has(name), name
 
 

@@ -114,10 +114,11 @@ GOLDEN_SCENARIOS = {'single_cell': True, 'squall_line': True, 'supercell_stretch
 
 @pytest.mark.parametrize('scen', list(GOLDEN_SCENARIOS))
 def test_golden_in_scope_dispatches(scen):
-    """A recorded step 1: every dispatch with a CUDA kernel runs on the GPU (the others on
-    the CPU reference build), its region hashes equal to the oracle's; where the oracle
-    reproduces the recording, region hashes and buffer FNVs are also compared with the
-    recording (scratch tend/fpk hashes exempt, as the reference documents)."""
+    """A recorded step 1, dispatch by dispatch: every dispatch runs on the GPU from the
+    CPU's memory, its region hashes equal to the oracle's (the reference's own kernel for
+    the Morrison column, with the WGSL builtins in binary64); where the oracle reproduces
+    the recording, region hashes and buffer FNVs are also compared with the recording
+    (scratch tend/fpk hashes exempt, as the reference documents)."""
     ref = helpers.reference()
     if ref is None:
         pytest.skip('oracle/_ref not built')
@@ -137,6 +138,11 @@ def test_golden_in_scope_dispatches(scen):
     lib.te_kernel_table_json(buf, n + 1)
     import json
     ours = set(json.loads(buf.value.decode()))
+    ref64 = helpers.reference64()
+
+    def cpu_kernel(name):
+        return ref64.get(name) if name == 'morr_column' else helpers.oracle().get(name)
+
     # CPU replay; before every in-scope dispatch, hand the GPU the regions written since
     ngpu = 0
     gpu_hashes = {}
@@ -158,7 +164,7 @@ def test_golden_in_scope_dispatches(scen):
                 gpu_hashes[slot] = int(h[slot])
             ngpu += 1
             # the CPU continues with the oracle so the two memories stay identical
-            cpu.run(helpers.oracle().get, with_hashes=True, ops=[o])
+            cpu.run(cpu_kernel, with_hashes=True, ops=[o])
             for slot, off, ln in o.hashes:
                 assert gpu_hashes[slot] == int(cpu.hashes[slot]), (oi, o.name)
         else:
@@ -167,8 +173,8 @@ def test_golden_in_scope_dispatches(scen):
                 dirty.append((o.dst, o.n))
             else:
                 dirty.extend((off, ln) for _, off, ln in o.hashes if off is not None and ln)
-    # every dispatch but the Morrison microphysics column (morr_column)
-    assert ngpu == sum(1 for o in cpu.ops if o.kind == 'k') - 1
+    # every dispatch, the Morrison microphysics column (morr_column) included
+    assert ngpu == sum(1 for o in cpu.ops if o.kind == 'k')
     if not GOLDEN_SCENARIOS[scen]:
         return
     fields = {v // 4 + cpu.base[2]: k for k, v in tape['fields'].items()}
@@ -455,3 +461,34 @@ def test_fast_power_route_equals_two_float_power_everywhere():
     first = ctypes.c_uint32(0)
     assert lib.te_check_pow(cpdrd, 0, 0x80000000, ctypes.byref(bad), ctypes.byref(first)) == 0
     assert bad.value == 0, 'first differing pattern 0x%08x' % first.value
+
+
+@pytest.mark.parametrize('scen', [k for k, v in GOLDEN_SCENARIOS.items() if v])
+def test_recorded_step_plays_whole_on_the_gpu(scen):
+    """The reference's recorded step 1 (full physics: turbulence, Morrison microphysics,
+    open boundaries, mass conservation) played as one te_run on the GPU, every dispatch on
+    the device: every buffer's FNV-1a equals the recording's, and every region hash but the
+    scratch tendencies the reference itself exempts (tend, fpk)."""
+    from oracle.player import CpuPlayer, fnv1a
+    tape, init, want, step1 = helpers.load_golden_scenario(scen)
+    km = helpers.kernels_meta()
+    from thunderengine_web_b200.replayer import Replayer
+    # the tape's diagnostics list (encodeDiag, not part of the step) names the radar
+    # reflectivity kernel morr_refl10cm, which this library does not build
+    gpu = Replayer(tape, km, defer_missing=True)
+    gpu.plan(True)
+    gpu.build()
+    for i, b in init.items():
+        gpu.upload(i, b)
+    gpu.encode_steps(1, with_hashes=True)
+    got = gpu.read_hashes()
+    mem = gpu.read(gpu.buffers_end)
+    cpu = CpuPlayer(tape, km)
+    cpu.plan(True)
+    fields = {v // 4 + cpu.base[2]: k for k, v in tape['fields'].items()}
+    slot_field = {s: fields.get(off) for o in cpu.ops if o.kind == 'k' for s, off, _ in o.hashes}
+    bad = np.nonzero(got[:want.size] != want)[0]
+    assert {slot_field[int(s)] for s in bad} <= {'tend', 'fpk'}
+    for b in tape['buffers']:
+        off = gpu.base[b['id']]
+        assert fnv1a(mem[off:off + b['length'] // 4]) == step1[b['id']], b['label']

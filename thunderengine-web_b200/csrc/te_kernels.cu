@@ -15,6 +15,22 @@
 #include "te_kernels.cuh"
 #include "te_math.cuh"
 
+// The Morrison column's arithmetic on the device (te_morr.cuh): WGSL builtins evaluated in
+// binary64 and rounded once, like every other kernel here (te_math.cuh).
+#define TE_MORR_HD __device__ __forceinline__
+namespace te {
+__device__ __forceinline__ float morr_div(float a, float b) { return dcr(a, b); }
+__device__ __forceinline__ float morr_min(float a, float b) { return wmin(a, b); }
+__device__ __forceinline__ float morr_max(float a, float b) { return wmax(a, b); }
+__device__ __forceinline__ float morr_pow(float x, float y) { return pow_f64(x, y); }
+__device__ __forceinline__ float morr_exp(float x) { return exp_f64(x); }
+__device__ __forceinline__ float morr_log(float x) { return log_f64(x); }
+// WGSL sin: only the gamma function's reflection for non-positive arguments reaches it,
+// and no caller passes one; CUDA's sinf.
+__device__ __forceinline__ float morr_sin(float x) { return sinf(x); }
+}  // namespace te
+#include "te_morr.cuh"
+
 // TE_R qualifies every field pointer a kernel takes from its bindings.  Built as is it
 // is empty; te_kernels_fast.cu compiles this file again with TE_R = __restrict__ into
 // te::fast, which the player uses for ops whose bound regions do not overlap (the
@@ -2356,6 +2372,55 @@ __global__ void k_morr_prep(KArgs A) {
 }
 TE_LAUNCH3(morr_prep)
 
+// morr_column.wgsl: one thread per column (te_morr.cuh morr::column), the dispatch's rows
+// taken scr_rows at a time (the reference's y tiles: the planned per-thread scratch holds
+// that many rows); each launch lays the scratch out by array, level, then column of the
+// tile, so the threads of a warp touch consecutive words.
+__global__ void __launch_bounds__(128) k_morr_column(KArgs A, int y0, int rows) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int ncol = A.gx * rows;
+  if (t >= ncol) return;
+  const int i = t % A.gx, j = y0 + t / A.gx;
+  if (j >= A.gy) return;
+  morr::Params p;
+  {
+    uint32_t* w = reinterpret_cast<uint32_t*>(&p);
+    for (int q = 0; q < (int)(sizeof(morr::Params) / 4); q++) w[q] = A.ref0[q];
+  }
+  if (i >= p.nx || j >= p.ny) return;
+  morr::Fields F;
+  F.T3 = A.p[1];
+  F.QV = A.p[2];
+  F.QC = A.p[3];
+  F.QR = A.p[4];
+  F.QI = A.p[5];
+  F.QS = A.p[6];
+  F.QG = A.p[7];
+  F.NI = A.p[8];
+  F.NS = A.p[9];
+  F.NR = A.p[10];
+  F.NG = A.p[11];
+  F.P3 = A.p[12];
+  F.RH3 = A.p[13];
+  F.DZQ = A.p[14];
+  F.sfc = A.p[15];
+  F.EFFC = A.p[16];
+  F.EFFI = A.p[17];
+  F.EFFS = A.p[18];
+  const morr::Scratch S{A.scr + t, (unsigned)ncol, p.nz};
+  morr::column(p, F, S, i, j, A.iv[19]);
+}
+
+// (nz <= 128 and a one-level dispatch grid are checked at plan time, Plan::finalize_args)
+static void launch_morr_column(const KArgs& A, cudaStream_t s) {
+  const int rows = A.scr_rows > 0 ? (int)A.scr_rows : A.gy;
+  for (int y0 = 0; y0 < A.gy; y0 += rows) {
+    const int r = std::min(rows, A.gy - y0);
+    const int ncol = A.gx * r;
+    launch_kernel(k_morr_column, dim3((ncol + 127) / 128), dim3(128), 0, s, A, y0, r);
+  }
+}
+
 // morr_post.wgsl: where the column changed T (by >= 1e-4) or qv (by >= 1e-14), pressure
 // from the equation of state, pi' from it (the reference's correctly rounded pow) and th
 __global__ void k_morr_post(KArgs A) {
@@ -3233,6 +3298,8 @@ static const KernelSpec kTable[] = {
     {"mass_reference_init", 3, {R(0), P(1), W(2)}, false, launch_mass_reference_init},
     {"mass_correction_apply", 13, {R(0), R(1), P(2), P(3), P(4), P(5), W(6), P(7), P(8), P(9), W(10), W(11), W(12)}, false, launch_mass_correction_apply},
     {"morr_prep", 8, {R(0), P(1), P(2), P(3), P(4), P(5), W(6), W(7)}, false, TE_ROWVEC(morr_prep, OpMorrPrep)},
+    {"morr_column", 20, {R(0), W(1), W(2), W(3), W(4), W(5), W(6), W(7), W(8), W(9), W(10), W(11), P(12), P(13), P(14),
+                         W(15), W(16), W(17), W(18), R(19)}, false, launch_morr_column},
     {"morr_post", 10, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), W(7), W(8), W(9)}, false, launch_morr_post},
     {"update_diagnostics", 10, {R(0), P(1), P(2), P(3), P(4), W(5), W(6), W(7), P(8), W(9)}, false, launch_update_diagnostics},
     {"stability_max", 11, {R(0), {1, kRefS, 0}, P(2), P(3), P(4), P(5), P(6), P(7), P(8), W(9), P(30)}, false, launch_stability_max},

@@ -23,6 +23,9 @@ struct KArgs {
   int iv2[kMaxBind];
   float sw[2][8];  // the first 8 words of the kernel's first and second struct bindings (kRefS)
   short bx, by;    // thread-block shape of the generic launchers (0: 32 x 4), set by te_autotune
+  const uint32_t* ref0;  // device address of binding 0's words (a kernel's parameter struct)
+  float* scr;            // the planned per-thread kernel scratch (kernels with scratch)
+  unsigned scr_rows;     // dispatch rows that share that scratch per launch (the reference's y tile)
 };
 
 // Thread-block shape of a generic launch: the op's tuned shape, else 32 x 4.

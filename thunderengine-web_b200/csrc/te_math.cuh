@@ -17,7 +17,15 @@ namespace te {
 // quotient in the normal range and the plain quotient for zero, huge, NaN and tiny
 // results; with an IEEE divider and flushed subnormals both cases are the IEEE
 // quotient, and the 2^64 pre-scaling of tiny numerators cancels exactly.
-__device__ __forceinline__ float dcr(float a, float b) { return a / b; }
+// The divisor passes through an empty asm so that the compiler cannot see a constant
+// there: with -prec-div=true nvcc still turns x / c for a compile-time constant c into a
+// multiplication by 1/c, which is not the correctly rounded quotient (measured on B200:
+// x / 3.0f differed from the IEEE quotient for 33 % of 2^20 random x, x / 6e-05f for 64 %;
+// a divisor only known at run time gave the IEEE quotient every time).
+__device__ __forceinline__ float dcr(float a, float b) {
+  asm("" : "+f"(b));
+  return a / b;
+}
 
 // WGSL min/max on f32: min(a,b) = b if b < a else a; max(a,b) = b if a < b else a;
 // a NaN operand yields the other one (fixes the sign of zero on +0/-0 ties).

@@ -213,6 +213,7 @@ std::vector<Op> Plan::build_ops(const JValue& cmds, const std::map<int, uint64_t
         tileY = std::max<uint64_t>(o.tg[1], (kScratchCap / row / o.tg[1]) * o.tg[1]);
       }
       scratch_need = std::max<uint64_t>(scratch_need, km->second.scratch * o.grid[0] * o.grid[2] * tileY);
+      o.tile_y = tileY;
       o.bind = bind;
       if (hashes) {
         for (auto& p : km->second.params) {
@@ -301,6 +302,9 @@ void Plan::finalize_args(std::vector<Op>& ops) {
     auto it0 = o.bind.find(0);
     if (it0 == o.bind.end()) throw ApiError(TE_EINVAL, o.name + ": GridDims (binding 0) not bound");
     uint64_t gd = it0->second;
+    A.ref0 = M + gd;
+    A.scr = reinterpret_cast<float*>(M + scratch_base);
+    A.scr_rows = (unsigned)std::min<uint64_t>(o.tile_y, 0xffffffffu);
     A.g.nx = (int)word(gd + 0);
     A.g.ny = (int)word(gd + 1);
     A.g.nz = (int)word(gd + 2);
@@ -350,6 +354,10 @@ void Plan::finalize_args(std::vector<Op>& ops) {
         }
       }
     }
+    // morr_column keeps 29 per-column arrays of nz levels in the scratch the reference sizes
+    // for 128 levels (3712 words per thread), one thread per column
+    if (o.name == "morr_column" && (A.g.nz < 1 || A.g.nz > 128 || o.grid[2] != 1 || !o.tile_y))
+      throw ApiError(TE_EINVAL, o.name + ": needs 1 <= nz <= 128 and a one-level dispatch grid");
     // turb_zero writes up to level nz + 1 of its binding (its own range check): the
     // highest word the dispatch grid reaches must lie in the planned memory
     if (o.name == "turb_zero" && A.p[1]) {

@@ -31,6 +31,7 @@ struct Op {
   std::vector<HashReq> hashes;
   KArgs args;
   short tile[2] = {0, 0};  // thread-block shape chosen by te_autotune (0: the launcher's default)
+  uint64_t tile_y = 0;     // dispatch rows per scratch tile (replay.js:104-108)
 };
 
 struct Step {
