@@ -673,6 +673,32 @@ static napi_value region_hash(napi_env env, napi_callback_info info) {
   return v;
 }
 
+/* checkPow(p, lo, hi) -> {mismatches, firstBad}: the library's self-check of its two
+ * routes to x^p over the binary32 patterns [lo, hi) (te_check_pow) */
+static napi_value check_pow(napi_env env, napi_callback_info info) {
+  size_t argc = 3;
+  napi_value argv[3], out, v;
+  NAPI_CALL(env, napi_get_cb_info(env, info, &argc, argv, NULL, NULL));
+  double p = 0;
+  uint32_t lo = 0, hi = 0;
+  napi_get_value_double(env, argv[0], &p);
+  napi_get_value_uint32(env, argv[1], &lo);
+  napi_get_value_uint32(env, argv[2], &hi);
+  uint64_t bad = 0;
+  uint32_t first = 0;
+  int rc = te_check_pow((float)p, lo, hi, &bad, &first);
+  if (rc != TE_OK) {
+    napi_throw_error(env, NULL, "te_check_pow failed");
+    return NULL;
+  }
+  napi_create_object(env, &out);
+  napi_create_double(env, (double)bad, &v);
+  napi_set_named_property(env, out, "mismatches", v);
+  napi_create_uint32(env, first, &v);
+  napi_set_named_property(env, out, "firstBad", v);
+  return out;
+}
+
 static napi_value init(napi_env env, napi_value exports) {
   napi_property_descriptor player_methods[] = {
       {"plan", NULL, player_plan, NULL, NULL, NULL, napi_default, NULL},
@@ -716,6 +742,8 @@ static napi_value init(napi_env env, napi_value exports) {
   NAPI_CALL(env, napi_set_named_property(env, exports, "kernelTable", v));
   NAPI_CALL(env, napi_create_function(env, "regionHash", NAPI_AUTO_LENGTH, region_hash, NULL, &v));
   NAPI_CALL(env, napi_set_named_property(env, exports, "regionHash", v));
+  NAPI_CALL(env, napi_create_function(env, "checkPow", NAPI_AUTO_LENGTH, check_pow, NULL, &v));
+  NAPI_CALL(env, napi_set_named_property(env, exports, "checkPow", v));
   return exports;
 }
 
