@@ -634,8 +634,8 @@ constexpr int kAdvTX = 32, kAdvTY = 8;
 // 33 x 8 x-faces and 32 x 9 y-faces of the tile are computed once into shared memory
 // (double-buffered, one barrier per level; the faces beyond 256 by warps 0 and 1), and
 // each cell computes the z-face above it, reusing the one below from the level before.
-// KZ = 4 where the z-face is a WENO reconstruction (momentum WENO: the saved face pays
-// for the shorter grid); KZ = 1 (most parallel) where faces are cheap.  Every index is
+// KZ = 4 where the z-face is a WENO reconstruction of momentum (the saved face pays for
+// the shorter grid), 2 for scalar WENO; KZ = 1 (most parallel) where faces are cheap.  Every index is
 // formed once per thread on the assembly's grid (the four dispatches share it) and
 // advanced by a level stride; a tile whose faces and cells all lie inside the dispatch
 // ranges (all but the edge tiles) skips the per-face range tests.
@@ -643,7 +643,7 @@ constexpr int kAdvTX = 32, kAdvTY = 8;
 #define TE_ADV_KZ_FAST 1   // levels per CTA, linear and staggered-linear kinds
 #endif
 #ifndef TE_ADV_KZ_WENO
-#define TE_ADV_KZ_WENO 1   // levels per CTA, scalar WENO
+#define TE_ADV_KZ_WENO 2   // levels per CTA, scalar WENO (158 -> 155 us per launch against 1)
 #endif
 #ifndef TE_ADV_KZ_WENO_MOM
 #define TE_ADV_KZ_WENO_MOM 4   // levels per CTA, momentum WENO
