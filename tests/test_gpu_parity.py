@@ -492,3 +492,35 @@ def test_recorded_step_plays_whole_on_the_gpu(scen):
     for b in tape['buffers']:
         off = gpu.base[b['id']]
         assert fnv1a(mem[off:off + b['length'] // 4]) == step1[b['id']], b['label']
+
+
+def test_recorded_step_in_fused_mode_equals_exact():
+    """The single_cell recording (open lateral boundaries, full physics) in fused mode: the
+    planner fuses the advection of every variable there (with adv_assemble's open-edge
+    branches) and runs the rest per dispatch; after one step every field but the step
+    scratch equals the exact-mode step, word for word."""
+    from thunderengine_web_b200.replayer import Replayer, TE_MODE_FUSED
+    tape, init, _, _ = helpers.load_golden_scenario('single_cell')
+    km = helpers.kernels_meta()
+    mems = []
+    for mode in (0, TE_MODE_FUSED):
+        r = Replayer(tape, km, defer_missing=True)
+        r.plan(False)
+        r.build()
+        for i, b in init.items():
+            r.upload(i, b)
+        r.set_mode(mode)
+        if mode:
+            segs = r.fused_segments()
+            assert sum(1 for s in segs if s[0] == 3) >= 10   # the advection phases are fused
+        r.encode_steps(1)
+        mems.append(r.read(r.buffers_end))
+        base = r.base[2]
+        r.close()
+    for name, off in tape['fields'].items():
+        if name in STEP_SCRATCH:
+            continue
+        n = (tape['nx'] + 7) * (tape['ny'] + 7) * (tape['nz'] + 1)
+        a = mems[0][base + off // 4:base + off // 4 + n]
+        b = mems[1][base + off // 4:base + off // 4 + n]
+        assert np.array_equal(a, b), name

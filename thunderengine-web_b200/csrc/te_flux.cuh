@@ -361,18 +361,19 @@ __device__ __forceinline__ float assemble_core(const KArgs& A, int i, int j, int
   return dcr(fmaf(sc, dv, -divF), rho);
 }
 
-// adv_assemble (adv_assemble.wgsl:139-279) at cell (i, j, k) from the flux differences:
-// returns the advective tendency t (before the accumulate/store).
-__device__ __forceinline__ float assemble_t(const KArgs& A, int i, int j, int k, int c, float dFx, float dFy, float dFz) {
+// The open lateral boundary branches of adv_assemble (adv_assemble.wgsl:139-279): at a cell
+// on an open edge whose boundary face is an inflow face, the face flux is dropped and the
+// divergence term loses the boundary piece.  Cells off the open edges are left alone.
+template <int SG = 0>
+__device__ __forceinline__ void assemble_open(const KArgs& A, int i, int j, int k, int c, float& dFx, float& dFy,
+                                              float& dv) {
   const Dims& g = A.g;
-  const int stag = A.iv[1];
-  const float *s = A.p[2], *divx = A.p[6];
+  const int stag = SG ? SG : A.iv[1];
   const float *rru = A.p[13], *rrv = A.p[14], *c1 = A.p[15], *c2 = A.p[16];
   const int openx = A.iv[17], openy = A.iv2[17];
   const float* hm = A.p[30];
   const int sj = g.sJ, sk = g.sJ * g.sK;
   const int st = stag < 0 ? -stag : stag;
-  float dv = assemble_dv(A, k, divx[c], divx[c - assemble_dv_off(A)]);
   if (openx != 0 && st != 2) {
     bool west = i == 0, east = i == g.nx - 1;
     if (west || east) {
@@ -421,6 +422,14 @@ __device__ __forceinline__ float assemble_t(const KArgs& A, int i, int j, int k,
       }
     }
   }
+}
+
+// adv_assemble (adv_assemble.wgsl:139-279) at cell (i, j, k) from the flux differences:
+// returns the advective tendency t (before the accumulate/store).
+__device__ __forceinline__ float assemble_t(const KArgs& A, int i, int j, int k, int c, float dFx, float dFy, float dFz) {
+  const float *s = A.p[2], *divx = A.p[6];
+  float dv = assemble_dv(A, k, divx[c], divx[c - assemble_dv_off(A)]);
+  assemble_open(A, i, j, k, c, dFx, dFy, dv);
   return assemble_core(A, i, j, k, s[c], dv, dFx, dFy, dFz);
 }
 

@@ -598,6 +598,7 @@ struct AdvArgs {
   int ilo, ihi, jlo, jhi, klo, khi;  // cells adv_assemble writes
   FaceRange rx, ry, rz;              // faces each flux dispatch produces
   int accumulate, write_dest;
+  int open;                          // the tape has open lateral edges (adv_assemble's branches)
   float* dest;                       // adv_assemble's tendency output
   const float *div3d, *thterm;       // apply_thterm (null if not fused)
   const float* phiA;                 // rk_update (null if not fused)
@@ -670,7 +671,7 @@ struct AdvMinBlocks {
                                                                : TE_ADV_MINB_WENO_MOM;
 };
 
-template <int KIND, int ST, bool FULL>
+template <int KIND, int ST, bool FULL, bool OPEN>
 __device__ __forceinline__ void adv_tile(const AdvArgs& A, float (*fxs)[kAdvTY][kAdvTX + 1], float (*fys)[kAdvTY + 1][kAdvTX]) {
   constexpr int kAdvKZ = AdvKZ<KIND>::value;
   constexpr int dx = ST == 2 ? -1 : 0, dy = ST == 3 ? -1 : 0, dz = ST == 4 ? -1 : 0;
@@ -733,12 +734,20 @@ __device__ __forceinline__ void adv_tile(const AdvArgs& A, float (*fxs)[kAdvTY][
       if (k == A.klo) A.fzo[c + dz * sk] = fzb;  // the lowest face of the column
     }
     __syncthreads();
-    if (cell) {
+    // adv_assemble leaves the boundary faces of u (v) on an open x (y) edge alone: no
+    // tendency there; a fused rk_update uses the tendency the field already holds
+    const bool edge = !OPEN ? false
+                    : ST == 2 ? A.as.iv[17] != 0 && (i == 0 || i == g.nx)
+                    : ST == 3 ? A.as.iv2[17] != 0 && (j == 0 || j == g.ny) : false;
+    if (cell && edge) {
+      if (!A.accumulate && A.phi) A.phi[c] = fmaf(A.dttmp, A.dest[c], pa);   // rk_update.wgsl
+    } else if (cell) {
       const float dFx = fxs[b][ly][lx + 1] - fxs[b][ly][lx];
       const float dFy = fys[b][ly + 1][lx] - fys[b][ly][lx];
-      // adv_assemble without its open-boundary branches (the planner fuses closed and
-      // periodic boundaries only)
-      float tn = assemble_core<ST>(A.as, i, j, k, sc, assemble_dv<ST>(A.as, k, d0, d1), dFx, dFy, fzt - fzb);
+      // adv_assemble, with its open-boundary branches where the tape has open edges
+      float dv = assemble_dv<ST>(A.as, k, d0, d1), gx = dFx, gy = dFy;
+      if (OPEN) assemble_open<ST>(A.as, i, j, k, c, gx, gy, dv);
+      float tn = assemble_core<ST>(A.as, i, j, k, sc, dv, gx, gy, fzt - fzb);
       if (A.accumulate) {
         A.dest[c] = dst + tn;
       } else {
@@ -751,7 +760,8 @@ __device__ __forceinline__ void adv_tile(const AdvArgs& A, float (*fxs)[kAdvTY][
   }
 }
 
-template <int KIND, int ST>
+// OPEN: the tape has open lateral edges (adv_assemble's open branches compiled in)
+template <int KIND, int ST, bool OPEN>
 __global__ void __launch_bounds__(kAdvTX* kAdvTY, AdvMinBlocks<KIND>::value) k_adv_fused(AdvArgs A) {
   constexpr int kAdvKZ = AdvKZ<KIND>::value;
   constexpr int dx = ST == 2 ? -1 : 0, dy = ST == 3 ? -1 : 0, dz = ST == 4 ? -1 : 0;
@@ -763,9 +773,9 @@ __global__ void __launch_bounds__(kAdvTX* kAdvTY, AdvMinBlocks<KIND>::value) k_a
   const bool full = i1 <= A.ihi && j1 <= A.jhi && box_in(A.rx, i0 + dx, i1 + dx + 1, j0, j1, kb, ke) &&
                     box_in(A.ry, i0, i1, j0 + dy, j1 + dy + 1, kb, ke) && box_in(A.rz, i0, i1, j0, j1, kb + dz, ke + dz + 1);
   if (full)
-    adv_tile<KIND, ST, true>(A, fxs, fys);
+    adv_tile<KIND, ST, true, OPEN>(A, fxs, fys);
   else
-    adv_tile<KIND, ST, false>(A, fxs, fys);
+    adv_tile<KIND, ST, false, OPEN>(A, fxs, fys);
 }
 
 template <int KIND, int ST>
@@ -773,7 +783,10 @@ static void launch_adv_t(const AdvArgs& A, cudaStream_t s) {
   const dim3 b(kAdvTX, kAdvTY, 1);
   constexpr int kz = AdvKZ<KIND>::value;
   const dim3 gr((A.ihi - A.ilo + kAdvTX) / kAdvTX, (A.jhi - A.jlo + kAdvTY) / kAdvTY, (A.khi - A.klo + kz) / kz);
-  launch_kernel(k_adv_fused<KIND, ST>, dim3(gr), dim3(b), 0, s, A);
+  if (A.open)
+    launch_kernel(k_adv_fused<KIND, ST, true>, dim3(gr), dim3(b), 0, s, A);
+  else
+    launch_kernel(k_adv_fused<KIND, ST, false>, dim3(gr), dim3(b), 0, s, A);
 }
 
 static void launch_adv(const AdvArgs& A, int kind, int st, cudaStream_t s) {
@@ -900,7 +913,6 @@ static bool match_advect(const std::vector<Op>& ops, size_t i, uint32_t* M, Fuse
   const Dims& g = oa.args.g;
   if (!same_dims(g, ox.args.g) || !same_dims(g, oy.args.g) || !same_dims(g, oz.args.g)) return false;
   if (g.nz < 3) return false;
-  if (oa.args.iv[17] != 0 || oa.args.iv2[17] != 0) return false;  // periodic / closed lateral boundaries
   const int stag = oa.args.iv[1];
   if (stag < 1 || stag > 4) return false;
   if ((fs->kind == kLin || fs->kind == kWeno) && stag != 1) return false;
@@ -934,6 +946,7 @@ static bool match_advect(const std::vector<Op>& ops, size_t i, uint32_t* M, Fuse
   if (!covers(A.ry, A.ilo, A.ihi, A.jlo + dy, A.jhi + dy + 1, A.klo, A.khi)) return false;
   if (!covers(A.rz, A.ilo, A.ihi, A.jlo, A.jhi, A.klo + dz, A.khi + dz + 1)) return false;
   A.accumulate = oa.args.iv[12] != 0;
+  A.open = oa.args.iv[17] != 0 || oa.args.iv2[17] != 0;
   A.dest = oa.args.p[11];
   A.write_dest = 1;
   // fields the kernel reads at other cells than the one it writes: nothing it writes may
