@@ -2039,6 +2039,43 @@ float te_log_f64(float x) {
   double lm = ln_mantissa(x, &e);
   return (float)((double)e * 0.6931471805599453 + lm);
 }
+/* log2 x = e + ln(m) / ln 2 from the same ln(m); atan2 in binary64: octant reduction to
+ * a = min/max in [0, 1], atan a = pi/6 + atan((a sqrt3 - 1) / (a + sqrt3)) above
+ * tan(pi/12), the odd power series to u^29, then the octant and the sign of y (zeros and
+ * infinities as C's atan2f).  WGSL leaves both precisions to the implementation; these are
+ * the CUDA kernels' (te_math.cuh log2_f64, atan2_f64), operation for operation. */
+float te_log2_f64(float x) {
+  if (x != x || x < 0.0f) return NAN;
+  if (x == 0.0f) return -INFINITY;
+  if (x == INFINITY) return INFINITY;
+  int e;
+  double lm = ln_mantissa(x, &e);
+  return (float)((double)e + lm * 1.4426950408889634);
+}
+float te_atan2_f64(float y, float x) {
+  if (x != x || y != y) return x + y;
+  double ax = fabs((double)x), ay = fabs((double)y), r;
+  int neg = (int)(fbits(y) >> 31), xneg = (int)(fbits(x) >> 31);
+  if (ax == INFINITY && ay == INFINITY) {
+    r = xneg ? 2.356194490192345 : 0.7853981633974483;
+  } else if (ax == 0.0 && ay == 0.0) {
+    r = xneg ? 3.141592653589793 : 0.0;
+  } else {
+    int swap = ay > ax;
+    double a = swap ? ax / ay : ay / ax, u = a, base = 0.0;
+    if (a > 0.2679491924311227) {
+      u = (a * 1.7320508075688772 - 1.0) / (a + 1.7320508075688772);
+      base = 0.5235987755982988;
+    }
+    double w = -(u * u), p = 1.0 / 29;
+    for (int k = 27; k >= 1; k -= 2) p = p * w + 1.0 / k;
+    r = base + u * p;
+    if (swap) r = 1.5707963267948966 - r;
+    if (xneg) r = 3.141592653589793 - r;
+  }
+  float f = (float)r;
+  return neg ? -f : f;
+}
 #endif /* !TE_ORACLE_F64 */
 
 void teor_turb_km_kh(uint32_t *M, const uint32_t *ARG) {

@@ -30,6 +30,8 @@ float te_rr_pow_cr(float x, float p);
 float te_pow_f64(float x, float y);
 float te_exp_f64(float x);
 float te_log_f64(float x);
+float te_log2_f64(float x);
+float te_atan2_f64(float y, float x);
 
 #define TE_ORACLE_KERNELS(X) \
   X(adv_flux_x) X(adv_flux_y) X(adv_flux_z) \

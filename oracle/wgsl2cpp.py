@@ -85,23 +85,27 @@ static inline f32 W_floor(f32 a) { return floorf(a); }
 static inline f32 W_round(f32 a) { return nearbyintf(a); }
 static inline f32 W_trunc(f32 a) { return truncf(a); }
 #ifdef TE_REF_F64_BUILTINS
-// WGSL leaves the precision of exp/log/pow to the implementation: this variant evaluates
-// them like the CUDA kernels (binary64, rounded once; oracle.c te_*_f64)
+// WGSL leaves the precision of exp/log/pow/log2/atan2 to the implementation: this variant
+// evaluates them like the CUDA kernels (binary64, rounded once; oracle.c te_*_f64)
 extern "C" float te_exp_f64(float x);
 extern "C" float te_log_f64(float x);
 extern "C" float te_pow_f64(float x, float y);
+extern "C" float te_log2_f64(float x);
+extern "C" float te_atan2_f64(float y, float x);
 static inline f32 W_exp(f32 a) { return te_exp_f64(a); }
 static inline f32 W_log(f32 a) { return te_log_f64(a); }
 static inline f32 W_pow(f32 a, f32 b) { return te_pow_f64(a, b); }
+static inline f32 W_log2(f32 a) { return te_log2_f64(a); }
+static inline f32 W_atan2(f32 a, f32 b) { return te_atan2_f64(a, b); }
 #else
 static inline f32 W_exp(f32 a) { return expf(a); }
 static inline f32 W_log(f32 a) { return logf(a); }
 static inline f32 W_pow(f32 a, f32 b) { return powf(a, b); }
-#endif
 static inline f32 W_log2(f32 a) { return log2f(a); }
+static inline f32 W_atan2(f32 a, f32 b) { return atan2f(a, b); }
+#endif
 static inline f32 W_sin(f32 a) { return sinf(a); }
 static inline f32 W_atan(f32 a) { return atanf(a); }
-static inline f32 W_atan2(f32 a, f32 b) { return atan2f(a, b); }
 static inline f32 W_length(vec2<f32> v) { return sqrtf(v.x * v.x + v.y * v.y); }
 static inline f32 W_length(vec3<f32> v) { return sqrtf(v.x * v.x + v.y * v.y + v.z * v.z); }
 static inline f32 W_dot(vec2<f32> a, vec2<f32> b) { return a.x * b.x + a.y * b.y; }

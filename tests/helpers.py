@@ -52,7 +52,7 @@ def kernels_meta():
 
 
 def reference64():
-    """The reference's kernels that call WGSL exp/log/pow, with those evaluated in binary64
+    """The reference's kernels that call WGSL exp/log/pow/log2/atan2, with those evaluated in binary64
     like the CUDA kernels (oracle/_ref/libteref64.so), or None."""
     global _REF64
     if _REF64 is None:

@@ -43,13 +43,14 @@ def test_kernel_table_is_the_reference_abi():
     lib.te_kernel_table_json(buf, n + 1)
     table = json.loads(buf.value.decode())
     ref = helpers.kernels_meta()
-    assert len(table) == 83
+    assert len(table) == 84
     for name, k in table.items():
         want = [(p['index'], p['kind'], bool(p['write'])) for p in ref[name]['params']]
         got = [(p['index'], p['kind'], bool(p['write'])) for p in k['params']]
         assert got == want, name
-        # per-thread scratch: only the Morrison column has some (its per-column arrays)
-        assert ref[name]['scratch'] == (3712 if name == 'morr_column' else 0), name
+        # per-thread scratch: only the Morrison column and its reflectivity diagnostic have
+        # some (their per-column arrays)
+        assert ref[name]['scratch'] == {'morr_column': 3712, 'morr_refl10cm': 1408}.get(name, 0), name
 
 
 def test_oracle_declares_the_same_kernels():
@@ -60,8 +61,8 @@ def test_oracle_declares_the_same_kernels():
     table = json.loads(buf.value.decode())
     o = helpers.oracle()
     for name in table:
-        if name == 'morr_column':
-            # checked against the reference's own kernel (tests/test_morr.py)
+        if name in ('morr_column', 'morr_refl10cm'):
+            # checked against the reference's own kernels (tests/test_morr.py)
             continue
         assert o.has(name), name
 

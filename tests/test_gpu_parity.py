@@ -147,7 +147,7 @@ def test_golden_in_scope_dispatches(scen):
     ngpu = 0
     gpu_hashes = {}
     from thunderengine_web_b200.replayer import Replayer
-    r = Replayer(tape, km, defer_missing=True)
+    r = Replayer(tape, km)
     r.plan(True)
     r.build()
     assert r.mem_words == cpu.mem_words and r.hash_count == want.size
@@ -202,7 +202,7 @@ def test_branches_the_recording_does_not_take():
     cpu.plan(False)
     for i, b in init.items():
         cpu.upload(i, b)
-    r = Replayer(tape, km, defer_missing=True)
+    r = Replayer(tape, km)
     r.plan(False)
     r.build()
     cmds0 = tape['steps'][0]
@@ -468,14 +468,13 @@ def test_recorded_step_plays_whole_on_the_gpu(scen):
     """The reference's recorded step 1 (full physics: turbulence, Morrison microphysics,
     open boundaries, mass conservation) played as one te_run on the GPU, every dispatch on
     the device: every buffer's FNV-1a equals the recording's, and every region hash but the
-    scratch tendencies the reference itself exempts (tend, fpk)."""
+    scratch tendencies the reference itself exempts (tend, fpk); then the tape's display
+    diagnostic (radar reflectivity) equals the reference's kernels on the CPU."""
     from oracle.player import CpuPlayer, fnv1a
     tape, init, want, step1 = helpers.load_golden_scenario(scen)
     km = helpers.kernels_meta()
     from thunderengine_web_b200.replayer import Replayer
-    # the tape's diagnostics list (encodeDiag, not part of the step) names the radar
-    # reflectivity kernel morr_refl10cm, which this library does not build
-    gpu = Replayer(tape, km, defer_missing=True)
+    gpu = Replayer(tape, km)
     gpu.plan(True)
     gpu.build()
     for i, b in init.items():
@@ -492,6 +491,18 @@ def test_recorded_step_plays_whole_on_the_gpu(scen):
     for b in tape['buffers']:
         off = gpu.base[b['id']]
         assert fnv1a(mem[off:off + b['length'] // 4]) == step1[b['id']], b['label']
+    # the display diagnostic after the step (encodeDiag: morr_prep, morr_refl10cm) equals
+    # the reference's kernels run on the CPU from the same memory
+    gpu.encode_diag()
+    dmem = gpu.read(gpu.buffers_end)
+    gpu.close()
+    cpu.M[:gpu.buffers_end] = mem
+    ref64 = helpers.reference64()
+    if ref64 is None:
+        pytest.skip('oracle/_ref not built (needs the reference checkout)')
+    cpu.run(lambda n: ref64.get(n) if n == 'morr_refl10cm' else helpers.oracle().get(n), ops=cpu.diag_ops)
+    assert np.count_nonzero(dmem != mem) > 0
+    assert np.array_equal(dmem, cpu.M[:gpu.buffers_end])
 
 
 def test_recorded_step_in_fused_mode_equals_exact():
@@ -504,7 +515,7 @@ def test_recorded_step_in_fused_mode_equals_exact():
     km = helpers.kernels_meta()
     mems = []
     for mode in (0, TE_MODE_FUSED):
-        r = Replayer(tape, km, defer_missing=True)
+        r = Replayer(tape, km)
         r.plan(False)
         r.build()
         for i, b in init.items():

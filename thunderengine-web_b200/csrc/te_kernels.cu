@@ -28,8 +28,14 @@ __device__ __forceinline__ float morr_log(float x) { return log_f64(x); }
 // WGSL sin: only the gamma function's reflection for non-positive arguments reaches it,
 // and no caller passes one; CUDA's sinf.
 __device__ __forceinline__ float morr_sin(float x) { return sinf(x); }
+// The reflectivity column's (te_refl.cuh): the correctly rounded square root and the
+// binary64 log2 and atan2.
+__device__ __forceinline__ float morr_sqrt(float x) { return __fsqrt_rn(x); }
+__device__ __forceinline__ float morr_log2(float x) { return log2_f64(x); }
+__device__ __forceinline__ float morr_atan2(float y, float x) { return atan2_f64(y, x); }
 }  // namespace te
 #include "te_morr.cuh"
+#include "te_refl.cuh"
 
 // TE_R qualifies every field pointer a kernel takes from its bindings.  Built as is it
 // is empty; te_kernels_fast.cu compiles this file again with TE_R = __restrict__ into
@@ -2421,6 +2427,55 @@ static void launch_morr_column(const KArgs& A, cudaStream_t s) {
   }
 }
 
+// morr_refl10cm.wgsl: one thread per column (te_refl.cuh morr::refl_column), the
+// dispatch's rows taken scr_rows at a time like morr_column, the 11 per-level arrays in the
+// planned scratch laid out by array, level, then column of the tile.
+__global__ void __launch_bounds__(128) k_morr_refl10cm(KArgs A, int y0, int rows) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int ncol = A.gx * rows;
+  if (t >= ncol) return;
+  const int i = t % A.gx, j = y0 + t / A.gx;
+  if (j >= A.gy) return;
+  morr::Params p;
+  {
+    uint32_t* w = reinterpret_cast<uint32_t*>(&p);
+    for (int q = 0; q < (int)(sizeof(morr::Params) / 4); q++) w[q] = A.ref0[q];
+  }
+  if (i >= p.nx || j >= p.ny) return;
+  morr::RadarHead h;
+  {
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(A.p[1]);
+    uint32_t* w = reinterpret_cast<uint32_t*>(&h);
+    for (int q = 0; q < (int)(sizeof(morr::RadarHead) / 4); q++) w[q] = src[q];
+  }
+  morr::RadarFields F;
+  F.bs = A.p[2];
+  F.bg = A.p[3];
+  F.simpson = A.p[4];
+  F.T = A.p[5];
+  F.QR = A.p[6];
+  F.QS = A.p[7];
+  F.QG = A.p[8];
+  F.NR = A.p[9];
+  F.NS = A.p[10];
+  F.NG = A.p[11];
+  F.RH = A.p[12];
+  F.dbz = A.p[13];
+  const morr::Scratch S{A.scr + t, (unsigned)ncol, p.nz};
+  morr::refl_column(p, h, F, S, i, j);
+}
+
+// (nz <= 128, a one-level dispatch grid and bound head, bins and weights are checked at
+// plan time, Plan::finalize_args)
+static void launch_morr_refl10cm(const KArgs& A, cudaStream_t s) {
+  const int rows = A.scr_rows > 0 ? (int)A.scr_rows : A.gy;
+  for (int y0 = 0; y0 < A.gy; y0 += rows) {
+    const int r = std::min(rows, A.gy - y0);
+    const int ncol = A.gx * r;
+    launch_kernel(k_morr_refl10cm, dim3((ncol + 127) / 128), dim3(128), 0, s, A, y0, r);
+  }
+}
+
 // morr_post.wgsl: where the column changed T (by >= 1e-4) or qv (by >= 1e-14), pressure
 // from the equation of state, pi' from it (the reference's correctly rounded pow) and th
 __global__ void k_morr_post(KArgs A) {
@@ -3300,6 +3355,8 @@ static const KernelSpec kTable[] = {
     {"morr_prep", 8, {R(0), P(1), P(2), P(3), P(4), P(5), W(6), W(7)}, false, TE_ROWVEC(morr_prep, OpMorrPrep)},
     {"morr_column", 20, {R(0), W(1), W(2), W(3), W(4), W(5), W(6), W(7), W(8), W(9), W(10), W(11), P(12), P(13), P(14),
                          W(15), W(16), W(17), W(18), R(19)}, false, launch_morr_column},
+    {"morr_refl10cm", 14, {R(0), R(1), P(2), P(3), P(4), P(5), P(6), P(7), P(8), P(9), P(10), P(11), P(12), W(13)},
+     false, launch_morr_refl10cm},
     {"morr_post", 10, {R(0), P(1), P(2), P(3), P(4), P(5), P(6), W(7), W(8), W(9)}, false, launch_morr_post},
     {"update_diagnostics", 10, {R(0), P(1), P(2), P(3), P(4), W(5), W(6), W(7), P(8), W(9)}, false, launch_update_diagnostics},
     {"stability_max", 11, {R(0), {1, kRefS, 0}, P(2), P(3), P(4), P(5), P(6), P(7), P(8), W(9), P(30)}, false, launch_stability_max},

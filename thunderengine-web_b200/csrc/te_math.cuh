@@ -83,6 +83,48 @@ __device__ __forceinline__ float log_f64(float x) {
   const double lm = ln_mantissa(x, e);
   return (float)((double)e * 0.6931471805599453 + lm);
 }
+// log2 x = e + ln(m) / ln 2, from the same ln(m).
+__device__ __forceinline__ float log2_f64(float x) {
+  if (x != x || x < 0.0f) return NAN;
+  if (x == 0.0f) return -INFINITY;
+  if (x == INFINITY) return INFINITY;
+  int e;
+  const double lm = ln_mantissa(x, e);
+  return (float)((double)e + lm * 1.4426950408889634);
+}
+// atan2(y, x) in binary64: a = min(|x|,|y|) / max(|x|,|y|) in [0, 1]; above tan(pi/12)
+// atan a = pi/6 + atan((a sqrt3 - 1) / (a + sqrt3)), which leaves |u| <= tan(pi/12);
+// atan u by its odd power series to u^29 (|u|^30 / 31 < 2^-57); then the octant
+// (pi/2 - r where |y| > |x|, pi - r where x < 0) and the sign of y.  Zeros and infinities
+// follow C's atan2f.
+__device__ __forceinline__ float atan2_f64(float y, float x) {
+  if (x != x || y != y) return x + y;
+  const double ax = fabs((double)x), ay = fabs((double)y);
+  const bool neg = __float_as_uint(y) >> 31, xneg = __float_as_uint(x) >> 31;
+  double r;
+  if (ax == INFINITY && ay == INFINITY) {
+    r = xneg ? 2.356194490192345 : 0.7853981633974483;
+  } else if (ax == 0.0 && ay == 0.0) {
+    r = xneg ? 3.141592653589793 : 0.0;
+  } else {
+    const bool swap = ay > ax;
+    const double a = swap ? ax / ay : ay / ax;
+    double u = a, base = 0.0;
+    if (a > 0.2679491924311227) {
+      u = (a * 1.7320508075688772 - 1.0) / (a + 1.7320508075688772);
+      base = 0.5235987755982988;
+    }
+    const double w = -(u * u);
+    double p = 1.0 / 29;
+#pragma unroll
+    for (int k = 27; k >= 1; k -= 2) p = p * w + 1.0 / k;
+    r = base + u * p;
+    if (swap) r = 1.5707963267948966 - r;
+    if (xneg) r = 3.141592653589793 - r;
+  }
+  const float f = (float)r;
+  return neg ? -f : f;
+}
 
 // Quotients of constants, rounded once (the reference writes e.g. div_cr(13.0, 12.0)).
 #define TE_C1312 (13.0f / 12.0f)

@@ -343,6 +343,12 @@ void Plan::finalize_args(std::vector<Op>& ops) {
         }
       } else if (ps.index >= 1 && !(ps.index == 1 && o.spec->acoustic)) {
         if (it == o.bind.end()) continue;
+        if (ps.kind == kRef && it->second < buffers_end) {
+          // a parameter struct that lives in a tape buffer (the radar head of
+          // morr_refl10cm): the kernel reads its words through the pointer
+          A.p[ps.index] = reinterpret_cast<float*>(M + it->second);
+          continue;
+        }
         A.iv[ps.index] = (int)word(it->second);
         A.f[ps.index] = fl(it->second);
         A.iv2[ps.index] = (int)word(it->second + 1);
@@ -358,6 +364,19 @@ void Plan::finalize_args(std::vector<Op>& ops) {
     // for 128 levels (3712 words per thread), one thread per column
     if (o.name == "morr_column" && (A.g.nz < 1 || A.g.nz > 128 || o.grid[2] != 1 || !o.tile_y))
       throw ApiError(TE_EINVAL, o.name + ": needs 1 <= nz <= 128 and a one-level dispatch grid");
+    // morr_refl10cm: 11 per-column arrays of nz levels in its 1408 scratch words, and reads
+    // the 14-word radar head, 100 bins of 6 words for snow and for graupel and 100 weights
+    // from tape buffers
+    if (o.name == "morr_refl10cm") {
+      if (A.g.nz < 1 || A.g.nz > 128 || o.grid[2] != 1 || !o.tile_y)
+        throw ApiError(TE_EINVAL, o.name + ": needs 1 <= nz <= 128 and a one-level dispatch grid");
+      const uint64_t need[5] = {0, 14, 600, 600, 100};
+      for (int b = 1; b <= 13; b++) {
+        if (!A.p[b]) throw ApiError(TE_EINVAL, o.name + ": binding " + std::to_string(b) + " not bound");
+        if (b <= 4 && o.bind.at(b) + need[b] > buffers_end)
+          throw ApiError(TE_ERANGE, o.name + ": binding " + std::to_string(b) + " runs past the tape buffers");
+      }
+    }
     // turb_zero writes up to level nz + 1 of its binding (its own range check): the
     // highest word the dispatch grid reaches must lie in the planned memory
     if (o.name == "turb_zero" && A.p[1]) {
