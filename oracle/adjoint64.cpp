@@ -25,6 +25,7 @@ using namespace te::adj;
 namespace {
 
 struct AccHost {
+  static constexpr bool skip_zero = true;
   static inline void add(double *p, double v) {
 #pragma omp atomic
     *p += v;

@@ -25,6 +25,7 @@
 
 #include "../../include/thunderstep.h"
 #include "te_adjoint.cuh"
+#include "te_fused.cuh"
 #include "te_kernels.cuh"
 #include "te_player.hpp"
 
@@ -32,6 +33,7 @@ namespace te {
 namespace adj {
 
 struct AccDevice {
+  static constexpr bool skip_zero = false;
   __device__ static void add(float* p, float v) { atomicAdd(p, v); }
 };
 
@@ -255,6 +257,97 @@ __global__ void k_adj_copy(float* L, uint64_t src, uint64_t dst, uint64_t n) {
   }
 }
 
+// Adjoint of a run of periodic halo pairs (bc_periodic_x(f) then bc_periodic_y(f)) on up
+// to 4 distinct fields.  The pair leaves every halo point of the box [-3, nx + 3] x
+// [-3, ny + 3] (levels 0..nz) with the value of its interior image (i mod nx, j mod ny), so
+// its adjoint moves each halo point's adjoint onto that image and clears it.  As a gather:
+// one thread per interior point that has images (the 7 columns i < 4, i >= nx - 3 and the
+// 7 rows j < 4, j >= ny - 3 of the interior; every other point has none), 3 levels each;
+// every halo point has exactly one image, so it is read and cleared by one thread and no
+// update needs an atomic.
+struct HaloRunArgs {
+  Dims g;
+  float* l[4];
+  int nf;
+};
+constexpr int kHaloRunLevels = 3;
+
+__global__ void __launch_bounds__(256) k_adj_halo_run(HaloRunArgs H) {
+  const Dims& g = H.g;
+  const int nx = g.nx, ny = g.ny;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j;
+  if (t < 7 * ny) {  // the x band, every row
+    j = t / 7;
+    const int c = t % 7;
+    i = c < 4 ? c : nx - 3 + (c - 4);
+    if (i < 0 || i >= nx || (c >= 4 && i < 4)) return;
+  } else {  // the y band, columns outside the x band
+    const int u = t - 7 * ny;
+    if (u >= 7 * nx) return;
+    const int r = u / nx;
+    i = u % nx;
+    j = r < 4 ? r : ny - 3 + (r - 4);
+    if (j < 0 || j >= ny || (r >= 4 && j < 4)) return;
+    if (i < 4 || i >= nx - 3) return;
+  }
+  // images i + a nx in [-3, nx + 3], j + b ny in [-3, ny + 3]
+  const int alo = -((i + 3) / nx), ahi = (nx + 3 - i) / nx;
+  const int blo = -((j + 3) / ny), bhi = (ny + 3 - j) / ny;
+  const int sk = g.sJ * g.sK;
+  for (int q = 0; q < kHaloRunLevels; q++) {
+    const int k = blockIdx.y * kHaloRunLevels + q;
+    if (k > g.nz) break;
+    for (int f = 0; f < H.nf; f++) {
+      float* L = H.l[f] + (size_t)k * sk;
+      float acc = 0.0f;
+      for (int a = alo; a <= ahi; a++)
+        for (int b = blo; b <= bhi; b++) {
+          if (a == 0 && b == 0) continue;
+          const int h = gidx(g, i + a * nx, j + b * ny, 0);
+          acc += L[h];
+          L[h] = 0.0f;
+        }
+      L[gidx(g, i, j, 0)] += acc;
+    }
+  }
+}
+
+static void launch_adj_halo_run(const HaloRunArgs& H, cudaStream_t s) {
+  const int threads = 7 * H.g.ny + 7 * H.g.nx;
+  launch_kernel(k_adj_halo_run, dim3((threads + 255) / 256, (H.g.nz + kHaloRunLevels) / kHaloRunLevels), dim3(256), 0,
+                s, H);
+}
+
+// The undo log's copies of a pitched region (`rows` rows of `width` words, `pitch` words
+// apart, at word `off` of the memory) to or from a packed run of the log: the halo planes
+// of the periodic fills, rows of 3 or 4 words, which a 2-D memcpy moves row by row.
+__global__ void k_strip_copy(uint32_t* M, uint64_t off, uint32_t width, uint64_t pitch, uint32_t n, uint32_t* log,
+                             int restore) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const uint32_t r = t / width, c = t - r * width;
+    uint32_t* m = M + off + (uint64_t)r * pitch + c;
+    if (restore) *m = log[t];
+    else log[t] = *m;
+  }
+}
+
+// The undo log's copy of a contiguous region (n words), as a kernel: inside the block
+// graphs a memcpy node of a device-to-device copy is slower than this.
+__global__ void __launch_bounds__(256) k_run_copy(uint32_t* __restrict__ dst, const uint32_t* __restrict__ src,
+                                                  uint64_t n) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; t + 3 * stride < n; t += 4 * stride) {
+    const uint32_t a = src[t], b = src[t + stride], c = src[t + 2 * stride], d = src[t + 3 * stride];
+    dst[t] = a;
+    dst[t + stride] = b;
+    dst[t + 2 * stride] = c;
+    dst[t + 3 * stride] = d;
+  }
+  for (; t < n; t += stride) dst[t] = src[t];
+}
+
 }  // namespace adj
 
 // A written region in words: `rows` rows of `width` words, `pitch` words apart.
@@ -276,6 +369,14 @@ struct AdjointState {
   uint32_t* undo = nullptr;
   uint64_t undo_cap = 0;  // words
   std::vector<cudaGraphExec_t> fwd_graph, rev_graph;  // per position in a block
+  // runs of periodic halo pairs (ops first..last) replayed and reversed as one launch each
+  struct HaloRun {
+    int first, last, nf;
+    float* f[4];
+    adj::HaloRunArgs adj;
+  };
+  std::vector<HaloRun> runs;
+  std::vector<int> run_from, run_to;  // per op: the run it starts / ends, or -1
 
   void drop_graphs() {
     for (auto g : fwd_graph)
@@ -386,7 +487,56 @@ void build_tables(Plan& P, AdjointState& S) {
       a.iv2[n] = o.args.iv2[n];
     }
   }
+  // runs of bc_periodic_x/y pairs on up to 4 distinct fields of the same grid
+  S.runs.clear();
+  S.run_from.assign(ops.size(), -1);
+  S.run_to.assign(ops.size(), -1);
+  for (size_t i = 0; i < ops.size();) {
+    float* f = nullptr;
+    if (!periodic_halo_pair(ops, i, &f)) {
+      i++;
+      continue;
+    }
+    AdjointState::HaloRun R;
+    std::memset(&R, 0, sizeof R);
+    R.first = (int)i;
+    const Dims& g = ops[i].args.g;
+    size_t e = i;
+    while (R.nf < 4 && periodic_halo_pair(ops, e, &f) && std::memcmp(&ops[e].args.g, &g, sizeof g) == 0 &&
+           std::find(R.f, R.f + R.nf, f) == R.f + R.nf) {
+      R.f[R.nf++] = f;
+      e += 2;
+    }
+    R.last = (int)e - 1;
+    R.adj.g = g;
+    R.adj.nf = R.nf;
+    for (int q = 0; q < R.nf; q++) R.adj.l[q] = S.L + (reinterpret_cast<const uint32_t*>(R.f[q]) - M);
+    S.run_from[R.first] = (int)S.runs.size();
+    S.run_to[R.last] = (int)S.runs.size();
+    S.runs.push_back(R);
+    i = e;
+  }
   S.step = P.active;
+}
+
+// Saves region r of the memory at `at` in the undo log, or restores it from there: a
+// contiguous region by k_run_copy, a pitched one (halo planes) by k_strip_copy.
+void copy_region(Plan& P, const Region& r, uint32_t* at, bool restore) {
+  if (r.rows == 1 || r.width == r.pitch) {
+    const uint64_t n = r.size();
+    const int blocks = (int)std::min<uint64_t>(148 * 8, (n + 1023) / 1024);
+    if (restore) launch_kernel(adj::k_run_copy, dim3(blocks), dim3(256), 0, P.stream, P.M + r.off, (const uint32_t*)at, n);
+    else launch_kernel(adj::k_run_copy, dim3(blocks), dim3(256), 0, P.stream, at, (const uint32_t*)(P.M + r.off), n);
+    ACU(cudaGetLastError());
+    return;
+  }
+  if (r.size() >= (1ull << 32) || r.width >= (1ull << 32))
+    throw AdjError(TE_ERANGE, "undo-log region of 2^32 words or more");
+  const uint32_t n = (uint32_t)r.size();
+  const int blocks = (int)std::min<uint64_t>(148 * 8, (n + 255) / 256);
+  launch_kernel(adj::k_strip_copy, dim3(blocks), dim3(256), 0, P.stream, P.M, r.off, (uint32_t)r.width, r.pitch, n, at,
+                restore ? 1 : 0);
+  ACU(cudaGetLastError());
 }
 
 // Replays the active step op by op, saving each op's written regions at log + cursor.
@@ -394,10 +544,21 @@ void logged_step(Plan& P, AdjointState& S, uint32_t* log) {
   std::vector<Op>& ops = P.active->ops;
   uint64_t cur = 0;
   for (size_t i = 0; i < ops.size(); i++) {
-    for (const Region& r : S.regions[i]) {
-      ACU(cudaMemcpy2DAsync(log + cur, r.width * 4, P.M + r.off, r.pitch * 4, r.width * 4, r.rows,
-                            cudaMemcpyDeviceToDevice, P.stream));
-      cur += r.size();
+    const int run = S.run_from[i];
+    const size_t last = run >= 0 ? (size_t)S.runs[run].last : i;
+    for (size_t q = i; q <= last; q++)
+      for (const Region& r : S.regions[q]) {
+        copy_region(P, r, log + cur, false);
+        cur += r.size();
+      }
+    if (run >= 0) {
+      // the pairs' halo fills leave the same memory as the per-dispatch kernels; the
+      // intermediate state between them is never read (their adjoints read no values)
+      const AdjointState::HaloRun& R = S.runs[run];
+      launch_periodic_halos(ops[i].args.g, R.f, R.nf, P.stream);
+      ACU(cudaGetLastError());
+      i = last;
+      continue;
     }
     P.launch_exact(ops, (int)i, (int)i, false);
   }
@@ -409,11 +570,23 @@ void reverse_step(Plan& P, AdjointState& S, const uint32_t* log) {
   uint64_t cur = S.step_undo_words;
   for (size_t ii = ops.size(); ii-- > 0;) {
     const Op& o = ops[ii];
+    if (S.run_to[ii] >= 0) {
+      const AdjointState::HaloRun& R = S.runs[S.run_to[ii]];
+      for (size_t op = ii + 1; op-- > (size_t)R.first;)
+        for (size_t q = S.regions[op].size(); q-- > 0;) {
+          const Region& r = S.regions[op][q];
+          cur -= r.size();
+          copy_region(P, r, const_cast<uint32_t*>(log + cur), true);
+        }
+      adj::launch_adj_halo_run(R.adj, P.stream);
+      ACU(cudaGetLastError());
+      ii = (size_t)R.first;
+      continue;
+    }
     for (size_t q = S.regions[ii].size(); q-- > 0;) {
       const Region& r = S.regions[ii][q];
       cur -= r.size();
-      ACU(cudaMemcpy2DAsync(P.M + r.off, r.pitch * 4, log + cur, r.width * 4, r.width * 4, r.rows,
-                            cudaMemcpyDeviceToDevice, P.stream));
+      copy_region(P, r, const_cast<uint32_t*>(log + cur), true);
     }
     if (o.copy) {
       const int blocks = (int)std::min<uint64_t>(1024, (o.n + 255) / 256);

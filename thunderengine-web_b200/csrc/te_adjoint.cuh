@@ -12,6 +12,9 @@
 //     identity part and passes the rest on.
 // Contributions to other points are added through the `Acc` policy (atomic adds on the GPU,
 // OpenMP atomics on the host), so the operators can run one thread per dispatch thread.
+// `Acc::skip_zero` says whether an operator returns early when the adjoint it reads is 0
+// (all it would add is 0): worth it on the host; on the GPU the branch would make every
+// thread wait for that load before issuing its other loads, so there it is off.
 //
 // The arithmetic is generic in the real type R: the library instantiates it in binary32
 // (te_adjoint.cu), the binary64 CPU adjoint of the test suite in binary64.  The local
@@ -277,7 +280,7 @@ TE_HD void adj_flux_lin_h(const AdjArgs<R>& A, int tx, int ty, int tz, int dir) 
   const int c = gidx(g, i, j, k), d = dir == 0 ? 1 : g.sJ;
   const R lam = A.l[3][c];
   A.l[3][c] = R(0);
-  if (lam == R(0)) return;
+  if (Acc::skip_zero && lam == R(0)) return;
   Face<Q> F;
   load_face(F, A.p[1], c, d, dir == 0 ? i : j, -3, dir == 0 ? g.nx + 3 : g.ny + 3);
   typedef typename Face<Q>::T T;
@@ -297,7 +300,7 @@ TE_HD void adj_flux_lin_z(const AdjArgs<R>& A, int tx, int ty, int tz) {
   const int c = gidx(g, i, j, k), sk = g.sJ * g.sK;
   const R lam = A.l[5][c];
   A.l[5][c] = R(0);
-  if (k == 0 || k == g.nz || lam == R(0)) return;
+  if (k == 0 || k == g.nz || (Acc::skip_zero && lam == R(0))) return;
   const R *c1 = A.p[3], *c2 = A.p[4];
   Face<Q> F;
   typedef typename Face<Q>::T T;
@@ -338,7 +341,7 @@ TE_HD void adj_flux_stag_h(const AdjArgs<R>& A, int tx, int ty, int tz, int dir)
   const int c = gidx(g, i, j, k), sj = g.sJ, sk = g.sJ * g.sK;
   const R lam = A.l[8][c];
   A.l[8][c] = R(0);
-  if ((stag == 4 && k == 0) || lam == R(0)) return;
+  if ((stag == 4 && k == 0) || (Acc::skip_zero && lam == R(0))) return;
   const int rb = dir == 0 ? 3 : 4;  // rru or rrv binding
   const R* rr = A.p[rb];
   R* lr = A.l[rb];
@@ -379,7 +382,7 @@ TE_HD void adj_flux_stag_z(const AdjArgs<R>& A, int tx, int ty, int tz) {
   const int c = gidx(g, i, j, k), sj = g.sJ, sk = g.sJ * g.sK;
   const R lam = A.l[8][c];
   A.l[8][c] = R(0);
-  if (lam == R(0)) return;
+  if (Acc::skip_zero && lam == R(0)) return;
   if (stag == 4 ? k > g.nz - 1 : (k == 0 || k == g.nz)) return;
   const R *rrw = A.p[5], *c1 = A.p[6], *c2 = A.p[7];
   R* lw = A.l[5];
@@ -441,7 +444,7 @@ TE_HD void adj_flux_weno_h(const AdjArgs<R>& A, int tx, int ty, int tz, int dir)
   const int c = gidx(g, i, j, k), d = dir == 0 ? 1 : g.sJ;
   const R lam = A.l[5][c];
   A.l[5][c] = R(0);
-  if (lam == R(0)) return;
+  if (Acc::skip_zero && lam == R(0)) return;
   const Q weps = (Q)A.f[3];
   const bool pdef = A.iv[4] == 1;
   Face<Q> F;
@@ -467,7 +470,7 @@ TE_HD void adj_flux_weno_z(const AdjArgs<R>& A, int tx, int ty, int tz) {
   const int c = gidx(g, i, j, k), sk = g.sJ * g.sK;
   const R lam = A.l[8][c];
   A.l[8][c] = R(0);
-  if (kf == 1 || kf == g.nz + 1 || lam == R(0)) return;
+  if (kf == 1 || kf == g.nz + 1 || (Acc::skip_zero && lam == R(0))) return;
   const R *c1 = A.p[3], *c2 = A.p[4];
   const Q weps = (Q)A.f[5];
   const bool pdefweno = A.iv[7] == 1;
@@ -523,7 +526,7 @@ TE_HD void adj_flux_weno_uv_h(const AdjArgs<R>& A, int tx, int ty, int tz, int d
   const int c = gidx(g, i, j, k), sj = g.sJ;
   const R lam = A.l[5][c];
   A.l[5][c] = R(0);
-  if (lam == R(0)) return;
+  if (Acc::skip_zero && lam == R(0)) return;
   const Q weps = (Q)A.f[4];
   const R* rr = A.p[3];
   R* lr = A.l[3];
@@ -551,7 +554,7 @@ TE_HD void adj_flux_weno_uv_z(const AdjArgs<R>& A, int tx, int ty, int tz) {
   const int c = gidx(g, i, j, k), sj = g.sJ, sk = g.sJ * g.sK;
   const R lam = A.l[7][c];
   A.l[7][c] = R(0);
-  if (k == 0 || k == g.nz || lam == R(0)) return;
+  if (k == 0 || k == g.nz || (Acc::skip_zero && lam == R(0))) return;
   const R *rrw = A.p[3], *c1 = A.p[4], *c2 = A.p[5];
   R* lw = A.l[3];
   const Q weps = (Q)A.f[6];
@@ -584,7 +587,7 @@ TE_HD void adj_flux_weno_w_h(const AdjArgs<R>& A, int tx, int ty, int tz, int di
   const int c = gidx(g, i, j, k), sk = g.sJ * g.sK;
   const R lam = A.l[5][c];
   A.l[5][c] = R(0);
-  if (k == 0 || lam == R(0)) return;
+  if (k == 0 || (Acc::skip_zero && lam == R(0))) return;
   const Q weps = (Q)A.f[4];
   const R* rr = A.p[2];
   R* lr = A.l[2];
@@ -609,7 +612,7 @@ TE_HD void adj_flux_weno_w_z(const AdjArgs<R>& A, int tx, int ty, int tz) {
   const int c = gidx(g, i, j, k), sk = g.sJ * g.sK;
   const R lam = A.l[4][c];
   A.l[4][c] = R(0);
-  if (k > g.nz - 1 || lam == R(0)) return;
+  if (k > g.nz - 1 || (Acc::skip_zero && lam == R(0))) return;
   const Q weps = (Q)A.f[3];
   const R* rrw = A.p[2];
   R* lw = A.l[2];
@@ -650,7 +653,7 @@ TE_HD void adj_assemble(const AdjArgs<R>& A, int tx, int ty, int tz) {
   R* ldest = A.l[11];
   const R lt = ldest[c];
   if (A.iv[12] == 0) ldest[c] = R(0);  // dest overwritten
-  if (lt == R(0)) return;
+  if (Acc::skip_zero && lt == R(0)) return;
   const R *s = A.p[2], *divx = A.p[6], *rho0 = A.p[7], *rf0 = A.p[8], *mh = A.p[9], *mf = A.p[10];
   const R *c1 = A.p[15], *c2 = A.p[16], *hm = A.p[30];
   R dv;
@@ -820,7 +823,7 @@ TE_HD void adj_div_massflux(const AdjArgs<R>& A, int tx, int ty, int tz) {
   const int c = gidx(g, i, j, k), sj = g.sJ, sk = g.sJ * g.sK;
   const R ld = A.l[5][c];
   A.l[5][c] = R(0);
-  if (ld == R(0)) return;
+  if (Acc::skip_zero && ld == R(0)) return;
   const R* hm = A.p[30];
   const R az = ld * (R)g.rdz * A.p[4][k], ax = ld * (R)g.rdx * hm_uh_(g, hm, i), ay = ld * (R)g.rdy * hm_vh_(g, hm, j);
   Acc::add(&A.l[3][c + sk], az);
@@ -840,7 +843,7 @@ TE_HD void adj_divergence3d(const AdjArgs<R>& A, int tx, int ty, int tz) {
   const int c = gidx(g, i, j, k), sj = g.sJ, sk = g.sJ * g.sK;
   const R ld = A.l[5][c];
   A.l[5][c] = R(0);
-  if (ld == R(0)) return;
+  if (Acc::skip_zero && ld == R(0)) return;
   const R *u = A.p[1], *v = A.p[2], *w = A.p[3], *mh = A.p[4], *hm = A.p[30];
   const R d = rfma((w[c + sk] - w[c]) * (R)g.rdz, mh[k],
                    rfma((u[c + 1] - u[c]) * (R)g.rdx, hm_uh_(g, hm, i), ((v[c + sj] - v[c]) * (R)g.rdy) * hm_vh_(g, hm, j)));
@@ -962,7 +965,7 @@ TE_HD void adj_acoustic_fpk(const AdjArgs<R>& A, int tx, int ty, int tz) {
   const int c = gidx(g, i, j, k), sj = g.sJ, sk = g.sJ * g.sK;
   const R lf = A.l[11][c];
   A.l[11][c] = R(0);
-  if (lf == R(0)) return;
+  if (Acc::skip_zero && lf == R(0)) return;
   const R *u = A.p[2], *v = A.p[3], *piadv = A.p[5], *ppterm = A.p[7], *pk1 = A.p[8], *pk2 = A.p[9], *qk = A.p[10];
   const R *hm = A.p[30];
   const R dts = (R)A.a.dts, beta = (R)A.a.beta;

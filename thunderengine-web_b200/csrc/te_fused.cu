@@ -1040,6 +1040,17 @@ static bool halo_pair(const std::vector<Op>& ops, size_t i, float** f) {
   return true;
 }
 
+bool periodic_halo_pair(const std::vector<Op>& ops, size_t i, float** f) { return halo_pair(ops, i, f); }
+
+void launch_periodic_halos(const Dims& g, float* const* f, int nf, cudaStream_t s) {
+  HaloArgs H;
+  std::memset(&H, 0, sizeof H);
+  H.g = g;
+  H.nf = nf;
+  for (int q = 0; q < nf && q < 4; q++) H.f[q] = f[q];
+  launch_halo(H, s);
+}
+
 static const char* kSubstep[] = {"acoustic_uv", "acoustic_fpk", "acoustic_w_solve", "acoustic_pp"};
 
 static bool match_substep(const std::vector<Op>& ops, size_t i, FusedSegment& s, AcuArgs& A) {

@@ -4,6 +4,8 @@
 
 #include <vector>
 
+#include "te_dims.cuh"
+
 namespace te {
 
 struct Op;
@@ -27,5 +29,13 @@ struct FusedStep {
   int launches_per_step() const;
   void release();
 };
+
+// ops[i], ops[i + 1] are bc_periodic_x(f) then bc_periodic_y(f) over the standard halo
+// grids (4 x (ny + 7) x (nz + 1), 4 x (nx + 7) x (nz + 1)): sets *f, returns true.
+bool periodic_halo_pair(const std::vector<Op>& ops, size_t i, float** f);
+
+// The final state of such pairs for nf <= 4 distinct fields in one launch: every halo point
+// of levels 0..nz holds the interior value at (i mod nx, j mod ny).
+void launch_periodic_halos(const Dims& g, float* const* f, int nf, cudaStream_t s);
 
 }  // namespace te
