@@ -665,9 +665,11 @@ TE_HD void adj_assemble(const AdjArgs<R>& A, int tx, int ty, int tz) {
   const R mx = st == 2 ? hm_uf_(g, hm, i) : hm_uh_(g, hm, i);
   const R my = st == 3 ? hm_vf_(g, hm, j) : hm_vh_(g, hm, j);
   const R rho = st == 4 ? rf0[k] : rho0[k];
+  // the values read after the first atomic add, loaded before it
+  const R sc = s[c], c1k = st == 4 ? c1[k] : R(0), c2k = st == 4 ? c2[k] : R(0);
   const R ln = lt / rho;  // adjoint of the numerator s dv - divF
   Acc::add(&A.l[2][c], ln * dv);
-  const R lsdv = ln * s[c];
+  const R lsdv = ln * sc;
   R* ld = A.l[6];
   if (st == 2) {
     Acc::add(&ld[c], R(0.5) * lsdv);
@@ -676,8 +678,8 @@ TE_HD void adj_assemble(const AdjArgs<R>& A, int tx, int ty, int tz) {
     Acc::add(&ld[c], R(0.5) * lsdv);
     Acc::add(&ld[c - sj], R(0.5) * lsdv);
   } else if (st == 4) {
-    Acc::add(&ld[c], c2[k] * lsdv);
-    Acc::add(&ld[c - sk], c1[k] * lsdv);
+    Acc::add(&ld[c], c2k * lsdv);
+    Acc::add(&ld[c - sk], c1k * lsdv);
   } else {
     Acc::add(&ld[c], lsdv);
   }
@@ -716,10 +718,10 @@ TE_HD void adj_rk_update(const AdjArgs<R>& A, int tx, int ty, int tz) {
   const int i = tx, j = ty, k = tz;
   if (i > iMax || j > jMax || k < kLo || k >= g.nz) return;
   const int c = gidx(g, i, j, k);
-  const R lp = A.l[4][c];
+  const R lp = A.l[4][c], l2 = A.l[2][c], l3 = A.l[3][c];
   A.l[4][c] = R(0);
-  own(&A.l[2][c], lp);
-  own(&A.l[3][c], (R)A.f[5] * lp);
+  A.l[2][c] = l2 + lp;
+  A.l[3][c] = l3 + (R)A.f[5] * lp;
 }
 
 // apply_thterm: tend = fma(-div, thterm, tend)
@@ -729,8 +731,8 @@ TE_HD void adj_apply_thterm(const AdjArgs<R>& A, int tx, int ty, int tz) {
   const int i = tx, j = ty, k = tz;
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
   const int c = gidx(g, i, j, k);
-  const R lt = A.l[3][c];
-  own(&A.l[1][c], -A.p[2][c] * lt);  // thterm is a constant of the core step
+  const R lt = A.l[3][c], l1 = A.l[1][c];
+  A.l[1][c] = l1 + -A.p[2][c] * lt;  // thterm is a constant of the core step
 }
 
 // buoyancy_apply: wten += c1 buoy(k-1) + c2 buoy(k) on interior faces
@@ -770,24 +772,23 @@ TE_HD void adj_update_diagnostics_moist(const AdjArgs<R>& A, int tx, int ty, int
   const R cpli = rfma(cpl, liq > R(0) ? liq : R(0), cpi * (ice > R(0) ? ice : R(0)));
   const R cpm = rfma(cpv, qvv, cp) + cpli;
   const R cvm = R(1) / (rfma(cvv, qvv, cv) + cpli);
+  // every adjoint this thread reads, before any of its stores (the bindings are distinct
+  // fields, so the loads need not wait for the stores)
+  const R l15 = A.l[15][c], l16 = A.l[16][c], l17 = A.l[17][c], l18 = A.l[18][c], l19 = A.l[19][c];
+  const R l1 = A.l[1][c], l2 = A.l[2][c];
   R lth = R(0), lpi = R(0);
-  R* L15 = A.l[15];
-  R* L16 = A.l[16];
-  R* L17 = A.l[17];
-  R* L18 = A.l[18];
-  R* L19 = A.l[19];
-  lth += L15[c] * (rfma(reps, qvv, R(1)) / ((R(1) + qvv) + qli));
-  L15[c] = R(0);
-  lpi += L16[c] * ((rovcp * cpm) * cvm);
-  L16[c] = R(0);
-  lpi += L17[c];
-  L17[c] = R(0);
-  lth += L18[c] * (rfma(-rovcp, cpm, rfma(rv, qvv, rd)) * cvm);
-  L18[c] = R(0);
-  lth += L19[c] * (gacc * rth0[k]);
-  L19[c] = R(0);
-  own(&A.l[1][c], lth);
-  own(&A.l[2][c], lpi);
+  lth += l15 * (rfma(reps, qvv, R(1)) / ((R(1) + qvv) + qli));
+  lpi += l16 * ((rovcp * cpm) * cvm);
+  lpi += l17;
+  lth += l18 * (rfma(-rovcp, cpm, rfma(rv, qvv, rd)) * cvm);
+  lth += l19 * (gacc * rth0[k]);
+  A.l[15][c] = R(0);
+  A.l[16][c] = R(0);
+  A.l[17][c] = R(0);
+  A.l[18][c] = R(0);
+  A.l[19][c] = R(0);
+  A.l[1][c] = l1 + lth;
+  A.l[2][c] = l2 + lpi;
 }
 
 // stage_tendency_reset: uten = vten = wten = 0
@@ -804,13 +805,16 @@ template <class R, class Acc>
 TE_HD void adj_massflux_from_state(const AdjArgs<R>& A, int tx, int ty, int tz) {
   TE_ADJ_WHOLE(k <= g.nz)
   const R *rho0 = A.p[4], *rf0 = A.p[5];
+  const bool wk = k != 0 && k != g.nz;
+  const R l8 = wk ? A.l[8][c] : R(0), l3 = wk ? A.l[3][c] : R(0);
   if (k < g.nz) {
-    own(&A.l[1][c], rho0[k] * A.l[6][c]);
-    own(&A.l[2][c], rho0[k] * A.l[7][c]);
+    const R l6 = A.l[6][c], l7 = A.l[7][c], l1 = A.l[1][c], l2 = A.l[2][c];
+    A.l[1][c] = l1 + rho0[k] * l6;
+    A.l[2][c] = l2 + rho0[k] * l7;
     A.l[6][c] = R(0);
     A.l[7][c] = R(0);
   }
-  if (k != 0 && k != g.nz) own(&A.l[3][c], rf0[k] * A.l[8][c]);
+  if (wk) A.l[3][c] = l3 + rf0[k] * l8;
   A.l[8][c] = R(0);
 }
 
@@ -862,18 +866,21 @@ template <class R, class Acc>
 TE_HD void adj_velocity_to_massflux(const AdjArgs<R>& A, int tx, int ty, int tz) {
   TE_ADJ_WHOLE(k <= g.nz)
   const R *rho0 = A.p[1], *rf0 = A.p[2];
+  const R l5 = A.l[5][c];
   if (k < g.nz) {
-    A.l[3][c] = A.l[3][c] * rho0[k];
-    A.l[4][c] = A.l[4][c] * rho0[k];
+    const R l3 = A.l[3][c], l4 = A.l[4][c];
+    A.l[3][c] = l3 * rho0[k];
+    A.l[4][c] = l4 * rho0[k];
   }
-  A.l[5][c] = (k == 0 || k == g.nz) ? R(0) : A.l[5][c] * rf0[k];
+  A.l[5][c] = (k == 0 || k == g.nz) ? R(0) : l5 * rf0[k];
 }
 
 // build_sadv: sadv = (th0 - 300) + th'
 template <class R, class Acc>
 TE_HD void adj_build_sadv(const AdjArgs<R>& A, int tx, int ty, int tz) {
   TE_ADJ_WHOLE(k < g.nz)
-  own(&A.l[2][c], A.l[3][c]);
+  const R l3 = A.l[3][c], l2 = A.l[2][c];
+  A.l[2][c] = l2 + l3;
   A.l[3][c] = R(0);
 }
 
@@ -881,11 +888,13 @@ TE_HD void adj_build_sadv(const AdjArgs<R>& A, int tx, int ty, int tz) {
 template <class R, class Acc>
 TE_HD void adj_stage_state_reset(const AdjArgs<R>& A, int tx, int ty, int tz) {
   TE_ADJ_WHOLE(k <= g.nz)
-  own(&A.l[1][c], A.l[5][c]);
-  own(&A.l[2][c], A.l[6][c]);
-  own(&A.l[3][c], A.l[7][c]);
-  own(&A.l[4][c], A.l[8][c]);
-  own(&A.l[10][c], A.l[9][c]);
+  const R l5 = A.l[5][c], l6 = A.l[6][c], l7 = A.l[7][c], l8 = A.l[8][c], l9 = A.l[9][c];
+  const R l1 = A.l[1][c], l2 = A.l[2][c], l3 = A.l[3][c], l4 = A.l[4][c], l10 = A.l[10][c];
+  A.l[1][c] = l1 + l5;
+  A.l[2][c] = l2 + l6;
+  A.l[3][c] = l3 + l7;
+  A.l[4][c] = l4 + l8;
+  A.l[10][c] = l10 + l9;
   A.l[5][c] = R(0);
   A.l[6][c] = R(0);
   A.l[7][c] = R(0);
@@ -912,9 +921,10 @@ TE_HD void adj_acoustic_prepare(const AdjArgs<R>& A, int tx, int ty, int tz) {
 template <class R, class Acc>
 TE_HD void adj_acoustic_begin(const AdjArgs<R>& A, int tx, int ty, int tz) {
   TE_ADJ_WHOLE(k <= g.nz)
+  const R l5 = A.l[5][c], l2 = A.l[2][c];
   A.l[3][c] = R(0);
   A.l[4][c] = R(0);
-  own(&A.l[2][c], (R)A.a.beta * A.l[5][c]);
+  A.l[2][c] = l2 + (R)A.a.beta * l5;
   A.l[5][c] = R(0);
 }
 
@@ -934,25 +944,23 @@ TE_HD void adj_acoustic_uv(const AdjArgs<R>& A, int tx, int ty, int tz) {
   // u' = u + dts (uten - tem1 uf (thv + thv_w) (ppd - ppd_w)); thv is a constant of the
   // core step (no adjoint); u and uten updated at the thread's own point
   R gc = R(0);
-  if (!uEdge) {
-    const R lu = A.l[6][c];
-    if (lu != R(0)) {
-      const R gp = lu * dts * (thv[c] + thv[c - 1]) * (-(tem1 * hm_uf_(g, hm, i)));
-      gc += gp;
-      Acc::add(&A.l[2][c - 1], -gp);
-      own(&A.l[4][c], lu * dts);
-    }
+  // the adjoints and values this thread reads, before any of its stores
+  const R lu = uEdge ? R(0) : A.l[6][c], lv = vEdge ? R(0) : A.l[7][c];
+  const R l4 = uEdge ? R(0) : A.l[4][c], l5 = vEdge ? R(0) : A.l[5][c];
+  const R tc = thv[c], tw = uEdge ? R(0) : thv[c - 1], ts = vEdge ? R(0) : thv[c - sj];
+  if (!uEdge && !(Acc::skip_zero && lu == R(0))) {
+    const R gp = lu * dts * (tc + tw) * (-(tem1 * hm_uf_(g, hm, i)));
+    gc += gp;
+    Acc::add(&A.l[2][c - 1], -gp);
+    A.l[4][c] = l4 + lu * dts;
   }
-  if (!vEdge) {
-    const R lv = A.l[7][c];
-    if (lv != R(0)) {
-      const R gp = lv * dts * (thv[c] + thv[c - sj]) * (-(tem2 * hm_vf_(g, hm, j)));
-      gc += gp;
-      Acc::add(&A.l[2][c - sj], -gp);
-      own(&A.l[5][c], lv * dts);
-    }
+  if (!vEdge && !(Acc::skip_zero && lv == R(0))) {
+    const R gp = lv * dts * (tc + ts) * (-(tem2 * hm_vf_(g, hm, j)));
+    gc += gp;
+    Acc::add(&A.l[2][c - sj], -gp);
+    A.l[5][c] = l5 + lv * dts;
   }
-  if (gc != R(0)) Acc::add(&A.l[2][c], gc);
+  if (!(Acc::skip_zero && gc == R(0))) Acc::add(&A.l[2][c], gc);
 }
 
 // acoustic_fpk (acoustic_fpk.wgsl:167-207): the explicit pi' forcing from u, v, w (pk1,
@@ -964,23 +972,31 @@ TE_HD void adj_acoustic_fpk(const AdjArgs<R>& A, int tx, int ty, int tz) {
   if (i >= g.nx || j >= g.ny || k >= g.nz) return;
   const int c = gidx(g, i, j, k), sj = g.sJ, sk = g.sJ * g.sK;
   const R lf = A.l[11][c];
-  A.l[11][c] = R(0);
-  if (Acc::skip_zero && lf == R(0)) return;
+  if (Acc::skip_zero && lf == R(0)) {
+    A.l[11][c] = R(0);
+    return;
+  }
   const R *u = A.p[2], *v = A.p[3], *piadv = A.p[5], *ppterm = A.p[7], *pk1 = A.p[8], *pk2 = A.p[9], *qk = A.p[10];
   const R *hm = A.p[30];
   const R dts = (R)A.a.dts, beta = (R)A.a.beta;
+  // every value this thread reads, before any of its stores
   const R uh = hm_uh_(g, hm, i), vh = hm_vh_(g, hm, j);
+  const R du = u[c + 1] - u[c], dv = v[c + sj] - v[c];
+  const R a1 = pk1[c] + qk[c], a2 = pk2[c] - qk[c], pt = ppterm[c];
+  const R pc = piadv[c], pxp = piadv[c + 1], pxm = piadv[c - 1], pyp = piadv[c + sj], pym = piadv[c - sj];
+  const R l6 = A.l[6][c];
+  A.l[11][c] = R(0);
   const R temx = (dts * R(0.5)) * (R)g.rdx, temy = (dts * R(0.5)) * (R)g.rdy;
-  const R div = rfma((u[c + 1] - u[c]) * (R)g.rdx, uh, ((v[c + sj] - v[c]) * (R)g.rdy) * vh);
+  const R div = rfma(du * (R)g.rdx, uh, (dv * (R)g.rdy) * vh);
   const bool clipped = rabs(div) < (R)A.a.smeps;
-  Acc::add(&A.l[4][c], lf * beta * (pk1[c] + qk[c]));
-  Acc::add(&A.l[4][c + sk], lf * beta * (pk2[c] - qk[c]));
-  own(&A.l[6][c], lf * dts);  // ppten, read at the thread's own point only
-  const R ldiv = clipped ? R(0) : lf * dts * (-ppterm[c]);
-  const R lu1 = ldiv * (R)g.rdx * uh - lf * (piadv[c + 1] - piadv[c]) * temx * uh;
-  const R lu0 = -ldiv * (R)g.rdx * uh - lf * (piadv[c] - piadv[c - 1]) * temx * uh;
-  const R lv1 = ldiv * (R)g.rdy * vh - lf * (piadv[c + sj] - piadv[c]) * temy * vh;
-  const R lv0 = -ldiv * (R)g.rdy * vh - lf * (piadv[c] - piadv[c - sj]) * temy * vh;
+  Acc::add(&A.l[4][c], lf * beta * a1);
+  Acc::add(&A.l[4][c + sk], lf * beta * a2);
+  A.l[6][c] = l6 + lf * dts;  // ppten, read at the thread's own point only
+  const R ldiv = clipped ? R(0) : lf * dts * (-pt);
+  const R lu1 = ldiv * (R)g.rdx * uh - lf * (pxp - pc) * temx * uh;
+  const R lu0 = -ldiv * (R)g.rdx * uh - lf * (pc - pxm) * temx * uh;
+  const R lv1 = ldiv * (R)g.rdy * vh - lf * (pyp - pc) * temy * vh;
+  const R lv0 = -ldiv * (R)g.rdy * vh - lf * (pc - pym) * temy * vh;
   Acc::add(&A.l[2][c + 1], lu1);
   Acc::add(&A.l[2][c], lu0);
   Acc::add(&A.l[3][c + sj], lv1);
@@ -998,7 +1014,8 @@ TE_HD void adj_acoustic_pp(const AdjArgs<R>& A, int tx, int ty, int tz) {
   const R alph = (R)A.a.alph, kdiv = (R)A.a.kdiv;
   const bool saveX = A.iv[10] != 0;
   const R prev = pp3d[c];
-  const R p = rfma(alph, rfma(w[c], pk1[c] + qk[c], w[c + sk] * (pk2[c] - qk[c])), prev + fpk[c]);
+  const R a1 = pk1[c] + qk[c], a2 = pk2[c] - qk[c];
+  const R p = rfma(alph, rfma(w[c], a1, w[c + sk] * a2), prev + fpk[c]);
   const bool clipped = rabs(p) < (R)A.a.smeps;
   const R lpp = A.l[7][c], lppd = A.l[8][c], lpx = saveX ? A.l[9][c] : R(0);
   A.l[8][c] = R(0);
@@ -1009,8 +1026,8 @@ TE_HD void adj_acoustic_pp(const AdjArgs<R>& A, int tx, int ty, int tz) {
   if (clipped) lp = R(0);
   A.l[7][c] = lprev + lp;  // pp3d before the op: prev, and through p
   Acc::add(&A.l[6][c], lp);
-  Acc::add(&A.l[2][c], lp * alph * (pk1[c] + qk[c]));
-  Acc::add(&A.l[2][c + sk], lp * alph * (pk2[c] - qk[c]));
+  Acc::add(&A.l[2][c], lp * alph * a1);
+  Acc::add(&A.l[2][c + sk], lp * alph * a2);
 }
 
 // acoustic_accumulate: rr += u (averaged on the last substep; w weighted by alph)
@@ -1019,17 +1036,18 @@ TE_HD void adj_acoustic_accumulate(const AdjArgs<R>& A, int tx, int ty, int tz) 
   TE_ADJ_WHOLE(k <= g.nz)
   const R tavg = (R)A.f[8];
   const R lu = A.l[5][c], lv = A.l[6][c], lw = A.l[7][c];
+  const R l2 = A.l[2][c], l3 = A.l[3][c], l4 = A.l[4][c];
   if (tavg > R(0)) {
     A.l[5][c] = lu * tavg;
     A.l[6][c] = lv * tavg;
     A.l[7][c] = lw * tavg;
-    own(&A.l[2][c], lu * tavg);
-    own(&A.l[3][c], lv * tavg);
-    own(&A.l[4][c], lw * tavg * (R)A.a.alph);
+    A.l[2][c] = l2 + lu * tavg;
+    A.l[3][c] = l3 + lv * tavg;
+    A.l[4][c] = l4 + lw * tavg * (R)A.a.alph;
   } else {
-    own(&A.l[2][c], lu);
-    own(&A.l[3][c], lv);
-    own(&A.l[4][c], lw);
+    A.l[2][c] = l2 + lu;
+    A.l[3][c] = l3 + lv;
+    A.l[4][c] = l4 + lw;
   }
 }
 
