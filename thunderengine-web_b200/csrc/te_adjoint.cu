@@ -261,18 +261,17 @@ __global__ void k_adj_copy(float* L, uint64_t src, uint64_t dst, uint64_t n) {
 // to 4 distinct fields.  The pair leaves every halo point of the box [-3, nx + 3] x
 // [-3, ny + 3] (levels 0..nz) with the value of its interior image (i mod nx, j mod ny), so
 // its adjoint moves each halo point's adjoint onto that image and clears it.  As a gather:
-// one thread per interior point that has images (the 7 columns i < 4, i >= nx - 3 and the
-// 7 rows j < 4, j >= ny - 3 of the interior; every other point has none), 3 levels each;
+// one thread per (interior point that has images, level, field) — the points with images
+// are the 7 columns i < 4, i >= nx - 3 and the 7 rows j < 4, j >= ny - 3 of the interior;
 // every halo point has exactly one image, so it is read and cleared by one thread and no
-// update needs an atomic.
+// update needs an atomic.  A thread reads all its halo points before its first store.
 struct HaloRunArgs {
   Dims g;
   float* l[4];
   int nf;
 };
-constexpr int kHaloRunLevels = 3;
 
-__global__ void __launch_bounds__(256) k_adj_halo_run(HaloRunArgs H) {
+__global__ void __launch_bounds__(128) k_adj_halo_run(HaloRunArgs H) {
   const Dims& g = H.g;
   const int nx = g.nx, ny = g.ny;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -291,61 +290,58 @@ __global__ void __launch_bounds__(256) k_adj_halo_run(HaloRunArgs H) {
     if (j < 0 || j >= ny || (r >= 4 && j < 4)) return;
     if (i < 4 || i >= nx - 3) return;
   }
+  const int k = blockIdx.y, f = blockIdx.z;
+  if (k > g.nz || f >= H.nf) return;
   // images i + a nx in [-3, nx + 3], j + b ny in [-3, ny + 3]
   const int alo = -((i + 3) / nx), ahi = (nx + 3 - i) / nx;
   const int blo = -((j + 3) / ny), bhi = (ny + 3 - j) / ny;
-  const int sk = g.sJ * g.sK;
-  for (int q = 0; q < kHaloRunLevels; q++) {
-    const int k = blockIdx.y * kHaloRunLevels + q;
-    if (k > g.nz) break;
-    for (int f = 0; f < H.nf; f++) {
-      float* L = H.l[f] + (size_t)k * sk;
-      float acc = 0.0f;
-      for (int a = alo; a <= ahi; a++)
-        for (int b = blo; b <= bhi; b++) {
-          if (a == 0 && b == 0) continue;
-          const int h = gidx(g, i + a * nx, j + b * ny, 0);
-          acc += L[h];
-          L[h] = 0.0f;
-        }
-      L[gidx(g, i, j, 0)] += acc;
-    }
-  }
+  float* L = H.l[f] + (size_t)k * g.sJ * g.sK;
+  float acc = 0.0f;
+  for (int a = alo; a <= ahi; a++)
+    for (int b = blo; b <= bhi; b++)
+      if (a != 0 || b != 0) acc += L[gidx(g, i + a * nx, j + b * ny, 0)];
+  const int c0 = gidx(g, i, j, 0);
+  const float own = L[c0];
+  for (int a = alo; a <= ahi; a++)
+    for (int b = blo; b <= bhi; b++)
+      if (a != 0 || b != 0) L[gidx(g, i + a * nx, j + b * ny, 0)] = 0.0f;
+  L[c0] = own + acc;
 }
 
 static void launch_adj_halo_run(const HaloRunArgs& H, cudaStream_t s) {
   const int threads = 7 * H.g.ny + 7 * H.g.nx;
-  launch_kernel(k_adj_halo_run, dim3((threads + 255) / 256, (H.g.nz + kHaloRunLevels) / kHaloRunLevels), dim3(256), 0,
-                s, H);
+  launch_kernel(k_adj_halo_run, dim3((threads + 127) / 128, H.g.nz + 1, H.nf), dim3(128), 0, s, H);
 }
 
-// The undo log's copies of a pitched region (`rows` rows of `width` words, `pitch` words
-// apart, at word `off` of the memory) to or from a packed run of the log: the halo planes
-// of the periodic fills, rows of 3 or 4 words, which a 2-D memcpy moves row by row.
-__global__ void k_strip_copy(uint32_t* M, uint64_t off, uint32_t width, uint64_t pitch, uint32_t n, uint32_t* log,
-                             int restore) {
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    const uint32_t r = t / width, c = t - r * width;
-    uint32_t* m = M + off + (uint64_t)r * pitch + c;
-    if (restore) *m = log[t];
-    else log[t] = *m;
-  }
-}
+// The undo log's copies of one op's regions in one launch: region q is `rows` rows of
+// `width` words, `pitch` words apart, at word `off` of the memory, packed at word `log` of
+// the undo log; `start` holds the prefix sums of the regions' sizes.  save: memory -> log,
+// restore: log -> memory.
+constexpr int kCopyBatch = 8;
+struct CopyBatch {
+  uint64_t off[kCopyBatch], pitch[kCopyBatch], log[kCopyBatch];
+  uint32_t width[kCopyBatch], rows[kCopyBatch];
+  uint32_t start[kCopyBatch + 1];
+  int n;
+};
 
-// The undo log's copy of a contiguous region (n words), as a kernel: inside the block
-// graphs a memcpy node of a device-to-device copy is slower than this.
-__global__ void __launch_bounds__(256) k_run_copy(uint32_t* __restrict__ dst, const uint32_t* __restrict__ src,
-                                                  uint64_t n) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  for (; t + 3 * stride < n; t += 4 * stride) {
-    const uint32_t a = src[t], b = src[t + stride], c = src[t + 2 * stride], d = src[t + 3 * stride];
-    dst[t] = a;
-    dst[t + stride] = b;
-    dst[t + 2 * stride] = c;
-    dst[t + 3 * stride] = d;
+__global__ void __launch_bounds__(256) k_batch_copy(uint32_t* M, uint32_t* L, CopyBatch B, int restore) {
+  const uint32_t total = B.start[B.n];
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    int q = 0;
+    while (q + 1 < B.n && t >= B.start[q + 1]) q++;
+    const uint32_t e = t - B.start[q];
+    uint64_t m;
+    if (B.rows[q] == 1) {
+      m = B.off[q] + e;
+    } else {
+      const uint32_t r = e / B.width[q], col = e - r * B.width[q];
+      m = B.off[q] + (uint64_t)r * B.pitch[q] + col;
+    }
+    const uint64_t l = B.log[q] + e;
+    if (restore) M[m] = L[l];
+    else L[l] = M[m];
   }
-  for (; t < n; t += stride) dst[t] = src[t];
 }
 
 }  // namespace adj
@@ -371,9 +367,10 @@ struct AdjointState {
   std::vector<cudaGraphExec_t> fwd_graph, rev_graph;  // per position in a block
   // runs of periodic halo pairs (ops first..last) replayed and reversed as one launch each
   struct HaloRun {
-    int first, last, nf;
-    float* f[4];
-    adj::HaloRunArgs adj;
+    int first = 0, last = 0, nf = 0;
+    float* f[4] = {nullptr, nullptr, nullptr, nullptr};
+    adj::HaloRunArgs adj{};
+    std::vector<Region> regions;  // the undo-log regions of ops first..last, in op order
   };
   std::vector<HaloRun> runs;
   std::vector<int> run_from, run_to;  // per op: the run it starts / ends, or -1
@@ -498,7 +495,6 @@ void build_tables(Plan& P, AdjointState& S) {
       continue;
     }
     AdjointState::HaloRun R;
-    std::memset(&R, 0, sizeof R);
     R.first = (int)i;
     const Dims& g = ops[i].args.g;
     size_t e = i;
@@ -508,6 +504,7 @@ void build_tables(Plan& P, AdjointState& S) {
       e += 2;
     }
     R.last = (int)e - 1;
+    for (int q = R.first; q <= R.last; q++) R.regions.insert(R.regions.end(), S.regions[q].begin(), S.regions[q].end());
     R.adj.g = g;
     R.adj.nf = R.nf;
     for (int q = 0; q < R.nf; q++) R.adj.l[q] = S.L + (reinterpret_cast<const uint32_t*>(R.f[q]) - M);
@@ -519,24 +516,39 @@ void build_tables(Plan& P, AdjointState& S) {
   S.step = P.active;
 }
 
-// Saves region r of the memory at `at` in the undo log, or restores it from there: a
-// contiguous region by k_run_copy, a pitched one (halo planes) by k_strip_copy.
-void copy_region(Plan& P, const Region& r, uint32_t* at, bool restore) {
-  if (r.rows == 1 || r.width == r.pitch) {
-    const uint64_t n = r.size();
-    const int blocks = (int)std::min<uint64_t>(148 * 8, (n + 1023) / 1024);
-    if (restore) launch_kernel(adj::k_run_copy, dim3(blocks), dim3(256), 0, P.stream, P.M + r.off, (const uint32_t*)at, n);
-    else launch_kernel(adj::k_run_copy, dim3(blocks), dim3(256), 0, P.stream, at, (const uint32_t*)(P.M + r.off), n);
+// Saves the regions of op `i` of the memory in the undo log from word `cur` on, or restores
+// them from there (k_batch_copy: one launch for up to kCopyBatch regions).
+void copy_regions(Plan& P, const std::vector<Region>& regs, uint32_t* log, uint64_t cur, bool restore) {
+  for (size_t q0 = 0; q0 < regs.size(); q0 += adj::kCopyBatch) {
+    adj::CopyBatch B;
+    std::memset(&B, 0, sizeof B);
+    uint64_t total = 0;
+    for (size_t q = q0; q < regs.size() && B.n < adj::kCopyBatch; q++) {
+      const Region& r = regs[q];
+      B.off[B.n] = r.off;
+      B.pitch[B.n] = r.pitch;
+      B.log[B.n] = cur;
+      B.width[B.n] = (uint32_t)r.width;
+      B.rows[B.n] = (uint32_t)r.rows;
+      B.start[B.n] = (uint32_t)total;
+      if (r.width >= (1ull << 32) || r.rows >= (1ull << 32)) throw AdjError(TE_ERANGE, "undo-log region too large");
+      total += r.size();
+      cur += r.size();
+      B.n++;
+    }
+    if (total >= (1ull << 32)) throw AdjError(TE_ERANGE, "undo-log regions of one op of 2^32 words or more");
+    B.start[B.n] = (uint32_t)total;
+    const int blocks = (int)std::min<uint64_t>(148 * 8, (total + 255) / 256);
+    launch_kernel(adj::k_batch_copy, dim3(blocks), dim3(256), 0, P.stream, P.M, log, B, restore ? 1 : 0);
     ACU(cudaGetLastError());
-    return;
   }
-  if (r.size() >= (1ull << 32) || r.width >= (1ull << 32))
-    throw AdjError(TE_ERANGE, "undo-log region of 2^32 words or more");
-  const uint32_t n = (uint32_t)r.size();
-  const int blocks = (int)std::min<uint64_t>(148 * 8, (n + 255) / 256);
-  launch_kernel(adj::k_strip_copy, dim3(blocks), dim3(256), 0, P.stream, P.M, r.off, (uint32_t)r.width, r.pitch, n, at,
-                restore ? 1 : 0);
-  ACU(cudaGetLastError());
+}
+
+// The undo-log words of one op's regions.
+uint64_t regions_words(const std::vector<Region>& regs) {
+  uint64_t n = 0;
+  for (const Region& r : regs) n += r.size();
+  return n;
 }
 
 // Replays the active step op by op, saving each op's written regions at log + cursor.
@@ -545,49 +557,44 @@ void logged_step(Plan& P, AdjointState& S, uint32_t* log) {
   uint64_t cur = 0;
   for (size_t i = 0; i < ops.size(); i++) {
     const int run = S.run_from[i];
-    const size_t last = run >= 0 ? (size_t)S.runs[run].last : i;
-    for (size_t q = i; q <= last; q++)
-      for (const Region& r : S.regions[q]) {
-        copy_region(P, r, log + cur, false);
-        cur += r.size();
-      }
     if (run >= 0) {
       // the pairs' halo fills leave the same memory as the per-dispatch kernels; the
-      // intermediate state between them is never read (their adjoints read no values)
+      // intermediate state between them is never read (their adjoints read no values), so
+      // every op's regions are saved before the run
       const AdjointState::HaloRun& R = S.runs[run];
+      copy_regions(P, R.regions, log, cur, false);
+      cur += regions_words(R.regions);
       launch_periodic_halos(ops[i].args.g, R.f, R.nf, P.stream);
       ACU(cudaGetLastError());
-      i = last;
+      i = (size_t)R.last;
       continue;
     }
+    copy_regions(P, S.regions[i], log, cur, false);
+    cur += regions_words(S.regions[i]);
     P.launch_exact(ops, (int)i, (int)i, false);
   }
 }
 
 // Walks the active step's ops in reverse: restore the op's written regions, run its adjoint.
+// An op's regions are disjoint, except the x and y halo strips of one field in a halo run,
+// whose shared corner words were saved at the same moment and restore the same value.
 void reverse_step(Plan& P, AdjointState& S, const uint32_t* log) {
   std::vector<Op>& ops = P.active->ops;
+  uint32_t* lg = const_cast<uint32_t*>(log);
   uint64_t cur = S.step_undo_words;
   for (size_t ii = ops.size(); ii-- > 0;) {
     const Op& o = ops[ii];
     if (S.run_to[ii] >= 0) {
       const AdjointState::HaloRun& R = S.runs[S.run_to[ii]];
-      for (size_t op = ii + 1; op-- > (size_t)R.first;)
-        for (size_t q = S.regions[op].size(); q-- > 0;) {
-          const Region& r = S.regions[op][q];
-          cur -= r.size();
-          copy_region(P, r, const_cast<uint32_t*>(log + cur), true);
-        }
+      cur -= regions_words(R.regions);
+      copy_regions(P, R.regions, lg, cur, true);
       adj::launch_adj_halo_run(R.adj, P.stream);
       ACU(cudaGetLastError());
       ii = (size_t)R.first;
       continue;
     }
-    for (size_t q = S.regions[ii].size(); q-- > 0;) {
-      const Region& r = S.regions[ii][q];
-      cur -= r.size();
-      copy_region(P, r, const_cast<uint32_t*>(log + cur), true);
-    }
+    cur -= regions_words(S.regions[ii]);
+    copy_regions(P, S.regions[ii], lg, cur, true);
     if (o.copy) {
       const int blocks = (int)std::min<uint64_t>(1024, (o.n + 255) / 256);
       launch_kernel(adj::k_adj_copy, dim3(blocks), dim3(256), 0, P.stream, S.L, o.src, o.dst, o.n);
