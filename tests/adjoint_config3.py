@@ -6,6 +6,9 @@ pytest); two parts, so that the binary64 work runs on any host:
     python -m tests.adjoint_config3 gpu   --out DIR   # on a B200: binary32 gradient + timing
     python -m tests.adjoint_config3 check --out DIR   # on the host: binary64 checks of it
 
+(`profile --steps N` runs one backward of an N-step window inside a profiler range, for an
+ncu launch list.)
+
 `gpu` writes DIR/grad32.npy (the concatenated th', u, v gradient), DIR/gpu.json (J, the
 timing of the plain window, the forward with checkpoints and the backward, device memory).
 `check` computes the binary64 adjoint of the same window (oracle/libadjoint64.so over
@@ -162,13 +165,51 @@ def part_check(out, ndir=16):
     print(json.dumps({k: v for k, v in res.items() if k != 'directions'}))
 
 
+def part_profile(steps):
+    """A `steps`-step window with one checkpoint: forward and backward once, then a second
+    backward between cudaProfilerStart/Stop, so that `ncu --profile-from-start off` lists
+    exactly the launches of one backward (the logged replay, the undo copies and the
+    reverse walk)."""
+    import torch
+    from tests import helpers
+    from thunderengine_web_b200.adjoint import CoreWindow
+    run = make_run()
+    tape = run.tape(1)
+    r = helpers.gpu_replayer(tape, run.initial_buffers(), hashes=False)
+    r.encode_steps(1)
+    r.sync()
+    init = {b['id']: r.read(b['length'] // 4, r.base[b['id']]).tobytes() for b in tape['buffers']}
+    r.close()
+    g = run.grid
+    win = CoreWindow(run, init, steps, checkpoint_every=steps)
+    arena = np.frombuffer(init[run.rec.ids['arena']], dtype=np.float32)
+    ctl = [arena[run.fields[n] // 4:run.fields[n] // 4 + g.count].reshape(g.nz + 1, g.strideK, g.strideJ)
+           [:g.nz, 3:3 + g.ny, 3:3 + g.nx] for n in ('th', 'u', 'v')]
+    win.forward(*ctl)
+    gw = 2.0 * win.read_w().astype(np.float64)
+    win.backward(gw)
+    win.r.sync()
+    t0 = time.perf_counter()
+    win.backward(gw)
+    win.r.sync()
+    print(json.dumps({'steps': steps, 'backward_s': time.perf_counter() - t0}))
+    torch.cuda.profiler.start()
+    win.backward(gw)
+    win.r.sync()
+    torch.cuda.profiler.stop()
+    win.close()
+
+
 if __name__ == '__main__':
     ap = argparse.ArgumentParser()
-    ap.add_argument('part', choices=['gpu', 'check'])
+    ap.add_argument('part', choices=['gpu', 'check', 'profile'])
     ap.add_argument('--out', default='gpurun_out/adjoint_config3')
     ap.add_argument('--directions', type=int, default=16)
+    ap.add_argument('--steps', type=int, default=2, help='window of the profile part')
     a = ap.parse_args()
     if a.part == 'gpu':
         part_gpu(a.out)
+    elif a.part == 'profile':
+        part_profile(a.steps)
     else:
         part_check(a.out, a.directions)
