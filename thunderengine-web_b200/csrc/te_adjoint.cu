@@ -349,7 +349,14 @@ __global__ void __launch_bounds__(256) k_batch_copy(uint32_t* M, uint32_t* L, Co
 // A written region in words: `rows` rows of `width` words, `pitch` words apart.
 struct Region {
   uint64_t off, width, pitch, rows;
+  uint64_t field;  // word offset of the field (binding) the region belongs to
   uint64_t size() const { return width * rows; }
+  uint64_t last() const { return off + (rows - 1) * pitch + width - 1; }
+  // every word of r lies in this region (a contiguous region, or the same pitched strip)
+  bool covers(const Region& r) const {
+    if (rows == 1) return off <= r.off && r.last() <= off + width - 1;
+    return off == r.off && width == r.width && pitch == r.pitch && rows == r.rows;
+  }
 };
 
 struct AdjointState {
@@ -414,6 +421,8 @@ AdjointState& state(Plan& P) {
   return *P.adjoint;
 }
 
+uint64_t regions_words(const std::vector<Region>& regs);
+
 // Per-op tables of the active step: written regions, adjoint arguments and operators.
 void build_tables(Plan& P, AdjointState& S) {
   if (S.step == P.active && !S.args.empty()) return;
@@ -426,19 +435,24 @@ void build_tables(Plan& P, AdjointState& S) {
   const uint32_t* M = P.M;
   // the memory regions whose values before an op some adjoint operator reads
   std::set<uint64_t> read;
-  for (const Op& o : ops) {
+  std::vector<std::vector<uint64_t>> reads(ops.size());  // per op: the fields its adjoint reads
+  for (size_t i = 0; i < ops.size(); i++) {
+    const Op& o = ops[i];
     if (o.copy) continue;
     if (!o.spec) throw AdjError(TE_ENOKERNEL, "no CUDA kernel for " + o.name);
     const adj::AdjEntry* e = adj::find_adjoint(o.name);
     if (!e) throw AdjError(TE_ENOKERNEL, "no adjoint operator for " + o.name);
     for (auto& kv : o.bind)
-      if (kv.first < 64 && (e->reads >> kv.first & 1u)) read.insert(kv.second);
+      if (kv.first < 64 && (e->reads >> kv.first & 1u)) {
+        read.insert(kv.second);
+        reads[i].push_back(kv.second);
+      }
   }
   for (size_t i = 0; i < ops.size(); i++) {
     const Op& o = ops[i];
     if (o.copy) {
       if (read.count(o.dst)) {
-        S.regions[i].push_back({o.dst, o.n, o.n, 1});
+        S.regions[i].push_back({o.dst, o.n, o.n, 1, o.dst});
         S.step_undo_words += o.n;
       }
       continue;
@@ -456,17 +470,17 @@ void build_tables(Plan& P, AdjointState& S) {
         // the halo points only: 3 columns (rows) below the interior and 4 above
         const uint64_t sJ = g.sJ, sK = g.sK, lv = (uint64_t)g.nz + 1;
         if (halo_x) {
-          S.regions[i].push_back({f0, 3, sJ, sK * lv});
-          S.regions[i].push_back({f0 + (uint64_t)g.nx + 3, 4, sJ, sK * lv});
+          S.regions[i].push_back({f0, 3, sJ, sK * lv, f0});
+          S.regions[i].push_back({f0 + (uint64_t)g.nx + 3, 4, sJ, sK * lv, f0});
         } else {
-          S.regions[i].push_back({f0, 3 * sJ, sJ * sK, lv});
-          S.regions[i].push_back({f0 + ((uint64_t)g.ny + 3) * sJ, 4 * sJ, sJ * sK, lv});
+          S.regions[i].push_back({f0, 3 * sJ, sJ * sK, lv, f0});
+          S.regions[i].push_back({f0 + ((uint64_t)g.ny + 3) * sJ, 4 * sJ, sJ * sK, lv, f0});
         }
         S.step_undo_words += S.regions[i][S.regions[i].size() - 2].size() + S.regions[i].back().size();
         continue;
       }
       const uint64_t len = P.region_len(f0);
-      S.regions[i].push_back({f0, len, len, 1});
+      S.regions[i].push_back({f0, len, len, 1, f0});
       S.step_undo_words += len;
     }
     adj::AdjArgs<float>& a = S.args[i];
@@ -483,6 +497,35 @@ void build_tables(Plan& P, AdjointState& S) {
       a.iv[n] = o.args.iv[n];
       a.iv2[n] = o.args.iv2[n];
     }
+  }
+  // A region's values before op i are needed only if some adjoint reads its field between
+  // the previous op that wrote all of the region (whose own restore then brings the field
+  // back for the adjoints before it) and op i, op i's own adjoint included.  The ops of a
+  // step repeat every step, so that previous writer is searched cyclically; the block's
+  // first step ends its reverse walk with fields some adjoint no longer reads left at later
+  // values, which the next block's checkpoint (or the final restore) replaces.
+  {
+    const size_t n = ops.size();
+    auto reads_field = [&](size_t k, uint64_t f) {
+      return std::find(reads[k].begin(), reads[k].end(), f) != reads[k].end();
+    };
+    std::vector<std::vector<Region>> kept(n);
+    for (size_t i = 0; i < n; i++)
+      for (const Region& r : S.regions[i]) {
+        bool need = reads_field(i, r.field);
+        for (size_t step = 1; step < n && !need; step++) {
+          const size_t k = (i + n - step) % n;
+          bool covered = false;
+          for (const Region& w : S.regions[k])
+            if (w.field == r.field && w.covers(r)) covered = true;
+          if (covered) break;
+          need = reads_field(k, r.field);
+        }
+        if (need) kept[i].push_back(r);
+      }
+    S.regions.swap(kept);
+    S.step_undo_words = 0;
+    for (const auto& rs : S.regions) S.step_undo_words += regions_words(rs);
   }
   // runs of bc_periodic_x/y pairs on up to 4 distinct fields of the same grid
   S.runs.clear();
