@@ -203,7 +203,7 @@ def part_profile(steps):
 if __name__ == '__main__':
     ap = argparse.ArgumentParser()
     ap.add_argument('part', choices=['gpu', 'check', 'profile'])
-    ap.add_argument('--out', default='gpurun_out/adjoint_config3')
+    ap.add_argument('--out', default='adjoint_config3_out')
     ap.add_argument('--directions', type=int, default=16)
     ap.add_argument('--steps', type=int, default=2, help='window of the profile part')
     a = ap.parse_args()
