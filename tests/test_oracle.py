@@ -70,6 +70,33 @@ def test_wgsl_pow_is_correctly_rounded(oracle_lib):
     assert p(8.0, 0.33333334) == 2.0 and p(1.0, 0.33333334) == 1.0 and p(0.0, 0.33333334) == 0.0
     assert math.isnan(p(-1.0, 0.33333334))
 
+
+def test_wgsl_log2_and_atan2_are_correctly_rounded(oracle_lib):
+    """te_log2_f64 and te_atan2_f64 (the WGSL log2 and atan2 builtins of morr_refl10cm.wgsl,
+    evaluated in binary64 like the CUDA kernels) against the binary64 functions rounded once
+    to binary32 on seeded normal arguments of every sign and octant, and the zero and
+    infinity cases of C's atan2f."""
+    L = oracle_lib.lib
+    L.te_log2_f64.restype = ctypes.c_float
+    L.te_log2_f64.argtypes = [ctypes.c_float]
+    L.te_atan2_f64.restype = ctypes.c_float
+    L.te_atan2_f64.argtypes = [ctypes.c_float, ctypes.c_float]
+    rng = np.random.default_rng(5)
+    xs = (10.0 ** rng.uniform(-30, 30, 4000)).astype(np.float32)
+    for x in xs:
+        assert L.te_log2_f64(float(x)) == np.float32(math.log2(float(x))), x
+    ys = (10.0 ** rng.uniform(-20, 20, 4000) * rng.choice([-1.0, 1.0], 4000)).astype(np.float32)
+    zs = (10.0 ** rng.uniform(-20, 20, 4000) * rng.choice([-1.0, 1.0], 4000)).astype(np.float32)
+    for y, x in zip(ys, zs):
+        assert L.te_atan2_f64(float(y), float(x)) == np.float32(math.atan2(float(y), float(x))), (y, x)
+    special = [0.0, -0.0, 1.0, -1.0, math.inf, -math.inf]
+    for y in special:
+        for x in special:
+            got, want = np.float32(L.te_atan2_f64(y, x)), np.float32(math.atan2(y, x))
+            assert got.tobytes() == want.tobytes(), (y, x)
+    assert L.te_log2_f64(1.0) == 0.0 and L.te_log2_f64(0.5) == -1.0 and L.te_log2_f64(0.0) == -math.inf
+    assert math.isnan(L.te_log2_f64(-1.0))
+
 def test_oracle_equals_reference_kernels_on_synthetic_step(oracle_lib, ref_lib, kernels_meta):
     """Hand-written oracle vs the reference's own kernels: every word after 2 steps."""
     run = timestep.Run(scenario.tiny(16, 12, 10))
