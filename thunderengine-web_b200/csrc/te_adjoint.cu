@@ -248,13 +248,14 @@ static const AdjEntry* find_adjoint(const std::string& name) {
   return nullptr;
 }
 
-// adjoint of a copy dst <- src (disjoint ranges): lambda_src += lambda_dst, lambda_dst = 0
-__global__ void k_adj_copy(float* L, uint64_t src, uint64_t dst, uint64_t n) {
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-    const float x = L[dst + i];
-    L[dst + i] = 0.0f;
-    L[src + i] += x;
-  }
+// adjoint of a copy dst <- src (disjoint ranges): lambda_src += lambda_dst, lambda_dst = 0;
+// one word per thread, both loads before the stores
+__global__ void __launch_bounds__(256) k_adj_copy(float* L, uint64_t src, uint64_t dst, uint64_t n) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float x = L[dst + i], y = L[src + i];
+  L[dst + i] = 0.0f;
+  L[src + i] = y + x;
 }
 
 // Adjoint of a run of periodic halo pairs (bc_periodic_x(f) then bc_periodic_y(f)) on up
@@ -639,8 +640,9 @@ void reverse_step(Plan& P, AdjointState& S, const uint32_t* log) {
     cur -= regions_words(S.regions[ii]);
     copy_regions(P, S.regions[ii], lg, cur, true);
     if (o.copy) {
-      const int blocks = (int)std::min<uint64_t>(1024, (o.n + 255) / 256);
-      launch_kernel(adj::k_adj_copy, dim3(blocks), dim3(256), 0, P.stream, S.L, o.src, o.dst, o.n);
+      if ((o.n + 255) / 256 > 0x7fffffffu) throw AdjError(TE_ERANGE, "copy of 2^39 words or more");
+      launch_kernel(adj::k_adj_copy, dim3((unsigned)((o.n + 255) / 256)), dim3(256), 0, P.stream, S.L, o.src, o.dst,
+                    o.n);
     } else {
       S.launch[ii](S.args[ii], P.stream);
     }
