@@ -144,13 +144,15 @@ __global__ void __launch_bounds__(kAdjCols * kAdjWarps) k_adj_wsolve_coop(AdjArg
     }
   __syncthreads();
   if (wq == 0 && on) {
+    // Thomas sweep of the transposed system: one correctly rounded reciprocal per level on
+    // the serial chain instead of two divisions
     float cp = 0.0f, dp = 0.0f;
     for (int k = 1; k <= nz - 1; k++) {
       const int e = k * kAdjCols + lane;
       const float sub = sSub[e];
-      const float den = sDia[e] - sub * cp;
-      cp = sSup[e] / den;
-      dp = (sRhs[e] - sub * dp) / den;
+      const float r = __frcp_rn(sDia[e] - sub * cp);
+      cp = sSup[e] * r;
+      dp = (sRhs[e] - sub * dp) * r;
       sSup[e] = cp;
       sRhs[e] = dp;
     }
